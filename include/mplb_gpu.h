@@ -1,0 +1,207 @@
+/*
+ * mplb_gpu.h -- C-ABI of the B200 lattice update for multiphaseLB.
+ *
+ * The reference advances its lattice with a fixed sequence of C calls on
+ * host structures (src/applications/solvers/multiPhasePP/multiPhasePP.c:157-240):
+ *
+ *     collision(f) lbstream(f) updateBoundaries(f)
+ *     collision(g) lbstream(g) updateBoundaries(g)
+ *     macroDensity  heatSource  macroTemperature  interForce  macroVelocity
+ *
+ * This header replaces that sequence with one device-resident handle.  The
+ * reference's readers, dictionaries and writers stay on the host; the driver
+ * packs what they produced into the plain descriptors below (flat arrays,
+ * sizes, no pointers-to-rows, no CUDA or torch types) and calls
+ * mplb_gpu_create once, mplb_gpu_step in its time loop, and
+ * mplb_gpu_download at write steps.  include/mplb_gpu_reference.h does the
+ * packing from the reference's own structs.
+ *
+ * Conventions
+ *  - Every function returns 0 on success and a negative MPLB_E* code on
+ *    failure; mplb_gpu_last_error() then describes the failure (per thread).
+ *    The library never exits, aborts or traps; the reference's errorMsg()
+ *    (src/basic/errorMsg.c:6-12, print + exit(1)) becomes a return code the
+ *    driver may pass to errorMsg itself.
+ *  - Host arrays use the reference's row-major layouts: PDFs [node][k]
+ *    (lbeField.value, src/dataTypes/lbeField.h:53), vectors [node][3]
+ *    (macroFields.U/Fi/Ft, src/dataTypes/macroFields.h:33-48), scalars [node].
+ *  - Arithmetic is IEEE binary64, the reference's DP build
+ *    (src/dataTypes/dataTypes.h:19-21).
+ *  - A handle is bound to one device and one CUDA stream and is not
+ *    thread-safe, like one reference MPI rank.
+ */
+#ifndef MPLB_GPU_H
+#define MPLB_GPU_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define MPLB_ABI_VERSION 1
+#define MPLB_MAX_Q 15
+#define MPLB_MAX_PATCHES 64
+
+/* Lattice models; same order as DdQq (src/dataTypes/latticeInfo.h:21-24). */
+enum { MPLB_D2Q9 = 0, MPLB_D3Q15 = 1 };
+
+/* Collision models; same values as lbeModel (src/lbEquation/lbeModel.h:4-22). */
+enum { MPLB_LIMRT = 0, MPLB_MYMRT = 1, MPLB_XUMRT = 2, MPLB_LITEMPMRT = 3, MPLB_NO_MODEL = -1 };
+
+/* Equations of state; same values as eosType (src/EOS/EOSInfo.h:17-31). */
+enum { MPLB_EOS_IDEAL = 0, MPLB_EOS_CS = 1, MPLB_EOS_PR = 2, MPLB_EOS_VDW = 3 };
+
+/* Boundary types; same values as bdType (src/boundary/bdType.h:4-33). */
+enum {
+    MPLB_BC_BOUNCEBACK = 0, MPLB_BC_FIXEDT = 1, MPLB_BC_FIXEDRANDOMT = 2,
+    MPLB_BC_FIXEDGRADT = 3, MPLB_BC_FIXEDU = 4, MPLB_BC_UHF = 5,
+    MPLB_BC_FIXEDEOSP = 6, MPLB_BC_OUTFLOW = 7, MPLB_BC_PERIODIC = 8
+};
+
+/* Field selectors for the per-operator entry points. */
+enum { MPLB_FIELD_F = 0, MPLB_FIELD_G = 1 };
+
+/* Storage precision of the PDFs. */
+enum { MPLB_FP64 = 0 };
+
+/* Execution path. */
+enum {
+    MPLB_PATH_AUTO = 0,      /* fused box kernels when the mesh is a box, else operators */
+    MPLB_PATH_OPERATORS = 1, /* one kernel per reference operator, neighbour-table driven */
+    MPLB_PATH_FUSED = 2      /* fused box kernels; create fails if the mesh is not a box */
+};
+
+/* Error codes. */
+enum {
+    MPLB_OK = 0,
+    MPLB_E_ARG = -1,         /* invalid argument or descriptor */
+    MPLB_E_UNSUPPORTED = -2, /* model / boundary / option outside the path */
+    MPLB_E_CUDA = -3,        /* CUDA runtime error */
+    MPLB_E_STATE = -4,       /* call not valid in the handle's current state */
+    MPLB_E_NONFINITE = -5    /* NaN/Inf found by a check */
+};
+
+/*
+ * Mesh of the single GPU domain.  Replaces latticeMesh.mesh
+ * (src/dataTypes/basicMesh.h:39-70) for one rank with no ghosts
+ * (nPoints == nlocal).
+ */
+typedef struct mplb_mesh_desc {
+    int32_t lattice;              /* MPLB_D2Q9 or MPLB_D3Q15 */
+    uint32_t n_points;            /* number of nodes */
+    const int32_t* nb;            /* [n_points][Q]: node at x - c_k (pull source), -1 = none */
+    const int32_t* points;        /* [n_points][3] integer coordinates, or NULL */
+    uint32_t n_patches;           /* boundary patches, in file order (basicBoundary.nbd) */
+    const uint32_t* patch_count;  /* [n_patches] nodes per patch (nbdelem) */
+    const uint32_t* patch_nodes;  /* concatenation of the patches' node lists (bdPoints) */
+} mplb_mesh_desc;
+
+/* Equation of state and body forces; replaces EOSInfo (src/EOS/EOSInfo.h:80-102). */
+typedef struct mplb_eos_desc {
+    int32_t type;   /* MPLB_EOS_* */
+    double a, b;    /* a_cs|a_pr|a_vdw, b_cs|b_pr|b_vdw */
+    double w;       /* w_pr (Peng-Robinson acentric factor) */
+    double R, G, M, Cv;
+    double g[3];    /* gravity */
+    double fext[3]; /* constant external force, applied off-boundary only */
+    double rho_0;   /* buoyancy reference density */
+} mplb_eos_desc;
+
+/*
+ * One population field; replaces lbeField's model, constants, update flag
+ * and boundary table (src/dataTypes/lbeField.h:49-108,
+ * src/lbEquation/lbParameters.h:16-31).
+ */
+typedef struct mplb_field_desc {
+    int32_t model;            /* MPLB_LIMRT, MPLB_XUMRT, MPLB_LITEMPMRT or MPLB_NO_MODEL */
+    int32_t update;           /* 0 = frozen (reference --frozen / --nht) */
+    double Lambda[MPLB_MAX_Q];
+    double sigma;             /* liMRT / xuMRT force coefficient */
+    int32_t surface_tension;  /* must be 0: surface-tension terms are outside this path */
+    double kappa_st;
+    const int32_t* bc_type;   /* [n_patches] MPLB_BC_* for this field */
+    const double* bc_value;   /* [n_patches][3]: fixedT uses [0], fixedU uses [0..2] */
+} mplb_field_desc;
+
+typedef struct mplb_opts {
+    int32_t precision;   /* MPLB_FP64 */
+    int32_t path;        /* MPLB_PATH_* */
+    int32_t device;      /* CUDA device ordinal; -1 = the calling thread's current device */
+    void* stream;        /* cudaStream_t to launch on; NULL = a stream owned by the handle */
+    uint32_t start_time; /* reference timeInfo.start: the time the first step leaves */
+} mplb_opts;
+
+/* What create decided; filled by mplb_gpu_info. */
+typedef struct mplb_info {
+    int32_t path;            /* MPLB_PATH_OPERATORS or MPLB_PATH_FUSED */
+    int32_t box_dims[3];     /* box extents when the mesh is a box, else 0 */
+    int32_t box_periodic[3]; /* 1 = axis wraps */
+    int32_t bc_sequential;   /* 1 = boundary updates run in the reference's serial order */
+    uint32_t current_time;   /* reference timeInfo.current */
+    uint64_t device_bytes;   /* device memory held by the handle */
+    uint64_t kernel_launches;/* kernels this handle has launched so far */
+} mplb_info;
+
+typedef struct mplb_gpu mplb_gpu_t;
+
+const char* mplb_gpu_version(void);
+const char* mplb_gpu_last_error(void);
+
+/* Build the device lattice.  Fields start at zero; upload them next. */
+int mplb_gpu_create(const mplb_mesh_desc* mesh, const mplb_eos_desc* eos,
+                    const mplb_field_desc* f, const mplb_field_desc* g,
+                    const mplb_opts* opts, mplb_gpu_t** out);
+int mplb_gpu_destroy(mplb_gpu_t* h);
+int mplb_gpu_info(mplb_gpu_t* h, mplb_info* info);
+
+/* Host -> device.  Any pointer may be NULL (field left as is).
+ * rho/T/S/p: [n]; U/Fi/Ft: [n][3]; f: [n][Q]; g: [n][Q]. */
+int mplb_gpu_upload(mplb_gpu_t* h, const double* rho, const double* U, const double* T,
+                    const double* f, const double* g, const double* S,
+                    const double* Fi, const double* Ft);
+/* Device -> host, same layouts; any pointer may be NULL. */
+int mplb_gpu_download(mplb_gpu_t* h, double* rho, double* U, double* T,
+                      double* Fi, double* Ft, double* S, double* f, double* g);
+
+/* Reference start-up (multiPhasePP.c:122-147): equilibrium(f), equilibrium(g),
+ * interForce, heatSource at time.current == start_time. */
+int mplb_gpu_initialize(mplb_gpu_t* h);
+
+/* Advance nsteps time steps, each exactly multiPhasePP.c:157-240 without the
+ * write block.  The handle's state is the reference's state after every call. */
+int mplb_gpu_step(mplb_gpu_t* h, uint32_t nsteps);
+
+/* Per-operator entry points, same names and semantics as
+ * src/lbEquation/general/generalLbe.h and src/lbEquation/pseudoPot/interForce.c.
+ * Each honours the field's update flag like the reference does. */
+int mplb_gpu_equilibrium(mplb_gpu_t* h, int32_t field);                 /* general/equilibrium.c:6-90 */
+int mplb_gpu_collision(mplb_gpu_t* h, int32_t field);                   /* general/collision.c:6-67 */
+int mplb_gpu_lbstream(mplb_gpu_t* h, int32_t field);                    /* general/lbstream.c:5-72 */
+int mplb_gpu_update_boundaries(mplb_gpu_t* h, int32_t field);           /* general/updateBoundaries.c:6-75 */
+int mplb_gpu_macro_density(mplb_gpu_t* h, uint32_t start, uint32_t end);    /* general/macroDensity.c:7-75 */
+int mplb_gpu_macro_velocity(mplb_gpu_t* h, uint32_t start, uint32_t end);   /* general/macroVelocity.c:6-65 */
+int mplb_gpu_macro_temperature(mplb_gpu_t* h, uint32_t start, uint32_t end);/* general/macroTemperature.c:7-68 */
+int mplb_gpu_inter_force(mplb_gpu_t* h);                                /* pseudoPot/interForce.c:7-52 */
+int mplb_gpu_heat_source(mplb_gpu_t* h);                                /* general/heatSource.c:7-202 */
+
+/* Time and buoyancy reference density (timeInfo.current, EOSInfo.rho_0). */
+int mplb_gpu_set_time(mplb_gpu_t* h, uint32_t current);
+int mplb_gpu_set_rho0(mplb_gpu_t* h, double rho_0);
+/* averageScalarField(rho) on the device (src/basic/averageScalarField.c:4-78):
+ * 0 if the current rho_0 <= 0, else the mean density summed in node order.
+ * The result is stored as the new rho_0 and returned in *rho_0. */
+int mplb_gpu_average_rho0(mplb_gpu_t* h, double* rho_0);
+
+/* Conservation checks: total mass sum(rho) and thermal energy sum(T) over all
+ * nodes, FP64 warp-shuffle tree reduction (not the reference's summation order). */
+int mplb_gpu_mass_energy(mplb_gpu_t* h, double* mass, double* energy);
+
+/* Wait for the handle's stream. */
+int mplb_gpu_sync(mplb_gpu_t* h);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* MPLB_GPU_H */

@@ -1,0 +1,146 @@
+"""ctypes mirror of include/mplb_gpu.h.
+
+The C header is the contract; these Structure classes must match it field
+for field.  tests/test_abi.py checks the sizes against the compiled library.
+"""
+import ctypes as C
+
+MAX_Q = 15
+MAX_PATCHES = 64
+
+D2Q9, D3Q15 = 0, 1
+LIMRT, MYMRT, XUMRT, LITEMPMRT, NO_MODEL = 0, 1, 2, 3, -1
+EOS_IDEAL, EOS_CS, EOS_PR, EOS_VDW = 0, 1, 2, 3
+(BC_BOUNCEBACK, BC_FIXEDT, BC_FIXEDRANDOMT, BC_FIXEDGRADT, BC_FIXEDU, BC_UHF,
+ BC_FIXEDEOSP, BC_OUTFLOW, BC_PERIODIC) = range(9)
+FIELD_F, FIELD_G = 0, 1
+FP64 = 0
+PATH_AUTO, PATH_OPERATORS, PATH_FUSED = 0, 1, 2
+
+OK, E_ARG, E_UNSUPPORTED, E_CUDA, E_STATE, E_NONFINITE = 0, -1, -2, -3, -4, -5
+
+Q_OF = {D2Q9: 9, D3Q15: 15}
+
+
+class MeshDesc(C.Structure):
+    _fields_ = [
+        ("lattice", C.c_int32),
+        ("n_points", C.c_uint32),
+        ("nb", C.POINTER(C.c_int32)),
+        ("points", C.POINTER(C.c_int32)),
+        ("n_patches", C.c_uint32),
+        ("patch_count", C.POINTER(C.c_uint32)),
+        ("patch_nodes", C.POINTER(C.c_uint32)),
+    ]
+
+
+class EosDesc(C.Structure):
+    _fields_ = [
+        ("type", C.c_int32),
+        ("a", C.c_double), ("b", C.c_double), ("w", C.c_double),
+        ("R", C.c_double), ("G", C.c_double), ("M", C.c_double), ("Cv", C.c_double),
+        ("g", C.c_double * 3),
+        ("fext", C.c_double * 3),
+        ("rho_0", C.c_double),
+    ]
+
+
+class FieldDesc(C.Structure):
+    _fields_ = [
+        ("model", C.c_int32),
+        ("update", C.c_int32),
+        ("Lambda", C.c_double * MAX_Q),
+        ("sigma", C.c_double),
+        ("surface_tension", C.c_int32),
+        ("kappa_st", C.c_double),
+        ("bc_type", C.POINTER(C.c_int32)),
+        ("bc_value", C.POINTER(C.c_double)),
+    ]
+
+
+class Opts(C.Structure):
+    _fields_ = [
+        ("precision", C.c_int32),
+        ("path", C.c_int32),
+        ("device", C.c_int32),
+        ("stream", C.c_void_p),
+        ("start_time", C.c_uint32),
+    ]
+
+
+class Info(C.Structure):
+    _fields_ = [
+        ("path", C.c_int32),
+        ("box_dims", C.c_int32 * 3),
+        ("box_periodic", C.c_int32 * 3),
+        ("bc_sequential", C.c_int32),
+        ("current_time", C.c_uint32),
+        ("device_bytes", C.c_uint64),
+        ("kernel_launches", C.c_uint64),
+    ]
+
+
+def dptr(a):
+    """double* of a contiguous float64 numpy array, or NULL for None."""
+    if a is None:
+        return None
+    assert a.dtype.name == "float64" and a.flags["C_CONTIGUOUS"]
+    return a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+def iptr(a):
+    if a is None:
+        return None
+    assert a.dtype.name == "int32" and a.flags["C_CONTIGUOUS"]
+    return a.ctypes.data_as(C.POINTER(C.c_int32))
+
+
+def uptr(a):
+    if a is None:
+        return None
+    assert a.dtype.name == "uint32" and a.flags["C_CONTIGUOUS"]
+    return a.ctypes.data_as(C.POINTER(C.c_uint32))
+
+
+class Descriptors:
+    """Owns the numpy buffers behind a (mesh, eos, f, g) descriptor set so the
+    pointers stay valid while a library handle is being created."""
+
+    def __init__(self, case):
+        import numpy as np
+        self.case = case
+        self.nb = np.ascontiguousarray(case.nb, dtype=np.int32)
+        self.points = np.ascontiguousarray(case.points, dtype=np.int32)
+        self.patch_count = np.ascontiguousarray([len(p) for p in case.patches], dtype=np.uint32)
+        if case.patches:
+            self.patch_nodes = np.ascontiguousarray(np.concatenate(
+                [np.asarray(p, dtype=np.uint32) for p in case.patches]), dtype=np.uint32)
+        else:
+            self.patch_nodes = np.zeros(1, dtype=np.uint32)
+        self.mesh = MeshDesc(case.lattice, case.n, iptr(self.nb), iptr(self.points),
+                             len(case.patches), uptr(self.patch_count), uptr(self.patch_nodes))
+        e = case.eos
+        self.eos = EosDesc(e["type"], e.get("a", 0.0), e.get("b", 0.0), e.get("w", 0.0),
+                           e.get("R", 1.0), e.get("G", -1.0), e.get("M", 1.0), e.get("Cv", 1.0),
+                           (C.c_double * 3)(*e.get("g", (0.0, 0.0, 0.0))),
+                           (C.c_double * 3)(*e.get("fext", (0.0, 0.0, 0.0))),
+                           e.get("rho_0", 0.0))
+        self._keep = []
+        self.f = self._field(case.f, len(case.patches))
+        self.g = self._field(case.g, len(case.patches))
+
+    def _field(self, fd, npatch):
+        import numpy as np
+        if fd is None:
+            d = FieldDesc()
+            d.model = NO_MODEL
+            return d
+        lam = list(fd["Lambda"]) + [0.0] * (MAX_Q - len(fd["Lambda"]))
+        bct = np.ascontiguousarray(fd.get("bc_type", [BC_PERIODIC] * npatch), dtype=np.int32)
+        bcv = np.ascontiguousarray(fd.get("bc_value", np.zeros((npatch, 3))), dtype=np.float64).reshape(-1)
+        if bct.size == 0:
+            bct = np.zeros(1, dtype=np.int32)
+            bcv = np.zeros(3, dtype=np.float64)
+        self._keep += [bct, bcv]
+        return FieldDesc(fd["model"], int(fd.get("update", 1)), (C.c_double * MAX_Q)(*lam),
+                         fd.get("sigma", 0.0), 0, 0.0, iptr(bct), dptr(bcv))

@@ -1,0 +1,67 @@
+/*
+ * Single-rank stand-in for <mpi.h>, used ONLY to compile the reference's
+ * hot-path C sources into the parity checker under oracle/_ref/.
+ *
+ * This is test infrastructure, not product code.  Every call behaves as if
+ * the job had exactly one rank: rank 0, world size 1.  At world size 1 the
+ * reference never posts a message (sendPdfField.c:10 returns early, the
+ * sync* helpers loop over zero peers), so the point-to-point calls below are
+ * never reached with real traffic; they exist so the sources link.
+ */
+#ifndef MPLB_ORACLE_MPI_STUB_H
+#define MPLB_ORACLE_MPI_STUB_H
+
+#include <string.h>
+
+typedef int MPI_Comm;
+typedef int MPI_Datatype;
+typedef int MPI_Op;
+typedef int MPI_Request;
+typedef int MPI_Info;
+typedef long long MPI_Offset;
+typedef int MPI_File;
+typedef struct { int MPI_SOURCE, MPI_TAG, MPI_ERROR; } MPI_Status;
+
+#define MPI_COMM_WORLD 0
+#define MPI_SUCCESS 0
+#define MPI_CHAR 1
+#define MPI_INT 2
+#define MPI_FLOAT 3
+#define MPI_DOUBLE 4
+#define MPI_SUM 1
+#define MPI_INFO_NULL 0
+#define MPI_STATUS_IGNORE ((MPI_Status*)0)
+#define MPI_STATUSES_IGNORE ((MPI_Status*)0)
+#define MPI_MODE_CREATE 1
+#define MPI_MODE_WRONLY 2
+#define MPI_MODE_RDONLY 4
+#define MPI_SEEK_SET 0
+
+static inline size_t mplb_stub_size(MPI_Datatype t) {
+    switch (t) {
+    case MPI_CHAR: return 1;
+    case MPI_INT: return sizeof(int);
+    case MPI_FLOAT: return sizeof(float);
+    default: return sizeof(double);
+    }
+}
+
+static inline int MPI_Init(int* c, char*** v) { (void)c; (void)v; return 0; }
+static inline int MPI_Finalize(void) { return 0; }
+static inline int MPI_Comm_rank(MPI_Comm c, int* r) { (void)c; *r = 0; return 0; }
+static inline int MPI_Comm_size(MPI_Comm c, int* s) { (void)c; *s = 1; return 0; }
+static inline int MPI_Barrier(MPI_Comm c) { (void)c; return 0; }
+static inline int MPI_Isend(const void* b, int n, MPI_Datatype t, int d, int tag, MPI_Comm c, MPI_Request* r)
+{ (void)b; (void)n; (void)t; (void)d; (void)tag; (void)c; *r = 0; return 0; }
+static inline int MPI_Irecv(void* b, int n, MPI_Datatype t, int s, int tag, MPI_Comm c, MPI_Request* r)
+{ (void)b; (void)n; (void)t; (void)s; (void)tag; (void)c; *r = 0; return 0; }
+static inline int MPI_Send(const void* b, int n, MPI_Datatype t, int d, int tag, MPI_Comm c)
+{ (void)b; (void)n; (void)t; (void)d; (void)tag; (void)c; return 0; }
+static inline int MPI_Recv(void* b, int n, MPI_Datatype t, int s, int tag, MPI_Comm c, MPI_Status* st)
+{ (void)b; (void)n; (void)t; (void)s; (void)tag; (void)c; (void)st; return 0; }
+static inline int MPI_Waitall(int n, MPI_Request* r, MPI_Status* s) { (void)n; (void)r; (void)s; return 0; }
+/* One rank: the reduction of a single contribution is the contribution. */
+static inline int MPI_Allreduce(const void* in, void* out, int n, MPI_Datatype t, MPI_Op op, MPI_Comm c)
+{ (void)op; (void)c; memcpy(out, in, (size_t)n * mplb_stub_size(t)); return 0; }
+
+#endif

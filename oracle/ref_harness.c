@@ -1,0 +1,304 @@
+/*
+ * ref_harness.c -- parity checker built from the reference's OWN sources.
+ *
+ * TEST INFRASTRUCTURE ONLY.  Linked with the reference's hot-path C files
+ * (compiled in place from the reference tree by oracle/Makefile) into
+ * oracle/_ref/libmplb_ref.so.  Only tests/, the smoke check and bench.py's
+ * CPU-baseline leg load it.
+ *
+ * The harness builds the reference's host structures (latticeMesh,
+ * macroFields, lbeField) in memory from the flat descriptors of
+ * include/mplb_gpu.h instead of reading dictionary and mesh files, and then
+ * calls the reference's functions in the order of its solver:
+ *   start-up   multiPhasePP.c:122-147 (equilibrium f, g; interForce; heatSource)
+ *   time step  multiPhasePP.c:157-240 (collision/lbstream/updateBoundaries f, g;
+ *              macroDensity; heatSource; macroTemperature; interForce;
+ *              macroVelocity), with updateTime() semantics for time.current
+ *              (src/IO/time/timeOptions.c:35-64).
+ * Results are copied out as doubles, so no float-precision writer is involved.
+ */
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+#include <stdint.h>
+
+#include <latticeMesh.h>
+#include <macroFields.h>
+#include <lbeField.h>
+#include <latticeModel.h>
+#include <basic.h>
+#include <generalLbe.h>
+#include <pseudoPot.h>
+
+#include "../include/mplb_gpu.h"
+
+typedef struct ref_case {
+    latticeMesh mesh;
+    macroFields mf;
+    lbeField f, g;
+    int has_f, has_g;
+    int Q;
+    uint32_t n;
+} ref_case;
+
+static double** rows_alloc(uint32_t n, uint32_t m) {
+    double** r = (double**)malloc((size_t)n * sizeof(double*));
+    for (uint32_t i = 0; i < n; i++) r[i] = (double*)calloc(m, sizeof(double));
+    return r;
+}
+
+static void rows_free(double** r, uint32_t n) {
+    if (!r) return;
+    for (uint32_t i = 0; i < n; i++) free(r[i]);
+    free(r);
+}
+
+static void setup_field(ref_case* c, lbeField* fl, const mplb_field_desc* d) {
+    memset(fl, 0, sizeof(*fl));
+    fl->value = rows_alloc(c->n, c->Q);
+    fl->swap = rows_alloc(c->n, c->Q);
+    fl->scalarSource = (scalar*)calloc(c->n, sizeof(scalar));
+    fl->model = (lbeModel)d->model;
+    fl->update = d->update ? 1 : 0;
+    scalar* lam = (scalar*)calloc(MPLB_MAX_Q, sizeof(scalar));
+    for (int k = 0; k < MPLB_MAX_Q; k++) lam[k] = d->Lambda[k];
+    switch (d->model) {
+    case MPLB_LIMRT:
+        fl->lbparam.liMRT.Lambda = lam;
+        fl->lbparam.liMRT.sigma = d->sigma;
+        fl->lbparam.liMRT.surfaceTension = no_st;
+        break;
+    case MPLB_XUMRT:
+        fl->lbparam.xuMRT.Lambda = lam;
+        fl->lbparam.xuMRT.sigma = d->sigma;
+        fl->lbparam.xuMRT.surfaceTension = noXuSurf;
+        break;
+    case MPLB_LITEMPMRT:
+        fl->lbparam.liTempMRT.Lambda = lam;
+        break;
+    default:
+        fl->lbparam.liMRT.Lambda = lam;
+        break;
+    }
+    uint32_t np = c->mesh.mesh.bd.nbd;
+    fl->boundary = (bdField*)calloc(np ? np : 1, sizeof(bdField));
+    for (uint32_t p = 0; p < np; p++) {
+        fl->boundary[p].type = d->bc_type ? (bdType)d->bc_type[p] : periodic;
+        if (d->bc_type && d->bc_value) {
+            if (d->bc_type[p] == MPLB_BC_FIXEDT) fl->boundary[p].param.ft.T = d->bc_value[3 * p];
+            if (d->bc_type[p] == MPLB_BC_FIXEDU)
+                for (int j = 0; j < 3; j++) fl->boundary[p].param.fu.U[j] = d->bc_value[3 * p + j];
+        }
+    }
+    fl->nreq = 0;
+}
+
+ref_case* ref_create(const mplb_mesh_desc* md, const mplb_eos_desc* ed,
+                     const mplb_field_desc* fd, const mplb_field_desc* gd, uint32_t start_time) {
+    ref_case* c = (ref_case*)calloc(1, sizeof(ref_case));
+    DdQq model = md->lattice == MPLB_D3Q15 ? D3Q15 : D2Q9;
+    c->n = md->n_points;
+
+    /* Lattice tables exactly as setLatticeInfo() assigns them (setLatticeInfo.c:68-84). */
+    latticeInfo* L = &c->mesh.lattice;
+    L->model = model;
+    L->cs2 = cs2(model);
+    L->Q = latticeQ(model);
+    L->d = latticeD(model);
+    L->vel = latticeVelocities(model);
+    L->reverse = latticeReverseDir(model);
+    L->omega = latticeWeights(model);
+    L->weights = ppWeights(model);
+    L->M = MRTMatrix(model);
+    L->invM = MRTInvMatrix(model);
+    c->Q = L->Q;
+
+    /* Single rank, no ghosts. */
+    c->mesh.parallel.pid = 0;
+    c->mesh.parallel.worldSize = 1;
+    c->mesh.parallel.nlocal = c->n;
+    c->mesh.parallel.nghosts = 0;
+    c->mesh.parallel.nrg = (uint*)calloc(1, sizeof(uint));
+    c->mesh.parallel.nsg = (uint*)calloc(1, sizeof(uint));
+
+    basicMesh* m = &c->mesh.mesh;
+    m->nPoints = c->n;
+    m->Q = c->Q;
+    m->nb = (int**)malloc((size_t)c->n * sizeof(int*));
+    m->isOnBnd = (uint*)malloc((size_t)c->n * sizeof(uint));
+    m->points = (int**)malloc((size_t)c->n * sizeof(int*));
+    for (uint32_t i = 0; i < c->n; i++) {
+        m->nb[i] = (int*)malloc((size_t)c->Q * sizeof(int));
+        m->points[i] = (int*)calloc(3, sizeof(int));
+        uint is_b = 0;
+        for (int k = 0; k < c->Q; k++) {
+            m->nb[i][k] = md->nb[(size_t)i * c->Q + k];
+            if (m->nb[i][k] == -1) is_b++;
+        }
+        /* readLatticeMesh.c:171-203: any missing neighbour marks the node. */
+        m->isOnBnd[i] = is_b ? 1 : 0;
+        if (md->points)
+            for (int j = 0; j < 3; j++) m->points[i][j] = md->points[(size_t)i * 3 + j];
+    }
+    m->bd.nbd = md->n_patches;
+    m->bd.nbdelem = (uint*)calloc(md->n_patches ? md->n_patches : 1, sizeof(uint));
+    m->bd.bdPoints = (uint**)calloc(md->n_patches ? md->n_patches : 1, sizeof(uint*));
+    size_t off = 0;
+    for (uint32_t p = 0; p < md->n_patches; p++) {
+        m->bd.nbdelem[p] = md->patch_count[p];
+        m->bd.bdPoints[p] = (uint*)malloc((size_t)(md->patch_count[p] ? md->patch_count[p] : 1) * sizeof(uint));
+        for (uint32_t i = 0; i < md->patch_count[p]; i++) m->bd.bdPoints[p][i] = md->patch_nodes[off + i];
+        off += md->patch_count[p];
+        snprintf(m->bd.bdNames[p], 100, "P%u", p);
+    }
+
+    EOSInfo* E = &c->mesh.EOS;
+    E->etype = (eosType)ed->type;
+    switch (ed->type) {
+    case MPLB_EOS_CS: E->eParam.csp.a = ed->a; E->eParam.csp.b = ed->b; break;
+    case MPLB_EOS_PR: E->eParam.prp.a = ed->a; E->eParam.prp.b = ed->b; E->eParam.prp.omega = ed->w; break;
+    case MPLB_EOS_VDW: E->eParam.vdwparam.a = ed->a; E->eParam.vdwparam.b = ed->b; break;
+    default: break;
+    }
+    E->R = ed->R; E->G = ed->G; E->M = ed->M; E->Cv = ed->Cv; E->rho_0 = ed->rho_0;
+    E->g = (scalar*)malloc(3 * sizeof(scalar));
+    E->fext = (scalar*)malloc(3 * sizeof(scalar));
+    for (int j = 0; j < 3; j++) { E->g[j] = ed->g[j]; E->fext[j] = ed->fext[j]; }
+
+    c->mesh.time.start = start_time;
+    c->mesh.time.current = start_time;
+    c->mesh.time.end = 0xffffffffu;
+    c->mesh.time.writeInterval = 0xffffffffu;
+    c->mesh.time.stp = 0;
+
+    c->mf.rho = (scalar*)calloc(c->n, sizeof(scalar));
+    c->mf.T = (scalar*)calloc(c->n, sizeof(scalar));
+    c->mf.p = (scalar*)calloc(c->n, sizeof(scalar));
+    c->mf.U = rows_alloc(c->n, 3);
+    c->mf.Fi = rows_alloc(c->n, 3);
+    c->mf.Ft = rows_alloc(c->n, 3);
+
+    c->has_f = fd && fd->model != MPLB_NO_MODEL;
+    c->has_g = gd && gd->model != MPLB_NO_MODEL;
+    mplb_field_desc none;
+    memset(&none, 0, sizeof(none));
+    none.model = MPLB_LIMRT;
+    setup_field(c, &c->f, c->has_f ? fd : &none);
+    setup_field(c, &c->g, c->has_g ? gd : &none);
+    if (!c->has_f) c->f.update = 0;
+    if (!c->has_g) c->g.update = 0;
+    return c;
+}
+
+void ref_destroy(ref_case* c) {
+    if (!c) return;
+    rows_free(c->f.value, c->n); rows_free(c->f.swap, c->n);
+    rows_free(c->g.value, c->n); rows_free(c->g.swap, c->n);
+    free(c->f.scalarSource); free(c->g.scalarSource);
+    rows_free(c->mf.U, c->n); rows_free(c->mf.Fi, c->n); rows_free(c->mf.Ft, c->n);
+    free(c->mf.rho); free(c->mf.T); free(c->mf.p);
+    free(c);
+}
+
+static void put_rows(double** r, const double* src, uint32_t n, int m) {
+    for (uint32_t i = 0; i < n; i++)
+        for (int j = 0; j < m; j++) r[i][j] = src[(size_t)i * m + j];
+}
+
+static void get_rows(double* dst, double** r, uint32_t n, int m) {
+    for (uint32_t i = 0; i < n; i++)
+        for (int j = 0; j < m; j++) dst[(size_t)i * m + j] = r[i][j];
+}
+
+int ref_upload(ref_case* c, const double* rho, const double* U, const double* T,
+               const double* f, const double* g, const double* S,
+               const double* Fi, const double* Ft) {
+    if (rho) memcpy(c->mf.rho, rho, c->n * sizeof(double));
+    if (T) memcpy(c->mf.T, T, c->n * sizeof(double));
+    if (U) put_rows(c->mf.U, U, c->n, 3);
+    if (Fi) put_rows(c->mf.Fi, Fi, c->n, 3);
+    if (Ft) put_rows(c->mf.Ft, Ft, c->n, 3);
+    if (f) put_rows(c->f.value, f, c->n, c->Q);
+    if (g) put_rows(c->g.value, g, c->n, c->Q);
+    if (S) memcpy(c->g.scalarSource, S, c->n * sizeof(double));
+    return 0;
+}
+
+int ref_download(ref_case* c, double* rho, double* U, double* T, double* Fi, double* Ft,
+                 double* S, double* f, double* g) {
+    if (rho) memcpy(rho, c->mf.rho, c->n * sizeof(double));
+    if (T) memcpy(T, c->mf.T, c->n * sizeof(double));
+    if (U) get_rows(U, c->mf.U, c->n, 3);
+    if (Fi) get_rows(Fi, c->mf.Fi, c->n, 3);
+    if (Ft) get_rows(Ft, c->mf.Ft, c->n, 3);
+    if (f) get_rows(f, c->f.value, c->n, c->Q);
+    if (g) get_rows(g, c->g.value, c->n, c->Q);
+    if (S) memcpy(S, c->g.scalarSource, c->n * sizeof(double));
+    return 0;
+}
+
+void ref_set_time(ref_case* c, uint32_t t) { c->mesh.time.current = t; }
+uint32_t ref_get_time(ref_case* c) { return c->mesh.time.current; }
+void ref_set_rho0(ref_case* c, double r) { c->mesh.EOS.rho_0 = r; }
+double ref_average_rho0(ref_case* c) {
+    c->mesh.EOS.rho_0 = averageScalarField(&c->mesh, c->mf.rho);
+    return c->mesh.EOS.rho_0;
+}
+
+/* Start-up block of the solver (multiPhasePP.c:122-147). */
+int ref_initialize(ref_case* c) {
+    equilibrium(&c->mesh, &c->mf, &c->f);
+    equilibrium(&c->mesh, &c->mf, &c->g);
+    interForce(&c->mesh, &c->mf);
+    heatSource(&c->mesh, &c->mf, &c->g);
+    return 0;
+}
+
+/* One pass of the time loop body (multiPhasePP.c:157-240), writes excluded.
+ * The --frozen / --nht switches act through the update flags exactly as
+ * mp.frozen / mp.ht do in the solver. */
+int ref_step(ref_case* c, uint32_t nsteps) {
+    latticeMesh* m = &c->mesh;
+    for (uint32_t s = 0; s < nsteps; s++) {
+        ++m->time.current;
+        collision(m, &c->mf, &c->f);
+        lbstream(m, &c->f);
+        updateBoundaries(m, &c->mf, &c->f);
+        collision(m, &c->mf, &c->g);
+        lbstream(m, &c->g);
+        updateBoundaries(m, &c->mf, &c->g);
+        macroDensity(m, &c->mf, &c->f, 0, m->parallel.nlocal);
+        macroDensity(m, &c->mf, &c->f, m->parallel.nlocal, m->mesh.nPoints);
+        if (c->g.update != 0) heatSource(m, &c->mf, &c->g);
+        macroTemperature(m, &c->mf, &c->g, 0, m->mesh.nPoints);
+        if (c->f.update != 0) interForce(m, &c->mf);
+        macroVelocity(m, &c->mf, &c->f, 0, m->mesh.nPoints);
+    }
+    return 0;
+}
+
+/* Single reference operators, for operator-level parity. */
+enum { OP_EQUILIBRIUM = 0, OP_COLLISION, OP_LBSTREAM, OP_BOUNDARIES, OP_DENSITY,
+       OP_VELOCITY, OP_TEMPERATURE, OP_INTERFORCE, OP_HEATSOURCE };
+
+int ref_op(ref_case* c, int op, int field, uint32_t start, uint32_t end) {
+    lbeField* fl = field == MPLB_FIELD_G ? &c->g : &c->f;
+    latticeMesh* m = &c->mesh;
+    switch (op) {
+    case OP_EQUILIBRIUM: equilibrium(m, &c->mf, fl); break;
+    case OP_COLLISION: collision(m, &c->mf, fl); break;
+    case OP_LBSTREAM: lbstream(m, fl); break;
+    case OP_BOUNDARIES: updateBoundaries(m, &c->mf, fl); break;
+    case OP_DENSITY: macroDensity(m, &c->mf, &c->f, start, end); break;
+    case OP_VELOCITY: macroVelocity(m, &c->mf, &c->f, start, end); break;
+    case OP_TEMPERATURE: macroTemperature(m, &c->mf, &c->g, start, end); break;
+    case OP_INTERFORCE: interForce(m, &c->mf); break;
+    case OP_HEATSOURCE: heatSource(m, &c->mf, &c->g); break;
+    default: return -1;
+    }
+    return 0;
+}
+
+/* p_eos and potential as scalar functions, for EOS-level checks. */
+double ref_p_eos(ref_case* c, double rho, double T) { return p_eos(&c->mesh.EOS, rho, T); }
+double ref_potential(ref_case* c, double rho, double T) { return potential(&c->mesh, rho, T); }
