@@ -1,1 +1,201 @@
-"""B200 lattice update for multiphaseLB (placeholder; filled in below)."""
+"""multiphaselb_b200 -- B200 (sm_100a) lattice update for multiphaseLB.
+
+The product is the C-ABI library ``lib/libmplb_gpu.so`` (include/mplb_gpu.h).
+This module is a thin ctypes mirror of it for Python callers, tests and the
+benchmark.  ``Lattice`` mirrors the reference's operator sequence: the same
+operator names as src/lbEquation/general (collision, lbstream,
+update_boundaries, macro_density, macro_velocity, macro_temperature,
+inter_force, heat_source, equilibrium) plus the solver-level calls
+initialize / step / download.
+
+There is no CPU fallback: if the library is missing or no CUDA device is
+present, constructing a Lattice raises.
+"""
+import ctypes as C
+import os
+
+import numpy as np
+
+from . import abi
+from .abi import FIELD_F, FIELD_G, PATH_AUTO, PATH_FUSED, PATH_OPERATORS  # noqa: F401
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "lib", "libmplb_gpu.so")
+
+_lib = None
+
+
+class MplbError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"mplb error {code}: {msg}")
+        self.code = code
+
+
+def load_library(path=LIB_PATH):
+    """Load the C-ABI library and declare its signatures."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise ImportError(f"{path} is missing: build it with `python -m multiphaselb_b200.build`")
+    lib = C.CDLL(path)
+    H = C.c_void_p
+    D = C.POINTER(C.c_double)
+    sig = {
+        "mplb_gpu_version": ([], C.c_char_p),
+        "mplb_gpu_last_error": ([], C.c_char_p),
+        "mplb_gpu_create": ([C.POINTER(abi.MeshDesc), C.POINTER(abi.EosDesc), C.POINTER(abi.FieldDesc),
+                             C.POINTER(abi.FieldDesc), C.POINTER(abi.Opts), C.POINTER(H)], C.c_int),
+        "mplb_gpu_destroy": ([H], C.c_int),
+        "mplb_gpu_info": ([H, C.POINTER(abi.Info)], C.c_int),
+        "mplb_gpu_upload": ([H] + [D] * 8, C.c_int),
+        "mplb_gpu_download": ([H] + [D] * 8, C.c_int),
+        "mplb_gpu_initialize": ([H], C.c_int),
+        "mplb_gpu_step": ([H, C.c_uint32], C.c_int),
+        "mplb_gpu_equilibrium": ([H, C.c_int32], C.c_int),
+        "mplb_gpu_collision": ([H, C.c_int32], C.c_int),
+        "mplb_gpu_lbstream": ([H, C.c_int32], C.c_int),
+        "mplb_gpu_update_boundaries": ([H, C.c_int32], C.c_int),
+        "mplb_gpu_macro_density": ([H, C.c_uint32, C.c_uint32], C.c_int),
+        "mplb_gpu_macro_velocity": ([H, C.c_uint32, C.c_uint32], C.c_int),
+        "mplb_gpu_macro_temperature": ([H, C.c_uint32, C.c_uint32], C.c_int),
+        "mplb_gpu_inter_force": ([H], C.c_int),
+        "mplb_gpu_heat_source": ([H], C.c_int),
+        "mplb_gpu_set_time": ([H, C.c_uint32], C.c_int),
+        "mplb_gpu_set_rho0": ([H, C.c_double], C.c_int),
+        "mplb_gpu_average_rho0": ([H, D], C.c_int),
+        "mplb_gpu_mass_energy": ([H, D, D], C.c_int),
+        "mplb_gpu_sync": ([H], C.c_int),
+    }
+    for name, (args, res) in sig.items():
+        fn = getattr(lib, name)
+        fn.argtypes = args
+        fn.restype = res
+    _lib = lib
+    return lib
+
+
+def version():
+    return load_library().mplb_gpu_version().decode()
+
+
+class Lattice:
+    """One device-resident lattice (a C-ABI handle).
+
+    ``case`` is a :class:`multiphaselb_b200.cases.Case` (or any object with
+    the same attributes: lattice, n, nb, points, patches, eos, f, g).
+    """
+
+    def __init__(self, case, path=PATH_AUTO, device=-1, stream=None, start_time=0):
+        self.lib = load_library()
+        self.case = case
+        self.n, self.Q = case.n, case.Q
+        self._desc = abi.Descriptors(case)
+        opts = abi.Opts(abi.FP64, path, device, stream, start_time)
+        h = C.c_void_p()
+        self._check(self.lib.mplb_gpu_create(C.byref(self._desc.mesh), C.byref(self._desc.eos),
+                                              C.byref(self._desc.f), C.byref(self._desc.g),
+                                              C.byref(opts), C.byref(h)))
+        self.h = h
+
+    # ---------------------------------------------------------------- plumbing
+    def _check(self, rc):
+        if rc != 0:
+            raise MplbError(rc, self.lib.mplb_gpu_last_error().decode())
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.mplb_gpu_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def info(self):
+        i = abi.Info()
+        self._check(self.lib.mplb_gpu_info(self.h, C.byref(i)))
+        return dict(path=i.path, box_dims=tuple(i.box_dims), box_periodic=tuple(i.box_periodic),
+                    bc_sequential=i.bc_sequential, current_time=i.current_time,
+                    device_bytes=i.device_bytes, kernel_launches=i.kernel_launches)
+
+    # -------------------------------------------------------------- host data
+    def upload(self, rho=None, U=None, T=None, f=None, g=None, S=None, Fi=None, Ft=None):
+        arrs = [None if a is None else np.ascontiguousarray(a, dtype=np.float64)
+                for a in (rho, U, T, f, g, S, Fi, Ft)]
+        self._check(self.lib.mplb_gpu_upload(self.h, *[abi.dptr(a) for a in arrs]))
+
+    def upload_case(self):
+        c = self.case
+        self.upload(rho=c.rho, U=c.U, T=c.T)
+
+    def download(self, out=None):
+        n, Q = self.n, self.Q
+        if out is None:
+            out = dict(rho=np.zeros(n), U=np.zeros((n, 3)), T=np.zeros(n), Fi=np.zeros((n, 3)),
+                       Ft=np.zeros((n, 3)), S=np.zeros(n), f=np.zeros((n, Q)), g=np.zeros((n, Q)))
+        self._check(self.lib.mplb_gpu_download(self.h, *[abi.dptr(out.get(k)) for k in
+                                                          ("rho", "U", "T", "Fi", "Ft", "S", "f", "g")]))
+        return out
+
+    # ------------------------------------------------------------ solver level
+    def initialize(self):
+        self._check(self.lib.mplb_gpu_initialize(self.h))
+
+    def step(self, n=1):
+        self._check(self.lib.mplb_gpu_step(self.h, n))
+
+    def sync(self):
+        self._check(self.lib.mplb_gpu_sync(self.h))
+
+    # ------------------------------------------------- reference operator names
+    def equilibrium(self, field=FIELD_F):
+        self._check(self.lib.mplb_gpu_equilibrium(self.h, field))
+
+    def collision(self, field=FIELD_F):
+        self._check(self.lib.mplb_gpu_collision(self.h, field))
+
+    def lbstream(self, field=FIELD_F):
+        self._check(self.lib.mplb_gpu_lbstream(self.h, field))
+
+    def update_boundaries(self, field=FIELD_F):
+        self._check(self.lib.mplb_gpu_update_boundaries(self.h, field))
+
+    def macro_density(self, start=0, end=None):
+        self._check(self.lib.mplb_gpu_macro_density(self.h, start, self.n if end is None else end))
+
+    def macro_velocity(self, start=0, end=None):
+        self._check(self.lib.mplb_gpu_macro_velocity(self.h, start, self.n if end is None else end))
+
+    def macro_temperature(self, start=0, end=None):
+        self._check(self.lib.mplb_gpu_macro_temperature(self.h, start, self.n if end is None else end))
+
+    def inter_force(self):
+        self._check(self.lib.mplb_gpu_inter_force(self.h))
+
+    def heat_source(self):
+        self._check(self.lib.mplb_gpu_heat_source(self.h))
+
+    def set_time(self, t):
+        self._check(self.lib.mplb_gpu_set_time(self.h, t))
+
+    def set_rho0(self, r):
+        self._check(self.lib.mplb_gpu_set_rho0(self.h, r))
+
+    def average_rho0(self):
+        r = C.c_double()
+        self._check(self.lib.mplb_gpu_average_rho0(self.h, C.byref(r)))
+        return r.value
+
+    def mass_energy(self):
+        m, e = C.c_double(), C.c_double()
+        self._check(self.lib.mplb_gpu_mass_energy(self.h, C.byref(m), C.byref(e)))
+        return m.value, e.value

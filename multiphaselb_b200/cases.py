@@ -121,8 +121,22 @@ def p_eos(eos, rho, T):
     raise ValueError(t)
 
 
+def _eos_key(eos):
+    return tuple(sorted((k, tuple(v) if isinstance(v, (list, tuple)) else v) for k, v in eos.items()))
+
+
+_TC_CACHE, _MAXWELL_CACHE = {}, {}
+
+
 def critical_temperature(eos):
-    """Tc from dp/drho = d2p/drho2 = 0, by nested bisection on T (FP64)."""
+    """Tc from dp/drho = d2p/drho2 = 0, by bisection on T (FP64)."""
+    key = _eos_key(eos)
+    if key not in _TC_CACHE:
+        _TC_CACHE[key] = _critical_temperature(eos)
+    return _TC_CACHE[key]
+
+
+def _critical_temperature(eos):
     if eos["type"] == abi.EOS_VDW and eos.get("M", 1.0) == 1.0:
         return 8 * eos["a"] / (27 * eos["b"] * eos.get("R", 1.0))
     rho = np.linspace(1e-4, 0.999 * _rho_max(eos), 20001)
@@ -133,7 +147,7 @@ def critical_temperature(eos):
     lo, hi = 1e-6, 10.0
     while not has_loop(lo):
         lo *= 0.5
-    for _ in range(200):
+    for _ in range(80):
         mid = 0.5 * (lo + hi)
         if has_loop(mid):
             lo = mid
@@ -155,6 +169,16 @@ def _rho_max(eos):
 def maxwell_densities(eos, T):
     """Coexistence (vapour, liquid) densities by the equal-area rule in the
     specific volume: p(v_v) = p(v_l) = P and int_{v_l}^{v_v} p dv = P (v_v - v_l)."""
+    key = (_eos_key(eos), float(T))
+    if key not in _MAXWELL_CACHE:
+        _MAXWELL_CACHE[key] = _maxwell_densities(eos, T)
+    return _MAXWELL_CACHE[key]
+
+
+_GL_X, _GL_W = np.polynomial.legendre.leggauss(96)
+
+
+def _maxwell_densities(eos, T):
     rmax = _rho_max(eos)
     rho = np.linspace(1e-6, 0.9999 * rmax, 400001)
     p = p_eos(eos, rho, T)
@@ -169,16 +193,20 @@ def maxwell_densities(eos, T):
         return rv, rl
 
     def area(P):
+        # split at the spinodals so each Gauss-Legendre piece is smooth
         rv, rl = roots(P)
-        v = np.linspace(1.0 / rl, 1.0 / rv, 200001)
-        pv = p_eos(eos, 1.0 / v, T)
-        return np.trapezoid(pv - P, v)
+        knots = [1.0 / rl, 1.0 / rho[i_min], 1.0 / rho[i_max], 1.0 / rv]
+        tot = 0.0
+        for a, b in zip(knots[:-1], knots[1:]):
+            v = 0.5 * (b - a) * _GL_X + 0.5 * (a + b)
+            tot += 0.5 * (b - a) * np.dot(_GL_W, p_eos(eos, 1.0 / v, T) - P)
+        return tot
 
-    P = _bisect(area, plo, phi)
+    P = _bisect(area, plo, phi, it=80)
     return roots(P)
 
 
-def _bisect(fn, lo, hi, it=200):
+def _bisect(fn, lo, hi, it=80):
     flo = fn(lo)
     for _ in range(it):
         mid = 0.5 * (lo + hi)

@@ -1,0 +1,311 @@
+// lattice.cuh -- lattice traits, parameter block and node-local physics.
+//
+// Everything here is __host__ __device__ arithmetic on one node.  The
+// expressions keep the reference's evaluation order term by term (C
+// left-to-right association, no contraction: the translation units that
+// include this header are compiled with -fmad=false) so that the device
+// results equal the reference's binary64 results bit for bit.
+#pragma once
+
+#include <stdint.h>
+#include <utility>
+#include <type_traits>
+#include "../../include/mplb_gpu.h"
+
+#ifndef MPLB_HD
+#define MPLB_HD __host__ __device__ __forceinline__
+#endif
+
+namespace mplb {
+
+// ----------------------------------------------------------------- lattices
+// Velocity sets in the reference's order (D2Q9_Vel.c:20-55, D3Q15_Vel.c) and
+// their reverse maps (D2Q9_Reverse.c, D3Q15_Reverse.c).  Components are packed
+// two bits each (value+1) and reverse indices four bits each, so both compile
+// time (static_for indices) and runtime indices work in device code.
+struct D2Q9T {
+    static constexpr int lattice = MPLB_D2Q9;
+    static constexpr int Q = 9, D = 2, NAX = 4;
+    static constexpr uint32_t PX = 133401u, PY = 10341u, PZ = 87381u;
+    static constexpr uint64_t PREV = 27253675056ull;
+};
+struct D3Q15T {
+    static constexpr int lattice = MPLB_D3Q15;
+    static constexpr int Q = 15, D = 3, NAX = 6;
+    static constexpr uint32_t PX = 143168841u, PY = 42112149u, PZ = 2787669u;
+    static constexpr uint64_t PREV = 543154130879988000ull;
+};
+
+template <class L> MPLB_HD constexpr int cxk(int k) { return (int)((L::PX >> (2 * k)) & 3u) - 1; }
+template <class L> MPLB_HD constexpr int cyk(int k) { return (int)((L::PY >> (2 * k)) & 3u) - 1; }
+template <class L> MPLB_HD constexpr int czk(int k) { return (int)((L::PZ >> (2 * k)) & 3u) - 1; }
+template <class L> MPLB_HD constexpr int ck(int k, int j) { return j == 0 ? cxk<L>(k) : j == 1 ? cyk<L>(k) : czk<L>(k); }
+template <class L> MPLB_HD constexpr int revk(int k) { return (int)((L::PREV >> (4 * k)) & 15ull); }
+// Axis finite-difference directions (scalarGradient.c:22-23,62-63,108-109,148-149,189-190):
+// a = direction whose pull source is x + e_d (c = -e_d), b = the one with c = +e_d.
+template <class L> MPLB_HD constexpr int fda(int d) { return L::Q == 9 ? (d == 0 ? 3 : 4) : 2 * d + 2; }
+template <class L> MPLB_HD constexpr int fdb(int d) { return L::Q == 9 ? (d == 0 ? 1 : 2) : 2 * d + 1; }
+
+// Moment polynomials of the MRT basis evaluated on a velocity (integers):
+// D2Q9 Lallemand-Luo rows (D2Q9_MRT.c:20-108), D3Q15 d'Humieres rows
+// (D3Q15_MRT.c).  Used at compile time for M f and on the host for M^-1.
+MPLB_HD constexpr int moment(int lat, int r, int cx, int cy, int cz) {
+    int c2 = cx * cx + cy * cy + cz * cz;
+    if (lat == MPLB_D2Q9) {
+        return r == 0 ? 1 : r == 1 ? -4 + 3 * c2 : r == 2 ? (8 - 21 * c2 + 9 * c2 * c2) / 2
+             : r == 3 ? cx : r == 4 ? (-5 + 3 * c2) * cx : r == 5 ? cy
+             : r == 6 ? (-5 + 3 * c2) * cy : r == 7 ? cx * cx - cy * cy : cx * cy;
+    }
+    return r == 0 ? 1 : r == 1 ? c2 - 2 : r == 2 ? (15 * c2 * c2 - 55 * c2 + 32) / 2
+         : r == 3 ? cx : r == 4 ? (5 * c2 - 13) * cx / 2 : r == 5 ? cy
+         : r == 6 ? (5 * c2 - 13) * cy / 2 : r == 7 ? cz : r == 8 ? (5 * c2 - 13) * cz / 2
+         : r == 9 ? 3 * cx * cx - c2 : r == 10 ? cy * cy - cz * cz : r == 11 ? cx * cy
+         : r == 12 ? cy * cz : r == 13 ? cx * cz : cx * cy * cz;
+}
+
+template <class L>
+MPLB_HD constexpr int Mint(int r, int k) { return moment(L::lattice, r, cxk<L>(k), cyk<L>(k), czk<L>(k)); }
+
+// ----------------------------------------------------------- parameter block
+// Passed by value to every kernel (lives in the kernel-parameter constant
+// bank), so several handles on one device never share mutable globals.
+struct Params {
+    int32_t lat, Q;
+    uint32_t n;
+    double cs2;
+    double w[MPLB_MAX_Q];      // LB weights (D2Q9_omega.c, D3Q15_omega.c)
+    double ppw[MPLB_MAX_Q];    // pseudopotential force weights (D2Q9_ppw.c, D3Q15_ppw.c)
+    double Mi[MPLB_MAX_Q][MPLB_MAX_Q];  // M^-1, host-computed as M[c][r]/|row c|^2
+    // flow field
+    int32_t f_model, f_update;
+    double Lf[MPLB_MAX_Q];
+    double relax_f[MPLB_MAX_Q];  // (1 - 0.5*Lambda[k])            liMRTCollision.c:92
+    double s1_den, s2_den;       // ((1/Lambda[1])-0.5), ((1/Lambda[2])-0.5)  liMRTForce.c:35-36
+    double sig12, sig6;          // 12*sigma (liMRTForce.c:35), 6.0*sigma (xuMRTForce.c:43)
+    // thermal field
+    int32_t g_model, g_update;
+    double Lg[MPLB_MAX_Q];
+    double corr3, corr5;         // (1 - L3/2)*L4, (1 - L5/2)*L6   liTempMRTCollision.c:75-77
+    double lam_fac;              // (1/Lambda[3] - 0.5)           heatSource.c:105
+    // EOS (EOSInfo.h:80-102)
+    int32_t eos;
+    double a, b, R, G, M, Cv, rho_0;
+    double g[3], fext[3];
+    double pr_tc, pr_kappa;      // Peng-Robinson: 0.170151343*a/(b*R), 0.37464+1.5422w-0.26992w^2
+};
+
+// ---------------------------------------------------------------------- EOS
+// p_eos.c:7-64
+MPLB_HD double p_eos(const Params& P, double rho, double T) {
+    switch (P.eos) {
+    case MPLB_EOS_IDEAL:
+        return rho * P.R * T;
+    case MPLB_EOS_CS: {
+        double al = P.b * rho / 4.0;
+        double be = 1 - al;
+        return rho * P.R * T * ((1 + al + al * al - al * al * al) / (be * be * be)) - P.a * rho * rho;
+    }
+    case MPLB_EOS_PR: {
+        double be = (1 + P.pr_kappa * (1 - sqrt(T / P.pr_tc)));
+        return rho * P.R * T / (1 - P.b * rho) - P.a * be * be * rho * rho / (1 + 2 * P.b * rho - P.b * rho * P.b * rho);
+    }
+    case MPLB_EOS_VDW:
+        return rho * P.R * T / (P.M - rho * P.b) - P.a * rho * rho / (P.M * P.M);
+    default:
+        return 0;
+    }
+}
+
+// potential.c:7-13
+MPLB_HD double potential(const Params& P, double rho, double T) {
+    return sqrt(2 * (p_eos(P, rho, T) - rho * P.cs2) / (P.G));
+}
+
+// --------------------------------------------------------------- matvecs
+// Compile-time loop: calls f(integral_constant<int, 0..N-1>) in order.
+template <class F, int... I>
+MPLB_HD void static_for_impl(F& f, std::integer_sequence<int, I...>) {
+    (f(std::integral_constant<int, I>{}), ...);
+}
+template <int N, class F>
+MPLB_HD void static_for(F&& f) { static_for_impl(f, std::make_integer_sequence<int, N>{}); }
+
+// matVecMult.c:4-20 evaluates res_i = sum_j M_ij v_j left to right from 0.
+// M has integer entries, so each product is exact; terms with a zero
+// coefficient are skipped (they add +-0 and leave a finite sum unchanged).
+template <class L>
+MPLB_HD void mul_M(const double* v, double* r) {
+    static_for<L::Q>([&](auto i) {
+        double s = 0;
+        static_for<L::Q>([&](auto j) {
+            constexpr int c = Mint<L>(decltype(i)::value, decltype(j)::value);
+            if constexpr (c == 1) s = s + v[j];
+            else if constexpr (c == -1) s = s - v[j];
+            else if constexpr (c != 0) s = s + (double)c * v[j];
+        });
+        r[i] = s;
+    });
+}
+
+// M^-1 entries are rounded constants: product rounded, then added.  Its
+// zero pattern is that of M^T.
+template <class L>
+MPLB_HD void mul_Mi(const Params& P, const double* v, double* r) {
+    static_for<L::Q>([&](auto i) {
+        double s = 0;
+        static_for<L::Q>([&](auto j) {
+            constexpr int c = Mint<L>(decltype(j)::value, decltype(i)::value);
+            if constexpr (c != 0) s = s + P.Mi[i][j] * v[j];
+        });
+        r[i] = s;
+    });
+}
+
+// ------------------------------------------------------------ equilibria
+// liMRTEquilibrium.c:3-29 / xuMRTEquilibrium.c:3-29
+template <class L>
+MPLB_HD double eq_flow_k(const Params& P, int k, double rho, const double* v) {
+    double al = 0, be = 0;
+    const int c[3] = {cxk<L>(k), cyk<L>(k), czk<L>(k)};
+#pragma unroll
+    for (int j = 0; j < 3; j++) {
+        al += c[j] * v[j];
+        be += v[j] * v[j];
+    }
+    return rho * P.w[k] * (1 + al / P.cs2 + 0.5 * al * al / (P.cs2 * P.cs2) - 0.5 * be / P.cs2);
+}
+
+// liTempMRTEquilibrium.c:5-44 (D2Q9): g = M^-1 n_eq(T, U)
+MPLB_HD void eq_heat(const Params& P, double T, double u0, double u1, double* g) {
+    double n[9];
+    n[0] = T;
+    n[1] = -2.0 * T;
+    n[2] = 2.0 * T;
+    n[3] = T * u0;
+    n[4] = T * (-u0);
+    n[5] = T * u1;
+    n[6] = T * (-u1);
+    n[7] = 0;
+    n[8] = 0;
+    mul_Mi<D2Q9T>(P, n, g);
+}
+
+// ---------------------------------------------------------- node collisions
+// liMRTCollision.c:48-106 with liMRTForce.c:18-42.  f in/out (9 values).
+MPLB_HD void collide_limrt(const Params& P, double* f, double rho, const double* U,
+                           const double* F, const double* Fi, double T) {
+    double um = 0;
+#pragma unroll
+    for (int k = 0; k < 3; k++) um += U[k] * U[k];
+    double meq[9], m[9], S[9];
+    meq[0] = rho;
+    meq[1] = rho * (-2 + 3 * um);
+    meq[2] = rho * (1 - 3 * um);
+    meq[3] = rho * U[0];
+    meq[4] = rho * (-U[0]);
+    meq[5] = rho * U[1];
+    meq[6] = rho * (-U[1]);
+    meq[7] = rho * (U[0] * U[0] - U[1] * U[1]);
+    meq[8] = rho * U[0] * U[1];
+    mul_M<D2Q9T>(f, m);
+    double ps = potential(P, rho, T);
+    double uf = U[0] * F[0] + U[1] * F[1];
+    double fi2 = Fi[0] * Fi[0] + Fi[1] * Fi[1];
+    S[0] = 0;
+    S[1] = 6 * uf + P.sig12 * fi2 / (ps * ps * P.s1_den);
+    S[2] = -6 * uf - P.sig12 * fi2 / (ps * ps * P.s2_den);
+    S[3] = F[0];
+    S[4] = -F[0];
+    S[5] = F[1];
+    S[6] = -F[1];
+    S[7] = 2 * (U[0] * F[0] - U[1] * F[1]);
+    S[8] = U[0] * F[1] + U[1] * F[0];
+#pragma unroll
+    for (int k = 0; k < 9; k++) m[k] = m[k] - P.Lf[k] * (m[k] - meq[k]) + P.relax_f[k] * S[k];
+    mul_Mi<D2Q9T>(P, m, f);
+}
+
+// xuMRTCollision.c:46-89, xuMRTEquilibriumMS.c:12-51, xuMRTForce.c:14-69.
+// F here is Fi + (rho - rho_0) g (no fext), xuMRTForce.c:18-22.
+MPLB_HD void collide_xumrt(const Params& P, double* f, double rho, const double* U,
+                           const double* Fi, double T) {
+    double um = 0;
+#pragma unroll
+    for (int k = 0; k < 3; k++) um += U[k] * U[k];
+    double meq[15], m[15], S[15], F[3];
+    meq[0] = rho;
+    meq[1] = rho * (-1.0 + um);
+    meq[2] = rho * (1.0 - 5.0 * um);
+    meq[3] = rho * U[0];
+    meq[4] = rho * -7.0 * U[0] / 3.0;
+    meq[5] = rho * U[1];
+    meq[6] = rho * -7.0 * U[1] / 3.0;
+    meq[7] = rho * U[2];
+    meq[8] = rho * -7.0 * U[2] / 3.0;
+    meq[9] = rho * (2.0 * U[0] * U[0] - U[1] * U[1] - U[2] * U[2]);
+    meq[10] = rho * (U[1] * U[1] - U[2] * U[2]);
+    meq[11] = rho * U[0] * U[1];
+    meq[12] = rho * U[1] * U[2];
+    meq[13] = rho * U[0] * U[2];
+    meq[14] = 0;
+    mul_M<D3Q15T>(f, m);
+#pragma unroll
+    for (int j = 0; j < 3; j++) F[j] = Fi[j] + (rho - P.rho_0) * P.g[j];
+    double ps = potential(P, rho, T);
+    double uf = U[0] * F[0] + U[1] * F[1] + U[2] * F[2];
+    double f2 = 0;
+#pragma unroll
+    for (int k = 0; k < 3; k++) f2 += F[k] * F[k];
+    S[0] = 0;
+    S[1] = 2.0 * uf + (P.sig6 * f2) / (ps * ps * P.s1_den);
+    S[2] = -10.0 * uf;
+    S[3] = F[0];
+    S[4] = -7.0 * F[0] / 3.0;
+    S[5] = F[1];
+    S[6] = -7.0 * F[1] / 3.0;
+    S[7] = F[2];
+    S[8] = -7.0 * F[2] / 3.0;
+    S[9] = 4.0 * U[0] * F[0] - 2.0 * U[1] * F[1] - 2.0 * U[2] * F[2];
+    S[10] = 2.0 * U[1] * F[1] - 2.0 * U[2] * F[2];
+    S[11] = U[0] * F[1] + U[1] * F[0];
+    S[12] = U[1] * F[2] + U[2] * F[1];
+    S[13] = U[0] * F[2] + U[2] * F[0];
+    S[14] = 0;
+#pragma unroll
+    for (int k = 0; k < 15; k++) m[k] = m[k] - P.Lf[k] * (m[k] - meq[k]) + P.relax_f[k] * S[k];
+    mul_Mi<D3Q15T>(P, m, f);
+}
+
+// liTempMRTCollision.c:38-84, liTempMRTEquilibriumMS.c:20-38, liTempMRTSource.c:17-24.
+MPLB_HD void collide_litemp(const Params& P, double* g, double T, double u0, double u1, double src) {
+    double neq[9], n[9];
+    neq[0] = T;
+    neq[1] = -2.0 * T;
+    neq[2] = 2.0 * T;
+    neq[3] = T * u0;
+    neq[4] = T * (-u0);
+    neq[5] = T * u1;
+    neq[6] = T * (-u1);
+    neq[7] = 0;
+    neq[8] = 0;
+    mul_M<D2Q9T>(g, n);
+    double n4 = n[4], n6 = n[6];
+    n[0] = n[0] - P.Lg[0] * (n[0] - neq[0]) + src;
+#pragma unroll
+    for (int k = 1; k < 9; k++) n[k] = n[k] - P.Lg[k] * (n[k] - neq[k]) + 0.0;
+    n[3] = n[3] + P.corr3 * n4;
+    n[5] = n[5] + P.corr5 * n6;
+    mul_Mi<D2Q9T>(P, n, g);
+}
+
+// heatSource.c:144-165: source from gradients (dot), divergence, rho, T_old.
+MPLB_HD double heat_source_value(const Params& P, double rho, double T, double dot, double divU,
+                                 double oldss) {
+    double lambda = rho * P.Cv * P.lam_fac;
+    double dpdT = p_eos(P, rho, 1.1 * T) - p_eos(P, rho, 0.9 * T);
+    dpdT = dpdT / (0.2 * T);
+    double s = -lambda * dot / P.Cv + divU * T * (1.0 - dpdT / (rho * P.Cv));
+    return s + 0.5 * (s - oldss);
+}
+
+}  // namespace mplb

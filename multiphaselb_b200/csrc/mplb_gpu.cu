@@ -1,0 +1,801 @@
+// mplb_gpu.cu -- C-ABI of the B200 lattice update (include/mplb_gpu.h).
+//
+// One handle = one device-resident lattice.  The handle keeps the
+// reference's state (f, g after streaming and boundaries; rho, U, T, Fi, Ft,
+// scalarSource) in structure-of-arrays FP64 buffers and advances it either
+// with one kernel per reference operator (any neighbour table) or with the
+// fused box kernels of fused.cuh (structured boxes).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <unordered_set>
+#include <vector>
+
+#include "ops.cuh"
+#include "fused.cuh"
+
+using namespace mplb;
+
+namespace {
+
+thread_local std::string g_err = "";
+
+int fail(int code, const std::string& msg) {
+    g_err = msg;
+    return code;
+}
+
+#define CK(call)                                                                        \
+    do {                                                                                \
+        cudaError_t e_ = (call);                                                        \
+        if (e_ != cudaSuccess)                                                          \
+            return fail(MPLB_E_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+    } while (0)
+
+constexpr int TPB = 256;
+
+inline unsigned blocks(size_t n, int tpb = TPB) { return (unsigned)((n + tpb - 1) / tpb); }
+
+struct PatchHost {
+    PatchDev d;
+};
+
+}  // namespace
+
+struct mplb_gpu {
+    int dev = 0;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    Params P{};
+    int lat = 0, Q = 0, D = 0;
+    uint32_t n = 0;
+    int path = MPLB_PATH_OPERATORS;
+    // box description (when the neighbour table is a structured box)
+    bool box = false;
+    int dims[3] = {0, 0, 0}, per[3] = {0, 0, 0};
+    // device state
+    int32_t* nb = nullptr;
+    uint8_t* onb = nullptr;
+    double* pdf[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};  // [field][buffer]
+    int cur[2] = {0, 0};
+    double *rho = nullptr, *T = nullptr, *S = nullptr, *U = nullptr, *Fi = nullptr, *Ft = nullptr;
+    double *T2 = nullptr, *U2 = nullptr;  // fused-path double buffers
+    uint8_t* bcmap = nullptr;             // fused-path per-node boundary-program index
+    uint32_t* pnodes = nullptr;
+    PatchDev* dpatches = nullptr;          // [field][patch] copies for the serial kernel
+    std::vector<PatchDev> fpatch[2];       // per-field patch tables (type, values)
+    std::vector<int32_t> bct[2];
+    bool serial[2] = {false, false};
+    int model[2] = {MPLB_NO_MODEL, MPLB_NO_MODEL};
+    double* stage = nullptr;
+    size_t stage_elems = 0;
+    double* red = nullptr;  // reduction partials + results
+    int red_parts = 0;
+    FusedConfig fc{};
+    uint32_t current = 0;
+    uint64_t launches = 0;
+    uint64_t bytes = 0;
+    bool initialized = false;
+
+    double* F() { return pdf[0][cur[0]]; }
+    double* G() { return pdf[1][cur[1]]; }
+};
+
+namespace {
+
+template <class T>
+int dalloc(mplb_gpu* h, T** p, size_t count) {
+    size_t b = std::max<size_t>(count, 1) * sizeof(T);
+    CK(cudaMalloc((void**)p, b));
+    CK(cudaMemsetAsync(*p, 0, b, h->stream));
+    h->bytes += b;
+    return 0;
+}
+
+void free_all(mplb_gpu* h) {
+    void* ps[] = {h->nb, h->onb, h->pdf[0][0], h->pdf[0][1], h->pdf[1][0], h->pdf[1][1], h->rho, h->T,
+                  h->S, h->U, h->Fi, h->Ft, h->T2, h->U2, h->bcmap, h->pnodes, h->dpatches, h->stage,
+                  h->red};
+    for (void* p : ps)
+        if (p) cudaFree(p);
+}
+
+// Lattice tables on the host, the same way the reference defines them
+// (D2Q9_omega.c, D2Q9_ppw.c, D3Q15_omega.c, D3Q15_ppw.c, D*_MRTInv.c).
+template <class L>
+void fill_tables(Params& P) {
+    P.Q = L::Q;
+    P.cs2 = 1.0 / 3.0;
+    for (int k = 0; k < L::Q; k++) {
+        int c2 = cxk<L>(k) * cxk<L>(k) + cyk<L>(k) * cyk<L>(k) + czk<L>(k) * czk<L>(k);
+        if (L::Q == 9) {
+            P.w[k] = c2 == 0 ? 4.0 / 9.0 : (c2 == 1 ? 1.0 / 9.0 : 1.0 / 36.0);
+            P.ppw[k] = c2 == 0 ? 0.0 : (c2 == 1 ? 1.0 / 3 : 1.0 / 12);
+        } else {
+            P.w[k] = c2 == 0 ? 2.0 / 9.0 : (c2 == 1 ? 1.0 / 9.0 : 1.0 / 72.0);
+            P.ppw[k] = c2 == 0 ? 0.0 : (c2 == 1 ? 1.0 / 3.0 : 1.0 / 24.0);
+        }
+    }
+    for (int r = 0; r < L::Q; r++) {
+        int norm = 0;
+        for (int k = 0; k < L::Q; k++) norm += Mint<L>(r, k) * Mint<L>(r, k);
+        for (int k = 0; k < L::Q; k++) P.Mi[k][r] = (double)Mint<L>(r, k) / (double)norm;
+    }
+}
+
+int check_field(const mplb_field_desc* d, int lat, int which, uint32_t npatch, std::string& why) {
+    if (!d || d->model == MPLB_NO_MODEL) return 0;
+    if (d->surface_tension != 0) { why = "surface tension terms are not part of this path"; return MPLB_E_UNSUPPORTED; }
+    if (which == 0) {
+        if (d->model == MPLB_LIMRT && lat != MPLB_D2Q9) { why = "liMRT is D2Q9 only (liMRTForce.c:13)"; return MPLB_E_UNSUPPORTED; }
+        if (d->model == MPLB_XUMRT && lat != MPLB_D3Q15) { why = "xuMRT is D3Q15 only (xuMRTForce.c:9)"; return MPLB_E_UNSUPPORTED; }
+        if (d->model != MPLB_LIMRT && d->model != MPLB_XUMRT) { why = "f model must be liMRT or xuMRT"; return MPLB_E_UNSUPPORTED; }
+    } else {
+        if (d->model != MPLB_LITEMPMRT) { why = "g model must be liTempMRT"; return MPLB_E_UNSUPPORTED; }
+        if (lat != MPLB_D2Q9) { why = "liTempMRT is D2Q9 only (liTempMRTEquilibriumMS.c:45-49)"; return MPLB_E_UNSUPPORTED; }
+    }
+    for (uint32_t p = 0; p < npatch; p++) {
+        int t = d->bc_type ? d->bc_type[p] : MPLB_BC_PERIODIC;
+        switch (t) {
+        case MPLB_BC_PERIODIC:
+        case MPLB_BC_BOUNCEBACK: break;
+        case MPLB_BC_FIXEDT:
+            if (d->model != MPLB_LITEMPMRT) { why = "fixedT needs the liTempMRT field (fixedT.c:150-153)"; return MPLB_E_UNSUPPORTED; }
+            break;
+        case MPLB_BC_FIXEDU: break;  // a no-op for models other than liMRT (fixedU.c:10)
+        default:
+            why = "boundary type " + std::to_string(t) + " is outside this path (bounceBack, fixedT, fixedU, periodic)";
+            return MPLB_E_UNSUPPORTED;
+        }
+        if ((t == MPLB_BC_FIXEDT || t == MPLB_BC_FIXEDU) && !d->bc_value) { why = "bc_value missing"; return MPLB_E_ARG; }
+    }
+    return 0;
+}
+
+// Does the neighbour table describe an Nx x Ny x Nz box in x-fastest node
+// order, each axis either wrapping or walled?  Needs coordinates.
+bool detect_box(mplb_gpu* h, const mplb_mesh_desc* m) {
+    if (!m->points) return false;
+    int lo[3], hi[3];
+    for (int j = 0; j < 3; j++) lo[j] = hi[j] = m->points[j];
+    for (uint32_t i = 0; i < h->n; i++)
+        for (int j = 0; j < 3; j++) {
+            lo[j] = std::min(lo[j], m->points[3 * (size_t)i + j]);
+            hi[j] = std::max(hi[j], m->points[3 * (size_t)i + j]);
+        }
+    long long d[3];
+    for (int j = 0; j < 3; j++) d[j] = (long long)hi[j] - lo[j] + 1;
+    if (d[0] * d[1] * d[2] != (long long)h->n) return false;
+    if (h->lat == MPLB_D2Q9 && d[2] != 1) return false;
+    for (uint32_t i = 0; i < h->n; i++) {
+        long long x = m->points[3 * (size_t)i] - lo[0], y = m->points[3 * (size_t)i + 1] - lo[1],
+                  z = m->points[3 * (size_t)i + 2] - lo[2];
+        if (x + d[0] * (y + d[1] * z) != (long long)i) return false;
+    }
+    // Decide each axis from the first node's neighbours, then verify all.
+    int per[3] = {1, 1, 1};
+    for (int ax = 0; ax < 3; ax++) {
+        if (d[ax] == 1) { per[ax] = 1; continue; }
+        // node at coordinate 0 along ax, others 0; direction with c_ax = +1 pulls from -1.
+        int k = -1;
+        for (int q = 0; q < h->Q; q++) {
+            int c[3] = {h->lat == MPLB_D2Q9 ? cxk<D2Q9T>(q) : cxk<D3Q15T>(q),
+                        h->lat == MPLB_D2Q9 ? cyk<D2Q9T>(q) : cyk<D3Q15T>(q),
+                        h->lat == MPLB_D2Q9 ? czk<D2Q9T>(q) : czk<D3Q15T>(q)};
+            int ok = c[ax] == 1;
+            for (int j = 0; j < 3; j++) if (j != ax && c[j] != 0) ok = 0;
+            if (ok) k = q;
+        }
+        per[ax] = m->nb[0 * (size_t)h->Q + k] != -1;
+    }
+    for (uint32_t i = 0; i < h->n; i++) {
+        long long x = i % d[0], y = (i / d[0]) % d[1], z = i / (d[0] * d[1]);
+        for (int q = 0; q < h->Q; q++) {
+            int c[3] = {h->lat == MPLB_D2Q9 ? cxk<D2Q9T>(q) : cxk<D3Q15T>(q),
+                        h->lat == MPLB_D2Q9 ? cyk<D2Q9T>(q) : cyk<D3Q15T>(q),
+                        h->lat == MPLB_D2Q9 ? czk<D2Q9T>(q) : czk<D3Q15T>(q)};
+            long long s[3] = {x - c[0], y - c[1], z - c[2]};
+            bool ok = true;
+            for (int j = 0; j < 3; j++) {
+                if (per[j]) s[j] = ((s[j] % d[j]) + d[j]) % d[j];
+                else if (s[j] < 0 || s[j] >= d[j]) ok = false;
+            }
+            long long want = ok ? s[0] + d[0] * (s[1] + d[1] * s[2]) : -1;
+            if (m->nb[(size_t)i * h->Q + q] != want) return false;
+        }
+    }
+    for (int j = 0; j < 3; j++) { h->dims[j] = (int)d[j]; h->per[j] = per[j]; }
+    return true;
+}
+
+// Can a field's boundary patches run one thread per node?  Not if a node
+// reads a population that any boundary op writes (the reference's serial
+// order would then be observable) or if a patch lists a node twice.
+bool needs_serial(const mplb_gpu* h, const mplb_mesh_desc* m, int fi) {
+    const int Q = h->Q;
+    const int nax = Q == 9 ? 4 : 6;
+    auto rev = [&](int k) { return Q == 9 ? revk<D2Q9T>(k) : revk<D3Q15T>(k); };
+    std::unordered_set<uint64_t> writes;
+    std::vector<uint64_t> reads;
+    size_t off = 0;
+    for (uint32_t p = 0; p < m->n_patches; p++) {
+        int t = h->bct[fi][p];
+        std::unordered_set<uint32_t> seen;
+        for (uint32_t i = 0; i < m->patch_count[p]; i++) {
+            uint32_t id = m->patch_nodes[off + i];
+            if (t == MPLB_BC_PERIODIC || (t == MPLB_BC_FIXEDU && h->model[fi] != MPLB_LIMRT)) continue;
+            if (!seen.insert(id).second) return true;
+            const int32_t* nb = m->nb + (size_t)id * Q;
+            for (int k = 0; k < Q; k++) {
+                if (t == MPLB_BC_BOUNCEBACK) {
+                    if (nb[k] == -1) writes.insert((uint64_t)id * Q + k);
+                    else if (nb[rev(k)] != -1 && k >= 1 && k <= nax) {
+                        writes.insert((uint64_t)id * Q + k);
+                        writes.insert((uint64_t)id * Q + rev(k));
+                    }
+                } else if (nb[k] == -1 && nb[rev(k)] != -1) {
+                    uint32_t nbid = (uint32_t)nb[rev(k)];
+                    writes.insert((uint64_t)id * Q + k);
+                    if (t == MPLB_BC_FIXEDT) reads.push_back((uint64_t)nbid * Q + k);
+                    else
+                        for (int q = 0; q < Q; q++) reads.push_back((uint64_t)nbid * Q + q);
+                }
+            }
+        }
+        off += m->patch_count[p];
+    }
+    for (uint64_t r : reads)
+        if (writes.count(r)) return true;
+    return false;
+}
+
+int launch_check(mplb_gpu* h) {
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return fail(MPLB_E_CUDA, std::string("kernel launch: ") + cudaGetErrorString(e));
+    return 0;
+}
+
+#define LAUNCH(kernel, grid, ...)                                    \
+    do {                                                             \
+        kernel<<<(grid), TPB, 0, h->stream>>>(__VA_ARGS__);          \
+        h->launches++;                                               \
+        if (int rc_ = launch_check(h)) return rc_;                   \
+    } while (0)
+
+// --------------------------------------------------------------- operators
+template <class L>
+int op_equilibrium(mplb_gpu* h, int fi) {
+    if (h->model[fi] == MPLB_NO_MODEL || !(fi == 0 ? h->P.f_update : h->P.g_update)) return 0;
+    if (fi == 0) LAUNCH(k_equilibrium_flow<L>, blocks(h->n), h->P, h->F(), h->rho, h->U);
+    else LAUNCH(k_equilibrium_heat, blocks(h->n), h->P, h->G(), h->T, h->U);
+    return 0;
+}
+
+template <class L>
+int op_collision(mplb_gpu* h, int fi) {
+    if (h->model[fi] == MPLB_NO_MODEL || !(fi == 0 ? h->P.f_update : h->P.g_update)) return 0;
+    if (fi == 0) LAUNCH(k_collide_flow<L>, blocks(h->n), h->P, h->F(), h->rho, h->U, h->T, h->Fi, h->Ft);
+    else LAUNCH(k_collide_heat, blocks(h->n), h->P, h->G(), h->T, h->U, h->S);
+    return 0;
+}
+
+template <class L>
+int op_stream(mplb_gpu* h, int fi) {
+    if (h->model[fi] == MPLB_NO_MODEL || !(fi == 0 ? h->P.f_update : h->P.g_update)) return 0;
+    double* in = h->pdf[fi][h->cur[fi]];
+    double* out = h->pdf[fi][h->cur[fi] ^ 1];
+    LAUNCH(k_stream<L::Q>, blocks(h->n), h->n, out, in, h->nb);
+    h->cur[fi] ^= 1;
+    return 0;
+}
+
+template <class L>
+int op_boundaries(mplb_gpu* h, int fi) {
+    if (h->model[fi] == MPLB_NO_MODEL || !(fi == 0 ? h->P.f_update : h->P.g_update)) return 0;
+    double* pdf = h->pdf[fi][h->cur[fi]];
+    const std::vector<PatchDev>& pts = h->fpatch[fi];
+    bool any = false;
+    for (const PatchDev& pt : pts) {
+        if (pt.type == MPLB_BC_PERIODIC || (pt.type == MPLB_BC_FIXEDU && h->model[fi] != MPLB_LIMRT)) continue;
+        any = true;
+    }
+    if (!any) return 0;
+    if (h->serial[fi]) {
+        LAUNCH(k_bc_serial<L>, 1, h->P, h->dpatches + fi * pts.size(), (int)pts.size(), h->model[fi],
+               h->pnodes, pdf, h->nb, h->rho, h->T, h->U, h->Fi);
+        return 0;
+    }
+    for (const PatchDev& pt : pts) {
+        if (pt.type == MPLB_BC_PERIODIC || pt.count == 0) continue;
+        if (pt.type == MPLB_BC_FIXEDU && h->model[fi] != MPLB_LIMRT) continue;
+        LAUNCH(k_bc_patch<L>, blocks(pt.count), h->P, pt, h->model[fi], h->pnodes, pdf, h->nb, h->rho,
+               h->T, h->U, h->Fi);
+    }
+    return 0;
+}
+
+template <class L>
+int op_density(mplb_gpu* h, uint32_t s, uint32_t e) {
+    if (h->model[0] == MPLB_NO_MODEL || !h->P.f_update || e <= s) return 0;
+    LAUNCH(k_moment0<L::Q>, blocks(e - s), h->n, h->rho, h->F(), s, e);
+    return 0;
+}
+
+template <class L>
+int op_temperature(mplb_gpu* h, uint32_t s, uint32_t e) {
+    if (h->model[1] == MPLB_NO_MODEL || !h->P.g_update || e <= s) return 0;
+    LAUNCH(k_moment0<L::Q>, blocks(e - s), h->n, h->T, h->G(), s, e);
+    return 0;
+}
+
+template <class L>
+int op_velocity(mplb_gpu* h, uint32_t s, uint32_t e) {
+    if (h->model[0] == MPLB_NO_MODEL || !h->P.f_update || e <= s) return 0;
+    LAUNCH(k_velocity<L>, blocks(e - s), h->P, h->U, h->F(), h->rho, h->Fi, h->Ft, s, e);
+    return 0;
+}
+
+template <class L>
+int op_interforce(mplb_gpu* h) {
+    LAUNCH(k_interforce<L>, blocks(h->n), h->P, h->Fi, h->Ft, h->rho, h->T, h->nb, h->onb);
+    return 0;
+}
+
+template <class L>
+int op_heatsource(mplb_gpu* h) {
+    if (h->model[1] == MPLB_NO_MODEL || !h->P.g_update) return 0;
+    LAUNCH(k_heatsource<L>, blocks(h->n), h->P, h->S, h->rho, h->T, h->U, h->nb, h->current == 0 ? 1 : 0);
+    return 0;
+}
+
+#define RET(x) do { if (int rc_ = (x)) return rc_; } while (0)
+
+// multiPhasePP.c:157-240, one operator after another.
+template <class L>
+int step_operators(mplb_gpu* h) {
+    ++h->current;
+    RET(op_collision<L>(h, 0));
+    RET(op_stream<L>(h, 0));
+    RET(op_boundaries<L>(h, 0));
+    RET(op_collision<L>(h, 1));
+    RET(op_stream<L>(h, 1));
+    RET(op_boundaries<L>(h, 1));
+    RET(op_density<L>(h, 0, h->n));
+    if (h->P.g_update) RET(op_heatsource<L>(h));
+    RET(op_temperature<L>(h, 0, h->n));
+    if (h->P.f_update) RET(op_interforce<L>(h));
+    RET(op_velocity<L>(h, 0, h->n));
+    return 0;
+}
+
+template <class L>
+int initialize_impl(mplb_gpu* h) {
+    RET(op_equilibrium<L>(h, 0));
+    RET(op_equilibrium<L>(h, 1));
+    RET(op_interforce<L>(h));
+    RET(op_heatsource<L>(h));
+    h->initialized = true;
+    return 0;
+}
+
+#define DISPATCH(h, fn, ...) \
+    ((h)->lat == MPLB_D2Q9 ? fn<D2Q9T>(__VA_ARGS__) : fn<D3Q15T>(__VA_ARGS__))
+
+int staging(mplb_gpu* h, size_t elems) {
+    if (h->stage_elems >= elems) return 0;
+    if (h->stage) { cudaFree(h->stage); h->bytes -= h->stage_elems * sizeof(double); }
+    h->stage = nullptr;
+    h->stage_elems = 0;
+    CK(cudaMalloc((void**)&h->stage, elems * sizeof(double)));
+    h->stage_elems = elems;
+    h->bytes += elems * sizeof(double);
+    return 0;
+}
+
+int put_aos(mplb_gpu* h, const double* host, double* dev, int m) {
+    if (!host) return 0;
+    size_t e = (size_t)h->n * m;
+    RET(staging(h, e));
+    CK(cudaMemcpyAsync(h->stage, host, e * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+    LAUNCH(k_aos_to_soa, blocks(e), h->n, m, h->stage, dev);
+    return 0;
+}
+
+int get_aos(mplb_gpu* h, double* host, const double* dev, int m) {
+    if (!host) return 0;
+    size_t e = (size_t)h->n * m;
+    RET(staging(h, e));
+    LAUNCH(k_soa_to_aos, blocks(e), h->n, m, dev, h->stage);
+    CK(cudaMemcpyAsync(host, h->stage, e * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    return 0;
+}
+
+int get_scalar(mplb_gpu* h, double* host, const double* dev) {
+    if (!host) return 0;
+    CK(cudaMemcpyAsync(host, dev, (size_t)h->n * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    return 0;
+}
+
+int put_scalar(mplb_gpu* h, const double* host, double* dev) {
+    if (!host) return 0;
+    CK(cudaMemcpyAsync(dev, host, (size_t)h->n * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+    return 0;
+}
+
+struct DeviceGuard {
+    int prev = -1;
+    explicit DeviceGuard(int dev) {
+        cudaGetDevice(&prev);
+        if (prev != dev) cudaSetDevice(dev);
+    }
+    ~DeviceGuard() {
+        int now = -1;
+        cudaGetDevice(&now);
+        if (prev >= 0 && now != prev) cudaSetDevice(prev);
+    }
+};
+
+}  // namespace
+
+// ================================================================= C-ABI
+extern "C" {
+
+const char* mplb_gpu_version(void) { return "multiphaselb-b200 1 (sm_100a, FP64)"; }
+const char* mplb_gpu_last_error(void) { return g_err.c_str(); }
+
+int mplb_gpu_create(const mplb_mesh_desc* mesh, const mplb_eos_desc* eos, const mplb_field_desc* f,
+                    const mplb_field_desc* g, const mplb_opts* opts, mplb_gpu_t** out) {
+    if (!out) return fail(MPLB_E_ARG, "out is NULL");
+    *out = nullptr;
+    if (!mesh || !eos) return fail(MPLB_E_ARG, "mesh and eos descriptors are required");
+    if (mesh->lattice != MPLB_D2Q9 && mesh->lattice != MPLB_D3Q15) return fail(MPLB_E_ARG, "unknown lattice");
+    if (mesh->n_points == 0 || !mesh->nb) return fail(MPLB_E_ARG, "empty mesh");
+    if (mesh->n_patches > MPLB_MAX_PATCHES) return fail(MPLB_E_ARG, "too many boundary patches");
+    if (mesh->n_patches && (!mesh->patch_count || !mesh->patch_nodes)) return fail(MPLB_E_ARG, "patch lists missing");
+    if (eos->type < MPLB_EOS_IDEAL || eos->type > MPLB_EOS_VDW) return fail(MPLB_E_ARG, "unknown EOS");
+    if (opts && opts->precision != MPLB_FP64) return fail(MPLB_E_UNSUPPORTED, "only FP64 storage is built");
+    const int Q = mesh->lattice == MPLB_D2Q9 ? 9 : 15;
+    const size_t nq = (size_t)mesh->n_points * Q;
+    for (size_t i = 0; i < nq; i++)
+        if (mesh->nb[i] < -1 || mesh->nb[i] >= (int64_t)mesh->n_points)
+            return fail(MPLB_E_ARG, "neighbour index out of range at entry " + std::to_string(i));
+    size_t tot = 0;
+    for (uint32_t p = 0; p < mesh->n_patches; p++) tot += mesh->patch_count[p];
+    for (size_t i = 0; i < tot; i++)
+        if (mesh->patch_nodes[i] >= mesh->n_points) return fail(MPLB_E_ARG, "boundary node out of range");
+    std::string why;
+    if (int rc = check_field(f, mesh->lattice, 0, mesh->n_patches, why)) return fail(rc, why);
+    if (int rc = check_field(g, mesh->lattice, 1, mesh->n_patches, why)) return fail(rc, why);
+
+    mplb_gpu* h = new mplb_gpu();
+    h->lat = mesh->lattice;
+    h->Q = Q;
+    h->D = Q == 9 ? 2 : 3;
+    h->n = mesh->n_points;
+    h->current = opts ? opts->start_time : 0;
+    int want_path = opts ? opts->path : MPLB_PATH_AUTO;
+    int dev = opts ? opts->device : -1;
+    if (dev < 0) {
+        if (cudaGetDevice(&dev) != cudaSuccess) { delete h; return fail(MPLB_E_CUDA, "no CUDA device"); }
+    }
+    h->dev = dev;
+    DeviceGuard guard(dev);
+    if (cudaSetDevice(dev) != cudaSuccess) { delete h; return fail(MPLB_E_CUDA, "cudaSetDevice failed"); }
+    if (opts && opts->stream) {
+        h->stream = (cudaStream_t)opts->stream;
+    } else {
+        if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess) {
+            delete h;
+            return fail(MPLB_E_CUDA, "stream creation failed");
+        }
+        h->own_stream = true;
+    }
+
+    // Parameter block.
+    Params& P = h->P;
+    P.lat = h->lat;
+    P.n = h->n;
+    if (h->lat == MPLB_D2Q9) fill_tables<D2Q9T>(P);
+    else fill_tables<D3Q15T>(P);
+    h->model[0] = f ? f->model : MPLB_NO_MODEL;
+    h->model[1] = g ? g->model : MPLB_NO_MODEL;
+    P.f_model = h->model[0];
+    P.g_model = h->model[1];
+    P.f_update = (f && f->model != MPLB_NO_MODEL && f->update) ? 1 : 0;
+    P.g_update = (g && g->model != MPLB_NO_MODEL && g->update) ? 1 : 0;
+    if (f && f->model != MPLB_NO_MODEL) {
+        for (int k = 0; k < MPLB_MAX_Q; k++) {
+            P.Lf[k] = f->Lambda[k];
+            P.relax_f[k] = (1 - 0.5 * f->Lambda[k]);
+        }
+        P.s1_den = ((1 / f->Lambda[1]) - 0.5);
+        P.s2_den = ((1 / f->Lambda[2]) - 0.5);
+        P.sig12 = 12 * f->sigma;
+        P.sig6 = 6.0 * f->sigma;
+    }
+    if (g && g->model != MPLB_NO_MODEL) {
+        for (int k = 0; k < MPLB_MAX_Q; k++) P.Lg[k] = g->Lambda[k];
+        P.corr3 = (1 - g->Lambda[3] / 2) * g->Lambda[4];
+        P.corr5 = (1 - g->Lambda[5] / 2) * g->Lambda[6];
+        P.lam_fac = (1 / g->Lambda[3] - 0.5);
+    }
+    P.eos = eos->type;
+    P.a = eos->a;
+    P.b = eos->b;
+    P.R = eos->R;
+    P.G = eos->G;
+    P.M = eos->M;
+    P.Cv = eos->Cv;
+    P.rho_0 = eos->rho_0;
+    for (int j = 0; j < 3; j++) { P.g[j] = eos->g[j]; P.fext[j] = eos->fext[j]; }
+    if (eos->type == MPLB_EOS_PR) {
+        P.pr_tc = 0.170151343 * eos->a / (eos->b * eos->R);
+        P.pr_kappa = 0.37464 + 1.5422 * eos->w - 0.26992 * eos->w * eos->w;
+    }
+
+    // Boundary tables per field.
+    const mplb_field_desc* fds[2] = {f, g};
+    for (int fi = 0; fi < 2; fi++) {
+        h->bct[fi].assign(mesh->n_patches, MPLB_BC_PERIODIC);
+        if (fds[fi] && fds[fi]->model != MPLB_NO_MODEL && fds[fi]->bc_type)
+            for (uint32_t p = 0; p < mesh->n_patches; p++) h->bct[fi][p] = fds[fi]->bc_type[p];
+    }
+    for (int fi = 0; fi < 2; fi++) {
+        uint32_t off = 0;
+        for (uint32_t p = 0; p < mesh->n_patches; p++) {
+            PatchDev d{};
+            d.off = off;
+            d.count = mesh->patch_count[p];
+            d.type = h->bct[fi][p];
+            if (fds[fi] && fds[fi]->model != MPLB_NO_MODEL && fds[fi]->bc_value)
+                for (int j = 0; j < 3; j++) d.val[j] = fds[fi]->bc_value[3 * p + j];
+            h->fpatch[fi].push_back(d);
+            off += mesh->patch_count[p];
+        }
+    }
+    for (int fi = 0; fi < 2; fi++) h->serial[fi] = needs_serial(h, mesh, fi);
+    h->box = detect_box(h, mesh);
+
+    // Device buffers.
+    int rc = 0;
+    auto bail = [&](int code) {
+        std::string keep = g_err;
+        free_all(h);
+        if (h->own_stream) cudaStreamDestroy(h->stream);
+        delete h;
+        g_err = keep;
+        return code;
+    };
+    if ((rc = dalloc(h, &h->nb, nq)) || (rc = dalloc(h, &h->onb, h->n)) || (rc = dalloc(h, &h->rho, h->n)) ||
+        (rc = dalloc(h, &h->T, h->n)) || (rc = dalloc(h, &h->S, h->n)) || (rc = dalloc(h, &h->U, 3 * (size_t)h->n)) ||
+        (rc = dalloc(h, &h->Fi, 3 * (size_t)h->n)) || (rc = dalloc(h, &h->Ft, 3 * (size_t)h->n)) ||
+        (rc = dalloc(h, &h->pnodes, tot)) || (rc = dalloc(h, &h->dpatches, 2 * std::max<size_t>(1, mesh->n_patches))))
+        return bail(rc);
+    for (int fi = 0; fi < 2; fi++) {
+        if (h->model[fi] == MPLB_NO_MODEL) continue;
+        if ((rc = dalloc(h, &h->pdf[fi][0], nq)) || (rc = dalloc(h, &h->pdf[fi][1], nq))) return bail(rc);
+    }
+    {
+        // neighbour table to [k][n], boundary flags
+        std::vector<int32_t> nbs(nq);
+        std::vector<uint8_t> onb(h->n, 0);
+        for (uint32_t i = 0; i < h->n; i++)
+            for (int k = 0; k < Q; k++) {
+                int32_t s = mesh->nb[(size_t)i * Q + k];
+                nbs[(size_t)k * h->n + i] = s;
+                if (s == -1) onb[i] = 1;  // readLatticeMesh.c:171-203
+            }
+        if (cudaMemcpy(h->nb, nbs.data(), nq * sizeof(int32_t), cudaMemcpyHostToDevice) != cudaSuccess ||
+            cudaMemcpy(h->onb, onb.data(), h->n, cudaMemcpyHostToDevice) != cudaSuccess ||
+            (tot && cudaMemcpy(h->pnodes, mesh->patch_nodes, tot * sizeof(uint32_t), cudaMemcpyHostToDevice) != cudaSuccess))
+            return bail(fail(MPLB_E_CUDA, "copying the mesh failed"));
+        std::vector<PatchDev> both(h->fpatch[0]);
+        both.insert(both.end(), h->fpatch[1].begin(), h->fpatch[1].end());
+        if (!both.empty() &&
+            cudaMemcpy(h->dpatches, both.data(), both.size() * sizeof(PatchDev), cudaMemcpyHostToDevice) != cudaSuccess)
+            return bail(fail(MPLB_E_CUDA, "copying the patches failed"));
+    }
+    // Execution path.
+    std::string fwhy;
+    bool fusable = h->box && fused_supported(h->lat, h->model, h->P, h->fpatch, h->serial, mesh, h->dims, h->per, fwhy);
+    if (want_path == MPLB_PATH_FUSED && !fusable) return bail(fail(MPLB_E_UNSUPPORTED, "fused path unavailable: " + (h->box ? fwhy : std::string("mesh is not a box"))));
+    h->path = (want_path == MPLB_PATH_OPERATORS || !fusable) ? MPLB_PATH_OPERATORS : MPLB_PATH_FUSED;
+    if (h->path == MPLB_PATH_FUSED) {
+        if ((rc = fused_setup(h->fc, h->lat, h->model, h->P, h->fpatch, mesh, h->dims, h->per, h->stream, &h->bytes)))
+            return bail(fail(rc, "fused setup: " + h->fc.err));
+        if ((rc = dalloc(h, &h->T2, h->n)) || (rc = dalloc(h, &h->U2, 3 * (size_t)h->n))) return bail(rc);
+    }
+    h->red_parts = 2 * 148;
+    if ((rc = dalloc(h, &h->red, 2 * (size_t)h->red_parts + 8))) return bail(rc);
+    if (cudaStreamSynchronize(h->stream) != cudaSuccess) return bail(fail(MPLB_E_CUDA, "device set-up failed"));
+    *out = h;
+    return 0;
+}
+
+int mplb_gpu_destroy(mplb_gpu_t* h) {
+    if (!h) return 0;
+    DeviceGuard guard(h->dev);
+    cudaStreamSynchronize(h->stream);
+    fused_free(h->fc);
+    free_all(h);
+    if (h->own_stream) cudaStreamDestroy(h->stream);
+    delete h;
+    return 0;
+}
+
+int mplb_gpu_info(mplb_gpu_t* h, mplb_info* info) {
+    if (!h || !info) return fail(MPLB_E_ARG, "NULL argument");
+    info->path = h->path;
+    for (int j = 0; j < 3; j++) { info->box_dims[j] = h->box ? h->dims[j] : 0; info->box_periodic[j] = h->box ? h->per[j] : 0; }
+    info->bc_sequential = (h->serial[0] ? 1 : 0) | (h->serial[1] ? 2 : 0);
+    info->current_time = h->current;
+    info->device_bytes = h->bytes;
+    info->kernel_launches = h->launches;
+    return 0;
+}
+
+int mplb_gpu_upload(mplb_gpu_t* h, const double* rho, const double* U, const double* T, const double* f,
+                    const double* g, const double* S, const double* Fi, const double* Ft) {
+    if (!h) return fail(MPLB_E_ARG, "NULL handle");
+    DeviceGuard guard(h->dev);
+    RET(put_scalar(h, rho, h->rho));
+    RET(put_scalar(h, T, h->T));
+    RET(put_scalar(h, S, h->S));
+    RET(put_aos(h, U, h->U, 3));
+    RET(put_aos(h, Fi, h->Fi, 3));
+    RET(put_aos(h, Ft, h->Ft, 3));
+    if (f && h->model[0] != MPLB_NO_MODEL) RET(put_aos(h, f, h->F(), h->Q));
+    if (g && h->model[1] != MPLB_NO_MODEL) RET(put_aos(h, g, h->G(), h->Q));
+    CK(cudaStreamSynchronize(h->stream));
+    return 0;
+}
+
+int mplb_gpu_download(mplb_gpu_t* h, double* rho, double* U, double* T, double* Fi, double* Ft, double* S,
+                      double* f, double* g) {
+    if (!h) return fail(MPLB_E_ARG, "NULL handle");
+    DeviceGuard guard(h->dev);
+    RET(get_scalar(h, rho, h->rho));
+    RET(get_scalar(h, T, h->T));
+    RET(get_scalar(h, S, h->S));
+    RET(get_aos(h, U, h->U, 3));
+    RET(get_aos(h, Fi, h->Fi, 3));
+    RET(get_aos(h, Ft, h->Ft, 3));
+    if (f) {
+        if (h->model[0] == MPLB_NO_MODEL) std::memset(f, 0, (size_t)h->n * h->Q * sizeof(double));
+        else RET(get_aos(h, f, h->F(), h->Q));
+    }
+    if (g) {
+        if (h->model[1] == MPLB_NO_MODEL) std::memset(g, 0, (size_t)h->n * h->Q * sizeof(double));
+        else RET(get_aos(h, g, h->G(), h->Q));
+    }
+    return 0;
+}
+
+int mplb_gpu_initialize(mplb_gpu_t* h) {
+    if (!h) return fail(MPLB_E_ARG, "NULL handle");
+    DeviceGuard guard(h->dev);
+    return DISPATCH(h, initialize_impl, h);
+}
+
+int mplb_gpu_step(mplb_gpu_t* h, uint32_t nsteps) {
+    if (!h) return fail(MPLB_E_ARG, "NULL handle");
+    if (nsteps == 0) return 0;
+    DeviceGuard guard(h->dev);
+    if (h->path == MPLB_PATH_FUSED) {
+        int rc = fused_run(h->fc, h->P, nsteps, h->current, h->pdf, h->cur, h->rho, h->T, h->T2, h->S, h->U,
+                           h->U2, h->Fi, h->Ft, h->stream, &h->launches);
+        if (rc) return fail(rc, h->fc.err);
+        h->current += nsteps;
+        return 0;
+    }
+    for (uint32_t s = 0; s < nsteps; s++) RET(DISPATCH(h, step_operators, h));
+    return 0;
+}
+
+int mplb_gpu_equilibrium(mplb_gpu_t* h, int32_t field) {
+    if (!h || (field != MPLB_FIELD_F && field != MPLB_FIELD_G)) return fail(MPLB_E_ARG, "bad handle or field");
+    DeviceGuard guard(h->dev);
+    return DISPATCH(h, op_equilibrium, h, field);
+}
+int mplb_gpu_collision(mplb_gpu_t* h, int32_t field) {
+    if (!h || (field != MPLB_FIELD_F && field != MPLB_FIELD_G)) return fail(MPLB_E_ARG, "bad handle or field");
+    DeviceGuard guard(h->dev);
+    return DISPATCH(h, op_collision, h, field);
+}
+int mplb_gpu_lbstream(mplb_gpu_t* h, int32_t field) {
+    if (!h || (field != MPLB_FIELD_F && field != MPLB_FIELD_G)) return fail(MPLB_E_ARG, "bad handle or field");
+    DeviceGuard guard(h->dev);
+    return DISPATCH(h, op_stream, h, field);
+}
+int mplb_gpu_update_boundaries(mplb_gpu_t* h, int32_t field) {
+    if (!h || (field != MPLB_FIELD_F && field != MPLB_FIELD_G)) return fail(MPLB_E_ARG, "bad handle or field");
+    DeviceGuard guard(h->dev);
+    return DISPATCH(h, op_boundaries, h, field);
+}
+int mplb_gpu_macro_density(mplb_gpu_t* h, uint32_t start, uint32_t end) {
+    if (!h || start > end || end > h->n) return fail(MPLB_E_ARG, "bad handle or node range");
+    if (h->model[0] != MPLB_LIMRT && h->model[0] != MPLB_XUMRT && h->P.f_update)
+        return fail(MPLB_E_UNSUPPORTED, "Density update not available (macroDensity.c:65-67)");
+    DeviceGuard guard(h->dev);
+    return DISPATCH(h, op_density, h, start, end);
+}
+int mplb_gpu_macro_velocity(mplb_gpu_t* h, uint32_t start, uint32_t end) {
+    if (!h || start > end || end > h->n) return fail(MPLB_E_ARG, "bad handle or node range");
+    DeviceGuard guard(h->dev);
+    return DISPATCH(h, op_velocity, h, start, end);
+}
+int mplb_gpu_macro_temperature(mplb_gpu_t* h, uint32_t start, uint32_t end) {
+    if (!h || start > end || end > h->n) return fail(MPLB_E_ARG, "bad handle or node range");
+    DeviceGuard guard(h->dev);
+    return DISPATCH(h, op_temperature, h, start, end);
+}
+int mplb_gpu_inter_force(mplb_gpu_t* h) {
+    if (!h) return fail(MPLB_E_ARG, "NULL handle");
+    DeviceGuard guard(h->dev);
+    return DISPATCH(h, op_interforce, h);
+}
+int mplb_gpu_heat_source(mplb_gpu_t* h) {
+    if (!h) return fail(MPLB_E_ARG, "NULL handle");
+    DeviceGuard guard(h->dev);
+    return DISPATCH(h, op_heatsource, h);
+}
+
+int mplb_gpu_set_time(mplb_gpu_t* h, uint32_t current) {
+    if (!h) return fail(MPLB_E_ARG, "NULL handle");
+    h->current = current;
+    return 0;
+}
+
+int mplb_gpu_set_rho0(mplb_gpu_t* h, double rho_0) {
+    if (!h) return fail(MPLB_E_ARG, "NULL handle");
+    h->P.rho_0 = rho_0;
+    return 0;
+}
+
+int mplb_gpu_average_rho0(mplb_gpu_t* h, double* rho_0) {
+    if (!h) return fail(MPLB_E_ARG, "NULL handle");
+    DeviceGuard guard(h->dev);
+    double avg = 0;
+    if (!(h->P.rho_0 <= 0)) {
+        LAUNCH(k_sum_serial, 1, h->n, h->rho, h->red);
+        double s = 0;
+        CK(cudaMemcpyAsync(&s, h->red, sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+        CK(cudaStreamSynchronize(h->stream));
+        avg = s / (int)h->n;
+    }
+    h->P.rho_0 = avg;
+    if (rho_0) *rho_0 = avg;
+    return 0;
+}
+
+int mplb_gpu_mass_energy(mplb_gpu_t* h, double* mass, double* energy) {
+    if (!h) return fail(MPLB_E_ARG, "NULL handle");
+    DeviceGuard guard(h->dev);
+    int parts = std::min<int>(h->red_parts, (int)blocks(h->n));
+    k_sum2_partial<<<parts, TPB, 0, h->stream>>>(h->n, h->rho, h->T, h->red);
+    h->launches++;
+    RET(launch_check(h));
+    k_sum2_final<<<1, TPB, 0, h->stream>>>(parts, h->red, h->red + 2 * h->red_parts);
+    h->launches++;
+    RET(launch_check(h));
+    double r[2] = {0, 0};
+    CK(cudaMemcpyAsync(r, h->red + 2 * h->red_parts, 2 * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    if (mass) *mass = r[0];
+    if (energy) *energy = r[1];
+    return 0;
+}
+
+int mplb_gpu_sync(mplb_gpu_t* h) {
+    if (!h) return fail(MPLB_E_ARG, "NULL handle");
+    DeviceGuard guard(h->dev);
+    CK(cudaStreamSynchronize(h->stream));
+    return 0;
+}
+
+}  // extern "C"
