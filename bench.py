@@ -1,0 +1,360 @@
+"""Benchmark of the B200 lattice update (multiphaseLB per-timestep path).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--workload NAME]
+
+Default workload: the thermal van der Waals column, D2Q9, 128 x 512 nodes,
+liMRT flow + liTempMRT heat, bounce-back / fixedT walls, FP64, on the fused
+box path.  One step = one time step of the whole lattice.  The lattice state
+(~21 MB) fits in L2, so a 256 MiB buffer is written between timed steps and
+each step is timed alone with CUDA events on the library's stream.
+
+For N > 1 (torchrun, one process per GPU) every rank advances its own
+replica of the workload (weak scaling; the path has no exchange step on one
+domain), and the time is the max over ranks.
+
+Prints one JSON line (rank 0).
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+METRIC = "GLUPS on 1 B200 (FP64 vs FP32-dev); time-to-equilibrium w/ warm start"
+
+# Algorithmic bytes per lattice-node update (FP64): every population read
+# once and written once, plus per-node state that cannot be rebuilt from the
+# populations (the heat-source history S: read + write).
+WORKLOADS = {
+    "column_d2q9_128x512": dict(bytes_per_lup=304, desc="thermal VdW column, D2Q9, f+g, bounceBack+fixedT walls, periodic x",
+                                build=lambda c: c.column_case(128, 512)),
+    "bubble_d2q9_256": dict(bytes_per_lup=144, desc="static bubble, D2Q9 liMRT, fully periodic",
+                            build=lambda c: c.bubble_case(0, 256, 40.0, 5.0, 0.8)),
+    "bubble_d3q15_192": dict(bytes_per_lup=240, desc="static bubble, D3Q15 xuMRT, fully periodic",
+                             build=lambda c: c.bubble_case(1, 192, 48.0, 5.0, 0.75)),
+}
+PROFILE_TRAFFIC = {  # per-launch DRAM bytes summaries committed under profiles/
+    "column_d2q9_128x512": "fused_d2q9_column_128x512.txt",
+    "bubble_d3q15_192": "fused_d3q15_bubble_192.txt",
+}
+FALLBACK_HBM_GBS = 6650.0
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as fh:
+            d = json.load(fh)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+def profiled_traffic(workload):
+    """DRAM bytes per launch of the fused kernel from the committed ncu summary."""
+    name = PROFILE_TRAFFIC.get(workload)
+    if not name:
+        return None
+    path = os.path.join(ROOT, "profiles", name)
+    try:
+        for line in open(path):
+            if line.startswith("dram_bytes_per_full_launch:"):
+                return float(line.split(":", 1)[1].split()[0])
+    except OSError:
+        return None
+    return None
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.rows = []
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) >= 9:
+                self.rows.append(parts)
+
+    def mark(self):
+        return len(self.rows)
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self, start=0):
+        rows = self.rows[start:] or self.rows
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import torch.distributed as dist
+        import datetime
+        backend = "nccl" if os.environ.get("MPLB_BENCH_BACKEND", "nccl") == "nccl" else "gloo"
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=120))
+    return world, rank, local
+
+
+def max_over_ranks(x, world, device):
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(world, device):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier(device_ids=[device.index] if device.type == "cuda" else None)
+
+
+# --------------------------------------------------------------- CPU baseline
+def _cpu_worker(args):
+    """One single-core reference run of `steps` steps on the workload (spawned process)."""
+    workload, steps, kind = args
+    sys.path.insert(0, ROOT)
+    from multiphaselb_b200 import cases
+    from oracle.oracle import Checker
+    case = WORKLOADS[workload]["build"](cases)
+    k = Checker(kind, case)
+    k.upload_case()
+    k.initialize()
+    t0 = time.perf_counter()
+    k.step(steps)
+    dt = time.perf_counter() - t0
+    return case.n * steps, dt
+
+
+def cpu_baseline(workload, steps, procs):
+    """Reference CPU solver (oracle/_ref, single-threaded like the reference)
+    on `procs` host cores, each running an independent copy for `steps` steps."""
+    from oracle import oracle as orc
+    kind = "ref" if orc.available("ref") else "port"
+    if not orc.available(kind):
+        orc.build(kind)
+    import multiprocessing as mp
+    ctx = mp.get_context("spawn")
+    t0 = time.perf_counter()
+    if procs == 1:
+        res = [_cpu_worker((workload, steps, kind))]
+    else:
+        with ctx.Pool(procs) as pool:
+            res = pool.map(_cpu_worker, [(workload, steps, kind)] * procs)
+    wall = time.perf_counter() - t0
+    lups = sum(r[0] for r in res)
+    slowest = max(r[1] for r in res)
+    return dict(value=lups / slowest / 1e9, unit="GLUPS", cores=procs,
+                kind="reference" if kind == "ref" else "port",
+                sample=f"{steps} steps of the full {WORKLOADS[workload]['desc']} lattice per core, "
+                       f"{procs} independent single-threaded copies (the reference has no threads; its "
+                       f"parallelism is MPI ranks, absent here); wall {wall:.1f}s")
+
+
+# -------------------------------------------------------------------- our arm
+def run_ours(a):
+    import torch
+    from multiphaselb_b200 import PATH_AUTO, PATH_FUSED, PATH_OPERATORS, Lattice, cases
+    world, rank, local = dist_setup()
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    wl = WORKLOADS[a.workload]
+    case = wl["build"](cases)
+    path = {"auto": PATH_AUTO, "fused": PATH_FUSED, "operators": PATH_OPERATORS}[a.path]
+    stream = torch.cuda.Stream(device=dev)
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)  # 256 MiB > 126 MB L2
+    peak, peak_kind = peaks()
+
+    with torch.cuda.stream(stream):
+        lat = Lattice(case, path=path, device=local, stream=stream.cuda_stream)
+        lat.upload_case()
+        lat.initialize()
+        info0 = lat.info()
+        for _ in range(a.warmup):
+            lat.step(1)
+        torch.cuda.synchronize()
+        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(a.steps)]
+        barrier(world, dev)
+        torch.cuda.synchronize()
+        with ClockSampler(local) as clk:
+            time.sleep(0.3)
+            mark = clk.mark()
+            launches0 = lat.info()["kernel_launches"]
+            for i in range(a.steps):
+                flush.zero_()
+                ev[i][0].record(stream)
+                lat.step(1)
+                ev[i][1].record(stream)
+            torch.cuda.synchronize()
+            launches = lat.info()["kernel_launches"] - launches0
+            time.sleep(0.25)
+            clocks = clk.summary(mark)
+        barrier(world, dev)
+        step_ms = [s.elapsed_time(e) for s, e in ev]
+        total_ms = max_over_ranks(sum(step_ms), world, dev)
+        kernel_ms = sum(step_ms) / len(step_ms)  # one fused launch per step
+        info = lat.info()
+        lat.close()
+
+    # end to end through the C-ABI: pinned host fields -> device, steps, all fields back
+    n, Q = case.n, case.Q
+    pin = lambda shape: torch.empty(shape, dtype=torch.float64, pin_memory=True).numpy()  # noqa: E731
+    h_rho, h_U, h_T = pin((n,)), pin((n, 3)), pin((n,))
+    h_rho[:], h_U[:], h_T[:] = case.rho, case.U, case.T
+    out = dict(rho=pin((n,)), U=pin((n, 3)), T=pin((n,)), Fi=pin((n, 3)), Ft=pin((n, 3)), S=pin((n,)),
+               f=pin((n, Q)), g=pin((n, Q)))
+    e2e_steps = a.steps
+    with torch.cuda.stream(stream):
+        lat = Lattice(case, path=path, device=local, stream=stream.cuda_stream)
+        lat.upload(rho=h_rho, U=h_U, T=h_T)
+        lat.initialize()
+        lat.step(a.warmup)
+        lat.download(out)
+        barrier(world, dev)
+        torch.cuda.synchronize()
+        t0 = torch.cuda.Event(enable_timing=True)
+        t1 = torch.cuda.Event(enable_timing=True)
+        t0.record(stream)
+        lat.upload(rho=h_rho, U=h_U, T=h_T)
+        lat.initialize()
+        lat.step(e2e_steps)
+        lat.download(out)
+        t1.record(stream)
+        torch.cuda.synchronize()
+        e2e_ms = max_over_ranks(t0.elapsed_time(t1), world, dev)
+        lat.close()
+    h2d = n * (1 + 3 + 1) * 8
+    d2h = n * (1 + 3 + 1 + 3 + 3 + 1 + Q + (Q if case.g is not None else Q)) * 8
+
+    glups = n * a.steps * world / (total_ms * 1e-3) / 1e9
+    achieved = wl["bytes_per_lup"] * n / (kernel_ms * 1e-3) / 1e9
+    traffic = profiled_traffic(a.workload)
+    line = {
+        "metric": METRIC, "value": round(glups, 4), "unit": "GLUPS", "n_gpus": world,
+        "steps": a.steps, "warmup": a.warmup, "ms_per_step": round(total_ms / a.steps, 6),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded lattice of the named shape; no dataset)",
+        "config": {"workload": a.workload, "desc": wl["desc"], "nodes_per_gpu": n,
+                   "path": {0: "auto", 1: "operators", 2: "fused"}[path] + f" -> {['', 'operators', 'fused'][info0['path']]}",
+                   "l2": "256 MiB buffer written between timed steps; each step timed alone",
+                   "parallelism": f"replicas x{world}", "bytes_per_lup": wl["bytes_per_lup"]},
+        "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                     "frac": round(achieved / peak, 4), "peak_source": f"{peak_kind} MEASURED_PEAKS hbm_gbs" if peak_kind == "measured" else "fallback 6.65 TB/s",
+                     "traffic": traffic,
+                     "kernel": "k_fused_d2q9" if case.lattice == 0 else "k_fused_d3q15",
+                     "kernel_ms": round(kernel_ms, 6)},
+        "e2e": {"value": round(n * e2e_steps * world / (e2e_ms * 1e-3) / 1e9, 4), "unit": "GLUPS",
+                "h2d_bytes_per_step": round(h2d / e2e_steps, 1), "d2h_bytes_per_step": round(d2h / e2e_steps, 1),
+                "timed": f"upload rho/U/T from pinned host memory, initialize, {e2e_steps} steps, download every field"},
+        "gpu_launches": int(launches),
+        "clocks": clocks,
+    }
+    if rank == 0 and world == 1 and not a.no_cpu:
+        line["cpu_baseline"] = cpu_baseline(a.workload, a.cpu_steps, 1)
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
+def run_reference(a):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    procs = a.cpu_procs or max(1, (os.cpu_count() or 1))
+    procs = min(procs, 64)
+    samples = []
+    for _ in range(a.warmup and 1 or 0):
+        cpu_baseline(a.workload, max(1, a.cpu_steps // 10), procs)
+    t0 = time.perf_counter()
+    for _ in range(max(1, a.ref_repeats)):
+        samples.append(cpu_baseline(a.workload, a.cpu_steps, procs))
+    wall = time.perf_counter() - t0
+    best = samples[-1]
+    v = statistics.median(s["value"] for s in samples)
+    line = {
+        "metric": METRIC, "value": round(v, 6), "unit": "GLUPS", "n_gpus": world, "steps": a.cpu_steps,
+        "warmup": a.warmup, "ms_per_step": None, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded lattice of the named shape)",
+        "impl": "reference",
+        "config": {"workload": a.workload, "desc": WORKLOADS[a.workload]["desc"],
+                   "parallelism": f"{procs} independent single-threaded reference processes"},
+        "cpu_baseline": {"value": round(v, 6), "unit": "GLUPS", "cores": procs, "kind": best["kind"],
+                         "sample": best["sample"]},
+        "e2e": {"value": round(v, 6), "unit": "GLUPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "wall_s": round(wall, 2),
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=2000)
+    ap.add_argument("--warmup", type=int, default=20)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="column_d2q9_128x512", choices=list(WORKLOADS))
+    ap.add_argument("--path", default="auto", choices=["auto", "fused", "operators"])
+    ap.add_argument("--cpu-steps", type=int, default=150)
+    ap.add_argument("--cpu-procs", type=int, default=0)
+    ap.add_argument("--ref-repeats", type=int, default=1)
+    ap.add_argument("--no-cpu", action="store_true")
+    a = ap.parse_args()
+    if a.warmup < 3:
+        ap.error("--warmup must be >= 3")
+    if a.impl == "reference":
+        run_reference(a)
+    else:
+        run_ours(a)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,31 +1,598 @@
-// fused.cuh -- fused box kernels (placeholder until the fused path lands).
+// fused.cuh -- one kernel per time step on structured boxes.
+//
+// The reference advances a step with eleven passes over the lattice
+// (multiPhasePP.c:163-240).  On a box mesh the whole step is one kernel that
+// reads each population once and writes it once:
+//
+//   step n:  pull-stream f*_n, g*_n  ->  f''_n, g''_n         (lbstream.c)
+//            boundary programs at wall nodes                   (bounceBack.c, fixedT.c)
+//            rho_n = sum f'', T_n = sum g''                    (macroDensity/Temperature)
+//            psi_n, 1/rho_n on the tile + a one-node ring      (potential.c)
+//            heat source S_n from rho_n, T_{n-1}, U_{n-1}      (heatSource.c)
+//            Fi_n, Ft_n, U_n                                   (interForce.c, liMRTVelocity.c)
+//            collide -> f*_{n+1}, g*_{n+1}                     (liMRTCollision.c, ...)
+//
+// so the state carried between kernels is the post-collision populations
+// (double-buffered), T and U (double-buffered: neighbours read the previous
+// step's values) and S.  The reference's own state after step n (f''_n,
+// rho_n, Fi_n, Ft_n) is rebuilt on demand by the same kernel in EMIT mode from
+// the retained input buffer of the last step.
+//
+// Arithmetic per node is the shared code of lattice.cuh, so results equal
+// the operator path (and the reference) bit for bit.
 #pragma once
+
+#include <algorithm>
+#include <cstring>
 #include <string>
 #include <vector>
+
 #include "ops.cuh"
 
 namespace mplb {
 
-struct FusedConfig {
-    std::string err;
+constexpr int FUSED_MAX_PROGS = 64;
+constexpr int FUSED_MAX_OPS = 3;
+
+// Boundary operations of one node, per field, in patch order.
+struct BCProg {
+    uint8_t nf, ng;
+    uint8_t ft[FUSED_MAX_OPS], gt[FUSED_MAX_OPS];  // MPLB_BC_BOUNCEBACK or MPLB_BC_FIXEDT
+    uint8_t gp[FUSED_MAX_OPS];                      // patch index of a fixedT op
 };
 
-inline bool fused_supported(int, const int*, const Params&, const std::vector<PatchDev>*, const bool*,
-                            const mplb_mesh_desc*, const int*, const int*, std::string& why) {
-    why = "fused kernels not built";
-    return false;
+struct FusedArgs {
+    int nx, ny, nz;
+    int px, py, pz;     // 1 = periodic axis
+    int tiles_x, tiles_y, zchunk;
+    const double* fin;
+    double* fout;
+    const double* gin;
+    double* gout;
+    const double* Told;  // T of the previous step (the only T when g is frozen)
+    double* Tnew;
+    const double* Uold;  // U of the previous step (the only U when f is frozen)
+    double* Unew;
+    double* S;
+    const double* rho_c;  // density when f is frozen
+    double* rho_out;      // EMIT outputs
+    double* Fi_out;
+    double* Ft_out;
+    const uint8_t* bcmap;  // per node: 0 = no boundary op, else index into prog
+    double Twall[MPLB_MAX_PATCHES];
+    BCProg prog[FUSED_MAX_PROGS];
+};
+
+// ------------------------------------------------------------- geometry
+// Wrap a coordinate one step outside [0, ext): periodic -> wrapped,
+// walled -> -1 (absent).  Inputs are within [-1, ext].
+MPLB_HD int wrap1(int c, int ext, int periodic) {
+    if (c < 0) return periodic ? c + ext : -1;
+    if (c >= ext) return periodic ? c - ext : -1;
+    return c;
 }
-inline int fused_setup(FusedConfig& fc, int, const int*, const Params&, const std::vector<PatchDev>*,
-                       const mplb_mesh_desc*, const int*, const int*, cudaStream_t, uint64_t*) {
-    fc.err = "fused kernels not built";
-    return MPLB_E_UNSUPPORTED;
+
+// Node held by ext-grid slot e (0..T+1) of a tile starting at t0 along an
+// axis: -1 when absent.  Only slots within one node of the box are ever read,
+// so slots further out are absent too.
+MPLB_HD int slot_coord(int t0, int e, int ext, int periodic) {
+    const int c = t0 - 1 + e;
+    return c <= ext ? wrap1(c, ext, periodic) : -1;
 }
-inline int fused_run(FusedConfig& fc, const Params&, uint32_t, uint32_t, double* (*)[2], int*, double*,
-                     double*&, double*&, double*, double*&, double*&, double*, double*, cudaStream_t,
-                     uint64_t*) {
-    fc.err = "fused kernels not built";
-    return MPLB_E_UNSUPPORTED;
+
+// Ring slot r (0..2*(TX+2)+2*TY-1) of a TX x TY tile -> ext coordinates.
+MPLB_HD void ring_slot(int r, int TX, int TY, int& ex, int& ey) {
+    const int EX = TX + 2;
+    if (r < EX) { ex = r; ey = 0; }
+    else if (r < 2 * EX) { ex = r - EX; ey = TY + 1; }
+    else if (r < 2 * EX + TY) { ex = 0; ey = r - 2 * EX + 1; }
+    else { ex = EX - 1; ey = r - 2 * EX - TY + 1; }
 }
-inline void fused_free(FusedConfig&) {}
+
+// Pull source of population (cx, cy, cz) at node (x, y, z); -1 if missing.
+MPLB_HD int64_t pull_src(int nx, int ny, int nz, int px, int py, int pz, int x, int y, int z, int cx, int cy,
+                         int cz) {
+    int sx = wrap1(x - cx, nx, px), sy = wrap1(y - cy, ny, py), sz = wrap1(z - cz, nz, pz);
+    if (sx < 0 || sy < 0 || sz < 0) return -1;
+    return (int64_t)sx + (int64_t)nx * ((int64_t)sy + (int64_t)ny * (int64_t)sz);
+}
+
+// Node on a walled face: it has a missing neighbour (readLatticeMesh.c:171-203).
+MPLB_HD bool on_wall(const FusedArgs& A, int x, int y, int z) {
+    return (!A.px && (x == 0 || x == A.nx - 1)) || (!A.py && (y == 0 || y == A.ny - 1)) ||
+           (!A.pz && (z == 0 || z == A.nz - 1));
+}
+
+// ------------------------------------------------------------ phase A
+// Pull-stream one node, apply its boundary program, sum moments.
+// f, g receive f''_n, g''_n; miss bit k = population k has no source.
+template <class L, bool F_ON, bool G_ON, bool HAS_BC>
+__device__ __forceinline__ void pull_node(const Params& P, const FusedArgs& A, int x, int y, int z,
+                                          uint32_t id, double* f, double* g, double& rho, double& T) {
+    const uint32_t n = P.n;
+    uint32_t miss = 0;
+    static_for<L::Q>([&](auto kk) {
+        constexpr int k = decltype(kk)::value;
+        const int64_t s = pull_src(A.nx, A.ny, A.nz, A.px, A.py, A.pz, x, y, z, cxk<L>(k), cyk<L>(k), czk<L>(k));
+        const bool m = s < 0;
+        const uint32_t src = m ? id : (uint32_t)s;
+        if constexpr (F_ON) f[k] = __ldg(A.fin + (size_t)k * n + src);
+        if constexpr (G_ON) g[k] = __ldg(A.gin + (size_t)k * n + src);
+        miss |= (uint32_t)m << k;
+    });
+    if constexpr (HAS_BC) {
+        uint8_t pi = A.bcmap[id];
+        if (pi) {
+            const BCProg& pr = A.prog[pi];
+            // bounceBack.c:21-70 on registers, k ascending, in place
+            auto bounce = [&](double* v) {
+#pragma unroll
+                for (int k = 0; k < L::Q; k++) {
+                    const int r = revk<L>(k);
+                    if ((miss >> k) & 1u) {
+                        v[k] = v[r];
+                    } else if (!((miss >> r) & 1u) && k >= 1 && k <= L::NAX) {
+                        v[k] = 0.5 * v[k] + 0.5 * v[r];
+                        v[r] = v[k];
+                    }
+                }
+            };
+            if constexpr (F_ON)
+                for (int o = 0; o < pr.nf; o++) bounce(f);
+            if constexpr (G_ON) {
+                for (int o = 0; o < pr.ng; o++) {
+                    if (pr.gt[o] == MPLB_BC_BOUNCEBACK) {
+                        bounce(g);
+                    } else {
+                        // fixedT.c:119-200.  The neighbour nbid = x + c_k; its
+                        // post-stream population k came from this node: g*_n(x)[k].
+                        const double Tw = A.Twall[pr.gp[o]];
+#pragma unroll
+                        for (int k = 0; k < L::Q; k++) {
+                            if (!((miss >> k) & 1u)) continue;
+                            int mx = wrap1(x + cxk<L>(k), A.nx, A.px);
+                            int my = wrap1(y + cyk<L>(k), A.ny, A.py);
+                            if (mx < 0 || my < 0) continue;
+                            uint32_t m = (uint32_t)mx + (uint32_t)A.nx * (uint32_t)my;
+                            double u0 = A.Uold[m], u1 = A.Uold[n + m];
+                            double eq_nb = eq_heat_k(P, k, A.Told[m], u0, u1);
+                            double eq_bnd = eq_heat_k(P, k, Tw, u0, u1);
+                            g[k] = eq_bnd + (A.gin[(size_t)k * n + id] - eq_nb);
+                        }
+                    }
+                }
+            }
+        }
+    }
+    if constexpr (F_ON) {
+        double s = 0;
+#pragma unroll
+        for (int k = 0; k < L::Q; k++) s += f[k];
+        rho = s;
+    } else {
+        rho = A.rho_c[id];
+    }
+    if constexpr (G_ON) {
+        double s = 0;
+#pragma unroll
+        for (int k = 0; k < L::Q; k++) s += g[k];
+        T = s;
+    } else {
+        T = A.Told[id];
+    }
+}
+
+// ------------------------------------------------------------ phase B
+// Everything after the macros for one node that owns an output.
+// nbpsi(k) returns psi_n at x + c_k.
+template <class L, bool F_ON, bool G_ON, bool EMIT, class PsiAt>
+__device__ __forceinline__ void finish_node(const Params& P, const FusedArgs& A, uint32_t id, bool onb,
+                                            double* f, double* g, double rho, double T, double psi,
+                                            PsiAt nbpsi, double src_heat) {
+    const uint32_t n = P.n;
+    double Fi[3] = {0, 0, 0}, Ft[3], U[3];
+    if constexpr (F_ON) {
+        // interactionForce.c:47-79 (zero force on boundary nodes)
+        if (!onb) {
+            double F[3] = {0.0, 0.0, 0.0};
+            static_for<L::Q - 1>([&](auto km1) {
+                constexpr int k = decltype(km1)::value + 1;
+                double al = P.ppw[k] * nbpsi(k);
+                static_for<3>([&](auto i) {
+                    constexpr int c = ck<L>(k, decltype(i)::value);
+                    if constexpr (c == 1) F[i] = F[i] + al;
+                    else if constexpr (c == -1) F[i] = F[i] - al;
+                });
+            });
+            double be = -P.G * psi;
+#pragma unroll
+            for (int i = 0; i < 3; i++) Fi[i] = F[i] * be;
+        }
+        // interForce.c:27-39
+#pragma unroll
+        for (int j = 0; j < 3; j++) {
+            double t = Fi[j] + (rho - P.rho_0) * P.g[j];
+            if (!onb) t += P.fext[j];
+            Ft[j] = t;
+        }
+        // liMRTVelocity.c:27-44 (F = Ft) / xuMRTVelocity.c:19-44 (F = Fi + (rho - rho_0) g).
+        // Zero velocity components contribute +-0 and are skipped.
+        static_for<3>([&](auto jj) {
+            constexpr int j = decltype(jj)::value;
+            double lv = 0;
+            static_for<L::Q>([&](auto kk) {
+                constexpr int c = ck<L>(decltype(kk)::value, j);
+                if constexpr (c == 1) lv = lv + f[kk];
+                else if constexpr (c == -1) lv = lv - f[kk];
+            });
+            double Fj = L::Q == 9 ? Ft[j] : Fi[j] + (rho - P.rho_0) * P.g[j];
+            U[j] = (lv + Fj * 0.5) / rho;
+        });
+    } else {
+#pragma unroll
+        for (int j = 0; j < 3; j++) U[j] = A.Uold[(size_t)j * n + id];
+    }
+    if constexpr (EMIT) {
+        if constexpr (F_ON) {
+#pragma unroll
+            for (int k = 0; k < L::Q; k++) A.fout[(size_t)k * n + id] = f[k];
+            A.rho_out[id] = rho;
+#pragma unroll
+            for (int j = 0; j < 3; j++) {
+                A.Fi_out[(size_t)j * n + id] = Fi[j];
+                A.Ft_out[(size_t)j * n + id] = Ft[j];
+                A.Unew[(size_t)j * n + id] = U[j];
+            }
+        }
+        if constexpr (G_ON) {
+#pragma unroll
+            for (int k = 0; k < L::Q; k++) A.gout[(size_t)k * n + id] = g[k];
+        }
+        return;
+    }
+    if constexpr (F_ON) {
+        if constexpr (L::Q == 9) collide_limrt(P, f, rho, U, Ft, Fi, T);
+        else collide_xumrt(P, f, rho, U, Fi, T);
+#pragma unroll
+        for (int k = 0; k < L::Q; k++) A.fout[(size_t)k * n + id] = f[k];
+        if constexpr (G_ON) {
+            // only the heat source and fixedT read U of the previous step
+            A.Unew[id] = U[0];
+            A.Unew[n + id] = U[1];
+        }
+    }
+    if constexpr (G_ON) {
+        collide_litemp(P, g, T, U[0], U[1], src_heat);
+#pragma unroll
+        for (int k = 0; k < 9; k++) A.gout[(size_t)k * n + id] = g[k];
+        A.Tnew[id] = T;
+        A.S[id] = src_heat;
+    }
+}
+
+// ------------------------------------------------------------ 2D kernel
+// Tile of TX x TY nodes, one thread each, plus the one-node ring around it
+// (psi, 1/rho, T_{n-1}, U_{n-1}) computed by the first threads.
+constexpr int F2_TX = 32, F2_TY = 8;
+
+template <bool F_ON, bool G_ON, bool HAS_BC, bool EMIT>
+__global__ void __launch_bounds__(F2_TX * F2_TY) k_fused_d2q9(Params P, FusedArgs A) {
+    using L = D2Q9T;
+    constexpr int EX = F2_TX + 2, EY = F2_TY + 2, NRING = 2 * EX + 2 * F2_TY;
+    constexpr int GY = G_ON ? EY : 1, GX = G_ON ? EX : 1;
+    __shared__ double s_psi[EY][EX];
+    __shared__ double s_inv[GY][GX];
+    __shared__ double s_To[GY][GX];
+    __shared__ double s_U0[GY][GX];
+    __shared__ double s_U1[GY][GX];
+    const uint32_t n = P.n;
+    const int tx = threadIdx.x % F2_TX, ty = threadIdx.x / F2_TX;
+    const int bx = blockIdx.x % A.tiles_x, by = blockIdx.x / A.tiles_x;
+    const int x0 = bx * F2_TX, y0 = by * F2_TY;
+
+    // one ext-grid slot: pull, moments, psi; shared-memory record
+    auto slot = [&](int ex, int ey, double* f, double* g, double& rho, double& T, uint32_t& id) -> bool {
+        const int x = slot_coord(x0, ex, A.nx, A.px);
+        const int y = slot_coord(y0, ey, A.ny, A.py);
+        if (x < 0 || y < 0) return false;
+        id = (uint32_t)x + (uint32_t)A.nx * (uint32_t)y;
+        pull_node<L, F_ON, G_ON, HAS_BC>(P, A, x, y, 0, id, f, g, rho, T);
+        if constexpr (F_ON) s_psi[ey][ex] = potential(P, rho, T);
+        if constexpr (G_ON) {
+            s_inv[ey][ex] = 1.0 / rho;
+            s_To[ey][ex] = A.Told[id];
+            s_U0[ey][ex] = A.Uold[id];
+            s_U1[ey][ex] = A.Uold[n + id];
+        }
+        return true;
+    };
+
+    double f[9], g[9], rho = 0, T = 0;
+    uint32_t id = 0;
+    const int gx = x0 + tx, gy = y0 + ty;
+    const bool own = gx < A.nx && gy < A.ny;
+    // interior slot (threads outside the box still fill the slot of the
+    // wrapped node, so partial tiles see their periodic neighbours)
+    const bool have = slot(tx + 1, ty + 1, f, g, rho, T, id);
+    for (int r = threadIdx.x; r < NRING; r += blockDim.x) {
+        int ex, ey;
+        ring_slot(r, F2_TX, F2_TY, ex, ey);
+        double rf[9], rg[9], rr, rt;
+        uint32_t rid;
+        slot(ex, ey, rf, rg, rr, rt, rid);
+    }
+    __syncthreads();
+    if (!own || !have) return;
+
+    const int ex = tx + 1, ey = ty + 1;
+    const bool onb = on_wall(A, gx, gy, 0);
+    double heat = 0;
+    if constexpr (G_ON && !EMIT) {
+        // heatSource.c:119-165 with the one-sided differences of finiteDifference/*.c
+        double gT[3] = {0, 0, 0}, gR[3] = {0, 0, 0}, div = 0;
+        const double To = s_To[ey][ex], iv = s_inv[ey][ex];
+        // x: a = x+1, b = x-1
+        {
+            bool a = wrap1(gx + 1, A.nx, A.px) >= 0, b = wrap1(gx - 1, A.nx, A.px) >= 0;
+            FD t = fd_pair(a ? 0 : -1, b ? 0 : -1, s_To[ey][ex + 1], s_To[ey][ex - 1], To);
+            FD r = fd_pair(a ? 0 : -1, b ? 0 : -1, s_inv[ey][ex + 1], s_inv[ey][ex - 1], iv);
+            FD u = fd_pair(a ? 0 : -1, b ? 0 : -1, s_U0[ey][ex + 1], s_U0[ey][ex - 1], s_U0[ey][ex]);
+            gT[0] = t.v;
+            gR[0] = r.v;
+            if (u.present) div += u.v;
+        }
+        {
+            bool a = wrap1(gy + 1, A.ny, A.py) >= 0, b = wrap1(gy - 1, A.ny, A.py) >= 0;
+            FD t = fd_pair(a ? 0 : -1, b ? 0 : -1, s_To[ey + 1][ex], s_To[ey - 1][ex], To);
+            FD r = fd_pair(a ? 0 : -1, b ? 0 : -1, s_inv[ey + 1][ex], s_inv[ey - 1][ex], iv);
+            FD u = fd_pair(a ? 0 : -1, b ? 0 : -1, s_U1[ey + 1][ex], s_U1[ey - 1][ex], s_U1[ey][ex]);
+            gT[1] = t.v;
+            gR[1] = r.v;
+            if (u.present) div += u.v;
+        }
+        double dot = 0;
+#pragma unroll
+        for (int k = 0; k < 3; k++) dot += gT[k] * gR[k];
+        heat = heat_source_value(P, rho, To, dot, div, A.S[id]);
+    }
+    double psi = 0;
+    if constexpr (F_ON) psi = s_psi[ey][ex];
+    auto nbpsi = [&](int k) { return s_psi[ey + cyk<L>(k)][ex + cxk<L>(k)]; };
+    finish_node<L, F_ON, G_ON, EMIT>(P, A, id, onb, f, g, rho, T, psi, nbpsi, heat);
+}
+
+// ------------------------------------------------------------ 3D kernel
+// xy tile of TX x TY columns marching along z over a chunk of planes, with
+// a three-plane ring buffer of psi (tile + one-node ring).  Isothermal:
+// liTempMRT is D2Q9 only, so T is read, never written.
+constexpr int F3_TX = 32, F3_TY = 8;
+
+template <bool HAS_BC, bool EMIT>
+__global__ void __launch_bounds__(F3_TX * F3_TY) k_fused_d3q15(Params P, FusedArgs A) {
+    using L = D3Q15T;
+    constexpr int EX = F3_TX + 2, EY = F3_TY + 2, NRING = 2 * EX + 2 * F3_TY;
+    __shared__ double s_psi[3][EY][EX];
+    const int tx = threadIdx.x % F3_TX, ty = threadIdx.x / F3_TX;
+    const int tiles = A.tiles_x * A.tiles_y;
+    const int col = blockIdx.x % tiles, chunk = blockIdx.x / tiles;
+    const int bx = col % A.tiles_x, by = col / A.tiles_x;
+    const int x0 = bx * F3_TX, y0 = by * F3_TY;
+    const int z0 = chunk * A.zchunk;
+    const int z1 = min(z0 + A.zchunk, A.nz);
+
+    // psi of the ext slot (ex, ey) at plane z into ring slot; own pull into f
+    auto plane = [&](int z, double* f, double& rho, double& T, uint32_t& id) -> bool {
+        const int zs = slot_coord(z, 1, A.nz, A.pz);
+        bool have = false;
+        double g_unused[1];
+        {
+            const int x = slot_coord(x0, tx + 1, A.nx, A.px);
+            const int y = slot_coord(y0, ty + 1, A.ny, A.py);
+            double& ps = s_psi[(z + 3) % 3][ty + 1][tx + 1];
+            if (x >= 0 && y >= 0 && zs >= 0) {
+                id = (uint32_t)x + (uint32_t)A.nx * ((uint32_t)y + (uint32_t)A.ny * (uint32_t)zs);
+                pull_node<L, true, false, HAS_BC>(P, A, x, y, zs, id, f, g_unused, rho, T);
+                ps = potential(P, rho, T);
+                have = true;
+            }
+        }
+        for (int r = threadIdx.x; r < NRING; r += blockDim.x) {
+            int ex, ey;
+            ring_slot(r, F3_TX, F3_TY, ex, ey);
+            const int x = slot_coord(x0, ex, A.nx, A.px);
+            const int y = slot_coord(y0, ey, A.ny, A.py);
+            if (x < 0 || y < 0 || zs < 0) continue;
+            uint32_t rid = (uint32_t)x + (uint32_t)A.nx * ((uint32_t)y + (uint32_t)A.ny * (uint32_t)zs);
+            double rf[15], rr, rt;
+            pull_node<L, true, false, HAS_BC>(P, A, x, y, zs, rid, rf, g_unused, rr, rt);
+            s_psi[(z + 3) % 3][ey][ex] = potential(P, rr, rt);
+        }
+        return have;
+    };
+
+    double fc[15], fn[15], rc = 0, rn = 0, Tc = 0, Tn = 0;
+    uint32_t idc = 0, idn = 0;
+    double dum[15], dr, dt;
+    uint32_t did;
+    plane(z0 - 1, dum, dr, dt, did);
+    bool hc = plane(z0, fc, rc, Tc, idc);
+    const bool own_xy = (x0 + tx) < A.nx && (y0 + ty) < A.ny;
+    for (int z = z0; z < z1; z++) {
+        bool hn = plane(z + 1, fn, rn, Tn, idn);
+        __syncthreads();
+        if (own_xy && hc) {
+            const int gx = x0 + tx, gy = y0 + ty;
+            const bool onb = on_wall(A, gx, gy, z);
+            const int ex = tx + 1, ey = ty + 1;
+            auto nbpsi = [&](int k) {
+                return s_psi[(z + czk<L>(k) + 3) % 3][ey + cyk<L>(k)][ex + cxk<L>(k)];
+            };
+            finish_node<L, true, false, EMIT>(P, A, idc, onb, fc, dum, rc, Tc, s_psi[z % 3][ey][ex], nbpsi, 0.0);
+        }
+        __syncthreads();
+#pragma unroll
+        for (int k = 0; k < 15; k++) fc[k] = fn[k];
+        rc = rn;
+        Tc = Tn;
+        idc = idn;
+        hc = hn;
+    }
+}
+
+// ================================================================= host side
+// Launch geometry: tiles per axis, z chunk (3D) and the number of blocks.
+inline int fused_geometry(int lat, FusedArgs& A) {
+    if (lat == MPLB_D2Q9) {
+        A.tiles_x = (A.nx + F2_TX - 1) / F2_TX;
+        A.tiles_y = (A.ny + F2_TY - 1) / F2_TY;
+        A.zchunk = 1;
+        return A.tiles_x * A.tiles_y;
+    }
+    A.tiles_x = (A.nx + F3_TX - 1) / F3_TX;
+    A.tiles_y = (A.ny + F3_TY - 1) / F3_TY;
+    // z chunks: aim for >= 4 blocks per SM of a 148-SM part, chunks of >= 8 planes
+    const int cols = A.tiles_x * A.tiles_y;
+    const int want = (4 * 148 + cols - 1) / cols;
+    int zc = (A.nz + want - 1) / want;
+    zc = std::max(zc, std::min(8, A.nz));
+    A.zchunk = zc;
+    return cols * ((A.nz + zc - 1) / zc);
+}
+
+struct FusedConfig {
+    std::string err;
+    FusedArgs args{};
+    uint8_t* bcmap = nullptr;
+    bool has_bc = false;
+    int nblocks = 0;
+};
+
+// Fused path preconditions: box mesh, no serial boundary dependence, only
+// bounceBack / fixedT / periodic patches, at most FUSED_MAX_OPS ops per node
+// and field, at most FUSED_MAX_PROGS distinct node programs.
+inline bool fused_supported(int lat, const int* model, const Params& P, const std::vector<PatchDev>* fp,
+                            const bool* serial, const mplb_mesh_desc* mesh, const int* dims, const int* per,
+                            std::string& why) {
+    (void)P;
+    (void)per;
+    if (serial[0] || serial[1]) { why = "boundary updates depend on the serial order"; return false; }
+    if (model[0] == MPLB_NO_MODEL) { why = "no flow field"; return false; }
+    if (lat == MPLB_D3Q15 && model[1] != MPLB_NO_MODEL) { why = "thermal field on D3Q15"; return false; }
+    for (int fi = 0; fi < 2; fi++)
+        for (const PatchDev& pt : fp[fi]) {
+            if (pt.type == MPLB_BC_PERIODIC) continue;
+            if (pt.type == MPLB_BC_BOUNCEBACK) continue;
+            if (pt.type == MPLB_BC_FIXEDT && fi == 1) continue;
+            if (pt.type == MPLB_BC_FIXEDU && model[fi] != MPLB_LIMRT) continue;  // no-op
+            why = "boundary type " + std::to_string(pt.type) + " is handled by the operator path only";
+            return false;
+        }
+    if (dims[0] < 2 || dims[1] < 2 || (lat == MPLB_D3Q15 && dims[2] < 2)) { why = "box thinner than 2 nodes"; return false; }
+    (void)mesh;
+    return true;
+}
+
+inline int fused_setup(FusedConfig& fc, int lat, const int* model, const Params& P, const std::vector<PatchDev>* fp,
+                       const mplb_mesh_desc* mesh, const int* dims, const int* per, cudaStream_t stream,
+                       uint64_t* bytes) {
+    (void)model;
+    FusedArgs& A = fc.args;
+    A.nx = dims[0];
+    A.ny = dims[1];
+    A.nz = lat == MPLB_D3Q15 ? dims[2] : 1;
+    A.px = per[0];
+    A.py = per[1];
+    A.pz = lat == MPLB_D3Q15 ? per[2] : 1;
+    // Node programs: for every node, the ops of every patch holding it, in
+    // patch order, per field.  Identical programs share one table entry.
+    const uint32_t n = P.n;
+    std::vector<uint8_t> map(n, 0);
+    std::vector<BCProg> progs(1, BCProg{});
+    std::vector<BCProg> per_node;
+    bool any = false;
+    {
+        std::vector<BCProg> node(n, BCProg{});
+        size_t off = 0;
+        for (size_t p = 0; p < fp[0].size(); p++) {
+            for (uint32_t i = 0; i < fp[0][p].count; i++) {
+                uint32_t id = mesh->patch_nodes[off + i];
+                for (int fi = 0; fi < 2; fi++) {
+                    int t = fp[fi][p].type;
+                    if (t != MPLB_BC_BOUNCEBACK && t != MPLB_BC_FIXEDT) continue;
+                    BCProg& b = node[id];
+                    if (fi == 0) {
+                        if (b.nf >= FUSED_MAX_OPS) { fc.err = "too many boundary ops on one node"; return MPLB_E_UNSUPPORTED; }
+                        b.ft[b.nf++] = (uint8_t)t;
+                    } else {
+                        if (b.ng >= FUSED_MAX_OPS) { fc.err = "too many boundary ops on one node"; return MPLB_E_UNSUPPORTED; }
+                        b.gp[b.ng] = (uint8_t)p;
+                        b.gt[b.ng++] = (uint8_t)t;
+                    }
+                    any = true;
+                }
+            }
+            off += fp[0][p].count;
+        }
+        for (uint32_t id = 0; id < n; id++) {
+            const BCProg& b = node[id];
+            if (b.nf == 0 && b.ng == 0) continue;
+            int found = -1;
+            for (size_t q = 1; q < progs.size(); q++)
+                if (std::memcmp(&progs[q], &b, sizeof(BCProg)) == 0) { found = (int)q; break; }
+            if (found < 0) {
+                if (progs.size() >= FUSED_MAX_PROGS) { fc.err = "too many distinct boundary programs"; return MPLB_E_UNSUPPORTED; }
+                progs.push_back(b);
+                found = (int)progs.size() - 1;
+            }
+            map[id] = (uint8_t)found;
+        }
+    }
+    for (size_t q = 0; q < progs.size(); q++) A.prog[q] = progs[q];
+    for (size_t p = 0; p < fp[1].size() && p < MPLB_MAX_PATCHES; p++) A.Twall[p] = fp[1][p].val[0];
+    fc.has_bc = any;
+    if (any) {
+        if (cudaMalloc((void**)&fc.bcmap, n) != cudaSuccess) { fc.err = "cudaMalloc bcmap"; return MPLB_E_CUDA; }
+        if (cudaMemcpyAsync(fc.bcmap, map.data(), n, cudaMemcpyHostToDevice, stream) != cudaSuccess) {
+            fc.err = "copy bcmap";
+            return MPLB_E_CUDA;
+        }
+        if (cudaStreamSynchronize(stream) != cudaSuccess) { fc.err = "copy bcmap"; return MPLB_E_CUDA; }
+        *bytes += n;
+    }
+    A.bcmap = fc.bcmap;
+    fc.nblocks = fused_geometry(lat, A);
+    return 0;
+}
+
+inline void fused_free(FusedConfig& fc) {
+    if (fc.bcmap) cudaFree(fc.bcmap);
+    fc.bcmap = nullptr;
+}
+
+// Launch one fused step (EMIT = rebuild the reference state, no collision).
+inline cudaError_t fused_launch(const FusedConfig& fc, const Params& P, const FusedArgs& A, int lat, bool f_on,
+                                bool g_on, bool emit, cudaStream_t s) {
+    const bool bc = fc.has_bc;
+#define MPLB_F2(F, G, B, E) k_fused_d2q9<F, G, B, E><<<fc.nblocks, F2_TX * F2_TY, 0, s>>>(P, A)
+#define MPLB_F2_E(F, G, B) (emit ? (MPLB_F2(F, G, B, true), 0) : (MPLB_F2(F, G, B, false), 0))
+#define MPLB_F2_B(F, G) (bc ? MPLB_F2_E(F, G, true) : MPLB_F2_E(F, G, false))
+    if (lat == MPLB_D2Q9) {
+        if (f_on && g_on) MPLB_F2_B(true, true);
+        else if (f_on) MPLB_F2_B(true, false);
+        else if (g_on) MPLB_F2_B(false, true);
+    } else {
+        if (bc) {
+            if (emit) k_fused_d3q15<true, true><<<fc.nblocks, F3_TX * F3_TY, 0, s>>>(P, A);
+            else k_fused_d3q15<true, false><<<fc.nblocks, F3_TX * F3_TY, 0, s>>>(P, A);
+        } else {
+            if (emit) k_fused_d3q15<false, true><<<fc.nblocks, F3_TX * F3_TY, 0, s>>>(P, A);
+            else k_fused_d3q15<false, false><<<fc.nblocks, F3_TX * F3_TY, 0, s>>>(P, A);
+        }
+    }
+#undef MPLB_F2
+#undef MPLB_F2_E
+#undef MPLB_F2_B
+    return cudaGetLastError();
+}
 
 }  // namespace mplb

@@ -75,6 +75,7 @@ struct mplb_gpu {
     double* red = nullptr;  // reduction partials + results
     int red_parts = 0;
     FusedConfig fc{};
+    int fstate = 0;  // 0: buffers hold the reference's state; 1: post-collision (fused)
     uint32_t current = 0;
     uint64_t launches = 0;
     uint64_t bytes = 0;
@@ -440,6 +441,52 @@ struct DeviceGuard {
     }
 };
 
+// One fused time step, or (emit) the rebuild of the reference state after
+// the last step from that step's retained input buffers.
+int fused_step(mplb_gpu* h, bool emit) {
+    const bool fon = h->P.f_update != 0, gon = h->P.g_update != 0;
+    FusedArgs A = h->fc.args;
+    const int c0 = h->cur[0], c1 = h->cur[1];
+    if (fon) {
+        A.fin = emit ? h->pdf[0][c0 ^ 1] : h->pdf[0][c0];
+        A.fout = emit ? h->pdf[0][c0] : h->pdf[0][c0 ^ 1];
+    }
+    if (gon) {
+        A.gin = emit ? h->pdf[1][c1 ^ 1] : h->pdf[1][c1];
+        A.gout = emit ? h->pdf[1][c1] : h->pdf[1][c1 ^ 1];
+    }
+    const bool udb = fon && gon;  // U double-buffered (the heat source reads U_{n-1})
+    A.Told = gon ? (emit ? h->T2 : h->T) : h->T;
+    A.Tnew = gon ? h->T2 : nullptr;
+    A.Uold = udb ? (emit ? h->U2 : h->U) : h->U;
+    A.Unew = udb ? (emit ? h->U : h->U2) : h->U;
+    A.S = h->S;
+    A.rho_c = h->rho;
+    A.rho_out = h->rho;
+    A.Fi_out = h->Fi;
+    A.Ft_out = h->Ft;
+    cudaError_t e = fused_launch(h->fc, h->P, A, h->lat, fon, gon, emit, h->stream);
+    h->launches++;
+    if (e != cudaSuccess) return fail(MPLB_E_CUDA, std::string("fused kernel launch: ") + cudaGetErrorString(e));
+    if (!emit) {
+        if (fon) h->cur[0] ^= 1;
+        if (gon) {
+            h->cur[1] ^= 1;
+            std::swap(h->T, h->T2);
+        }
+        if (udb) std::swap(h->U, h->U2);
+    }
+    return 0;
+}
+
+// Bring the buffers back to the reference's state (after the last step).
+int materialize(mplb_gpu* h) {
+    if (h->fstate == 0) return 0;
+    RET(fused_step(h, true));
+    h->fstate = 0;
+    return 0;
+}
+
 }  // namespace
 
 // ================================================================= C-ABI
@@ -643,6 +690,7 @@ int mplb_gpu_upload(mplb_gpu_t* h, const double* rho, const double* U, const dou
                     const double* g, const double* S, const double* Fi, const double* Ft) {
     if (!h) return fail(MPLB_E_ARG, "NULL handle");
     DeviceGuard guard(h->dev);
+    RET(materialize(h));
     RET(put_scalar(h, rho, h->rho));
     RET(put_scalar(h, T, h->T));
     RET(put_scalar(h, S, h->S));
@@ -659,6 +707,7 @@ int mplb_gpu_download(mplb_gpu_t* h, double* rho, double* U, double* T, double* 
                       double* f, double* g) {
     if (!h) return fail(MPLB_E_ARG, "NULL handle");
     DeviceGuard guard(h->dev);
+    RET(materialize(h));
     RET(get_scalar(h, rho, h->rho));
     RET(get_scalar(h, T, h->T));
     RET(get_scalar(h, S, h->S));
@@ -679,6 +728,7 @@ int mplb_gpu_download(mplb_gpu_t* h, double* rho, double* U, double* T, double* 
 int mplb_gpu_initialize(mplb_gpu_t* h) {
     if (!h) return fail(MPLB_E_ARG, "NULL handle");
     DeviceGuard guard(h->dev);
+    RET(materialize(h));
     return DISPATCH(h, initialize_impl, h);
 }
 
@@ -687,9 +737,13 @@ int mplb_gpu_step(mplb_gpu_t* h, uint32_t nsteps) {
     if (nsteps == 0) return 0;
     DeviceGuard guard(h->dev);
     if (h->path == MPLB_PATH_FUSED) {
-        int rc = fused_run(h->fc, h->P, nsteps, h->current, h->pdf, h->cur, h->rho, h->T, h->T2, h->S, h->U,
-                           h->U2, h->Fi, h->Ft, h->stream, &h->launches);
-        if (rc) return fail(rc, h->fc.err);
+        if (h->fstate == 0) {
+            // prologue: the first collision of the loop, on the reference state
+            RET(DISPATCH(h, op_collision, h, 0));
+            RET(DISPATCH(h, op_collision, h, 1));
+            h->fstate = 1;
+        }
+        for (uint32_t s = 0; s < nsteps; s++) RET(fused_step(h, false));
         h->current += nsteps;
         return 0;
     }
@@ -700,21 +754,25 @@ int mplb_gpu_step(mplb_gpu_t* h, uint32_t nsteps) {
 int mplb_gpu_equilibrium(mplb_gpu_t* h, int32_t field) {
     if (!h || (field != MPLB_FIELD_F && field != MPLB_FIELD_G)) return fail(MPLB_E_ARG, "bad handle or field");
     DeviceGuard guard(h->dev);
+    RET(materialize(h));
     return DISPATCH(h, op_equilibrium, h, field);
 }
 int mplb_gpu_collision(mplb_gpu_t* h, int32_t field) {
     if (!h || (field != MPLB_FIELD_F && field != MPLB_FIELD_G)) return fail(MPLB_E_ARG, "bad handle or field");
     DeviceGuard guard(h->dev);
+    RET(materialize(h));
     return DISPATCH(h, op_collision, h, field);
 }
 int mplb_gpu_lbstream(mplb_gpu_t* h, int32_t field) {
     if (!h || (field != MPLB_FIELD_F && field != MPLB_FIELD_G)) return fail(MPLB_E_ARG, "bad handle or field");
     DeviceGuard guard(h->dev);
+    RET(materialize(h));
     return DISPATCH(h, op_stream, h, field);
 }
 int mplb_gpu_update_boundaries(mplb_gpu_t* h, int32_t field) {
     if (!h || (field != MPLB_FIELD_F && field != MPLB_FIELD_G)) return fail(MPLB_E_ARG, "bad handle or field");
     DeviceGuard guard(h->dev);
+    RET(materialize(h));
     return DISPATCH(h, op_boundaries, h, field);
 }
 int mplb_gpu_macro_density(mplb_gpu_t* h, uint32_t start, uint32_t end) {
@@ -722,26 +780,31 @@ int mplb_gpu_macro_density(mplb_gpu_t* h, uint32_t start, uint32_t end) {
     if (h->model[0] != MPLB_LIMRT && h->model[0] != MPLB_XUMRT && h->P.f_update)
         return fail(MPLB_E_UNSUPPORTED, "Density update not available (macroDensity.c:65-67)");
     DeviceGuard guard(h->dev);
+    RET(materialize(h));
     return DISPATCH(h, op_density, h, start, end);
 }
 int mplb_gpu_macro_velocity(mplb_gpu_t* h, uint32_t start, uint32_t end) {
     if (!h || start > end || end > h->n) return fail(MPLB_E_ARG, "bad handle or node range");
     DeviceGuard guard(h->dev);
+    RET(materialize(h));
     return DISPATCH(h, op_velocity, h, start, end);
 }
 int mplb_gpu_macro_temperature(mplb_gpu_t* h, uint32_t start, uint32_t end) {
     if (!h || start > end || end > h->n) return fail(MPLB_E_ARG, "bad handle or node range");
     DeviceGuard guard(h->dev);
+    RET(materialize(h));
     return DISPATCH(h, op_temperature, h, start, end);
 }
 int mplb_gpu_inter_force(mplb_gpu_t* h) {
     if (!h) return fail(MPLB_E_ARG, "NULL handle");
     DeviceGuard guard(h->dev);
+    RET(materialize(h));
     return DISPATCH(h, op_interforce, h);
 }
 int mplb_gpu_heat_source(mplb_gpu_t* h) {
     if (!h) return fail(MPLB_E_ARG, "NULL handle");
     DeviceGuard guard(h->dev);
+    RET(materialize(h));
     return DISPATCH(h, op_heatsource, h);
 }
 
@@ -753,6 +816,9 @@ int mplb_gpu_set_time(mplb_gpu_t* h, uint32_t current) {
 
 int mplb_gpu_set_rho0(mplb_gpu_t* h, double rho_0) {
     if (!h) return fail(MPLB_E_ARG, "NULL handle");
+    DeviceGuard guard(h->dev);
+    // the post-collision buffers were made with the old rho_0
+    RET(materialize(h));
     h->P.rho_0 = rho_0;
     return 0;
 }
@@ -760,6 +826,7 @@ int mplb_gpu_set_rho0(mplb_gpu_t* h, double rho_0) {
 int mplb_gpu_average_rho0(mplb_gpu_t* h, double* rho_0) {
     if (!h) return fail(MPLB_E_ARG, "NULL handle");
     DeviceGuard guard(h->dev);
+    RET(materialize(h));
     double avg = 0;
     if (!(h->P.rho_0 <= 0)) {
         LAUNCH(k_sum_serial, 1, h->n, h->rho, h->red);
@@ -776,6 +843,7 @@ int mplb_gpu_average_rho0(mplb_gpu_t* h, double* rho_0) {
 int mplb_gpu_mass_energy(mplb_gpu_t* h, double* mass, double* energy) {
     if (!h) return fail(MPLB_E_ARG, "NULL handle");
     DeviceGuard guard(h->dev);
+    RET(materialize(h));
     int parts = std::min<int>(h->red_parts, (int)blocks(h->n));
     k_sum2_partial<<<parts, TPB, 0, h->stream>>>(h->n, h->rho, h->T, h->red);
     h->launches++;

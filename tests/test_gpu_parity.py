@@ -144,3 +144,56 @@ def test_serial_boundary_order(gpu_lib):
     got, info = run_gpu(c2, 6, path=abi.PATH_OPERATORS)
     assert info["bc_sequential"] & 1
     assert_same(got, run_checker("port", c2, 6), ctx="serial bc")
+
+
+FUSABLE = ["bubble_d2q9", "column_d2q9", "bubble_d3q15", "walls_d3q15"]
+
+
+@pytest.mark.parametrize("name", FUSABLE)
+@pytest.mark.parametrize("steps", [1, 2, 11])
+def test_fused_path_matches_oracle(gpu_lib, name, steps):
+    case = small_cases()[name]
+    want = run_checker("port", case, steps)
+    got, info = run_gpu(case, steps, path=abi.PATH_FUSED)
+    assert info["path"] == abi.PATH_FUSED
+    assert_same(got, want, ctx=f"fused {name}@{steps}")
+
+
+@pytest.mark.parametrize("name", FUSABLE)
+def test_fused_interleaved_with_downloads(gpu_lib, name):
+    """Materialise the reference state mid-run, then keep stepping."""
+    from multiphaselb_b200 import Lattice
+    case = small_cases()[name]
+    k = orc.Checker("port", case)
+    k.upload_case()
+    k.initialize()
+    with Lattice(case, path=abi.PATH_FUSED) as lat:
+        lat.upload_case()
+        lat.initialize()
+        for chunk in (3, 1, 4):
+            k.step(chunk)
+            lat.step(chunk)
+            assert_same(lat.download(), k.download(), ctx=f"{name} after chunk {chunk}")
+        # an operator call on the materialised state, then fused steps again
+        k.op(orc.OP_INTERFORCE)
+        lat.inter_force()
+        k.step(2)
+        lat.step(2)
+        assert_same(lat.download(), k.download(), ctx=f"{name} after operator + 2 steps")
+
+
+def test_fused_auto_selects_box_path(gpu_lib):
+    _, info = run_gpu(small_cases()["column_d2q9"], 1)
+    assert info["path"] == abi.PATH_FUSED
+    _, info = run_gpu(small_cases()["lid_d2q9"], 1)
+    assert info["path"] == abi.PATH_OPERATORS  # fixedU is an operator-path boundary
+
+
+@pytest.mark.parametrize("fu,gu", [(0, 1), (1, 0)])
+def test_fused_frozen_fields(gpu_lib, fu, gu):
+    case = small_cases()["column_d2q9"]
+    c2 = type(case)(**{**case.__dict__})
+    c2.f = dict(case.f, update=fu)
+    c2.g = dict(case.g, update=gu)
+    got, info = run_gpu(c2, 6, path=abi.PATH_FUSED)
+    assert_same(got, run_checker("port", c2, 6), ctx=f"fused update f={fu} g={gu}")
