@@ -97,6 +97,47 @@ MPLB_HD int64_t pull_src(int nx, int ny, int nz, int px, int py, int pz, int x, 
     return (int64_t)sx + (int64_t)nx * ((int64_t)sy + (int64_t)ny * (int64_t)sz);
 }
 
+// Offsets from a node to its axis neighbours (wrapped on periodic axes) and
+// which of them lie beyond a walled face.  Computed once per node; the pull
+// source of population k (x - c_k) is then one offset per non-zero component.
+struct NodeOffsets {
+    int xm, xp, ym, yp, zm, zp;  // index offsets to the sources at x-1, x+1, y-1, ...
+    bool mxm, mxp, mym, myp, mzm, mzp;  // that source is missing
+};
+MPLB_HD NodeOffsets node_offsets(const FusedArgs& A, int x, int y, int z, int D) {
+    NodeOffsets o;
+    const int nxy = A.nx * A.ny;
+    const bool xlo = x == 0, xhi = x == A.nx - 1, ylo = y == 0, yhi = y == A.ny - 1;
+    const bool zlo = D == 3 && z == 0, zhi = D == 3 && z == A.nz - 1;
+    o.xm = xlo ? A.nx - 1 : -1;
+    o.xp = xhi ? 1 - A.nx : 1;
+    o.ym = ylo ? (A.ny - 1) * A.nx : -A.nx;
+    o.yp = yhi ? (1 - A.ny) * A.nx : A.nx;
+    o.zm = zlo ? (A.nz - 1) * nxy : -nxy;
+    o.zp = zhi ? (1 - A.nz) * nxy : nxy;
+    o.mxm = xlo && !A.px;
+    o.mxp = xhi && !A.px;
+    o.mym = ylo && !A.py;
+    o.myp = yhi && !A.py;
+    o.mzm = zlo && !A.pz;
+    o.mzp = zhi && !A.pz;
+    return o;
+}
+// Pull source of the population with velocity (cx, cy, cz) at node id: the
+// node id itself when the source is missing (lbstream.c:36-42 keeps the value).
+MPLB_HD uint32_t source_of(const NodeOffsets& o, uint32_t id, int cx, int cy, int cz, bool& missing) {
+    int off = 0;
+    bool m = false;
+    if (cx == 1) { off += o.xm; m |= o.mxm; }
+    if (cx == -1) { off += o.xp; m |= o.mxp; }
+    if (cy == 1) { off += o.ym; m |= o.mym; }
+    if (cy == -1) { off += o.yp; m |= o.myp; }
+    if (cz == 1) { off += o.zm; m |= o.mzm; }
+    if (cz == -1) { off += o.zp; m |= o.mzp; }
+    missing = m;
+    return m ? id : (uint32_t)((int)id + off);
+}
+
 // Node on a walled face: it has a missing neighbour (readLatticeMesh.c:171-203).
 MPLB_HD bool on_wall(const FusedArgs& A, int x, int y, int z) {
     return (!A.px && (x == 0 || x == A.nx - 1)) || (!A.py && (y == 0 || y == A.ny - 1)) ||
@@ -110,12 +151,12 @@ template <class L, bool F_ON, bool G_ON, bool HAS_BC>
 __device__ __forceinline__ void pull_node(const Params& P, const FusedArgs& A, int x, int y, int z,
                                           uint32_t id, double* f, double* g, double& rho, double& T) {
     const uint32_t n = P.n;
+    const NodeOffsets no = node_offsets(A, x, y, L::D == 3 ? z : 0, L::D);
     uint32_t miss = 0;
     static_for<L::Q>([&](auto kk) {
         constexpr int k = decltype(kk)::value;
-        const int64_t s = pull_src(A.nx, A.ny, A.nz, A.px, A.py, A.pz, x, y, z, cxk<L>(k), cyk<L>(k), czk<L>(k));
-        const bool m = s < 0;
-        const uint32_t src = m ? id : (uint32_t)s;
+        bool m;
+        const uint32_t src = source_of(no, id, cxk<L>(k), cyk<L>(k), czk<L>(k), m);
         if constexpr (F_ON) f[k] = __ldg(A.fin + (size_t)k * n + src);
         if constexpr (G_ON) g[k] = __ldg(A.gin + (size_t)k * n + src);
         miss |= (uint32_t)m << k;
@@ -187,7 +228,7 @@ __device__ __forceinline__ void pull_node(const Params& P, const FusedArgs& A, i
 // nbpsi(k) returns psi_n at x + c_k.
 template <class L, bool F_ON, bool G_ON, bool EMIT, class PsiAt>
 __device__ __forceinline__ void finish_node(const Params& P, const FusedArgs& A, uint32_t id, bool onb,
-                                            double* f, double* g, double rho, double T, double psi,
+                                            double* f, double* g, double rho, double rr, double T, double psi,
                                             PsiAt nbpsi, double src_heat) {
     const uint32_t n = P.n;
     double Fi[3] = {0, 0, 0}, Ft[3], U[3];
@@ -226,7 +267,7 @@ __device__ __forceinline__ void finish_node(const Params& P, const FusedArgs& A,
                 else if constexpr (c == -1) lv = lv - f[kk];
             });
             double Fj = L::Q == 9 ? Ft[j] : Fi[j] + (rho - P.rho_0) * P.g[j];
-            U[j] = (lv + Fj * 0.5) / rho;
+            U[j] = div_rcp(lv + Fj * 0.5, rho, rr);  // == (lv + Fj*0.5)/rho
         });
     } else {
 #pragma unroll
@@ -251,8 +292,8 @@ __device__ __forceinline__ void finish_node(const Params& P, const FusedArgs& A,
         return;
     }
     if constexpr (F_ON) {
-        if constexpr (L::Q == 9) collide_limrt(P, f, rho, U, Ft, Fi, T);
-        else collide_xumrt(P, f, rho, U, Fi, T);
+        if constexpr (L::Q == 9) collide_limrt_psi(P, f, rho, U, Ft, Fi, psi);
+        else collide_xumrt_psi(P, f, rho, U, Fi, psi);
 #pragma unroll
         for (int k = 0; k < L::Q; k++) A.fout[(size_t)k * n + id] = f[k];
         if constexpr (G_ON) {
@@ -276,7 +317,7 @@ __device__ __forceinline__ void finish_node(const Params& P, const FusedArgs& A,
 constexpr int F2_TX = 32, F2_TY = 8;
 
 template <bool F_ON, bool G_ON, bool HAS_BC, bool EMIT>
-__global__ void __launch_bounds__(F2_TX * F2_TY) k_fused_d2q9(Params P, FusedArgs A) {
+__global__ void __launch_bounds__(F2_TX * F2_TY, 2) k_fused_d2q9(Params P, FusedArgs A) {
     using L = D2Q9T;
     constexpr int EX = F2_TX + 2, EY = F2_TY + 2, NRING = 2 * EX + 2 * F2_TY;
     constexpr int GY = G_ON ? EY : 1, GX = G_ON ? EX : 1;
@@ -290,16 +331,25 @@ __global__ void __launch_bounds__(F2_TX * F2_TY) k_fused_d2q9(Params P, FusedArg
     const int bx = blockIdx.x % A.tiles_x, by = blockIdx.x / A.tiles_x;
     const int x0 = bx * F2_TX, y0 = by * F2_TY;
 
-    // one ext-grid slot: pull, moments, psi; shared-memory record
-    auto slot = [&](int ex, int ey, double* f, double* g, double& rho, double& T, uint32_t& id) -> bool {
+    // one ext-grid slot: pull, moments, psi; shared-memory record.  The own
+    // slot keeps RN(1/rho) and the density's EOS parts for phase B.
+    auto slot = [&](int ex, int ey, double* f, double* g, double& rho, double& T, uint32_t& id, bool mine,
+                    double& rr, EosRho& er) -> bool {
         const int x = slot_coord(x0, ex, A.nx, A.px);
         const int y = slot_coord(y0, ey, A.ny, A.py);
         if (x < 0 || y < 0) return false;
         id = (uint32_t)x + (uint32_t)A.nx * (uint32_t)y;
         pull_node<L, F_ON, G_ON, HAS_BC>(P, A, x, y, 0, id, f, g, rho, T);
-        if constexpr (F_ON) s_psi[ey][ex] = potential(P, rho, T);
+        if (mine) {
+            rr = rcp_rn(rho);
+            er = eos_rho(P, rho);
+            if constexpr (F_ON) s_psi[ey][ex] = potential_p(P, rho, p_eos_at(P, er, rho, T));
+            if constexpr (G_ON) s_inv[ey][ex] = rr;
+        } else {
+            if constexpr (F_ON) s_psi[ey][ex] = potential(P, rho, T);
+            if constexpr (G_ON) s_inv[ey][ex] = 1.0 / rho;
+        }
         if constexpr (G_ON) {
-            s_inv[ey][ex] = 1.0 / rho;
             s_To[ey][ex] = A.Told[id];
             s_U0[ey][ex] = A.Uold[id];
             s_U1[ey][ex] = A.Uold[n + id];
@@ -307,20 +357,23 @@ __global__ void __launch_bounds__(F2_TX * F2_TY) k_fused_d2q9(Params P, FusedArg
         return true;
     };
 
-    double f[9], g[9], rho = 0, T = 0;
+    // the ring first, so the own node's populations are live only across the barrier
+    for (int r = threadIdx.x; r < NRING; r += blockDim.x) {
+        int ex, ey;
+        ring_slot(r, F2_TX, F2_TY, ex, ey);
+        double rf[9], rg[9], rrho, rt, rrr;
+        EosRho rer;
+        uint32_t rid;
+        slot(ex, ey, rf, rg, rrho, rt, rid, false, rrr, rer);
+    }
+    double f[9], g[9], rho = 0, T = 0, rr = 0;
+    EosRho er{};
     uint32_t id = 0;
     const int gx = x0 + tx, gy = y0 + ty;
     const bool own = gx < A.nx && gy < A.ny;
     // interior slot (threads outside the box still fill the slot of the
     // wrapped node, so partial tiles see their periodic neighbours)
-    const bool have = slot(tx + 1, ty + 1, f, g, rho, T, id);
-    for (int r = threadIdx.x; r < NRING; r += blockDim.x) {
-        int ex, ey;
-        ring_slot(r, F2_TX, F2_TY, ex, ey);
-        double rf[9], rg[9], rr, rt;
-        uint32_t rid;
-        slot(ex, ey, rf, rg, rr, rt, rid);
-    }
+    const bool have = slot(tx + 1, ty + 1, f, g, rho, T, id, own, rr, er);
     __syncthreads();
     if (!own || !have) return;
 
@@ -353,86 +406,95 @@ __global__ void __launch_bounds__(F2_TX * F2_TY) k_fused_d2q9(Params P, FusedArg
         double dot = 0;
 #pragma unroll
         for (int k = 0; k < 3; k++) dot += gT[k] * gR[k];
-        heat = heat_source_value(P, rho, To, dot, div, A.S[id]);
+        heat = heat_source_value_er(P, er, rho, rr, To, dot, div, A.S[id]);
     }
     double psi = 0;
     if constexpr (F_ON) psi = s_psi[ey][ex];
     auto nbpsi = [&](int k) { return s_psi[ey + cyk<L>(k)][ex + cxk<L>(k)]; };
-    finish_node<L, F_ON, G_ON, EMIT>(P, A, id, onb, f, g, rho, T, psi, nbpsi, heat);
+    finish_node<L, F_ON, G_ON, EMIT>(P, A, id, onb, f, g, rho, rr, T, psi, nbpsi, heat);
 }
 
 // ------------------------------------------------------------ 3D kernel
-// xy tile of TX x TY columns marching along z over a chunk of planes, with
-// a three-plane ring buffer of psi (tile + one-node ring).  Isothermal:
-// liTempMRT is D2Q9 only, so T is read, never written.
+// xy tile of TX x TY columns marching along z over a chunk of planes.
+// Shared memory: a three-plane ring buffer of psi (tile + one-node ring) and
+// the pulled populations of the current and next plane (k-major, thread
+// fastest: conflict-free), so only a few scalars stay in registers across
+// the plane barriers.  Isothermal: liTempMRT is D2Q9 only, so T is read,
+// never written.
 constexpr int F3_TX = 32, F3_TY = 8;
+constexpr int F3_EX = F3_TX + 2, F3_EY = F3_TY + 2;
+constexpr size_t F3_SMEM = (size_t)(3 * F3_EY * F3_EX + 2 * 15 * F3_TX * F3_TY) * sizeof(double);
 
 template <bool HAS_BC, bool EMIT>
-__global__ void __launch_bounds__(F3_TX * F3_TY) k_fused_d3q15(Params P, FusedArgs A) {
+__global__ void __launch_bounds__(F3_TX * F3_TY, 2) k_fused_d3q15(Params P, FusedArgs A) {
     using L = D3Q15T;
-    constexpr int EX = F3_TX + 2, EY = F3_TY + 2, NRING = 2 * EX + 2 * F3_TY;
-    __shared__ double s_psi[3][EY][EX];
-    const int tx = threadIdx.x % F3_TX, ty = threadIdx.x / F3_TX;
+    constexpr int EX = F3_EX, EY = F3_EY, NT = F3_TX * F3_TY, NRING = 2 * EX + 2 * F3_TY;
+    extern __shared__ double dsm[];
+    double(*s_psi)[EY][EX] = reinterpret_cast<double(*)[EY][EX]>(dsm);
+    double* s_f = dsm + 3 * EY * EX;  // [2][15][NT]
+    const int tid = threadIdx.x;
+    const int tx = tid % F3_TX, ty = tid / F3_TX;
     const int tiles = A.tiles_x * A.tiles_y;
     const int col = blockIdx.x % tiles, chunk = blockIdx.x / tiles;
     const int bx = col % A.tiles_x, by = col / A.tiles_x;
     const int x0 = bx * F3_TX, y0 = by * F3_TY;
     const int z0 = chunk * A.zchunk;
     const int z1 = min(z0 + A.zchunk, A.nz);
+    const int ox = slot_coord(x0, tx + 1, A.nx, A.px), oy = slot_coord(y0, ty + 1, A.ny, A.py);
+    const bool own_xy = (x0 + tx) < A.nx && (y0 + ty) < A.ny;
 
-    // psi of the ext slot (ex, ey) at plane z into ring slot; own pull into f
-    auto plane = [&](int z, double* f, double& rho, double& T, uint32_t& id) -> bool {
+    // Plane z: psi of every ext slot into the ring buffer; the own node's
+    // pulled populations into s_f[buf]; returns whether the own slot exists.
+    auto plane = [&](int z, int buf, double& rho, double& T, double& rr, uint32_t& id) -> bool {
         const int zs = slot_coord(z, 1, A.nz, A.pz);
-        bool have = false;
         double g_unused[1];
-        {
-            const int x = slot_coord(x0, tx + 1, A.nx, A.px);
-            const int y = slot_coord(y0, ty + 1, A.ny, A.py);
-            double& ps = s_psi[(z + 3) % 3][ty + 1][tx + 1];
-            if (x >= 0 && y >= 0 && zs >= 0) {
-                id = (uint32_t)x + (uint32_t)A.nx * ((uint32_t)y + (uint32_t)A.ny * (uint32_t)zs);
-                pull_node<L, true, false, HAS_BC>(P, A, x, y, zs, id, f, g_unused, rho, T);
-                ps = potential(P, rho, T);
-                have = true;
-            }
-        }
-        for (int r = threadIdx.x; r < NRING; r += blockDim.x) {
+        for (int r = tid; r < NRING; r += NT) {
             int ex, ey;
             ring_slot(r, F3_TX, F3_TY, ex, ey);
             const int x = slot_coord(x0, ex, A.nx, A.px);
             const int y = slot_coord(y0, ey, A.ny, A.py);
             if (x < 0 || y < 0 || zs < 0) continue;
             uint32_t rid = (uint32_t)x + (uint32_t)A.nx * ((uint32_t)y + (uint32_t)A.ny * (uint32_t)zs);
-            double rf[15], rr, rt;
-            pull_node<L, true, false, HAS_BC>(P, A, x, y, zs, rid, rf, g_unused, rr, rt);
-            s_psi[(z + 3) % 3][ey][ex] = potential(P, rr, rt);
+            double rf[15], rrho, rt;
+            pull_node<L, true, false, HAS_BC>(P, A, x, y, zs, rid, rf, g_unused, rrho, rt);
+            s_psi[(z + 3) % 3][ey][ex] = potential(P, rrho, rt);
         }
-        return have;
+        if (ox < 0 || oy < 0 || zs < 0) return false;
+        id = (uint32_t)ox + (uint32_t)A.nx * ((uint32_t)oy + (uint32_t)A.ny * (uint32_t)zs);
+        double f[15];
+        pull_node<L, true, false, HAS_BC>(P, A, ox, oy, zs, id, f, g_unused, rho, T);
+        s_psi[(z + 3) % 3][ty + 1][tx + 1] = potential(P, rho, T);
+        rr = rcp_rn(rho);
+#pragma unroll
+        for (int k = 0; k < 15; k++) s_f[(buf * 15 + k) * NT + tid] = f[k];
+        return true;
     };
 
-    double fc[15], fn[15], rc = 0, rn = 0, Tc = 0, Tn = 0;
+    double rc = 0, Tc = 0, rrc = 0, rn = 0, Tn = 0, rrn = 0;
     uint32_t idc = 0, idn = 0;
-    double dum[15], dr, dt;
-    uint32_t did;
-    plane(z0 - 1, dum, dr, dt, did);
-    bool hc = plane(z0, fc, rc, Tc, idc);
-    const bool own_xy = (x0 + tx) < A.nx && (y0 + ty) < A.ny;
+    {
+        double dr, dt, drr;
+        uint32_t did;
+        plane(z0 - 1, 1, dr, dt, drr, did);  // psi only; its populations are never read
+    }
+    bool hc = plane(z0, z0 & 1, rc, Tc, rrc, idc);
     for (int z = z0; z < z1; z++) {
-        bool hn = plane(z + 1, fn, rn, Tn, idn);
+        bool hn = plane(z + 1, (z + 1) & 1, rn, Tn, rrn, idn);
         __syncthreads();
         if (own_xy && hc) {
-            const int gx = x0 + tx, gy = y0 + ty;
-            const bool onb = on_wall(A, gx, gy, z);
+            const bool onb = on_wall(A, ox, oy, z);
             const int ex = tx + 1, ey = ty + 1;
+            double f[15], dum[1];
+#pragma unroll
+            for (int k = 0; k < 15; k++) f[k] = s_f[((z & 1) * 15 + k) * NT + tid];
             auto nbpsi = [&](int k) {
                 return s_psi[(z + czk<L>(k) + 3) % 3][ey + cyk<L>(k)][ex + cxk<L>(k)];
             };
-            finish_node<L, true, false, EMIT>(P, A, idc, onb, fc, dum, rc, Tc, s_psi[z % 3][ey][ex], nbpsi, 0.0);
+            finish_node<L, true, false, EMIT>(P, A, idc, onb, f, dum, rc, rrc, Tc, s_psi[z % 3][ey][ex], nbpsi, 0.0);
         }
         __syncthreads();
-#pragma unroll
-        for (int k = 0; k < 15; k++) fc[k] = fn[k];
         rc = rn;
+        rrc = rrn;
         Tc = Tn;
         idc = idn;
         hc = hn;
@@ -440,6 +502,15 @@ __global__ void __launch_bounds__(F3_TX * F3_TY) k_fused_d3q15(Params P, FusedAr
 }
 
 // ================================================================= host side
+// The 3D kernel uses more than the 48 KB of static shared memory.
+inline cudaError_t fused_attributes() {
+    cudaError_t e;
+    if ((e = cudaFuncSetAttribute(k_fused_d3q15<true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)F3_SMEM))) return e;
+    if ((e = cudaFuncSetAttribute(k_fused_d3q15<true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)F3_SMEM))) return e;
+    if ((e = cudaFuncSetAttribute(k_fused_d3q15<false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)F3_SMEM))) return e;
+    return cudaFuncSetAttribute(k_fused_d3q15<false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)F3_SMEM);
+}
+
 // Launch geometry: tiles per axis, z chunk (3D) and the number of blocks.
 inline int fused_geometry(int lat, FusedArgs& A) {
     if (lat == MPLB_D2Q9) {
@@ -561,6 +632,10 @@ inline int fused_setup(FusedConfig& fc, int lat, const int* model, const Params&
     }
     A.bcmap = fc.bcmap;
     fc.nblocks = fused_geometry(lat, A);
+    if (lat == MPLB_D3Q15 && fused_attributes() != cudaSuccess) {
+        fc.err = "cannot raise the dynamic shared memory limit";
+        return MPLB_E_CUDA;
+    }
     return 0;
 }
 
@@ -582,11 +657,11 @@ inline cudaError_t fused_launch(const FusedConfig& fc, const Params& P, const Fu
         else if (g_on) MPLB_F2_B(false, true);
     } else {
         if (bc) {
-            if (emit) k_fused_d3q15<true, true><<<fc.nblocks, F3_TX * F3_TY, 0, s>>>(P, A);
-            else k_fused_d3q15<true, false><<<fc.nblocks, F3_TX * F3_TY, 0, s>>>(P, A);
+            if (emit) k_fused_d3q15<true, true><<<fc.nblocks, F3_TX * F3_TY, F3_SMEM, s>>>(P, A);
+            else k_fused_d3q15<true, false><<<fc.nblocks, F3_TX * F3_TY, F3_SMEM, s>>>(P, A);
         } else {
-            if (emit) k_fused_d3q15<false, true><<<fc.nblocks, F3_TX * F3_TY, 0, s>>>(P, A);
-            else k_fused_d3q15<false, false><<<fc.nblocks, F3_TX * F3_TY, 0, s>>>(P, A);
+            if (emit) k_fused_d3q15<false, true><<<fc.nblocks, F3_TX * F3_TY, F3_SMEM, s>>>(P, A);
+            else k_fused_d3q15<false, false><<<fc.nblocks, F3_TX * F3_TY, F3_SMEM, s>>>(P, A);
         }
     }
 #undef MPLB_F2

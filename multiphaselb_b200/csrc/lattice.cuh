@@ -92,7 +92,33 @@ struct Params {
     double a, b, R, G, M, Cv, rho_0;
     double g[3], fext[3];
     double pr_tc, pr_kappa;      // Peng-Robinson: 0.170151343*a/(b*R), 0.37464+1.5422w-0.26992w^2
+    // exact shortcuts, decided on the host: x/G == -x when G == -1,
+    // x/Cv == x when Cv == 1, x/(M*M) == x when M*M == 1
+    int32_t g_neg1, cv_one, m2_one;
 };
+
+// ----------------------------------------------------------- exact division
+// Markstein's theorem (P. Markstein, IBM J. Res. Dev. 34(1), 1990; see also
+// Muller et al., Handbook of Floating-Point Arithmetic, ch. 5): if yr is the
+// correctly rounded reciprocal RN(1/y) and q = RN(x*yr), the remainder
+// e = x - q*y is exact in one FMA and RN(q + e*yr) = RN(x/y), for results
+// that neither overflow nor underflow.  So several quotients with the same
+// divisor cost one reciprocal and three operations each, and are bit-equal to
+// IEEE division.  A zero numerator returns q, which keeps the sign of x/y.
+MPLB_HD double div_rcp(double x, double y, double yr) {
+    const double q = x * yr;
+    const double e = fma(-q, y, x);
+    return q == 0.0 ? q : fma(e, yr, q);
+}
+// RN(1/3) for x/3.0.
+constexpr double RCP3 = 1.0 / 3.0;
+MPLB_HD double div3(double x) { return div_rcp(x, 3.0, RCP3); }
+
+#ifdef __CUDA_ARCH__
+__device__ __forceinline__ double rcp_rn(double y) { return __drcp_rn(y); }
+#else
+inline double rcp_rn(double y) { return 1.0 / y; }
+#endif
 
 // ---------------------------------------------------------------------- EOS
 // p_eos.c:7-64
@@ -110,15 +136,71 @@ MPLB_HD double p_eos(const Params& P, double rho, double T) {
         return rho * P.R * T / (1 - P.b * rho) - P.a * be * be * rho * rho / (1 + 2 * P.b * rho - P.b * rho * P.b * rho);
     }
     case MPLB_EOS_VDW:
-        return rho * P.R * T / (P.M - rho * P.b) - P.a * rho * rho / (P.M * P.M);
+        return rho * P.R * T / (P.M - rho * P.b) - (P.m2_one ? P.a * rho * rho : P.a * rho * rho / (P.M * P.M));
     default:
         return 0;
     }
 }
 
-// potential.c:7-13
-MPLB_HD double potential(const Params& P, double rho, double T) {
-    return sqrt(2 * (p_eos(P, rho, T) - rho * P.cs2) / (P.G));
+// potential.c:7-13, given p_EOS(rho, T)
+MPLB_HD double potential_p(const Params& P, double rho, double p) {
+    const double v = 2 * (p - rho * P.cs2);
+    return sqrt(P.g_neg1 ? -v : v / (P.G));
+}
+MPLB_HD double potential(const Params& P, double rho, double T) { return potential_p(P, rho, p_eos(P, rho, T)); }
+
+// p_eos for several temperatures at one density: the density-only parts are
+// evaluated once (each is the same operation on the same operands as in
+// p_eos, so the values are identical); quotients whose numerator depends on T
+// use one shared reciprocal and div_rcp.
+struct EosRho {
+    double z;   // CS: (1+al+al^2-al^3)/(be^3)
+    double d;   // VdW: M - rho*b; PR: 1 - b*rho
+    double dr;  // RN(1/d)
+    double d2;  // PR: 1 + 2*b*rho - b*rho*b*rho
+    double d2r;
+    double att; // VdW: a*rho*rho/(M*M)
+};
+MPLB_HD EosRho eos_rho(const Params& P, double rho) {
+    EosRho e{};
+    switch (P.eos) {
+    case MPLB_EOS_CS: {
+        double al = P.b * rho / 4.0;
+        double be = 1 - al;
+        e.z = (1 + al + al * al - al * al * al) / (be * be * be);
+        break;
+    }
+    case MPLB_EOS_PR:
+        e.d = 1 - P.b * rho;
+        e.dr = rcp_rn(e.d);
+        e.d2 = 1 + 2 * P.b * rho - P.b * rho * P.b * rho;
+        e.d2r = rcp_rn(e.d2);
+        break;
+    case MPLB_EOS_VDW:
+        e.d = P.M - rho * P.b;
+        e.dr = rcp_rn(e.d);
+        e.att = P.m2_one ? P.a * rho * rho : P.a * rho * rho / (P.M * P.M);
+        break;
+    default:
+        break;
+    }
+    return e;
+}
+MPLB_HD double p_eos_at(const Params& P, const EosRho& e, double rho, double T) {
+    switch (P.eos) {
+    case MPLB_EOS_IDEAL:
+        return rho * P.R * T;
+    case MPLB_EOS_CS:
+        return rho * P.R * T * e.z - P.a * rho * rho;
+    case MPLB_EOS_PR: {
+        double be = (1 + P.pr_kappa * (1 - sqrt(T / P.pr_tc)));
+        return div_rcp(rho * P.R * T, e.d, e.dr) - div_rcp(P.a * be * be * rho * rho, e.d2, e.d2r);
+    }
+    case MPLB_EOS_VDW:
+        return div_rcp(rho * P.R * T, e.d, e.dr) - e.att;
+    default:
+        return 0;
+    }
 }
 
 // --------------------------------------------------------------- matvecs
@@ -147,15 +229,34 @@ MPLB_HD void mul_M(const double* v, double* r) {
     });
 }
 
-// M^-1 entries are rounded constants: product rounded, then added.  Its
-// zero pattern is that of M^T.
+// Squared norm of moment row r (rows of M are orthogonal: M^-1 = M^T D^-1).
+template <class L>
+MPLB_HD constexpr int row_norm2(int r) {
+    int s = 0;
+    for (int k = 0; k < L::Q; k++) s += Mint<L>(r, k) * Mint<L>(r, k);
+    return s;
+}
+
+// M^-1 m.  The reference's M^-1 entries are RN(M[j][i] / |row j|^2)
+// (D2Q9_MRTInv.c, D3Q15_MRTInv.c), and every |M[j][i]| is a power of two,
+// so each entry is exactly M[j][i] * RN(1/|row j|^2) and each rounded product
+// RN(entry * m_j) is exactly M[j][i] * p_j with p_j = RN(RN(1/|row j|^2) * m_j).
+// One multiply per column, then the reference's row sums in j order.
 template <class L>
 MPLB_HD void mul_Mi(const Params& P, const double* v, double* r) {
+    (void)P;
+    double p[L::Q];
+    static_for<L::Q>([&](auto j) {
+        constexpr double c = 1.0 / (double)row_norm2<L>(decltype(j)::value);
+        p[j] = c * v[j];
+    });
     static_for<L::Q>([&](auto i) {
         double s = 0;
         static_for<L::Q>([&](auto j) {
             constexpr int c = Mint<L>(decltype(j)::value, decltype(i)::value);
-            if constexpr (c != 0) s = s + P.Mi[i][j] * v[j];
+            if constexpr (c == 1) s = s + p[j];
+            else if constexpr (c == -1) s = s - p[j];
+            else if constexpr (c != 0) s = s + (double)c * p[j];
         });
         r[i] = s;
     });
@@ -192,8 +293,8 @@ MPLB_HD void eq_heat(const Params& P, double T, double u0, double u1, double* g)
 
 // ---------------------------------------------------------- node collisions
 // liMRTCollision.c:48-106 with liMRTForce.c:18-42.  f in/out (9 values).
-MPLB_HD void collide_limrt(const Params& P, double* f, double rho, const double* U,
-                           const double* F, const double* Fi, double T) {
+MPLB_HD void collide_limrt_psi(const Params& P, double* f, double rho, const double* U,
+                               const double* F, const double* Fi, double ps) {
     double um = 0;
 #pragma unroll
     for (int k = 0; k < 3; k++) um += U[k] * U[k];
@@ -208,7 +309,6 @@ MPLB_HD void collide_limrt(const Params& P, double* f, double rho, const double*
     meq[7] = rho * (U[0] * U[0] - U[1] * U[1]);
     meq[8] = rho * U[0] * U[1];
     mul_M<D2Q9T>(f, m);
-    double ps = potential(P, rho, T);
     double uf = U[0] * F[0] + U[1] * F[1];
     double fi2 = Fi[0] * Fi[0] + Fi[1] * Fi[1];
     S[0] = 0;
@@ -224,11 +324,15 @@ MPLB_HD void collide_limrt(const Params& P, double* f, double rho, const double*
     for (int k = 0; k < 9; k++) m[k] = m[k] - P.Lf[k] * (m[k] - meq[k]) + P.relax_f[k] * S[k];
     mul_Mi<D2Q9T>(P, m, f);
 }
+MPLB_HD void collide_limrt(const Params& P, double* f, double rho, const double* U, const double* F,
+                           const double* Fi, double T) {
+    collide_limrt_psi(P, f, rho, U, F, Fi, potential(P, rho, T));
+}
 
 // xuMRTCollision.c:46-89, xuMRTEquilibriumMS.c:12-51, xuMRTForce.c:14-69.
 // F here is Fi + (rho - rho_0) g (no fext), xuMRTForce.c:18-22.
-MPLB_HD void collide_xumrt(const Params& P, double* f, double rho, const double* U,
-                           const double* Fi, double T) {
+MPLB_HD void collide_xumrt_psi(const Params& P, double* f, double rho, const double* U,
+                               const double* Fi, double ps) {
     double um = 0;
 #pragma unroll
     for (int k = 0; k < 3; k++) um += U[k] * U[k];
@@ -237,11 +341,11 @@ MPLB_HD void collide_xumrt(const Params& P, double* f, double rho, const double*
     meq[1] = rho * (-1.0 + um);
     meq[2] = rho * (1.0 - 5.0 * um);
     meq[3] = rho * U[0];
-    meq[4] = rho * -7.0 * U[0] / 3.0;
+    meq[4] = div3(rho * -7.0 * U[0]);
     meq[5] = rho * U[1];
-    meq[6] = rho * -7.0 * U[1] / 3.0;
+    meq[6] = div3(rho * -7.0 * U[1]);
     meq[7] = rho * U[2];
-    meq[8] = rho * -7.0 * U[2] / 3.0;
+    meq[8] = div3(rho * -7.0 * U[2]);
     meq[9] = rho * (2.0 * U[0] * U[0] - U[1] * U[1] - U[2] * U[2]);
     meq[10] = rho * (U[1] * U[1] - U[2] * U[2]);
     meq[11] = rho * U[0] * U[1];
@@ -251,7 +355,6 @@ MPLB_HD void collide_xumrt(const Params& P, double* f, double rho, const double*
     mul_M<D3Q15T>(f, m);
 #pragma unroll
     for (int j = 0; j < 3; j++) F[j] = Fi[j] + (rho - P.rho_0) * P.g[j];
-    double ps = potential(P, rho, T);
     double uf = U[0] * F[0] + U[1] * F[1] + U[2] * F[2];
     double f2 = 0;
 #pragma unroll
@@ -260,11 +363,11 @@ MPLB_HD void collide_xumrt(const Params& P, double* f, double rho, const double*
     S[1] = 2.0 * uf + (P.sig6 * f2) / (ps * ps * P.s1_den);
     S[2] = -10.0 * uf;
     S[3] = F[0];
-    S[4] = -7.0 * F[0] / 3.0;
+    S[4] = div3(-7.0 * F[0]);
     S[5] = F[1];
-    S[6] = -7.0 * F[1] / 3.0;
+    S[6] = div3(-7.0 * F[1]);
     S[7] = F[2];
-    S[8] = -7.0 * F[2] / 3.0;
+    S[8] = div3(-7.0 * F[2]);
     S[9] = 4.0 * U[0] * F[0] - 2.0 * U[1] * F[1] - 2.0 * U[2] * F[2];
     S[10] = 2.0 * U[1] * F[1] - 2.0 * U[2] * F[2];
     S[11] = U[0] * F[1] + U[1] * F[0];
@@ -274,6 +377,9 @@ MPLB_HD void collide_xumrt(const Params& P, double* f, double rho, const double*
 #pragma unroll
     for (int k = 0; k < 15; k++) m[k] = m[k] - P.Lf[k] * (m[k] - meq[k]) + P.relax_f[k] * S[k];
     mul_Mi<D3Q15T>(P, m, f);
+}
+MPLB_HD void collide_xumrt(const Params& P, double* f, double rho, const double* U, const double* Fi, double T) {
+    collide_xumrt_psi(P, f, rho, U, Fi, potential(P, rho, T));
 }
 
 // liTempMRTCollision.c:38-84, liTempMRTEquilibriumMS.c:20-38, liTempMRTSource.c:17-24.
@@ -305,6 +411,17 @@ MPLB_HD double heat_source_value(const Params& P, double rho, double T, double d
     double dpdT = p_eos(P, rho, 1.1 * T) - p_eos(P, rho, 0.9 * T);
     dpdT = dpdT / (0.2 * T);
     double s = -lambda * dot / P.Cv + divU * T * (1.0 - dpdT / (rho * P.Cv));
+    return s + 0.5 * (s - oldss);
+}
+// Same value, with the density's EOS parts er and rr = RN(1/rho) shared.
+MPLB_HD double heat_source_value_er(const Params& P, const EosRho& er, double rho, double rr, double T,
+                                    double dot, double divU, double oldss) {
+    double lambda = rho * P.Cv * P.lam_fac;
+    double dpdT = p_eos_at(P, er, rho, 1.1 * T) - p_eos_at(P, er, rho, 0.9 * T);
+    dpdT = dpdT / (0.2 * T);
+    double a = P.cv_one ? -lambda * dot : -lambda * dot / P.Cv;
+    double b = P.cv_one ? div_rcp(dpdT, rho, rr) : dpdT / (rho * P.Cv);
+    double s = a + divU * T * (1.0 - b);
     return s + 0.5 * (s - oldss);
 }
 

@@ -580,6 +580,9 @@ int mplb_gpu_create(const mplb_mesh_desc* mesh, const mplb_eos_desc* eos, const 
     P.Cv = eos->Cv;
     P.rho_0 = eos->rho_0;
     for (int j = 0; j < 3; j++) { P.g[j] = eos->g[j]; P.fext[j] = eos->fext[j]; }
+    P.g_neg1 = eos->G == -1.0;
+    P.cv_one = eos->Cv == 1.0;
+    P.m2_one = eos->M * eos->M == 1.0;
     if (eos->type == MPLB_EOS_PR) {
         P.pr_tc = 0.170151343 * eos->a / (eos->b * eos->R);
         P.pr_kappa = 0.37464 + 1.5422 * eos->w - 0.26992 * eos->w * eos->w;

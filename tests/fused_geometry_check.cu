@@ -25,9 +25,15 @@ void check(int nx, int ny, int nz, int px, int py, int pz) {
     auto check_node = [&](int x, int y, int z, const char* what) {
         REQUIRE(x >= 0 && x < A.nx && y >= 0 && y < A.ny && z >= 0 && z < A.nz, "%s node (%d,%d,%d)", what, x, y, z);
         int64_t id = (int64_t)x + (int64_t)A.nx * ((int64_t)y + (int64_t)A.ny * z);
+        const NodeOffsets no = node_offsets(A, x, y, z, L::D);
         for (int k = 0; k < L::Q; k++) {
             int64_t s = pull_src(A.nx, A.ny, A.nz, A.px, A.py, A.pz, x, y, z, cxk<L>(k), cyk<L>(k), czk<L>(k));
             REQUIRE(s >= -1 && s < n, "pull src %lld of node %lld k %d", (long long)s, (long long)id, k);
+            bool miss;
+            uint32_t src = source_of(no, (uint32_t)id, cxk<L>(k), cyk<L>(k), czk<L>(k), miss);
+            REQUIRE(miss == (s < 0), "missing flag of node %lld k %d", (long long)id, k);
+            REQUIRE((int64_t)src == (s < 0 ? id : s), "offset source %u != %lld (node %lld k %d)", src, (long long)s,
+                    (long long)id, k);
             // fixedT neighbour x + c_k (2D)
             int mx = wrap1(x + cxk<L>(k), A.nx, A.px), my = wrap1(y + cyk<L>(k), A.ny, A.py);
             if (mx >= 0 && my >= 0) REQUIRE((int64_t)mx + (int64_t)A.nx * my < n || L::D == 3, "fixedT nb");
