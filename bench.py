@@ -43,8 +43,9 @@ WORKLOADS = {
                              build=lambda c: c.bubble_case(1, 192, 48.0, 5.0, 0.75)),
 }
 PROFILE_TRAFFIC = {  # per-launch DRAM bytes summaries committed under profiles/
-    "column_d2q9_128x512": "fused_d2q9_column_128x512.txt",
-    "bubble_d3q15_192": "fused_d3q15_bubble_192.txt",
+    "column_d2q9_128x512": "k_fused_d2q9_column_128x512.txt",
+    "bubble_d2q9_256": "k_fused_d2q9_bubble_256.txt",
+    "bubble_d3q15_192": "k_fused_d3q15_bubble.txt",
 }
 FALLBACK_HBM_GBS = 6650.0
 
