@@ -200,6 +200,21 @@ int mplb_gpu_mass_energy(mplb_gpu_t* h, double* mass, double* energy);
 /* Wait for the handle's stream. */
 int mplb_gpu_sync(mplb_gpu_t* h);
 
+/* Total mass sum(rho[i]) and energy sum(T[i]) of plain device arrays, without
+ * allocating device memory.  No counterpart in the reference: it is for
+ * callers that may not call cudaMalloc where they want this check (a
+ * framework allocator that owns device memory, a time loop with a
+ * no-allocation policy, code that must not synchronise the device).
+ * rho, T (may be NULL: energy 0) and out (2 doubles: mass, energy) are device
+ * pointers on the current device; work is queued on `stream` (a cudaStream_t,
+ * NULL = the default stream) and not waited for.
+ * Scratch is a fixed 64 KiB array inside the library, held by every GPU that
+ * loads it until exit; n is limited to 16,777,216 nodes (larger n returns
+ * MPLB_E_ARG).  The first call on a device looks up that array's device
+ * address; make that first call before any stream capture.  Calls that
+ * overlap on the GPU share the array and race; order them on one stream. */
+int mplb_mass_energy_noalloc(const double* rho, const double* T, uint32_t n, double* out, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -16,7 +16,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 LIB_DIR = os.path.join(HERE, "lib")
 LIB = os.path.join(LIB_DIR, "libmplb_gpu.so")
-SOURCES = [os.path.join(HERE, "csrc", "mplb_gpu.cu")]
+SOURCES = [os.path.join(HERE, "csrc", "mplb_gpu.cu"), os.path.join(HERE, "csrc", "mplb_noalloc.cu")]
 HEADERS = [os.path.join(HERE, "csrc", f) for f in ("lattice.cuh", "ops.cuh", "fused.cuh")] + \
           [os.path.join(ROOT, "include", "mplb_gpu.h")]
 

@@ -489,6 +489,9 @@ int materialize(mplb_gpu* h) {
 
 }  // namespace
 
+// Error text for the library's other translation units.
+int mplb_internal_fail(int code, const std::string& msg) { return fail(code, msg); }
+
 // ================================================================= C-ABI
 extern "C" {
 
