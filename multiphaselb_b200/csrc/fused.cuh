@@ -544,12 +544,14 @@ struct FusedConfig {
 inline bool fused_supported(int lat, const int* model, const Params& P, const std::vector<PatchDev>* fp,
                             const bool* serial, const mplb_mesh_desc* mesh, const int* dims, const int* per,
                             std::string& why) {
-    (void)P;
     (void)per;
+    const bool active[2] = {model[0] != MPLB_NO_MODEL && P.f_update != 0, model[1] != MPLB_NO_MODEL && P.g_update != 0};
     if (serial[0] || serial[1]) { why = "boundary updates depend on the serial order"; return false; }
-    if (model[0] == MPLB_NO_MODEL) { why = "no flow field"; return false; }
-    if (lat == MPLB_D3Q15 && model[1] != MPLB_NO_MODEL) { why = "thermal field on D3Q15"; return false; }
-    for (int fi = 0; fi < 2; fi++)
+    if (!active[0] && !active[1]) { why = "no field is updated"; return false; }
+    if (!active[0] && model[0] == MPLB_NO_MODEL) { why = "no flow field"; return false; }
+    if (lat == MPLB_D3Q15 && active[1]) { why = "thermal field on D3Q15"; return false; }
+    for (int fi = 0; fi < 2; fi++) {
+        if (!active[fi]) continue;
         for (const PatchDev& pt : fp[fi]) {
             if (pt.type == MPLB_BC_PERIODIC) continue;
             if (pt.type == MPLB_BC_BOUNCEBACK) continue;
@@ -558,6 +560,7 @@ inline bool fused_supported(int lat, const int* model, const Params& P, const st
             why = "boundary type " + std::to_string(pt.type) + " is handled by the operator path only";
             return false;
         }
+    }
     if (dims[0] < 2 || dims[1] < 2 || (lat == MPLB_D3Q15 && dims[2] < 2)) { why = "box thinner than 2 nodes"; return false; }
     (void)mesh;
     return true;
@@ -588,6 +591,7 @@ inline int fused_setup(FusedConfig& fc, int lat, const int* model, const Params&
             for (uint32_t i = 0; i < fp[0][p].count; i++) {
                 uint32_t id = mesh->patch_nodes[off + i];
                 for (int fi = 0; fi < 2; fi++) {
+                    if (!(fi == 0 ? P.f_update : P.g_update)) continue;
                     int t = fp[fi][p].type;
                     if (t != MPLB_BC_BOUNCEBACK && t != MPLB_BC_FIXEDT) continue;
                     BCProg& b = node[id];

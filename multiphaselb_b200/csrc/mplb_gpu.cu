@@ -129,6 +129,9 @@ void fill_tables(Params& P) {
 
 int check_field(const mplb_field_desc* d, int lat, int which, uint32_t npatch, std::string& why) {
     if (!d || d->model == MPLB_NO_MODEL) return 0;
+    // A frozen field is never touched by the reference (every operator checks
+    // field->update first), so any model and boundary set is accepted for it.
+    if (!d->update) return 0;
     if (d->surface_tension != 0) { why = "surface tension terms are not part of this path"; return MPLB_E_UNSUPPORTED; }
     if (which == 0) {
         if (d->model == MPLB_LIMRT && lat != MPLB_D2Q9) { why = "liMRT is D2Q9 only (liMRTForce.c:13)"; return MPLB_E_UNSUPPORTED; }
@@ -216,6 +219,7 @@ bool detect_box(mplb_gpu* h, const mplb_mesh_desc* m) {
 // reads a population that any boundary op writes (the reference's serial
 // order would then be observable) or if a patch lists a node twice.
 bool needs_serial(const mplb_gpu* h, const mplb_mesh_desc* m, int fi) {
+    if (!(fi == 0 ? h->P.f_update : h->P.g_update)) return false;
     const int Q = h->Q;
     const int nax = Q == 9 ? 4 : 6;
     auto rev = [&](int k) { return Q == 9 ? revk<D2Q9T>(k) : revk<D3Q15T>(k); };

@@ -299,6 +299,14 @@ int ref_op(ref_case* c, int op, int field, uint32_t start, uint32_t end) {
     return 0;
 }
 
+/* The reference structures of a case, for the adapter check. */
+void ref_structs(ref_case* c, latticeMesh** m, macroFields** mf, lbeField** f, lbeField** g) {
+    *m = &c->mesh;
+    *mf = &c->mf;
+    *f = &c->f;
+    *g = &c->g;
+}
+
 /* p_eos and potential as scalar functions, for EOS-level checks. */
 double ref_p_eos(ref_case* c, double rho, double T) { return p_eos(&c->mesh.EOS, rho, T); }
 double ref_potential(ref_case* c, double rho, double T) { return potential(&c->mesh, rho, T); }
