@@ -130,6 +130,8 @@ typedef struct mplb_opts {
     int32_t device;      /* CUDA device ordinal; -1 = the calling thread's current device */
     void* stream;        /* cudaStream_t to launch on; NULL = a stream owned by the handle */
     uint32_t start_time; /* reference timeInfo.start: the time the first step leaves */
+    int32_t tile_config; /* fused path: 0 = time the tile candidates on the first step and keep
+                            the fastest; k > 0 = use candidate k-1; -1 = candidate 0, no timing */
 } mplb_opts;
 
 /* What create decided; filled by mplb_gpu_info. */
@@ -141,6 +143,8 @@ typedef struct mplb_info {
     uint32_t current_time;   /* reference timeInfo.current */
     uint64_t device_bytes;   /* device memory held by the handle */
     uint64_t kernel_launches;/* kernels this handle has launched so far */
+    int32_t tile_config;     /* fused path: candidate in use (0-based), -1 before the first step */
+    float tile_ms[8];        /* fused path: autotuner time per candidate (ms per step), 0 = not timed */
 } mplb_info;
 
 typedef struct mplb_gpu mplb_gpu_t;

@@ -86,12 +86,12 @@ class Lattice:
     the same attributes: lattice, n, nb, points, patches, eos, f, g).
     """
 
-    def __init__(self, case, path=PATH_AUTO, device=-1, stream=None, start_time=0):
+    def __init__(self, case, path=PATH_AUTO, device=-1, stream=None, start_time=0, tile_config=0):
         self.lib = load_library()
         self.case = case
         self.n, self.Q = case.n, case.Q
         self._desc = abi.Descriptors(case)
-        opts = abi.Opts(abi.FP64, path, device, stream, start_time)
+        opts = abi.Opts(abi.FP64, path, device, stream, start_time, tile_config)
         h = C.c_void_p()
         self._check(self.lib.mplb_gpu_create(C.byref(self._desc.mesh), C.byref(self._desc.eos),
                                               C.byref(self._desc.f), C.byref(self._desc.g),
@@ -125,7 +125,8 @@ class Lattice:
         self._check(self.lib.mplb_gpu_info(self.h, C.byref(i)))
         return dict(path=i.path, box_dims=tuple(i.box_dims), box_periodic=tuple(i.box_periodic),
                     bc_sequential=i.bc_sequential, current_time=i.current_time,
-                    device_bytes=i.device_bytes, kernel_launches=i.kernel_launches)
+                    device_bytes=i.device_bytes, kernel_launches=i.kernel_launches,
+                    tile_config=i.tile_config, tile_ms=list(i.tile_ms))
 
     # -------------------------------------------------------------- host data
     def upload(self, rho=None, U=None, T=None, f=None, g=None, S=None, Fi=None, Ft=None):

@@ -65,6 +65,7 @@ class Opts(C.Structure):
         ("device", C.c_int32),
         ("stream", C.c_void_p),
         ("start_time", C.c_uint32),
+        ("tile_config", C.c_int32),
     ]
 
 
@@ -77,6 +78,8 @@ class Info(C.Structure):
         ("current_time", C.c_uint32),
         ("device_bytes", C.c_uint64),
         ("kernel_launches", C.c_uint64),
+        ("tile_config", C.c_int32),
+        ("tile_ms", C.c_float * 8),
     ]
 
 

@@ -144,6 +144,28 @@ MPLB_HD bool on_wall(const FusedArgs& A, int x, int y, int z) {
            (!A.pz && (z == 0 || z == A.nz - 1));
 }
 
+// bounceBack.c:21-70 on registers, k ascending, in place.
+template <class L>
+__device__ __forceinline__ void bounce_back(uint32_t miss, double* v) {
+#pragma unroll
+    for (int k = 0; k < L::Q; k++) {
+        const int r = revk<L>(k);
+        if ((miss >> k) & 1u) {
+            v[k] = v[r];
+        } else if (!((miss >> r) & 1u) && k >= 1 && k <= L::NAX) {
+            v[k] = 0.5 * v[k] + 0.5 * v[r];
+            v[r] = v[k];
+        }
+    }
+}
+
+// The flow field's boundary program of node id (bounce-back ops in patch order).
+template <class L>
+__device__ __forceinline__ void apply_flow_program(const FusedArgs& A, uint32_t id, uint32_t miss, double* f) {
+    const BCProg& pr = A.prog[A.bcmap[id]];
+    for (int o = 0; o < pr.nf; o++) bounce_back<L>(miss, f);
+}
+
 // ------------------------------------------------------------ phase A
 // Pull-stream one node, apply its boundary program, sum moments.
 // f, g receive f''_n, g''_n; miss bit k = population k has no source.
@@ -165,19 +187,7 @@ __device__ __forceinline__ void pull_node(const Params& P, const FusedArgs& A, i
         uint8_t pi = A.bcmap[id];
         if (pi) {
             const BCProg& pr = A.prog[pi];
-            // bounceBack.c:21-70 on registers, k ascending, in place
-            auto bounce = [&](double* v) {
-#pragma unroll
-                for (int k = 0; k < L::Q; k++) {
-                    const int r = revk<L>(k);
-                    if ((miss >> k) & 1u) {
-                        v[k] = v[r];
-                    } else if (!((miss >> r) & 1u) && k >= 1 && k <= L::NAX) {
-                        v[k] = 0.5 * v[k] + 0.5 * v[r];
-                        v[r] = v[k];
-                    }
-                }
-            };
+            auto bounce = [&](double* v) { bounce_back<L>(miss, v); };
             if constexpr (F_ON)
                 for (int o = 0; o < pr.nf; o++) bounce(f);
             if constexpr (G_ON) {
@@ -314,10 +324,10 @@ __device__ __forceinline__ void finish_node(const Params& P, const FusedArgs& A,
 // ------------------------------------------------------------ 2D kernel
 // Tile of TX x TY nodes, one thread each, plus the one-node ring around it
 // (psi, 1/rho, T_{n-1}, U_{n-1}) computed by the first threads.
-constexpr int F2_TX = 32, F2_TY = 8;
+constexpr int min_blocks(int threads) { return threads <= 128 ? 4 : (threads <= 256 ? 2 : 1); }
 
-template <bool F_ON, bool G_ON, bool HAS_BC, bool EMIT>
-__global__ void __launch_bounds__(F2_TX * F2_TY, 2) k_fused_d2q9(Params P, FusedArgs A) {
+template <int F2_TX, int F2_TY, bool F_ON, bool G_ON, bool HAS_BC, bool EMIT>
+__global__ void __launch_bounds__(F2_TX * F2_TY, min_blocks(F2_TX * F2_TY)) k_fused_d2q9(Params P, FusedArgs A) {
     using L = D2Q9T;
     constexpr int EX = F2_TX + 2, EY = F2_TY + 2, NRING = 2 * EX + 2 * F2_TY;
     constexpr int GY = G_ON ? EY : 1, GX = G_ON ? EX : 1;
@@ -414,21 +424,22 @@ __global__ void __launch_bounds__(F2_TX * F2_TY, 2) k_fused_d2q9(Params P, Fused
     finish_node<L, F_ON, G_ON, EMIT>(P, A, id, onb, f, g, rho, rr, T, psi, nbpsi, heat);
 }
 
-// ------------------------------------------------------------ 3D kernel
+// ------------------------------------------------------------ 3D kernels
 // xy tile of TX x TY columns marching along z over a chunk of planes.
 // Shared memory: a three-plane ring buffer of psi (tile + one-node ring) and
 // the pulled populations of the current and next plane (k-major, thread
 // fastest: conflict-free), so only a few scalars stay in registers across
 // the plane barriers.  Isothermal: liTempMRT is D2Q9 only, so T is read,
 // never written.
-constexpr int F3_TX = 32, F3_TY = 8;
-constexpr int F3_EX = F3_TX + 2, F3_EY = F3_TY + 2;
-constexpr size_t F3_SMEM = (size_t)(3 * F3_EY * F3_EX + 2 * 15 * F3_TX * F3_TY) * sizeof(double);
+template <int TX, int TY, bool PIPE>
+constexpr size_t f3_smem() {
+    return (size_t)(3 * (TY + 2) * (TX + 2) + (PIPE ? 3 : 2) * 15 * TX * TY) * sizeof(double);
+}
 
-template <bool HAS_BC, bool EMIT>
-__global__ void __launch_bounds__(F3_TX * F3_TY, 2) k_fused_d3q15(Params P, FusedArgs A) {
+template <int F3_TX, int F3_TY, bool HAS_BC, bool EMIT>
+__global__ void __launch_bounds__(F3_TX * F3_TY, min_blocks(F3_TX * F3_TY)) k_fused_d3q15(Params P, FusedArgs A) {
     using L = D3Q15T;
-    constexpr int EX = F3_EX, EY = F3_EY, NT = F3_TX * F3_TY, NRING = 2 * EX + 2 * F3_TY;
+    constexpr int EX = F3_TX + 2, EY = F3_TY + 2, NT = F3_TX * F3_TY, NRING = 2 * EX + 2 * F3_TY;
     extern __shared__ double dsm[];
     double(*s_psi)[EY][EX] = reinterpret_cast<double(*)[EY][EX]>(dsm);
     double* s_f = dsm + 3 * EY * EX;  // [2][15][NT]
@@ -501,33 +512,183 @@ __global__ void __launch_bounds__(F3_TX * F3_TY, 2) k_fused_d3q15(Params P, Fuse
     }
 }
 
-// ================================================================= host side
-// The 3D kernel uses more than the 48 KB of static shared memory.
-inline cudaError_t fused_attributes() {
-    cudaError_t e;
-    if ((e = cudaFuncSetAttribute(k_fused_d3q15<true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)F3_SMEM))) return e;
-    if ((e = cudaFuncSetAttribute(k_fused_d3q15<true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)F3_SMEM))) return e;
-    if ((e = cudaFuncSetAttribute(k_fused_d3q15<false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)F3_SMEM))) return e;
-    return cudaFuncSetAttribute(k_fused_d3q15<false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)F3_SMEM);
+// Pipelined variant: each node's pulled populations are fetched with cp.async two planes ahead
+// into a three-slot shared-memory ring (k-major, thread fastest: conflict
+// free), so their DRAM latency overlaps the collision of the current plane.
+// psi lives in a three-plane ring (tile + one-node ring); the ring nodes'
+// pulls are plain loads.  Isothermal: liTempMRT is D2Q9 only, so T is read,
+// never written.
+constexpr int F3_STAGES = 3;
+
+__device__ __forceinline__ void cp_async8(double* smem, const double* gmem) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait1() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
+
+template <int F3_TX, int F3_TY, bool HAS_BC, bool EMIT>
+__global__ void __launch_bounds__(F3_TX * F3_TY, min_blocks(F3_TX * F3_TY)) k_fused_d3q15_pipe(Params P, FusedArgs A) {
+    using L = D3Q15T;
+    constexpr int EX = F3_TX + 2, EY = F3_TY + 2, NT = F3_TX * F3_TY, NRING = 2 * EX + 2 * F3_TY;
+    extern __shared__ double dsm[];
+    double(*s_psi)[EY][EX] = reinterpret_cast<double(*)[EY][EX]>(dsm);
+    double* s_f = dsm + 3 * EY * EX;  // [F3_STAGES][15][NT]
+    const uint32_t n = P.n;
+    const int tid = threadIdx.x;
+    const int tx = tid % F3_TX, ty = tid / F3_TX;
+    const int tiles = A.tiles_x * A.tiles_y;
+    const int col = blockIdx.x % tiles, chunk = blockIdx.x / tiles;
+    const int bx = col % A.tiles_x, by = col / A.tiles_x;
+    const int x0 = bx * F3_TX, y0 = by * F3_TY;
+    const int z0 = chunk * A.zchunk;
+    const int z1 = min(z0 + A.zchunk, A.nz);
+    const int ox = slot_coord(x0, tx + 1, A.nx, A.px), oy = slot_coord(y0, ty + 1, A.ny, A.py);
+    const bool own_xy = (x0 + tx) < A.nx && (y0 + ty) < A.ny;
+
+    // Plane z's own pulls -> stage (z+3)%3 (nothing when the slot is absent).
+    auto prefetch = [&](int z) {
+        const int zs = slot_coord(z, 1, A.nz, A.pz);
+        if (ox >= 0 && oy >= 0 && zs >= 0) {
+            const uint32_t id = (uint32_t)ox + (uint32_t)A.nx * ((uint32_t)oy + (uint32_t)A.ny * (uint32_t)zs);
+            const NodeOffsets no = node_offsets(A, ox, oy, zs, 3);
+            double* dst = s_f + ((z + 3) % F3_STAGES) * 15 * NT + tid;
+            static_for<15>([&](auto kk) {
+                constexpr int k = decltype(kk)::value;
+                bool m;
+                const uint32_t src = source_of(no, id, cxk<L>(k), cyk<L>(k), czk<L>(k), m);
+                cp_async8(dst + k * NT, A.fin + (size_t)k * n + src);
+            });
+        }
+        cp_async_commit();
+    };
+    // Plane z after its pulls landed: own boundary program, moments, psi; the
+    // ring's psi from plain loads.  Returns whether the own slot exists.
+    auto process = [&](int z, double& rho, double& T, double& rr, uint32_t& id) -> bool {
+        const int zs = slot_coord(z, 1, A.nz, A.pz);
+        double g_unused[1];
+        bool have = false;
+        if (ox >= 0 && oy >= 0 && zs >= 0) {
+            id = (uint32_t)ox + (uint32_t)A.nx * ((uint32_t)oy + (uint32_t)A.ny * (uint32_t)zs);
+            double* src = s_f + ((z + 3) % F3_STAGES) * 15 * NT + tid;
+            double f[15];
+#pragma unroll
+            for (int k = 0; k < 15; k++) f[k] = src[k * NT];
+            bool changed = false;
+            if constexpr (HAS_BC) {
+                if (A.bcmap[id]) {
+                    const NodeOffsets no = node_offsets(A, ox, oy, zs, 3);
+                    uint32_t miss = 0;
+                    static_for<15>([&](auto kk) {
+                        constexpr int k = decltype(kk)::value;
+                        bool m;
+                        source_of(no, id, cxk<L>(k), cyk<L>(k), czk<L>(k), m);
+                        miss |= (uint32_t)m << k;
+                    });
+                    apply_flow_program<L>(A, id, miss, f);
+                    changed = true;
+                }
+            }
+            double s = 0;
+#pragma unroll
+            for (int k = 0; k < 15; k++) s += f[k];
+            rho = s;
+            T = A.Told[id];
+            rr = rcp_rn(rho);
+            s_psi[(z + 3) % 3][ty + 1][tx + 1] = potential(P, rho, T);
+            if (changed) {
+#pragma unroll
+                for (int k = 0; k < 15; k++) src[k * NT] = f[k];
+            }
+            have = true;
+        }
+        for (int r = tid; r < NRING; r += NT) {
+            int ex, ey;
+            ring_slot(r, F3_TX, F3_TY, ex, ey);
+            const int x = slot_coord(x0, ex, A.nx, A.px);
+            const int y = slot_coord(y0, ey, A.ny, A.py);
+            if (x < 0 || y < 0 || zs < 0) continue;
+            uint32_t rid = (uint32_t)x + (uint32_t)A.nx * ((uint32_t)y + (uint32_t)A.ny * (uint32_t)zs);
+            double rf[15], rrho, rt;
+            pull_node<L, true, false, HAS_BC>(P, A, x, y, zs, rid, rf, g_unused, rrho, rt);
+            s_psi[(z + 3) % 3][ey][ex] = potential(P, rrho, rt);
+        }
+        return have;
+    };
+
+    double rc = 0, Tc = 0, rrc = 0, rn = 0, Tn = 0, rrn = 0;
+    uint32_t idc = 0, idn = 0;
+    bool hc = false;
+    prefetch(z0 - 1);
+    prefetch(z0);
+    for (int j = z0 - 1; j <= z1; j++) {
+        cp_async_wait1();  // plane j's group is complete (only j+1's may be pending)
+        const bool hn = process(j, rn, Tn, rrn, idn);
+        __syncthreads();
+        const int z = j - 1;
+        if (z >= z0 && own_xy && hc) {
+            const bool onb = on_wall(A, ox, oy, z);
+            const int ex = tx + 1, ey = ty + 1;
+            double f[15], dum[1];
+            const double* src = s_f + ((z + 3) % F3_STAGES) * 15 * NT + tid;
+#pragma unroll
+            for (int k = 0; k < 15; k++) f[k] = src[k * NT];
+            auto nbpsi = [&](int k) {
+                return s_psi[(z + czk<L>(k) + 3) % 3][ey + cyk<L>(k)][ex + cxk<L>(k)];
+            };
+            finish_node<L, true, false, EMIT>(P, A, idc, onb, f, dum, rc, rrc, Tc, s_psi[(z + 3) % 3][ey][ex], nbpsi, 0.0);
+        }
+        __syncthreads();
+        if (j + 2 <= z1) prefetch(j + 2);
+        else cp_async_commit();  // empty group keeps the wait count uniform
+        rc = rn;
+        rrc = rrn;
+        Tc = Tn;
+        idc = idn;
+        hc = hn;
+    }
 }
 
-// Launch geometry: tiles per axis, z chunk (3D) and the number of blocks.
-inline int fused_geometry(int lat, FusedArgs& A) {
+// ================================================================= host side
+// Candidate tile shapes.  The autotuner times each on the real state at the
+// first fused step and keeps the fastest; results are identical for all.
+struct TileCfg {
+    int tx, ty;
+    bool pipe;  // 3D only: cp.async-staged pulls
+};
+constexpr int N_CFG2 = 5, N_CFG3 = 6;
+constexpr TileCfg CFG2[N_CFG2] = {{32, 8, false}, {32, 4, false}, {64, 4, false}, {16, 8, false}, {32, 16, false}};
+constexpr TileCfg CFG3[N_CFG3] = {{32, 8, false}, {32, 8, true}, {32, 4, false}, {64, 4, false}, {32, 16, false}, {64, 8, false}};
+
+struct Geom {
+    int tiles_x, tiles_y, zchunk, nblocks;
+};
+
+// Launch geometry for one tile shape: tiles per axis, z chunk (3D), blocks.
+inline Geom fused_geometry(int lat, const FusedArgs& A, int TX, int TY) {
+    Geom g;
+    g.tiles_x = (A.nx + TX - 1) / TX;
+    g.tiles_y = (A.ny + TY - 1) / TY;
     if (lat == MPLB_D2Q9) {
-        A.tiles_x = (A.nx + F2_TX - 1) / F2_TX;
-        A.tiles_y = (A.ny + F2_TY - 1) / F2_TY;
-        A.zchunk = 1;
-        return A.tiles_x * A.tiles_y;
+        g.zchunk = 1;
+        g.nblocks = g.tiles_x * g.tiles_y;
+        return g;
     }
-    A.tiles_x = (A.nx + F3_TX - 1) / F3_TX;
-    A.tiles_y = (A.ny + F3_TY - 1) / F3_TY;
-    // z chunks: aim for >= 4 blocks per SM of a 148-SM part, chunks of >= 8 planes
-    const int cols = A.tiles_x * A.tiles_y;
-    const int want = (4 * 148 + cols - 1) / cols;
+    // z chunks: aim for >= 4 blocks of 256 threads per SM of a 148-SM part, chunks of >= 8 planes
+    const int cols = g.tiles_x * g.tiles_y;
+    const int per_sm = std::max(1, 4 * 256 / (TX * TY));
+    const int want = (per_sm * 148 + cols - 1) / cols;
     int zc = (A.nz + want - 1) / want;
     zc = std::max(zc, std::min(8, A.nz));
-    A.zchunk = zc;
-    return cols * ((A.nz + zc - 1) / zc);
+    g.zchunk = zc;
+    g.nblocks = cols * ((A.nz + zc - 1) / zc);
+    return g;
+}
+
+inline void apply_geom(FusedArgs& A, const Geom& g) {
+    A.tiles_x = g.tiles_x;
+    A.tiles_y = g.tiles_y;
+    A.zchunk = g.zchunk;
 }
 
 struct FusedConfig {
@@ -535,8 +696,156 @@ struct FusedConfig {
     FusedArgs args{};
     uint8_t* bcmap = nullptr;
     bool has_bc = false;
+    int lat = 0;
+    int cfg = 0;           // chosen candidate
+    bool tuned = false;    // autotuner has run (or a candidate was forced)
+    Geom geom[N_CFG3 > N_CFG2 ? N_CFG3 : N_CFG2];
+    float tune_ms[N_CFG3 > N_CFG2 ? N_CFG3 : N_CFG2] = {};
+    int ncfg = 0;
     int nblocks = 0;
 };
+
+template <int TX, int TY, bool PIPE, bool HAS_BC, bool EMIT>
+cudaError_t set_smem3() {
+    if constexpr (PIPE)
+        return cudaFuncSetAttribute(k_fused_d3q15_pipe<TX, TY, HAS_BC, EMIT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)f3_smem<TX, TY, PIPE>());
+    else
+        return cudaFuncSetAttribute(k_fused_d3q15<TX, TY, HAS_BC, EMIT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)f3_smem<TX, TY, PIPE>());
+}
+
+// The 3D kernels use more than the 48 KB of static shared memory.
+inline cudaError_t fused_attributes() {
+    cudaError_t e = cudaSuccess;
+    auto chk = [&](cudaError_t r) { if (e == cudaSuccess) e = r; };
+    chk(set_smem3<32, 8, false, true, true>());
+    chk(set_smem3<32, 8, false, false, true>());
+#define MPLB_SET3(TX, TY, PIPE) chk(set_smem3<TX, TY, PIPE, true, false>()); chk(set_smem3<TX, TY, PIPE, false, false>());
+    MPLB_SET3(32, 8, false)
+    MPLB_SET3(32, 8, true)
+    MPLB_SET3(32, 4, false)
+    MPLB_SET3(64, 4, false)
+    MPLB_SET3(32, 16, false)
+    MPLB_SET3(64, 8, false)
+#undef MPLB_SET3
+    return e;
+}
+
+template <int TX, int TY, bool F_ON, bool G_ON, bool EMIT>
+void launch2(bool bc, int nb, const Params& P, const FusedArgs& A, cudaStream_t s) {
+    if (bc) k_fused_d2q9<TX, TY, F_ON, G_ON, true, EMIT><<<nb, TX * TY, 0, s>>>(P, A);
+    else k_fused_d2q9<TX, TY, F_ON, G_ON, false, EMIT><<<nb, TX * TY, 0, s>>>(P, A);
+}
+
+template <int TX, int TY, bool EMIT>
+void launch2_fg(bool fon, bool gon, bool bc, int nb, const Params& P, const FusedArgs& A, cudaStream_t s) {
+    if (fon && gon) launch2<TX, TY, true, true, EMIT>(bc, nb, P, A, s);
+    else if (fon) launch2<TX, TY, true, false, EMIT>(bc, nb, P, A, s);
+    else if (gon) launch2<TX, TY, false, true, EMIT>(bc, nb, P, A, s);
+}
+
+template <int TX, int TY, bool PIPE, bool EMIT>
+void launch3(bool bc, int nb, const Params& P, const FusedArgs& A, cudaStream_t s) {
+    constexpr size_t sm = f3_smem<TX, TY, PIPE>();
+    if constexpr (PIPE) {
+        if (bc) k_fused_d3q15_pipe<TX, TY, true, EMIT><<<nb, TX * TY, sm, s>>>(P, A);
+        else k_fused_d3q15_pipe<TX, TY, false, EMIT><<<nb, TX * TY, sm, s>>>(P, A);
+    } else {
+        if (bc) k_fused_d3q15<TX, TY, true, EMIT><<<nb, TX * TY, sm, s>>>(P, A);
+        else k_fused_d3q15<TX, TY, false, EMIT><<<nb, TX * TY, sm, s>>>(P, A);
+    }
+}
+
+// Launch one fused step with candidate `cfg` (EMIT always uses candidate 0).
+inline cudaError_t fused_launch_cfg(const FusedConfig& fc, int cfg, const Params& P, FusedArgs A, bool f_on, bool g_on,
+                                    bool emit, cudaStream_t s) {
+    if (emit) cfg = 0;
+    apply_geom(A, fc.geom[cfg]);
+    const int nb = fc.geom[cfg].nblocks;
+    const bool bc = fc.has_bc;
+    if (fc.lat == MPLB_D2Q9) {
+        if (emit) {
+            launch2_fg<32, 8, true>(f_on, g_on, bc, nb, P, A, s);
+        } else {
+            switch (cfg) {
+            case 0: launch2_fg<32, 8, false>(f_on, g_on, bc, nb, P, A, s); break;
+            case 1: launch2_fg<32, 4, false>(f_on, g_on, bc, nb, P, A, s); break;
+            case 2: launch2_fg<64, 4, false>(f_on, g_on, bc, nb, P, A, s); break;
+            case 3: launch2_fg<16, 8, false>(f_on, g_on, bc, nb, P, A, s); break;
+            default: launch2_fg<32, 16, false>(f_on, g_on, bc, nb, P, A, s); break;
+            }
+        }
+    } else {
+        if (emit) {
+            launch3<32, 8, false, true>(bc, nb, P, A, s);
+        } else {
+            switch (cfg) {
+            case 0: launch3<32, 8, false, false>(bc, nb, P, A, s); break;
+            case 1: launch3<32, 8, true, false>(bc, nb, P, A, s); break;
+            case 2: launch3<32, 4, false, false>(bc, nb, P, A, s); break;
+            case 3: launch3<64, 4, false, false>(bc, nb, P, A, s); break;
+            case 4: launch3<32, 16, false, false>(bc, nb, P, A, s); break;
+            default: launch3<64, 8, false, false>(bc, nb, P, A, s); break;
+            }
+        }
+    }
+    return cudaGetLastError();
+}
+
+inline cudaError_t fused_launch(const FusedConfig& fc, const Params& P, const FusedArgs& A, int lat, bool f_on,
+                                bool g_on, bool emit, cudaStream_t s) {
+    (void)lat;
+    return fused_launch_cfg(fc, fc.cfg, P, A, f_on, g_on, emit, s);
+}
+
+// Time every candidate on the current state (2 warm-up + 3 timed launches)
+// and keep the fastest.  The step's outputs are rewritten by the real launch
+// that follows; the heat-source history S, updated in place, is saved to
+// `save` before and restored after every trial.
+inline int fused_autotune(FusedConfig& fc, const Params& P, const FusedArgs& A, bool f_on, bool g_on, double* S,
+                          double* save, size_t n, cudaStream_t s) {
+    cudaEvent_t e0, e1;
+    if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess) {
+        fc.err = "autotune: event creation failed";
+        return MPLB_E_CUDA;
+    }
+    const bool keep_s = g_on && S && save;
+    if (keep_s && cudaMemcpyAsync(save, S, n * sizeof(double), cudaMemcpyDeviceToDevice, s) != cudaSuccess) {
+        fc.err = "autotune: saving S failed";
+        return MPLB_E_CUDA;
+    }
+    float best = 1e30f;
+    int best_cfg = 0;
+    for (int c = 0; c < fc.ncfg; c++) {
+        float tot = 0;
+        bool ok = true;
+        for (int r = 0; r < 5 && ok; r++) {
+            if (r >= 2) cudaEventRecord(e0, s);
+            ok = fused_launch_cfg(fc, c, P, A, f_on, g_on, false, s) == cudaSuccess;
+            if (r >= 2) {
+                cudaEventRecord(e1, s);
+                cudaEventSynchronize(e1);
+                float ms = 0;
+                cudaEventElapsedTime(&ms, e0, e1);
+                tot += ms;
+            }
+            if (keep_s) cudaMemcpyAsync(S, save, n * sizeof(double), cudaMemcpyDeviceToDevice, s);
+        }
+        fc.tune_ms[c] = ok ? tot / 3 : -1.0f;
+        if (ok && tot < best) {
+            best = tot;
+            best_cfg = c;
+        }
+    }
+    cudaGetLastError();
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    fc.cfg = best_cfg;
+    fc.nblocks = fc.geom[best_cfg].nblocks;
+    fc.tuned = true;
+    return cudaStreamSynchronize(s) == cudaSuccess ? 0 : MPLB_E_CUDA;
+}
 
 // Fused path preconditions: box mesh, no serial boundary dependence, only
 // bounceBack / fixedT / periodic patches, at most FUSED_MAX_OPS ops per node
@@ -635,7 +944,15 @@ inline int fused_setup(FusedConfig& fc, int lat, const int* model, const Params&
         *bytes += n;
     }
     A.bcmap = fc.bcmap;
-    fc.nblocks = fused_geometry(lat, A);
+    fc.lat = lat;
+    fc.ncfg = lat == MPLB_D2Q9 ? N_CFG2 : N_CFG3;
+    for (int c = 0; c < fc.ncfg; c++) {
+        const TileCfg t = lat == MPLB_D2Q9 ? CFG2[c] : CFG3[c];
+        fc.geom[c] = fused_geometry(lat, A, t.tx, t.ty);
+    }
+    fc.cfg = 0;
+    apply_geom(A, fc.geom[0]);
+    fc.nblocks = fc.geom[0].nblocks;
     if (lat == MPLB_D3Q15 && fused_attributes() != cudaSuccess) {
         fc.err = "cannot raise the dynamic shared memory limit";
         return MPLB_E_CUDA;
@@ -648,30 +965,5 @@ inline void fused_free(FusedConfig& fc) {
     fc.bcmap = nullptr;
 }
 
-// Launch one fused step (EMIT = rebuild the reference state, no collision).
-inline cudaError_t fused_launch(const FusedConfig& fc, const Params& P, const FusedArgs& A, int lat, bool f_on,
-                                bool g_on, bool emit, cudaStream_t s) {
-    const bool bc = fc.has_bc;
-#define MPLB_F2(F, G, B, E) k_fused_d2q9<F, G, B, E><<<fc.nblocks, F2_TX * F2_TY, 0, s>>>(P, A)
-#define MPLB_F2_E(F, G, B) (emit ? (MPLB_F2(F, G, B, true), 0) : (MPLB_F2(F, G, B, false), 0))
-#define MPLB_F2_B(F, G) (bc ? MPLB_F2_E(F, G, true) : MPLB_F2_E(F, G, false))
-    if (lat == MPLB_D2Q9) {
-        if (f_on && g_on) MPLB_F2_B(true, true);
-        else if (f_on) MPLB_F2_B(true, false);
-        else if (g_on) MPLB_F2_B(false, true);
-    } else {
-        if (bc) {
-            if (emit) k_fused_d3q15<true, true><<<fc.nblocks, F3_TX * F3_TY, F3_SMEM, s>>>(P, A);
-            else k_fused_d3q15<true, false><<<fc.nblocks, F3_TX * F3_TY, F3_SMEM, s>>>(P, A);
-        } else {
-            if (emit) k_fused_d3q15<false, true><<<fc.nblocks, F3_TX * F3_TY, F3_SMEM, s>>>(P, A);
-            else k_fused_d3q15<false, false><<<fc.nblocks, F3_TX * F3_TY, F3_SMEM, s>>>(P, A);
-        }
-    }
-#undef MPLB_F2
-#undef MPLB_F2_E
-#undef MPLB_F2_B
-    return cudaGetLastError();
-}
 
 }  // namespace mplb

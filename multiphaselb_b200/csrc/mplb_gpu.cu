@@ -76,6 +76,7 @@ struct mplb_gpu {
     int red_parts = 0;
     FusedConfig fc{};
     int fstate = 0;  // 0: buffers hold the reference's state; 1: post-collision (fused)
+    int tile_request = 0;  // mplb_opts.tile_config
     uint32_t current = 0;
     uint64_t launches = 0;
     uint64_t bytes = 0;
@@ -469,6 +470,18 @@ int fused_step(mplb_gpu* h, bool emit) {
     A.rho_out = h->rho;
     A.Fi_out = h->Fi;
     A.Ft_out = h->Ft;
+    if (!emit && !h->fc.tuned) {
+        if (h->tile_request == 0) {
+            RET(staging(h, h->n));
+            if (int rc = fused_autotune(h->fc, h->P, A, fon, gon, h->S, h->stage, h->n, h->stream))
+                return fail(rc, h->fc.err);
+        } else {
+            int c = h->tile_request > 0 ? h->tile_request - 1 : 0;
+            if (c >= h->fc.ncfg) return fail(MPLB_E_ARG, "tile_config out of range");
+            h->fc.cfg = c;
+            h->fc.tuned = true;
+        }
+    }
     cudaError_t e = fused_launch(h->fc, h->P, A, h->lat, fon, gon, emit, h->stream);
     h->launches++;
     if (e != cudaSuccess) return fail(MPLB_E_CUDA, std::string("fused kernel launch: ") + cudaGetErrorString(e));
@@ -532,6 +545,7 @@ int mplb_gpu_create(const mplb_mesh_desc* mesh, const mplb_eos_desc* eos, const 
     h->D = Q == 9 ? 2 : 3;
     h->n = mesh->n_points;
     h->current = opts ? opts->start_time : 0;
+    h->tile_request = opts ? opts->tile_config : 0;
     int want_path = opts ? opts->path : MPLB_PATH_AUTO;
     int dev = opts ? opts->device : -1;
     if (dev < 0) {
@@ -693,6 +707,8 @@ int mplb_gpu_info(mplb_gpu_t* h, mplb_info* info) {
     info->current_time = h->current;
     info->device_bytes = h->bytes;
     info->kernel_launches = h->launches;
+    info->tile_config = (h->path == MPLB_PATH_FUSED && h->fc.tuned) ? h->fc.cfg : -1;
+    for (int c = 0; c < 8; c++) info->tile_ms[c] = c < h->fc.ncfg ? h->fc.tune_ms[c] : 0.0f;
     return 0;
 }
 

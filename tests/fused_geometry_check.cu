@@ -13,14 +13,15 @@ static int fails = 0;
 #define REQUIRE(c, ...) do { if (!(c)) { if (fails++ < 10) { printf("FAIL %s:%d ", __FILE__, __LINE__); printf(__VA_ARGS__); printf("\n"); } } } while (0)
 
 template <class L>
-void check(int nx, int ny, int nz, int px, int py, int pz) {
+void check_cfg(int nx, int ny, int nz, int px, int py, int pz, int TX, int TY) {
     FusedArgs A{};
     A.nx = nx; A.ny = ny; A.nz = L::D == 3 ? nz : 1;
     A.px = px; A.py = py; A.pz = L::D == 3 ? pz : 1;
-    const int nblocks = fused_geometry(L::lattice, A);
+    const Geom gm = fused_geometry(L::lattice, A, TX, TY);
+    apply_geom(A, gm);
+    const int nblocks = gm.nblocks;
     const int64_t n = (int64_t)A.nx * A.ny * A.nz;
     std::vector<int> owned(n, 0);
-    const int TX = L::D == 2 ? F2_TX : F3_TX, TY = L::D == 2 ? F2_TY : F3_TY;
     const int EX = TX + 2, EY = TY + 2, NRING = 2 * EX + 2 * TY;
     auto check_node = [&](int x, int y, int z, const char* what) {
         REQUIRE(x >= 0 && x < A.nx && y >= 0 && y < A.ny && z >= 0 && z < A.nz, "%s node (%d,%d,%d)", what, x, y, z);
@@ -89,13 +90,21 @@ void check(int nx, int ny, int nz, int px, int py, int pz) {
     for (int64_t i = 0; i < n; i++) REQUIRE(owned[i] == 1, "node %lld owned %d times (dims %d %d %d)", (long long)i, owned[i], nx, ny, nz);
 }
 
+template <class L>
+void check(int nx, int ny, int nz, int px, int py, int pz) {
+    if (L::D == 2)
+        for (int c = 0; c < N_CFG2; c++) check_cfg<L>(nx, ny, nz, px, py, pz, CFG2[c].tx, CFG2[c].ty);
+    else
+        for (int c = 0; c < N_CFG3; c++) check_cfg<L>(nx, ny, nz, px, py, pz, CFG3[c].tx, CFG3[c].ty);
+}
+
 int main() {
     int cases = 0;
     int dims2[][2] = {{2, 2}, {3, 5}, {24, 20}, {12, 24}, {12, 16}, {32, 8}, {33, 9}, {128, 512}, {256, 256}, {100, 3}};
     for (auto& d : dims2)
         for (int px = 0; px < 2; px++)
             for (int py = 0; py < 2; py++) { check<D2Q9T>(d[0], d[1], 1, px, py, 1); cases++; }
-    int dims3[][3] = {{2, 2, 2}, {10, 8, 6}, {8, 6, 7}, {33, 9, 17}, {64, 64, 64}, {96, 96, 96}, {40, 24, 100}};
+    int dims3[][3] = {{2, 2, 2}, {10, 8, 6}, {8, 6, 7}, {33, 9, 17}, {40, 40, 40}, {70, 20, 30}, {40, 24, 100}};
     for (auto& d : dims3)
         for (int p = 0; p < 8; p++) { check<D3Q15T>(d[0], d[1], d[2], p & 1, (p >> 1) & 1, (p >> 2) & 1); cases++; }
     if (fails) { printf("FAILED %d checks\n", fails); return 1; }

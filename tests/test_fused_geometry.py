@@ -15,7 +15,8 @@ def test_fused_indices_in_bounds():
         pytest.skip("nvcc not available")
     with tempfile.TemporaryDirectory() as d:
         exe = os.path.join(d, "geom")
-        subprocess.run([nvcc, "-std=c++17", "--expt-relaxed-constexpr", "-I", os.path.join(HERE, "..", "include"),
+        subprocess.run([nvcc, "-std=c++17", "--expt-relaxed-constexpr", "-gencode", "arch=compute_100a,code=sm_100a",
+                        "-I", os.path.join(HERE, "..", "include"),
                         "-o", exe, os.path.join(HERE, "fused_geometry_check.cu")], check=True, capture_output=True)
         r = subprocess.run([exe], capture_output=True, text=True, timeout=300)
     assert r.returncode == 0 and r.stdout.startswith("OK"), r.stdout + r.stderr

@@ -197,3 +197,28 @@ def test_fused_frozen_fields(gpu_lib, fu, gu):
     c2.g = dict(case.g, update=gu)
     got, info = run_gpu(c2, 6, path=abi.PATH_FUSED)
     assert_same(got, run_checker("port", c2, 6), ctx=f"fused update f={fu} g={gu}")
+
+
+@pytest.mark.parametrize("name", ["column_d2q9", "bubble_d2q9", "bubble_d3q15", "walls_d3q15"])
+def test_every_tile_candidate_is_exact(gpu_lib, name):
+    """Each fused tile shape (forced) gives the oracle's bits; the autotuner
+    then times them all and picks one."""
+    from multiphaselb_b200 import Lattice
+    case = small_cases()[name]
+    want = run_checker("port", case, 4)
+    ncand = 5 if case.lattice == abi.D2Q9 else 6
+    for c in range(1, ncand + 1):
+        with Lattice(case, path=abi.PATH_FUSED, tile_config=c) as lat:
+            lat.upload_case()
+            lat.initialize()
+            lat.step(4)
+            assert lat.info()["tile_config"] == c - 1
+            assert_same(lat.download(), want, ctx=f"{name} tile candidate {c - 1}")
+    with Lattice(case, path=abi.PATH_FUSED) as lat:
+        lat.upload_case()
+        lat.initialize()
+        lat.step(4)
+        info = lat.info()
+        assert 0 <= info["tile_config"] < ncand
+        assert all(t > 0 for t in info["tile_ms"][:ncand])
+        assert_same(lat.download(), want, ctx=f"{name} autotuned")
