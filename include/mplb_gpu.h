@@ -62,8 +62,12 @@ enum {
 /* Field selectors for the per-operator entry points. */
 enum { MPLB_FIELD_F = 0, MPLB_FIELD_G = 1 };
 
-/* Storage precision of the PDFs. */
-enum { MPLB_FP64 = 0 };
+/* Storage precision of the PDFs.  MPLB_FP32_DEV stores them in FP32 as
+ * deviations from the rest state (f - w rho_ref, g - wg T_ref), collides in
+ * FP32 and keeps the density / temperature sums, EOS, psi, force, heat source
+ * and T, U, S in FP64; fused box path only; not bit-identical to the
+ * reference (its error against FP64 is measured). */
+enum { MPLB_FP64 = 0, MPLB_FP32_DEV = 1 };
 
 /* Execution path. */
 enum {

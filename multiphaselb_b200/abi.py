@@ -14,7 +14,7 @@ EOS_IDEAL, EOS_CS, EOS_PR, EOS_VDW = 0, 1, 2, 3
 (BC_BOUNCEBACK, BC_FIXEDT, BC_FIXEDRANDOMT, BC_FIXEDGRADT, BC_FIXEDU, BC_UHF,
  BC_FIXEDEOSP, BC_OUTFLOW, BC_PERIODIC) = range(9)
 FIELD_F, FIELD_G = 0, 1
-FP64 = 0
+FP64, FP32_DEV = 0, 1
 PATH_AUTO, PATH_OPERATORS, PATH_FUSED = 0, 1, 2
 
 OK, E_ARG, E_UNSUPPORTED, E_CUDA, E_STATE, E_NONFINITE = 0, -1, -2, -3, -4, -5

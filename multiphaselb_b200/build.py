@@ -16,14 +16,18 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 LIB_DIR = os.path.join(HERE, "lib")
 LIB = os.path.join(LIB_DIR, "libmplb_gpu.so")
-SOURCES = [os.path.join(HERE, "csrc", "mplb_gpu.cu"), os.path.join(HERE, "csrc", "mplb_noalloc.cu")]
-HEADERS = [os.path.join(HERE, "csrc", f) for f in ("lattice.cuh", "ops.cuh", "fused.cuh")] + \
+# (source, multiply-add contraction): the bitwise FP64 path must not contract;
+# the FP32-deviation path may.
+SOURCES = [(os.path.join(HERE, "csrc", "mplb_gpu.cu"), False),
+           (os.path.join(HERE, "csrc", "mplb_noalloc.cu"), False),
+           (os.path.join(HERE, "csrc", "mplb_fp32.cu"), True)]
+HEADERS = [os.path.join(HERE, "csrc", f) for f in ("lattice.cuh", "ops.cuh", "fused.cuh", "fused_host.cuh", "fused32.cuh")] + \
           [os.path.join(ROOT, "include", "mplb_gpu.h")]
 
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
-    "-O3", "-lineinfo", "-std=c++17", "-fmad=false",
-    "-Xcompiler", "-fPIC", "-shared", "--expt-relaxed-constexpr",
+    "-O3", "-lineinfo", "-std=c++17",
+    "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr",
     "-Xptxas", "-warn-spills",
 ]
 
@@ -39,14 +43,10 @@ def needs_build():
     if not os.path.exists(LIB):
         return True
     t = os.path.getmtime(LIB)
-    return any(os.path.getmtime(s) > t for s in SOURCES + HEADERS)
+    return any(os.path.getmtime(s) > t for s in [s for s, _ in SOURCES] + HEADERS)
 
 
-def build(force=False, verbose=False, extra=()):
-    if not force and not needs_build():
-        return LIB
-    os.makedirs(LIB_DIR, exist_ok=True)
-    cmd = [nvcc()] + NVCC_FLAGS + list(extra) + ["-I", os.path.join(ROOT, "include"), "-o", LIB] + SOURCES
+def _run(cmd, verbose):
     if verbose:
         print(" ".join(cmd))
     r = subprocess.run(cmd, capture_output=True, text=True)
@@ -54,6 +54,42 @@ def build(force=False, verbose=False, extra=()):
         raise RuntimeError("nvcc failed:\n" + r.stdout + r.stderr)
     if verbose and (r.stdout or r.stderr):
         print(r.stdout + r.stderr)
+
+
+def compile_objects(out_dir, verbose=False, extra=()):
+    """Compile every translation unit to an object in out_dir (in parallel)."""
+    import concurrent.futures as cf
+    objs, jobs = [], []
+    for src, fmad in SOURCES:
+        obj = os.path.join(out_dir, os.path.basename(src) + ".o")
+        cmd = [nvcc()] + NVCC_FLAGS + ["-fmad=" + ("true" if fmad else "false")] + list(extra) + \
+              ["-I", os.path.join(ROOT, "include"), "-c", "-o", obj, src]
+        jobs.append(cmd)
+        objs.append(obj)
+    with cf.ThreadPoolExecutor(max_workers=len(jobs)) as ex:
+        list(ex.map(lambda c: _run(c, verbose), jobs))
+    return objs
+
+
+def build(force=False, verbose=False, extra=()):
+    if not force and not needs_build():
+        return LIB
+    os.makedirs(LIB_DIR, exist_ok=True)
+    objs = []
+    import concurrent.futures as cf
+    jobs = []
+    for src, fmad in SOURCES:
+        obj = os.path.join(LIB_DIR, os.path.basename(src) + ".o")
+        cmd = [nvcc()] + NVCC_FLAGS + ["-fmad=" + ("true" if fmad else "false")] + list(extra) + \
+              ["-I", os.path.join(ROOT, "include"), "-c", "-o", obj, src]
+        jobs.append(cmd)
+        objs.append(obj)
+    with cf.ThreadPoolExecutor(max_workers=len(jobs)) as ex:
+        list(ex.map(lambda c: _run(c, verbose), jobs))
+    _run([nvcc(), "-gencode", "arch=compute_100a,code=sm_100a", "-shared", "-Xcompiler", "-fPIC", "-o", LIB] + objs,
+         verbose)
+    for o in objs:
+        os.remove(o)
     return LIB
 
 

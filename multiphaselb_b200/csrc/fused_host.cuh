@@ -1,0 +1,286 @@
+// fused_host.cuh -- host side of the fused box path: boundary-program
+// tables, candidate launches, the tile autotuner.  Included only by the FP64
+// translation unit, so the FP64 kernels are instantiated in exactly one
+// object (compiled without multiply-add contraction).
+#pragma once
+
+#include "fused.cuh"
+
+namespace mplb {
+
+struct FusedConfig {
+    std::string err;
+    FusedArgs args{};
+    uint8_t* bcmap = nullptr;
+    bool has_bc = false;
+    int lat = 0;
+    int cfg = 0;           // chosen candidate
+    bool tuned = false;    // autotuner has run (or a candidate was forced)
+    Geom geom[N_CFG3 > N_CFG2 ? N_CFG3 : N_CFG2];
+    float tune_ms[N_CFG3 > N_CFG2 ? N_CFG3 : N_CFG2] = {};
+    int ncfg = 0;
+    int nblocks = 0;
+};
+
+template <int TX, int TY, bool PIPE, bool HAS_BC, bool EMIT>
+cudaError_t set_smem3() {
+    if constexpr (PIPE)
+        return cudaFuncSetAttribute(k_fused_d3q15_pipe<TX, TY, HAS_BC, EMIT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)f3_smem<TX, TY, PIPE>());
+    else
+        return cudaFuncSetAttribute(k_fused_d3q15<TX, TY, HAS_BC, EMIT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)f3_smem<TX, TY, PIPE>());
+}
+
+// The 3D kernels use more than the 48 KB of static shared memory.
+inline cudaError_t fused_attributes() {
+    cudaError_t e = cudaSuccess;
+    auto chk = [&](cudaError_t r) { if (e == cudaSuccess) e = r; };
+    chk(set_smem3<32, 8, false, true, true>());
+    chk(set_smem3<32, 8, false, false, true>());
+#define MPLB_SET3(TX, TY, PIPE) chk(set_smem3<TX, TY, PIPE, true, false>()); chk(set_smem3<TX, TY, PIPE, false, false>());
+    MPLB_SET3(32, 8, false)
+    MPLB_SET3(32, 8, true)
+    MPLB_SET3(32, 4, false)
+    MPLB_SET3(64, 4, false)
+    MPLB_SET3(32, 16, false)
+    MPLB_SET3(64, 8, false)
+#undef MPLB_SET3
+    return e;
+}
+
+template <int TX, int TY, bool F_ON, bool G_ON, bool EMIT>
+void launch2(bool bc, int nb, const Params& P, const FusedArgs& A, cudaStream_t s) {
+    if (bc) k_fused_d2q9<TX, TY, F_ON, G_ON, true, EMIT><<<nb, TX * TY, 0, s>>>(P, A);
+    else k_fused_d2q9<TX, TY, F_ON, G_ON, false, EMIT><<<nb, TX * TY, 0, s>>>(P, A);
+}
+
+template <int TX, int TY, bool EMIT>
+void launch2_fg(bool fon, bool gon, bool bc, int nb, const Params& P, const FusedArgs& A, cudaStream_t s) {
+    if (fon && gon) launch2<TX, TY, true, true, EMIT>(bc, nb, P, A, s);
+    else if (fon) launch2<TX, TY, true, false, EMIT>(bc, nb, P, A, s);
+    else if (gon) launch2<TX, TY, false, true, EMIT>(bc, nb, P, A, s);
+}
+
+template <int TX, int TY, bool PIPE, bool EMIT>
+void launch3(bool bc, int nb, const Params& P, const FusedArgs& A, cudaStream_t s) {
+    constexpr size_t sm = f3_smem<TX, TY, PIPE>();
+    if constexpr (PIPE) {
+        if (bc) k_fused_d3q15_pipe<TX, TY, true, EMIT><<<nb, TX * TY, sm, s>>>(P, A);
+        else k_fused_d3q15_pipe<TX, TY, false, EMIT><<<nb, TX * TY, sm, s>>>(P, A);
+    } else {
+        if (bc) k_fused_d3q15<TX, TY, true, EMIT><<<nb, TX * TY, sm, s>>>(P, A);
+        else k_fused_d3q15<TX, TY, false, EMIT><<<nb, TX * TY, sm, s>>>(P, A);
+    }
+}
+
+// Launch one fused step with candidate `cfg` (EMIT always uses candidate 0).
+inline cudaError_t fused_launch_cfg(const FusedConfig& fc, int cfg, const Params& P, FusedArgs A, bool f_on, bool g_on,
+                                    bool emit, cudaStream_t s) {
+    if (emit) cfg = 0;
+    apply_geom(A, fc.geom[cfg]);
+    const int nb = fc.geom[cfg].nblocks;
+    const bool bc = fc.has_bc;
+    if (fc.lat == MPLB_D2Q9) {
+        if (emit) {
+            launch2_fg<32, 8, true>(f_on, g_on, bc, nb, P, A, s);
+        } else {
+            switch (cfg) {
+            case 0: launch2_fg<32, 8, false>(f_on, g_on, bc, nb, P, A, s); break;
+            case 1: launch2_fg<32, 4, false>(f_on, g_on, bc, nb, P, A, s); break;
+            case 2: launch2_fg<64, 4, false>(f_on, g_on, bc, nb, P, A, s); break;
+            case 3: launch2_fg<16, 8, false>(f_on, g_on, bc, nb, P, A, s); break;
+            default: launch2_fg<32, 16, false>(f_on, g_on, bc, nb, P, A, s); break;
+            }
+        }
+    } else {
+        if (emit) {
+            launch3<32, 8, false, true>(bc, nb, P, A, s);
+        } else {
+            switch (cfg) {
+            case 0: launch3<32, 8, false, false>(bc, nb, P, A, s); break;
+            case 1: launch3<32, 8, true, false>(bc, nb, P, A, s); break;
+            case 2: launch3<32, 4, false, false>(bc, nb, P, A, s); break;
+            case 3: launch3<64, 4, false, false>(bc, nb, P, A, s); break;
+            case 4: launch3<32, 16, false, false>(bc, nb, P, A, s); break;
+            default: launch3<64, 8, false, false>(bc, nb, P, A, s); break;
+            }
+        }
+    }
+    return cudaGetLastError();
+}
+
+inline cudaError_t fused_launch(const FusedConfig& fc, const Params& P, const FusedArgs& A, int lat, bool f_on,
+                                bool g_on, bool emit, cudaStream_t s) {
+    (void)lat;
+    return fused_launch_cfg(fc, fc.cfg, P, A, f_on, g_on, emit, s);
+}
+
+// Time every candidate on the current state (2 warm-up + 3 timed launches)
+// and keep the fastest.  The step's outputs are rewritten by the real launch
+// that follows; the heat-source history S, updated in place, is saved to
+// `save` before and restored after every trial.
+inline int fused_autotune(FusedConfig& fc, const Params& P, const FusedArgs& A, bool f_on, bool g_on, double* S,
+                          double* save, size_t n, cudaStream_t s) {
+    cudaEvent_t e0, e1;
+    if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess) {
+        fc.err = "autotune: event creation failed";
+        return MPLB_E_CUDA;
+    }
+    const bool keep_s = g_on && S && save;
+    if (keep_s && cudaMemcpyAsync(save, S, n * sizeof(double), cudaMemcpyDeviceToDevice, s) != cudaSuccess) {
+        fc.err = "autotune: saving S failed";
+        return MPLB_E_CUDA;
+    }
+    float best = 1e30f;
+    int best_cfg = 0;
+    for (int c = 0; c < fc.ncfg; c++) {
+        float tot = 0;
+        bool ok = true;
+        for (int r = 0; r < 5 && ok; r++) {
+            if (r >= 2) cudaEventRecord(e0, s);
+            ok = fused_launch_cfg(fc, c, P, A, f_on, g_on, false, s) == cudaSuccess;
+            if (r >= 2) {
+                cudaEventRecord(e1, s);
+                cudaEventSynchronize(e1);
+                float ms = 0;
+                cudaEventElapsedTime(&ms, e0, e1);
+                tot += ms;
+            }
+            if (keep_s) cudaMemcpyAsync(S, save, n * sizeof(double), cudaMemcpyDeviceToDevice, s);
+        }
+        fc.tune_ms[c] = ok ? tot / 3 : -1.0f;
+        if (ok && tot < best) {
+            best = tot;
+            best_cfg = c;
+        }
+    }
+    cudaGetLastError();
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    fc.cfg = best_cfg;
+    fc.nblocks = fc.geom[best_cfg].nblocks;
+    fc.tuned = true;
+    return cudaStreamSynchronize(s) == cudaSuccess ? 0 : MPLB_E_CUDA;
+}
+
+// Fused path preconditions: box mesh, no serial boundary dependence, only
+// bounceBack / fixedT / periodic patches, at most FUSED_MAX_OPS ops per node
+// and field, at most FUSED_MAX_PROGS distinct node programs.
+inline bool fused_supported(int lat, const int* model, const Params& P, const std::vector<PatchDev>* fp,
+                            const bool* serial, const mplb_mesh_desc* mesh, const int* dims, const int* per,
+                            std::string& why) {
+    (void)per;
+    const bool active[2] = {model[0] != MPLB_NO_MODEL && P.f_update != 0, model[1] != MPLB_NO_MODEL && P.g_update != 0};
+    if (serial[0] || serial[1]) { why = "boundary updates depend on the serial order"; return false; }
+    if (!active[0] && !active[1]) { why = "no field is updated"; return false; }
+    if (!active[0] && model[0] == MPLB_NO_MODEL) { why = "no flow field"; return false; }
+    if (lat == MPLB_D3Q15 && active[1]) { why = "thermal field on D3Q15"; return false; }
+    for (int fi = 0; fi < 2; fi++) {
+        if (!active[fi]) continue;
+        for (const PatchDev& pt : fp[fi]) {
+            if (pt.type == MPLB_BC_PERIODIC) continue;
+            if (pt.type == MPLB_BC_BOUNCEBACK) continue;
+            if (pt.type == MPLB_BC_FIXEDT && fi == 1) continue;
+            if (pt.type == MPLB_BC_FIXEDU && model[fi] != MPLB_LIMRT) continue;  // no-op
+            why = "boundary type " + std::to_string(pt.type) + " is handled by the operator path only";
+            return false;
+        }
+    }
+    if (dims[0] < 2 || dims[1] < 2 || (lat == MPLB_D3Q15 && dims[2] < 2)) { why = "box thinner than 2 nodes"; return false; }
+    (void)mesh;
+    return true;
+}
+
+inline int fused_setup(FusedConfig& fc, int lat, const int* model, const Params& P, const std::vector<PatchDev>* fp,
+                       const mplb_mesh_desc* mesh, const int* dims, const int* per, cudaStream_t stream,
+                       uint64_t* bytes) {
+    (void)model;
+    FusedArgs& A = fc.args;
+    A.nx = dims[0];
+    A.ny = dims[1];
+    A.nz = lat == MPLB_D3Q15 ? dims[2] : 1;
+    A.px = per[0];
+    A.py = per[1];
+    A.pz = lat == MPLB_D3Q15 ? per[2] : 1;
+    // Node programs: for every node, the ops of every patch holding it, in
+    // patch order, per field.  Identical programs share one table entry.
+    const uint32_t n = P.n;
+    std::vector<uint8_t> map(n, 0);
+    std::vector<BCProg> progs(1, BCProg{});
+    std::vector<BCProg> per_node;
+    bool any = false;
+    {
+        std::vector<BCProg> node(n, BCProg{});
+        size_t off = 0;
+        for (size_t p = 0; p < fp[0].size(); p++) {
+            for (uint32_t i = 0; i < fp[0][p].count; i++) {
+                uint32_t id = mesh->patch_nodes[off + i];
+                for (int fi = 0; fi < 2; fi++) {
+                    if (!(fi == 0 ? P.f_update : P.g_update)) continue;
+                    int t = fp[fi][p].type;
+                    if (t != MPLB_BC_BOUNCEBACK && t != MPLB_BC_FIXEDT) continue;
+                    BCProg& b = node[id];
+                    if (fi == 0) {
+                        if (b.nf >= FUSED_MAX_OPS) { fc.err = "too many boundary ops on one node"; return MPLB_E_UNSUPPORTED; }
+                        b.ft[b.nf++] = (uint8_t)t;
+                    } else {
+                        if (b.ng >= FUSED_MAX_OPS) { fc.err = "too many boundary ops on one node"; return MPLB_E_UNSUPPORTED; }
+                        b.gp[b.ng] = (uint8_t)p;
+                        b.gt[b.ng++] = (uint8_t)t;
+                    }
+                    any = true;
+                }
+            }
+            off += fp[0][p].count;
+        }
+        for (uint32_t id = 0; id < n; id++) {
+            const BCProg& b = node[id];
+            if (b.nf == 0 && b.ng == 0) continue;
+            int found = -1;
+            for (size_t q = 1; q < progs.size(); q++)
+                if (std::memcmp(&progs[q], &b, sizeof(BCProg)) == 0) { found = (int)q; break; }
+            if (found < 0) {
+                if (progs.size() >= FUSED_MAX_PROGS) { fc.err = "too many distinct boundary programs"; return MPLB_E_UNSUPPORTED; }
+                progs.push_back(b);
+                found = (int)progs.size() - 1;
+            }
+            map[id] = (uint8_t)found;
+        }
+    }
+    for (size_t q = 0; q < progs.size(); q++) A.prog[q] = progs[q];
+    for (size_t p = 0; p < fp[1].size() && p < MPLB_MAX_PATCHES; p++) A.Twall[p] = fp[1][p].val[0];
+    fc.has_bc = any;
+    if (any) {
+        if (cudaMalloc((void**)&fc.bcmap, n) != cudaSuccess) { fc.err = "cudaMalloc bcmap"; return MPLB_E_CUDA; }
+        if (cudaMemcpyAsync(fc.bcmap, map.data(), n, cudaMemcpyHostToDevice, stream) != cudaSuccess) {
+            fc.err = "copy bcmap";
+            return MPLB_E_CUDA;
+        }
+        if (cudaStreamSynchronize(stream) != cudaSuccess) { fc.err = "copy bcmap"; return MPLB_E_CUDA; }
+        *bytes += n;
+    }
+    A.bcmap = fc.bcmap;
+    fc.lat = lat;
+    fc.ncfg = lat == MPLB_D2Q9 ? N_CFG2 : N_CFG3;
+    for (int c = 0; c < fc.ncfg; c++) {
+        const TileCfg t = lat == MPLB_D2Q9 ? CFG2[c] : CFG3[c];
+        fc.geom[c] = fused_geometry(lat, A, t.tx, t.ty);
+    }
+    fc.cfg = 0;
+    apply_geom(A, fc.geom[0]);
+    fc.nblocks = fc.geom[0].nblocks;
+    if (lat == MPLB_D3Q15 && fused_attributes() != cudaSuccess) {
+        fc.err = "cannot raise the dynamic shared memory limit";
+        return MPLB_E_CUDA;
+    }
+    return 0;
+}
+
+inline void fused_free(FusedConfig& fc) {
+    if (fc.bcmap) cudaFree(fc.bcmap);
+    fc.bcmap = nullptr;
+}
+
+
+}  // namespace mplb

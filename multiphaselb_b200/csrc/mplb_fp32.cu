@@ -1,0 +1,290 @@
+// mplb_fp32.cu -- fused box kernels of the FP32-deviation form (fused32.cuh).
+// Compiled with -fmad=true: this path is measured against FP64, not bitwise.
+#include <cuda_runtime.h>
+
+#include "fused32.cuh"
+
+namespace mplb {
+
+// ------------------------------------------------------------- 2D kernel
+template <int TX, int TY, bool F_ON, bool G_ON, bool HAS_BC, bool EMIT>
+__global__ void __launch_bounds__(TX * TY, min_blocks(TX * TY))
+    k_fused32_d2q9(Params P, FusedArgs32 A, double* emit_f, double* emit_g, double* rho_out, double* Fi_out,
+                   double* Ft_out) {
+    using L = D2Q9T;
+    constexpr int EX = TX + 2, EY = TY + 2, NRING = 2 * EX + 2 * TY;
+    constexpr int GY = G_ON ? EY : 1, GX = G_ON ? EX : 1;
+    __shared__ double s_psi[EY][EX];
+    __shared__ double s_inv[GY][GX];
+    __shared__ double s_To[GY][GX];
+    __shared__ double s_U0[GY][GX];
+    __shared__ double s_U1[GY][GX];
+    const uint32_t n = P.n;
+    const int tx = threadIdx.x % TX, ty = threadIdx.x / TX;
+    const int bx = blockIdx.x % A.tiles_x, by = blockIdx.x / A.tiles_x;
+    const int x0 = bx * TX, y0 = by * TY;
+
+    auto slot = [&](int ex, int ey, float* f, float* g, double& rho, double& T, float& dr, float& dT, uint32_t& id,
+                    bool mine, double& rr, EosRho& er) -> bool {
+        const int x = slot_coord(x0, ex, A.nx, A.px);
+        const int y = slot_coord(y0, ey, A.ny, A.py);
+        if (x < 0 || y < 0) return false;
+        id = (uint32_t)x + (uint32_t)A.nx * (uint32_t)y;
+        pull_node32<L, F_ON, G_ON, HAS_BC>(P, A, x, y, 0, id, f, g, rho, T, dr, dT);
+        if (mine) {
+            rr = rcp_rn(rho);
+            er = eos_rho(P, rho);
+            if constexpr (F_ON) s_psi[ey][ex] = potential_p(P, rho, p_eos_at(P, er, rho, T));
+            if constexpr (G_ON) s_inv[ey][ex] = rr;
+        } else {
+            if constexpr (F_ON) s_psi[ey][ex] = potential(P, rho, T);
+            if constexpr (G_ON) s_inv[ey][ex] = 1.0 / rho;
+        }
+        if constexpr (G_ON) {
+            s_To[ey][ex] = A.Told[id];
+            s_U0[ey][ex] = A.Uold[id];
+            s_U1[ey][ex] = A.Uold[n + id];
+        }
+        return true;
+    };
+    for (int r = threadIdx.x; r < NRING; r += blockDim.x) {
+        int ex, ey;
+        ring_slot(r, TX, TY, ex, ey);
+        float rf[9], rg[9], rdr, rdt;
+        double rrho, rt, rrr;
+        EosRho rer;
+        uint32_t rid;
+        slot(ex, ey, rf, rg, rrho, rt, rdr, rdt, rid, false, rrr, rer);
+    }
+    float f[9], g[9], dr = 0.f, dT = 0.f;
+    double rho = 0, T = 0, rr = 0;
+    EosRho er{};
+    uint32_t id = 0;
+    const int gx = x0 + tx, gy = y0 + ty;
+    const bool own = gx < A.nx && gy < A.ny;
+    const bool have = slot(tx + 1, ty + 1, f, g, rho, T, dr, dT, id, own, rr, er);
+    __syncthreads();
+    if (!own || !have) return;
+
+    const int ex = tx + 1, ey = ty + 1;
+    FusedArgs Gm{};
+    Gm.nx = A.nx; Gm.ny = A.ny; Gm.nz = 1; Gm.px = A.px; Gm.py = A.py; Gm.pz = 1;
+    const bool onb = on_wall(Gm, gx, gy, 0);
+    double heat = 0;
+    if constexpr (G_ON && !EMIT) {
+        double gT[3] = {0, 0, 0}, gR[3] = {0, 0, 0}, div = 0;
+        const double To = s_To[ey][ex], iv = s_inv[ey][ex];
+        {
+            const bool a = wrap1(gx + 1, A.nx, A.px) >= 0, b = wrap1(gx - 1, A.nx, A.px) >= 0;
+            FD t = fd_pair(a ? 0 : -1, b ? 0 : -1, s_To[ey][ex + 1], s_To[ey][ex - 1], To);
+            FD r = fd_pair(a ? 0 : -1, b ? 0 : -1, s_inv[ey][ex + 1], s_inv[ey][ex - 1], iv);
+            FD u = fd_pair(a ? 0 : -1, b ? 0 : -1, s_U0[ey][ex + 1], s_U0[ey][ex - 1], s_U0[ey][ex]);
+            gT[0] = t.v;
+            gR[0] = r.v;
+            if (u.present) div += u.v;
+        }
+        {
+            const bool a = wrap1(gy + 1, A.ny, A.py) >= 0, b = wrap1(gy - 1, A.ny, A.py) >= 0;
+            FD t = fd_pair(a ? 0 : -1, b ? 0 : -1, s_To[ey + 1][ex], s_To[ey - 1][ex], To);
+            FD r = fd_pair(a ? 0 : -1, b ? 0 : -1, s_inv[ey + 1][ex], s_inv[ey - 1][ex], iv);
+            FD u = fd_pair(a ? 0 : -1, b ? 0 : -1, s_U1[ey + 1][ex], s_U1[ey - 1][ex], s_U1[ey][ex]);
+            gT[1] = t.v;
+            gR[1] = r.v;
+            if (u.present) div += u.v;
+        }
+        const double dot = gT[0] * gR[0] + gT[1] * gR[1] + gT[2] * gR[2];
+        heat = heat_source_value_er(P, er, rho, rr, To, dot, div, A.S[id]);
+    }
+    const double psi = F_ON ? s_psi[ey][ex] : 0.0;
+    auto nbpsi = [&](int k) { return s_psi[ey + cyk<L>(k)][ex + cxk<L>(k)]; };
+    finish_node32<L, F_ON, G_ON, EMIT>(P, A, id, onb, f, g, rho, dr, T, dT, psi, nbpsi, heat, emit_f, emit_g,
+                                       rho_out, Fi_out, Ft_out);
+}
+
+// ------------------------------------------------------------- 3D kernel
+template <int TX, int TY>
+constexpr size_t f3_smem32() {
+    return (size_t)3 * (TY + 2) * (TX + 2) * sizeof(double) + (size_t)2 * 15 * TX * TY * sizeof(float);
+}
+
+template <int TX, int TY, bool HAS_BC, bool EMIT>
+__global__ void __launch_bounds__(TX * TY, min_blocks(TX * TY))
+    k_fused32_d3q15(Params P, FusedArgs32 A, double* emit_f, double* rho_out, double* Fi_out, double* Ft_out) {
+    using L = D3Q15T;
+    constexpr int EX = TX + 2, EY = TY + 2, NT = TX * TY, NRING = 2 * EX + 2 * TY;
+    extern __shared__ double dsm[];
+    double(*s_psi)[EY][EX] = reinterpret_cast<double(*)[EY][EX]>(dsm);
+    float* s_f = reinterpret_cast<float*>(dsm + 3 * EY * EX);  // [2][15][NT]
+    const int tid = threadIdx.x;
+    const int tx = tid % TX, ty = tid / TX;
+    const int tiles = A.tiles_x * A.tiles_y;
+    const int col = blockIdx.x % tiles, chunk = blockIdx.x / tiles;
+    const int bx = col % A.tiles_x, by = col / A.tiles_x;
+    const int x0 = bx * TX, y0 = by * TY;
+    const int z0 = chunk * A.zchunk;
+    const int z1 = min(z0 + A.zchunk, A.nz);
+    const int ox = slot_coord(x0, tx + 1, A.nx, A.px), oy = slot_coord(y0, ty + 1, A.ny, A.py);
+    const bool own_xy = (x0 + tx) < A.nx && (y0 + ty) < A.ny;
+    FusedArgs Gm{};
+    Gm.nx = A.nx; Gm.ny = A.ny; Gm.nz = A.nz; Gm.px = A.px; Gm.py = A.py; Gm.pz = A.pz;
+
+    auto plane = [&](int z, int buf, double& rho, float& dr, double& T, uint32_t& id) -> bool {
+        const int zs = slot_coord(z, 1, A.nz, A.pz);
+        float g_unused[1];
+        float dT_unused;
+        for (int r = tid; r < NRING; r += NT) {
+            int ex, ey;
+            ring_slot(r, TX, TY, ex, ey);
+            const int x = slot_coord(x0, ex, A.nx, A.px);
+            const int y = slot_coord(y0, ey, A.ny, A.py);
+            if (x < 0 || y < 0 || zs < 0) continue;
+            const uint32_t rid = (uint32_t)x + (uint32_t)A.nx * ((uint32_t)y + (uint32_t)A.ny * (uint32_t)zs);
+            float rf[15], rdr;
+            double rrho, rt;
+            pull_node32<L, true, false, HAS_BC>(P, A, x, y, zs, rid, rf, g_unused, rrho, rt, rdr, dT_unused);
+            s_psi[(z + 3) % 3][ey][ex] = potential(P, rrho, rt);
+        }
+        if (ox < 0 || oy < 0 || zs < 0) return false;
+        id = (uint32_t)ox + (uint32_t)A.nx * ((uint32_t)oy + (uint32_t)A.ny * (uint32_t)zs);
+        float f[15];
+        pull_node32<L, true, false, HAS_BC>(P, A, ox, oy, zs, id, f, g_unused, rho, T, dr, dT_unused);
+        s_psi[(z + 3) % 3][ty + 1][tx + 1] = potential(P, rho, T);
+#pragma unroll
+        for (int k = 0; k < 15; k++) s_f[(buf * 15 + k) * NT + tid] = f[k];
+        return true;
+    };
+
+    double rc = 0, Tc = 0, rn = 0, Tn = 0;
+    float drc = 0.f, drn = 0.f;
+    uint32_t idc = 0, idn = 0;
+    {
+        double a, b;
+        float c;
+        uint32_t d;
+        plane(z0 - 1, 1, a, c, b, d);
+    }
+    bool hc = plane(z0, z0 & 1, rc, drc, Tc, idc);
+    for (int z = z0; z < z1; z++) {
+        const bool hn = plane(z + 1, (z + 1) & 1, rn, drn, Tn, idn);
+        __syncthreads();
+        if (own_xy && hc) {
+            const bool onb = on_wall(Gm, ox, oy, z);
+            const int ex = tx + 1, ey = ty + 1;
+            float f[15], dum[1];
+#pragma unroll
+            for (int k = 0; k < 15; k++) f[k] = s_f[((z & 1) * 15 + k) * NT + tid];
+            auto nbpsi = [&](int k) { return s_psi[(z + czk<L>(k) + 3) % 3][ey + cyk<L>(k)][ex + cxk<L>(k)]; };
+            finish_node32<L, true, false, EMIT>(P, A, idc, onb, f, dum, rc, drc, Tc, 0.f, s_psi[(z + 3) % 3][ey][ex],
+                                                nbpsi, 0.0, emit_f, nullptr, rho_out, Fi_out, Ft_out);
+        }
+        __syncthreads();
+        rc = rn;
+        drc = drn;
+        Tc = Tn;
+        idc = idn;
+        hc = hn;
+    }
+}
+
+template <int TX, int TY, bool BC, bool EMIT>
+static cudaError_t set32() {
+    return cudaFuncSetAttribute(k_fused32_d3q15<TX, TY, BC, EMIT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)f3_smem32<TX, TY>());
+}
+
+}  // namespace mplb
+
+using namespace mplb;
+
+// FP32 constants and deviation weights from the FP64 parameter block.
+FusedArgs32 mplb_make_args32(const FusedArgs& A, const Params& P, double rho_ref, double T_ref) {
+    FusedArgs32 B{};
+    B.nx = A.nx; B.ny = A.ny; B.nz = A.nz; B.px = A.px; B.py = A.py; B.pz = A.pz;
+    B.bcmap = A.bcmap;
+    for (int p = 0; p < MPLB_MAX_PATCHES; p++) B.Twall[p] = A.Twall[p];
+    for (int q = 0; q < FUSED_MAX_PROGS; q++) B.prog[q] = A.prog[q];
+    B.rho_ref = rho_ref;
+    B.T_ref = T_ref;
+    for (int k = 0; k < MPLB_MAX_Q; k++) {
+        B.wf[k] = (float)P.w[k];
+        B.Lf[k] = (float)P.Lf[k];
+        B.relax_f[k] = (float)P.relax_f[k];
+    }
+    for (int k = 0; k < 9; k++) {
+        B.Lg[k] = (float)P.Lg[k];
+        // rest state of liTempMRT: M^-1 (1, -2, 2, 0, ...)
+        B.wg[k] = (float)(P.Mi[k][0] - 2.0 * P.Mi[k][1] + 2.0 * P.Mi[k][2]);
+    }
+    B.s1_den = (float)P.s1_den;
+    B.s2_den = (float)P.s2_den;
+    B.sig12 = (float)P.sig12;
+    B.sig6 = (float)P.sig6;
+    B.corr3 = (float)P.corr3;
+    B.corr5 = (float)P.corr5;
+    return B;
+}
+
+int mplb_fused32_attributes() {
+    cudaError_t e = cudaSuccess;
+    auto chk = [&](cudaError_t r) { if (e == cudaSuccess) e = r; };
+    chk(set32<32, 8, true, true>());
+    chk(set32<32, 8, false, true>());
+    chk(set32<32, 4, true, false>());
+    chk(set32<32, 4, false, false>());
+    return e == cudaSuccess ? 0 : -1;
+}
+
+// One FP32-deviation fused step (EMIT: rebuild the FP64 reference state).
+cudaError_t mplb_fused32_launch(int lat, bool has_bc, bool f_on, bool g_on, bool emit, FusedArgs32 B,
+                                const Params& P, double* emit_f, double* emit_g, double* rho_out, double* Fi_out,
+                                double* Ft_out, cudaStream_t s) {
+    if (lat == MPLB_D2Q9) {
+        FusedArgs tmp{};
+        tmp.nx = B.nx; tmp.ny = B.ny; tmp.nz = 1;
+        const Geom g = fused_geometry(MPLB_D2Q9, tmp, 32, 8);
+        B.tiles_x = g.tiles_x;
+        B.tiles_y = g.tiles_y;
+        B.zchunk = 1;
+#define MPLB_L32(F, G, BC, E) k_fused32_d2q9<32, 8, F, G, BC, E><<<g.nblocks, 256, 0, s>>>(P, B, emit_f, emit_g, rho_out, Fi_out, Ft_out)
+#define MPLB_L32_E(F, G, BC) (emit ? (MPLB_L32(F, G, BC, true), 0) : (MPLB_L32(F, G, BC, false), 0))
+#define MPLB_L32_B(F, G) (has_bc ? MPLB_L32_E(F, G, true) : MPLB_L32_E(F, G, false))
+        if (f_on && g_on) MPLB_L32_B(true, true);
+        else if (f_on) MPLB_L32_B(true, false);
+        else if (g_on) MPLB_L32_B(false, true);
+#undef MPLB_L32
+#undef MPLB_L32_E
+#undef MPLB_L32_B
+    } else {
+        FusedArgs tmp{};
+        tmp.nx = B.nx; tmp.ny = B.ny; tmp.nz = B.nz;
+        if (emit) {
+            const Geom g = fused_geometry(MPLB_D3Q15, tmp, 32, 8);
+            B.tiles_x = g.tiles_x; B.tiles_y = g.tiles_y; B.zchunk = g.zchunk;
+            if (has_bc) k_fused32_d3q15<32, 8, true, true><<<g.nblocks, 256, f3_smem32<32, 8>(), s>>>(P, B, emit_f, rho_out, Fi_out, Ft_out);
+            else k_fused32_d3q15<32, 8, false, true><<<g.nblocks, 256, f3_smem32<32, 8>(), s>>>(P, B, emit_f, rho_out, Fi_out, Ft_out);
+        } else {
+            const Geom g = fused_geometry(MPLB_D3Q15, tmp, 32, 4);
+            B.tiles_x = g.tiles_x; B.tiles_y = g.tiles_y; B.zchunk = g.zchunk;
+            if (has_bc) k_fused32_d3q15<32, 4, true, false><<<g.nblocks, 128, f3_smem32<32, 4>(), s>>>(P, B, emit_f, rho_out, Fi_out, Ft_out);
+            else k_fused32_d3q15<32, 4, false, false><<<g.nblocks, 128, f3_smem32<32, 4>(), s>>>(P, B, emit_f, rho_out, Fi_out, Ft_out);
+        }
+    }
+    return cudaGetLastError();
+}
+
+// FP64 post-collision populations -> FP32 deviations (after the prologue).
+__global__ void k_to_dev32(uint32_t n, int Q, const double* __restrict__ src, float* __restrict__ dst, FusedArgs32 B,
+                           int heat) {
+    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= (size_t)n * Q) return;
+    const int k = (int)(i / n);
+    const double ref = heat ? (double)B.wg[k] * B.T_ref : (double)B.wf[k] * B.rho_ref;
+    dst[i] = (float)(src[i] - ref);
+}
+
+cudaError_t mplb_to_dev32(uint32_t n, int Q, const double* src, float* dst, const FusedArgs32& B, int heat,
+                          cudaStream_t s) {
+    const size_t tot = (size_t)n * Q;
+    k_to_dev32<<<(unsigned)((tot + 255) / 256), 256, 0, s>>>(n, Q, src, dst, B, heat);
+    return cudaGetLastError();
+}

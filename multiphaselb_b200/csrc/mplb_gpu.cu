@@ -15,9 +15,19 @@
 #include <vector>
 
 #include "ops.cuh"
-#include "fused.cuh"
+#include "fused_host.cuh"
+#include "fused32.cuh"
 
 using namespace mplb;
+
+// FP32-deviation kernels (mplb_fp32.cu, compiled with contraction on).
+FusedArgs32 mplb_make_args32(const FusedArgs& A, const Params& P, double rho_ref, double T_ref);
+int mplb_fused32_attributes();
+cudaError_t mplb_fused32_launch(int lat, bool has_bc, bool f_on, bool g_on, bool emit, FusedArgs32 B, const Params& P,
+                                double* emit_f, double* emit_g, double* rho_out, double* Fi_out, double* Ft_out,
+                                cudaStream_t s);
+cudaError_t mplb_to_dev32(uint32_t n, int Q, const double* src, float* dst, const FusedArgs32& B, int heat,
+                          cudaStream_t s);
 
 namespace {
 
@@ -76,6 +86,10 @@ struct mplb_gpu {
     int red_parts = 0;
     FusedConfig fc{};
     int fstate = 0;  // 0: buffers hold the reference's state; 1: post-collision (fused)
+    int precision = MPLB_FP64;
+    float* p32[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};  // FP32 deviations [field][buffer]
+    int cur32[2] = {0, 0};
+    double rho_ref = 0, T_ref = 0;
     int tile_request = 0;  // mplb_opts.tile_config
     uint32_t current = 0;
     uint64_t launches = 0;
@@ -103,6 +117,9 @@ void free_all(mplb_gpu* h) {
                   h->red};
     for (void* p : ps)
         if (p) cudaFree(p);
+    for (int i = 0; i < 2; i++)
+        for (int j = 0; j < 2; j++)
+            if (h->p32[i][j]) cudaFree(h->p32[i][j]);
 }
 
 // Lattice tables on the host, the same way the reference defines them
@@ -496,10 +513,73 @@ int fused_step(mplb_gpu* h, bool emit) {
     return 0;
 }
 
+// FP32-deviation step (or emit: rebuild the FP64 reference state).
+int fused32_step(mplb_gpu* h, bool emit) {
+    const bool fon = h->P.f_update != 0, gon = h->P.g_update != 0;
+    FusedArgs32 B = mplb_make_args32(h->fc.args, h->P, h->rho_ref, h->T_ref);
+    const int c0 = h->cur32[0], c1 = h->cur32[1];
+    if (fon) {
+        B.fin = emit ? h->p32[0][c0 ^ 1] : h->p32[0][c0];
+        B.fout = emit ? nullptr : h->p32[0][c0 ^ 1];
+    }
+    if (gon) {
+        B.gin = emit ? h->p32[1][c1 ^ 1] : h->p32[1][c1];
+        B.gout = emit ? nullptr : h->p32[1][c1 ^ 1];
+    }
+    const bool udb = fon && gon;
+    B.Told = gon ? (emit ? h->T2 : h->T) : h->T;
+    B.Tnew = gon ? (emit ? h->T : h->T2) : nullptr;
+    B.Uold = udb ? (emit ? h->U2 : h->U) : h->U;
+    B.Unew = udb ? (emit ? h->U : h->U2) : h->U;
+    B.S = h->S;
+    B.rho_c = h->rho;
+    cudaError_t e = mplb_fused32_launch(h->lat, h->fc.has_bc, fon, gon, emit, B, h->P, fon ? h->F() : nullptr,
+                                        gon ? h->G() : nullptr, h->rho, h->Fi, h->Ft, h->stream);
+    h->launches++;
+    if (e != cudaSuccess) return fail(MPLB_E_CUDA, std::string("FP32 fused kernel launch: ") + cudaGetErrorString(e));
+    if (!emit) {
+        if (fon) h->cur32[0] ^= 1;
+        if (gon) {
+            h->cur32[1] ^= 1;
+            std::swap(h->T, h->T2);
+        }
+        if (udb) std::swap(h->U, h->U2);
+    }
+    return 0;
+}
+
+// FP64 reference state -> FP32 post-collision deviations.  The reference
+// values are the lattice means of rho and T (any value is valid; the mean
+// keeps deviations small).
+int prologue32(mplb_gpu* h) {
+    const int parts = std::min<int>(h->red_parts, (int)blocks(h->n));
+    k_sum2_partial<<<parts, TPB, 0, h->stream>>>(h->n, h->rho, h->T, h->red);
+    k_sum2_final<<<1, TPB, 0, h->stream>>>(parts, h->red, h->red + 2 * h->red_parts);
+    h->launches += 2;
+    RET(launch_check(h));
+    double r[2] = {0, 0};
+    CK(cudaMemcpyAsync(r, h->red + 2 * h->red_parts, 2 * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    h->rho_ref = r[0] / h->n;
+    h->T_ref = r[1] / h->n;
+    RET(DISPATCH(h, op_collision, h, 0));
+    RET(DISPATCH(h, op_collision, h, 1));
+    FusedArgs32 B = mplb_make_args32(h->fc.args, h->P, h->rho_ref, h->T_ref);
+    for (int fi = 0; fi < 2; fi++) {
+        if (!(fi == 0 ? h->P.f_update : h->P.g_update)) continue;
+        cudaError_t e = mplb_to_dev32(h->n, h->Q, h->pdf[fi][h->cur[fi]], h->p32[fi][h->cur32[fi]], B, fi, h->stream);
+        h->launches++;
+        if (e != cudaSuccess) return fail(MPLB_E_CUDA, std::string("FP32 conversion: ") + cudaGetErrorString(e));
+    }
+    h->fstate = 1;
+    return 0;
+}
+
 // Bring the buffers back to the reference's state (after the last step).
 int materialize(mplb_gpu* h) {
     if (h->fstate == 0) return 0;
-    RET(fused_step(h, true));
+    if (h->precision == MPLB_FP32_DEV) RET(fused32_step(h, true));
+    else RET(fused_step(h, true));
     h->fstate = 0;
     return 0;
 }
@@ -525,7 +605,8 @@ int mplb_gpu_create(const mplb_mesh_desc* mesh, const mplb_eos_desc* eos, const 
     if (mesh->n_patches > MPLB_MAX_PATCHES) return fail(MPLB_E_ARG, "too many boundary patches");
     if (mesh->n_patches && (!mesh->patch_count || !mesh->patch_nodes)) return fail(MPLB_E_ARG, "patch lists missing");
     if (eos->type < MPLB_EOS_IDEAL || eos->type > MPLB_EOS_VDW) return fail(MPLB_E_ARG, "unknown EOS");
-    if (opts && opts->precision != MPLB_FP64) return fail(MPLB_E_UNSUPPORTED, "only FP64 storage is built");
+    if (opts && opts->precision != MPLB_FP64 && opts->precision != MPLB_FP32_DEV)
+        return fail(MPLB_E_ARG, "unknown precision");
     const int Q = mesh->lattice == MPLB_D2Q9 ? 9 : 15;
     const size_t nq = (size_t)mesh->n_points * Q;
     for (size_t i = 0; i < nq; i++)
@@ -546,6 +627,7 @@ int mplb_gpu_create(const mplb_mesh_desc* mesh, const mplb_eos_desc* eos, const 
     h->n = mesh->n_points;
     h->current = opts ? opts->start_time : 0;
     h->tile_request = opts ? opts->tile_config : 0;
+    h->precision = opts ? opts->precision : MPLB_FP64;
     int want_path = opts ? opts->path : MPLB_PATH_AUTO;
     int dev = opts ? opts->device : -1;
     if (dev < 0) {
@@ -674,12 +756,23 @@ int mplb_gpu_create(const mplb_mesh_desc* mesh, const mplb_eos_desc* eos, const 
     // Execution path.
     std::string fwhy;
     bool fusable = h->box && fused_supported(h->lat, h->model, h->P, h->fpatch, h->serial, mesh, h->dims, h->per, fwhy);
-    if (want_path == MPLB_PATH_FUSED && !fusable) return bail(fail(MPLB_E_UNSUPPORTED, "fused path unavailable: " + (h->box ? fwhy : std::string("mesh is not a box"))));
+    if ((want_path == MPLB_PATH_FUSED || h->precision == MPLB_FP32_DEV) && !fusable)
+        return bail(fail(MPLB_E_UNSUPPORTED, std::string(h->precision == MPLB_FP32_DEV ? "FP32-deviation storage needs the fused box path; " : "") +
+                                                 "fused path unavailable: " + (h->box ? fwhy : std::string("mesh is not a box"))));
+    if (h->precision == MPLB_FP32_DEV && want_path == MPLB_PATH_OPERATORS)
+        return bail(fail(MPLB_E_UNSUPPORTED, "FP32-deviation storage runs on the fused path only"));
     h->path = (want_path == MPLB_PATH_OPERATORS || !fusable) ? MPLB_PATH_OPERATORS : MPLB_PATH_FUSED;
     if (h->path == MPLB_PATH_FUSED) {
         if ((rc = fused_setup(h->fc, h->lat, h->model, h->P, h->fpatch, mesh, h->dims, h->per, h->stream, &h->bytes)))
             return bail(fail(rc, "fused setup: " + h->fc.err));
         if ((rc = dalloc(h, &h->T2, h->n)) || (rc = dalloc(h, &h->U2, 3 * (size_t)h->n))) return bail(rc);
+        if (h->precision == MPLB_FP32_DEV) {
+            for (int fi = 0; fi < 2; fi++) {
+                if (h->model[fi] == MPLB_NO_MODEL) continue;
+                if ((rc = dalloc(h, &h->p32[fi][0], nq)) || (rc = dalloc(h, &h->p32[fi][1], nq))) return bail(rc);
+            }
+            if (mplb_fused32_attributes()) return bail(fail(MPLB_E_CUDA, "cannot raise the shared memory limit (FP32 kernels)"));
+        }
     }
     h->red_parts = 2 * 148;
     if ((rc = dalloc(h, &h->red, 2 * (size_t)h->red_parts + 8))) return bail(rc);
@@ -762,6 +855,12 @@ int mplb_gpu_step(mplb_gpu_t* h, uint32_t nsteps) {
     if (!h) return fail(MPLB_E_ARG, "NULL handle");
     if (nsteps == 0) return 0;
     DeviceGuard guard(h->dev);
+    if (h->path == MPLB_PATH_FUSED && h->precision == MPLB_FP32_DEV) {
+        if (h->fstate == 0) RET(prologue32(h));
+        for (uint32_t s = 0; s < nsteps; s++) RET(fused32_step(h, false));
+        h->current += nsteps;
+        return 0;
+    }
     if (h->path == MPLB_PATH_FUSED) {
         if (h->fstate == 0) {
             // prologue: the first collision of the loop, on the reference state

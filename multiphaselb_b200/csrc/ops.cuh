@@ -31,7 +31,7 @@ __global__ void k_equilibrium_flow(Params P, double* __restrict__ f, const doubl
 }
 
 // general/equilibrium.c:49-55 (liTempMRT)
-__global__ void k_equilibrium_heat(Params P, double* __restrict__ g, const double* __restrict__ T,
+static __global__ void k_equilibrium_heat(Params P, double* __restrict__ g, const double* __restrict__ T,
                                    const double* __restrict__ U) {
     uint32_t n = P.n, id = blockIdx.x * blockDim.x + threadIdx.x;
     if (id >= n) return;
@@ -65,7 +65,7 @@ __global__ void k_collide_flow(Params P, double* __restrict__ f, const double* _
 }
 
 // liTempMRTCollision.c:31-87 over all nodes.
-__global__ void k_collide_heat(Params P, double* __restrict__ g, const double* __restrict__ T,
+static __global__ void k_collide_heat(Params P, double* __restrict__ g, const double* __restrict__ T,
                                const double* __restrict__ U, const double* __restrict__ S) {
     uint32_t n = P.n, id = blockIdx.x * blockDim.x + threadIdx.x;
     if (id >= n) return;
@@ -308,14 +308,14 @@ __global__ void k_bc_serial(Params P, const PatchDev* __restrict__ pts, int npat
 
 // ----------------------------------------------------------------- layout
 // [n][m] host order <-> [m][n] device order.
-__global__ void k_aos_to_soa(uint32_t n, int m, const double* __restrict__ aos, double* __restrict__ soa) {
+static __global__ void k_aos_to_soa(uint32_t n, int m, const double* __restrict__ aos, double* __restrict__ soa) {
     size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= (size_t)n * m) return;
     uint32_t id = (uint32_t)(i / m);
     int j = (int)(i % m);
     soa[(size_t)j * n + id] = aos[i];
 }
-__global__ void k_soa_to_aos(uint32_t n, int m, const double* __restrict__ soa, double* __restrict__ aos) {
+static __global__ void k_soa_to_aos(uint32_t n, int m, const double* __restrict__ soa, double* __restrict__ aos) {
     size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= (size_t)n * m) return;
     uint32_t id = (uint32_t)(i / m);
@@ -325,7 +325,7 @@ __global__ void k_soa_to_aos(uint32_t n, int m, const double* __restrict__ soa, 
 
 // ------------------------------------------------------------- reductions
 // averageScalarField.c:28-32 order: one thread, node order.
-__global__ void k_sum_serial(uint32_t n, const double* __restrict__ x, double* __restrict__ out) {
+static __global__ void k_sum_serial(uint32_t n, const double* __restrict__ x, double* __restrict__ out) {
     if (blockIdx.x != 0 || threadIdx.x != 0) return;
     double s = 0;
     for (uint32_t i = 0; i < n; i++) s += x[i];
@@ -333,7 +333,7 @@ __global__ void k_sum_serial(uint32_t n, const double* __restrict__ x, double* _
 }
 
 // Block partial sums of two arrays with warp shuffles; partials[2*block+{0,1}].
-__global__ void k_sum2_partial(uint32_t n, const double* __restrict__ x, const double* __restrict__ y,
+static __global__ void k_sum2_partial(uint32_t n, const double* __restrict__ x, const double* __restrict__ y,
                                double* __restrict__ partials) {
     double a = 0, b = 0;
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
@@ -363,7 +363,7 @@ __global__ void k_sum2_partial(uint32_t n, const double* __restrict__ x, const d
 }
 
 // Final pass over the block partials (one block).
-__global__ void k_sum2_final(int nparts, const double* __restrict__ partials, double* __restrict__ out) {
+static __global__ void k_sum2_final(int nparts, const double* __restrict__ partials, double* __restrict__ out) {
     double a = 0, b = 0;
     for (int i = threadIdx.x; i < nparts; i += blockDim.x) {
         a += partials[2 * i];
