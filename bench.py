@@ -31,15 +31,17 @@ if ROOT not in sys.path:
 
 METRIC = "GLUPS on 1 B200 (FP64 vs FP32-dev); time-to-equilibrium w/ warm start"
 
-# Algorithmic bytes per lattice-node update (FP64): every population read
-# once and written once, plus per-node state that cannot be rebuilt from the
-# populations (the heat-source history S: read + write).
+# Algorithmic bytes per lattice-node update: every population read once and
+# written once, plus per-node state that cannot be rebuilt from the
+# populations (the heat-source history S: read + write, kept FP64).
+# bytes_per_lup: FP64 storage; bytes_per_lup32: FP32-deviation storage.
 WORKLOADS = {
-    "column_d2q9_128x512": dict(bytes_per_lup=304, desc="thermal VdW column, D2Q9, f+g, bounceBack+fixedT walls, periodic x",
+    "column_d2q9_128x512": dict(bytes_per_lup=304, bytes_per_lup32=160,
+                                desc="thermal VdW column, D2Q9, f+g, bounceBack+fixedT walls, periodic x",
                                 build=lambda c: c.column_case(128, 512)),
-    "bubble_d2q9_256": dict(bytes_per_lup=144, desc="static bubble, D2Q9 liMRT, fully periodic",
+    "bubble_d2q9_256": dict(bytes_per_lup=144, bytes_per_lup32=72, desc="static bubble, D2Q9 liMRT, fully periodic",
                             build=lambda c: c.bubble_case(0, 256, 40.0, 5.0, 0.8)),
-    "bubble_d3q15_192": dict(bytes_per_lup=240, desc="static bubble, D3Q15 xuMRT, fully periodic",
+    "bubble_d3q15_192": dict(bytes_per_lup=240, bytes_per_lup32=120, desc="static bubble, D3Q15 xuMRT, fully periodic",
                              build=lambda c: c.bubble_case(1, 192, 48.0, 5.0, 0.75)),
 }
 PROFILE_TRAFFIC = {  # per-launch DRAM bytes summaries committed under profiles/
@@ -211,44 +213,51 @@ def run_ours(a):
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)  # 256 MiB > 126 MB L2
     peak, peak_kind = peaks()
 
-    with torch.cuda.stream(stream):
-        lat = Lattice(case, path=path, device=local, stream=stream.cuda_stream)
-        lat.upload_case()
-        lat.initialize()
-        info0 = lat.info()
-        for _ in range(a.warmup):
-            lat.step(1)
-        torch.cuda.synchronize()
-        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(a.steps)]
-        barrier(world, dev)
-        torch.cuda.synchronize()
-        with ClockSampler(local) as clk:
-            time.sleep(0.3)
-            mark = clk.mark()
-            launches0 = lat.info()["kernel_launches"]
-            for i in range(a.steps):
-                flush.zero_()
-                ev[i][0].record(stream)
+    def timed(precision, steps):
+        """Warm-up, then `steps` steps each timed alone after an L2 flush;
+        then the same steps back to back (informational)."""
+        with torch.cuda.stream(stream):
+            lat = Lattice(case, path=path, device=local, stream=stream.cuda_stream, precision=precision)
+            lat.upload_case()
+            lat.initialize()
+            info0 = lat.info()
+            for _ in range(a.warmup):
                 lat.step(1)
-                ev[i][1].record(stream)
             torch.cuda.synchronize()
-            launches = lat.info()["kernel_launches"] - launches0
-            time.sleep(0.25)
-            clocks = clk.summary(mark)
-        # informational: the same steps back to back without the flush (the
-        # lattice then stays in L2, as in a long run of this size)
-        s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        s0.record(stream)
-        lat.step(a.steps)
-        s1.record(stream)
-        torch.cuda.synchronize()
-        steady_ms = s0.elapsed_time(s1) / a.steps
-        barrier(world, dev)
-        step_ms = [s.elapsed_time(e) for s, e in ev]
-        total_ms = max_over_ranks(sum(step_ms), world, dev)
-        kernel_ms = sum(step_ms) / len(step_ms)  # one fused launch per step
-        info = lat.info()
-        lat.close()
+            ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+            barrier(world, dev)
+            torch.cuda.synchronize()
+            with ClockSampler(local) as clk:
+                time.sleep(0.3)
+                mark = clk.mark()
+                launches0 = lat.info()["kernel_launches"]
+                for i in range(steps):
+                    flush.zero_()
+                    ev[i][0].record(stream)
+                    lat.step(1)
+                    ev[i][1].record(stream)
+                torch.cuda.synchronize()
+                launches = lat.info()["kernel_launches"] - launches0
+                time.sleep(0.25)
+                clocks = clk.summary(mark)
+            s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            s0.record(stream)
+            lat.step(steps)
+            s1.record(stream)
+            torch.cuda.synchronize()
+            steady_ms = s0.elapsed_time(s1) / steps
+            barrier(world, dev)
+            step_ms = [st.elapsed_time(en) for st, en in ev]
+            info = lat.info()
+            lat.close()
+        return dict(step_ms=step_ms, steady_ms=steady_ms, launches=launches, clocks=clocks, info=info, info0=info0)
+
+    from multiphaselb_b200 import abi
+    r64 = timed(abi.FP64, a.steps)
+    total_ms = max_over_ranks(sum(r64["step_ms"]), world, dev)
+    kernel_ms = sum(r64["step_ms"]) / len(r64["step_ms"])  # one fused launch per step
+    steady_ms, launches, clocks, info, info0 = r64["steady_ms"], r64["launches"], r64["clocks"], r64["info"], r64["info0"]
+    r32 = timed(abi.FP32_DEV, a.steps) if not a.no_fp32 else None
 
     # end to end through the C-ABI: pinned host fields -> device, steps, all fields back
     n, Q = case.n, case.Q
@@ -302,9 +311,18 @@ def run_ours(a):
                 "timed": f"upload rho/U/T from pinned host memory, initialize, {e2e_steps} steps, download every field"},
         "steady_state": {"ms_per_step": round(steady_ms, 6), "value": round(n / (steady_ms * 1e-3) / 1e9, 4),
                          "unit": "GLUPS", "note": "no L2 flush between steps (informational, not the headline)"},
+        "tile_config": info["tile_config"],
         "gpu_launches": int(launches),
         "clocks": clocks,
     }
+    if r32 is not None:
+        ms32 = max_over_ranks(sum(r32["step_ms"]), world, dev) / a.steps
+        ach32 = wl["bytes_per_lup32"] * n / (sum(r32["step_ms"]) / a.steps * 1e-3) / 1e9
+        line["fp32_dev"] = {"value": round(n * world / (ms32 * 1e-3) / 1e9, 4), "unit": "GLUPS",
+                            "ms_per_step": round(ms32, 6), "bytes_per_lup": wl["bytes_per_lup32"],
+                            "roofline_frac": round(ach32 / peak, 4),
+                            "steady_state_glups": round(n / (r32["steady_ms"] * 1e-3) / 1e9, 4),
+                            "note": "same workload, FP32-deviation storage (not bit-identical; error in DESIGN)"}
     if rank == 0 and world == 1 and not a.no_cpu:
         line["cpu_baseline"] = cpu_baseline(a.workload, a.cpu_steps, 1)
     if world > 1:
@@ -358,6 +376,7 @@ def main():
     ap.add_argument("--cpu-procs", type=int, default=0)
     ap.add_argument("--ref-repeats", type=int, default=1)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-fp32", action="store_true")
     a = ap.parse_args()
     if a.warmup < 3:
         ap.error("--warmup must be >= 3")

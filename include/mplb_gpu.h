@@ -192,6 +192,11 @@ int mplb_gpu_macro_velocity(mplb_gpu_t* h, uint32_t start, uint32_t end);   /* g
 int mplb_gpu_macro_temperature(mplb_gpu_t* h, uint32_t start, uint32_t end);/* general/macroTemperature.c:7-68 */
 int mplb_gpu_inter_force(mplb_gpu_t* h);                                /* pseudoPot/interForce.c:7-52 */
 int mplb_gpu_heat_source(mplb_gpu_t* h);                                /* general/heatSource.c:7-202 */
+/* Write-time pressure (multiPhasePP.c:264): macroPressure on the device
+ * (general/macroPressure.c:8-69, liMRTPressure.c:6-253, xuMRTPressure.c:6-22),
+ * then the field to the host ([n] doubles). */
+int mplb_gpu_macro_pressure(mplb_gpu_t* h);
+int mplb_gpu_download_pressure(mplb_gpu_t* h, double* p);
 
 /* Time and buoyancy reference density (timeInfo.current, EOSInfo.rho_0). */
 int mplb_gpu_set_time(mplb_gpu_t* h, uint32_t current);

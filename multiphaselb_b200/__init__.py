@@ -61,6 +61,8 @@ def load_library(path=LIB_PATH):
         "mplb_gpu_macro_temperature": ([H, C.c_uint32, C.c_uint32], C.c_int),
         "mplb_gpu_inter_force": ([H], C.c_int),
         "mplb_gpu_heat_source": ([H], C.c_int),
+        "mplb_gpu_macro_pressure": ([H], C.c_int),
+        "mplb_gpu_download_pressure": ([H, D], C.c_int),
         "mplb_gpu_set_time": ([H, C.c_uint32], C.c_int),
         "mplb_gpu_set_rho0": ([H, C.c_double], C.c_int),
         "mplb_gpu_average_rho0": ([H, D], C.c_int),
@@ -86,12 +88,13 @@ class Lattice:
     the same attributes: lattice, n, nb, points, patches, eos, f, g).
     """
 
-    def __init__(self, case, path=PATH_AUTO, device=-1, stream=None, start_time=0, tile_config=0):
+    def __init__(self, case, path=PATH_AUTO, device=-1, stream=None, start_time=0, tile_config=0,
+                 precision=abi.FP64):
         self.lib = load_library()
         self.case = case
         self.n, self.Q = case.n, case.Q
         self._desc = abi.Descriptors(case)
-        opts = abi.Opts(abi.FP64, path, device, stream, start_time, tile_config)
+        opts = abi.Opts(precision, path, device, stream, start_time, tile_config)
         h = C.c_void_p()
         self._check(self.lib.mplb_gpu_create(C.byref(self._desc.mesh), C.byref(self._desc.eos),
                                               C.byref(self._desc.f), C.byref(self._desc.g),
@@ -184,6 +187,13 @@ class Lattice:
 
     def heat_source(self):
         self._check(self.lib.mplb_gpu_heat_source(self.h))
+
+    def macro_pressure(self):
+        """macroPressure on the device; returns the pressure field."""
+        self._check(self.lib.mplb_gpu_macro_pressure(self.h))
+        p = np.zeros(self.n)
+        self._check(self.lib.mplb_gpu_download_pressure(self.h, abi.dptr(p)))
+        return p
 
     def set_time(self, t):
         self._check(self.lib.mplb_gpu_set_time(self.h, t))

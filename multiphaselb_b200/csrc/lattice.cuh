@@ -82,6 +82,7 @@ struct Params {
     double relax_f[MPLB_MAX_Q];  // (1 - 0.5*Lambda[k])            liMRTCollision.c:92
     double s1_den, s2_den;       // ((1/Lambda[1])-0.5), ((1/Lambda[2])-0.5)  liMRTForce.c:35-36
     double sig12, sig6;          // 12*sigma (liMRTForce.c:35), 6.0*sigma (xuMRTForce.c:43)
+    double sigma_p;              // sigma of the pressure's gradient term (liMRTPressure.c:246)
     // thermal field
     int32_t g_model, g_update;
     double Lg[MPLB_MAX_Q];

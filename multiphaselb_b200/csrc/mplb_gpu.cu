@@ -72,6 +72,7 @@ struct mplb_gpu {
     double* pdf[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};  // [field][buffer]
     int cur[2] = {0, 0};
     double *rho = nullptr, *T = nullptr, *S = nullptr, *U = nullptr, *Fi = nullptr, *Ft = nullptr;
+    double* p = nullptr;                  // pressure (write-time output)
     double *T2 = nullptr, *U2 = nullptr;  // fused-path double buffers
     uint8_t* bcmap = nullptr;             // fused-path per-node boundary-program index
     uint32_t* pnodes = nullptr;
@@ -112,7 +113,7 @@ int dalloc(mplb_gpu* h, T** p, size_t count) {
 }
 
 void free_all(mplb_gpu* h) {
-    void* ps[] = {h->nb, h->onb, h->pdf[0][0], h->pdf[0][1], h->pdf[1][0], h->pdf[1][1], h->rho, h->T,
+    void* ps[] = {h->p, h->nb, h->onb, h->pdf[0][0], h->pdf[0][1], h->pdf[1][0], h->pdf[1][1], h->rho, h->T,
                   h->S, h->U, h->Fi, h->Ft, h->T2, h->U2, h->bcmap, h->pnodes, h->dpatches, h->stage,
                   h->red};
     for (void* p : ps)
@@ -375,6 +376,13 @@ int op_heatsource(mplb_gpu* h) {
 }
 
 #define RET(x) do { if (int rc_ = (x)) return rc_; } while (0)
+
+template <class L>
+int op_pressure(mplb_gpu* h) {
+    if (!h->P.f_update) return 0;
+    LAUNCH(k_pressure<L>, blocks(h->n), h->P, h->p, h->rho, h->T, h->nb);
+    return 0;
+}
 
 // multiPhasePP.c:157-240, one operator after another.
 template <class L>
@@ -667,6 +675,7 @@ int mplb_gpu_create(const mplb_mesh_desc* mesh, const mplb_eos_desc* eos, const 
         P.s2_den = ((1 / f->Lambda[2]) - 0.5);
         P.sig12 = 12 * f->sigma;
         P.sig6 = 6.0 * f->sigma;
+        P.sigma_p = f->sigma;
     }
     if (g && g->model != MPLB_NO_MODEL) {
         for (int k = 0; k < MPLB_MAX_Q; k++) P.Lg[k] = g->Lambda[k];
@@ -725,7 +734,7 @@ int mplb_gpu_create(const mplb_mesh_desc* mesh, const mplb_eos_desc* eos, const 
         return code;
     };
     if ((rc = dalloc(h, &h->nb, nq)) || (rc = dalloc(h, &h->onb, h->n)) || (rc = dalloc(h, &h->rho, h->n)) ||
-        (rc = dalloc(h, &h->T, h->n)) || (rc = dalloc(h, &h->S, h->n)) || (rc = dalloc(h, &h->U, 3 * (size_t)h->n)) ||
+        (rc = dalloc(h, &h->T, h->n)) || (rc = dalloc(h, &h->S, h->n)) || (rc = dalloc(h, &h->p, h->n)) || (rc = dalloc(h, &h->U, 3 * (size_t)h->n)) ||
         (rc = dalloc(h, &h->Fi, 3 * (size_t)h->n)) || (rc = dalloc(h, &h->Ft, 3 * (size_t)h->n)) ||
         (rc = dalloc(h, &h->pnodes, tot)) || (rc = dalloc(h, &h->dpatches, 2 * std::max<size_t>(1, mesh->n_patches))))
         return bail(rc);
@@ -931,6 +940,21 @@ int mplb_gpu_heat_source(mplb_gpu_t* h) {
     DeviceGuard guard(h->dev);
     RET(materialize(h));
     return DISPATCH(h, op_heatsource, h);
+}
+
+int mplb_gpu_macro_pressure(mplb_gpu_t* h) {
+    if (!h) return fail(MPLB_E_ARG, "NULL handle");
+    if (h->P.f_update && h->model[0] != MPLB_LIMRT && h->model[0] != MPLB_XUMRT)
+        return fail(MPLB_E_UNSUPPORTED, "Pressure update not available (macroPressure.c:60-64)");
+    DeviceGuard guard(h->dev);
+    RET(materialize(h));
+    return DISPATCH(h, op_pressure, h);
+}
+
+int mplb_gpu_download_pressure(mplb_gpu_t* h, double* p) {
+    if (!h || !p) return fail(MPLB_E_ARG, "NULL argument");
+    DeviceGuard guard(h->dev);
+    return get_scalar(h, p, h->p);
 }
 
 int mplb_gpu_set_time(mplb_gpu_t* h, uint32_t current) {

@@ -205,6 +205,55 @@ __global__ void k_heatsource(Params P, double* __restrict__ S, const double* __r
     S[id] = heat_source_value(P, r, t, dot, div, old);
 }
 
+// ---------------------------------------------------------------- pressure
+// macroPressure.c:8-69 with liMRTPressure.c:6-253 (D2Q9) and
+// xuMRTPressure.c:6-22 (D3Q15, rho cs2 + G psi^2 / 2 only).
+template <class L>
+__global__ void k_pressure(Params P, double* __restrict__ p, const double* __restrict__ rho,
+                           const double* __restrict__ T, const int32_t* __restrict__ nb) {
+    const uint32_t n = P.n, id = blockIdx.x * blockDim.x + threadIdx.x;
+    if (id >= n) return;
+    auto psi_at = [&](uint32_t i) { return potential(P, rho[i], T[i]); };
+    const double ps = psi_at(id);
+    double pr = rho[id] * P.cs2 + 0.5 * P.G * ps * ps;
+    if constexpr (L::Q == 9) {
+        // x term assigns lap, the y term adds to it left to right (liMRTPressure.c:27-110);
+        // one-sided second differences reach two nodes into the lattice
+        double lap = 0;
+#pragma unroll
+        for (int d = 0; d < 2; d++) {
+            const int ka = fda<L>(d), kb = fdb<L>(d);
+            const int32_t a = nb[(size_t)ka * n + id], b = nb[(size_t)kb * n + id];
+            const double s0 = d == 0 ? 0.0 : lap;
+            if (a != -1 && b != -1) {
+                lap = d == 0 ? psi_at(a) + psi_at(b) - 2 * ps : s0 + psi_at(a) + psi_at(b) - 2 * ps;
+            } else if (a == -1 && b != -1) {
+                const int32_t c = nb[(size_t)kb * n + b];
+                lap = d == 0 ? psi_at(c) - 2 * psi_at(b) + ps : s0 + psi_at(c) - 2 * psi_at(b) + ps;
+            } else if (a != -1 && b == -1) {
+                const int32_t c = nb[(size_t)ka * n + a];
+                lap = d == 0 ? psi_at(c) - 2 * psi_at(a) + ps : s0 + psi_at(c) - 2 * psi_at(a) + ps;
+            } else if (d == 0) {
+                lap = 0;
+            }
+        }
+        pr = pr + P.G * ps * lap / 12;
+        double grad[3] = {0, 0, 0};
+#pragma unroll
+        for (int d = 0; d < 2; d++) {
+            const int32_t a = nb[(size_t)fda<L>(d) * n + id], b = nb[(size_t)fdb<L>(d) * n + id];
+            if (a != -1 && b != -1) grad[d] = 0.5 * (psi_at(a) - psi_at(b));
+            else if (a == -1 && b != -1) grad[d] = (ps - psi_at(b));
+            else if (a != -1 && b == -1) grad[d] = (psi_at(a) - ps);
+        }
+        double g2 = 0;
+#pragma unroll
+        for (int k = 0; k < 3; k++) g2 += grad[k] * grad[k];
+        pr = pr + 2.0 * P.G * P.G * P.sigma_p * g2;
+    }
+    p[id] = pr;
+}
+
 // -------------------------------------------------------------- boundaries
 // liTempMRTEquilibrium row k (fixedT.c:145,178): sum_j Mi[k][j] n_eq[j].
 __device__ __forceinline__ double eq_heat_k(const Params& P, int k, double T, double u0, double u1) {

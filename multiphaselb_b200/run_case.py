@@ -23,10 +23,13 @@ def main(argv=None):
     ap.add_argument("workload", choices=list(WORKLOADS))
     ap.add_argument("steps", type=int)
     ap.add_argument("--path", default="auto", choices=["auto", "fused", "operators"])
+    ap.add_argument("--tile", type=int, default=0, help="0 = autotune, k > 0 = candidate k-1")
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32dev"])
     a = ap.parse_args(argv)
     path = {"auto": PATH_AUTO, "fused": PATH_FUSED, "operators": PATH_OPERATORS}[a.path]
     case = WORKLOADS[a.workload]()
-    with Lattice(case, path=path, device=0) as lat:
+    prec = abi.FP64 if a.precision == "fp64" else abi.FP32_DEV
+    with Lattice(case, path=path, device=0, tile_config=a.tile, precision=prec) as lat:
         lat.upload_case()
         lat.initialize()
         lat.step(a.steps)

@@ -40,7 +40,7 @@ typedef struct orc {
     int32_t* bct[2];
     double* bcv[2];
     int has[2];
-    double *rho, *T, *U, *Fi, *Ft, *S; /* U/Fi/Ft: [n][3] */
+    double *rho, *T, *U, *Fi, *Ft, *S, *p; /* U/Fi/Ft: [n][3] */
     double *pdf[2], *swap;             /* [n][Q] */
     uint32_t current;
     /* lattice tables */
@@ -531,6 +531,59 @@ static int op_heatsource(orc* o) {
     return 0;
 }
 
+/* liMRTPressure.c:6-253 (D2Q9): rho cs2 + G psi^2/2 + G psi lap(psi)/12
+ * + 2 G^2 sigma |grad psi|^2, with one-sided second differences at a missing
+ * neighbour; xuMRTPressure.c:6-22 (D3Q15) keeps rho cs2 + G psi^2/2. */
+static double pressure_node(orc* o, uint32_t id) {
+    const int Q = o->Q;
+    double ps = psi(o, o->rho[id], o->T[id]);
+    double p = o->rho[id] * o->cs2 + 0.5 * o->eos.G * ps * ps;
+    if (o->lat != MPLB_D2Q9) return p;
+#define PSI(i) psi(o, o->rho[i], o->T[i])
+#define NB(i, k) o->nb[(size_t)(i) * Q + (k)]
+    /* x term assigns lap, y term adds to it left to right:
+     * lap = lap + psi_a + psi_b - 2 psi (liMRTPressure.c:27-110). */
+    double lap = 0;
+    for (int d = 0; d < 2; d++) {
+        int ka = o->fd_a[d], kb = o->fd_b[d];
+        int a = NB(id, ka), b = NB(id, kb);
+        double s0 = d == 0 ? 0.0 : lap;
+        if (a != -1 && b != -1) {
+            lap = d == 0 ? PSI(a) + PSI(b) - 2 * PSI(id) : s0 + PSI(a) + PSI(b) - 2 * PSI(id);
+        } else if (a == -1 && b != -1) {
+            int c = NB(b, kb);
+            lap = d == 0 ? PSI(c) - 2 * PSI(b) + PSI(id) : s0 + PSI(c) - 2 * PSI(b) + PSI(id);
+        } else if (a != -1 && b == -1) {
+            int c = NB(a, ka);
+            lap = d == 0 ? PSI(c) - 2 * PSI(a) + PSI(id) : s0 + PSI(c) - 2 * PSI(a) + PSI(id);
+        } else if (d == 0) {
+            lap = 0;
+        }
+    }
+    p = p + o->eos.G * ps * lap / 12;
+    double grad[3] = {0, 0, 0};
+    for (int d = 0; d < 2; d++) {
+        int a = NB(id, o->fd_a[d]), b = NB(id, o->fd_b[d]);
+        if (a != -1 && b != -1) grad[d] = 0.5 * (PSI(a) - PSI(b));
+        else if (a == -1 && b != -1) grad[d] = (PSI(id) - PSI(b));
+        else if (a != -1 && b == -1) grad[d] = (PSI(a) - PSI(id));
+        else grad[d] = 0;
+    }
+#undef PSI
+#undef NB
+    double g2 = 0;
+    for (int k = 0; k < 3; k++) g2 += grad[k] * grad[k];
+    return p + 2.0 * o->eos.G * o->eos.G * o->fd[0].sigma * g2;
+}
+
+/* general/macroPressure.c:8-69 */
+static int op_pressure(orc* o) {
+    if (!o->fd[0].update) return 0;
+    if (o->fd[0].model != MPLB_LIMRT && o->fd[0].model != MPLB_XUMRT) return -1;
+    for (uint32_t id = 0; id < o->n; id++) o->p[id] = pressure_node(o, id);
+    return 0;
+}
+
 /* general/equilibrium.c:6-90 */
 static int op_equilibrium(orc* o, int fi) {
     if (!o->fd[fi].update) return 0;
@@ -587,6 +640,7 @@ orc* orc_create(const mplb_mesh_desc* md, const mplb_eos_desc* ed, const mplb_fi
     o->rho = (double*)calloc(o->n, sizeof(double));
     o->T = (double*)calloc(o->n, sizeof(double));
     o->S = (double*)calloc(o->n, sizeof(double));
+    o->p = (double*)calloc(o->n, sizeof(double));
     o->U = (double*)calloc(3 * (size_t)o->n, sizeof(double));
     o->Fi = (double*)calloc(3 * (size_t)o->n, sizeof(double));
     o->Ft = (double*)calloc(3 * (size_t)o->n, sizeof(double));
@@ -598,7 +652,7 @@ void orc_destroy(orc* o) {
     if (!o) return;
     free(o->nb); free(o->onb); free(o->pcount); free(o->poff); free(o->pnodes);
     for (int i = 0; i < 2; i++) { free(o->bct[i]); free(o->bcv[i]); free(o->pdf[i]); }
-    free(o->swap); free(o->rho); free(o->T); free(o->S); free(o->U); free(o->Fi); free(o->Ft);
+    free(o->swap); free(o->rho); free(o->T); free(o->S); free(o->p); free(o->U); free(o->Fi); free(o->Ft);
     free(o);
 }
 
@@ -684,9 +738,11 @@ int orc_op(orc* o, int op, int field, uint32_t start, uint32_t end) {
     case 6: op_temperature(o, start, end); return 0;
     case 7: op_interforce(o); return 0;
     case 8: return op_heatsource(o);
+    case 9: return op_pressure(o);
     default: return -1;
     }
 }
 
+void orc_get_p(orc* o, double* p) { memcpy(p, o->p, o->n * sizeof(double)); }
 double orc_p_eos(orc* o, double rho, double T) { return p_eos(&o->eos, rho, T); }
 double orc_potential(orc* o, double rho, double T) { return psi(o, rho, T); }

@@ -26,7 +26,7 @@ LIBS = {"port": os.path.join(HERE, "liboracle.so"),
 PREFIX = {"port": "orc_", "ref": "ref_"}
 
 OP_EQUILIBRIUM, OP_COLLISION, OP_LBSTREAM, OP_BOUNDARIES, OP_DENSITY, OP_VELOCITY, \
-    OP_TEMPERATURE, OP_INTERFORCE, OP_HEATSOURCE = range(9)
+    OP_TEMPERATURE, OP_INTERFORCE, OP_HEATSOURCE, OP_PRESSURE = range(10)
 
 _loaded = {}
 
@@ -65,6 +65,7 @@ def _lib(kind):
     fn("set_rho0").argtypes = [C.c_void_p, C.c_double]
     fn("average_rho0").argtypes = [C.c_void_p]
     fn("average_rho0").restype = C.c_double
+    fn("get_p").argtypes = [C.c_void_p, D]
     for name in ("p_eos", "potential"):
         fn(name).argtypes = [C.c_void_p, C.c_double, C.c_double]
         fn(name).restype = C.c_double
@@ -136,6 +137,13 @@ class Checker:
 
     def average_rho0(self):
         return self._f("average_rho0")(self.h)
+
+    def pressure(self):
+        """macroPressure, then the pressure field."""
+        self.op(OP_PRESSURE)
+        p = np.zeros(self.case.n)
+        self._f("get_p")(self.h, abi.dptr(p))
+        return p
 
     def p_eos(self, rho, T):
         return self._f("p_eos")(self.h, rho, T)

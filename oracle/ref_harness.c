@@ -279,7 +279,7 @@ int ref_step(ref_case* c, uint32_t nsteps) {
 
 /* Single reference operators, for operator-level parity. */
 enum { OP_EQUILIBRIUM = 0, OP_COLLISION, OP_LBSTREAM, OP_BOUNDARIES, OP_DENSITY,
-       OP_VELOCITY, OP_TEMPERATURE, OP_INTERFORCE, OP_HEATSOURCE };
+       OP_VELOCITY, OP_TEMPERATURE, OP_INTERFORCE, OP_HEATSOURCE, OP_PRESSURE };
 
 int ref_op(ref_case* c, int op, int field, uint32_t start, uint32_t end) {
     lbeField* fl = field == MPLB_FIELD_G ? &c->g : &c->f;
@@ -294,10 +294,14 @@ int ref_op(ref_case* c, int op, int field, uint32_t start, uint32_t end) {
     case OP_TEMPERATURE: macroTemperature(m, &c->mf, &c->g, start, end); break;
     case OP_INTERFORCE: interForce(m, &c->mf); break;
     case OP_HEATSOURCE: heatSource(m, &c->mf, &c->g); break;
+    case OP_PRESSURE: macroPressure(m, &c->mf, &c->f); break;  /* multiPhasePP.c:264 */
     default: return -1;
     }
     return 0;
 }
+
+/* Pressure field (macroFields.p), filled by OP_PRESSURE. */
+void ref_get_p(ref_case* c, double* p) { memcpy(p, c->mf.p, c->n * sizeof(double)); }
 
 /* The reference structures of a case, for the adapter check. */
 void ref_structs(ref_case* c, latticeMesh** m, macroFields** mf, lbeField** f, lbeField** g) {

@@ -222,3 +222,22 @@ def test_every_tile_candidate_is_exact(gpu_lib, name):
         assert 0 <= info["tile_config"] < ncand
         assert all(t > 0 for t in info["tile_ms"][:ncand])
         assert_same(lat.download(), want, ctx=f"{name} autotuned")
+
+
+@pytest.mark.parametrize("name", CASES)
+@pytest.mark.parametrize("path", [abi.PATH_OPERATORS, abi.PATH_AUTO])
+def test_pressure_matches_oracle(gpu_lib, name, path):
+    """Write-time pressure (macroPressure) after a few steps, bit for bit."""
+    from multiphaselb_b200 import Lattice
+    case = small_cases()[name]
+    k = orc.Checker("port", case)
+    k.upload_case()
+    k.initialize()
+    k.step(5)
+    want = k.pressure()
+    with Lattice(case, path=path) as lat:
+        lat.upload_case()
+        lat.initialize()
+        lat.step(5)
+        got = lat.macro_pressure()
+    assert np.array_equal(got, want), float(np.abs(got - want).max())

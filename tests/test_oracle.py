@@ -101,3 +101,16 @@ def test_port_matches_golden(fname):
     case, steps, want = load_case(os.path.join(GOLDEN, fname))
     got = run_checker("port", case, steps)
     assert_same(got, want, fields=[k for k in FIELDS if k in want], ctx=fname)
+
+
+@pytest.mark.parametrize("name", list(small_cases().keys()))
+def test_port_pressure_matches_reference(name):
+    if not ref_available():
+        pytest.skip("reference build not present")
+    case = small_cases()[name]
+    ks = {k: orc.Checker(k, case) for k in ("port", "ref")}
+    for k in ks.values():
+        k.upload_case()
+        k.initialize()
+        k.step(3)
+    assert np.array_equal(ks["port"].pressure(), ks["ref"].pressure())
