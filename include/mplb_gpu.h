@@ -228,6 +228,59 @@ int mplb_gpu_sync(mplb_gpu_t* h);
  * overlap on the GPU share the array and race; order them on one stream. */
 int mplb_mass_energy_noalloc(const double* rho, const double* T, uint32_t n, double* out, void* stream);
 
+/* ------------------------------------------------------------------------
+ * Batched ensemble.  No counterpart in the reference, whose driver
+ * (src/app/multiPhasePP.c) advances one lattice per process: here many
+ * independent lattices -- each an ordinary handle created above -- advance
+ * together, one kernel launch per time step for all of them, a block taking
+ * (lattice, tile) pairs from a work table.  Each lattice's steps are the
+ * same arithmetic as mplb_gpu_step on that handle.
+ *
+ * Eligible handles: D2Q9, precision MPLB_FP32_DEV, fused path, a fully
+ * periodic box without boundary patches, isothermal (g frozen or absent),
+ * all on one device.  The handles stay owned by the caller and must outlive
+ * the batch; between batch calls they can be used (download, pressure, ...)
+ * as usual.  Work runs on the first handle's stream; every call returns with
+ * the handles' state current and their streams ordered after it.
+ * ---------------------------------------------------------------------- */
+typedef struct mplb_batch mplb_batch_t;
+
+typedef struct {
+    int32_t tile_config;      /* 0: time every tile candidate on the real
+                                 state at the first call, keep the fastest;
+                                 k > 0: candidate k-1 */
+    uint32_t check_interval;  /* steps between convergence checks (even, >= 2) */
+    double tol;               /* converged when max |rho(t) - rho(t-K)| / K < tol */
+} mplb_batch_opts;
+
+typedef struct {
+    uint32_t n_lattices;
+    uint64_t nodes;           /* sum over lattices */
+    int32_t tile_config;      /* candidate in use (-1 before the first call) */
+    int32_t n_candidates;
+    int32_t tile_x[8], tile_y[8];
+    float tile_ms[8];         /* autotuner: ms per step of each candidate */
+    int32_t grid;             /* persistent blocks per step launch */
+    uint64_t kernel_launches;
+    uint64_t graph_launches;  /* check intervals replayed from the captured graph */
+} mplb_batch_info;
+
+int mplb_batch_create(mplb_gpu_t* const* lattices, uint32_t count, const mplb_batch_opts* opts,
+                      mplb_batch_t** out);
+int mplb_batch_destroy(mplb_batch_t* b);
+int mplb_batch_info_get(mplb_batch_t* b, mplb_batch_info* info);
+/* nsteps time steps of every lattice, no convergence checks. */
+int mplb_batch_step(mplb_batch_t* b, uint32_t nsteps);
+/* Advance lattices in check intervals of K = check_interval steps until each
+ * has max |drho/dt| < tol (rho as the next step sums it, over one interval),
+ * or has taken max_steps (rounded up to a whole interval).  A converged
+ * lattice leaves the work table and stops.  Each interval -- K step launches
+ * and one check launch -- replays one captured CUDA graph.
+ * steps_out[i]: steps lattice i took; rate_out[i]: its last max |drho/dt|
+ * (may be NULL); *n_converged: lattices that met tol. */
+int mplb_batch_run(mplb_batch_t* b, uint32_t max_steps, uint32_t* steps_out, double* rate_out,
+                   uint32_t* n_converged);
+
 #ifdef __cplusplus
 }
 #endif

@@ -6,7 +6,8 @@ benchmark.  ``Lattice`` mirrors the reference's operator sequence: the same
 operator names as src/lbEquation/general (collision, lbstream,
 update_boundaries, macro_density, macro_velocity, macro_temperature,
 inter_force, heat_source, equilibrium) plus the solver-level calls
-initialize / step / download.
+initialize / step / download.  ``Batch`` advances many such lattices
+together (one launch per step for all of them).
 
 There is no CPU fallback: if the library is missing or no CUDA device is
 present, constructing a Lattice raises.
@@ -68,6 +69,11 @@ def load_library(path=LIB_PATH):
         "mplb_gpu_average_rho0": ([H, D], C.c_int),
         "mplb_gpu_mass_energy": ([H, D, D], C.c_int),
         "mplb_gpu_sync": ([H], C.c_int),
+        "mplb_batch_create": ([C.POINTER(H), C.c_uint32, C.POINTER(abi.BatchOpts), C.POINTER(H)], C.c_int),
+        "mplb_batch_destroy": ([H], C.c_int),
+        "mplb_batch_info_get": ([H, C.POINTER(abi.BatchInfo)], C.c_int),
+        "mplb_batch_step": ([H, C.c_uint32], C.c_int),
+        "mplb_batch_run": ([H, C.c_uint32, C.POINTER(C.c_uint32), D, C.POINTER(C.c_uint32)], C.c_int),
     }
     for name, (args, res) in sig.items():
         fn = getattr(lib, name)
@@ -210,3 +216,63 @@ class Lattice:
         m, e = C.c_double(), C.c_double()
         self._check(self.lib.mplb_gpu_mass_energy(self.h, C.byref(m), C.byref(e)))
         return m.value, e.value
+
+
+class Batch:
+    """Many independent lattices advanced together (mplb_batch_*).
+
+    ``lattices`` are :class:`Lattice` objects (D2Q9, FP32-deviation, fused,
+    fully periodic, isothermal); they stay usable between batch calls and
+    must outlive the batch.
+    """
+
+    def __init__(self, lattices, check_interval=1000, tol=1e-9, tile_config=0):
+        self.lib = load_library()
+        self.lattices = list(lattices)
+        arr = (C.c_void_p * len(self.lattices))(*[lat.h.value for lat in self.lattices])
+        opts = abi.BatchOpts(tile_config, check_interval, tol)
+        h = C.c_void_p()
+        self._check(self.lib.mplb_batch_create(arr, len(self.lattices), C.byref(opts), C.byref(h)))
+        self.h = h
+
+    def _check(self, rc):
+        if rc != 0:
+            raise MplbError(rc, self.lib.mplb_gpu_last_error().decode())
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.mplb_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def info(self):
+        i = abi.BatchInfo()
+        self._check(self.lib.mplb_batch_info_get(self.h, C.byref(i)))
+        nc = i.n_candidates
+        return dict(n_lattices=i.n_lattices, nodes=i.nodes, tile_config=i.tile_config,
+                    tiles=[(i.tile_x[c], i.tile_y[c]) for c in range(nc)],
+                    tile_ms=list(i.tile_ms)[:nc], grid=i.grid, kernel_launches=i.kernel_launches,
+                    graph_launches=i.graph_launches)
+
+    def step(self, n=1):
+        self._check(self.lib.mplb_batch_step(self.h, n))
+
+    def run(self, max_steps):
+        """Run to convergence; returns (steps per lattice, last max |drho/dt|, converged count)."""
+        m = len(self.lattices)
+        steps = np.zeros(m, dtype=np.uint32)
+        rate = np.zeros(m)
+        conv = C.c_uint32()
+        self._check(self.lib.mplb_batch_run(self.h, max_steps, abi.uptr(steps), abi.dptr(rate), C.byref(conv)))
+        return steps, rate, conv.value

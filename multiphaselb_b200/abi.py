@@ -83,6 +83,29 @@ class Info(C.Structure):
     ]
 
 
+class BatchOpts(C.Structure):
+    _fields_ = [
+        ("tile_config", C.c_int32),
+        ("check_interval", C.c_uint32),
+        ("tol", C.c_double),
+    ]
+
+
+class BatchInfo(C.Structure):
+    _fields_ = [
+        ("n_lattices", C.c_uint32),
+        ("nodes", C.c_uint64),
+        ("tile_config", C.c_int32),
+        ("n_candidates", C.c_int32),
+        ("tile_x", C.c_int32 * 8),
+        ("tile_y", C.c_int32 * 8),
+        ("tile_ms", C.c_float * 8),
+        ("grid", C.c_int32),
+        ("kernel_launches", C.c_uint64),
+        ("graph_launches", C.c_uint64),
+    ]
+
+
 def dptr(a):
     """double* of a contiguous float64 numpy array, or NULL for None."""
     if a is None:

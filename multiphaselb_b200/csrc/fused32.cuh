@@ -21,6 +21,7 @@ namespace mplb {
 
 struct FusedArgs32 {
     int nx, ny, nz, px, py, pz, tiles_x, tiles_y, zchunk;
+    uint32_t n;  // nodes of this lattice (array stride)
     const float* fin;
     float* fout;
     const float* gin;
@@ -181,7 +182,7 @@ __device__ __forceinline__ void collide_litemp32(const FusedArgs32& A, float* g,
 template <class L, bool F_ON, bool G_ON, bool HAS_BC>
 __device__ __forceinline__ void pull_node32(const Params& P, const FusedArgs32& A, int x, int y, int z, uint32_t id,
                                             float* f, float* g, double& rho, double& T, float& dr, float& dT) {
-    const uint32_t n = P.n;
+    const uint32_t n = A.n;
     FusedArgs G{};
     G.nx = A.nx; G.ny = A.ny; G.nz = A.nz; G.px = A.px; G.py = A.py; G.pz = A.pz;
     const NodeOffsets no = node_offsets(G, x, y, L::D == 3 ? z : 0, L::D);
@@ -262,7 +263,7 @@ __device__ __forceinline__ void finish_node32(const Params& P, const FusedArgs32
                                               float* g, double rho, float dr, double T, float dT, double psi,
                                               PsiAt nbpsi, double heat, double* emit_f, double* emit_g,
                                               double* rho_out, double* Fi_out, double* Ft_out) {
-    const uint32_t n = P.n;
+    const uint32_t n = A.n;
     double Fi[3] = {0, 0, 0}, Ft[3], Ud[3];
     if constexpr (F_ON) {
         if (!onb) {

@@ -2,26 +2,33 @@
 // Compiled with -fmad=true: this path is measured against FP64, not bitwise.
 #include <cuda_runtime.h>
 
+#include <algorithm>
+
 #include "fused32.cuh"
 
 namespace mplb {
 
-// ------------------------------------------------------------- 2D kernel
+// ------------------------------------------------------------- 2D tile
+// Shared memory of one 2D tile (psi, 1/rho, T_{n-1}, U_{n-1} on tile + ring).
+template <int TX, int TY, bool G_ON>
+struct Smem32 {
+    static constexpr int EX = TX + 2, EY = TY + 2, GY = G_ON ? EY : 1, GX = G_ON ? EX : 1;
+    double psi[EY][EX];
+    double inv[GY][GX];
+    double To[GY][GX];
+    double U0[GY][GX];
+    double U1[GY][GX];
+};
+
+// One TX x TY tile (tile coordinates bx, by) of the lattice described by A.
 template <int TX, int TY, bool F_ON, bool G_ON, bool HAS_BC, bool EMIT>
-__global__ void __launch_bounds__(TX * TY, min_blocks(TX * TY))
-    k_fused32_d2q9(Params P, FusedArgs32 A, double* emit_f, double* emit_g, double* rho_out, double* Fi_out,
-                   double* Ft_out) {
+__device__ __forceinline__ void fused32_tile_d2q9(const Params& P, const FusedArgs32& A, Smem32<TX, TY, G_ON>& sm,
+                                                  int bx, int by, double* emit_f, double* emit_g, double* rho_out,
+                                                  double* Fi_out, double* Ft_out) {
     using L = D2Q9T;
-    constexpr int EX = TX + 2, EY = TY + 2, NRING = 2 * EX + 2 * TY;
-    constexpr int GY = G_ON ? EY : 1, GX = G_ON ? EX : 1;
-    __shared__ double s_psi[EY][EX];
-    __shared__ double s_inv[GY][GX];
-    __shared__ double s_To[GY][GX];
-    __shared__ double s_U0[GY][GX];
-    __shared__ double s_U1[GY][GX];
-    const uint32_t n = P.n;
+    constexpr int NRING = 2 * (TX + 2) + 2 * TY;
+    const uint32_t n = A.n;
     const int tx = threadIdx.x % TX, ty = threadIdx.x / TX;
-    const int bx = blockIdx.x % A.tiles_x, by = blockIdx.x / A.tiles_x;
     const int x0 = bx * TX, y0 = by * TY;
 
     auto slot = [&](int ex, int ey, float* f, float* g, double& rho, double& T, float& dr, float& dT, uint32_t& id,
@@ -34,16 +41,16 @@ __global__ void __launch_bounds__(TX * TY, min_blocks(TX * TY))
         if (mine) {
             rr = rcp_rn(rho);
             er = eos_rho(P, rho);
-            if constexpr (F_ON) s_psi[ey][ex] = potential_p(P, rho, p_eos_at(P, er, rho, T));
-            if constexpr (G_ON) s_inv[ey][ex] = rr;
+            if constexpr (F_ON) sm.psi[ey][ex] = potential_p(P, rho, p_eos_at(P, er, rho, T));
+            if constexpr (G_ON) sm.inv[ey][ex] = rr;
         } else {
-            if constexpr (F_ON) s_psi[ey][ex] = potential(P, rho, T);
-            if constexpr (G_ON) s_inv[ey][ex] = 1.0 / rho;
+            if constexpr (F_ON) sm.psi[ey][ex] = potential(P, rho, T);
+            if constexpr (G_ON) sm.inv[ey][ex] = 1.0 / rho;
         }
         if constexpr (G_ON) {
-            s_To[ey][ex] = A.Told[id];
-            s_U0[ey][ex] = A.Uold[id];
-            s_U1[ey][ex] = A.Uold[n + id];
+            sm.To[ey][ex] = A.Told[id];
+            sm.U0[ey][ex] = A.Uold[id];
+            sm.U1[ey][ex] = A.Uold[n + id];
         }
         return true;
     };
@@ -64,41 +71,51 @@ __global__ void __launch_bounds__(TX * TY, min_blocks(TX * TY))
     const bool own = gx < A.nx && gy < A.ny;
     const bool have = slot(tx + 1, ty + 1, f, g, rho, T, dr, dT, id, own, rr, er);
     __syncthreads();
-    if (!own || !have) return;
-
-    const int ex = tx + 1, ey = ty + 1;
-    FusedArgs Gm{};
-    Gm.nx = A.nx; Gm.ny = A.ny; Gm.nz = 1; Gm.px = A.px; Gm.py = A.py; Gm.pz = 1;
-    const bool onb = on_wall(Gm, gx, gy, 0);
-    double heat = 0;
-    if constexpr (G_ON && !EMIT) {
-        double gT[3] = {0, 0, 0}, gR[3] = {0, 0, 0}, div = 0;
-        const double To = s_To[ey][ex], iv = s_inv[ey][ex];
-        {
-            const bool a = wrap1(gx + 1, A.nx, A.px) >= 0, b = wrap1(gx - 1, A.nx, A.px) >= 0;
-            FD t = fd_pair(a ? 0 : -1, b ? 0 : -1, s_To[ey][ex + 1], s_To[ey][ex - 1], To);
-            FD r = fd_pair(a ? 0 : -1, b ? 0 : -1, s_inv[ey][ex + 1], s_inv[ey][ex - 1], iv);
-            FD u = fd_pair(a ? 0 : -1, b ? 0 : -1, s_U0[ey][ex + 1], s_U0[ey][ex - 1], s_U0[ey][ex]);
-            gT[0] = t.v;
-            gR[0] = r.v;
-            if (u.present) div += u.v;
+    if (own && have) {
+        const int ex = tx + 1, ey = ty + 1;
+        FusedArgs Gm{};
+        Gm.nx = A.nx; Gm.ny = A.ny; Gm.nz = 1; Gm.px = A.px; Gm.py = A.py; Gm.pz = 1;
+        const bool onb = on_wall(Gm, gx, gy, 0);
+        double heat = 0;
+        if constexpr (G_ON && !EMIT) {
+            double gT[3] = {0, 0, 0}, gR[3] = {0, 0, 0}, div = 0;
+            const double To = sm.To[ey][ex], iv = sm.inv[ey][ex];
+            {
+                const bool a = wrap1(gx + 1, A.nx, A.px) >= 0, b = wrap1(gx - 1, A.nx, A.px) >= 0;
+                FD t = fd_pair(a ? 0 : -1, b ? 0 : -1, sm.To[ey][ex + 1], sm.To[ey][ex - 1], To);
+                FD r = fd_pair(a ? 0 : -1, b ? 0 : -1, sm.inv[ey][ex + 1], sm.inv[ey][ex - 1], iv);
+                FD u = fd_pair(a ? 0 : -1, b ? 0 : -1, sm.U0[ey][ex + 1], sm.U0[ey][ex - 1], sm.U0[ey][ex]);
+                gT[0] = t.v;
+                gR[0] = r.v;
+                if (u.present) div += u.v;
+            }
+            {
+                const bool a = wrap1(gy + 1, A.ny, A.py) >= 0, b = wrap1(gy - 1, A.ny, A.py) >= 0;
+                FD t = fd_pair(a ? 0 : -1, b ? 0 : -1, sm.To[ey + 1][ex], sm.To[ey - 1][ex], To);
+                FD r = fd_pair(a ? 0 : -1, b ? 0 : -1, sm.inv[ey + 1][ex], sm.inv[ey - 1][ex], iv);
+                FD u = fd_pair(a ? 0 : -1, b ? 0 : -1, sm.U1[ey + 1][ex], sm.U1[ey - 1][ex], sm.U1[ey][ex]);
+                gT[1] = t.v;
+                gR[1] = r.v;
+                if (u.present) div += u.v;
+            }
+            const double dot = gT[0] * gR[0] + gT[1] * gR[1] + gT[2] * gR[2];
+            heat = heat_source_value_er(P, er, rho, rr, To, dot, div, A.S[id]);
         }
-        {
-            const bool a = wrap1(gy + 1, A.ny, A.py) >= 0, b = wrap1(gy - 1, A.ny, A.py) >= 0;
-            FD t = fd_pair(a ? 0 : -1, b ? 0 : -1, s_To[ey + 1][ex], s_To[ey - 1][ex], To);
-            FD r = fd_pair(a ? 0 : -1, b ? 0 : -1, s_inv[ey + 1][ex], s_inv[ey - 1][ex], iv);
-            FD u = fd_pair(a ? 0 : -1, b ? 0 : -1, s_U1[ey + 1][ex], s_U1[ey - 1][ex], s_U1[ey][ex]);
-            gT[1] = t.v;
-            gR[1] = r.v;
-            if (u.present) div += u.v;
-        }
-        const double dot = gT[0] * gR[0] + gT[1] * gR[1] + gT[2] * gR[2];
-        heat = heat_source_value_er(P, er, rho, rr, To, dot, div, A.S[id]);
+        const double psi = F_ON ? sm.psi[ey][ex] : 0.0;
+        auto nbpsi = [&](int k) { return sm.psi[ey + cyk<L>(k)][ex + cxk<L>(k)]; };
+        finish_node32<L, F_ON, G_ON, EMIT>(P, A, id, onb, f, g, rho, dr, T, dT, psi, nbpsi, heat, emit_f, emit_g,
+                                           rho_out, Fi_out, Ft_out);
     }
-    const double psi = F_ON ? s_psi[ey][ex] : 0.0;
-    auto nbpsi = [&](int k) { return s_psi[ey + cyk<L>(k)][ex + cxk<L>(k)]; };
-    finish_node32<L, F_ON, G_ON, EMIT>(P, A, id, onb, f, g, rho, dr, T, dT, psi, nbpsi, heat, emit_f, emit_g,
-                                       rho_out, Fi_out, Ft_out);
+}
+
+// ------------------------------------------------------------- 2D kernel
+template <int TX, int TY, bool F_ON, bool G_ON, bool HAS_BC, bool EMIT>
+__global__ void __launch_bounds__(TX * TY, min_blocks(TX * TY))
+    k_fused32_d2q9(Params P, FusedArgs32 A, double* emit_f, double* emit_g, double* rho_out, double* Fi_out,
+                   double* Ft_out) {
+    __shared__ Smem32<TX, TY, G_ON> sm;
+    fused32_tile_d2q9<TX, TY, F_ON, G_ON, HAS_BC, EMIT>(P, A, sm, blockIdx.x % A.tiles_x, blockIdx.x / A.tiles_x,
+                                                         emit_f, emit_g, rho_out, Fi_out, Ft_out);
 }
 
 // ------------------------------------------------------------- 3D kernel
@@ -200,6 +217,8 @@ using namespace mplb;
 FusedArgs32 mplb_make_args32(const FusedArgs& A, const Params& P, double rho_ref, double T_ref) {
     FusedArgs32 B{};
     B.nx = A.nx; B.ny = A.ny; B.nz = A.nz; B.px = A.px; B.py = A.py; B.pz = A.pz;
+    B.tiles_x = A.tiles_x; B.tiles_y = A.tiles_y; B.zchunk = A.zchunk;
+    B.n = P.n;
     B.bcmap = A.bcmap;
     for (int p = 0; p < MPLB_MAX_PATCHES; p++) B.Twall[p] = A.Twall[p];
     for (int q = 0; q < FUSED_MAX_PROGS; q++) B.prog[q] = A.prog[q];
@@ -279,6 +298,7 @@ __global__ void k_to_dev32(uint32_t n, int Q, const double* __restrict__ src, fl
     if (i >= (size_t)n * Q) return;
     const int k = (int)(i / n);
     const double ref = heat ? (double)B.wg[k] * B.T_ref : (double)B.wf[k] * B.rho_ref;
+    (void)B.n;
     dst[i] = (float)(src[i] - ref);
 }
 
@@ -286,5 +306,123 @@ cudaError_t mplb_to_dev32(uint32_t n, int Q, const double* src, float* dst, cons
                           cudaStream_t s) {
     const size_t tot = (size_t)n * Q;
     k_to_dev32<<<(unsigned)((tot + 255) / 256), 256, 0, s>>>(n, Q, src, dst, B, heat);
+    return cudaGetLastError();
+}
+
+// ============================================================ batched ensemble
+// Many independent periodic D2Q9 lattices (isothermal, FP32 deviations) in one
+// persistent launch: blocks stride over a table of (lattice, tile) pairs.
+// Each lattice has its own parameter block and arguments (both parities of
+// its ping-pong buffers) in device memory.
+namespace mplb {
+
+constexpr int N_BATCH_CFG = 4;
+constexpr TileCfg BATCH_CFG[N_BATCH_CFG] = {{32, 8, false}, {32, 4, false}, {16, 8, false}, {64, 4, false}};
+
+template <int TX, int TY>
+__global__ void __launch_bounds__(TX * TY, min_blocks(TX * TY))
+    k_batch32_d2q9(const Params* __restrict__ Ps, const FusedArgs32* __restrict__ As, const int2* __restrict__ tiles,
+                   const int* __restrict__ ntiles, int parity) {
+    __shared__ Smem32<TX, TY, false> sm;
+    const int nt = *ntiles;
+    for (int t = blockIdx.x; t < nt; t += gridDim.x) {
+        const int2 w = tiles[t];
+        const FusedArgs32& A = As[2 * w.x + parity];
+        if (A.tiles_x <= 0 || w.y < 0 || w.y >= A.tiles_x * A.tiles_y) continue;  // block-uniform
+        fused32_tile_d2q9<TX, TY, true, false, false, false>(Ps[w.x], A, sm, w.y % A.tiles_x, w.y / A.tiles_x,
+                                                              nullptr, nullptr, nullptr, nullptr, nullptr);
+        __syncthreads();
+    }
+}
+
+// Per lattice: max over nodes of |rho_now - rho_snapshot|, then the snapshot
+// becomes rho_now.  rho_now is what the next step's pull sums to.
+template <int TX, int TY>
+__global__ void __launch_bounds__(TX * TY)
+    k_batch32_check(const Params* __restrict__ Ps, const FusedArgs32* __restrict__ As,
+                    const int2* __restrict__ tiles, const int* __restrict__ ntiles, int parity,
+                    double* const* __restrict__ snaps, unsigned long long* __restrict__ dmax) {
+    __shared__ double red[TX * TY / 32];
+    const int nt = *ntiles;
+    for (int t = blockIdx.x; t < nt; t += gridDim.x) {
+        const int2 w = tiles[t];
+        const FusedArgs32& A = As[2 * w.x + parity];
+        if (A.tiles_x <= 0 || w.y < 0 || w.y >= A.tiles_x * A.tiles_y) continue;  // block-uniform
+        const int bx = w.y % A.tiles_x, by = w.y / A.tiles_x;
+        const int x = bx * TX + (int)threadIdx.x % TX, y = by * TY + (int)threadIdx.x / TX;
+        double d = 0.0;
+        if (x < A.nx && y < A.ny) {
+            const uint32_t id = (uint32_t)x + (uint32_t)A.nx * (uint32_t)y;
+            float f[9], g[1], dr, dT;
+            double rho, T;
+            pull_node32<D2Q9T, true, false, false>(Ps[w.x], A, x, y, 0, id, f, g, rho, T, dr, dT);
+            double* snap = snaps[w.x];
+            d = fabs(rho - snap[id]);
+            snap[id] = rho;
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) d = fmax(d, __shfl_down_sync(0xffffffffu, d, o));
+        if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = d;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            double m = 0.0;
+            for (int i = 0; i < TX * TY / 32; i++) m = fmax(m, red[i]);
+            // non-negative doubles order like their bit patterns
+            atomicMax(dmax + w.x, (unsigned long long)__double_as_longlong(m));
+        }
+        __syncthreads();
+    }
+}
+
+}  // namespace mplb
+
+namespace {
+template <int TX, int TY>
+int batch_grid() {
+    int dev = 0, sms = 0, per = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_batch32_d2q9<TX, TY>, TX * TY, 0);
+    return std::max(per, 1) * std::max(sms, 1);
+}
+}  // namespace
+
+int mplb_batch_ncfg() { return N_BATCH_CFG; }
+void mplb_batch_cfg(int c, int* tx, int* ty) {
+    *tx = BATCH_CFG[c].tx;
+    *ty = BATCH_CFG[c].ty;
+}
+
+// Resident blocks of the step kernel for candidate c on the current device
+// (the persistent grid).
+int mplb_batch_grid(int c) {
+    switch (c) {
+    case 0: return batch_grid<32, 8>();
+    case 1: return batch_grid<32, 4>();
+    case 2: return batch_grid<16, 8>();
+    default: return batch_grid<64, 4>();
+    }
+}
+
+cudaError_t mplb_batch32_launch(int cfg, const Params* dP, const FusedArgs32* dA, const int2* tiles,
+                                const int* ntiles, int parity, int grid, cudaStream_t s) {
+    switch (cfg) {
+    case 0: k_batch32_d2q9<32, 8><<<grid, 256, 0, s>>>(dP, dA, tiles, ntiles, parity); break;
+    case 1: k_batch32_d2q9<32, 4><<<grid, 128, 0, s>>>(dP, dA, tiles, ntiles, parity); break;
+    case 2: k_batch32_d2q9<16, 8><<<grid, 128, 0, s>>>(dP, dA, tiles, ntiles, parity); break;
+    default: k_batch32_d2q9<64, 4><<<grid, 256, 0, s>>>(dP, dA, tiles, ntiles, parity); break;
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t mplb_batch32_check(int cfg, const Params* dP, const FusedArgs32* dA, const int2* tiles,
+                               const int* ntiles, int parity, int grid, double* const* snaps,
+                               unsigned long long* dmax, cudaStream_t s) {
+    switch (cfg) {
+    case 0: k_batch32_check<32, 8><<<grid, 256, 0, s>>>(dP, dA, tiles, ntiles, parity, snaps, dmax); break;
+    case 1: k_batch32_check<32, 4><<<grid, 128, 0, s>>>(dP, dA, tiles, ntiles, parity, snaps, dmax); break;
+    case 2: k_batch32_check<16, 8><<<grid, 128, 0, s>>>(dP, dA, tiles, ntiles, parity, snaps, dmax); break;
+    default: k_batch32_check<64, 4><<<grid, 256, 0, s>>>(dP, dA, tiles, ntiles, parity, snaps, dmax); break;
+    }
     return cudaGetLastError();
 }

@@ -28,6 +28,15 @@ cudaError_t mplb_fused32_launch(int lat, bool has_bc, bool f_on, bool g_on, bool
                                 cudaStream_t s);
 cudaError_t mplb_to_dev32(uint32_t n, int Q, const double* src, float* dst, const FusedArgs32& B, int heat,
                           cudaStream_t s);
+// Batched ensemble kernels (mplb_fp32.cu).
+int mplb_batch_ncfg();
+void mplb_batch_cfg(int c, int* tx, int* ty);
+int mplb_batch_grid(int c);
+cudaError_t mplb_batch32_launch(int cfg, const Params* dP, const FusedArgs32* dA, const int2* tiles,
+                                const int* ntiles, int parity, int grid, cudaStream_t s);
+cudaError_t mplb_batch32_check(int cfg, const Params* dP, const FusedArgs32* dA, const int2* tiles,
+                               const int* ntiles, int parity, int grid, double* const* snaps,
+                               unsigned long long* dmax, cudaStream_t s);
 
 namespace {
 
@@ -1013,6 +1022,394 @@ int mplb_gpu_sync(mplb_gpu_t* h) {
     DeviceGuard guard(h->dev);
     CK(cudaStreamSynchronize(h->stream));
     return 0;
+}
+
+}  // extern "C"
+
+// ================================================================= batch
+struct mplb_batch {
+    int dev = 0;
+    cudaStream_t stream = nullptr;
+    std::vector<mplb_gpu*> lat;
+    uint64_t nodes = 0;
+    uint32_t K = 0;
+    double tol = 0;
+    int tile_request = 0;
+    int cfg = -1;
+    int grid = 0;
+    float tile_ms[8] = {};
+    Params* dP = nullptr;
+    FusedArgs32* dA = nullptr;  // [lattice][parity]
+    int2* dtiles = nullptr;
+    int* dnt = nullptr;
+    size_t tile_cap = 0;
+    double** dsnap = nullptr;   // per-lattice pointers into snap
+    double* snap = nullptr;
+    unsigned long long* dmax = nullptr;
+    unsigned long long* hmax = nullptr;  // pinned
+    cudaGraphExec_t graph = nullptr;
+    int graph_cfg = -1;
+    uint32_t graph_K = 0;
+    uint64_t launches = 0, graph_launches = 0;
+};
+
+namespace {
+
+void batch_free(mplb_batch* b) {
+    if (b->graph) cudaGraphExecDestroy(b->graph);
+    void* ps[] = {b->dP, b->dA, b->dtiles, b->dnt, b->dsnap, b->snap, b->dmax};
+    for (void* p : ps)
+        if (p) cudaFree(p);
+    if (b->hmax) cudaFreeHost(b->hmax);
+}
+
+// Order the batch stream after every handle's queued work.
+int batch_enter(mplb_batch* b) {
+    for (mplb_gpu* h : b->lat)
+        if (h->stream != b->stream) CK(cudaStreamSynchronize(h->stream));
+    for (mplb_gpu* h : b->lat) {
+        if (h->fstate == 0) {
+            RET(prologue32(h));
+            CK(cudaStreamSynchronize(h->stream));
+        }
+    }
+    return 0;
+}
+
+// ... and every handle's later work after the batch.
+int batch_leave(mplb_batch* b) {
+    cudaEvent_t ev;
+    CK(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+    cudaError_t e = cudaEventRecord(ev, b->stream);
+    for (mplb_gpu* h : b->lat)
+        if (e == cudaSuccess && h->stream != b->stream) e = cudaStreamWaitEvent(h->stream, ev, 0);
+    cudaEventDestroy(ev);
+    CK(e);
+    return 0;
+}
+
+// Kernel arguments of every lattice for candidate c: [2i] steps from the
+// handle's current buffer, [2i+1] back.
+int batch_args(mplb_batch* b, int c) {
+    int tx = 0, ty = 0;
+    mplb_batch_cfg(c, &tx, &ty);
+    std::vector<FusedArgs32> A(2 * b->lat.size());
+    for (size_t i = 0; i < b->lat.size(); i++) {
+        mplb_gpu* h = b->lat[i];
+        FusedArgs a = h->fc.args;
+        a.tiles_x = (a.nx + tx - 1) / tx;
+        a.tiles_y = (a.ny + ty - 1) / ty;
+        FusedArgs32 B = mplb_make_args32(a, h->P, h->rho_ref, h->T_ref);
+        if (B.tiles_x != a.tiles_x || B.tiles_y != a.tiles_y || B.tiles_x <= 0 || B.tiles_y <= 0 || B.n != h->n)
+            return fail(MPLB_E_STATE, "batch: inconsistent tile geometry");
+        B.Told = h->T;  // the frozen temperature field, read by every pull
+        B.Tnew = nullptr;
+        B.Uold = B.Unew = h->U;
+        B.S = h->S;
+        B.rho_c = h->rho;
+        const int c0 = h->cur32[0];
+        for (int par = 0; par < 2; par++) {
+            FusedArgs32 Bp = B;
+            Bp.fin = h->p32[0][c0 ^ par];
+            Bp.fout = h->p32[0][c0 ^ par ^ 1];
+            if (!Bp.fin || !Bp.fout || !Bp.Told || !Bp.Uold || !Bp.S || !Bp.rho_c)
+                return fail(MPLB_E_STATE, "batch: lattice buffers missing");
+            A[2 * i + par] = Bp;
+        }
+    }
+    CK(cudaMemcpyAsync(b->dA, A.data(), A.size() * sizeof(FusedArgs32), cudaMemcpyHostToDevice, b->stream));
+    return 0;
+}
+
+// Work table of the lattices flagged in `active` for candidate c.
+int batch_table(mplb_batch* b, int c, const std::vector<char>& active, int* count) {
+    int tx = 0, ty = 0;
+    mplb_batch_cfg(c, &tx, &ty);
+    std::vector<int2> t;
+    for (size_t i = 0; i < b->lat.size(); i++) {
+        if (!active[i]) continue;
+        const FusedArgs& a = b->lat[i]->fc.args;
+        const int nt = ((a.nx + tx - 1) / tx) * ((a.ny + ty - 1) / ty);
+        for (int k = 0; k < nt; k++) t.push_back(make_int2((int)i, k));
+    }
+    if (t.size() > b->tile_cap) return fail(MPLB_E_STATE, "batch work table overflow");
+    const int nt = (int)t.size();
+    if (nt) CK(cudaMemcpyAsync(b->dtiles, t.data(), t.size() * sizeof(int2), cudaMemcpyHostToDevice, b->stream));
+    CK(cudaMemcpyAsync(b->dnt, &nt, sizeof(int), cudaMemcpyHostToDevice, b->stream));
+    // the host vector and nt leave scope: finish the copies first
+    CK(cudaStreamSynchronize(b->stream));
+    if (count) *count = nt;
+    return 0;
+}
+
+int batch_launch(mplb_batch* b, int c, int grid, int parity) {
+    cudaError_t e = mplb_batch32_launch(c, b->dP, b->dA, b->dtiles, b->dnt, parity, grid, b->stream);
+    b->launches++;
+    if (e != cudaSuccess) return fail(MPLB_E_CUDA, std::string("batch step launch: ") + cudaGetErrorString(e));
+    return 0;
+}
+
+int batch_check(mplb_batch* b, int parity) {
+    cudaError_t e = mplb_batch32_check(b->cfg, b->dP, b->dA, b->dtiles, b->dnt, parity, b->grid, b->dsnap, b->dmax,
+                                       b->stream);
+    b->launches++;
+    if (e != cudaSuccess) return fail(MPLB_E_CUDA, std::string("batch check launch: ") + cudaGetErrorString(e));
+    return 0;
+}
+
+// Autotuner: each candidate re-runs the first step from the current state
+// (parity 0 only, so the state does not advance: the step reads the current
+// buffers and rewrites the spare ones), best of a few timed launches.
+int batch_tune(mplb_batch* b) {
+    const std::vector<char> all(b->lat.size(), 1);
+    if (b->tile_request > 0) {
+        b->cfg = std::min(b->tile_request - 1, mplb_batch_ncfg() - 1);
+    } else {
+        cudaEvent_t e0, e1;
+        CK(cudaEventCreate(&e0));
+        CK(cudaEventCreate(&e1));
+        float best = 1e30f;
+        int pick = 0;
+        for (int c = 0; c < mplb_batch_ncfg(); c++) {
+            RET(batch_args(b, c));
+            int nt = 0;
+            RET(batch_table(b, c, all, &nt));
+            const int grid = std::max(1, std::min(mplb_batch_grid(c), nt));
+            RET(batch_launch(b, c, grid, 0));
+            float ms = 1e30f;
+            for (int r = 0; r < 3; r++) {
+                CK(cudaEventRecord(e0, b->stream));
+                RET(batch_launch(b, c, grid, 0));
+                CK(cudaEventRecord(e1, b->stream));
+                CK(cudaEventSynchronize(e1));
+                float t = 0;
+                CK(cudaEventElapsedTime(&t, e0, e1));
+                ms = std::min(ms, t);
+            }
+            b->tile_ms[c] = ms;
+            if (ms < best) {
+                best = ms;
+                pick = c;
+            }
+        }
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        b->cfg = pick;
+    }
+    return 0;
+}
+
+// Arguments and full work table for the chosen candidate.
+int batch_ready(mplb_batch* b, const std::vector<char>& active, int* nt) {
+    if (b->cfg < 0) RET(batch_tune(b));
+    RET(batch_args(b, b->cfg));
+    RET(batch_table(b, b->cfg, active, nt));
+    int tiles = 0;
+    for (size_t i = 0; i < b->lat.size(); i++) {
+        int tx = 0, ty = 0;
+        mplb_batch_cfg(b->cfg, &tx, &ty);
+        const FusedArgs& a = b->lat[i]->fc.args;
+        tiles += ((a.nx + tx - 1) / tx) * ((a.ny + ty - 1) / ty);
+    }
+    b->grid = std::max(1, std::min(mplb_batch_grid(b->cfg), tiles));
+    return 0;
+}
+
+// One check interval as a graph: K step launches (parity alternating, K is
+// even so every lattice ends on the buffer it started from), then the check.
+int batch_graph(mplb_batch* b) {
+    if (b->graph && b->graph_cfg == b->cfg && b->graph_K == b->K) return 0;
+    if (b->graph) {
+        cudaGraphExecDestroy(b->graph);
+        b->graph = nullptr;
+    }
+    cudaGraph_t g;
+    CK(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
+    int rc = 0;
+    for (uint32_t s = 0; s < b->K && !rc; s++) rc = batch_launch(b, b->cfg, b->grid, (int)(s & 1));
+    cudaError_t e = rc ? cudaSuccess : cudaMemsetAsync(b->dmax, 0, b->lat.size() * sizeof(unsigned long long), b->stream);
+    if (!rc && e == cudaSuccess) rc = batch_check(b, 0);
+    cudaError_t ee = cudaStreamEndCapture(b->stream, &g);
+    b->launches -= b->K + 1;  // counted when replayed
+    if (rc) {
+        if (ee == cudaSuccess) cudaGraphDestroy(g);
+        return rc;
+    }
+    CK(e);
+    CK(ee);
+    e = cudaGraphInstantiate(&b->graph, g, 0);
+    cudaGraphDestroy(g);
+    CK(e);
+    b->graph_cfg = b->cfg;
+    b->graph_K = b->K;
+    return 0;
+}
+
+}  // namespace
+
+extern "C" {
+
+int mplb_batch_create(mplb_gpu_t* const* lattices, uint32_t count, const mplb_batch_opts* opts, mplb_batch_t** out) {
+    if (!out) return fail(MPLB_E_ARG, "out is NULL");
+    *out = nullptr;
+    if (!lattices || count == 0) return fail(MPLB_E_ARG, "no lattices");
+    const uint32_t K = opts ? opts->check_interval : 1000;
+    if (K < 2 || (K & 1)) return fail(MPLB_E_ARG, "check_interval must be even and >= 2");
+    std::unordered_set<const mplb_gpu*> seen;
+    for (uint32_t i = 0; i < count; i++) {
+        const mplb_gpu* h = lattices[i];
+        if (!h) return fail(MPLB_E_ARG, "NULL handle in batch");
+        if (!seen.insert(h).second) return fail(MPLB_E_ARG, "handle listed twice in batch");
+        const std::string at = "lattice " + std::to_string(i) + ": ";
+        if (h->dev != lattices[0]->dev) return fail(MPLB_E_ARG, at + "batch lattices must share one device");
+        if (h->lat != MPLB_D2Q9) return fail(MPLB_E_UNSUPPORTED, at + "batch needs D2Q9");
+        if (h->precision != MPLB_FP32_DEV) return fail(MPLB_E_UNSUPPORTED, at + "batch needs MPLB_FP32_DEV");
+        if (h->path != MPLB_PATH_FUSED) return fail(MPLB_E_UNSUPPORTED, at + "batch needs the fused path");
+        if (h->fc.has_bc || !h->per[0] || !h->per[1])
+            return fail(MPLB_E_UNSUPPORTED, at + "batch needs a fully periodic box without boundary patches");
+        if (!h->P.f_update || h->P.g_update) return fail(MPLB_E_UNSUPPORTED, at + "batch needs f updated, g frozen");
+    }
+    mplb_batch* b = new mplb_batch();
+    b->dev = lattices[0]->dev;
+    b->stream = lattices[0]->stream;
+    b->lat.assign(lattices, lattices + count);
+    b->K = K;
+    b->tol = opts ? opts->tol : 1e-9;
+    b->tile_request = opts ? opts->tile_config : 0;
+    DeviceGuard guard(b->dev);
+    size_t cap = 0;
+    for (int c = 0; c < mplb_batch_ncfg(); c++) {
+        int tx = 0, ty = 0;
+        mplb_batch_cfg(c, &tx, &ty);
+        size_t t = 0;
+        for (mplb_gpu* h : b->lat) t += (size_t)((h->fc.args.nx + tx - 1) / tx) * ((h->fc.args.ny + ty - 1) / ty);
+        cap = std::max(cap, t);
+    }
+    b->tile_cap = cap;
+    std::vector<Params> P(count);
+    std::vector<double*> snaps(count);
+    for (uint32_t i = 0; i < count; i++) {
+        P[i] = b->lat[i]->P;
+        b->nodes += b->lat[i]->n;
+    }
+    auto setup = [&]() -> int {
+        CK(cudaMalloc((void**)&b->dP, count * sizeof(Params)));
+        CK(cudaMalloc((void**)&b->dA, 2 * count * sizeof(FusedArgs32)));
+        CK(cudaMalloc((void**)&b->dtiles, std::max<size_t>(cap, 1) * sizeof(int2)));
+        CK(cudaMalloc((void**)&b->dnt, sizeof(int)));
+        CK(cudaMalloc((void**)&b->dsnap, count * sizeof(double*)));
+        CK(cudaMalloc((void**)&b->snap, b->nodes * sizeof(double)));
+        CK(cudaMalloc((void**)&b->dmax, count * sizeof(unsigned long long)));
+        CK(cudaMallocHost((void**)&b->hmax, count * sizeof(unsigned long long)));
+        size_t off = 0;
+        for (uint32_t i = 0; i < count; i++) {
+            snaps[i] = b->snap + off;
+            off += b->lat[i]->n;
+        }
+        CK(cudaMemcpyAsync(b->dP, P.data(), count * sizeof(Params), cudaMemcpyHostToDevice, b->stream));
+        CK(cudaMemcpyAsync(b->dsnap, snaps.data(), count * sizeof(double*), cudaMemcpyHostToDevice, b->stream));
+        CK(cudaStreamSynchronize(b->stream));
+        return 0;
+    };
+    if (int rc = setup()) {
+        batch_free(b);
+        delete b;
+        return rc;
+    }
+    *out = b;
+    return 0;
+}
+
+int mplb_batch_destroy(mplb_batch_t* b) {
+    if (!b) return 0;
+    DeviceGuard guard(b->dev);
+    cudaStreamSynchronize(b->stream);
+    batch_free(b);
+    delete b;
+    return 0;
+}
+
+int mplb_batch_info_get(mplb_batch_t* b, mplb_batch_info* info) {
+    if (!b || !info) return fail(MPLB_E_ARG, "NULL argument");
+    std::memset(info, 0, sizeof(*info));
+    info->n_lattices = (uint32_t)b->lat.size();
+    info->nodes = b->nodes;
+    info->tile_config = b->cfg;
+    info->n_candidates = mplb_batch_ncfg();
+    for (int c = 0; c < mplb_batch_ncfg() && c < 8; c++) {
+        int tx = 0, ty = 0;
+        mplb_batch_cfg(c, &tx, &ty);
+        info->tile_x[c] = tx;
+        info->tile_y[c] = ty;
+        info->tile_ms[c] = b->tile_ms[c];
+    }
+    info->grid = b->grid;
+    info->kernel_launches = b->launches;
+    info->graph_launches = b->graph_launches;
+    return 0;
+}
+
+int mplb_batch_step(mplb_batch_t* b, uint32_t nsteps) {
+    if (!b) return fail(MPLB_E_ARG, "NULL batch");
+    if (nsteps == 0) return 0;
+    DeviceGuard guard(b->dev);
+    RET(batch_enter(b));
+    const std::vector<char> all(b->lat.size(), 1);
+    int nt = 0;
+    RET(batch_ready(b, all, &nt));
+    for (uint32_t s = 0; s < nsteps; s++) RET(batch_launch(b, b->cfg, b->grid, (int)(s & 1)));
+    for (mplb_gpu* h : b->lat) {
+        if (nsteps & 1) h->cur32[0] ^= 1;
+        h->current += nsteps;
+    }
+    return batch_leave(b);
+}
+
+int mplb_batch_run(mplb_batch_t* b, uint32_t max_steps, uint32_t* steps_out, double* rate_out,
+                   uint32_t* n_converged) {
+    if (!b) return fail(MPLB_E_ARG, "NULL batch");
+    DeviceGuard guard(b->dev);
+    const size_t N = b->lat.size();
+    RET(batch_enter(b));
+    std::vector<char> active(N, 1);
+    std::vector<uint32_t> steps(N, 0);
+    std::vector<double> rate(N, -1.0);
+    int nt = 0;
+    RET(batch_ready(b, active, &nt));
+    RET(batch_graph(b));
+    RET(batch_check(b, 0));  // snapshot of the starting rho
+    size_t left = N;
+    uint32_t done = 0, conv = 0;
+    while (left && done < max_steps) {
+        CK(cudaGraphLaunch(b->graph, b->stream));
+        b->graph_launches++;
+        b->launches += b->K + 1;
+        CK(cudaMemcpyAsync(b->hmax, b->dmax, N * sizeof(unsigned long long), cudaMemcpyDeviceToHost, b->stream));
+        CK(cudaStreamSynchronize(b->stream));
+        done += b->K;
+        bool retired = false;
+        for (size_t i = 0; i < N; i++) {
+            if (!active[i]) continue;
+            steps[i] += b->K;
+            double d;
+            std::memcpy(&d, &b->hmax[i], sizeof(double));
+            rate[i] = d / b->K;
+            if (rate[i] < b->tol) {
+                active[i] = 0;
+                left--;
+                conv++;
+                retired = true;
+            }
+        }
+        if (retired && left) RET(batch_table(b, b->cfg, active, &nt));
+    }
+    for (size_t i = 0; i < N; i++) {
+        b->lat[i]->current += steps[i];
+        if (steps_out) steps_out[i] = steps[i];
+        if (rate_out) rate_out[i] = rate[i];
+    }
+    if (n_converged) *n_converged = conv;
+    return batch_leave(b);
 }
 
 }  // extern "C"
