@@ -210,6 +210,24 @@ int mplb_gpu_average_rho0(mplb_gpu_t* h, double* rho_0);
  * nodes, FP64 warp-shuffle tree reduction (not the reference's summation order). */
 int mplb_gpu_mass_energy(mplb_gpu_t* h, double* mass, double* energy);
 
+/* Equilibrium and mass monitor without leaving the fused state (no rebuild
+ * of the reference state, unlike mass_energy): node density = mass of the
+ * current populations (FP64 sum; for MPLB_FP32_DEV the FP32 sum of
+ * deviations + the reference density).  *max_drho: largest change of a node
+ * density since the previous monitor call (0 when reset != 0 or at the first
+ * call); *mass: sum over nodes in a fixed order (deterministic).  Either
+ * pointer may be NULL.  Needs an updated flow field. */
+int mplb_gpu_monitor(mplb_gpu_t* h, int32_t reset, double* max_drho, double* mass);
+
+/* Step to equilibrium.  The reference's driver (src/app/multiPhasePP.c)
+ * runs a fixed number of steps; this runs whole intervals of check_interval
+ * steps until max over nodes |rho(t) - rho(t - K)| / K < tol, or max_steps
+ * (rounded up to a whole interval).  rho is monitored as by mplb_gpu_monitor,
+ * one read pass per check.  *steps: steps taken; *rate:
+ * the last max |drho/dt| (either may be NULL).  Needs an updated flow field. */
+int mplb_gpu_run_to_equilibrium(mplb_gpu_t* h, uint32_t max_steps, uint32_t check_interval, double tol,
+                                uint32_t* steps, double* rate);
+
 /* Wait for the handle's stream. */
 int mplb_gpu_sync(mplb_gpu_t* h);
 

@@ -69,6 +69,9 @@ def load_library(path=LIB_PATH):
         "mplb_gpu_average_rho0": ([H, D], C.c_int),
         "mplb_gpu_mass_energy": ([H, D, D], C.c_int),
         "mplb_gpu_sync": ([H], C.c_int),
+        "mplb_gpu_monitor": ([H, C.c_int32, D, D], C.c_int),
+        "mplb_gpu_run_to_equilibrium": ([H, C.c_uint32, C.c_uint32, C.c_double, C.POINTER(C.c_uint32), D],
+                                        C.c_int),
         "mplb_batch_create": ([C.POINTER(H), C.c_uint32, C.POINTER(abi.BatchOpts), C.POINTER(H)], C.c_int),
         "mplb_batch_destroy": ([H], C.c_int),
         "mplb_batch_info_get": ([H, C.POINTER(abi.BatchInfo)], C.c_int),
@@ -211,6 +214,20 @@ class Lattice:
         r = C.c_double()
         self._check(self.lib.mplb_gpu_average_rho0(self.h, C.byref(r)))
         return r.value
+
+    def monitor(self, reset=False):
+        """(max |drho| since the previous call, total mass), from the current populations."""
+        d, m = C.c_double(), C.c_double()
+        self._check(self.lib.mplb_gpu_monitor(self.h, 1 if reset else 0, C.byref(d), C.byref(m)))
+        return d.value, m.value
+
+    def run_to_equilibrium(self, max_steps, check_interval=1000, tol=1e-9):
+        """Step until max |drho/dt| < tol (whole check intervals); returns (steps, rate)."""
+        st = C.c_uint32()
+        r = C.c_double()
+        self._check(self.lib.mplb_gpu_run_to_equilibrium(self.h, max_steps, check_interval, tol, C.byref(st),
+                                                         C.byref(r)))
+        return st.value, r.value
 
     def mass_energy(self):
         m, e = C.c_double(), C.c_double()

@@ -100,6 +100,7 @@ struct mplb_gpu {
     float* p32[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};  // FP32 deviations [field][buffer]
     int cur32[2] = {0, 0};
     double rho_ref = 0, T_ref = 0;
+    double* snap = nullptr;  // equilibrium monitor: density at the last check
     int tile_request = 0;  // mplb_opts.tile_config
     uint32_t current = 0;
     uint64_t launches = 0;
@@ -130,6 +131,58 @@ void free_all(mplb_gpu* h) {
     for (int i = 0; i < 2; i++)
         for (int j = 0; j < 2; j++)
             if (h->p32[i][j]) cudaFree(h->p32[i][j]);
+    if (h->snap) cudaFree(h->snap);
+}
+
+// Equilibrium monitor.  Per node the mass of the current populations, sum
+// over k: after a fused step these are post-collision (the collision
+// conserves mass, so the sum is the node's density), on the operator path
+// post-streaming (the sum is what macroDensity computes).  Per block: the
+// largest change against the snapshot of the previous call and the block's
+// mass; the snapshot is refreshed.  Fixed grid and order: deterministic.
+template <class T>
+__global__ void k_monitor_partial(uint32_t n, int Q, const T* __restrict__ f, double ref, double* __restrict__ snap,
+                                  int first, double* __restrict__ partials) {
+    double m = 0.0, mass = 0.0;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        T s = 0;
+        for (int k = 0; k < Q; k++) s += f[(size_t)k * n + i];
+        const double r = ref + (double)s;
+        if (!first) m = fmax(m, fabs(r - snap[i]));
+        snap[i] = r;
+        mass += r;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        m = fmax(m, __shfl_down_sync(0xffffffffu, m, o));
+        mass += __shfl_down_sync(0xffffffffu, mass, o);
+    }
+    __shared__ double sm[32], ss[32];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    if (lane == 0) {
+        sm[w] = m;
+        ss[w] = mass;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int j = 1; j < (int)((blockDim.x + 31) >> 5); j++) {
+            m = fmax(m, sm[j]);
+            mass += ss[j];
+        }
+        partials[2 * blockIdx.x] = m;
+        partials[2 * blockIdx.x + 1] = mass;
+    }
+}
+
+__global__ void k_monitor_final(int nparts, const double* __restrict__ partials, double* __restrict__ out) {
+    if (threadIdx.x != 0) return;
+    double m = 0.0, mass = 0.0;
+    for (int b = 0; b < nparts; b++) {
+        m = fmax(m, partials[2 * b]);
+        mass += partials[2 * b + 1];
+    }
+    out[0] = m;
+    out[1] = mass;
 }
 
 // Lattice tables on the host, the same way the reference defines them
@@ -1014,6 +1067,62 @@ int mplb_gpu_mass_energy(mplb_gpu_t* h, double* mass, double* energy) {
     CK(cudaStreamSynchronize(h->stream));
     if (mass) *mass = r[0];
     if (energy) *energy = r[1];
+    return 0;
+}
+
+int mplb_gpu_monitor(mplb_gpu_t* h, int32_t reset, double* max_drho, double* mass) {
+    if (!h) return fail(MPLB_E_ARG, "NULL handle");
+    if (!h->P.f_update || h->model[0] == MPLB_NO_MODEL)
+        return fail(MPLB_E_UNSUPPORTED, "the monitor needs an updated flow field");
+    DeviceGuard guard(h->dev);
+    if (!h->snap) {
+        RET(dalloc(h, &h->snap, h->n));
+        reset = 1;
+    }
+    const int parts = std::min<int>(h->red_parts, (int)blocks(h->n));
+    double* out = h->red + 2 * (size_t)h->red_parts + 4;
+    if (h->path == MPLB_PATH_FUSED && h->precision == MPLB_FP32_DEV) {
+        if (h->fstate == 0) RET(prologue32(h));
+        k_monitor_partial<float><<<parts, TPB, 0, h->stream>>>(h->n, h->Q, h->p32[0][h->cur32[0]], h->rho_ref,
+                                                               h->snap, reset, h->red);
+    } else {
+        if (h->path == MPLB_PATH_FUSED && h->fstate == 0) {
+            RET(DISPATCH(h, op_collision, h, 0));
+            RET(DISPATCH(h, op_collision, h, 1));
+            h->fstate = 1;
+        }
+        k_monitor_partial<double><<<parts, TPB, 0, h->stream>>>(h->n, h->Q, h->F(), 0.0, h->snap, reset, h->red);
+    }
+    h->launches++;
+    RET(launch_check(h));
+    k_monitor_final<<<1, 32, 0, h->stream>>>(parts, h->red, out);
+    h->launches++;
+    RET(launch_check(h));
+    double r[2] = {0, 0};
+    CK(cudaMemcpyAsync(r, out, sizeof(r), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    if (max_drho) *max_drho = reset ? 0.0 : r[0];
+    if (mass) *mass = r[1];
+    return 0;
+}
+
+int mplb_gpu_run_to_equilibrium(mplb_gpu_t* h, uint32_t max_steps, uint32_t check_interval, double tol,
+                                uint32_t* steps, double* rate) {
+    if (!h) return fail(MPLB_E_ARG, "NULL handle");
+    if (check_interval == 0) return fail(MPLB_E_ARG, "check_interval must be >= 1");
+    double d = 0;
+    RET(mplb_gpu_monitor(h, 1, &d, nullptr));
+    uint32_t done = 0;
+    double r = -1.0;
+    while (done < max_steps) {
+        RET(mplb_gpu_step(h, check_interval));
+        done += check_interval;
+        RET(mplb_gpu_monitor(h, 0, &d, nullptr));
+        r = d / check_interval;
+        if (r < tol) break;
+    }
+    if (steps) *steps = done;
+    if (rate) *rate = r;
     return 0;
 }
 

@@ -1,0 +1,154 @@
+"""Time to equilibrium of static-bubble ensembles (D2Q9, Carnahan-Starling).
+
+    python -m multiphaselb_b200.ensemble [--cases N] [--plain M] [--init tanh|mlp] ...
+
+The ensemble: N independent fully periodic D2Q9 bubbles; lattice size L drawn
+uniformly from {64, 96, 128, 192, 256, 384, 512} (L x L), T/Tc uniform in
+[0.6, 0.95], bubble radius uniform in [8, 0.3 L]; CS EOS a = 1, b = 4, the
+Li-MRT relaxation of the static-bubble workload, tanh width 5.  A case is at
+equilibrium when max over nodes |drho/dt| < tol, measured over one check
+interval of K steps.
+
+Two ways to get there are timed:
+
+* plain: each case alone, FP64, fused path, tanh/Maxwell initial profile,
+  one case after the other (mplb_gpu_run_to_equilibrium);
+* batched: all cases as FP32-deviation lattices advanced together
+  (mplb_batch_run), initial profile from the tanh/Maxwell formula or from the
+  learned warm start (multiphaselb_b200.warmstart).
+
+The report gives per-case steps, the coexistence densities (rho at the bubble
+centre and at the corner farthest from it) of both runs and their relative
+difference, and the wall times.  Seeded; no dataset.
+"""
+import argparse
+import json
+import sys
+import time
+
+import numpy as np
+
+from . import Batch, Lattice, abi, cases
+
+SIZES = (64, 96, 128, 192, 256, 384, 512)
+SEED = 20240611
+WIDTH = 5.0
+
+
+def draw(n, seed=SEED):
+    """n case specs (L, T/Tc, R), seeded."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    L = rng.choice(np.array(SIZES), size=n)
+    t = rng.uniform(0.6, 0.95, size=n)
+    R = rng.uniform(8.0, 0.3 * L)
+    return [dict(L=int(a), t_ratio=float(b), radius=float(c)) for a, b, c in zip(L, t, R)]
+
+
+def make_case(spec, init=None):
+    c = cases.bubble_case(abi.D2Q9, L=spec["L"], radius=spec["radius"], width=WIDTH, t_ratio=spec["t_ratio"],
+                          name=f"bubble_d2q9_{spec['L']}_t{spec['t_ratio']:.3f}_r{spec['radius']:.1f}")
+    if init is not None:
+        c.rho = np.ascontiguousarray(init(c), dtype=np.float64)
+    return c
+
+
+def coexistence(case, rho):
+    """rho at the bubble centre (vapour) and at the corner farthest from it (liquid)."""
+    nx, ny = case.dims
+    cx, cy = nx // 2, ny // 2
+    return float(rho[cx + nx * cy]), float(rho[0])
+
+
+def run_plain(specs, K, tol, max_steps, log=None):
+    out = []
+    for i, s in enumerate(specs):
+        c = make_case(s)
+        with Lattice(c, path=abi.PATH_FUSED, precision=abi.FP64) as lat:
+            lat.upload_case()
+            lat.initialize()
+            lat.sync()
+            t0 = time.perf_counter()
+            steps, rate = lat.run_to_equilibrium(max_steps, K, tol)
+            lat.sync()
+            wall = time.perf_counter() - t0
+            rv, rl = coexistence(c, lat.download()["rho"])
+        out.append(dict(steps=steps, rate=rate, wall_s=wall, rho_v=rv, rho_l=rl))
+        if log:
+            log(f"plain {i} L={s['L']} t={s['t_ratio']:.3f} R={s['radius']:.1f}: {steps} steps {wall:.2f} s")
+    return out
+
+
+def run_batched(specs, K, tol, max_steps, init=None, tile_config=0):
+    t0 = time.perf_counter()
+    cs = [make_case(s, init) for s in specs]
+    lats = []
+    for c in cs:
+        lat = Lattice(c, path=abi.PATH_FUSED, precision=abi.FP32_DEV)
+        lat.upload_case()
+        lat.initialize()
+        lats.append(lat)
+    for lat in lats:
+        lat.sync()
+    setup = time.perf_counter() - t0
+    with Batch(lats, check_interval=K, tol=tol, tile_config=tile_config) as b:
+        t0 = time.perf_counter()
+        steps, rate, conv = b.run(max_steps)
+        lats[0].sync()
+        wall = time.perf_counter() - t0
+        info = b.info()
+    res = []
+    for c, lat, st, r in zip(cs, lats, steps, rate):
+        rv, rl = coexistence(c, lat.download()["rho"])
+        res.append(dict(steps=int(st), rate=float(r), rho_v=rv, rho_l=rl))
+        lat.close()
+    return dict(cases=res, wall_s=wall, setup_s=setup, converged=conv, info=info,
+                nodes=int(sum(c.n for c in cs)))
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--cases", type=int, default=512)
+    ap.add_argument("--plain", type=int, default=16, help="first M cases also run plain (FP64, one by one)")
+    ap.add_argument("--seed", type=int, default=SEED)
+    ap.add_argument("--tol", type=float, default=1e-9)
+    ap.add_argument("--check", type=int, default=1000)
+    ap.add_argument("--max-steps", type=int, default=400000)
+    ap.add_argument("--init", choices=("tanh", "mlp"), default="tanh")
+    ap.add_argument("--sizes", default=None, help="comma list: one case per size at T/Tc=0.8, R=0.2L")
+    ap.add_argument("--out", default=None)
+    a = ap.parse_args(argv)
+    if a.sizes:
+        specs = [dict(L=int(x), t_ratio=0.8, radius=0.2 * int(x)) for x in a.sizes.split(",")]
+    else:
+        specs = draw(a.cases, a.seed)
+    init = None
+    if a.init == "mlp":
+        from . import warmstart
+        init = warmstart.initializer(abi.D2Q9)
+    log = lambda m: print(m, file=sys.stderr, flush=True)  # noqa: E731
+    rep = dict(specs=specs, tol=a.tol, check_interval=a.check, max_steps=a.max_steps, init=a.init)
+    b = run_batched(specs, a.check, a.tol, a.max_steps, init)
+    rep["batched"] = b
+    log(f"batched: {b['converged']}/{len(specs)} converged, {b['wall_s']:.2f} s, steps max {max(c['steps'] for c in b['cases'])}")
+    m = min(a.plain, len(specs))
+    if m:
+        p = run_plain(specs[:m], a.check, a.tol, a.max_steps, log)
+        rep["plain"] = p
+        sub = run_batched(specs[:m], a.check, a.tol, a.max_steps, init)
+        rep["batched_subset"] = sub
+        rel = [max(abs(x["rho_v"] - y["rho_v"]) / y["rho_v"], abs(x["rho_l"] - y["rho_l"]) / y["rho_l"])
+               for x, y in zip(sub["cases"], p)]
+        rep["subset"] = dict(cases=m, plain_wall_s=sum(x["wall_s"] for x in p), batched_wall_s=sub["wall_s"],
+                             speedup=sum(x["wall_s"] for x in p) / sub["wall_s"], max_rel_coexistence=max(rel))
+        log(json.dumps(rep["subset"]))
+    txt = json.dumps(rep, indent=1)
+    if a.out:
+        with open(a.out, "w") as fh:
+            fh.write(txt + "\n")
+    else:
+        print(txt)
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())
