@@ -188,18 +188,21 @@ def _maxwell_densities(eos, T):
     plo, phi = max(p[i_min], 1e-14), p[i_max]
 
     def roots(P):
-        rv = _bisect(lambda r: p_eos(eos, r, T) - P, rho[0], rho[i_max])
+        # p(0) = 0 < P: the vapour root may lie below the grid's first point
+        rv = _bisect(lambda r: p_eos(eos, r, T) - P, 0.0, rho[i_max], it=200)
         rl = _bisect(lambda r: p_eos(eos, r, T) - P, rho[i_min], rho[-1])
         return rv, rl
 
     def area(P):
-        # split at the spinodals so each Gauss-Legendre piece is smooth
+        # split at the spinodals so each Gauss-Legendre piece is smooth, and
+        # integrate in s = ln v (dv = v ds): at low T the vapour volume is
+        # orders of magnitude above the liquid's and p ~ RT/v there
         rv, rl = roots(P)
-        knots = [1.0 / rl, 1.0 / rho[i_min], 1.0 / rho[i_max], 1.0 / rv]
+        knots = np.log([1.0 / rl, 1.0 / rho[i_min], 1.0 / rho[i_max], 1.0 / rv])
         tot = 0.0
         for a, b in zip(knots[:-1], knots[1:]):
-            v = 0.5 * (b - a) * _GL_X + 0.5 * (a + b)
-            tot += 0.5 * (b - a) * np.dot(_GL_W, p_eos(eos, 1.0 / v, T) - P)
+            v = np.exp(0.5 * (b - a) * _GL_X + 0.5 * (a + b))
+            tot += 0.5 * (b - a) * np.dot(_GL_W, (p_eos(eos, 1.0 / v, T) - P) * v)
         return tot
 
     P = _bisect(area, plo, phi, it=80)
