@@ -20,7 +20,8 @@ LIB = os.path.join(LIB_DIR, "libmplb_gpu.so")
 # the FP32-deviation path may.
 SOURCES = [(os.path.join(HERE, "csrc", "mplb_gpu.cu"), False),
            (os.path.join(HERE, "csrc", "mplb_noalloc.cu"), False),
-           (os.path.join(HERE, "csrc", "mplb_fp32.cu"), True)]
+           (os.path.join(HERE, "csrc", "mplb_fp32.cu"), True),
+           (os.path.join(HERE, "csrc", "mplb_mlp.cu"), False)]
 HEADERS = [os.path.join(HERE, "csrc", f) for f in ("lattice.cuh", "ops.cuh", "fused.cuh", "fused_host.cuh", "fused32.cuh")] + \
           [os.path.join(ROOT, "include", "mplb_gpu.h")]
 

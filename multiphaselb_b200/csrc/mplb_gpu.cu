@@ -28,6 +28,11 @@ cudaError_t mplb_fused32_launch(int lat, bool has_bc, bool f_on, bool g_on, bool
                                 cudaStream_t s);
 cudaError_t mplb_to_dev32(uint32_t n, int Q, const double* src, float* dst, const FusedArgs32& B, int heat,
                           cudaStream_t s);
+// Learned warm start (mplb_mlp.cu).
+int mplb_mlp_bubble_launch(mplb_mlp* m, double* rho, uint32_t n, int nx, int ny, const double* c, double R,
+                           double t_ratio, double a, double b, cudaStream_t s);
+int mplb_mlp_device(const mplb_mlp* m);
+
 // Batched ensemble kernels (mplb_fp32.cu).
 int mplb_batch_ncfg();
 void mplb_batch_cfg(int c, int* tx, int* ty);
@@ -132,6 +137,11 @@ void free_all(mplb_gpu* h) {
         for (int j = 0; j < 2; j++)
             if (h->p32[i][j]) cudaFree(h->p32[i][j]);
     if (h->snap) cudaFree(h->snap);
+}
+
+__global__ void k_fill(uint32_t n, double v, double* __restrict__ x) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) x[i] = v;
 }
 
 // Equilibrium monitor.  Per node the mass of the current populations, sum
@@ -1123,6 +1133,26 @@ int mplb_gpu_run_to_equilibrium(mplb_gpu_t* h, uint32_t max_steps, uint32_t chec
     }
     if (steps) *steps = done;
     if (rate) *rate = r;
+    return 0;
+}
+
+int mplb_mlp_init_bubble(mplb_mlp_t* m, mplb_gpu_t* h, double t_ratio, const double* center, double radius,
+                         double T) {
+    if (!m || !h || !center) return fail(MPLB_E_ARG, "NULL argument");
+    if (!(radius > 0.0)) return fail(MPLB_E_ARG, "radius must be positive");
+    if (!h->box) return fail(MPLB_E_UNSUPPORTED, "warm start needs a box lattice");
+    if (h->P.eos != MPLB_EOS_CS) return fail(MPLB_E_UNSUPPORTED, "warm start is trained on the Carnahan-Starling EOS");
+    if (mplb_mlp_device(m) != h->dev) return fail(MPLB_E_ARG, "network and lattice on different devices");
+    DeviceGuard guard(h->dev);
+    RET(materialize(h));
+    RET(mplb_mlp_bubble_launch(m, h->rho, h->n, h->dims[0], h->dims[1], center, radius, t_ratio, h->P.a, h->P.b,
+                               h->stream));
+    h->launches++;
+    CK(cudaMemsetAsync(h->U, 0, 3 * (size_t)h->n * sizeof(double), h->stream));
+    k_fill<<<blocks(h->n), TPB, 0, h->stream>>>(h->n, T, h->T);
+    h->launches++;
+    RET(launch_check(h));
+    h->initialized = false;
     return 0;
 }
 

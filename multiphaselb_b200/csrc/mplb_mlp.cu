@@ -1,0 +1,621 @@
+// mplb_mlp.cu -- learned warm start: a 4-64-64-64-1 tanh network that maps
+// (T/Tc, a, b, r/R) to the equilibrium density of a static bubble, trained
+// on the GPU on density profiles the solver itself converged.
+//
+// Precision: weights and activations are BF16 (round-to-nearest-even of the
+// FP32 value), every dot product accumulates in FP32 with fmaf in a fixed
+// order, biases, gradients and the Adam state are FP32.  The master weights
+// are FP32; the BF16 copy is refreshed after every update.
+//
+// Kernels (CUDA cores): at 64 units a layer is a 64 x 64 matrix, far below a
+// tensor-core tile's useful size; one block of 64 threads (thread j = unit j)
+// carries SB samples through all layers with the weights in shared memory.
+// Training writes per-block gradient partials that a second kernel sums in a
+// fixed order (deterministic) and feeds to Adam.
+//
+// This translation unit is compiled without FMA contraction: the feature
+// normalisation below runs on host and device and must agree bit for bit.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/mplb_gpu.h"
+
+int mplb_internal_fail(int code, const std::string& msg);
+
+namespace {
+
+constexpr int NIN = 4, NH = 64;
+constexpr int OFF_W1 = 0, OFF_B1 = OFF_W1 + NH * NIN, OFF_W2 = OFF_B1 + NH, OFF_B2 = OFF_W2 + NH * NH,
+              OFF_W3 = OFF_B2 + NH, OFF_B3 = OFF_W3 + NH * NH, OFF_W4 = OFF_B3 + NH, OFF_B4 = OFF_W4 + NH,
+              NPARAM = OFF_B4 + 1;
+static_assert(NPARAM == MPLB_MLP_PARAMS, "parameter layout");
+constexpr int SB = 32;        // samples per block
+constexpr int WS = NH + 1;    // padded row stride of the weight tiles (bank-conflict free)
+
+// ---------------------------------------------------------------- features
+__host__ __device__ inline uint32_t f2u(float f) {
+#ifdef __CUDA_ARCH__
+    return __float_as_uint(f);
+#else
+    uint32_t u;
+    std::memcpy(&u, &f, 4);
+    return u;
+#endif
+}
+__host__ __device__ inline float u2f(uint32_t u) {
+#ifdef __CUDA_ARCH__
+    return __uint_as_float(u);
+#else
+    float f;
+    std::memcpy(&f, &u, 4);
+    return f;
+#endif
+}
+// Round to the nearest BF16 value, ties to even (finite inputs).
+__host__ __device__ inline float bf16_round(float f) {
+    uint32_t u = f2u(f);
+    u += 0x7FFFu + ((u >> 16) & 1u);
+    return u2f(u & 0xFFFF0000u);
+}
+__host__ __device__ inline uint16_t bf16_bits(float f) { return (uint16_t)(f2u(bf16_round(f)) >> 16); }
+__device__ inline float bf16_float(uint16_t b) { return __uint_as_float((uint32_t)b << 16); }
+
+// Network inputs: T/Tc centred on the trained range [0.6, 0.95], the CS
+// constants relative to a = 1, b = 4, and r/R clamped to [0, 3] (beyond
+// three radii the profile is bulk liquid).  Rounded to BF16 (they are GEMM
+// operands).  Output: b * rho.
+__host__ __device__ inline void features(double t_ratio, double a, double b, double r_over_R, float* x) {
+    const double r = r_over_R < 0.0 ? 0.0 : (r_over_R > 3.0 ? 3.0 : r_over_R);
+    x[0] = bf16_round((float)((t_ratio - 0.775) / 0.175));
+    x[1] = bf16_round((float)(a - 1.0));
+    x[2] = bf16_round((float)(b * 0.25 - 1.0));
+    x[3] = bf16_round((float)((r - 1.5) / 1.5));
+}
+
+// ------------------------------------------------------------ block state
+struct Block {
+    float W1[NH * NIN], b1[NH], W2[NH * WS], b2[NH], W3[NH * WS], b3[NH], W4[NH], b4;
+    float x[SB][NIN], h1[SB][NH], h2[SB][NH], h3[SB][NH], out[SB], dout[SB];
+    float dzA[SB][NH], dzB[SB][NH];
+};
+
+__device__ void load_weights(Block& s, const float* __restrict__ P, const uint16_t* __restrict__ Wb) {
+    const int t = threadIdx.x;
+    for (int i = t; i < NH * NIN; i += blockDim.x) s.W1[i] = bf16_float(Wb[OFF_W1 + i]);
+    for (int i = t; i < NH * NH; i += blockDim.x) {
+        const int r = i / NH, c = i % NH;
+        s.W2[r * WS + c] = bf16_float(Wb[OFF_W2 + i]);
+        s.W3[r * WS + c] = bf16_float(Wb[OFF_W3 + i]);
+    }
+    for (int i = t; i < NH; i += blockDim.x) {
+        s.b1[i] = P[OFF_B1 + i];
+        s.b2[i] = P[OFF_B2 + i];
+        s.b3[i] = P[OFF_B3 + i];
+        s.W4[i] = bf16_float(Wb[OFF_W4 + i]);
+    }
+    if (t == 0) s.b4 = P[OFF_B4];
+}
+
+// Forward pass of the block's samples; thread j = hidden unit j, then
+// thread s < SB = sample s for the output unit.
+__device__ void forward(Block& s) {
+    const int j = threadIdx.x;
+    for (int q = 0; q < SB; q++) {
+        float z = s.b1[j];
+#pragma unroll
+        for (int i = 0; i < NIN; i++) z = fmaf(s.W1[j * NIN + i], s.x[q][i], z);
+        s.h1[q][j] = bf16_round(tanhf(z));
+    }
+    __syncthreads();
+    for (int q = 0; q < SB; q++) {
+        float z = s.b2[j];
+#pragma unroll 16
+        for (int i = 0; i < NH; i++) z = fmaf(s.W2[j * WS + i], s.h1[q][i], z);
+        s.h2[q][j] = bf16_round(tanhf(z));
+    }
+    __syncthreads();
+    for (int q = 0; q < SB; q++) {
+        float z = s.b3[j];
+#pragma unroll 16
+        for (int i = 0; i < NH; i++) z = fmaf(s.W3[j * WS + i], s.h2[q][i], z);
+        s.h3[q][j] = bf16_round(tanhf(z));
+    }
+    __syncthreads();
+    if (j < SB) {
+        float z = s.b4;
+#pragma unroll 16
+        for (int i = 0; i < NH; i++) z = fmaf(s.W4[i], s.h3[j][i], z);
+        s.out[j] = z;
+    }
+    __syncthreads();
+}
+
+__device__ inline uint32_t mix32(uint32_t x) {
+    x ^= x >> 16;
+    x *= 0x7feb352dU;
+    x ^= x >> 15;
+    x *= 0x846ca68bU;
+    x ^= x >> 16;
+    return x;
+}
+
+// Sample q of this block: batch entry `e`, drawn from the data set by a
+// counter-based hash of (seed, step, e), or entry e itself (full pass).
+__device__ inline uint32_t pick(uint32_t e, uint32_t ndata, uint32_t seed, uint32_t step, int draw) {
+    if (!draw) return e;
+    return mix32(mix32(seed ^ 0x9e3779b9u * (step + 1)) ^ (e * 0x85ebca6bu)) % ndata;
+}
+
+// Forward + backward of one batch; per-block gradient partials.
+__global__ void __launch_bounds__(NH) k_mlp_grad(const float* __restrict__ P, const uint16_t* __restrict__ Wb,
+                                                 const float* __restrict__ X, const float* __restrict__ Y,
+                                                 uint32_t ndata, uint32_t nbatch, int draw, uint32_t seed,
+                                                 uint32_t step, float inv_n, float* __restrict__ partial,
+                                                 double* __restrict__ loss_partial) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    Block& s = *reinterpret_cast<Block*>(smem_raw);
+    const int j = threadIdx.x;
+    load_weights(s, P, Wb);
+    const uint32_t base = blockIdx.x * SB;
+    __shared__ float ys[SB];
+    __shared__ int valid[SB];
+    if (j < SB) {
+        const uint32_t e = base + j;
+        valid[j] = e < nbatch;
+        const uint32_t id = e < nbatch ? pick(e, ndata, seed, step, draw) : 0;
+#pragma unroll
+        for (int i = 0; i < NIN; i++) s.x[j][i] = e < nbatch ? X[(size_t)id * NIN + i] : 0.f;
+        ys[j] = e < nbatch ? Y[id] : 0.f;
+    }
+    __syncthreads();
+    forward(s);
+    // loss and output gradient: L = (1/n) sum (out - y)^2
+    if (j < SB) {
+        const float d = valid[j] ? s.out[j] - ys[j] : 0.f;
+        s.dout[j] = 2.f * d * inv_n;
+        s.out[j] = d * d;
+    }
+    __syncthreads();
+    float* g = partial + (size_t)blockIdx.x * NPARAM;
+    if (j == 0) {
+        double l = 0.0, db4 = 0.0;
+        for (int q = 0; q < SB; q++) {
+            l += (double)s.out[q];
+            db4 += (double)s.dout[q];
+        }
+        loss_partial[blockIdx.x] = l;
+        g[OFF_B4] = (float)db4;
+    }
+    // layer 4
+    {
+        float acc = 0.f;
+        for (int q = 0; q < SB; q++) acc = fmaf(s.dout[q], s.h3[q][j], acc);
+        g[OFF_W4 + j] = acc;
+        for (int q = 0; q < SB; q++) {
+            const float h = s.h3[q][j];
+            s.dzA[q][j] = s.dout[q] * s.W4[j] * (1.f - h * h);
+        }
+    }
+    __syncthreads();
+    // layer 3: dW3 row j, db3, then dz2 = (W3^T dz3) * (1 - h2^2) (column j)
+    {
+        float acc[NH];
+#pragma unroll
+        for (int i = 0; i < NH; i++) acc[i] = 0.f;
+        float bacc = 0.f;
+        for (int q = 0; q < SB; q++) {
+            const float d = s.dzA[q][j];
+            bacc += d;
+#pragma unroll
+            for (int i = 0; i < NH; i++) acc[i] = fmaf(d, s.h2[q][i], acc[i]);
+        }
+#pragma unroll
+        for (int i = 0; i < NH; i++) g[OFF_W3 + j * NH + i] = acc[i];
+        g[OFF_B3 + j] = bacc;
+        for (int q = 0; q < SB; q++) {
+            float t = 0.f;
+#pragma unroll 16
+            for (int r = 0; r < NH; r++) t = fmaf(s.W3[r * WS + j], s.dzA[q][r], t);
+            const float h = s.h2[q][j];
+            s.dzB[q][j] = t * (1.f - h * h);
+        }
+    }
+    __syncthreads();
+    // layer 2
+    {
+        float acc[NH];
+#pragma unroll
+        for (int i = 0; i < NH; i++) acc[i] = 0.f;
+        float bacc = 0.f;
+        for (int q = 0; q < SB; q++) {
+            const float d = s.dzB[q][j];
+            bacc += d;
+#pragma unroll
+            for (int i = 0; i < NH; i++) acc[i] = fmaf(d, s.h1[q][i], acc[i]);
+        }
+#pragma unroll
+        for (int i = 0; i < NH; i++) g[OFF_W2 + j * NH + i] = acc[i];
+        g[OFF_B2 + j] = bacc;
+        for (int q = 0; q < SB; q++) {
+            float t = 0.f;
+#pragma unroll 16
+            for (int r = 0; r < NH; r++) t = fmaf(s.W2[r * WS + j], s.dzB[q][r], t);
+            const float h = s.h1[q][j];
+            s.dzA[q][j] = t * (1.f - h * h);
+        }
+    }
+    __syncthreads();
+    // layer 1
+    {
+        float acc[NIN] = {0.f, 0.f, 0.f, 0.f};
+        float bacc = 0.f;
+        for (int q = 0; q < SB; q++) {
+            const float d = s.dzA[q][j];
+            bacc += d;
+#pragma unroll
+            for (int i = 0; i < NIN; i++) acc[i] = fmaf(d, s.x[q][i], acc[i]);
+        }
+#pragma unroll
+        for (int i = 0; i < NIN; i++) g[OFF_W1 + j * NIN + i] = acc[i];
+        g[OFF_B1 + j] = bacc;
+    }
+}
+
+// Sum of the block partials in block order; optionally one Adam step on the
+// FP32 master weights and a fresh BF16 copy.
+__global__ void k_mlp_reduce(const float* __restrict__ partial, int nblk, const double* __restrict__ loss_partial,
+                             float* __restrict__ P, float* __restrict__ M, float* __restrict__ V,
+                             uint16_t* __restrict__ Wb, float lr, float c1, float c2, int update,
+                             float* __restrict__ grad_out, double* __restrict__ loss_out) {
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p == 0) {
+        double l = 0.0;
+        for (int b = 0; b < nblk; b++) l += loss_partial[b];
+        *loss_out = l;
+    }
+    if (p >= NPARAM) return;
+    float gsum = 0.f;
+    for (int b = 0; b < nblk; b++) gsum += partial[(size_t)b * NPARAM + p];
+    if (grad_out) grad_out[p] = gsum;
+    if (!update) return;
+    constexpr float B1 = 0.9f, B2 = 0.999f, EPS = 1e-8f;
+    const float m = B1 * M[p] + (1.f - B1) * gsum;
+    const float v = B2 * V[p] + (1.f - B2) * gsum * gsum;
+    M[p] = m;
+    V[p] = v;
+    const float w = P[p] - lr * (m * c1) / (sqrtf(v * c2) + EPS);
+    P[p] = w;
+    Wb[p] = bf16_bits(w);
+}
+
+// Forward pass over arbitrary samples (features already normalised).
+__global__ void __launch_bounds__(NH) k_mlp_predict(const float* __restrict__ P, const uint16_t* __restrict__ Wb,
+                                                    const float* __restrict__ X, uint32_t n,
+                                                    float* __restrict__ Y) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    Block& s = *reinterpret_cast<Block*>(smem_raw);
+    const int j = threadIdx.x;
+    load_weights(s, P, Wb);
+    const uint32_t e = blockIdx.x * SB + j;
+    if (j < SB) {
+#pragma unroll
+        for (int i = 0; i < NIN; i++) s.x[j][i] = e < n ? X[(size_t)e * NIN + i] : 0.f;
+    }
+    __syncthreads();
+    forward(s);
+    if (j < SB && e < n) Y[e] = s.out[j];
+}
+
+// Initial density of a box lattice: node i at (i % nx, i / nx % ny, i / (nx ny)),
+// r = distance to the bubble centre, rho = network(T/Tc, a, b, r/R) / b.
+__global__ void __launch_bounds__(NH) k_mlp_bubble(const float* __restrict__ P, const uint16_t* __restrict__ Wb,
+                                                   uint32_t n, int nx, int ny, double cx, double cy, double cz,
+                                                   double R, double t_ratio, double a, double b,
+                                                   double* __restrict__ rho) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    Block& s = *reinterpret_cast<Block*>(smem_raw);
+    const int j = threadIdx.x;
+    load_weights(s, P, Wb);
+    const uint32_t e = blockIdx.x * SB + j;
+    if (j < SB) {
+        const uint32_t i = e < n ? e : 0;
+        const double x = (double)(i % (uint32_t)nx) - cx, y = (double)((i / (uint32_t)nx) % (uint32_t)ny) - cy,
+                     z = (double)(i / ((uint32_t)nx * (uint32_t)ny)) - cz;
+        features(t_ratio, a, b, sqrt(x * x + y * y + z * z) / R, s.x[j]);
+    }
+    __syncthreads();
+    forward(s);
+    if (j < SB && e < n) rho[e] = (double)s.out[j] / b;
+}
+
+constexpr size_t SMEM = sizeof(Block);
+
+int set_attrs() {
+    static std::once_flag once;
+    static cudaError_t err = cudaSuccess;
+    std::call_once(once, [] {
+        err = cudaFuncSetAttribute(k_mlp_grad, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM);
+        if (err == cudaSuccess)
+            err = cudaFuncSetAttribute(k_mlp_predict, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM);
+        if (err == cudaSuccess)
+            err = cudaFuncSetAttribute(k_mlp_bubble, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM);
+    });
+    return err == cudaSuccess ? 0 : mplb_internal_fail(MPLB_E_CUDA, std::string("MLP kernel attributes: ") +
+                                                                       cudaGetErrorString(err));
+}
+
+#define CKM(call)                                                                                   \
+    do {                                                                                            \
+        cudaError_t e_ = (call);                                                                    \
+        if (e_ != cudaSuccess) return mplb_internal_fail(MPLB_E_CUDA, std::string(#call) + ": " +   \
+                                                                          cudaGetErrorString(e_));  \
+    } while (0)
+
+struct DevGuard {
+    int prev = -1;
+    explicit DevGuard(int dev) {
+        cudaGetDevice(&prev);
+        if (prev != dev) cudaSetDevice(dev);
+    }
+    ~DevGuard() {
+        if (prev >= 0) cudaSetDevice(prev);
+    }
+};
+
+}  // namespace
+
+struct mplb_mlp {
+    int dev = 0;
+    cudaStream_t stream = nullptr;
+    float *P = nullptr, *M = nullptr, *V = nullptr;
+    uint16_t* Wb = nullptr;
+    float *X = nullptr, *Y = nullptr;
+    uint32_t ndata = 0, cap = 0;
+    float* partial = nullptr;
+    double* loss_partial = nullptr;
+    int nblk_cap = 0;
+    double* loss = nullptr;
+    float* grad = nullptr;
+    uint32_t seed = 0;
+    uint64_t step = 0;
+};
+
+namespace {
+
+void mlp_free(mplb_mlp* m) {
+    void* ps[] = {m->P, m->M, m->V, m->Wb, m->X, m->Y, m->partial, m->loss_partial, m->loss, m->grad};
+    for (void* p : ps)
+        if (p) cudaFree(p);
+    if (m->stream) cudaStreamDestroy(m->stream);
+}
+
+int ensure_blocks(mplb_mlp* m, int nblk) {
+    if (nblk <= m->nblk_cap) return 0;
+    if (m->partial) cudaFree(m->partial);
+    if (m->loss_partial) cudaFree(m->loss_partial);
+    m->partial = nullptr;
+    m->loss_partial = nullptr;
+    m->nblk_cap = 0;
+    CKM(cudaMalloc((void**)&m->partial, (size_t)nblk * NPARAM * sizeof(float)));
+    CKM(cudaMalloc((void**)&m->loss_partial, (size_t)nblk * sizeof(double)));
+    m->nblk_cap = nblk;
+    return 0;
+}
+
+int upload_params(mplb_mlp* m, const float* host) {
+    std::vector<uint16_t> b(NPARAM);
+    for (int i = 0; i < NPARAM; i++) b[i] = bf16_bits(host[i]);
+    CKM(cudaMemcpyAsync(m->P, host, NPARAM * sizeof(float), cudaMemcpyHostToDevice, m->stream));
+    CKM(cudaMemcpyAsync(m->Wb, b.data(), NPARAM * sizeof(uint16_t), cudaMemcpyHostToDevice, m->stream));
+    CKM(cudaMemsetAsync(m->M, 0, NPARAM * sizeof(float), m->stream));
+    CKM(cudaMemsetAsync(m->V, 0, NPARAM * sizeof(float), m->stream));
+    CKM(cudaStreamSynchronize(m->stream));
+    m->step = 0;
+    return 0;
+}
+
+// One pass: gradient over `nbatch` samples (drawn, or the first nbatch in
+// order), optionally followed by an Adam step.
+int pass(mplb_mlp* m, uint32_t nbatch, int draw, int update, float lr, float* grad_host, double* loss_host) {
+    const int nblk = (int)((nbatch + SB - 1) / SB);
+    if (int rc = ensure_blocks(m, nblk)) return rc;
+    k_mlp_grad<<<nblk, NH, SMEM, m->stream>>>(m->P, m->Wb, m->X, m->Y, m->ndata, nbatch, draw, m->seed,
+                                             (uint32_t)m->step, 1.f / (float)nbatch, m->partial, m->loss_partial);
+    CKM(cudaGetLastError());
+    const double t = (double)(m->step + 1);
+    const float c1 = (float)(1.0 / (1.0 - std::pow(0.9, t))), c2 = (float)(1.0 / (1.0 - std::pow(0.999, t)));
+    k_mlp_reduce<<<(NPARAM + 255) / 256, 256, 0, m->stream>>>(m->partial, nblk, m->loss_partial, m->P, m->M, m->V,
+                                                              m->Wb, lr, c1, c2, update,
+                                                              grad_host ? m->grad : nullptr, m->loss);
+    CKM(cudaGetLastError());
+    if (update) m->step++;
+    if (grad_host) CKM(cudaMemcpyAsync(grad_host, m->grad, NPARAM * sizeof(float), cudaMemcpyDeviceToHost, m->stream));
+    if (loss_host) {
+        double l = 0;
+        CKM(cudaMemcpyAsync(&l, m->loss, sizeof(double), cudaMemcpyDeviceToHost, m->stream));
+        CKM(cudaStreamSynchronize(m->stream));
+        *loss_host = l / nbatch;
+    }
+    return 0;
+}
+
+}  // namespace
+
+// Used by mplb_gpu.cu for mplb_mlp_init_bubble.
+int mplb_mlp_bubble_launch(mplb_mlp* m, double* rho, uint32_t n, int nx, int ny, const double* c, double R,
+                           double t_ratio, double a, double b, cudaStream_t s) {
+    DevGuard g(m->dev);
+    if (int rc = set_attrs()) return rc;
+    // order the handle's stream after the network's last update
+    cudaEvent_t ev;
+    CKM(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+    cudaError_t e = cudaEventRecord(ev, m->stream);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(s, ev, 0);
+    cudaEventDestroy(ev);
+    CKM(e);
+    k_mlp_bubble<<<(n + SB - 1) / SB, NH, SMEM, s>>>(m->P, m->Wb, n, nx, ny, c[0], c[1], c[2], R, t_ratio, a, b, rho);
+    CKM(cudaGetLastError());
+    return 0;
+}
+
+int mplb_mlp_device(const mplb_mlp* m) { return m->dev; }
+
+extern "C" {
+
+void mplb_mlp_features(double t_ratio, double a, double b, double r_over_R, float* out) {
+    features(t_ratio, a, b, r_over_R, out);
+}
+
+int mplb_mlp_create(int32_t device, uint64_t seed, mplb_mlp_t** out) {
+    if (!out) return mplb_internal_fail(MPLB_E_ARG, "out is NULL");
+    *out = nullptr;
+    int dev = device;
+    if (dev < 0) CKM(cudaGetDevice(&dev));
+    DevGuard g(dev);
+    if (int rc = set_attrs()) return rc;
+    mplb_mlp* m = new mplb_mlp();
+    m->dev = dev;
+    m->seed = (uint32_t)(seed ^ (seed >> 32));
+    auto setup = [&]() -> int {
+        CKM(cudaStreamCreateWithFlags(&m->stream, cudaStreamNonBlocking));
+        CKM(cudaMalloc((void**)&m->P, NPARAM * sizeof(float)));
+        CKM(cudaMalloc((void**)&m->M, NPARAM * sizeof(float)));
+        CKM(cudaMalloc((void**)&m->V, NPARAM * sizeof(float)));
+        CKM(cudaMalloc((void**)&m->Wb, NPARAM * sizeof(uint16_t)));
+        CKM(cudaMalloc((void**)&m->grad, NPARAM * sizeof(float)));
+        CKM(cudaMalloc((void**)&m->loss, sizeof(double)));
+        // Glorot-uniform weights from a seeded xorshift generator, zero biases.
+        std::vector<float> p(NPARAM, 0.f);
+        uint64_t st = seed * 0x9E3779B97F4A7C15ull + 1;
+        auto uni = [&]() {
+            st ^= st << 13;
+            st ^= st >> 7;
+            st ^= st << 17;
+            return (double)(st >> 11) * (1.0 / 9007199254740992.0) * 2.0 - 1.0;
+        };
+        auto fill = [&](int off, int fan_out, int fan_in) {
+            const double lim = std::sqrt(6.0 / (fan_in + fan_out));
+            for (int i = 0; i < fan_out * fan_in; i++) p[off + i] = (float)(lim * uni());
+        };
+        fill(OFF_W1, NH, NIN);
+        fill(OFF_W2, NH, NH);
+        fill(OFF_W3, NH, NH);
+        fill(OFF_W4, 1, NH);
+        return upload_params(m, p.data());
+    };
+    if (int rc = setup()) {
+        mlp_free(m);
+        delete m;
+        return rc;
+    }
+    *out = m;
+    return 0;
+}
+
+int mplb_mlp_destroy(mplb_mlp_t* m) {
+    if (!m) return 0;
+    DevGuard g(m->dev);
+    cudaStreamSynchronize(m->stream);
+    mlp_free(m);
+    delete m;
+    return 0;
+}
+
+int mplb_mlp_get_params(mplb_mlp_t* m, float* out) {
+    if (!m || !out) return mplb_internal_fail(MPLB_E_ARG, "NULL argument");
+    DevGuard g(m->dev);
+    CKM(cudaMemcpyAsync(out, m->P, NPARAM * sizeof(float), cudaMemcpyDeviceToHost, m->stream));
+    CKM(cudaStreamSynchronize(m->stream));
+    return 0;
+}
+
+int mplb_mlp_set_params(mplb_mlp_t* m, const float* in) {
+    if (!m || !in) return mplb_internal_fail(MPLB_E_ARG, "NULL argument");
+    for (int i = 0; i < NPARAM; i++)
+        if (!std::isfinite(in[i])) return mplb_internal_fail(MPLB_E_NONFINITE, "non-finite parameter");
+    DevGuard g(m->dev);
+    return upload_params(m, in);
+}
+
+int mplb_mlp_set_samples(mplb_mlp_t* m, const double* t_ratio, const double* a, const double* b,
+                         const double* r_over_R, const double* rho, uint32_t n) {
+    if (!m || !t_ratio || !a || !b || !r_over_R || !rho || n == 0)
+        return mplb_internal_fail(MPLB_E_ARG, "samples missing");
+    std::vector<float> x((size_t)n * NIN), y(n);
+    for (uint32_t i = 0; i < n; i++) {
+        if (!(b[i] > 0.0)) return mplb_internal_fail(MPLB_E_ARG, "b must be positive");
+        features(t_ratio[i], a[i], b[i], r_over_R[i], &x[(size_t)i * NIN]);
+        y[i] = (float)(b[i] * rho[i]);
+    }
+    DevGuard g(m->dev);
+    if (n > m->cap) {
+        if (m->X) cudaFree(m->X);
+        if (m->Y) cudaFree(m->Y);
+        m->X = m->Y = nullptr;
+        m->cap = 0;
+        CKM(cudaMalloc((void**)&m->X, (size_t)n * NIN * sizeof(float)));
+        CKM(cudaMalloc((void**)&m->Y, (size_t)n * sizeof(float)));
+        m->cap = n;
+    }
+    CKM(cudaMemcpyAsync(m->X, x.data(), x.size() * sizeof(float), cudaMemcpyHostToDevice, m->stream));
+    CKM(cudaMemcpyAsync(m->Y, y.data(), y.size() * sizeof(float), cudaMemcpyHostToDevice, m->stream));
+    CKM(cudaStreamSynchronize(m->stream));
+    m->ndata = n;
+    return 0;
+}
+
+int mplb_mlp_gradient(mplb_mlp_t* m, float* grad, double* loss) {
+    if (!m || !grad) return mplb_internal_fail(MPLB_E_ARG, "NULL argument");
+    if (!m->ndata) return mplb_internal_fail(MPLB_E_STATE, "no samples");
+    DevGuard g(m->dev);
+    if (int rc = pass(m, m->ndata, 0, 0, 0.f, grad, loss)) return rc;
+    CKM(cudaStreamSynchronize(m->stream));
+    return 0;
+}
+
+int mplb_mlp_train(mplb_mlp_t* m, uint32_t steps, uint32_t batch, float lr, double* loss) {
+    if (!m || batch == 0) return mplb_internal_fail(MPLB_E_ARG, "bad argument");
+    if (!m->ndata) return mplb_internal_fail(MPLB_E_STATE, "no samples");
+    DevGuard g(m->dev);
+    for (uint32_t s = 0; s < steps; s++)
+        if (int rc = pass(m, batch, 1, 1, lr, nullptr, (loss && s + 1 == steps) ? loss : nullptr)) return rc;
+    CKM(cudaStreamSynchronize(m->stream));
+    return 0;
+}
+
+int mplb_mlp_predict(mplb_mlp_t* m, const double* t_ratio, const double* a, const double* b,
+                     const double* r_over_R, uint32_t n, double* rho) {
+    if (!m || !t_ratio || !a || !b || !r_over_R || !rho) return mplb_internal_fail(MPLB_E_ARG, "NULL argument");
+    if (n == 0) return 0;
+    std::vector<float> x((size_t)n * NIN), y(n);
+    for (uint32_t i = 0; i < n; i++) {
+        if (!(b[i] > 0.0)) return mplb_internal_fail(MPLB_E_ARG, "b must be positive");
+        features(t_ratio[i], a[i], b[i], r_over_R[i], &x[(size_t)i * NIN]);
+    }
+    DevGuard g(m->dev);
+    float *dx = nullptr, *dy = nullptr;
+    auto run = [&]() -> int {
+        CKM(cudaMalloc((void**)&dx, x.size() * sizeof(float)));
+        CKM(cudaMalloc((void**)&dy, y.size() * sizeof(float)));
+        CKM(cudaMemcpyAsync(dx, x.data(), x.size() * sizeof(float), cudaMemcpyHostToDevice, m->stream));
+        k_mlp_predict<<<(n + SB - 1) / SB, NH, SMEM, m->stream>>>(m->P, m->Wb, dx, n, dy);
+        CKM(cudaGetLastError());
+        CKM(cudaMemcpyAsync(y.data(), dy, y.size() * sizeof(float), cudaMemcpyDeviceToHost, m->stream));
+        CKM(cudaStreamSynchronize(m->stream));
+        return 0;
+    };
+    const int rc = run();
+    if (dx) cudaFree(dx);
+    if (dy) cudaFree(dy);
+    if (rc) return rc;
+    for (uint32_t i = 0; i < n; i++) rho[i] = (double)y[i] / b[i];
+    return 0;
+}
+
+}  // extern "C"

@@ -1,0 +1,112 @@
+"""Warm-start network on the device (mplb_mlp_*): forward pass and gradients
+against the CPU oracle (oracle/mlp_oracle.py), training, lattice
+initialisation, and what the trained network gains over the tanh/Maxwell
+initial state on small bubbles judged by the converged plain solver."""
+import numpy as np
+import pytest
+
+from multiphaselb_b200 import Lattice, abi, cases, warmstart
+from oracle import mlp_oracle as mo
+
+pytestmark = pytest.mark.gpu
+
+
+def samples(n, seed=0):
+    rng = np.random.default_rng(seed)
+    t = rng.uniform(0.6, 0.95, n)
+    q = rng.uniform(0.0, 3.2, n)
+    # a smooth stand-in for a bubble profile: vapour inside, liquid outside
+    rho = 0.02 + 0.3 * (0.5 + 0.5 * np.tanh(6.0 * (q - 1.0))) * (1.3 - t)
+    return t, q, rho
+
+
+def oracle_inputs(t, q, rho):
+    X = np.stack([np.ravel(mo.features(a, 1.0, 4.0, b)) for a, b in zip(t, q)])
+    Y = (4.0 * rho).astype(np.float32).astype(np.float64)
+    return X, Y
+
+
+@pytest.mark.parametrize("n", [1, 31, 32, 33, 1000])
+def test_gradient_matches_oracle(gpu_lib, n):
+    t, q, rho = samples(n, seed=n)
+    with warmstart.Network(seed=11) as net:
+        net.set_samples(t, 1.0, 4.0, q, rho)
+        g, loss = net.gradient()
+        p = net.params()
+    X, Y = oracle_inputs(t, q, rho)
+    lw, gw = mo.loss_and_grad(p, X, Y)
+    # FP32 accumulation (device) against FP64 (oracle) on the same BF16 operands
+    assert abs(loss - lw) <= 1e-5 * lw, (loss, lw)
+    err = np.linalg.norm(g - gw) / np.linalg.norm(gw)
+    assert err <= 1e-4, err
+    big = np.abs(gw) > 1e-3 * np.abs(gw).max()
+    assert np.allclose(g[big], gw[big], rtol=5e-3, atol=0), np.abs(g - gw)[big].max()
+
+
+def test_predict_matches_oracle(gpu_lib):
+    t, q, _ = samples(777, seed=2)
+    with warmstart.Network(seed=5) as net:
+        y = net.predict(t, 1.0, 4.0, q)
+        p = net.params()
+    X, _ = oracle_inputs(t, q, q)
+    _, out = mo.forward(p, X)
+    # Agreement to FP32 accumulation, except where an activation sits on a
+    # BF16 rounding boundary and the FP32 (device) and FP64 (oracle) sums
+    # round it to neighbouring BF16 values: a one-ulp (2^-8) step in one unit.
+    d = np.abs(y * 4.0 - out)
+    scale = np.max(np.abs(out))
+    assert np.mean(d > 1e-5 * scale) <= 0.02, np.mean(d > 1e-5 * scale)
+    assert d.max() <= 1e-2 * scale
+
+
+def test_training_reduces_loss(gpu_lib):
+    t, q, rho = samples(20000, seed=4)
+    with warmstart.Network(seed=3) as net:
+        net.set_samples(t, 1.0, 4.0, q, rho)
+        _, l0 = net.gradient()
+        hist = warmstart.train(net, t, q, rho, steps=3000, batch=512, lr=2e-3, lr_end=2e-4, chunks=3)
+        _, l1 = net.gradient()
+    print("loss", l0, hist, l1)
+    assert l1 < 1e-2 * l0
+
+
+def test_init_bubble_equals_predict(gpu_lib):
+    c = cases.bubble_case(abi.D2Q9, L=40, radius=9.0, width=4.0, t_ratio=0.8)
+    with warmstart.Network(seed=8) as net, Lattice(c, path=abi.PATH_FUSED) as lat:
+        lat.upload_case()
+        net.init_bubble(lat, 0.8, warmstart.centre(c), 9.0, c.meta["T"])
+        lat.initialize()
+        out = lat.download()
+        want = net.predict(0.8, 1.0, 4.0, warmstart.radial(c) / 9.0)
+    assert np.array_equal(out["rho"], want)
+    assert np.all(out["U"] == 0.0) and np.all(out["T"] == c.meta["T"])
+
+
+def test_warm_start_gains_over_tanh(gpu_lib):
+    """Train on converged small bubbles, then start a held-out bubble from the
+    network: the plain solver, run to equilibrium from both initial states,
+    needs fewer steps from the network's, and the network's initial profile
+    is closer to the converged one than the tanh/Maxwell profile."""
+    grid = [(48, R, t) for R in (7.0, 10.0, 13.0) for t in (0.65, 0.75, 0.85, 0.95)]
+    K, tol = 500, 1e-9
+    t, q, rho, meta = warmstart.build_training_set(abi.D2Q9, grid, K=K, tol=tol, max_steps=60000)
+    with warmstart.Network(seed=2) as net:
+        warmstart.train(net, t, q, rho, steps=6000, batch=1024, lr=3e-3, lr_end=1e-4, chunks=6)
+        spec = dict(L=48, radius=11.5, t_ratio=0.8)
+        c = warmstart.bubble(abi.D2Q9, spec["L"], spec["radius"], spec["t_ratio"])
+        rho_eq, plain_steps, _, _ = warmstart.converge(c, K=K, tol=tol, max_steps=60000)
+        with Lattice(c, path=abi.PATH_FUSED) as lat:
+            lat.upload_case()
+            net.init_bubble(lat, spec["t_ratio"], warmstart.centre(c), spec["radius"], c.meta["T"])
+            lat.initialize()
+            rho_warm0 = lat.download()["rho"]
+            warm_steps, rate = lat.run_to_equilibrium(60000, K, tol)
+            rho_warm = lat.download()["rho"]
+    err_tanh = np.abs(c.rho - rho_eq).max()
+    err_warm = np.abs(rho_warm0 - rho_eq).max()
+    print("steps plain", plain_steps, "warm", warm_steps, "init err tanh", err_tanh, "warm", err_warm)
+    assert rate < tol
+    assert err_warm < 0.5 * err_tanh
+    assert warm_steps < plain_steps
+    # both runs end at the same equilibrium
+    assert np.abs(rho_warm - rho_eq).max() < 1e-4 * rho_eq.max()
