@@ -66,8 +66,22 @@ class Case:
         return abi.Q_OF[self.lattice]
 
 
+_MESH_CACHE = {}
+
+
 def box_mesh(lattice, dims, periodic):
-    """Neighbour table, coordinates and wall patches of an Nx x Ny (x Nz) box."""
+    """Neighbour table, coordinates and wall patches of an Nx x Ny (x Nz) box
+    (cached per shape; each call returns fresh copies)."""
+    key = (lattice, tuple(dims), tuple(bool(p) for p in periodic))
+    if key not in _MESH_CACHE:
+        if len(_MESH_CACHE) > 16:
+            _MESH_CACHE.clear()
+        _MESH_CACHE[key] = _box_mesh(lattice, dims, periodic)
+    nb, points, patches, names = _MESH_CACHE[key]
+    return nb.copy(), points.copy(), [p.copy() for p in patches], list(names)
+
+
+def _box_mesh(lattice, dims, periodic):
     nx, ny, nz = (list(dims) + [1, 1])[:3]
     px, py, pz = (list(periodic) + [True, True])[:3]
     if lattice == abi.D2Q9:
@@ -180,7 +194,7 @@ _GL_X, _GL_W = np.polynomial.legendre.leggauss(96)
 
 def _maxwell_densities(eos, T):
     rmax = _rho_max(eos)
-    rho = np.linspace(1e-6, 0.9999 * rmax, 400001)
+    rho = np.linspace(1e-6, 0.9999 * rmax, 100001)
     p = p_eos(eos, rho, T)
     dp = np.diff(p)
     i_max = np.argmax(dp < 0)                # first local max (vapour spinodal)
