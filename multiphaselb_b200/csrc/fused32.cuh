@@ -86,29 +86,102 @@ constexpr int first_diagonal() {
     return L::Q - 1;
 }
 
-// Exact mass bookkeeping for the FP32 collision.  The collision conserves its
-// own FP32 mass moment (a rounded sum of the inputs), and rounding in
-// M^-1 m and in the stores adds a little more; at a steady state those
-// errors repeat every step at every node and the lattice mass drifts
-// (measured: +2.7e-10 per node and step on a 128^2 CS bubble).  Here the sum
-// of the stored outputs is made equal to the exact sum of the inputs: both
-// sums are exact in FP64 (nine or fifteen FP32 values).  The difference goes
-// into the rest population (no momentum), and what that one cannot represent
-// is split evenly over an opposite diagonal pair (momentum unchanged but for
-// their own roundings).  What remains is below half an ulp of a diagonal
-// population, of either sign.  (Putting the difference into two populations
-// that do not cancel in momentum drives a spurious flow: tried, unstable.)
+// Exact bookkeeping of the conserved moments for the FP32 collision.  In
+// exact arithmetic the collision keeps the node's mass and adds the force to
+// its momentum.  In FP32 it conserves rounded moments (FP32 sums of the
+// inputs), and rounding in M^-1 m and in the stores adds more; at a steady
+// state those errors repeat every step at every node, so the lattice mass
+// drifts (measured: +2.7e-10 per node and step on a 128^2 CS bubble) and the
+// momentum wanders, which moves the interface and holds max |drho/dt| near
+// 1e-9 instead of letting it decay.  Here the stored outputs are corrected so
+// that their exact sums (FP64 sums of FP32 values: exact) equal the targets:
+//   momentum, axis by axis: half the residual onto the population along +e_d,
+//     half off the one along -e_d (mass unchanged);
+//   mass: the residual onto the rest population (momentum unchanged), what
+//     it cannot represent split evenly over an opposite diagonal pair.
+// What remains is a fraction of an ulp of the populations involved, of
+// either sign.  (Putting the mass residual into two populations that do not
+// cancel in momentum drives a spurious flow: tried, unstable.)
 template <class L>
-__device__ __forceinline__ void restore_mass(float* f, double pre) {
+constexpr int axis_population(int d) {
+    for (int k = 1; k < L::Q; k++)
+        if (ck<L>(k, d) == 1 && cxk<L>(k) * cxk<L>(k) + cyk<L>(k) * cyk<L>(k) + czk<L>(k) * czk<L>(k) == 1)
+            return k;
+    return 0;
+}
+
+template <class L>
+__device__ __forceinline__ void restore_conserved(float* f, double mass, const double* mom) {
+    static_for<L::D>([&](auto dd) {
+        constexpr int d = decltype(dd)::value;
+        double j = 0.0;
+        static_for<L::Q>([&](auto kk) {
+            constexpr int c = ck<L>(decltype(kk)::value, d);
+            if constexpr (c == 1) j += (double)f[kk];
+            else if constexpr (c == -1) j -= (double)f[kk];
+        });
+        const double half = 0.5 * (mom[d] - j);
+        constexpr int a = axis_population<L>(d), b = revk<L>(a);
+        f[a] = (float)((double)f[a] + half);
+        f[b] = (float)((double)f[b] - half);
+    });
     double post = 0.0;
 #pragma unroll
     for (int k = 0; k < L::Q; k++) post += (double)f[k];
-    const double v = (double)f[0] + (pre - post);
+    const double v = (double)f[0] + (mass - post);
     f[0] = (float)v;
     const double half = 0.5 * (v - (double)f[0]);
     constexpr int a = first_diagonal<L>(), b = revk<L>(a);
     f[a] = (float)((double)f[a] + half);
     f[b] = (float)((double)f[b] + half);
+}
+
+// Total momentum of a periodic lattice without net body force is conserved
+// exactly by the model; FP32 rounding (below an ulp per node and step, but
+// not of zero mean at a steady state) lets it drift, and the drift carries
+// the bubble along (|drho/dt| = |grad rho| v at the interface).  Equilibrium
+// runs of the FP32 form therefore reset the total momentum to its value at
+// the start of the run at every convergence check.  The total is kept in
+// fixed point (resolution 2^-40): each node's exact FP64 momentum is rounded
+// to a multiple of 2^-40 and the integers are summed, so the result does not
+// depend on summation order or tiling.
+constexpr double MOM_SCALE = 1099511627776.0;  // 2^40
+
+template <class L>
+__device__ __forceinline__ void node_momentum_fx(const float* __restrict__ f, uint32_t n, uint32_t id,
+                                                 long long* m) {
+    static_for<L::D>([&](auto dd) {
+        constexpr int d = decltype(dd)::value;
+        double j = 0.0;
+        static_for<L::Q>([&](auto kk) {
+            constexpr int k = decltype(kk)::value;
+            constexpr int c = ck<L>(k, d);
+            if constexpr (c == 1) j += (double)f[(size_t)k * n + id];
+            else if constexpr (c == -1) j -= (double)f[(size_t)k * n + id];
+        });
+        m[d] = __double2ll_rn(j * MOM_SCALE);
+    });
+}
+
+// Warp sum (exact: integers) and one atomic per warp.
+__device__ __forceinline__ void warp_add_ll(long long v, long long* out) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    if ((threadIdx.x & 31) == 0 && v != 0) atomicAdd(reinterpret_cast<unsigned long long*>(out), (unsigned long long)v);
+}
+
+// Remove a per-node momentum excess: half off the population along +e_d,
+// half onto the one along -e_d (mass unchanged but for the two roundings).
+template <class L>
+__device__ __forceinline__ void momentum_fix_node(float* __restrict__ f, uint32_t n, uint32_t id,
+                                                  const long long* J, const long long* J0) {
+    static_for<L::D>([&](auto dd) {
+        constexpr int d = decltype(dd)::value;
+        const double half = 0.5 * ((double)(J[d] - J0[d]) / MOM_SCALE / (double)n);
+        constexpr int a = axis_population<L>(d), b = revk<L>(a);
+        f[(size_t)a * n + id] = (float)((double)f[(size_t)a * n + id] - half);
+        f[(size_t)b * n + id] = (float)((double)f[(size_t)b * n + id] + half);
+    });
 }
 
 // liMRT collision on deviations (liMRTCollision.c / liMRTForce.c in FP32).
@@ -359,21 +432,34 @@ __device__ __forceinline__ void finish_node32(const Params& P, const FusedArgs32
     }
     const float U[3] = {(float)Ud[0], (float)Ud[1], (float)Ud[2]};
     if constexpr (F_ON) {
-        double pre = 0.0;
-#pragma unroll
-        for (int k = 0; k < L::Q; k++) pre += (double)f[k];
+        // conserved moments the collision must produce: the input mass, and
+        // the input momentum plus the force the collision applies
+        double mass = 0.0, mom[3] = {0.0, 0.0, 0.0};
+        static_for<L::Q>([&](auto kk) {
+            constexpr int k = decltype(kk)::value;
+            mass += (double)f[k];
+            static_for<L::D>([&](auto dd) {
+                constexpr int c = ck<L>(k, decltype(dd)::value);
+                if constexpr (c == 1) mom[dd] += (double)f[k];
+                else if constexpr (c == -1) mom[dd] -= (double)f[k];
+            });
+        });
         if constexpr (L::Q == 9) {
             const float F[3] = {(float)Ft[0], (float)Ft[1], (float)Ft[2]};
             const float Fv[3] = {(float)Fi[0], (float)Fi[1], (float)Fi[2]};
             collide_limrt32(A, f, rho, dr, U, F, Fv, psi);
+#pragma unroll
+            for (int j = 0; j < 3; j++) mom[j] += Ft[j];
         } else {
             double Fx[3];
 #pragma unroll
             for (int j = 0; j < 3; j++) Fx[j] = Fi[j] + (rho - P.rho_0) * P.g[j];
             const float F[3] = {(float)Fx[0], (float)Fx[1], (float)Fx[2]};
             collide_xumrt32(A, f, rho, dr, U, F, psi);
+#pragma unroll
+            for (int j = 0; j < 3; j++) mom[j] += Fx[j];
         }
-        restore_mass<L>(f, pre);
+        restore_conserved<L>(f, mass, mom);
 #pragma unroll
         for (int k = 0; k < L::Q; k++) A.fout[(size_t)k * n + id] = f[k];
         if constexpr (G_ON) {

@@ -341,7 +341,8 @@ template <int TX, int TY>
 __global__ void __launch_bounds__(TX * TY)
     k_batch32_check(const Params* __restrict__ Ps, const FusedArgs32* __restrict__ As,
                     const int2* __restrict__ tiles, const int* __restrict__ ntiles, int parity,
-                    double* const* __restrict__ snaps, unsigned long long* __restrict__ dmax) {
+                    double* const* __restrict__ snaps, unsigned long long* __restrict__ dmax,
+                    long long* __restrict__ jsum) {
     __shared__ double red[TX * TY / 32];
     const int nt = *ntiles;
     for (int t = blockIdx.x; t < nt; t += gridDim.x) {
@@ -351,6 +352,7 @@ __global__ void __launch_bounds__(TX * TY)
         const int bx = w.y % A.tiles_x, by = w.y / A.tiles_x;
         const int x = bx * TX + (int)threadIdx.x % TX, y = by * TY + (int)threadIdx.x / TX;
         double d = 0.0;
+        long long m[2] = {0, 0};
         if (x < A.nx && y < A.ny) {
             const uint32_t id = (uint32_t)x + (uint32_t)A.nx * (uint32_t)y;
             float f[9], g[1], dr, dT;
@@ -359,7 +361,10 @@ __global__ void __launch_bounds__(TX * TY)
             double* snap = snaps[w.x];
             d = fabs(rho - snap[id]);
             snap[id] = rho;
+            node_momentum_fx<D2Q9T>(A.fin, A.n, id, m);
         }
+        warp_add_ll(m[0], jsum + 3 * w.x);
+        warp_add_ll(m[1], jsum + 3 * w.x + 1);
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) d = fmax(d, __shfl_down_sync(0xffffffffu, d, o));
         if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = d;
@@ -374,7 +379,60 @@ __global__ void __launch_bounds__(TX * TY)
     }
 }
 
+// Reset each flagged lattice's total momentum to J0 (see momentum_fix_node).
+template <int TX, int TY>
+__global__ void __launch_bounds__(TX * TY)
+    k_batch32_fix(const FusedArgs32* __restrict__ As, const int2* __restrict__ tiles, const int* __restrict__ ntiles,
+                  int parity, const long long* __restrict__ jsum, const long long* __restrict__ j0,
+                  const int* __restrict__ proj) {
+    const int nt = *ntiles;
+    for (int t = blockIdx.x; t < nt; t += gridDim.x) {
+        const int2 w = tiles[t];
+        if (!proj[w.x]) continue;
+        const FusedArgs32& A = As[2 * w.x + parity];
+        if (A.tiles_x <= 0 || w.y < 0 || w.y >= A.tiles_x * A.tiles_y) continue;
+        const int bx = w.y % A.tiles_x, by = w.y / A.tiles_x;
+        const int x = bx * TX + (int)threadIdx.x % TX, y = by * TY + (int)threadIdx.x / TX;
+        if (x < A.nx && y < A.ny)
+            momentum_fix_node<D2Q9T>(const_cast<float*>(A.fin), A.n, (uint32_t)x + (uint32_t)A.nx * (uint32_t)y,
+                                     jsum + 3 * w.x, j0 + 3 * w.x);
+    }
+}
+
+// Lone lattice: total momentum of the current FP32 buffer, and its reset.
+template <class L>
+__global__ void k_mom_sum32(uint32_t n, const float* __restrict__ f, long long* __restrict__ J) {
+    long long m[3] = {0, 0, 0};
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) node_momentum_fx<L>(f, n, i, m);
+#pragma unroll
+    for (int d = 0; d < L::D; d++) warp_add_ll(m[d], J + d);
+}
+
+template <class L>
+__global__ void k_mom_fix32(uint32_t n, float* __restrict__ f, const long long* __restrict__ J,
+                            const long long* __restrict__ J0) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) momentum_fix_node<L>(f, n, i, J, J0);
+}
+
 }  // namespace mplb
+
+cudaError_t mplb_mom_sum32(int lat, uint32_t n, const float* f, long long* J, cudaStream_t s) {
+    cudaError_t e = cudaMemsetAsync(J, 0, 3 * sizeof(long long), s);
+    if (e != cudaSuccess) return e;
+    const unsigned nb = (n + 255) / 256;
+    if (lat == MPLB_D2Q9) k_mom_sum32<D2Q9T><<<nb, 256, 0, s>>>(n, f, J);
+    else k_mom_sum32<D3Q15T><<<nb, 256, 0, s>>>(n, f, J);
+    return cudaGetLastError();
+}
+
+cudaError_t mplb_mom_fix32(int lat, uint32_t n, float* f, const long long* J, const long long* J0, cudaStream_t s) {
+    const unsigned nb = (n + 255) / 256;
+    if (lat == MPLB_D2Q9) k_mom_fix32<D2Q9T><<<nb, 256, 0, s>>>(n, f, J, J0);
+    else k_mom_fix32<D3Q15T><<<nb, 256, 0, s>>>(n, f, J, J0);
+    return cudaGetLastError();
+}
 
 namespace {
 template <int TX, int TY>
@@ -417,12 +475,24 @@ cudaError_t mplb_batch32_launch(int cfg, const Params* dP, const FusedArgs32* dA
 
 cudaError_t mplb_batch32_check(int cfg, const Params* dP, const FusedArgs32* dA, const int2* tiles,
                                const int* ntiles, int parity, int grid, double* const* snaps,
-                               unsigned long long* dmax, cudaStream_t s) {
+                               unsigned long long* dmax, long long* jsum, cudaStream_t s) {
     switch (cfg) {
-    case 0: k_batch32_check<32, 8><<<grid, 256, 0, s>>>(dP, dA, tiles, ntiles, parity, snaps, dmax); break;
-    case 1: k_batch32_check<32, 4><<<grid, 128, 0, s>>>(dP, dA, tiles, ntiles, parity, snaps, dmax); break;
-    case 2: k_batch32_check<16, 8><<<grid, 128, 0, s>>>(dP, dA, tiles, ntiles, parity, snaps, dmax); break;
-    default: k_batch32_check<64, 4><<<grid, 256, 0, s>>>(dP, dA, tiles, ntiles, parity, snaps, dmax); break;
+    case 0: k_batch32_check<32, 8><<<grid, 256, 0, s>>>(dP, dA, tiles, ntiles, parity, snaps, dmax, jsum); break;
+    case 1: k_batch32_check<32, 4><<<grid, 128, 0, s>>>(dP, dA, tiles, ntiles, parity, snaps, dmax, jsum); break;
+    case 2: k_batch32_check<16, 8><<<grid, 128, 0, s>>>(dP, dA, tiles, ntiles, parity, snaps, dmax, jsum); break;
+    default: k_batch32_check<64, 4><<<grid, 256, 0, s>>>(dP, dA, tiles, ntiles, parity, snaps, dmax, jsum); break;
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t mplb_batch32_fix(int cfg, const FusedArgs32* dA, const int2* tiles, const int* ntiles, int parity,
+                             int grid, const long long* jsum, const long long* j0, const int* proj,
+                             cudaStream_t s) {
+    switch (cfg) {
+    case 0: k_batch32_fix<32, 8><<<grid, 256, 0, s>>>(dA, tiles, ntiles, parity, jsum, j0, proj); break;
+    case 1: k_batch32_fix<32, 4><<<grid, 128, 0, s>>>(dA, tiles, ntiles, parity, jsum, j0, proj); break;
+    case 2: k_batch32_fix<16, 8><<<grid, 128, 0, s>>>(dA, tiles, ntiles, parity, jsum, j0, proj); break;
+    default: k_batch32_fix<64, 4><<<grid, 256, 0, s>>>(dA, tiles, ntiles, parity, jsum, j0, proj); break;
     }
     return cudaGetLastError();
 }

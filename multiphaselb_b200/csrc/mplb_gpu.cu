@@ -41,7 +41,12 @@ cudaError_t mplb_batch32_launch(int cfg, const Params* dP, const FusedArgs32* dA
                                 const int* ntiles, int parity, int grid, cudaStream_t s);
 cudaError_t mplb_batch32_check(int cfg, const Params* dP, const FusedArgs32* dA, const int2* tiles,
                                const int* ntiles, int parity, int grid, double* const* snaps,
-                               unsigned long long* dmax, cudaStream_t s);
+                               unsigned long long* dmax, long long* jsum, cudaStream_t s);
+cudaError_t mplb_batch32_fix(int cfg, const FusedArgs32* dA, const int2* tiles, const int* ntiles, int parity,
+                             int grid, const long long* jsum, const long long* j0, const int* proj,
+                             cudaStream_t s);
+cudaError_t mplb_mom_sum32(int lat, uint32_t n, const float* f, long long* J, cudaStream_t s);
+cudaError_t mplb_mom_fix32(int lat, uint32_t n, float* f, const long long* J, const long long* J0, cudaStream_t s);
 
 namespace {
 
@@ -106,6 +111,7 @@ struct mplb_gpu {
     int cur32[2] = {0, 0};
     double rho_ref = 0, T_ref = 0;
     double* snap = nullptr;  // equilibrium monitor: density at the last check
+    long long* mom = nullptr;  // FP32 equilibrium runs: total momentum now [0..2] and at the start [3..5]
     int tile_request = 0;  // mplb_opts.tile_config
     uint32_t current = 0;
     uint64_t launches = 0;
@@ -137,6 +143,18 @@ void free_all(mplb_gpu* h) {
         for (int j = 0; j < 2; j++)
             if (h->p32[i][j]) cudaFree(h->p32[i][j]);
     if (h->snap) cudaFree(h->snap);
+    if (h->mom) cudaFree(h->mom);
+}
+
+// Does the FP32 form's momentum reset apply?  Fully periodic box without
+// boundary patches and without net body force (gravity, external force).
+bool momentum_conserved(const mplb_gpu* h) {
+    if (h->precision != MPLB_FP32_DEV || h->path != MPLB_PATH_FUSED || !h->box || h->fc.has_bc) return false;
+    for (int d = 0; d < h->D; d++)
+        if (!h->per[d]) return false;
+    for (int j = 0; j < 3; j++)
+        if (h->P.g[j] != 0.0 || h->P.fext[j] != 0.0) return false;
+    return h->P.f_update != 0;
 }
 
 __global__ void k_fill(uint32_t n, double v, double* __restrict__ x) {
@@ -1120,14 +1138,33 @@ int mplb_gpu_run_to_equilibrium(mplb_gpu_t* h, uint32_t max_steps, uint32_t chec
                                 uint32_t* steps, double* rate) {
     if (!h) return fail(MPLB_E_ARG, "NULL handle");
     if (check_interval == 0) return fail(MPLB_E_ARG, "check_interval must be >= 1");
+    DeviceGuard guard(h->dev);
     double d = 0;
     RET(mplb_gpu_monitor(h, 1, &d, nullptr));
+    // FP32 form: reset the total momentum to its starting value at every check
+    const bool fix = momentum_conserved(h);
+    auto momentum = [&](long long* J) -> int {
+        cudaError_t e = mplb_mom_sum32(h->lat, h->n, h->p32[0][h->cur32[0]], J, h->stream);
+        h->launches++;
+        if (e != cudaSuccess) return fail(MPLB_E_CUDA, std::string("momentum sum: ") + cudaGetErrorString(e));
+        return 0;
+    };
+    if (fix) {
+        if (!h->mom) CK(cudaMalloc((void**)&h->mom, 6 * sizeof(long long)));
+        RET(momentum(h->mom + 3));
+    }
     uint32_t done = 0;
     double r = -1.0;
     while (done < max_steps) {
         RET(mplb_gpu_step(h, check_interval));
         done += check_interval;
         RET(mplb_gpu_monitor(h, 0, &d, nullptr));
+        if (fix) {
+            RET(momentum(h->mom));
+            cudaError_t e = mplb_mom_fix32(h->lat, h->n, h->p32[0][h->cur32[0]], h->mom, h->mom + 3, h->stream);
+            h->launches++;
+            if (e != cudaSuccess) return fail(MPLB_E_CUDA, std::string("momentum reset: ") + cudaGetErrorString(e));
+        }
         r = d / check_interval;
         if (r < tol) break;
     }
@@ -1186,6 +1223,9 @@ struct mplb_batch {
     double* snap = nullptr;
     unsigned long long* dmax = nullptr;
     unsigned long long* hmax = nullptr;  // pinned
+    long long* jsum = nullptr;  // per lattice total momentum (fixed point), now
+    long long* j0 = nullptr;    // ... and at the start of the run
+    int* proj = nullptr;        // per lattice: momentum reset applies
     cudaGraphExec_t graph = nullptr;
     int graph_cfg = -1;
     uint32_t graph_K = 0;
@@ -1196,7 +1236,7 @@ namespace {
 
 void batch_free(mplb_batch* b) {
     if (b->graph) cudaGraphExecDestroy(b->graph);
-    void* ps[] = {b->dP, b->dA, b->dtiles, b->dnt, b->dsnap, b->snap, b->dmax};
+    void* ps[] = {b->dP, b->dA, b->dtiles, b->dnt, b->dsnap, b->snap, b->dmax, b->jsum, b->j0, b->proj};
     for (void* p : ps)
         if (p) cudaFree(p);
     if (b->hmax) cudaFreeHost(b->hmax);
@@ -1288,11 +1328,21 @@ int batch_launch(mplb_batch* b, int c, int grid, int parity) {
     return 0;
 }
 
-int batch_check(mplb_batch* b, int parity) {
+// Convergence check (max |drho| per lattice, density snapshot, total
+// momentum), then the FP32 momentum reset; dmax and jsum are cleared first.
+int batch_check(mplb_batch* b, int parity, bool fix) {
+    const size_t N = b->lat.size();
+    CK(cudaMemsetAsync(b->dmax, 0, N * sizeof(unsigned long long), b->stream));
+    CK(cudaMemsetAsync(b->jsum, 0, 3 * N * sizeof(long long), b->stream));
     cudaError_t e = mplb_batch32_check(b->cfg, b->dP, b->dA, b->dtiles, b->dnt, parity, b->grid, b->dsnap, b->dmax,
-                                       b->stream);
+                                       b->jsum, b->stream);
     b->launches++;
     if (e != cudaSuccess) return fail(MPLB_E_CUDA, std::string("batch check launch: ") + cudaGetErrorString(e));
+    if (fix) {
+        e = mplb_batch32_fix(b->cfg, b->dA, b->dtiles, b->dnt, parity, b->grid, b->jsum, b->j0, b->proj, b->stream);
+        b->launches++;
+        if (e != cudaSuccess) return fail(MPLB_E_CUDA, std::string("batch fix launch: ") + cudaGetErrorString(e));
+    }
     return 0;
 }
 
@@ -1355,7 +1405,8 @@ int batch_ready(mplb_batch* b, const std::vector<char>& active, int* nt) {
 }
 
 // One check interval as a graph: K step launches (parity alternating, K is
-// even so every lattice ends on the buffer it started from), then the check.
+// even so every lattice ends on the buffer it started from), then the check
+// and the momentum reset.
 int batch_graph(mplb_batch* b) {
     if (b->graph && b->graph_cfg == b->cfg && b->graph_K == b->K) return 0;
     if (b->graph) {
@@ -1366,17 +1417,15 @@ int batch_graph(mplb_batch* b) {
     CK(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
     int rc = 0;
     for (uint32_t s = 0; s < b->K && !rc; s++) rc = batch_launch(b, b->cfg, b->grid, (int)(s & 1));
-    cudaError_t e = rc ? cudaSuccess : cudaMemsetAsync(b->dmax, 0, b->lat.size() * sizeof(unsigned long long), b->stream);
-    if (!rc && e == cudaSuccess) rc = batch_check(b, 0);
+    if (!rc) rc = batch_check(b, 0, true);
     cudaError_t ee = cudaStreamEndCapture(b->stream, &g);
-    b->launches -= b->K + 1;  // counted when replayed
+    b->launches -= b->K + 2;  // counted when replayed
     if (rc) {
         if (ee == cudaSuccess) cudaGraphDestroy(g);
         return rc;
     }
-    CK(e);
     CK(ee);
-    e = cudaGraphInstantiate(&b->graph, g, 0);
+    cudaError_t e = cudaGraphInstantiate(&b->graph, g, 0);
     cudaGraphDestroy(g);
     CK(e);
     b->graph_cfg = b->cfg;
@@ -1440,6 +1489,13 @@ int mplb_batch_create(mplb_gpu_t* const* lattices, uint32_t count, const mplb_ba
         CK(cudaMalloc((void**)&b->snap, b->nodes * sizeof(double)));
         CK(cudaMalloc((void**)&b->dmax, count * sizeof(unsigned long long)));
         CK(cudaMallocHost((void**)&b->hmax, count * sizeof(unsigned long long)));
+        CK(cudaMalloc((void**)&b->jsum, 3 * count * sizeof(long long)));
+        CK(cudaMalloc((void**)&b->j0, 3 * count * sizeof(long long)));
+        CK(cudaMalloc((void**)&b->proj, count * sizeof(int)));
+        std::vector<int> pr(count);
+        for (uint32_t i = 0; i < count; i++) pr[i] = momentum_conserved(b->lat[i]) ? 1 : 0;
+        CK(cudaMemcpyAsync(b->proj, pr.data(), count * sizeof(int), cudaMemcpyHostToDevice, b->stream));
+        CK(cudaStreamSynchronize(b->stream));
         size_t off = 0;
         for (uint32_t i = 0; i < count; i++) {
             snaps[i] = b->snap + off;
@@ -1516,13 +1572,14 @@ int mplb_batch_run(mplb_batch_t* b, uint32_t max_steps, uint32_t* steps_out, dou
     int nt = 0;
     RET(batch_ready(b, active, &nt));
     RET(batch_graph(b));
-    RET(batch_check(b, 0));  // snapshot of the starting rho
+    RET(batch_check(b, 0, false));  // snapshot of the starting rho and momentum
+    CK(cudaMemcpyAsync(b->j0, b->jsum, 3 * N * sizeof(long long), cudaMemcpyDeviceToDevice, b->stream));
     size_t left = N;
     uint32_t done = 0, conv = 0;
     while (left && done < max_steps) {
         CK(cudaGraphLaunch(b->graph, b->stream));
         b->graph_launches++;
-        b->launches += b->K + 1;
+        b->launches += b->K + 2;
         CK(cudaMemcpyAsync(b->hmax, b->dmax, N * sizeof(unsigned long long), cudaMemcpyDeviceToHost, b->stream));
         CK(cudaStreamSynchronize(b->stream));
         done += b->K;

@@ -31,6 +31,17 @@ def lone(case, steps):
         return lat.download()
 
 
+def lone_run(case, steps, K):
+    """A lone lattice through the same equilibrium-run procedure (checks and
+    FP32 momentum resets every K steps), held for exactly `steps` steps."""
+    with Lattice(case, path=abi.PATH_FUSED, precision=abi.FP32_DEV) as lat:
+        lat.upload_case()
+        lat.initialize()
+        got, _ = lat.run_to_equilibrium(steps, K, 0.0)
+        assert got == steps
+        return lat.download()
+
+
 def make(cs):
     lats = []
     for c in cs:
@@ -85,7 +96,8 @@ def test_batch_then_handle_steps(gpu_lib):
 def test_batch_run_retires_converged_lattices(gpu_lib):
     """Run to a loose tolerance: each lattice's step count is a whole number of
     check intervals, converged ones report a rate under tol, and every
-    lattice's state is that of a lone lattice stepped as many times."""
+    lattice's state is that of a lone lattice run through the same
+    equilibrium procedure for as many steps."""
     cs = ensemble()
     lats = make(cs)
     K, tol, max_steps = 100, 2e-5, 3000
@@ -103,7 +115,7 @@ def test_batch_run_retires_converged_lattices(gpu_lib):
             assert s == max_steps
     assert info["graph_launches"] == max(steps) // K
     for c, lat, s in zip(cs, lats, steps):
-        same(lat.download(), lone(c, [int(s)]), c.name)
+        same(lat.download(), lone_run(c, int(s), K), c.name)
         lat.close()
 
 
