@@ -302,17 +302,19 @@ int mplb_batch_run(mplb_batch_t* b, uint32_t max_steps, uint32_t* steps_out, dou
 /* ------------------------------------------------------------------------
  * Learned warm start.  No counterpart in the reference, whose initial fields
  * come from its dictionaries (a tanh/Maxwell bubble in the workloads here).
- * A 4-64-64-64-1 tanh network maps (T/Tc, a, b, r/R) -- Carnahan-Starling
- * constants a, b, distance r to the bubble centre over the radius R -- to
- * b * rho at equilibrium.  Weights and activations BF16, accumulation FP32,
- * FP32 master weights and Adam state; trained on the device by this
- * library's own forward and backward kernels on density samples the caller
- * takes from converged lattices.
+ * A 5-64-64-64-1 tanh network maps (T/Tc, a, b, r/R, R) -- Carnahan-Starling
+ * constants a, b, distance r of a node to the bubble centre, radius R -- to
+ * b * rho at equilibrium.  r/R and R enter as the pair ((r - R)/5, 5/R)
+ * (interface at 0 with a width independent of R, curvature for the Laplace
+ * shift).  Weights and activations BF16, accumulation FP32, FP32 master
+ * weights and Adam state; trained on the device by this library's own
+ * forward and backward kernels on density samples the caller takes from
+ * converged lattices.
  *
- * Parameter vector (MPLB_MLP_PARAMS floats): W1[64][4], b1[64], W2[64][64],
+ * Parameter vector (MPLB_MLP_PARAMS floats): W1[64][5], b1[64], W2[64][64],
  * b2[64], W3[64][64], b3[64], W4[64], b4 -- each W row-major [out][in].
  * ---------------------------------------------------------------------- */
-#define MPLB_MLP_PARAMS 8705
+#define MPLB_MLP_PARAMS 8769
 typedef struct mplb_mlp mplb_mlp_t;
 
 /* Glorot-uniform weights from `seed`, zero biases. */
@@ -322,18 +324,18 @@ int mplb_mlp_get_params(mplb_mlp_t* m, float* params);
 /* Replaces the master weights (and their BF16 copy); resets Adam. */
 int mplb_mlp_set_params(mplb_mlp_t* m, const float* params);
 /* The network's normalised, BF16-rounded inputs for one sample (host). */
-void mplb_mlp_features(double t_ratio, double a, double b, double r_over_R, float* out4);
+void mplb_mlp_features(double t_ratio, double a, double b, double r, double R, float* out5);
 /* Training set: n samples (target b * rho), copied to the device. */
-int mplb_mlp_set_samples(mplb_mlp_t* m, const double* t_ratio, const double* a, const double* b,
-                         const double* r_over_R, const double* rho, uint32_t n);
+int mplb_mlp_set_samples(mplb_mlp_t* m, const double* t_ratio, const double* a, const double* b, const double* r,
+                         const double* R, const double* rho, uint32_t n);
 /* Gradient of the mean squared error over the whole training set, no update. */
 int mplb_mlp_gradient(mplb_mlp_t* m, float* grad, double* loss);
 /* `steps` Adam steps (beta 0.9 / 0.999) on minibatches of `batch` samples
  * drawn by a counter-based hash; *loss = the last minibatch's MSE. */
 int mplb_mlp_train(mplb_mlp_t* m, uint32_t steps, uint32_t batch, float lr, double* loss);
 /* rho for n samples. */
-int mplb_mlp_predict(mplb_mlp_t* m, const double* t_ratio, const double* a, const double* b,
-                     const double* r_over_R, uint32_t n, double* rho);
+int mplb_mlp_predict(mplb_mlp_t* m, const double* t_ratio, const double* a, const double* b, const double* r,
+                     const double* R, uint32_t n, double* rho);
 /* Initial state of a box lattice with a Carnahan-Starling EOS: rho of every
  * node from the network (r = distance of the node's box coordinates to
  * `center`), U = 0, T = T.  Call mplb_gpu_initialize next, as after

@@ -1,5 +1,5 @@
-// mplb_mlp.cu -- learned warm start: a 4-64-64-64-1 tanh network that maps
-// (T/Tc, a, b, r/R) to the equilibrium density of a static bubble, trained
+// mplb_mlp.cu -- learned warm start: a 5-64-64-64-1 tanh network that maps
+// (T/Tc, a, b, r/R, R) to the equilibrium density of a static bubble, trained
 // on the GPU on density profiles the solver itself converged.
 //
 // Precision: weights and activations are BF16 (round-to-nearest-even of the
@@ -30,7 +30,7 @@ int mplb_internal_fail(int code, const std::string& msg);
 
 namespace {
 
-constexpr int NIN = 4, NH = 64;
+constexpr int NIN = 5, NH = 64;
 constexpr int OFF_W1 = 0, OFF_B1 = OFF_W1 + NH * NIN, OFF_W2 = OFF_B1 + NH, OFF_B2 = OFF_W2 + NH * NH,
               OFF_W3 = OFF_B2 + NH, OFF_B3 = OFF_W3 + NH * NH, OFF_W4 = OFF_B3 + NH, OFF_B4 = OFF_W4 + NH,
               NPARAM = OFF_B4 + 1;
@@ -66,16 +66,22 @@ __host__ __device__ inline float bf16_round(float f) {
 __host__ __device__ inline uint16_t bf16_bits(float f) { return (uint16_t)(f2u(bf16_round(f)) >> 16); }
 __device__ inline float bf16_float(uint16_t b) { return __uint_as_float((uint32_t)b << 16); }
 
-// Network inputs: T/Tc centred on the trained range [0.6, 0.95], the CS
-// constants relative to a = 1, b = 4, and r/R clamped to [0, 3] (beyond
-// three radii the profile is bulk liquid).  Rounded to BF16 (they are GEMM
-// operands).  Output: b * rho.
-__host__ __device__ inline void features(double t_ratio, double a, double b, double r_over_R, float* x) {
-    const double r = r_over_R < 0.0 ? 0.0 : (r_over_R > 3.0 ? 3.0 : r_over_R);
+// Network inputs.  T/Tc centred on the trained range [0.6, 0.95]; the CS
+// constants relative to a = 1, b = 4; the node position r/R and the radius R
+// as the pair d = (r - R)/W and k = W/R (W = 5 lattice units, the initial
+// interface width; r/R = 1 + d k), so the interface sits at d = 0 with a
+// width independent of R and the curvature k carries the Laplace shift of
+// the bulk densities.  d is clamped to [-6, 6] (bulk beyond).  Rounded to
+// BF16 (GEMM operands).  Output: b * rho.
+constexpr double W_IFACE = 5.0;
+__host__ __device__ inline void features(double t_ratio, double a, double b, double r, double R, float* x) {
+    double d = (r - R) / W_IFACE;
+    d = d < -6.0 ? -6.0 : (d > 6.0 ? 6.0 : d);
     x[0] = bf16_round((float)((t_ratio - 0.775) / 0.175));
     x[1] = bf16_round((float)(a - 1.0));
     x[2] = bf16_round((float)(b * 0.25 - 1.0));
-    x[3] = bf16_round((float)((r - 1.5) / 1.5));
+    x[3] = bf16_round((float)(d / 6.0));
+    x[4] = bf16_round((float)((W_IFACE / R - 0.3) / 0.3));
 }
 
 // ------------------------------------------------------------ block state
@@ -253,7 +259,9 @@ __global__ void __launch_bounds__(NH) k_mlp_grad(const float* __restrict__ P, co
     __syncthreads();
     // layer 1
     {
-        float acc[NIN] = {0.f, 0.f, 0.f, 0.f};
+        float acc[NIN];
+#pragma unroll
+        for (int i = 0; i < NIN; i++) acc[i] = 0.f;
         float bacc = 0.f;
         for (int q = 0; q < SB; q++) {
             const float d = s.dzA[q][j];
@@ -327,7 +335,7 @@ __global__ void __launch_bounds__(NH) k_mlp_bubble(const float* __restrict__ P, 
         const uint32_t i = e < n ? e : 0;
         const double x = (double)(i % (uint32_t)nx) - cx, y = (double)((i / (uint32_t)nx) % (uint32_t)ny) - cy,
                      z = (double)(i / ((uint32_t)nx * (uint32_t)ny)) - cz;
-        features(t_ratio, a, b, sqrt(x * x + y * y + z * z) / R, s.x[j]);
+        features(t_ratio, a, b, sqrt(x * x + y * y + z * z), R, s.x[j]);
     }
     __syncthreads();
     forward(s);
@@ -468,8 +476,8 @@ int mplb_mlp_device(const mplb_mlp* m) { return m->dev; }
 
 extern "C" {
 
-void mplb_mlp_features(double t_ratio, double a, double b, double r_over_R, float* out) {
-    features(t_ratio, a, b, r_over_R, out);
+void mplb_mlp_features(double t_ratio, double a, double b, double r, double R, float* out) {
+    features(t_ratio, a, b, r, R, out);
 }
 
 int mplb_mlp_create(int32_t device, uint64_t seed, mplb_mlp_t** out) {
@@ -543,14 +551,14 @@ int mplb_mlp_set_params(mplb_mlp_t* m, const float* in) {
     return upload_params(m, in);
 }
 
-int mplb_mlp_set_samples(mplb_mlp_t* m, const double* t_ratio, const double* a, const double* b,
-                         const double* r_over_R, const double* rho, uint32_t n) {
-    if (!m || !t_ratio || !a || !b || !r_over_R || !rho || n == 0)
+int mplb_mlp_set_samples(mplb_mlp_t* m, const double* t_ratio, const double* a, const double* b, const double* r,
+                         const double* R, const double* rho, uint32_t n) {
+    if (!m || !t_ratio || !a || !b || !r || !R || !rho || n == 0)
         return mplb_internal_fail(MPLB_E_ARG, "samples missing");
     std::vector<float> x((size_t)n * NIN), y(n);
     for (uint32_t i = 0; i < n; i++) {
-        if (!(b[i] > 0.0)) return mplb_internal_fail(MPLB_E_ARG, "b must be positive");
-        features(t_ratio[i], a[i], b[i], r_over_R[i], &x[(size_t)i * NIN]);
+        if (!(b[i] > 0.0) || !(R[i] > 0.0)) return mplb_internal_fail(MPLB_E_ARG, "b and R must be positive");
+        features(t_ratio[i], a[i], b[i], r[i], R[i], &x[(size_t)i * NIN]);
         y[i] = (float)(b[i] * rho[i]);
     }
     DevGuard g(m->dev);
@@ -589,14 +597,14 @@ int mplb_mlp_train(mplb_mlp_t* m, uint32_t steps, uint32_t batch, float lr, doub
     return 0;
 }
 
-int mplb_mlp_predict(mplb_mlp_t* m, const double* t_ratio, const double* a, const double* b,
-                     const double* r_over_R, uint32_t n, double* rho) {
-    if (!m || !t_ratio || !a || !b || !r_over_R || !rho) return mplb_internal_fail(MPLB_E_ARG, "NULL argument");
+int mplb_mlp_predict(mplb_mlp_t* m, const double* t_ratio, const double* a, const double* b, const double* r,
+                     const double* R, uint32_t n, double* rho) {
+    if (!m || !t_ratio || !a || !b || !r || !R || !rho) return mplb_internal_fail(MPLB_E_ARG, "NULL argument");
     if (n == 0) return 0;
     std::vector<float> x((size_t)n * NIN), y(n);
     for (uint32_t i = 0; i < n; i++) {
-        if (!(b[i] > 0.0)) return mplb_internal_fail(MPLB_E_ARG, "b must be positive");
-        features(t_ratio[i], a[i], b[i], r_over_R[i], &x[(size_t)i * NIN]);
+        if (!(b[i] > 0.0) || !(R[i] > 0.0)) return mplb_internal_fail(MPLB_E_ARG, "b and R must be positive");
+        features(t_ratio[i], a[i], b[i], r[i], R[i], &x[(size_t)i * NIN]);
     }
     DevGuard g(m->dev);
     float *dx = nullptr, *dy = nullptr;

@@ -6,8 +6,8 @@
 Pipeline:
   1. converge a grid of bubbles (T/Tc, R) with the plain FP64 solver
      (mplb_gpu_run_to_equilibrium) and take their radial density profiles;
-  2. train the 4-64-64-64-1 network on the device (the library's own forward,
-     backward and Adam kernels) on (T/Tc, a, b, r/R) -> b * rho samples;
+  2. train the 5-64-64-64-1 network on the device (the library's own forward,
+     backward and Adam kernels) on (T/Tc, a, b, r/R, R) -> b * rho samples;
   3. initialise new lattices from the network on the device
      (mplb_mlp_init_bubble) instead of the tanh/Maxwell profile.
 
@@ -29,7 +29,7 @@ import numpy as np
 
 from . import Lattice, MplbError, abi, cases, load_library
 
-NPARAM = 8705
+NPARAM = 8769
 HERE = os.path.dirname(os.path.abspath(__file__))
 DEFAULT_WEIGHTS = {abi.D2Q9: os.path.join(HERE, "data", "warmstart_d2q9.npz"),
                    abi.D3Q15: os.path.join(HERE, "data", "warmstart_d3q15.npz")}
@@ -48,11 +48,11 @@ def _lib():
             "mplb_mlp_destroy": ([H], C.c_int),
             "mplb_mlp_get_params": ([H, F], C.c_int),
             "mplb_mlp_set_params": ([H, F], C.c_int),
-            "mplb_mlp_features": ([C.c_double, C.c_double, C.c_double, C.c_double, F], None),
-            "mplb_mlp_set_samples": ([H, D, D, D, D, D, C.c_uint32], C.c_int),
+            "mplb_mlp_features": ([C.c_double, C.c_double, C.c_double, C.c_double, C.c_double, F], None),
+            "mplb_mlp_set_samples": ([H, D, D, D, D, D, D, C.c_uint32], C.c_int),
             "mplb_mlp_gradient": ([H, F, D], C.c_int),
             "mplb_mlp_train": ([H, C.c_uint32, C.c_uint32, C.c_float, D], C.c_int),
-            "mplb_mlp_predict": ([H, D, D, D, D, C.c_uint32, D], C.c_int),
+            "mplb_mlp_predict": ([H, D, D, D, D, D, C.c_uint32, D], C.c_int),
             "mplb_mlp_init_bubble": ([H, H, C.c_double, D, C.c_double, C.c_double], C.c_int),
         }
         for name, (args, res) in sig.items():
@@ -73,10 +73,10 @@ def _f64(a, n=None):
     return a, a.ctypes.data_as(C.POINTER(C.c_double))
 
 
-def features(t_ratio, a, b, r_over_R):
+def features(t_ratio, a, b, r, R):
     """The network's normalised inputs for one sample (library host code)."""
-    out = np.zeros(4, dtype=np.float32)
-    _lib().mplb_mlp_features(t_ratio, a, b, r_over_R, out.ctypes.data_as(C.POINTER(C.c_float)))
+    out = np.zeros(5, dtype=np.float32)
+    _lib().mplb_mlp_features(t_ratio, a, b, r, R, out.ctypes.data_as(C.POINTER(C.c_float)))
     return out
 
 
@@ -122,9 +122,9 @@ class Network:
         assert a.size == NPARAM
         self._check(self.lib.mplb_mlp_set_params(self.h, ptr))
 
-    def set_samples(self, t_ratio, a, b, r_over_R, rho):
+    def set_samples(self, t_ratio, a, b, r, R, rho):
         n = len(rho)
-        keep = [_f64(x, n) for x in (t_ratio, a, b, r_over_R, rho)]
+        keep = [_f64(x, n) for x in (t_ratio, a, b, r, R, rho)]
         self._check(self.lib.mplb_mlp_set_samples(self.h, *[k[1] for k in keep], n))
 
     def gradient(self):
@@ -138,9 +138,9 @@ class Network:
         self._check(self.lib.mplb_mlp_train(self.h, steps, batch, lr, C.byref(loss)))
         return loss.value
 
-    def predict(self, t_ratio, a, b, r_over_R):
-        n = len(np.atleast_1d(r_over_R))
-        keep = [_f64(x, n) for x in (t_ratio, a, b, r_over_R)]
+    def predict(self, t_ratio, a, b, r, R):
+        n = len(np.atleast_1d(r))
+        keep = [_f64(x, n) for x in (t_ratio, a, b, r, R)]
         out = np.zeros(n)
         self._check(self.lib.mplb_mlp_predict(self.h, *[k[1] for k in keep], n, abi.dptr(out)))
         return out
@@ -170,19 +170,22 @@ def radial(case):
     return np.sqrt(sum((case.points[:, i] - c[i]) ** 2 for i in range(D)))
 
 
-def profile_samples(case, rho, radius, rng, per_bin=48, bins=60):
+def profile_samples(case, rho, radius, rng, per_bin=48, bins=64):
     """Stratified samples of a converged profile: up to per_bin nodes in each
-    of `bins` equal r/R intervals on [0, 3], plus a few bulk nodes beyond."""
-    q = radial(case) / radius
+    of `bins` equal intervals of r - R on [-30, 30] (the network's clamped
+    range, 6 interface widths), plus some bulk nodes on either side beyond.
+    Returns (r, rho)."""
+    r = radial(case)
+    d = r - radius
     idx = []
-    edges = np.linspace(0.0, 3.0, bins + 1)
-    which = np.digitize(q, edges) - 1
-    for k in range(bins + 1):
-        sel = np.flatnonzero(which == k) if k < bins else np.flatnonzero(q >= 3.0)
+    edges = np.linspace(-30.0, 30.0, bins + 1)
+    which = np.digitize(d, edges) - 1
+    for k in range(-1, bins + 1):
+        sel = np.flatnonzero(which == k)
         if sel.size:
-            idx.append(rng.choice(sel, size=min(per_bin, sel.size), replace=False))
+            idx.append(rng.choice(sel, size=min(per_bin * (4 if k in (-1, bins) else 1), sel.size), replace=False))
     idx = np.concatenate(idx)
-    return q[idx], rho[idx]
+    return r[idx], rho[idx]
 
 
 def bubble(lattice, L, R, t_ratio):
@@ -216,24 +219,26 @@ def training_grid(lattice):
 
 
 def build_training_set(lattice, grid=None, seed=1, log=None, **conv):
+    """Converged bubbles of the grid -> samples (T/Tc, r, R, rho) and a record per bubble."""
     rng = np.random.default_rng(seed)
-    T, Q, Y, meta = [], [], [], []
+    T, Rs, Rr, Y, meta = [], [], [], [], []
     for L, R, t in grid or training_grid(lattice):
         c = bubble(lattice, L, R, t)
         rho, steps, rate, wall = converge(c, **conv)
-        q, r = profile_samples(c, rho, R, rng)
-        T.append(np.full(q.size, t))
-        Q.append(q)
-        Y.append(r)
+        r, y = profile_samples(c, rho, R, rng)
+        T.append(np.full(r.size, t))
+        Rs.append(r)
+        Rr.append(np.full(r.size, R))
+        Y.append(y)
         meta.append(dict(L=L, R=R, t_ratio=t, steps=steps, rate=rate, wall_s=wall))
         if log:
-            log(f"train-set L={L} R={R} t={t:.3f}: {steps} steps, {q.size} samples")
-    return np.concatenate(T), np.concatenate(Q), np.concatenate(Y), meta
+            log(f"train-set L={L} R={R} t={t:.3f}: {steps} steps, {r.size} samples")
+    return np.concatenate(T), np.concatenate(Rs), np.concatenate(Rr), np.concatenate(Y), meta
 
 
-def train(net, t, q, rho, steps=20000, batch=1024, lr=2e-3, lr_end=1e-4, chunks=10):
+def train(net, t, r, R, rho, steps=40000, batch=2048, lr=3e-3, lr_end=5e-5, chunks=12):
     """Adam with a stepwise geometric learning-rate decay; returns the loss history."""
-    net.set_samples(t, CS_A, CS_B, q, rho)
+    net.set_samples(t, CS_A, CS_B, r, R, rho)
     hist = []
     for k in range(chunks):
         rate = lr * (lr_end / lr) ** (k / max(chunks - 1, 1))
@@ -311,7 +316,7 @@ def main(argv=None):
     ap.add_argument("--lattice", choices=("d2q9", "d3q15"), default="d3q15")
     ap.add_argument("--weights", default=None)
     ap.add_argument("--out", default=None)
-    ap.add_argument("--steps", type=int, default=20000)
+    ap.add_argument("--steps", type=int, default=40000)
     ap.add_argument("--cases", type=int, default=64)
     ap.add_argument("--tol", type=float, default=1e-9)
     ap.add_argument("--check", type=int, default=1000)
@@ -322,13 +327,13 @@ def main(argv=None):
     log = lambda m: print(m, file=sys.stderr, flush=True)  # noqa: E731
     if a.cmd == "train":
         t0 = time.perf_counter()
-        t, q, rho, meta = build_training_set(lat, log=log, K=a.check, tol=a.tol)
+        t, r, R, rho, meta = build_training_set(lat, log=log, K=a.check, tol=a.tol)
         t1 = time.perf_counter()
         net = Network(seed=1)
-        hist = train(net, t, q, rho, steps=a.steps)
+        hist = train(net, t, r, R, rho, steps=a.steps)
         t2 = time.perf_counter()
-        pred = net.predict(t, CS_A, CS_B, q)
-        rep = dict(samples=int(q.size), cases=meta, loss=hist, data_s=t1 - t0, train_s=t2 - t1,
+        pred = net.predict(t, CS_A, CS_B, r, R)
+        rep = dict(samples=int(r.size), cases=meta, loss=hist, data_s=t1 - t0, train_s=t2 - t1,
                    fit_max_abs=float(np.abs(pred - rho).max()), fit_rms=float(np.sqrt(np.mean((pred - rho) ** 2))))
         net.save(a.weights or DEFAULT_WEIGHTS[lat])
         txt = json.dumps(rep, indent=1)

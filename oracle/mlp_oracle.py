@@ -3,9 +3,10 @@ TEST INFRASTRUCTURE ONLY: tests use it to check the device forward pass and
 gradients; the product never imports it.
 
 The network has no counterpart in the reference.  What is restated here:
-  * the parameter layout W1[64][4], b1, W2[64][64], b2, W3[64][64], b3,
-    W4[64], b4 (8705 floats);
-  * the input features (T/Tc, a, b, r/R) -> normalised, BF16-rounded;
+  * the parameter layout W1[64][5], b1, W2[64][64], b2, W3[64][64], b3,
+    W4[64], b4 (8769 floats);
+  * the input features (T/Tc, a, b, r, R) -> (T/Tc, a, b, (r - R)/5 clamped
+    to [-6, 6], 5/R), normalised, BF16-rounded;
   * the forward pass: BF16 weights, tanh hidden units whose outputs are
     rounded to BF16, FP32 biases, a linear output (b * rho);
   * the gradient of the mean squared error, with the BF16 roundings treated
@@ -16,7 +17,7 @@ to FP32 rounding, not bit for bit.
 """
 import numpy as np
 
-NIN, NH = 4, 64
+NIN, NH = 5, 64
 OFF = {}
 _o = 0
 for _name, _size in (("W1", NH * NIN), ("b1", NH), ("W2", NH * NH), ("b2", NH), ("W3", NH * NH), ("b3", NH),
@@ -33,12 +34,14 @@ def bf16(x):
     return u.astype(np.uint32).view(np.float32)
 
 
-def features(t_ratio, a, b, r_over_R):
-    r = np.clip(np.asarray(r_over_R, dtype=np.float64), 0.0, 3.0)
+def features(t_ratio, a, b, r, R):
+    R = np.asarray(R, dtype=np.float64)
+    d = np.clip((np.asarray(r, dtype=np.float64) - R) / 5.0, -6.0, 6.0)
     cols = [(np.asarray(t_ratio, dtype=np.float64) - 0.775) / 0.175,
             np.asarray(a, dtype=np.float64) - 1.0,
             np.asarray(b, dtype=np.float64) * 0.25 - 1.0,
-            (r - 1.5) / 1.5]
+            d / 6.0,
+            (5.0 / R - 0.3) / 0.3]
     return np.stack([bf16(np.asarray(c, dtype=np.float32)) for c in np.broadcast_arrays(*cols)], axis=-1)
 
 

@@ -14,26 +14,27 @@ pytestmark = pytest.mark.gpu
 def samples(n, seed=0):
     rng = np.random.default_rng(seed)
     t = rng.uniform(0.6, 0.95, n)
-    q = rng.uniform(0.0, 3.2, n)
+    R = rng.uniform(8.0, 60.0, n)
+    r = rng.uniform(0.0, 2.5, n) * R
     # a smooth stand-in for a bubble profile: vapour inside, liquid outside
-    rho = 0.02 + 0.3 * (0.5 + 0.5 * np.tanh(6.0 * (q - 1.0))) * (1.3 - t)
-    return t, q, rho
+    rho = 0.02 + 0.3 * (0.5 + 0.5 * np.tanh((r - R) / 2.5)) * (1.3 - t) + 0.05 / R
+    return t, r, R, rho
 
 
-def oracle_inputs(t, q, rho):
-    X = np.stack([np.ravel(mo.features(a, 1.0, 4.0, b)) for a, b in zip(t, q)])
+def oracle_inputs(t, r, R, rho):
+    X = np.stack([np.ravel(mo.features(a, 1.0, 4.0, x, y)) for a, x, y in zip(t, r, R)])
     Y = (4.0 * rho).astype(np.float32).astype(np.float64)
     return X, Y
 
 
 @pytest.mark.parametrize("n", [1, 31, 32, 33, 1000])
 def test_gradient_matches_oracle(gpu_lib, n):
-    t, q, rho = samples(n, seed=n)
+    t, r, R, rho = samples(n, seed=n)
     with warmstart.Network(seed=11) as net:
-        net.set_samples(t, 1.0, 4.0, q, rho)
+        net.set_samples(t, 1.0, 4.0, r, R, rho)
         g, loss = net.gradient()
         p = net.params()
-    X, Y = oracle_inputs(t, q, rho)
+    X, Y = oracle_inputs(t, r, R, rho)
     lw, gw = mo.loss_and_grad(p, X, Y)
     # FP32 accumulation (device) against FP64 (oracle) on the same BF16 operands
     assert abs(loss - lw) <= 1e-5 * lw, (loss, lw)
@@ -44,11 +45,11 @@ def test_gradient_matches_oracle(gpu_lib, n):
 
 
 def test_predict_matches_oracle(gpu_lib):
-    t, q, _ = samples(777, seed=2)
+    t, r, R, rho = samples(777, seed=2)
     with warmstart.Network(seed=5) as net:
-        y = net.predict(t, 1.0, 4.0, q)
+        y = net.predict(t, 1.0, 4.0, r, R)
         p = net.params()
-    X, _ = oracle_inputs(t, q, q)
+    X, _ = oracle_inputs(t, r, R, rho)
     _, out = mo.forward(p, X)
     # Agreement to FP32 accumulation, except where an activation sits on a
     # BF16 rounding boundary and the FP32 (device) and FP64 (oracle) sums
@@ -60,11 +61,11 @@ def test_predict_matches_oracle(gpu_lib):
 
 
 def test_training_reduces_loss(gpu_lib):
-    t, q, rho = samples(20000, seed=4)
+    t, r, R, rho = samples(20000, seed=4)
     with warmstart.Network(seed=3) as net:
-        net.set_samples(t, 1.0, 4.0, q, rho)
+        net.set_samples(t, 1.0, 4.0, r, R, rho)
         _, l0 = net.gradient()
-        hist = warmstart.train(net, t, q, rho, steps=3000, batch=512, lr=2e-3, lr_end=2e-4, chunks=3)
+        hist = warmstart.train(net, t, r, R, rho, steps=3000, batch=512, lr=2e-3, lr_end=2e-4, chunks=3)
         _, l1 = net.gradient()
     print("loss", l0, hist, l1)
     assert l1 < 1e-2 * l0
@@ -77,7 +78,7 @@ def test_init_bubble_equals_predict(gpu_lib):
         net.init_bubble(lat, 0.8, warmstart.centre(c), 9.0, c.meta["T"])
         lat.initialize()
         out = lat.download()
-        want = net.predict(0.8, 1.0, 4.0, warmstart.radial(c) / 9.0)
+        want = net.predict(0.8, 1.0, 4.0, warmstart.radial(c), 9.0)
     assert np.array_equal(out["rho"], want)
     assert np.all(out["U"] == 0.0) and np.all(out["T"] == c.meta["T"])
 
@@ -89,9 +90,9 @@ def test_warm_start_gains_over_tanh(gpu_lib):
     is closer to the converged one than the tanh/Maxwell profile."""
     grid = [(48, R, t) for R in (7.0, 10.0, 13.0) for t in (0.65, 0.75, 0.85, 0.95)]
     K, tol = 500, 1e-9
-    t, q, rho, meta = warmstart.build_training_set(abi.D2Q9, grid, K=K, tol=tol, max_steps=60000)
+    t, r, R, rho, meta = warmstart.build_training_set(abi.D2Q9, grid, K=K, tol=tol, max_steps=60000)
     with warmstart.Network(seed=2) as net:
-        warmstart.train(net, t, q, rho, steps=6000, batch=1024, lr=3e-3, lr_end=1e-4, chunks=6)
+        warmstart.train(net, t, r, R, rho, steps=8000, batch=2048, lr=3e-3, lr_end=1e-4, chunks=8)
         spec = dict(L=48, radius=11.5, t_ratio=0.8)
         c = warmstart.bubble(abi.D2Q9, spec["L"], spec["radius"], spec["t_ratio"])
         rho_eq, plain_steps, _, _ = warmstart.converge(c, K=K, tol=tol, max_steps=60000)

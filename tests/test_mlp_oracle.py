@@ -8,7 +8,7 @@ from oracle import mlp_oracle as mo
 def test_oracle_backward_matches_finite_differences():
     rng = np.random.default_rng(3)
     p = rng.normal(0.0, 0.3, mo.NPARAM)
-    X = rng.uniform(-1, 1, (40, 4))
+    X = rng.uniform(-1, 1, (40, mo.NIN))
     Y = rng.uniform(0, 1.5, 40)
     _, g = mo.loss_and_grad64(p, X, Y)
     idx = np.concatenate([rng.choice(mo.NPARAM, 60, replace=False),
@@ -31,9 +31,10 @@ def test_bf16_rounding_is_nearest_even():
 def test_features_match_library_host_code():
     from multiphaselb_b200 import warmstart
     rng = np.random.default_rng(5)
-    for _ in range(200):
-        t, r = rng.uniform(0.5, 1.0), rng.uniform(-0.5, 4.0)
+    for _ in range(300):
+        t, R = rng.uniform(0.5, 1.0), rng.uniform(4.0, 200.0)
+        r = rng.uniform(0.0, 3.0 * R)
         a, b = rng.choice([1.0, 0.5]), rng.choice([4.0, 2.0])
-        want = np.ravel(mo.features(t, a, b, r)).astype(np.float32)
-        got = warmstart.features(t, a, b, r)
-        assert np.array_equal(got, want), (t, a, b, r, got, want)
+        want = np.ravel(mo.features(t, a, b, r, R)).astype(np.float32)
+        got = warmstart.features(t, a, b, r, R)
+        assert np.array_equal(got, want), (t, a, b, r, R, got, want)
