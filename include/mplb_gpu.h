@@ -219,12 +219,16 @@ int mplb_gpu_mass_energy(mplb_gpu_t* h, double* mass, double* energy);
  * pointer may be NULL.  Needs an updated flow field. */
 int mplb_gpu_monitor(mplb_gpu_t* h, int32_t reset, double* max_drho, double* mass);
 
-/* Step to equilibrium.  The reference's driver (src/app/multiPhasePP.c)
+/* Step to equilibrium.  The reference's driver (src/applications/solvers/multiPhasePP/multiPhasePP.c)
  * runs a fixed number of steps; this runs whole intervals of check_interval
  * steps until max over nodes |rho(t) - rho(t - K)| / K < tol, or max_steps
  * (rounded up to a whole interval).  rho is monitored as by mplb_gpu_monitor,
- * one read pass per check.  *steps: steps taken; *rate:
- * the last max |drho/dt| (either may be NULL).  Needs an updated flow field. */
+ * one read pass per check.  *steps: steps taken; *rate: the last
+ * max |drho/dt| (either may be NULL).  A non-finite density stops the run
+ * with MPLB_E_NONFINITE (*steps and *rate = inf filled in).  FP32-deviation
+ * form: the lattice's total momentum is reset to its starting value at every
+ * check when the lattice is fully periodic without net body force.  Needs an
+ * updated flow field. */
 int mplb_gpu_run_to_equilibrium(mplb_gpu_t* h, uint32_t max_steps, uint32_t check_interval, double tol,
                                 uint32_t* steps, double* rate);
 
@@ -248,7 +252,7 @@ int mplb_mass_energy_noalloc(const double* rho, const double* T, uint32_t n, dou
 
 /* ------------------------------------------------------------------------
  * Batched ensemble.  No counterpart in the reference, whose driver
- * (src/app/multiPhasePP.c) advances one lattice per process: here many
+ * (src/applications/solvers/multiPhasePP/multiPhasePP.c) advances one lattice per process: here many
  * independent lattices -- each an ordinary handle created above -- advance
  * together, one kernel launch per time step for all of them, a block taking
  * (lattice, tile) pairs from a work table.  Each lattice's steps are the
@@ -291,7 +295,10 @@ int mplb_batch_info_get(mplb_batch_t* b, mplb_batch_info* info);
 int mplb_batch_step(mplb_batch_t* b, uint32_t nsteps);
 /* Advance lattices in check intervals of K = check_interval steps until each
  * has max |drho/dt| < tol (rho as the next step sums it, over one interval),
- * or has taken max_steps (rounded up to a whole interval).  A converged
+ * or has taken max_steps (rounded up to a whole interval), or has a
+ * non-finite density (retired, rate = inf, not counted as converged).  Each
+ * check also resets every lattice's total momentum to its starting value
+ * (lattices without net body force).  A converged
  * lattice leaves the work table and stops.  Each interval -- K step launches
  * and one check launch -- replays one captured CUDA graph.
  * steps_out[i]: steps lattice i took; rate_out[i]: its last max |drho/dt|
@@ -342,6 +349,16 @@ int mplb_mlp_predict(mplb_mlp_t* m, const double* t_ratio, const double* a, cons
  * mplb_gpu_upload.  The handle and the network must be on one device. */
 int mplb_mlp_init_bubble(mplb_mlp_t* m, mplb_gpu_t* h, double t_ratio, const double* center, double radius,
                          double T);
+/* As mplb_mlp_init_bubble, with the lattice's total density made equal to
+ * target_mass (e.g. the mass of the tanh/Maxwell state being replaced, so
+ * that both relax to the same equilibrium).  The network's inputs are BF16,
+ * so its mass is a step function of the radius: the radius is bracketed to
+ * one step (secant, then bisection) and the two fields are blended to hold
+ * the target mass -- the bulk densities stay the network's, the interface
+ * moves by a fraction of a step.  *radius_used (may be NULL) receives the
+ * effective radius.  Allocates one scratch array of n doubles. */
+int mplb_mlp_init_bubble_mass(mplb_mlp_t* m, mplb_gpu_t* h, double t_ratio, const double* center, double radius,
+                              double T, double target_mass, double* radius_used);
 
 #ifdef __cplusplus
 }

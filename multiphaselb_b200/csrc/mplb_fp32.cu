@@ -359,7 +359,7 @@ __global__ void __launch_bounds__(TX * TY)
             double rho, T;
             pull_node32<D2Q9T, true, false, false>(Ps[w.x], A, x, y, 0, id, f, g, rho, T, dr, dT);
             double* snap = snaps[w.x];
-            d = fabs(rho - snap[id]);
+            d = isfinite(rho) ? fabs(rho - snap[id]) : INFINITY;  // +inf orders above every finite bit pattern
             snap[id] = rho;
             node_momentum_fx<D2Q9T>(A.fin, A.n, id, m);
         }

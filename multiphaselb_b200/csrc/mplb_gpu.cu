@@ -8,6 +8,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cmath>
 #include <cstdio>
 #include <cstring>
 #include <string>
@@ -157,6 +158,17 @@ bool momentum_conserved(const mplb_gpu* h) {
     return h->P.f_update != 0;
 }
 
+// x = (1 - w) a + w x
+__global__ void k_blend(uint32_t n, double w, const double* __restrict__ a, double* __restrict__ x) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) x[i] = (1.0 - w) * a[i] + w * x[i];
+}
+
+__global__ void k_add(uint32_t n, double v, double* __restrict__ x) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) x[i] += v;
+}
+
 __global__ void k_fill(uint32_t n, double v, double* __restrict__ x) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n) x[i] = v;
@@ -176,7 +188,8 @@ __global__ void k_monitor_partial(uint32_t n, int Q, const T* __restrict__ f, do
         T s = 0;
         for (int k = 0; k < Q; k++) s += f[(size_t)k * n + i];
         const double r = ref + (double)s;
-        if (!first) m = fmax(m, fabs(r - snap[i]));
+        // fmax drops NaN: a non-finite density must show as an infinite change
+        if (!first) m = isfinite(r) ? fmax(m, fabs(r - snap[i])) : INFINITY;
         snap[i] = r;
         mass += r;
     }
@@ -1159,6 +1172,11 @@ int mplb_gpu_run_to_equilibrium(mplb_gpu_t* h, uint32_t max_steps, uint32_t chec
         RET(mplb_gpu_step(h, check_interval));
         done += check_interval;
         RET(mplb_gpu_monitor(h, 0, &d, nullptr));
+        if (!std::isfinite(d)) {
+            if (steps) *steps = done;
+            if (rate) *rate = d;
+            return fail(MPLB_E_NONFINITE, "non-finite density after " + std::to_string(done) + " steps");
+        }
         if (fix) {
             RET(momentum(h->mom));
             cudaError_t e = mplb_mom_fix32(h->lat, h->n, h->p32[0][h->cur32[0]], h->mom, h->mom + 3, h->stream);
@@ -1190,6 +1208,96 @@ int mplb_mlp_init_bubble(mplb_mlp_t* m, mplb_gpu_t* h, double t_ratio, const dou
     h->launches++;
     RET(launch_check(h));
     h->initialized = false;
+    return 0;
+}
+
+int mplb_mlp_init_bubble_mass(mplb_mlp_t* m, mplb_gpu_t* h, double t_ratio, const double* center, double radius,
+                              double T, double target_mass, double* radius_used) {
+    if (!m || !h || !center) return fail(MPLB_E_ARG, "NULL argument");
+    if (!(radius > 0.0) || !(target_mass > 0.0)) return fail(MPLB_E_ARG, "radius and mass must be positive");
+    DeviceGuard guard(h->dev);
+    const int parts = std::min<int>(h->red_parts, (int)blocks(h->n));
+    auto total = [&](double* M) -> int {
+        k_sum2_partial<<<parts, TPB, 0, h->stream>>>(h->n, h->rho, nullptr, h->red);
+        k_sum2_final<<<1, TPB, 0, h->stream>>>(parts, h->red, h->red + 2 * h->red_parts);
+        h->launches += 2;
+        RET(launch_check(h));
+        CK(cudaMemcpyAsync(M, h->red + 2 * h->red_parts, sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+        CK(cudaStreamSynchronize(h->stream));
+        return 0;
+    };
+    // mass of the network's bubble of radius R, minus the target
+    auto mass_at = [&](double R, double* f) -> int {
+        RET(mplb_mlp_init_bubble(m, h, t_ratio, center, R, T));
+        RET(total(f));
+        *f -= target_mass;
+        return 0;
+    };
+    // The mass falls as the bubble grows, but the network's inputs are BF16,
+    // so it is a step function of R.  Secant steps to get close, bracket
+    // [ra, rb] with f(ra) >= 0 >= f(rb), bisect down to one step, then blend
+    // the two fields so that the lattice holds the target mass exactly: the
+    // bulk densities stay the network's, the interface moves by a fraction of
+    // a step.
+    double r0 = radius, r1 = radius * 1.02, f0 = 0, f1 = 0;
+    RET(mass_at(r0, &f0));
+    RET(mass_at(r1, &f1));
+    for (int it = 0; it < 8 && f1 != f0 && f1 != 0.0; it++) {
+        const double r2 = std::min(2.0 * radius, std::max(0.5 * radius, r1 - f1 * (r1 - r0) / (f1 - f0)));
+        r0 = r1;
+        f0 = f1;
+        r1 = r2;
+        RET(mass_at(r1, &f1));
+    }
+    double ra = r1, fa = f1, rb = r1, fb = f1, step = 0.01 * r1;
+    for (int it = 0; it < 40 && !(fa >= 0.0 && fb <= 0.0); it++, step *= 2.0) {
+        if (fa < 0.0) {
+            ra = std::max(1e-3, ra - step);
+            RET(mass_at(ra, &fa));
+        }
+        if (fb > 0.0) {
+            rb += step;
+            RET(mass_at(rb, &fb));
+        }
+    }
+    double w = 0.0;  // weight of the rb field
+    if (fa >= 0.0 && fb <= 0.0) {
+        for (int it = 0; it < 40 && rb - ra > 1e-9 * radius && fa != 0.0 && fb != 0.0; it++) {
+            const double rm = 0.5 * (ra + rb);
+            double fm = 0;
+            RET(mass_at(rm, &fm));
+            if (fm >= 0.0) {
+                ra = rm;
+                fa = fm;
+            } else {
+                rb = rm;
+                fb = fm;
+            }
+        }
+        w = (fa == fb) ? 0.0 : fa / (fa - fb);
+    }
+    double* tmp = nullptr;
+    CK(cudaMalloc((void**)&tmp, (size_t)h->n * sizeof(double)));
+    auto blend = [&]() -> int {
+        RET(mass_at(ra, &fa));
+        CK(cudaMemcpyAsync(tmp, h->rho, (size_t)h->n * sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
+        RET(mass_at(rb, &fb));
+        k_blend<<<blocks(h->n), TPB, 0, h->stream>>>(h->n, w, tmp, h->rho);
+        h->launches++;
+        RET(launch_check(h));
+        // the blend's rounding (far below the network's error) goes uniformly
+        double M = 0;
+        RET(total(&M));
+        k_add<<<blocks(h->n), TPB, 0, h->stream>>>(h->n, (target_mass - M) / (double)h->n, h->rho);
+        h->launches++;
+        RET(launch_check(h));
+        CK(cudaStreamSynchronize(h->stream));
+        return 0;
+    };
+    const int rc = blend();
+    cudaFree(tmp);
+    if (rc) return rc;
+    if (radius_used) *radius_used = ra + w * (rb - ra);
     return 0;
 }
 
@@ -1590,10 +1698,10 @@ int mplb_batch_run(mplb_batch_t* b, uint32_t max_steps, uint32_t* steps_out, dou
             double d;
             std::memcpy(&d, &b->hmax[i], sizeof(double));
             rate[i] = d / b->K;
-            if (rate[i] < b->tol) {
+            if (rate[i] < b->tol || !std::isfinite(rate[i])) {  // converged, or failed (non-finite)
                 active[i] = 0;
                 left--;
-                conv++;
+                if (std::isfinite(rate[i])) conv++;
                 retired = true;
             }
         }

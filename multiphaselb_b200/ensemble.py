@@ -28,7 +28,7 @@ import time
 
 import numpy as np
 
-from . import Batch, Lattice, abi, cases
+from . import Batch, Lattice, abi, cases, warmstart
 
 SIZES = (64, 96, 128, 192, 256, 384, 512)
 SEED = 20240611
@@ -44,12 +44,9 @@ def draw(n, seed=SEED):
     return [dict(L=int(a), t_ratio=float(b), radius=float(c)) for a, b, c in zip(L, t, R)]
 
 
-def make_case(spec, init=None):
-    c = cases.bubble_case(abi.D2Q9, L=spec["L"], radius=spec["radius"], width=WIDTH, t_ratio=spec["t_ratio"],
-                          name=f"bubble_d2q9_{spec['L']}_t{spec['t_ratio']:.3f}_r{spec['radius']:.1f}")
-    if init is not None:
-        c.rho = np.ascontiguousarray(init(c), dtype=np.float64)
-    return c
+def make_case(spec):
+    return cases.bubble_case(abi.D2Q9, L=spec["L"], radius=spec["radius"], width=WIDTH, t_ratio=spec["t_ratio"],
+                             name=f"bubble_d2q9_{spec['L']}_t{spec['t_ratio']:.3f}_r{spec['radius']:.1f}")
 
 
 def coexistence(case, rho):
@@ -68,28 +65,35 @@ def run_plain(specs, K, tol, max_steps, log=None):
             lat.initialize()
             lat.sync()
             t0 = time.perf_counter()
-            steps, rate = lat.run_to_equilibrium(max_steps, K, tol)
+            steps, rate = warmstart.run_eq(lat, max_steps, K, tol)
             lat.sync()
             wall = time.perf_counter() - t0
             rv, rl = coexistence(c, lat.download()["rho"])
-        out.append(dict(steps=steps, rate=rate, wall_s=wall, rho_v=rv, rho_l=rl))
+        out.append(dict(steps=steps, rate=rate, wall_s=wall, rho_v=rv, rho_l=rl, diverged=bool(not np.isfinite(rate))))
         if log:
             log(f"plain {i} L={s['L']} t={s['t_ratio']:.3f} R={s['radius']:.1f}: {steps} steps {wall:.2f} s")
     return out
 
 
 def run_batched(specs, K, tol, max_steps, init=None, tile_config=0):
+    """All specs as one batch.  `init(lat, case)` (the learned warm start) may
+    replace a lattice's tanh/Maxwell state on the device; it returns False to
+    keep the fallback."""
     t0 = time.perf_counter()
-    cs = [make_case(s, init) for s in specs]
-    lats = []
+    cs = [make_case(s) for s in specs]
+    t1 = time.perf_counter()
+    lats, warm = [], 0
     for c in cs:
         lat = Lattice(c, path=abi.PATH_FUSED, precision=abi.FP32_DEV)
         lat.upload_case()
+        if init is not None and init(lat, c):
+            warm += 1
         lat.initialize()
         lats.append(lat)
     for lat in lats:
         lat.sync()
-    setup = time.perf_counter() - t0
+    t2 = time.perf_counter()
+    host_s, setup = t1 - t0, t2 - t1
     with Batch(lats, check_interval=K, tol=tol, tile_config=tile_config) as b:
         t0 = time.perf_counter()
         steps, rate, conv = b.run(max_steps)
@@ -99,10 +103,10 @@ def run_batched(specs, K, tol, max_steps, init=None, tile_config=0):
     res = []
     for c, lat, st, r in zip(cs, lats, steps, rate):
         rv, rl = coexistence(c, lat.download()["rho"])
-        res.append(dict(steps=int(st), rate=float(r), rho_v=rv, rho_l=rl))
+        res.append(dict(steps=int(st), rate=float(r), rho_v=rv, rho_l=rl, diverged=bool(not np.isfinite(r))))
         lat.close()
-    return dict(cases=res, wall_s=wall, setup_s=setup, converged=conv, info=info,
-                nodes=int(sum(c.n for c in cs)))
+    return dict(cases=res, wall_s=wall, setup_s=setup, host_build_s=host_s, warm_started=warm, converged=conv,
+                info=info, nodes=int(sum(c.n for c in cs)))
 
 
 def main(argv=None):
@@ -114,6 +118,7 @@ def main(argv=None):
     ap.add_argument("--check", type=int, default=1000)
     ap.add_argument("--max-steps", type=int, default=400000)
     ap.add_argument("--init", choices=("tanh", "mlp"), default="tanh")
+    ap.add_argument("--weights", default=None, help="warm-start weights (.npz); default: the packaged D2Q9 network")
     ap.add_argument("--sizes", default=None, help="comma list: one case per size at T/Tc=0.8, R=0.2L")
     ap.add_argument("--out", default=None)
     a = ap.parse_args(argv)
@@ -123,8 +128,9 @@ def main(argv=None):
         specs = draw(a.cases, a.seed)
     init = None
     if a.init == "mlp":
-        from . import warmstart
-        init = warmstart.initializer(abi.D2Q9)
+        init = warmstart.initializer(abi.D2Q9, a.weights)
+        if init is None:
+            raise SystemExit("no trained warm-start weights")
     log = lambda m: print(m, file=sys.stderr, flush=True)  # noqa: E731
     rep = dict(specs=specs, tol=a.tol, check_interval=a.check, max_steps=a.max_steps, init=a.init)
     b = run_batched(specs, a.check, a.tol, a.max_steps, init)
@@ -136,10 +142,15 @@ def main(argv=None):
         rep["plain"] = p
         sub = run_batched(specs[:m], a.check, a.tol, a.max_steps, init)
         rep["batched_subset"] = sub
+        both = [(x, y) for x, y in zip(sub["cases"], p) if not x["diverged"] and not y["diverged"]]
         rel = [max(abs(x["rho_v"] - y["rho_v"]) / y["rho_v"], abs(x["rho_l"] - y["rho_l"]) / y["rho_l"])
-               for x, y in zip(sub["cases"], p)]
+               for x, y in both]
         rep["subset"] = dict(cases=m, plain_wall_s=sum(x["wall_s"] for x in p), batched_wall_s=sub["wall_s"],
-                             speedup=sum(x["wall_s"] for x in p) / sub["wall_s"], max_rel_coexistence=max(rel))
+                             speedup=sum(x["wall_s"] for x in p) / sub["wall_s"],
+                             plain_diverged=sum(1 for y in p if y["diverged"]),
+                             batched_diverged=sum(1 for x in sub["cases"] if x["diverged"]),
+                             max_rel_coexistence=max(rel, default=None),
+                             within_1e3=sum(1 for r in rel if r < 1e-3), compared=len(rel))
         log(json.dumps(rep["subset"]))
     txt = json.dumps(rep, indent=1)
     if a.out:

@@ -54,6 +54,7 @@ def _lib():
             "mplb_mlp_train": ([H, C.c_uint32, C.c_uint32, C.c_float, D], C.c_int),
             "mplb_mlp_predict": ([H, D, D, D, D, D, C.c_uint32, D], C.c_int),
             "mplb_mlp_init_bubble": ([H, H, C.c_double, D, C.c_double, C.c_double], C.c_int),
+            "mplb_mlp_init_bubble_mass": ([H, H, C.c_double, D, C.c_double, C.c_double, C.c_double, D], C.c_int),
         }
         for name, (args, res) in sig.items():
             fn = getattr(lib, name)
@@ -194,14 +195,26 @@ def bubble(lattice, L, R, t_ratio):
     return cases.bubble_case(abi.D3Q15, L=L, radius=R, width=5.0, t_ratio=t_ratio)
 
 
+def run_eq(lat, max_steps, K, tol):
+    """run_to_equilibrium that reports a diverged run (non-finite density) as
+    (steps, inf) instead of raising."""
+    try:
+        return lat.run_to_equilibrium(max_steps, K, tol)
+    except MplbError as e:
+        if e.code != abi.E_NONFINITE:
+            raise
+        return max_steps, float("inf")
+
+
 def converge(case, K=1000, tol=1e-9, max_steps=400000, precision=abi.FP64):
-    """The plain solver to equilibrium: (rho, steps, rate, wall seconds)."""
+    """The plain solver to equilibrium: (rho, steps, rate, wall seconds);
+    rate = inf if the run diverged."""
     with Lattice(case, path=abi.PATH_FUSED, precision=precision) as lat:
         lat.upload_case()
         lat.initialize()
         lat.sync()
         t0 = time.perf_counter()
-        steps, rate = lat.run_to_equilibrium(max_steps, K, tol)
+        steps, rate = run_eq(lat, max_steps, K, tol)
         lat.sync()
         wall = time.perf_counter() - t0
         rho = lat.download()["rho"]
@@ -225,6 +238,10 @@ def build_training_set(lattice, grid=None, seed=1, log=None, **conv):
     for L, R, t in grid or training_grid(lattice):
         c = bubble(lattice, L, R, t)
         rho, steps, rate, wall = converge(c, **conv)
+        if not np.isfinite(rate) or not np.all(np.isfinite(rho)):
+            if log:
+                log(f"train-set L={L} R={R} t={t:.3f}: diverged, skipped")
+            continue
         r, y = profile_samples(c, rho, R, rng)
         T.append(np.full(r.size, t))
         Rs.append(r)
@@ -246,11 +263,23 @@ def train(net, t, r, R, rho, steps=40000, batch=2048, lr=3e-3, lr_end=5e-5, chun
     return hist
 
 
+def place(net, lat, t_ratio, centre_, R, T, mass):
+    """The network's bubble on the lattice with the lattice holding `mass`
+    (the mass of the state it replaces), so that the case relaxes to the same
+    equilibrium as from its tanh/Maxwell state, only from closer
+    (mplb_mlp_init_bubble_mass).  Returns the effective radius."""
+    c, cp = _f64(np.asarray(centre_, dtype=np.float64).ravel().tolist() + [0.0] * (3 - len(centre_)))
+    used = C.c_double()
+    net._check(net.lib.mplb_mlp_init_bubble_mass(net.h, lat.h, t_ratio, cp, R, T, mass, C.byref(used)))
+    return used.value
+
+
 def initializer(lattice, weights=None, device=-1):
     """Function (lat, case) -> bool that overwrites a freshly uploaded bubble
-    lattice with the network's profile, or returns False (the caller keeps
-    the tanh/Maxwell state) when the case is outside the trained ranges or no
-    trained weights exist."""
+    lattice with the network's profile (same mass as the uploaded state, see
+    `place`), or returns False (the caller keeps the tanh/Maxwell state) when
+    the case is outside the trained ranges.  None when no trained weights
+    exist."""
     path = weights or DEFAULT_WEIGHTS[lattice]
     if not os.path.exists(path):
         return None
@@ -261,10 +290,12 @@ def initializer(lattice, weights=None, device=-1):
         t_ratio = m["T"] / m["Tc"]
         if not (T_RANGE[0] - 1e-9 <= t_ratio <= T_RANGE[1] + 1e-9) or case.eos["type"] != abi.EOS_CS:
             return False
-        net.init_bubble(lat, t_ratio, centre(case), m["radius"], m["T"])
+        mass = lat.mass_energy()[0]
+        init.radius = place(net, lat, t_ratio, centre(case), m["radius"], m["T"], mass)
         return True
 
     init.net = net
+    init.radius = None
     return init
 
 
@@ -286,17 +317,23 @@ def evaluate(lattice, init, specs, K=1000, tol=1e-9, max_steps=400000, precision
                 rho0 = lat.download()["rho"] if mode == "warm" else None
                 lat.sync()
                 t0 = time.perf_counter()
-                steps, rate = lat.run_to_equilibrium(max_steps, K, tol)
+                steps, rate = run_eq(lat, max_steps, K, tol)
                 lat.sync()
                 wall = time.perf_counter() - t0
                 rho = lat.download()["rho"]
-            rec[mode] = dict(steps=steps, rate=rate, wall_s=wall)
+            rec[mode] = dict(steps=steps, rate=rate, wall_s=wall, diverged=bool(not np.isfinite(rate)))
+            if mode == "warm":
+                rec["warm"]["radius_used"] = init.radius
             if mode == "plain":
                 rho_eq = rho
-            else:
+                rec["tanh_err_max"] = float(np.abs(c.rho - rho_eq).max() / rho_eq.max())
+            elif not rec["plain"]["diverged"] and not rec["warm"]["diverged"]:
                 # the converged plain solver judges the network's initial profile
                 rec["init_err_max"] = float(np.abs(rho0 - rho_eq).max() / rho_eq.max())
                 rec["final_rel_diff"] = float(np.abs(rho - rho_eq).max() / rho_eq.max())
+                ctr = int(np.argmin(radial(c)))
+                rec["coexistence_rel_diff"] = float(max(abs(rho[ctr] - rho_eq[ctr]) / rho_eq[ctr],
+                                                        abs(rho[0] - rho_eq[0]) / rho_eq[0]))
         rows.append(rec)
         if log:
             log(json.dumps(rec))
@@ -346,12 +383,20 @@ def main(argv=None):
             from .ensemble import draw
             specs = draw(a.cases)
         rows = evaluate(lat, init, specs, a.check, a.tol, precision=prec, log=log)
-        ok = [r for r in rows if r.get("warm")]
-        summ = dict(cases=len(rows), warm_used=len(ok),
-                    plain_steps=int(sum(r["plain"]["steps"] for r in rows)),
+        ok = [r for r in rows if r.get("warm") and not r["warm"]["diverged"] and not r["plain"]["diverged"]]
+        summ = dict(cases=len(rows), warm_used=sum(1 for r in rows if r.get("warm")),
+                    plain_diverged=sum(1 for r in rows if r["plain"]["diverged"]),
+                    warm_diverged=sum(1 for r in rows if r.get("warm") and r["warm"]["diverged"]),
+                    compared=len(ok),
+                    plain_steps=int(sum(r["plain"]["steps"] for r in ok)),
                     warm_steps=int(sum(r["warm"]["steps"] for r in ok)),
-                    plain_wall_s=float(sum(r["plain"]["wall_s"] for r in rows)),
-                    warm_wall_s=float(sum(r["warm"]["wall_s"] for r in ok)))
+                    plain_wall_s=float(sum(r["plain"]["wall_s"] for r in ok)),
+                    warm_wall_s=float(sum(r["warm"]["wall_s"] for r in ok)),
+                    fewer_steps=sum(1 for r in ok if r["warm"]["steps"] < r["plain"]["steps"]),
+                    more_steps=sum(1 for r in ok if r["warm"]["steps"] > r["plain"]["steps"]),
+                    median_tanh_err=float(np.median([r["tanh_err_max"] for r in ok])) if ok else None,
+                    median_init_err=float(np.median([r["init_err_max"] for r in ok])) if ok else None,
+                    max_coexistence_rel_diff=max([r["coexistence_rel_diff"] for r in ok], default=None))
         txt = json.dumps(dict(summary=summ, rows=rows), indent=1)
         log(json.dumps(summ))
     if a.out:

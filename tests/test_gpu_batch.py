@@ -140,3 +140,17 @@ def test_batch_rejects_ineligible(gpu_lib):
         Batch([good], check_interval=3)
     assert e.value.code == abi.E_ARG
     good.close()
+
+
+def test_batch_run_retires_diverged_lattice(gpu_lib):
+    cs = ensemble()[:3]
+    cs[1].rho = cs[1].rho.copy()
+    cs[1].rho[5] = np.nan
+    lats = make(cs)
+    with Batch(lats, check_interval=20, tol=1e-30) as b:
+        steps, rate, conv = b.run(200)
+    assert conv == 0
+    assert steps[1] == 20 and np.isinf(rate[1])
+    assert steps[0] == 200 and steps[2] == 200 and np.isfinite(rate[0]) and np.isfinite(rate[2])
+    for lat in lats:
+        lat.close()

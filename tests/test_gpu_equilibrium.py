@@ -109,3 +109,19 @@ def test_fp32dev_conserves_mass(gpu_lib):
     drift_per_node_step = abs(m1 - m0) / (c.n * 8000)
     print("mass", m0, m1, drift_per_node_step)
     assert drift_per_node_step < 1e-12
+
+
+@pytest.mark.parametrize("precision", [abi.FP64, abi.FP32_DEV])
+def test_run_to_equilibrium_reports_divergence(gpu_lib, precision):
+    """A non-finite density (here: planted in the initial state on the host)
+    stops the run with MPLB_E_NONFINITE instead of passing for converged
+    (NaN drops out of a max)."""
+    c = bubble(L=32, R=7.0)
+    c.rho = c.rho.copy()
+    c.rho[100] = np.nan
+    with Lattice(c, path=abi.PATH_FUSED, precision=precision) as lat:
+        lat.upload_case()
+        lat.initialize()
+        with pytest.raises(MplbError) as e:
+            lat.run_to_equilibrium(1000, 10, 1e-9)
+        assert e.value.code == abi.E_NONFINITE
