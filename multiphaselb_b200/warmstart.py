@@ -371,7 +371,8 @@ def main(argv=None):
         t2 = time.perf_counter()
         pred = net.predict(t, CS_A, CS_B, r, R)
         rep = dict(samples=int(r.size), cases=meta, loss=hist, data_s=t1 - t0, train_s=t2 - t1,
-                   fit_max_abs=float(np.abs(pred - rho).max()), fit_rms=float(np.sqrt(np.mean((pred - rho) ** 2))))
+                   fit_max_abs=float(np.abs(pred - rho).max()), fit_rms=float(np.sqrt(np.mean((pred - rho) ** 2))),
+                   fit_max_rel=float(np.abs(pred / rho - 1.0).max()))
         net.save(a.weights or DEFAULT_WEIGHTS[lat])
         txt = json.dumps(rep, indent=1)
     else:
