@@ -319,8 +319,13 @@ namespace mplb {
 constexpr int N_BATCH_CFG = 4;
 constexpr TileCfg BATCH_CFG[N_BATCH_CFG] = {{32, 8, false}, {32, 4, false}, {16, 8, false}, {64, 4, false}};
 
+// The batch fills every SM with a persistent grid, so resident warps hide
+// its memory latency: registers are capped for 24 warps per SM (3 blocks of
+// 256 threads, 6 of 128) instead of the lone kernel's 16.
+constexpr int batch_min_blocks(int threads) { return threads <= 128 ? 6 : 3; }
+
 template <int TX, int TY>
-__global__ void __launch_bounds__(TX * TY, min_blocks(TX * TY))
+__global__ void __launch_bounds__(TX * TY, batch_min_blocks(TX * TY))
     k_batch32_d2q9(const Params* __restrict__ Ps, const FusedArgs32* __restrict__ As, const int2* __restrict__ tiles,
                    const int* __restrict__ ntiles, int parity) {
     __shared__ Smem32<TX, TY, false> sm;
