@@ -169,4 +169,5 @@ class Descriptors:
             bcv = np.zeros(3, dtype=np.float64)
         self._keep += [bct, bcv]
         return FieldDesc(fd["model"], int(fd.get("update", 1)), (C.c_double * MAX_Q)(*lam),
-                         fd.get("sigma", 0.0), 0, 0.0, iptr(bct), dptr(bcv))
+                         fd.get("sigma", 0.0), int(fd.get("surface_tension", 0)), fd.get("kappa_st", 0.0),
+                         iptr(bct), dptr(bcv))

@@ -200,6 +200,46 @@ static void eq_heat(const orc* o, double T, const double* U, double* g) {
 }
 
 /* ---------------------------------------------------------------- operators */
+/* Surface-tension moments of one node: liMRTSurfaceTension.c:7-150 (D2Q9)
+ * and xuMRTSurfaceTension.c:7-168 (D3Q15).  Q_ij = sum_k w_k (psi(x + c_k) -
+ * psi(x)) c_ki c_kj with w the pseudopotential weights (lattice.weights is
+ * ppWeights, setLatticeInfo.c:80; the neighbour is nb[id][rev k]), scaled by
+ * 0.5 psi G kappa; C = 0 on a node with any missing neighbour.  D2Q9 fills
+ * the whole 2x2 tensor, D3Q15 its upper triangle. */
+static void surface_tension(const orc* o, uint32_t id, double* C) {
+    for (int k = 0; k < o->Q; k++) C[k] = 0;
+    int noneigh = 0;
+    for (int k = 1; k < o->Q; k++)
+        if (o->nb[(size_t)id * o->Q + k] == -1) noneigh++;
+    if (noneigh) return;
+    const int D = o->lat == MPLB_D2Q9 ? 2 : 3;
+    double Qt[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+    double ps = psi(o, o->rho[id], o->T[id]);
+    for (int k = 1; k < o->Q; k++) {
+        int nid = o->nb[(size_t)id * o->Q + o->rev[k]];
+        double alpha = o->ppw[k] * (psi(o, o->rho[nid], o->T[nid]) - ps);
+        for (int i = 0; i < D; i++)
+            for (int j = (D == 2 ? 0 : i); j < D; j++) Qt[i][j] += alpha * o->c[k][i] * o->c[k][j];
+    }
+    const double kap = o->fd[0].kappa_st;
+    for (int i = 0; i < D; i++)
+        for (int j = (D == 2 ? 0 : i); j < D; j++) Qt[i][j] = Qt[i][j] * 0.5 * ps * o->eos.G * kap;
+    const double* L = o->fd[0].Lambda;
+    if (D == 2) {
+        C[1] = 1.5 * L[1] * (Qt[0][0] + Qt[1][1]);
+        C[2] = -1.5 * L[2] * (Qt[0][0] + Qt[1][1]);
+        C[7] = -L[8] * (Qt[0][0] - Qt[1][1]);
+        C[8] = -L[8] * Qt[0][1];
+    } else {
+        C[1] = 4.0 * L[1] * (Qt[0][0] + Qt[1][1] + Qt[2][2]) / 5.0;
+        C[9] = -L[10] * (2 * Qt[0][0] - Qt[1][1] - Qt[2][2]);
+        C[10] = -L[10] * (Qt[1][1] - Qt[2][2]);
+        C[11] = -L[10] * Qt[0][1];
+        C[12] = -L[10] * Qt[1][2];
+        C[13] = -L[10] * Qt[0][2];
+    }
+}
+
 /* liMRTCollision.c:43-109 with liMRTForce.c:10-44 */
 static void collide_limrt(orc* o) {
     const double* L = o->fd[0].Lambda;
@@ -233,7 +273,12 @@ static void collide_limrt(orc* o) {
         S[6] = -F[1];
         S[7] = 2 * (U[0] * F[0] - U[1] * F[1]);
         S[8] = U[0] * F[1] + U[1] * F[0];
-        for (int k = 0; k < 9; k++) m[k] = m[k] - L[k] * (m[k] - meq[k]) + (1 - 0.5 * L[k]) * S[k];
+        double Cst[9];
+        if (o->fd[0].surface_tension) surface_tension(o, id, Cst);
+        for (int k = 0; k < 9; k++) {
+            m[k] = m[k] - L[k] * (m[k] - meq[k]) + (1 - 0.5 * L[k]) * S[k];
+            if (o->fd[0].surface_tension) m[k] = m[k] + Cst[k];
+        }
         matvec(o, o->Mi, m, f);
     }
 }
@@ -285,7 +330,12 @@ static void collide_xumrt(orc* o) {
         S[12] = U[1] * F[2] + U[2] * F[1];
         S[13] = U[0] * F[2] + U[2] * F[0];
         S[14] = 0;
-        for (int k = 0; k < 15; k++) m[k] = m[k] - L[k] * (m[k] - meq[k]) + (1 - 0.5 * L[k]) * S[k];
+        double Cst[15];
+        if (o->fd[0].surface_tension) surface_tension(o, id, Cst);
+        for (int k = 0; k < 15; k++) {
+            m[k] = m[k] - L[k] * (m[k] - meq[k]) + (1 - 0.5 * L[k]) * S[k];
+            if (o->fd[0].surface_tension) m[k] = m[k] + Cst[k];
+        }
         matvec(o, o->Mi, m, f);
     }
 }

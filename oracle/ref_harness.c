@@ -66,12 +66,14 @@ static void setup_field(ref_case* c, lbeField* fl, const mplb_field_desc* d) {
     case MPLB_LIMRT:
         fl->lbparam.liMRT.Lambda = lam;
         fl->lbparam.liMRT.sigma = d->sigma;
-        fl->lbparam.liMRT.surfaceTension = no_st;
+        fl->lbparam.liMRT.surfaceTension = d->surface_tension ? liSurfTen : no_st;
+        fl->lbparam.liMRT.kappa_st = d->kappa_st;
         break;
     case MPLB_XUMRT:
         fl->lbparam.xuMRT.Lambda = lam;
         fl->lbparam.xuMRT.sigma = d->sigma;
-        fl->lbparam.xuMRT.surfaceTension = noXuSurf;
+        fl->lbparam.xuMRT.surfaceTension = d->surface_tension ? xuSurfTen : noXuSurf;
+        fl->lbparam.xuMRT.kappa_st = d->kappa_st;
         break;
     case MPLB_LITEMPMRT:
         fl->lbparam.liTempMRT.Lambda = lam;

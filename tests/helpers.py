@@ -16,7 +16,30 @@ def small_cases():
                                                       name="lid_d2q9_12x16"), du=1e-3),
         "bubble_d3q15": cases.perturbed(cases.bubble_case(abi.D3Q15, 10, 3.0, 2.0, 0.75, dims=(10, 8, 6)), du=1e-3),
         "walls_d3q15": walled_d3q15(),
+        "st_d2q9": surface_tension_d2q9(),
+        "st_d3q15": surface_tension_d3q15(),
     }
+
+
+def surface_tension_d2q9():
+    """D2Q9 bubble with the surface-tension term (liMRTSurfaceTension), periodic
+    x and bounce-back walls in y (wall nodes take C = 0)."""
+    c = cases.bubble_case(abi.D2Q9, 20, 5.0, 3.0, 0.8, dims=(20, 18))
+    nb, points, patches, names = cases.box_mesh(abi.D2Q9, c.dims, (True, False))
+    c.nb, c.points, c.patches, c.patch_names = nb, points, patches, names
+    c.periodic = (True, False)
+    c.f = dict(c.f, surface_tension=1, kappa_st=0.4, bc_type=[abi.BC_BOUNCEBACK] * len(patches),
+               bc_value=np.zeros((len(patches), 3)))
+    c.name = "st_d2q9_20x18"
+    return cases.perturbed(c, du=1e-3)
+
+
+def surface_tension_d3q15():
+    """The walled D3Q15 box with the surface-tension term (xuMRTSurfaceTension)."""
+    c = walled_d3q15()
+    c.f = dict(c.f, surface_tension=1, kappa_st=0.4)
+    c.name = "st_d3q15_8x6x7"
+    return c
 
 
 def walled_d3q15():
