@@ -122,7 +122,7 @@ typedef struct mplb_field_desc {
     int32_t update;           /* 0 = frozen (reference --frozen / --nht) */
     double Lambda[MPLB_MAX_Q];
     double sigma;             /* liMRT / xuMRT force coefficient */
-    int32_t surface_tension;  /* must be 0: surface-tension terms are outside this path */
+    int32_t surface_tension;  /* 1 = liMRT / xuMRT surface-tension term (liMRTSurfaceTension.c, xuMRTSurfaceTension.c); FP64 only */
     double kappa_st;
     const int32_t* bc_type;   /* [n_patches] MPLB_BC_* for this field */
     const double* bc_value;   /* [n_patches][3]: fixedT uses [0], fixedU uses [0..2] */

@@ -302,8 +302,20 @@ __device__ __forceinline__ void finish_node(const Params& P, const FusedArgs& A,
         return;
     }
     if constexpr (F_ON) {
-        if constexpr (L::Q == 9) collide_limrt_psi(P, f, rho, U, Ft, Fi, psi);
-        else collide_xumrt_psi(P, f, rho, U, Fi, psi);
+        // surface-tension term (zero on wall nodes, which miss a neighbour)
+        double C[L::Q];
+        const double* Cp = nullptr;
+        if (P.st_on) {
+            if (!onb) {
+                surface_tension<L>(P, psi, nbpsi, C);
+            } else {
+#pragma unroll
+                for (int k = 0; k < L::Q; k++) C[k] = 0;
+            }
+            Cp = C;
+        }
+        if constexpr (L::Q == 9) collide_limrt_psi(P, f, rho, U, Ft, Fi, psi, Cp);
+        else collide_xumrt_psi(P, f, rho, U, Fi, psi, Cp);
 #pragma unroll
         for (int k = 0; k < L::Q; k++) A.fout[(size_t)k * n + id] = f[k];
         if constexpr (G_ON) {

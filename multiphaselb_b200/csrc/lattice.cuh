@@ -96,6 +96,9 @@ struct Params {
     // exact shortcuts, decided on the host: x/G == -x when G == -1,
     // x/Cv == x when Cv == 1, x/(M*M) == x when M*M == 1
     int32_t g_neg1, cv_one, m2_one;
+    // surface-tension term of the flow field (liMRT/xuMRT surfaceTension, kappa_st)
+    int32_t st_on;
+    double kappa_st;
 };
 
 // ----------------------------------------------------------- exact division
@@ -294,8 +297,60 @@ MPLB_HD void eq_heat(const Params& P, double T, double u0, double u1, double* g)
 
 // ---------------------------------------------------------- node collisions
 // liMRTCollision.c:48-106 with liMRTForce.c:18-42.  f in/out (9 values).
+// Surface-tension moments C of an interior node: liMRTSurfaceTension.c:7-150
+// (D2Q9, full 2x2 tensor) and xuMRTSurfaceTension.c:7-168 (D3Q15, upper
+// triangle).  Q_ij = sum_k ppw_k (psi(x + c_k) - psi(x)) c_ki c_kj -- the
+// reference's lattice.weights are the pseudopotential weights
+// (setLatticeInfo.c:80) -- then Q *= 0.5 psi G kappa left to right.  With
+// c in {-1, 0, 1} the products are exact: zero terms are skipped, the others
+// add or subtract alpha.  nbpsi(k) = psi at x + c_k.
+template <class L, class PsiAt>
+MPLB_HD void surface_tension(const Params& P, double ps, PsiAt nbpsi, double* C) {
+    double Q00 = 0, Q01 = 0, Q02 = 0, Q11 = 0, Q12 = 0, Q22 = 0;
+    static_for<L::Q - 1>([&](auto km1) {
+        constexpr int k = decltype(km1)::value + 1;
+        const double al = P.ppw[k] * (nbpsi(k) - ps);
+        auto acc = [&](double& q, int c) {
+            if (c == 1) q += al;
+            else if (c == -1) q -= al;
+        };
+        acc(Q00, cxk<L>(k) * cxk<L>(k));
+        acc(Q01, cxk<L>(k) * cyk<L>(k));
+        acc(Q11, cyk<L>(k) * cyk<L>(k));
+        if constexpr (L::D == 3) {
+            acc(Q02, cxk<L>(k) * czk<L>(k));
+            acc(Q12, cyk<L>(k) * czk<L>(k));
+            acc(Q22, czk<L>(k) * czk<L>(k));
+        }
+    });
+    const double kap = P.kappa_st;
+    Q00 = Q00 * 0.5 * ps * P.G * kap;
+    Q01 = Q01 * 0.5 * ps * P.G * kap;
+    Q11 = Q11 * 0.5 * ps * P.G * kap;
+#pragma unroll
+    for (int k = 0; k < L::Q; k++) C[k] = 0;
+    if constexpr (L::D == 2) {
+        C[1] = 1.5 * P.Lf[1] * (Q00 + Q11);
+        C[2] = -1.5 * P.Lf[2] * (Q00 + Q11);
+        C[7] = -P.Lf[8] * (Q00 - Q11);
+        C[8] = -P.Lf[8] * Q01;
+    } else {
+        Q02 = Q02 * 0.5 * ps * P.G * kap;
+        Q12 = Q12 * 0.5 * ps * P.G * kap;
+        Q22 = Q22 * 0.5 * ps * P.G * kap;
+        C[1] = 4.0 * P.Lf[1] * (Q00 + Q11 + Q22) / 5.0;
+        C[9] = -P.Lf[10] * (2 * Q00 - Q11 - Q22);
+        C[10] = -P.Lf[10] * (Q11 - Q22);
+        C[11] = -P.Lf[10] * Q01;
+        C[12] = -P.Lf[10] * Q12;
+        C[13] = -P.Lf[10] * Q02;
+    }
+}
+
+// C (may be NULL) is the surface-tension term, added to every moment after
+// the relaxation (liMRTCollision.c:90-98).
 MPLB_HD void collide_limrt_psi(const Params& P, double* f, double rho, const double* U,
-                               const double* F, const double* Fi, double ps) {
+                               const double* F, const double* Fi, double ps, const double* C = nullptr) {
     double um = 0;
 #pragma unroll
     for (int k = 0; k < 3; k++) um += U[k] * U[k];
@@ -323,6 +378,10 @@ MPLB_HD void collide_limrt_psi(const Params& P, double* f, double rho, const dou
     S[8] = U[0] * F[1] + U[1] * F[0];
 #pragma unroll
     for (int k = 0; k < 9; k++) m[k] = m[k] - P.Lf[k] * (m[k] - meq[k]) + P.relax_f[k] * S[k];
+    if (C) {
+#pragma unroll
+        for (int k = 0; k < 9; k++) m[k] = m[k] + C[k];
+    }
     mul_Mi<D2Q9T>(P, m, f);
 }
 MPLB_HD void collide_limrt(const Params& P, double* f, double rho, const double* U, const double* F,
@@ -333,7 +392,7 @@ MPLB_HD void collide_limrt(const Params& P, double* f, double rho, const double*
 // xuMRTCollision.c:46-89, xuMRTEquilibriumMS.c:12-51, xuMRTForce.c:14-69.
 // F here is Fi + (rho - rho_0) g (no fext), xuMRTForce.c:18-22.
 MPLB_HD void collide_xumrt_psi(const Params& P, double* f, double rho, const double* U,
-                               const double* Fi, double ps) {
+                               const double* Fi, double ps, const double* C = nullptr) {
     double um = 0;
 #pragma unroll
     for (int k = 0; k < 3; k++) um += U[k] * U[k];
@@ -377,6 +436,10 @@ MPLB_HD void collide_xumrt_psi(const Params& P, double* f, double rho, const dou
     S[14] = 0;
 #pragma unroll
     for (int k = 0; k < 15; k++) m[k] = m[k] - P.Lf[k] * (m[k] - meq[k]) + P.relax_f[k] * S[k];
+    if (C) {
+#pragma unroll
+        for (int k = 0; k < 15; k++) m[k] = m[k] + C[k];
+    }
     mul_Mi<D3Q15T>(P, m, f);
 }
 MPLB_HD void collide_xumrt(const Params& P, double* f, double rho, const double* U, const double* Fi, double T) {

@@ -254,7 +254,10 @@ int check_field(const mplb_field_desc* d, int lat, int which, uint32_t npatch, s
     // A frozen field is never touched by the reference (every operator checks
     // field->update first), so any model and boundary set is accepted for it.
     if (!d->update) return 0;
-    if (d->surface_tension != 0) { why = "surface tension terms are not part of this path"; return MPLB_E_UNSUPPORTED; }
+    if (d->surface_tension != 0 && (which != 0 || (d->model != MPLB_LIMRT && d->model != MPLB_XUMRT))) {
+        why = "surface tension is a liMRT / xuMRT flow-field option";
+        return MPLB_E_UNSUPPORTED;
+    }
     if (which == 0) {
         if (d->model == MPLB_LIMRT && lat != MPLB_D2Q9) { why = "liMRT is D2Q9 only (liMRTForce.c:13)"; return MPLB_E_UNSUPPORTED; }
         if (d->model == MPLB_XUMRT && lat != MPLB_D3Q15) { why = "xuMRT is D3Q15 only (xuMRTForce.c:9)"; return MPLB_E_UNSUPPORTED; }
@@ -404,7 +407,7 @@ int op_equilibrium(mplb_gpu* h, int fi) {
 template <class L>
 int op_collision(mplb_gpu* h, int fi) {
     if (h->model[fi] == MPLB_NO_MODEL || !(fi == 0 ? h->P.f_update : h->P.g_update)) return 0;
-    if (fi == 0) LAUNCH(k_collide_flow<L>, blocks(h->n), h->P, h->F(), h->rho, h->U, h->T, h->Fi, h->Ft);
+    if (fi == 0) LAUNCH(k_collide_flow<L>, blocks(h->n), h->P, h->F(), h->rho, h->U, h->T, h->Fi, h->Ft, h->nb);
     else LAUNCH(k_collide_heat, blocks(h->n), h->P, h->G(), h->T, h->U, h->S);
     return 0;
 }
@@ -779,6 +782,8 @@ int mplb_gpu_create(const mplb_mesh_desc* mesh, const mplb_eos_desc* eos, const 
         P.sig12 = 12 * f->sigma;
         P.sig6 = 6.0 * f->sigma;
         P.sigma_p = f->sigma;
+        P.st_on = (f->update && f->surface_tension) ? 1 : 0;
+        P.kappa_st = f->kappa_st;
     }
     if (g && g->model != MPLB_NO_MODEL) {
         for (int k = 0; k < MPLB_MAX_Q; k++) P.Lg[k] = g->Lambda[k];
@@ -871,6 +876,8 @@ int mplb_gpu_create(const mplb_mesh_desc* mesh, const mplb_eos_desc* eos, const 
     if ((want_path == MPLB_PATH_FUSED || h->precision == MPLB_FP32_DEV) && !fusable)
         return bail(fail(MPLB_E_UNSUPPORTED, std::string(h->precision == MPLB_FP32_DEV ? "FP32-deviation storage needs the fused box path; " : "") +
                                                  "fused path unavailable: " + (h->box ? fwhy : std::string("mesh is not a box"))));
+    if (h->precision == MPLB_FP32_DEV && h->P.st_on)
+        return bail(fail(MPLB_E_UNSUPPORTED, "FP32-deviation storage has no surface-tension term"));
     if (h->precision == MPLB_FP32_DEV && want_path == MPLB_PATH_OPERATORS)
         return bail(fail(MPLB_E_UNSUPPORTED, "FP32-deviation storage runs on the fused path only"));
     h->path = (want_path == MPLB_PATH_OPERATORS || !fusable) ? MPLB_PATH_OPERATORS : MPLB_PATH_FUSED;

@@ -46,7 +46,8 @@ static __global__ void k_equilibrium_heat(Params P, double* __restrict__ g, cons
 template <class L>
 __global__ void k_collide_flow(Params P, double* __restrict__ f, const double* __restrict__ rho,
                                const double* __restrict__ U, const double* __restrict__ T,
-                               const double* __restrict__ Fi, const double* __restrict__ Ft) {
+                               const double* __restrict__ Fi, const double* __restrict__ Ft,
+                               const int32_t* __restrict__ nb) {
     uint32_t n = P.n, id = blockIdx.x * blockDim.x + threadIdx.x;
     if (id >= n) return;
     double v[L::Q];
@@ -54,11 +55,32 @@ __global__ void k_collide_flow(Params P, double* __restrict__ f, const double* _
     for (int k = 0; k < L::Q; k++) v[k] = f[(size_t)k * n + id];
     double u[3] = {U[id], U[n + id], U[2 * n + id]};
     double fi[3] = {Fi[id], Fi[n + id], Fi[2 * n + id]};
+    const double ps = potential(P, rho[id], T[id]);
+    // surface-tension term: zero on a node with any missing neighbour
+    // (liMRTSurfaceTension.c:33-45), else from psi at x + c_k = nb[rev k]
+    double C[L::Q];
+    const double* Cp = nullptr;
+    if (P.st_on) {
+        bool interior = true;
+#pragma unroll
+        for (int k = 1; k < L::Q; k++) interior &= nb[(size_t)k * n + id] != -1;
+        if (interior) {
+            auto nbpsi = [&](int k) {
+                const uint32_t m = (uint32_t)nb[(size_t)revk<L>(k) * n + id];
+                return potential(P, rho[m], T[m]);
+            };
+            surface_tension<L>(P, ps, nbpsi, C);
+        } else {
+#pragma unroll
+            for (int k = 0; k < L::Q; k++) C[k] = 0;
+        }
+        Cp = C;
+    }
     if constexpr (L::Q == 9) {
         double ft[3] = {Ft[id], Ft[n + id], Ft[2 * n + id]};
-        collide_limrt(P, v, rho[id], u, ft, fi, T[id]);
+        collide_limrt_psi(P, v, rho[id], u, ft, fi, ps, Cp);
     } else {
-        collide_xumrt(P, v, rho[id], u, fi, T[id]);
+        collide_xumrt_psi(P, v, rho[id], u, fi, ps, Cp);
     }
 #pragma unroll
     for (int k = 0; k < L::Q; k++) f[(size_t)k * n + id] = v[k];

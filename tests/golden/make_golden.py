@@ -1,6 +1,6 @@
 """Generate the golden vectors in this directory from the REFERENCE build.
 
-    python -m tests.golden.make_golden
+    python -m tests.golden.make_golden [case names]
 
 Each .npz holds a self-contained small case (neighbour table, patches, EOS,
 field constants, initial rho/U/T) and the reference's state after `steps`
@@ -23,7 +23,8 @@ if ROOT not in sys.path:
 from multiphaselb_b200 import cases  # noqa: E402
 from tests.helpers import FIELDS, run_checker, small_cases  # noqa: E402
 
-STEPS = {"bubble_d2q9": 12, "column_d2q9": 12, "lid_d2q9": 9, "bubble_d3q15": 5, "walls_d3q15": 5}
+STEPS = {"bubble_d2q9": 12, "column_d2q9": 12, "lid_d2q9": 9, "bubble_d3q15": 5, "walls_d3q15": 5,
+         "st_d2q9": 10, "st_d3q15": 5}
 
 
 def save_case(path, case, steps, out):
@@ -50,8 +51,11 @@ def load_case(path):
     return c, spec["steps"], want
 
 
-def main():
+def main(names=None):
+    """Write the fixtures of `names` (default: every small case)."""
     for name, case in small_cases().items():
+        if names and name not in names:
+            continue
         steps = STEPS[name]
         out = run_checker("ref", case, steps)
         path = os.path.join(HERE, f"{name}_{steps}steps.npz")
@@ -60,4 +64,4 @@ def main():
 
 
 if __name__ == "__main__":
-    main()
+    main(sys.argv[1:])

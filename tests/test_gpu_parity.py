@@ -146,7 +146,7 @@ def test_serial_boundary_order(gpu_lib):
     assert_same(got, run_checker("port", c2, 6), ctx="serial bc")
 
 
-FUSABLE = ["bubble_d2q9", "column_d2q9", "bubble_d3q15", "walls_d3q15"]
+FUSABLE = ["bubble_d2q9", "column_d2q9", "bubble_d3q15", "walls_d3q15", "st_d2q9", "st_d3q15"]
 
 
 @pytest.mark.parametrize("name", FUSABLE)
@@ -199,7 +199,7 @@ def test_fused_frozen_fields(gpu_lib, fu, gu):
     assert_same(got, run_checker("port", c2, 6), ctx=f"fused update f={fu} g={gu}")
 
 
-@pytest.mark.parametrize("name", ["column_d2q9", "bubble_d2q9", "bubble_d3q15", "walls_d3q15"])
+@pytest.mark.parametrize("name", ["column_d2q9", "bubble_d2q9", "bubble_d3q15", "walls_d3q15", "st_d2q9", "st_d3q15"])
 def test_every_tile_candidate_is_exact(gpu_lib, name):
     """Each fused tile shape (forced) gives the oracle's bits; the autotuner
     then times them all and picks one."""
@@ -241,3 +241,11 @@ def test_pressure_matches_oracle(gpu_lib, name, path):
         lat.step(5)
         got = lat.macro_pressure()
     assert np.array_equal(got, want), float(np.abs(got - want).max())
+
+
+def test_surface_tension_rejected_in_fp32(gpu_lib):
+    """The FP32-deviation collision has no surface-tension term: create says so."""
+    from multiphaselb_b200 import Lattice, MplbError
+    with pytest.raises(MplbError) as e:
+        Lattice(small_cases()["st_d2q9"], path=abi.PATH_FUSED, precision=abi.FP32_DEV)
+    assert e.value.code == abi.E_UNSUPPORTED
