@@ -198,6 +198,20 @@ int mplb_gpu_heat_source(mplb_gpu_t* h);                                /* gener
 int mplb_gpu_macro_pressure(mplb_gpu_t* h);
 int mplb_gpu_download_pressure(mplb_gpu_t* h, double* p);
 
+/* Write step without stalling the time loop (the driver's write block,
+ * multiPhasePP.c:249-310, downloads synchronously).  mplb_gpu_snapshot
+ * queues on the handle's stream: the reference state of the current step
+ * (and, with with_pressure, macroPressure), a device copy of rho, T, p and U,
+ * then starts its transfer to pinned host memory on a side stream and
+ * returns; the caller can go on stepping while it crosses PCIe.
+ * mplb_gpu_snapshot_wait waits for the last snapshot and copies it out in the
+ * reference's layouts (rho, T, p [node], U [node][3]; any pointer may be NULL;
+ * p needs with_pressure).  A second snapshot before the wait replaces the
+ * first.  The handle holds 6 n doubles on the device and 6 n pinned on the
+ * host from the first call until destroy. */
+int mplb_gpu_snapshot(mplb_gpu_t* h, int32_t with_pressure);
+int mplb_gpu_snapshot_wait(mplb_gpu_t* h, double* rho, double* U, double* T, double* p);
+
 /* Time and buoyancy reference density (timeInfo.current, EOSInfo.rho_0). */
 int mplb_gpu_set_time(mplb_gpu_t* h, uint32_t current);
 int mplb_gpu_set_rho0(mplb_gpu_t* h, double rho_0);

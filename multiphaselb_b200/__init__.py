@@ -69,6 +69,8 @@ def load_library(path=LIB_PATH):
         "mplb_gpu_average_rho0": ([H, D], C.c_int),
         "mplb_gpu_mass_energy": ([H, D, D], C.c_int),
         "mplb_gpu_sync": ([H], C.c_int),
+        "mplb_gpu_snapshot": ([H, C.c_int32], C.c_int),
+        "mplb_gpu_snapshot_wait": ([H, D, D, D, D], C.c_int),
         "mplb_gpu_monitor": ([H, C.c_int32, D, D], C.c_int),
         "mplb_gpu_run_to_equilibrium": ([H, C.c_uint32, C.c_uint32, C.c_double, C.POINTER(C.c_uint32), D],
                                         C.c_int),
@@ -228,6 +230,21 @@ class Lattice:
         self._check(self.lib.mplb_gpu_run_to_equilibrium(self.h, max_steps, check_interval, tol, C.byref(st),
                                                          C.byref(r)))
         return st.value, r.value
+
+    def snapshot(self, pressure=False):
+        """Queue a write-step copy of rho, U, T (and p) and its transfer to the
+        host; stepping may continue before snapshot_wait."""
+        self._check(self.lib.mplb_gpu_snapshot(self.h, 1 if pressure else 0))
+        self._snap_p = pressure
+
+    def snapshot_wait(self):
+        n = self.n
+        out = dict(rho=np.zeros(n), U=np.zeros((n, 3)), T=np.zeros(n))
+        if getattr(self, "_snap_p", False):
+            out["p"] = np.zeros(n)
+        self._check(self.lib.mplb_gpu_snapshot_wait(self.h, abi.dptr(out["rho"]), abi.dptr(out["U"]),
+                                                    abi.dptr(out["T"]), abi.dptr(out.get("p"))))
+        return out
 
     def mass_energy(self):
         m, e = C.c_double(), C.c_double()

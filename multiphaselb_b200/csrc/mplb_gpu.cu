@@ -113,6 +113,13 @@ struct mplb_gpu {
     double rho_ref = 0, T_ref = 0;
     double* snap = nullptr;  // equilibrium monitor: density at the last check
     long long* mom = nullptr;  // FP32 equilibrium runs: total momentum now [0..2] and at the start [3..5]
+    // write-step snapshot: device copy [rho | T | p | U as [node][3]], its
+    // pinned host image, the side stream that transfers it, and events
+    double* snap_dev = nullptr;
+    double* snap_host = nullptr;
+    cudaStream_t snap_stream = nullptr;
+    cudaEvent_t snap_ready = nullptr, snap_done = nullptr;
+    bool snap_pending = false, snap_has_p = false;
     int tile_request = 0;  // mplb_opts.tile_config
     uint32_t current = 0;
     uint64_t launches = 0;
@@ -904,6 +911,14 @@ int mplb_gpu_destroy(mplb_gpu_t* h) {
     if (!h) return 0;
     DeviceGuard guard(h->dev);
     cudaStreamSynchronize(h->stream);
+    if (h->snap_stream) {
+        cudaStreamSynchronize(h->snap_stream);
+        cudaStreamDestroy(h->snap_stream);
+    }
+    if (h->snap_ready) cudaEventDestroy(h->snap_ready);
+    if (h->snap_done) cudaEventDestroy(h->snap_done);
+    if (h->snap_dev) cudaFree(h->snap_dev);
+    if (h->snap_host) cudaFreeHost(h->snap_host);
     fused_free(h->fc);
     free_all(h);
     if (h->own_stream) cudaStreamDestroy(h->stream);
@@ -1059,6 +1074,52 @@ int mplb_gpu_macro_pressure(mplb_gpu_t* h) {
     DeviceGuard guard(h->dev);
     RET(materialize(h));
     return DISPATCH(h, op_pressure, h);
+}
+
+int mplb_gpu_snapshot(mplb_gpu_t* h, int32_t with_pressure) {
+    if (!h) return fail(MPLB_E_ARG, "NULL handle");
+    if (with_pressure && h->P.f_update && h->model[0] != MPLB_LIMRT && h->model[0] != MPLB_XUMRT)
+        return fail(MPLB_E_UNSUPPORTED, "Pressure update not available (macroPressure.c:60-64)");
+    DeviceGuard guard(h->dev);
+    const size_t n = h->n;
+    if (!h->snap_dev) {
+        CK(cudaMalloc((void**)&h->snap_dev, 6 * n * sizeof(double)));
+        h->bytes += 6 * n * sizeof(double);
+        CK(cudaMallocHost((void**)&h->snap_host, 6 * n * sizeof(double)));
+        CK(cudaStreamCreateWithFlags(&h->snap_stream, cudaStreamNonBlocking));
+        CK(cudaEventCreateWithFlags(&h->snap_ready, cudaEventDisableTiming));
+        CK(cudaEventCreateWithFlags(&h->snap_done, cudaEventDisableTiming));
+    }
+    // the device copy must not be rewritten while the previous one is in flight
+    if (h->snap_pending) CK(cudaStreamWaitEvent(h->stream, h->snap_done, 0));
+    RET(materialize(h));
+    if (with_pressure) RET(DISPATCH(h, op_pressure, h));
+    CK(cudaMemcpyAsync(h->snap_dev, h->rho, n * sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
+    CK(cudaMemcpyAsync(h->snap_dev + n, h->T, n * sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
+    if (with_pressure)
+        CK(cudaMemcpyAsync(h->snap_dev + 2 * n, h->p, n * sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
+    LAUNCH(k_soa_to_aos, blocks(3 * n), h->n, 3, h->U, h->snap_dev + 3 * n);
+    CK(cudaEventRecord(h->snap_ready, h->stream));
+    CK(cudaStreamWaitEvent(h->snap_stream, h->snap_ready, 0));
+    CK(cudaMemcpyAsync(h->snap_host, h->snap_dev, 6 * n * sizeof(double), cudaMemcpyDeviceToHost, h->snap_stream));
+    CK(cudaEventRecord(h->snap_done, h->snap_stream));
+    h->snap_pending = true;
+    h->snap_has_p = with_pressure != 0;
+    return 0;
+}
+
+int mplb_gpu_snapshot_wait(mplb_gpu_t* h, double* rho, double* U, double* T, double* p) {
+    if (!h) return fail(MPLB_E_ARG, "NULL handle");
+    if (!h->snap_pending) return fail(MPLB_E_STATE, "no snapshot was taken");
+    if (p && !h->snap_has_p) return fail(MPLB_E_STATE, "the snapshot was taken without the pressure");
+    DeviceGuard guard(h->dev);
+    CK(cudaEventSynchronize(h->snap_done));
+    const size_t n = h->n;
+    if (rho) std::memcpy(rho, h->snap_host, n * sizeof(double));
+    if (T) std::memcpy(T, h->snap_host + n, n * sizeof(double));
+    if (p) std::memcpy(p, h->snap_host + 2 * n, n * sizeof(double));
+    if (U) std::memcpy(U, h->snap_host + 3 * n, 3 * n * sizeof(double));
+    return 0;
 }
 
 int mplb_gpu_download_pressure(mplb_gpu_t* h, double* p) {
