@@ -83,7 +83,8 @@ enum {
     MPLB_E_UNSUPPORTED = -2, /* model / boundary / option outside the path */
     MPLB_E_CUDA = -3,        /* CUDA runtime error */
     MPLB_E_STATE = -4,       /* call not valid in the handle's current state */
-    MPLB_E_NONFINITE = -5    /* NaN/Inf found by a check */
+    MPLB_E_NONFINITE = -5,   /* NaN/Inf found by a check */
+    MPLB_E_IO = -6           /* a field file or its folder could not be made or written */
 };
 
 /*
@@ -201,16 +202,35 @@ int mplb_gpu_download_pressure(mplb_gpu_t* h, double* p);
 /* Write step without stalling the time loop (the driver's write block,
  * multiPhasePP.c:249-310, downloads synchronously).  mplb_gpu_snapshot
  * queues on the handle's stream: the reference state of the current step
- * (and, with with_pressure, macroPressure), a device copy of rho, T, p and U,
+ * (and, with MPLB_SNAP_PRESSURE, macroPressure), a device copy of rho, T, p
+ * and U (and, with MPLB_SNAP_PDFS, f and g),
  * then starts its transfer to pinned host memory on a side stream and
  * returns; the caller can go on stepping while it crosses PCIe.
  * mplb_gpu_snapshot_wait waits for the last snapshot and copies it out in the
  * reference's layouts (rho, T, p [node], U [node][3]; any pointer may be NULL;
- * p needs with_pressure).  A second snapshot before the wait replaces the
- * first.  The handle holds 6 n doubles on the device and 6 n pinned on the
- * host from the first call until destroy. */
-int mplb_gpu_snapshot(mplb_gpu_t* h, int32_t with_pressure);
+ * p needs MPLB_SNAP_PRESSURE).  A second snapshot before the wait replaces
+ * the first.  The handle holds 6 n doubles (6 n + 2 Q n with MPLB_SNAP_PDFS)
+ * on the device and as many pinned on the host from the first call until
+ * destroy. */
+enum {
+    MPLB_SNAP_PRESSURE = 1,  /* also run macroPressure and keep p */
+    MPLB_SNAP_PDFS = 2       /* also keep f and g ([node][Q] each) for the writer */
+};
+int mplb_gpu_snapshot(mplb_gpu_t* h, int32_t flags);
 int mplb_gpu_snapshot_wait(mplb_gpu_t* h, double* rho, double* U, double* T, double* p);
+/* Write the last snapshot as the driver's write block does
+ * (multiPhasePP.c:289-301): rho, T, p (if taken), U (3 components), f and g
+ * (if taken with MPLB_SNAP_PDFS), in that order, with mplb_write_*_field's
+ * formats and folders, at the time the snapshot was taken.  The files are
+ * written by a host thread that first waits for the snapshot's transfer, so
+ * the call returns at once and stepping goes on.  mplb_gpu_snapshot_join
+ * waits for that thread and returns the first error of the writes started
+ * since the last join (MPLB_E_NONFINITE for a NaN field: the fields before it
+ * are written, as in the reference).  A new snapshot, or destroy, waits for a
+ * running writer first.  For pvtu the driver writes the mesh part
+ * (writeMeshToVTK) before this call and writePvtuExtra after the join. */
+int mplb_gpu_snapshot_write(mplb_gpu_t* h, const char* root, int32_t pid, int32_t format);
+int mplb_gpu_snapshot_join(mplb_gpu_t* h);
 
 /* Time and buoyancy reference density (timeInfo.current, EOSInfo.rho_0). */
 int mplb_gpu_set_time(mplb_gpu_t* h, uint32_t current);
@@ -373,6 +393,33 @@ int mplb_mlp_init_bubble(mplb_mlp_t* m, mplb_gpu_t* h, double t_ratio, const dou
  * effective radius.  Allocates one scratch array of n doubles. */
 int mplb_mlp_init_bubble_mass(mplb_mlp_t* m, mplb_gpu_t* h, double t_ratio, const double* center, double radius,
                               double T, double target_mass, double* radius_used);
+
+/*
+ * Field files in the reference's per-rank formats, the data format chosen as
+ * timeInfo.data does (include/dataTypes.h:53).  Replace writeScalarField
+ * (src/IO/writeScalarField.c:10-59) and writeVectorField
+ * (src/IO/writeVectorField.c:9-70) for the asciiRaw, binaryRaw and pvtu
+ * formats with the same bytes: asciiRaw "%g" text, binaryRaw float values in
+ * node order, both in <root>/processor<pid>/<time>/<name> (folders made as
+ * needed); pvtu appends a DataArray block to
+ * <root>/processor<pid>/<time>/fields.vtu.  root NULL or "" is the current
+ * folder, as in the reference.  field is [n] (scalar) or [n][vsize] doubles
+ * on the host.  A NaN anywhere returns MPLB_E_NONFINITE and writes nothing
+ * (the reference stops the run there).  EnSight returns MPLB_E_UNSUPPORTED.
+ * Host code only: no GPU is needed.  Text is formatted by several host
+ * threads (MPLB_IO_THREADS, default: the hardware threads up to 32); the
+ * bytes do not depend on their number.
+ */
+enum {
+    MPLB_FMT_ASCII_RAW = 0,
+    MPLB_FMT_BINARY_RAW = 1,
+    MPLB_FMT_PVTU = 2,
+    MPLB_FMT_ENSIGHT = 3
+};
+int mplb_write_scalar_field(const char* root, int32_t pid, uint32_t time, int32_t format, const char* name,
+                            const double* field, uint64_t n);
+int mplb_write_vector_field(const char* root, int32_t pid, uint32_t time, int32_t format, const char* name,
+                            const double* field, uint64_t n, uint32_t vsize);
 
 #ifdef __cplusplus
 }

@@ -71,6 +71,12 @@ def load_library(path=LIB_PATH):
         "mplb_gpu_sync": ([H], C.c_int),
         "mplb_gpu_snapshot": ([H, C.c_int32], C.c_int),
         "mplb_gpu_snapshot_wait": ([H, D, D, D, D], C.c_int),
+        "mplb_gpu_snapshot_write": ([H, C.c_char_p, C.c_int32, C.c_int32], C.c_int),
+        "mplb_gpu_snapshot_join": ([H], C.c_int),
+        "mplb_write_scalar_field": ([C.c_char_p, C.c_int32, C.c_uint32, C.c_int32, C.c_char_p, D, C.c_uint64],
+                                    C.c_int),
+        "mplb_write_vector_field": ([C.c_char_p, C.c_int32, C.c_uint32, C.c_int32, C.c_char_p, D, C.c_uint64,
+                                     C.c_uint32], C.c_int),
         "mplb_gpu_monitor": ([H, C.c_int32, D, D], C.c_int),
         "mplb_gpu_run_to_equilibrium": ([H, C.c_uint32, C.c_uint32, C.c_double, C.POINTER(C.c_uint32), D],
                                         C.c_int),
@@ -90,6 +96,30 @@ def load_library(path=LIB_PATH):
 
 def version():
     return load_library().mplb_gpu_version().decode()
+
+
+def _format(fmt):
+    return abi.FORMATS[fmt] if isinstance(fmt, str) else int(fmt)
+
+
+def write_field(name, field, time, root="", pid=0, fmt="asciiRaw", scalar=None):
+    """Write one field file in the reference's format (mplb_write_scalar_field
+    / mplb_write_vector_field; host code, no GPU needed).  ``field`` is [n]
+    (scalar) or [n][vsize]; ``scalar`` defaults to ``field.ndim == 1``."""
+    lib = load_library()
+    a = np.ascontiguousarray(field, dtype=np.float64)
+    if scalar is None:
+        scalar = a.ndim == 1
+    root = os.fsencode(root)
+    if scalar:
+        rc = lib.mplb_write_scalar_field(root, pid, time, _format(fmt), name.encode(), abi.dptr(a.reshape(-1)),
+                                         a.size)
+    else:
+        a2 = a.reshape(a.shape[0], -1) if a.ndim > 1 else a.reshape(-1, 1)
+        rc = lib.mplb_write_vector_field(root, pid, time, _format(fmt), name.encode(), abi.dptr(a2.reshape(-1)),
+                                         a2.shape[0], a2.shape[1])
+    if rc != 0:
+        raise MplbError(rc, lib.mplb_gpu_last_error().decode())
 
 
 class Lattice:
@@ -231,11 +261,22 @@ class Lattice:
                                                          C.byref(r)))
         return st.value, r.value
 
-    def snapshot(self, pressure=False):
-        """Queue a write-step copy of rho, U, T (and p) and its transfer to the
-        host; stepping may continue before snapshot_wait."""
-        self._check(self.lib.mplb_gpu_snapshot(self.h, 1 if pressure else 0))
+    def snapshot(self, pressure=False, pdfs=False):
+        """Queue a write-step copy of rho, U, T (and p; and f, g with pdfs)
+        and its transfer to the host; stepping may continue before
+        snapshot_wait / snapshot_write."""
+        flags = (abi.SNAP_PRESSURE if pressure else 0) | (abi.SNAP_PDFS if pdfs else 0)
+        self._check(self.lib.mplb_gpu_snapshot(self.h, flags))
         self._snap_p = pressure
+
+    def snapshot_write(self, root="", pid=0, fmt="asciiRaw"):
+        """Write the last snapshot's fields (rho, T, p, U, f, g as taken) to
+        <root>/processor<pid>/<time>/ on a host thread; returns at once."""
+        self._check(self.lib.mplb_gpu_snapshot_write(self.h, os.fsencode(root), pid, _format(fmt)))
+
+    def snapshot_join(self):
+        """Wait for the snapshot writer; raises the first error of its writes."""
+        self._check(self.lib.mplb_gpu_snapshot_join(self.h))
 
     def snapshot_wait(self):
         n = self.n

@@ -12,9 +12,11 @@
 #include <cstdio>
 #include <cstring>
 #include <string>
+#include <thread>
 #include <unordered_set>
 #include <vector>
 
+#include "mplb_io.h"
 #include "ops.cuh"
 #include "fused_host.cuh"
 #include "fused32.cuh"
@@ -113,13 +115,21 @@ struct mplb_gpu {
     double rho_ref = 0, T_ref = 0;
     double* snap = nullptr;  // equilibrium monitor: density at the last check
     long long* mom = nullptr;  // FP32 equilibrium runs: total momentum now [0..2] and at the start [3..5]
-    // write-step snapshot: device copy [rho | T | p | U as [node][3]], its
-    // pinned host image, the side stream that transfers it, and events
+    // write-step snapshot: device copy [rho | T | p | U as [node][3] | f, g
+    // as [node][Q]], its pinned host image, the side stream that transfers
+    // it, and events
     double* snap_dev = nullptr;
     double* snap_host = nullptr;
+    size_t snap_cap = 0;  // doubles held by snap_dev and snap_host
     cudaStream_t snap_stream = nullptr;
     cudaEvent_t snap_ready = nullptr, snap_done = nullptr;
-    bool snap_pending = false, snap_has_p = false;
+    bool snap_pending = false, snap_has_p = false, snap_has_pdfs = false;
+    uint32_t snap_time = 0;
+    // host thread writing the last snapshot's files, and the first error of
+    // the writes since the last join
+    std::thread writer;
+    int writer_rc = 0;
+    std::string writer_err;
     int tile_request = 0;  // mplb_opts.tile_config
     uint32_t current = 0;
     uint64_t launches = 0;
@@ -571,6 +581,12 @@ int put_scalar(mplb_gpu* h, const double* host, double* dev) {
     return 0;
 }
 
+// Waits for the snapshot writer thread, if one runs; its status stays in
+// writer_rc for the next join.
+void writer_wait(mplb_gpu* h) {
+    if (h->writer.joinable()) h->writer.join();
+}
+
 struct DeviceGuard {
     int prev = -1;
     explicit DeviceGuard(int dev) {
@@ -910,6 +926,7 @@ int mplb_gpu_create(const mplb_mesh_desc* mesh, const mplb_eos_desc* eos, const 
 int mplb_gpu_destroy(mplb_gpu_t* h) {
     if (!h) return 0;
     DeviceGuard guard(h->dev);
+    writer_wait(h);
     cudaStreamSynchronize(h->stream);
     if (h->snap_stream) {
         cudaStreamSynchronize(h->snap_stream);
@@ -1076,16 +1093,35 @@ int mplb_gpu_macro_pressure(mplb_gpu_t* h) {
     return DISPATCH(h, op_pressure, h);
 }
 
-int mplb_gpu_snapshot(mplb_gpu_t* h, int32_t with_pressure) {
+int mplb_gpu_snapshot(mplb_gpu_t* h, int32_t flags) {
     if (!h) return fail(MPLB_E_ARG, "NULL handle");
-    if (with_pressure && h->P.f_update && h->model[0] != MPLB_LIMRT && h->model[0] != MPLB_XUMRT)
+    if (flags & ~(MPLB_SNAP_PRESSURE | MPLB_SNAP_PDFS)) return fail(MPLB_E_ARG, "unknown snapshot flags");
+    const bool with_p = flags & MPLB_SNAP_PRESSURE, with_pdfs = flags & MPLB_SNAP_PDFS;
+    if (with_p && h->P.f_update && h->model[0] != MPLB_LIMRT && h->model[0] != MPLB_XUMRT)
         return fail(MPLB_E_UNSUPPORTED, "Pressure update not available (macroPressure.c:60-64)");
     DeviceGuard guard(h->dev);
-    const size_t n = h->n;
-    if (!h->snap_dev) {
-        CK(cudaMalloc((void**)&h->snap_dev, 6 * n * sizeof(double)));
-        h->bytes += 6 * n * sizeof(double);
-        CK(cudaMallocHost((void**)&h->snap_host, 6 * n * sizeof(double)));
+    const size_t n = h->n, Q = h->Q;
+    const size_t need = 6 * n + (with_pdfs ? 2 * Q * n : 0);
+    // the host image must not be rewritten while a writer reads it
+    writer_wait(h);
+    if (need > h->snap_cap) {
+        if (h->snap_pending) CK(cudaEventSynchronize(h->snap_done));
+        if (h->snap_dev) {
+            CK(cudaStreamSynchronize(h->stream));
+            cudaFree(h->snap_dev);
+            h->bytes -= h->snap_cap * sizeof(double);
+            h->snap_dev = nullptr;
+        }
+        if (h->snap_host) cudaFreeHost(h->snap_host);
+        h->snap_host = nullptr;
+        h->snap_cap = 0;
+        h->snap_pending = false;
+        CK(cudaMalloc((void**)&h->snap_dev, need * sizeof(double)));
+        h->bytes += need * sizeof(double);
+        CK(cudaMallocHost((void**)&h->snap_host, need * sizeof(double)));
+        h->snap_cap = need;
+    }
+    if (!h->snap_stream) {
         CK(cudaStreamCreateWithFlags(&h->snap_stream, cudaStreamNonBlocking));
         CK(cudaEventCreateWithFlags(&h->snap_ready, cudaEventDisableTiming));
         CK(cudaEventCreateWithFlags(&h->snap_done, cudaEventDisableTiming));
@@ -1093,18 +1129,27 @@ int mplb_gpu_snapshot(mplb_gpu_t* h, int32_t with_pressure) {
     // the device copy must not be rewritten while the previous one is in flight
     if (h->snap_pending) CK(cudaStreamWaitEvent(h->stream, h->snap_done, 0));
     RET(materialize(h));
-    if (with_pressure) RET(DISPATCH(h, op_pressure, h));
+    if (with_p) RET(DISPATCH(h, op_pressure, h));
     CK(cudaMemcpyAsync(h->snap_dev, h->rho, n * sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
     CK(cudaMemcpyAsync(h->snap_dev + n, h->T, n * sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
-    if (with_pressure)
+    if (with_p)
         CK(cudaMemcpyAsync(h->snap_dev + 2 * n, h->p, n * sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
     LAUNCH(k_soa_to_aos, blocks(3 * n), h->n, 3, h->U, h->snap_dev + 3 * n);
+    if (with_pdfs) {
+        for (int fi = 0; fi < 2; fi++) {
+            double* dst = h->snap_dev + 6 * n + fi * Q * n;
+            if (h->model[fi] == MPLB_NO_MODEL) CK(cudaMemsetAsync(dst, 0, Q * n * sizeof(double), h->stream));
+            else LAUNCH(k_soa_to_aos, blocks(Q * n), h->n, h->Q, fi ? h->G() : h->F(), dst);
+        }
+    }
     CK(cudaEventRecord(h->snap_ready, h->stream));
     CK(cudaStreamWaitEvent(h->snap_stream, h->snap_ready, 0));
-    CK(cudaMemcpyAsync(h->snap_host, h->snap_dev, 6 * n * sizeof(double), cudaMemcpyDeviceToHost, h->snap_stream));
+    CK(cudaMemcpyAsync(h->snap_host, h->snap_dev, need * sizeof(double), cudaMemcpyDeviceToHost, h->snap_stream));
     CK(cudaEventRecord(h->snap_done, h->snap_stream));
     h->snap_pending = true;
-    h->snap_has_p = with_pressure != 0;
+    h->snap_has_p = with_p;
+    h->snap_has_pdfs = with_pdfs;
+    h->snap_time = h->current;
     return 0;
 }
 
@@ -1120,6 +1165,53 @@ int mplb_gpu_snapshot_wait(mplb_gpu_t* h, double* rho, double* U, double* T, dou
     if (p) std::memcpy(p, h->snap_host + 2 * n, n * sizeof(double));
     if (U) std::memcpy(U, h->snap_host + 3 * n, 3 * n * sizeof(double));
     return 0;
+}
+
+int mplb_gpu_snapshot_write(mplb_gpu_t* h, const char* root, int32_t pid, int32_t format) {
+    if (!h) return fail(MPLB_E_ARG, "NULL handle");
+    if (!h->snap_pending) return fail(MPLB_E_STATE, "no snapshot was taken");
+    if (format == MPLB_FMT_ENSIGHT) return fail(MPLB_E_UNSUPPORTED, "EnSight output (MPI-IO) is not provided");
+    if (format != MPLB_FMT_ASCII_RAW && format != MPLB_FMT_BINARY_RAW && format != MPLB_FMT_PVTU)
+        return fail(MPLB_E_ARG, "unknown data format");
+    writer_wait(h);
+    std::string dir = root ? root : "";
+    h->writer = std::thread([h, dir, pid, format]() {
+        int rc = 0;
+        std::string err;
+        cudaSetDevice(h->dev);
+        cudaError_t e = cudaEventSynchronize(h->snap_done);
+        if (e != cudaSuccess) {
+            rc = MPLB_E_CUDA;
+            err = std::string("snapshot transfer: ") + cudaGetErrorString(e);
+        }
+        const size_t n = h->n, Q = h->Q;
+        const double* s = h->snap_host;
+        struct Item { const char* name; const double* v; uint32_t vs; bool scalar; bool on; };
+        const Item items[] = {{"rho", s, 1, true, true},
+                              {"T", s + n, 1, true, true},
+                              {"p", s + 2 * n, 1, true, h->snap_has_p},
+                              {"U", s + 3 * n, 3, false, true},
+                              {"f", s + 6 * n, (uint32_t)Q, false, h->snap_has_pdfs},
+                              {"g", s + 6 * n + Q * n, (uint32_t)Q, false, h->snap_has_pdfs}};
+        for (const Item& it : items) {
+            if (rc) break;
+            if (!it.on) continue;
+            rc = mplb_io_write(dir.c_str(), pid, h->snap_time, format, it.name, it.v, n, it.vs, it.scalar, &err);
+        }
+        if (rc && !h->writer_rc) {
+            h->writer_rc = rc;
+            h->writer_err = err;
+        }
+    });
+    return 0;
+}
+
+int mplb_gpu_snapshot_join(mplb_gpu_t* h) {
+    if (!h) return fail(MPLB_E_ARG, "NULL handle");
+    writer_wait(h);
+    const int rc = h->writer_rc;
+    h->writer_rc = 0;
+    return rc ? fail(rc, h->writer_err) : 0;
 }
 
 int mplb_gpu_download_pressure(mplb_gpu_t* h, double* p) {

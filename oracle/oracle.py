@@ -150,3 +150,48 @@ class Checker:
 
     def potential(self, rho, T):
         return self._f("potential")(self.h, rho, T)
+
+
+# ------------------------------------------------------------- field files
+def field_file_bytes(fmt, name, field, scalar):
+    """The bytes the reference's writers put in one file, restated in Python.
+
+    asciiRaw: "%g\\n" per node for a scalar (asciiRaw/writeScalarToAsciiRaw.c:36),
+    "%g " per component and "\\n" per node for an array
+    (asciiRaw/writeArrayToAsciiRaw.c:36-44).  binaryRaw: every value cast to
+    float32, node order (binaryRaw/writeScalarToBinaryRaw.c:32-40,
+    writeArrayToBinaryRaw.c:36-46).  pvtu: the DataArray block appended to
+    fields.vtu (pvtu/writeScalarToPvtu.c:22-31, pvtu/writeArrayToPvtu.c:22-42).
+    Python's '%g' is correctly rounded like the C library's, so the text is
+    the same.
+    """
+    a = np.asarray(field, dtype=np.float64)
+    if fmt == abi.FMT_BINARY_RAW:
+        with np.errstate(over="ignore"):  # out-of-range values become +-inf, as the C cast does here
+            return a.astype(np.float32).tobytes()
+    rows = a.reshape(-1, 1) if scalar else a.reshape(a.shape[0], -1)
+    lead = "          " if fmt == abi.FMT_PVTU else ""
+    if scalar:
+        body = "".join(f"{lead}{v:g}\n" for v in rows[:, 0].tolist())
+    else:
+        body = "".join(lead + "".join(f"{v:g} " for v in r) + "\n" for r in rows.tolist())
+    if fmt == abi.FMT_PVTU:
+        if scalar:
+            head = f'        <DataArray type="Float32" Name="{name}" format="ascii">\n'
+        else:
+            head = f'        <DataArray type="Float32" Name="{name}"  NumberOfComponents="{rows.shape[1]}" format="ascii">\n'
+        body = head + body + "        </DataArray>\n"
+    return body.encode()
+
+
+def ref_write_field(fmt, name, field, scalar, pid, time):
+    """Run the reference's own writer (oracle/_ref) on ``field``; files go
+    under the current folder, as in the reference."""
+    lib = _lib("ref")
+    lib.ref_write_field.argtypes = [C.c_int, C.c_int, C.c_char_p, C.POINTER(C.c_double), C.c_uint32, C.c_uint32,
+                                    C.c_int, C.c_uint32]
+    a = np.ascontiguousarray(field, dtype=np.float64)
+    n = a.shape[0]
+    vs = 1 if scalar else int(a.size // max(n, 1))
+    rc = lib.ref_write_field(fmt, 1 if scalar else 0, name.encode(), abi.dptr(a.reshape(-1)), n, vs, pid, time)
+    assert rc == 0

@@ -15,7 +15,9 @@
  *              macroDensity; heatSource; macroTemperature; interForce;
  *              macroVelocity), with updateTime() semantics for time.current
  *              (src/IO/time/timeOptions.c:35-64).
- * Results are copied out as doubles, so no float-precision writer is involved.
+ * Results are copied out as doubles, so no float-precision writer is involved
+ * in the lattice checks; ref_write_field runs the reference's field writers
+ * for the byte-for-byte check of the library's writers.
  */
 #include <stdio.h>
 #include <stdlib.h>
@@ -29,6 +31,9 @@
 #include <basic.h>
 #include <generalLbe.h>
 #include <pseudoPot.h>
+#include <asciiRaw.h>
+#include <binaryRaw.h>
+#include <pvtu.h>
 
 #include "../include/mplb_gpu.h"
 
@@ -316,3 +321,45 @@ void ref_structs(ref_case* c, latticeMesh** m, macroFields** mf, lbeField** f, l
 /* p_eos and potential as scalar functions, for EOS-level checks. */
 double ref_p_eos(ref_case* c, double rho, double T) { return p_eos(&c->mesh.EOS, rho, T); }
 double ref_potential(ref_case* c, double rho, double T) { return potential(&c->mesh, rho, T); }
+
+/*
+ * The reference's own field writers (src/IO/asciiRaw, binaryRaw, pvtu) on a
+ * host array: format 0 asciiRaw, 1 binaryRaw, 2 pvtu (include/dataTypes.h:53);
+ * scalar != 0 takes writeScalarTo*, else writeArrayTo* with vsize columns.
+ * Files go to processor<pid>/<time>/ under the CURRENT folder, as in the
+ * reference; pvtu appends to an existing fields.vtu there.  field is
+ * [n][vsize] doubles.  Never called with a NaN (the reference's NaN check
+ * lives in writeScalarField, which exits).
+ */
+int ref_write_field(int format, int scalar, const char* name, const double* field, uint32_t n, uint32_t vsize,
+                    int pid, uint32_t time) {
+    latticeMesh mesh;
+    memset(&mesh, 0, sizeof mesh);
+    mesh.mesh.nPoints = n;
+    mesh.parallel.pid = pid;
+    mesh.time.current = time;
+    char nm[100];
+    snprintf(nm, sizeof nm, "%s", name);
+    if (scalar) {
+        double* v = (double*)malloc((n ? n : 1) * sizeof(double));
+        memcpy(v, field, n * sizeof(double));
+        switch (format) {
+        case 0: writeScalarToAsciiRaw(nm, v, &mesh); break;
+        case 1: writeScalarToBinaryRaw(nm, v, &mesh); break;
+        case 2: writeScalarToPvtu(nm, v, &mesh); break;
+        default: free(v); return -1;
+        }
+        free(v);
+        return 0;
+    }
+    double** r = rows_alloc(n, vsize);
+    put_rows(r, field, n, (int)vsize);
+    switch (format) {
+    case 0: writeArrayToAsciiRaw(nm, r, &mesh, vsize); break;
+    case 1: writeArrayToBinaryRaw(nm, r, &mesh, vsize); break;
+    case 2: writeArrayToPvtu(nm, r, &mesh, vsize); break;
+    default: rows_free(r, n); return -1;
+    }
+    rows_free(r, n);
+    return 0;
+}

@@ -92,7 +92,7 @@ GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
 
 
 def golden_files():
-    return sorted(f for f in os.listdir(GOLDEN) if f.endswith(".npz"))
+    return sorted(f for f in os.listdir(GOLDEN) if f.endswith("steps.npz"))
 
 
 @pytest.mark.parametrize("fname", golden_files())
