@@ -119,14 +119,17 @@ typedef struct mplb_eos_desc {
  * src/lbEquation/lbParameters.h:16-31).
  */
 typedef struct mplb_field_desc {
-    int32_t model;            /* MPLB_LIMRT, MPLB_XUMRT, MPLB_LITEMPMRT or MPLB_NO_MODEL */
+    int32_t model;            /* MPLB_LIMRT, MPLB_XUMRT (flow); MPLB_LITEMPMRT, MPLB_MYMRT (thermal); MPLB_NO_MODEL */
     int32_t update;           /* 0 = frozen (reference --frozen / --nht) */
     double Lambda[MPLB_MAX_Q];
     double sigma;             /* liMRT / xuMRT force coefficient */
     int32_t surface_tension;  /* 1 = liMRT / xuMRT surface-tension term (liMRTSurfaceTension.c, xuMRTSurfaceTension.c); FP64 only */
     double kappa_st;
     const int32_t* bc_type;   /* [n_patches] MPLB_BC_* for this field */
-    const double* bc_value;   /* [n_patches][3]: fixedT uses [0], fixedU uses [0..2] */
+    const double* bc_value;   /* [n_patches][3]: fixedT uses [0], fixedU uses [0..2]; fixedRandomT:
+                                 [0] T, [1] perturbation in percent, [2] boundary updates still
+                                 perturbed (psteps - localTStep, fixedRandomTParam.h); outflow: none */
+    double alpha_1, alpha_2;  /* myMRT equilibrium constants (myMRTConstants.h) */
 } mplb_field_desc;
 
 typedef struct mplb_opts {
@@ -137,6 +140,8 @@ typedef struct mplb_opts {
     uint32_t start_time; /* reference timeInfo.start: the time the first step leaves */
     int32_t tile_config; /* fused path: 0 = time the tile candidates on the first step and keep
                             the fastest; k > 0 = use candidate k-1; -1 = candidate 0, no timing */
+    int32_t rank;        /* parallel.pid of this domain: fixedRandomT seeds rand() with it
+                            (fixedRandomT.c:37) */
 } mplb_opts;
 
 /* What create decided; filled by mplb_gpu_info. */

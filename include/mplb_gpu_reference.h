@@ -79,6 +79,11 @@ static inline void mplb_ref_pack_field(const latticeMesh* mesh, const lbeField* 
     case liTempMRT:
         lam = fl->lbparam.liTempMRT.Lambda;
         break;
+    case myMRT:
+        lam = fl->lbparam.myMRT.Lambda;
+        fd->alpha_1 = fl->lbparam.myMRT.alpha_1;
+        fd->alpha_2 = fl->lbparam.myMRT.alpha_2;
+        break;
     default:
         lam = fl->lbparam.myMRT.Lambda;
         break;
@@ -91,6 +96,12 @@ static inline void mplb_ref_pack_field(const latticeMesh* mesh, const lbeField* 
         if (fl->boundary[p].type == ft) d->bc_value[which][3 * p] = fl->boundary[p].param.ft.T;
         if (fl->boundary[p].type == fu)
             for (int j = 0; j < 3; j++) d->bc_value[which][3 * p + j] = fl->boundary[p].param.fu.U[j];
+        if (fl->boundary[p].type == frdt) {
+            d->bc_value[which][3 * p] = fl->boundary[p].param.frdt.T;
+            d->bc_value[which][3 * p + 1] = fl->boundary[p].param.frdt.p;
+            d->bc_value[which][3 * p + 2] =
+                (double)fl->boundary[p].param.frdt.psteps - (double)fl->boundary[p].param.frdt.localTStep;
+        }
     }
     fd->bc_type = d->bc_type[which];
     fd->bc_value = d->bc_value[which];
@@ -164,7 +175,15 @@ static inline int mplb_ref_create(const latticeMesh* mesh, const macroFields* mf
     mplb_ref_descs d;
     int rc = mplb_ref_pack(mesh, f, g, &d);
     if (rc) return rc;
-    rc = mplb_gpu_create(&d.mesh, &d.eos, &d.field[0], &d.field[1], opts, out);
+    mplb_opts o;
+    if (opts) o = *opts;
+    else {
+        memset(&o, 0, sizeof(o));
+        o.device = -1;
+        o.start_time = mesh->time.current;
+    }
+    o.rank = mesh->parallel.pid;  /* fixedRandomT seeds rand() with it */
+    rc = mplb_gpu_create(&d.mesh, &d.eos, &d.field[0], &d.field[1], &o, out);
     if (rc == 0) {
         uint32_t n = mesh->mesh.nPoints;
         int Q = mesh->lattice.Q;

@@ -130,12 +130,14 @@ class Lattice:
     """
 
     def __init__(self, case, path=PATH_AUTO, device=-1, stream=None, start_time=0, tile_config=0,
-                 precision=abi.FP64):
+                 precision=abi.FP64, rank=None):
         self.lib = load_library()
         self.case = case
         self.n, self.Q = case.n, case.Q
         self._desc = abi.Descriptors(case)
-        opts = abi.Opts(precision, path, device, stream, start_time, tile_config)
+        if rank is None:
+            rank = (getattr(case, "meta", None) or {}).get("rank", 0)
+        opts = abi.Opts(precision, path, device, stream, start_time, tile_config, rank)
         h = C.c_void_p()
         self._check(self.lib.mplb_gpu_create(C.byref(self._desc.mesh), C.byref(self._desc.eos),
                                               C.byref(self._desc.f), C.byref(self._desc.g),

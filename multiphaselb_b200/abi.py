@@ -58,6 +58,8 @@ class FieldDesc(C.Structure):
         ("kappa_st", C.c_double),
         ("bc_type", C.POINTER(C.c_int32)),
         ("bc_value", C.POINTER(C.c_double)),
+        ("alpha_1", C.c_double),
+        ("alpha_2", C.c_double),
     ]
 
 
@@ -69,6 +71,7 @@ class Opts(C.Structure):
         ("stream", C.c_void_p),
         ("start_time", C.c_uint32),
         ("tile_config", C.c_int32),
+        ("rank", C.c_int32),
     ]
 
 
@@ -173,4 +176,4 @@ class Descriptors:
         self._keep += [bct, bcv]
         return FieldDesc(fd["model"], int(fd.get("update", 1)), (C.c_double * MAX_Q)(*lam),
                          fd.get("sigma", 0.0), int(fd.get("surface_tension", 0)), fd.get("kappa_st", 0.0),
-                         iptr(bct), dptr(bcv))
+                         iptr(bct), dptr(bcv), fd.get("alpha_1", 0.0), fd.get("alpha_2", 0.0))

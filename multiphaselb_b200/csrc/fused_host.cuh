@@ -176,6 +176,7 @@ inline bool fused_supported(int lat, const int* model, const Params& P, const st
     if (!active[0] && !active[1]) { why = "no field is updated"; return false; }
     if (!active[0] && model[0] == MPLB_NO_MODEL) { why = "no flow field"; return false; }
     if (lat == MPLB_D3Q15 && active[1]) { why = "thermal field on D3Q15"; return false; }
+    if (active[1] && model[1] != MPLB_LITEMPMRT) { why = "myMRT thermal field"; return false; }
     for (int fi = 0; fi < 2; fi++) {
         if (!active[fi]) continue;
         for (const PatchDev& pt : fp[fi]) {

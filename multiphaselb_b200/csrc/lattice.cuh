@@ -87,7 +87,12 @@ struct Params {
     int32_t g_model, g_update;
     double Lg[MPLB_MAX_Q];
     double corr3, corr5;         // (1 - L3/2)*L4, (1 - L5/2)*L6   liTempMRTCollision.c:75-77
-    double lam_fac;              // (1/Lambda[3] - 0.5)           heatSource.c:105
+    double lam_fac;              // (1/Lambda[3] - 0.5)           heatSource.c:40,105
+    // myMRT thermal model (myMRTCollision.c, myMRTEquilibriumMS.c, heatSource.c:28-90)
+    double my_a1, my_a2;         // alpha_1, alpha_2
+    double my_qo[3];             // off-diagonal rates Q[3][4], Q[5][6], Q[7][8]   myMRTCollision.c:80-116
+    double my_qa0;               // (I - Q/2)[0][0] = 1.0 + (-0.5*Lambda[0])      myMRTCollision.c:125-140
+    double my_lgeo, my_ldiv;     // conductivity factor: (4 + 3a1 + 2a2), 6 (D2Q9); (6 + 11a1 + a2), 9 (D3Q15)
     // EOS (EOSInfo.h:80-102)
     int32_t eos;
     double a, b, R, G, M, Cv, rho_0;
@@ -466,6 +471,69 @@ MPLB_HD void collide_litemp(const Params& P, double* g, double T, double u0, dou
     n[3] = n[3] + P.corr3 * n4;
     n[5] = n[5] + P.corr5 * n6;
     mul_Mi<D2Q9T>(P, n, g);
+}
+
+// ------------------------------------------------------------ myMRT (thermal)
+// Moments of the equilibrium, myMRTEquilibriumMS.c:17-75 (= myMRTEquilibrium.c:
+// 10-88): T, alpha_1 T, alpha_2 T, +-T u_d, zeros.  T*(-u) and -(T*u) (the
+// D3Q15 form) are the same double.
+template <class L>
+MPLB_HD void neq_mymrt(const Params& P, double T, const double* u, double* ne) {
+    ne[0] = T;
+    ne[1] = P.my_a1 * T;
+    ne[2] = P.my_a2 * T;
+    ne[3] = T * u[0];
+    ne[4] = T * (-u[0]);
+    ne[5] = T * u[1];
+    ne[6] = T * (-u[1]);
+    if constexpr (L::Q == 15) {
+        ne[7] = T * u[2];
+        ne[8] = T * (-u[2]);
+#pragma unroll
+        for (int k = 9; k < 15; k++) ne[k] = 0;
+    } else {
+        ne[7] = 0;
+        ne[8] = 0;
+    }
+}
+
+// myMRTEquilibrium.c: g = M^-1 n_eq.
+template <class L>
+MPLB_HD void eq_mymrt(const Params& P, double T, const double* u, double* g) {
+    double ne[L::Q];
+    neq_mymrt<L>(P, T, u, ne);
+    mul_Mi<L>(P, ne, g);
+}
+
+// myMRTCollision.c:150-210: n = M g; n <- n - Q (n - n_eq) + (I - Q/2) Gamma,
+// Q diagonal (Lambda) plus the pairs (3,4), (5,6) [, (7,8)], Gamma =
+// (scalarSource, 0, ...) (myMRTSource.c:17-25), both products as the sparse
+// row sums of sparseMatVecMult.c:4-28.  Rows k >= 1 of (I - Q/2) Gamma are
+// +-0, and n - Q (n - n_eq) is never -0 (M g sums start from +0), so those
+// additions leave it unchanged and are not made.
+template <class L>
+MPLB_HD void collide_mymrt(const Params& P, double* g, double T, const double* u, double src) {
+    double ne[L::Q], n[L::Q], a[L::Q];
+    neq_mymrt<L>(P, T, u, ne);
+    mul_M<L>(g, n);
+#pragma unroll
+    for (int k = 0; k < L::Q; k++) a[k] = P.Lg[k] * (n[k] - ne[k]);
+    a[3] = a[3] + P.my_qo[0] * (n[4] - ne[4]);
+    a[5] = a[5] + P.my_qo[1] * (n[6] - ne[6]);
+    if constexpr (L::Q == 15) a[7] = a[7] + P.my_qo[2] * (n[8] - ne[8]);
+    n[0] = n[0] - a[0] + P.my_qa0 * src;
+#pragma unroll
+    for (int k = 1; k < L::Q; k++) n[k] = n[k] - a[k];
+    mul_Mi<L>(P, n, g);
+}
+
+// heatSource.c:28-90 (myMRT): the liTempMRT source without the time
+// extrapolation, conductivity rho Cv (1/L3 - 1/2) (geo) / div.
+MPLB_HD double heat_source_value_my(const Params& P, double rho, double T, double dot, double divU) {
+    double lambda = rho * P.Cv * P.lam_fac * P.my_lgeo / P.my_ldiv;
+    double dpdT = p_eos(P, rho, 1.1 * T) - p_eos(P, rho, 0.9 * T);
+    dpdT = dpdT / (0.2 * T);
+    return -lambda * dot / P.Cv + divU * T * (1.0 - dpdT / (rho * P.Cv));
 }
 
 // heatSource.c:144-165: source from gradients (dot), divergence, rho, T_old.

@@ -98,6 +98,13 @@ struct mplb_gpu {
     double *T2 = nullptr, *U2 = nullptr;  // fused-path double buffers
     uint8_t* bcmap = nullptr;             // fused-path per-node boundary-program index
     uint32_t* pnodes = nullptr;
+    // per field, [patch nodes][Q] tables made at create for outflow (normal,
+    // normal direction) and fixedRandomT (perturbed wall temperatures)
+    double* bctab[2] = {nullptr, nullptr};
+    // fixedRandomT: boundary updates made on each field, and per patch how
+    // many of the first ones are perturbed (psteps - localTStep)
+    uint64_t bc_calls[2] = {0, 0};
+    std::vector<int64_t> rnd_left[2];
     PatchDev* dpatches = nullptr;          // [field][patch] copies for the serial kernel
     std::vector<PatchDev> fpatch[2];       // per-field patch tables (type, values)
     std::vector<int32_t> bct[2];
@@ -162,6 +169,8 @@ void free_all(mplb_gpu* h) {
             if (h->p32[i][j]) cudaFree(h->p32[i][j]);
     if (h->snap) cudaFree(h->snap);
     if (h->mom) cudaFree(h->mom);
+    for (int i = 0; i < 2; i++)
+        if (h->bctab[i]) cudaFree(h->bctab[i]);
 }
 
 // Does the FP32 form's momentum reset apply?  Fully periodic box without
@@ -280,8 +289,8 @@ int check_field(const mplb_field_desc* d, int lat, int which, uint32_t npatch, s
         if (d->model == MPLB_XUMRT && lat != MPLB_D3Q15) { why = "xuMRT is D3Q15 only (xuMRTForce.c:9)"; return MPLB_E_UNSUPPORTED; }
         if (d->model != MPLB_LIMRT && d->model != MPLB_XUMRT) { why = "f model must be liMRT or xuMRT"; return MPLB_E_UNSUPPORTED; }
     } else {
-        if (d->model != MPLB_LITEMPMRT) { why = "g model must be liTempMRT"; return MPLB_E_UNSUPPORTED; }
-        if (lat != MPLB_D2Q9) { why = "liTempMRT is D2Q9 only (liTempMRTEquilibriumMS.c:45-49)"; return MPLB_E_UNSUPPORTED; }
+        if (d->model != MPLB_LITEMPMRT && d->model != MPLB_MYMRT) { why = "g model must be liTempMRT or myMRT"; return MPLB_E_UNSUPPORTED; }
+        if (d->model == MPLB_LITEMPMRT && lat != MPLB_D2Q9) { why = "liTempMRT is D2Q9 only (liTempMRTEquilibriumMS.c:45-49)"; return MPLB_E_UNSUPPORTED; }
     }
     for (uint32_t p = 0; p < npatch; p++) {
         int t = d->bc_type ? d->bc_type[p] : MPLB_BC_PERIODIC;
@@ -289,14 +298,18 @@ int check_field(const mplb_field_desc* d, int lat, int which, uint32_t npatch, s
         case MPLB_BC_PERIODIC:
         case MPLB_BC_BOUNCEBACK: break;
         case MPLB_BC_FIXEDT:
-            if (d->model != MPLB_LITEMPMRT) { why = "fixedT needs the liTempMRT field (fixedT.c:150-153)"; return MPLB_E_UNSUPPORTED; }
+            if (d->model != MPLB_LITEMPMRT && d->model != MPLB_MYMRT) { why = "fixedT needs a liTempMRT or myMRT field (fixedT.c:57-73)"; return MPLB_E_UNSUPPORTED; }
             break;
+        case MPLB_BC_FIXEDRANDOMT:
+            if (d->model != MPLB_MYMRT) { why = "fixedRandomT needs the myMRT field (fixedRandomT.c:20,125)"; return MPLB_E_UNSUPPORTED; }
+            break;
+        case MPLB_BC_OUTFLOW: break;
         case MPLB_BC_FIXEDU: break;  // a no-op for models other than liMRT (fixedU.c:10)
         default:
-            why = "boundary type " + std::to_string(t) + " is outside this path (bounceBack, fixedT, fixedU, periodic)";
+            why = "boundary type " + std::to_string(t) + " is outside this path (bounceBack, fixedT, fixedU, fixedRandomT, outflow, periodic)";
             return MPLB_E_UNSUPPORTED;
         }
-        if ((t == MPLB_BC_FIXEDT || t == MPLB_BC_FIXEDU) && !d->bc_value) { why = "bc_value missing"; return MPLB_E_ARG; }
+        if ((t == MPLB_BC_FIXEDT || t == MPLB_BC_FIXEDU || t == MPLB_BC_FIXEDRANDOMT) && !d->bc_value) { why = "bc_value missing"; return MPLB_E_ARG; }
     }
     return 0;
 }
@@ -357,6 +370,60 @@ bool detect_box(mplb_gpu* h, const mplb_mesh_desc* m) {
     return true;
 }
 
+// outflow.c:29-90 for one boundary node: the normal, sum of the velocities
+// whose node x + c_k is missing, normalised in float as the reference does,
+// and ln, the last direction equal to the normal truncated to int.  Returns
+// false where no normal exists ("Unable to detect normal in outflow boundary").
+bool outflow_normal(int Q, const int32_t* nb, float* normal, int* ln) {
+    auto rev = [&](int k) { return Q == 9 ? revk<D2Q9T>(k) : revk<D3Q15T>(k); };
+    auto c = [&](int k, int j) { return Q == 9 ? ck<D2Q9T>(k, j) : ck<D3Q15T>(k, j); };
+    normal[0] = normal[1] = normal[2] = 0;
+    for (int k = 0; k < Q; k++)
+        if (nb[rev(k)] == -1)
+            for (int j = 0; j < 3; j++) normal[j] += c(k, j);
+    float nmag = 0;
+    for (int j = 0; j < 3; j++) nmag += normal[j] * normal[j];
+    if (nmag == 0) return false;
+    nmag = (float)std::sqrt((double)nmag);
+    for (int j = 0; j < 3; j++) normal[j] = normal[j] / nmag;
+    *ln = 0;
+    for (int k = 0; k < Q; k++)
+        if (c(k, 0) == (int)normal[0] && c(k, 1) == (int)normal[1] && c(k, 2) == (int)normal[2]) *ln = k;
+    return true;
+}
+
+// rand() of the GNU C library after srand(seed), which fixedRandomT calls at
+// every application (fixedRandomT.c:37,81): the additive feedback generator
+// r_i = r_{i-3} + r_{i-31} (mod 2^32) over 31 words seeded by the Park-Miller
+// generator r_i = 16807 r_{i-1} mod (2^31 - 1) (seed 0 taken as 1), the
+// first 310 outputs discarded, each output r_i >> 1 (P. Selinger, "The GLIBC
+// pseudo-random number generator", 2007).
+class GnuRand {
+public:
+    explicit GnuRand(uint32_t seed) {
+        int64_t w = seed == 0 ? 1 : seed;
+        r_[0] = (uint32_t)w;
+        for (int i = 1; i < 31; i++) {
+            w = (16807 * w) % 2147483647;
+            if (w < 0) w += 2147483647;
+            r_[i] = (uint32_t)w;
+        }
+        for (int i = 31; i < 34; i++) r_[i] = r_[i - 31];
+        i_ = 34;
+        for (int i = 0; i < 310; i++) next();
+    }
+    int next() {
+        uint32_t v = r_[(i_ - 31) % 34] + r_[(i_ - 3) % 34];
+        r_[i_ % 34] = v;
+        i_++;
+        return (int)(v >> 1);
+    }
+
+private:
+    uint32_t r_[34];
+    uint64_t i_;
+};
+
 // Can a field's boundary patches run one thread per node?  Not if a node
 // reads a population that any boundary op writes (the reference's serial
 // order would then be observable) or if a patch lists a node twice.
@@ -383,12 +450,24 @@ bool needs_serial(const mplb_gpu* h, const mplb_mesh_desc* m, int fi) {
                         writes.insert((uint64_t)id * Q + k);
                         writes.insert((uint64_t)id * Q + rev(k));
                     }
+                } else if (t == MPLB_BC_OUTFLOW) {
+                    if (nb[k] == -1) writes.insert((uint64_t)id * Q + k);
                 } else if (nb[k] == -1 && nb[rev(k)] != -1) {
                     uint32_t nbid = (uint32_t)nb[rev(k)];
                     writes.insert((uint64_t)id * Q + k);
-                    if (t == MPLB_BC_FIXEDT) reads.push_back((uint64_t)nbid * Q + k);
+                    if (t == MPLB_BC_FIXEDT || t == MPLB_BC_FIXEDRANDOMT) reads.push_back((uint64_t)nbid * Q + k);
                     else
                         for (int q = 0; q < Q; q++) reads.push_back((uint64_t)nbid * Q + q);
+                }
+            }
+            if (t == MPLB_BC_OUTFLOW) {
+                // outflow.c:93-175: every population of the inner neighbour along the normal
+                int ln;
+                float nrm[3];
+                if (outflow_normal(Q, nb, nrm, &ln)) {
+                    int32_t m = nb[ln];
+                    if (m != -1)
+                        for (int q = 0; q < Q; q++) reads.push_back((uint64_t)m * Q + q);
                 }
             }
         }
@@ -417,7 +496,7 @@ template <class L>
 int op_equilibrium(mplb_gpu* h, int fi) {
     if (h->model[fi] == MPLB_NO_MODEL || !(fi == 0 ? h->P.f_update : h->P.g_update)) return 0;
     if (fi == 0) LAUNCH(k_equilibrium_flow<L>, blocks(h->n), h->P, h->F(), h->rho, h->U);
-    else LAUNCH(k_equilibrium_heat, blocks(h->n), h->P, h->G(), h->T, h->U);
+    else LAUNCH(k_equilibrium_heat<L>, blocks(h->n), h->P, h->G(), h->T, h->U);
     return 0;
 }
 
@@ -425,7 +504,7 @@ template <class L>
 int op_collision(mplb_gpu* h, int fi) {
     if (h->model[fi] == MPLB_NO_MODEL || !(fi == 0 ? h->P.f_update : h->P.g_update)) return 0;
     if (fi == 0) LAUNCH(k_collide_flow<L>, blocks(h->n), h->P, h->F(), h->rho, h->U, h->T, h->Fi, h->Ft, h->nb);
-    else LAUNCH(k_collide_heat, blocks(h->n), h->P, h->G(), h->T, h->U, h->S);
+    else LAUNCH(k_collide_heat<L>, blocks(h->n), h->P, h->G(), h->T, h->U, h->S);
     return 0;
 }
 
@@ -450,16 +529,23 @@ int op_boundaries(mplb_gpu* h, int fi) {
         any = true;
     }
     if (!any) return 0;
+    // fixedRandomT: the first psteps - localTStep updates are perturbed
+    // (fixedRandomT.c:79,117); one update per call, as updateBoundaries
+    unsigned long long rnd = 0;
+    for (size_t p = 0; p < pts.size(); p++)
+        if (pts[p].type == MPLB_BC_FIXEDRANDOMT && (int64_t)h->bc_calls[fi] < h->rnd_left[fi][p]) rnd |= 1ull << p;
+    h->bc_calls[fi]++;
     if (h->serial[fi]) {
         LAUNCH(k_bc_serial<L>, 1, h->P, h->dpatches + fi * pts.size(), (int)pts.size(), h->model[fi],
-               h->pnodes, pdf, h->nb, h->rho, h->T, h->U, h->Fi);
+               h->pnodes, pdf, h->nb, h->rho, h->T, h->U, h->Fi, h->bctab[fi], rnd);
         return 0;
     }
-    for (const PatchDev& pt : pts) {
+    for (size_t p = 0; p < pts.size(); p++) {
+        const PatchDev& pt = pts[p];
         if (pt.type == MPLB_BC_PERIODIC || pt.count == 0) continue;
         if (pt.type == MPLB_BC_FIXEDU && h->model[fi] != MPLB_LIMRT) continue;
         LAUNCH(k_bc_patch<L>, blocks(pt.count), h->P, pt, h->model[fi], h->pnodes, pdf, h->nb, h->rho,
-               h->T, h->U, h->Fi);
+               h->T, h->U, h->Fi, h->bctab[fi], (int)((rnd >> p) & 1ull));
     }
     return 0;
 }
@@ -474,7 +560,8 @@ int op_density(mplb_gpu* h, uint32_t s, uint32_t e) {
 template <class L>
 int op_temperature(mplb_gpu* h, uint32_t s, uint32_t e) {
     if (h->model[1] == MPLB_NO_MODEL || !h->P.g_update || e <= s) return 0;
-    LAUNCH(k_moment0<L::Q>, blocks(e - s), h->n, h->T, h->G(), s, e);
+    if (h->model[1] == MPLB_MYMRT) LAUNCH(k_temperature_my<L::Q>, blocks(e - s), h->n, h->T, h->G(), h->S, s, e);
+    else LAUNCH(k_moment0<L::Q>, blocks(e - s), h->n, h->T, h->G(), s, e);
     return 0;
 }
 
@@ -813,6 +900,22 @@ int mplb_gpu_create(const mplb_mesh_desc* mesh, const mplb_eos_desc* eos, const 
         P.corr3 = (1 - g->Lambda[3] / 2) * g->Lambda[4];
         P.corr5 = (1 - g->Lambda[5] / 2) * g->Lambda[6];
         P.lam_fac = (1 / g->Lambda[3] - 0.5);
+        if (g->model == MPLB_MYMRT) {
+            // myMRTCollision.c:47-140 and heatSource.c:36-48, evaluated as there
+            P.my_a1 = g->alpha_1;
+            P.my_a2 = g->alpha_2;
+            P.my_qo[0] = g->Lambda[4] * (g->Lambda[3] / 2.0 - 1.0);
+            P.my_qo[1] = g->Lambda[6] * (g->Lambda[5] / 2.0 - 1.0);
+            P.my_qo[2] = h->lat == MPLB_D3Q15 ? g->Lambda[8] * (g->Lambda[7] / 2.0 - 1.0) : 0.0;
+            P.my_qa0 = 1.0 + -0.5 * g->Lambda[0];
+            if (h->lat == MPLB_D2Q9) {
+                P.my_lgeo = 4.0 + 3.0 * g->alpha_1 + 2.0 * g->alpha_2;
+                P.my_ldiv = 6.0;
+            } else {
+                P.my_lgeo = 6.0 + 11.0 * g->alpha_1 + g->alpha_2;
+                P.my_ldiv = 9.0;
+            }
+        }
     }
     P.eos = eos->type;
     P.a = eos->a;
@@ -851,6 +954,55 @@ int mplb_gpu_create(const mplb_mesh_desc* mesh, const mplb_eos_desc* eos, const 
             off += mesh->patch_count[p];
         }
     }
+    // outflow normals and fixedRandomT wall temperatures, per field
+    std::vector<double> tabs[2];
+    const int32_t rank = opts ? opts->rank : 0;
+    for (int fi = 0; fi < 2; fi++) {
+        h->rnd_left[fi].assign(mesh->n_patches, 0);
+        if (!fds[fi] || fds[fi]->model == MPLB_NO_MODEL || !fds[fi]->update) continue;
+        for (uint32_t p = 0; p < mesh->n_patches; p++) {
+            const int t = h->bct[fi][p];
+            if (t != MPLB_BC_OUTFLOW && t != MPLB_BC_FIXEDRANDOMT) continue;
+            if (tabs[fi].empty()) tabs[fi].assign(std::max<size_t>(tot, 1) * Q, 0.0);
+            const PatchDev& pt = h->fpatch[fi][p];
+            if (t == MPLB_BC_OUTFLOW) {
+                for (uint32_t i = 0; i < pt.count; i++) {
+                    const uint32_t id = mesh->patch_nodes[pt.off + i];
+                    float nrm[3];
+                    int ln;
+                    if (!outflow_normal(Q, mesh->nb + (size_t)id * Q, nrm, &ln)) {
+                        if (h->own_stream) cudaStreamDestroy(h->stream);
+                        delete h;
+                        return fail(MPLB_E_ARG, "Unable to detect normal in outflow boundary (node " +
+                                                    std::to_string(id) + ", outflow.c:67-71)");
+                    }
+                    double* row = tabs[fi].data() + (size_t)(pt.off + i) * Q;
+                    for (int j = 0; j < 3; j++) row[j] = (double)nrm[j];
+                    row[3] = ln;
+                }
+            } else {
+                // fixedRandomT.c:37-41,79-85: srand(pid) at every call, so
+                // every perturbed update draws the same sequence, one value
+                // per (node, missing direction with an inner neighbour)
+                const double T0 = pt.val[0], pc = pt.val[1];
+                const double minT = T0 * (100.0 - pc) / 100.0, maxT = T0 * (100.0 + pc) / 100.0;
+                h->rnd_left[fi][p] = (int64_t)pt.val[2];
+                GnuRand rng((uint32_t)rank);
+                for (uint32_t i = 0; i < pt.count; i++) {
+                    const uint32_t id = mesh->patch_nodes[pt.off + i];
+                    const int32_t* nbi = mesh->nb + (size_t)id * Q;
+                    double* row = tabs[fi].data() + (size_t)(pt.off + i) * Q;
+                    for (int k = 0; k < Q; k++) {
+                        if (nbi[k] != -1) continue;
+                        const int r = Q == 9 ? revk<D2Q9T>(k) : revk<D3Q15T>(k);
+                        if (nbi[r] == -1) continue;
+                        const double u = (double)rng.next() / 2147483647;
+                        row[k] = minT + (maxT - minT) * u;
+                    }
+                }
+            }
+        }
+    }
     for (int fi = 0; fi < 2; fi++) h->serial[fi] = needs_serial(h, mesh, fi);
     h->box = detect_box(h, mesh);
 
@@ -872,6 +1024,13 @@ int mplb_gpu_create(const mplb_mesh_desc* mesh, const mplb_eos_desc* eos, const 
     for (int fi = 0; fi < 2; fi++) {
         if (h->model[fi] == MPLB_NO_MODEL) continue;
         if ((rc = dalloc(h, &h->pdf[fi][0], nq)) || (rc = dalloc(h, &h->pdf[fi][1], nq))) return bail(rc);
+    }
+    for (int fi = 0; fi < 2; fi++) {
+        if (tabs[fi].empty()) continue;
+        if ((rc = dalloc(h, &h->bctab[fi], tabs[fi].size()))) return bail(rc);
+        if (cudaMemcpy(h->bctab[fi], tabs[fi].data(), tabs[fi].size() * sizeof(double), cudaMemcpyHostToDevice) !=
+            cudaSuccess)
+            return bail(fail(MPLB_E_CUDA, "copying the boundary tables failed"));
     }
     {
         // neighbour table to [k][n], boundary flags

@@ -30,15 +30,21 @@ __global__ void k_equilibrium_flow(Params P, double* __restrict__ f, const doubl
     static_for<L::Q>([&](auto k) { f[(size_t)k * n + id] = eq_flow_k<L>(P, k, r, v); });
 }
 
-// general/equilibrium.c:49-55 (liTempMRT)
-static __global__ void k_equilibrium_heat(Params P, double* __restrict__ g, const double* __restrict__ T,
+// general/equilibrium.c:37-55 (myMRT, liTempMRT)
+template <class L>
+__global__ void k_equilibrium_heat(Params P, double* __restrict__ g, const double* __restrict__ T,
                                    const double* __restrict__ U) {
     uint32_t n = P.n, id = blockIdx.x * blockDim.x + threadIdx.x;
     if (id >= n) return;
-    double v[9];
-    eq_heat(P, T[id], U[id], U[n + id], v);
+    double v[L::Q];
+    if (P.g_model == MPLB_MYMRT) {
+        const double u[3] = {U[id], U[n + id], U[2 * n + id]};
+        eq_mymrt<L>(P, T[id], u, v);
+    } else {
+        if constexpr (L::Q == 9) eq_heat(P, T[id], U[id], U[n + id], v);
+    }
 #pragma unroll
-    for (int k = 0; k < 9; k++) g[(size_t)k * n + id] = v[k];
+    for (int k = 0; k < L::Q; k++) g[(size_t)k * n + id] = v[k];
 }
 
 // --------------------------------------------------------------- collision
@@ -86,17 +92,23 @@ __global__ void k_collide_flow(Params P, double* __restrict__ f, const double* _
     for (int k = 0; k < L::Q; k++) f[(size_t)k * n + id] = v[k];
 }
 
-// liTempMRTCollision.c:31-87 over all nodes.
-static __global__ void k_collide_heat(Params P, double* __restrict__ g, const double* __restrict__ T,
+// liTempMRTCollision.c:31-87 / myMRTCollision.c:141-212 over all nodes.
+template <class L>
+__global__ void k_collide_heat(Params P, double* __restrict__ g, const double* __restrict__ T,
                                const double* __restrict__ U, const double* __restrict__ S) {
     uint32_t n = P.n, id = blockIdx.x * blockDim.x + threadIdx.x;
     if (id >= n) return;
-    double v[9];
+    double v[L::Q];
 #pragma unroll
-    for (int k = 0; k < 9; k++) v[k] = g[(size_t)k * n + id];
-    collide_litemp(P, v, T[id], U[id], U[n + id], S[id]);
+    for (int k = 0; k < L::Q; k++) v[k] = g[(size_t)k * n + id];
+    if (P.g_model == MPLB_MYMRT) {
+        const double u[3] = {U[id], U[n + id], U[2 * n + id]};
+        collide_mymrt<L>(P, v, T[id], u, S[id]);
+    } else {
+        if constexpr (L::Q == 9) collide_litemp(P, v, T[id], U[id], U[n + id], S[id]);
+    }
 #pragma unroll
-    for (int k = 0; k < 9; k++) g[(size_t)k * n + id] = v[k];
+    for (int k = 0; k < L::Q; k++) g[(size_t)k * n + id] = v[k];
 }
 
 // --------------------------------------------------------------- streaming
@@ -125,6 +137,18 @@ __global__ void k_moment0(uint32_t n, double* __restrict__ out, const double* __
 #pragma unroll
     for (int k = 0; k < Q; k++) s += pdf[(size_t)k * n + id];
     out[id] = s;
+}
+
+// myMRTTemperature.c:5-37: sum over k ascending plus half the source.
+template <int Q>
+__global__ void k_temperature_my(uint32_t n, double* __restrict__ T, const double* __restrict__ g,
+                                 const double* __restrict__ S, uint32_t start, uint32_t end) {
+    uint32_t id = start + blockIdx.x * blockDim.x + threadIdx.x;
+    if (id >= end) return;
+    double s = 0;
+#pragma unroll
+    for (int k = 0; k < Q; k++) s += g[(size_t)k * n + id];
+    T[id] = s + 0.5 * S[id];
 }
 
 // liMRTVelocity.c:6-55 (F = Ft) and xuMRTVelocity.c:6-55 (F = Fi + (rho - rho_0) g).
@@ -201,7 +225,7 @@ __device__ __forceinline__ FD fd_pair(int32_t a, int32_t b, double fa, double fb
     return {0.0, false};
 }
 
-// general/heatSource.c:96-166 (liTempMRT): uses rho (new), T and U (old).
+// general/heatSource.c:28-166 (myMRT, liTempMRT): uses rho (new), T and U (old).
 template <class L>
 __global__ void k_heatsource(Params P, double* __restrict__ S, const double* __restrict__ rho,
                              const double* __restrict__ T, const double* __restrict__ U,
@@ -223,8 +247,12 @@ __global__ void k_heatsource(Params P, double* __restrict__ S, const double* __r
     double dot = 0;
 #pragma unroll
     for (int k = 0; k < 3; k++) dot += gT[k] * gR[k];
-    double old = first ? 0.0 : S[id];
-    S[id] = heat_source_value(P, r, t, dot, div, old);
+    if (P.g_model == MPLB_MYMRT) {
+        S[id] = heat_source_value_my(P, r, t, dot, div);
+    } else {
+        double old = first ? 0.0 : S[id];
+        S[id] = heat_source_value(P, r, t, dot, div, old);
+    }
 }
 
 // ---------------------------------------------------------------- pressure
@@ -287,13 +315,29 @@ __device__ __forceinline__ double eq_heat_k(const Params& P, int k, double T, do
     return s;
 }
 
+// myMRTEquilibrium row k (fixedT.c:59-61,93-95, fixedRandomT.c:72-91).
+template <class L>
+__device__ __forceinline__ double eq_my_k(const Params& P, int k, double T, const double* u) {
+    double ne[L::Q];
+    neq_mymrt<L>(P, T, u, ne);
+    double s = 0;
+#pragma unroll
+    for (int j = 0; j < L::Q; j++)
+        if (Mint<L>(j, k) != 0) s = s + P.Mi[k][j] * ne[j];
+    return s;
+}
+
 // One boundary node of one patch, in place (bounceBack.c:14-72,
-// fixedT.c:110-206, fixedU.c:31-131).  Remote reads go through pdf.
+// fixedT.c:33-134, fixedU.c:31-131, outflow.c:24-185, fixedRandomT.c:46-115).
+// Remote reads go through pdf.  tab + slot*Q holds the node's host-made
+// table: outflow [0..2] the normal, [3] the normal direction's index;
+// fixedRandomT the perturbed wall temperature per direction, used while rnd.
 template <class L>
 __device__ void bc_node(const Params& P, const PatchDev& pt, int model, uint32_t id,
                         double* __restrict__ pdf, const int32_t* __restrict__ nb,
                         const double* __restrict__ rho, const double* __restrict__ T,
-                        const double* __restrict__ U, const double* __restrict__ Fi) {
+                        const double* __restrict__ U, const double* __restrict__ Fi,
+                        const double* __restrict__ tab, uint32_t slot, bool rnd) {
     const uint32_t n = P.n;
     if (pt.type == MPLB_BC_BOUNCEBACK) {
         double v[L::Q];
@@ -320,10 +364,51 @@ __device__ void bc_node(const Params& P, const PatchDev& pt, int model, uint32_t
             if (nb[(size_t)k * n + id] != -1) continue;
             int32_t m = nb[(size_t)revk<L>(k) * n + id];
             if (m == -1) continue;
-            double u0 = U[m], u1 = U[n + m];
-            double eq_nb = eq_heat_k(P, k, T[m], u0, u1);
-            double eq_bnd = eq_heat_k(P, k, pt.val[0], u0, u1);
+            double eq_nb, eq_bnd;
+            if (model == MPLB_MYMRT) {
+                const double u[3] = {U[m], U[n + m], U[2 * n + m]};
+                eq_nb = eq_my_k<L>(P, k, T[m], u);
+                eq_bnd = eq_my_k<L>(P, k, pt.val[0], u);
+            } else {
+                double u0 = U[m], u1 = U[n + m];
+                eq_nb = eq_heat_k(P, k, T[m], u0, u1);
+                eq_bnd = eq_heat_k(P, k, pt.val[0], u0, u1);
+            }
             pdf[(size_t)k * n + id] = eq_bnd + (pdf[(size_t)k * n + m] - eq_nb);
+        }
+    } else if (pt.type == MPLB_BC_FIXEDRANDOMT) {
+        for (int k = 0; k < L::Q; k++) {
+            if (nb[(size_t)k * n + id] != -1) continue;
+            int32_t m = nb[(size_t)revk<L>(k) * n + id];
+            if (m == -1) continue;
+            const double u[3] = {U[m], U[n + m], U[2 * n + m]};
+            const double eq_nb = eq_my_k<L>(P, k, T[m], u);
+            const double Tb = rnd ? tab[(size_t)slot * L::Q + k] : pt.val[0];
+            const double eq_bnd = eq_my_k<L>(P, k, Tb, u);
+            pdf[(size_t)k * n + id] = eq_bnd + (pdf[(size_t)k * n + m] - eq_nb);
+        }
+    } else if (pt.type == MPLB_BC_OUTFLOW) {
+        const double* t = tab + (size_t)slot * L::Q;
+        const int32_t nbm = nb[(size_t)(int)t[3] * n + id];
+        if (nbm != -1) {
+            const uint32_t m = (uint32_t)nbm;
+            double F[3], v[3] = {0, 0, 0}, nbrho = 0;
+#pragma unroll
+            for (int j = 0; j < 3; j++) F[j] = Fi[(size_t)j * n + m] + (rho[m] - P.rho_0) * P.g[j];
+#pragma unroll
+            for (int j = 0; j < 3; j++)
+#pragma unroll
+                for (int q = 0; q < L::Q; q++) v[j] += ck<L>(q, j) * pdf[(size_t)q * n + m];
+#pragma unroll
+            for (int q = 0; q < L::Q; q++) nbrho += pdf[(size_t)q * n + m];
+#pragma unroll
+            for (int j = 0; j < 3; j++) v[j] = (v[j] + F[j] * 0.5) / nbrho;
+            double uadv = 0;
+#pragma unroll
+            for (int j = 0; j < 3; j++) uadv += t[j] * v[j];
+            for (int k = 0; k < L::Q; k++)
+                if (nb[(size_t)k * n + id] == -1)
+                    pdf[(size_t)k * n + id] = (pdf[(size_t)k * n + id] + uadv * pdf[(size_t)k * n + m]) / (1 + uadv);
         }
     } else if (pt.type == MPLB_BC_FIXEDU && model == MPLB_LIMRT) {
         for (int k = 0; k < L::Q; k++) {
@@ -354,10 +439,11 @@ template <class L>
 __global__ void k_bc_patch(Params P, PatchDev pt, int model, const uint32_t* __restrict__ nodes,
                            double* __restrict__ pdf, const int32_t* __restrict__ nb,
                            const double* __restrict__ rho, const double* __restrict__ T,
-                           const double* __restrict__ U, const double* __restrict__ Fi) {
+                           const double* __restrict__ U, const double* __restrict__ Fi,
+                           const double* __restrict__ tab, int rnd) {
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= pt.count) return;
-    bc_node<L>(P, pt, model, nodes[pt.off + i], pdf, nb, rho, T, U, Fi);
+    bc_node<L>(P, pt, model, nodes[pt.off + i], pdf, nb, rho, T, U, Fi, tab, pt.off + i, rnd != 0);
 }
 
 // All patches in file order, one node after another: the reference's exact
@@ -368,12 +454,14 @@ __global__ void k_bc_serial(Params P, const PatchDev* __restrict__ pts, int npat
                             const uint32_t* __restrict__ nodes, double* __restrict__ pdf,
                             const int32_t* __restrict__ nb, const double* __restrict__ rho,
                             const double* __restrict__ T, const double* __restrict__ U,
-                            const double* __restrict__ Fi) {
+                            const double* __restrict__ Fi, const double* __restrict__ tab,
+                            unsigned long long rnd_mask) {
     if (blockIdx.x != 0 || threadIdx.x != 0) return;
     for (int p = 0; p < npatch; p++) {
         PatchDev pt = pts[p];
+        const bool rnd = (rnd_mask >> p) & 1ull;
         for (uint32_t i = 0; i < pt.count; i++)
-            bc_node<L>(P, pt, model, nodes[pt.off + i], pdf, nb, rho, T, U, Fi);
+            bc_node<L>(P, pt, model, nodes[pt.off + i], pdf, nb, rho, T, U, Fi, tab, pt.off + i, rnd);
     }
 }
 

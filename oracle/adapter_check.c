@@ -57,6 +57,19 @@ int adapter_pack_check(ref_case* c) {
     if (f->model == liMRT)
         for (int k = 0; k < 9; k++)
             if (d.field[0].Lambda[k] != f->lbparam.liMRT.Lambda[k]) bad |= 256;
+    if (g->model == myMRT) {
+        if (d.field[1].alpha_1 != g->lbparam.myMRT.alpha_1 || d.field[1].alpha_2 != g->lbparam.myMRT.alpha_2) bad |= 512;
+        for (int k = 0; k < m->lattice.Q; k++)
+            if (d.field[1].Lambda[k] != g->lbparam.myMRT.Lambda[k]) bad |= 512;
+    }
+    for (int w = 0; w < 2; w++)
+        for (uint32_t p = 0; p < m->mesh.bd.nbd; p++)
+            if (fl[w]->boundary[p].type == frdt &&
+                (d.field[w].bc_value[3 * p] != fl[w]->boundary[p].param.frdt.T ||
+                 d.field[w].bc_value[3 * p + 1] != fl[w]->boundary[p].param.frdt.p ||
+                 d.field[w].bc_value[3 * p + 2] != (double)(fl[w]->boundary[p].param.frdt.psteps -
+                                                            fl[w]->boundary[p].param.frdt.localTStep)))
+                bad |= 1024;
     mplb_ref_free(&d);
     return bad;
 }

@@ -43,6 +43,8 @@ typedef struct orc {
     double *rho, *T, *U, *Fi, *Ft, *S, *p; /* U/Fi/Ft: [n][3] */
     double *pdf[2], *swap;             /* [n][Q] */
     uint32_t current;
+    int32_t rank;                      /* parallel.pid (fixedRandomT's srand seed) */
+    int64_t frdt_step[2][MPLB_MAX_PATCHES];  /* fixedRandomT localTStep per field and patch */
     /* lattice tables */
     int c[MPLB_MAX_Q][3];
     int rev[MPLB_MAX_Q];
@@ -196,6 +198,30 @@ static void eq_heat(const orc* o, double T, const double* U, double* g) {
     n[6] = T * (-U[1]);
     n[7] = 0;
     n[8] = 0;
+    matvec(o, o->Mi, n, g);
+}
+
+/* myMRTEquilibrium.c:5-95: moments T, a1 T, a2 T, T U_x, T (-U_x), T U_y,
+ * T (-U_y) [, T U_z, -(T U_z)], zeros; then M^-1. */
+static void neq_my(const orc* o, double T, const double* U, double* n) {
+    const mplb_field_desc* d = &o->fd[1];
+    for (int k = 0; k < MPLB_MAX_Q; k++) n[k] = 0;
+    n[0] = T;
+    n[1] = d->alpha_1 * T;
+    n[2] = d->alpha_2 * T;
+    n[3] = T * U[0];
+    n[4] = T * (-U[0]);
+    n[5] = T * U[1];
+    n[6] = T * (-U[1]);
+    if (o->lat == MPLB_D3Q15) {
+        n[7] = T * U[2];
+        n[8] = -(T * U[2]);
+    }
+}
+
+static void eq_my(const orc* o, double T, const double* U, double* g) {
+    double n[MPLB_MAX_Q];
+    neq_my(o, T, U, n);
     matvec(o, o->Mi, n, g);
 }
 
@@ -368,6 +394,45 @@ static void collide_litemp(orc* o) {
     }
 }
 
+/* sparseMatVecMult.c:4-28: diagonal products, then the listed pairs added. */
+static void sparse_mv(int Q, const double (*A)[MPLB_MAX_Q], const double* v, double* r, const int (*nz)[2],
+                      int nnz) {
+    for (int i = 0; i < Q; i++) r[i] = A[i][i] * v[i];
+    for (int i = 0; i < nnz; i++) r[nz[i][0]] = r[nz[i][0]] + A[nz[i][0]][nz[i][1]] * v[nz[i][1]];
+}
+
+/* myMRTCollision.c:8-260: Q = diag(Lambda) with Q[3][4], Q[5][6] (and
+ * Q[7][8] on D3Q15) = Q[j+1][j+1] (Q[j][j]/2 - 1); n = M g; n <- n -
+ * Q (n - n_eq) + (I - Q/2) Gamma with Gamma = (S, 0, ...); g = M^-1 n. */
+static void collide_my(orc* o) {
+    const double* L = o->fd[1].Lambda;
+    const int Q = o->Q;
+    static const int nz[3][2] = {{3, 4}, {5, 6}, {7, 8}};
+    const int nnz = o->lat == MPLB_D2Q9 ? 2 : 3;
+    double A[MPLB_MAX_Q][MPLB_MAX_Q], B[MPLB_MAX_Q][MPLB_MAX_Q];
+    memset(A, 0, sizeof A);
+    for (int k = 0; k < Q; k++) A[k][k] = L[k];
+    for (int i = 0; i < nnz; i++) A[nz[i][0]][nz[i][1]] = A[nz[i][1]][nz[i][1]] * (A[nz[i][0]][nz[i][0]] / 2.0 - 1.0);
+    for (int j = 0; j < Q; j++)
+        for (int k = 0; k < Q; k++) {
+            B[j][k] = -0.5 * A[j][k];
+            if (j == k) B[j][k] = 1.0 + B[j][k];
+        }
+    for (uint32_t id = 0; id < o->n; id++) {
+        double ne[MPLB_MAX_Q], n[MPLB_MAX_Q], G[MPLB_MAX_Q], a1[MPLB_MAX_Q], a2[MPLB_MAX_Q];
+        neq_my(o, o->T[id], o->U + 3 * (size_t)id, ne);
+        double* g = o->pdf[1] + (size_t)Q * id;
+        matvec(o, o->M, g, n);
+        for (int k = 0; k < Q; k++) G[k] = 0;
+        G[0] = o->S[id];
+        for (int k = 0; k < Q; k++) a2[k] = n[k] - ne[k];
+        sparse_mv(Q, (const double (*)[MPLB_MAX_Q])A, a2, a1, nz, nnz);
+        sparse_mv(Q, (const double (*)[MPLB_MAX_Q])B, G, a2, nz, nnz);
+        for (int k = 0; k < Q; k++) n[k] = n[k] - a1[k] + a2[k];
+        matvec(o, o->Mi, n, g);
+    }
+}
+
 /* general/collision.c:6-67 */
 static int op_collision(orc* o, int fi) {
     if (!o->fd[fi].update) return 0;
@@ -375,6 +440,7 @@ static int op_collision(orc* o, int fi) {
     case MPLB_LIMRT: if (fi != 0) return -1; collide_limrt(o); return 0;
     case MPLB_XUMRT: if (fi != 0) return -1; collide_xumrt(o); return 0;
     case MPLB_LITEMPMRT: if (fi != 1) return -1; collide_litemp(o); return 0;
+    case MPLB_MYMRT: if (fi != 1) return -1; collide_my(o); return 0;
     default: return -1;
     }
 }
@@ -411,7 +477,7 @@ static void bc_bounceback(orc* o, double* v, uint32_t p) {
     }
 }
 
-/* boundary/fixedT/fixedT.c:15-142 with liTempMRTEquilibrium. */
+/* boundary/fixedT/fixedT.c:15-142 with liTempMRTEquilibrium or myMRTEquilibrium. */
 static void bc_fixedt(orc* o, double* v, uint32_t p, double Tw) {
     int Q = o->Q;
     double fn[MPLB_MAX_Q], fb[MPLB_MAX_Q];
@@ -422,9 +488,14 @@ static void bc_fixedt(orc* o, double* v, uint32_t p, double Tw) {
             if (nb[k] != -1) continue;
             int nbid = nb[o->rev[k]];
             if (nbid == -1) continue;
-            eq_heat(o, o->T[nbid], o->U + 3 * (size_t)nbid, fn);
+            if (o->fd[1].model == MPLB_MYMRT) {
+                eq_my(o, o->T[nbid], o->U + 3 * (size_t)nbid, fn);
+                eq_my(o, Tw, o->U + 3 * (size_t)nbid, fb);
+            } else {
+                eq_heat(o, o->T[nbid], o->U + 3 * (size_t)nbid, fn);
+                eq_heat(o, Tw, o->U + 3 * (size_t)nbid, fb);
+            }
             double eq_nb = fn[k];
-            eq_heat(o, Tw, o->U + 3 * (size_t)nbid, fb);
             double eq_bnd = fb[k];
             v[(size_t)id * Q + k] = eq_bnd + (v[(size_t)nbid * Q + k] - eq_nb);
         }
@@ -457,6 +528,107 @@ static void bc_fixedu(orc* o, double* v, uint32_t p, const double* Uw) {
     }
 }
 
+/* rand() of the GNU C library after srand(seed) (fixedRandomT.c:37,81),
+ * restated from its published description (P. Selinger, "The GLIBC
+ * pseudo-random number generator", 2007): r_0 = seed (0 -> 1), r_i = 16807
+ * r_{i-1} mod (2^31 - 1) for i < 31, r_i = r_{i-31} for i = 31..33, then
+ * r_i = r_{i-3} + r_{i-31} mod 2^32; the k-th output is r_{k+344} >> 1. */
+typedef struct { uint32_t r[34]; uint64_t i; } gnu_rand;  /* the last 34 words, r_i at r[i % 34] */
+
+static int gnu_rand_step(gnu_rand* g) {
+    uint32_t v = g->r[(g->i - 31) % 34] + g->r[(g->i - 3) % 34];
+    g->r[g->i % 34] = v;
+    g->i++;
+    return (int)(v >> 1);
+}
+
+static void gnu_srand(gnu_rand* g, uint32_t seed) {
+    int64_t w = seed == 0 ? 1 : seed;
+    g->r[0] = (uint32_t)w;
+    for (int i = 1; i < 31; i++) {
+        w = (16807 * w) % 2147483647;
+        g->r[i] = (uint32_t)w;
+    }
+    for (int i = 31; i < 34; i++) g->r[i] = g->r[i - 31];
+    g->i = 34;
+    for (int i = 34; i < 344; i++) gnu_rand_step(g);
+}
+
+static int gnu_rand_next(gnu_rand* g) { return gnu_rand_step(g); }
+
+/* boundary/fixedRandomT/fixedRandomT.c:15-125 (myMRT): while localTStep <
+ * psteps the wall temperature of each (node, missing direction) is drawn
+ * uniformly in T (1 -+ p/100), with srand(pid) at every call. */
+static void bc_fixedrandomt(orc* o, double* v, uint32_t p, const double* bcv, int64_t* local_step) {
+    int Q = o->Q;
+    double fn[MPLB_MAX_Q], fb[MPLB_MAX_Q];
+    static gnu_rand g;
+    gnu_srand(&g, (uint32_t)o->rank);
+    double T0 = bcv[0], pc = bcv[1];
+    double minT = T0 * (100.0 - pc) / 100.0;
+    double maxT = T0 * (100.0 + pc) / 100.0;
+    int64_t psteps = (int64_t)bcv[2];
+    for (uint32_t i = 0; i < o->pcount[p]; i++) {
+        uint32_t id = o->pnodes[o->poff[p] + i];
+        const int32_t* nb = o->nb + (size_t)id * Q;
+        for (int k = 0; k < Q; k++) {
+            if (nb[k] != -1) continue;
+            int nbid = nb[o->rev[k]];
+            if (nbid == -1) continue;
+            eq_my(o, o->T[nbid], o->U + 3 * (size_t)nbid, fn);
+            double eq_nb = fn[k];
+            if (*local_step < psteps) {
+                double r = (double)gnu_rand_next(&g) / 2147483647;
+                double Tb = minT + (maxT - minT) * r;
+                eq_my(o, Tb, o->U + 3 * (size_t)nbid, fb);
+            } else {
+                eq_my(o, T0, o->U + 3 * (size_t)nbid, fb);
+            }
+            v[(size_t)id * Q + k] = fb[k] + (v[(size_t)nbid * Q + k] - eq_nb);
+        }
+    }
+    (*local_step)++;
+}
+
+/* boundary/outflow/outflow.c:12-208: the normal is the sum of the velocities
+ * whose node x + c_k is missing, normalised in float; ln the last direction
+ * equal to its (int) truncation; the unknown populations are advected from
+ * the inner neighbour nb[id][ln] with its normal velocity (force-corrected,
+ * from the previous step's Fi and rho). */
+static int bc_outflow(orc* o, double* v, uint32_t p) {
+    int Q = o->Q;
+    for (uint32_t i = 0; i < o->pcount[p]; i++) {
+        uint32_t id = o->pnodes[o->poff[p] + i];
+        const int32_t* nb = o->nb + (size_t)id * Q;
+        float normal[3] = {0, 0, 0};
+        for (int k = 0; k < Q; k++)
+            if (nb[o->rev[k]] == -1)
+                for (int j = 0; j < 3; j++) normal[j] += o->c[k][j];
+        float nmag = 0;
+        for (int j = 0; j < 3; j++) nmag += normal[j] * normal[j];
+        if (nmag == 0) return -1;
+        nmag = sqrt(nmag);
+        for (int j = 0; j < 3; j++) normal[j] = normal[j] / nmag;
+        int ln = 0;
+        for (int k = 0; k < Q; k++)
+            if (o->c[k][0] == (int)normal[0] && o->c[k][1] == (int)normal[1] && o->c[k][2] == (int)normal[2]) ln = k;
+        int m = nb[ln];
+        if (m == -1) continue;
+        const double* fm = v + (size_t)m * Q;
+        double F[3], nbv[3] = {0, 0, 0}, nbrho = 0, uadv = 0;
+        for (int j = 0; j < 3; j++)
+            F[j] = o->Fi[3 * (size_t)m + j] + (o->rho[m] - o->eos.rho_0) * o->eos.g[j];
+        for (int j = 0; j < 3; j++)
+            for (int q = 0; q < Q; q++) nbv[j] += o->c[q][j] * fm[q];
+        for (int q = 0; q < Q; q++) nbrho += fm[q];
+        for (int j = 0; j < 3; j++) nbv[j] = (nbv[j] + F[j] * 0.5) / nbrho;
+        for (int j = 0; j < 3; j++) uadv += normal[j] * nbv[j];
+        for (int k = 0; k < Q; k++)
+            if (nb[k] == -1) v[(size_t)id * Q + k] = (v[(size_t)id * Q + k] + uadv * fm[k]) / (1 + uadv);
+    }
+    return 0;
+}
+
 /* general/updateBoundaries.c:6-75: patches in file order. */
 static int op_boundaries(orc* o, int fi) {
     if (!o->fd[fi].update) return 0;
@@ -466,8 +638,15 @@ static int op_boundaries(orc* o, int fi) {
         case MPLB_BC_PERIODIC: break;
         case MPLB_BC_BOUNCEBACK: bc_bounceback(o, o->pdf[fi], p); break;
         case MPLB_BC_FIXEDT:
-            if (o->fd[fi].model != MPLB_LITEMPMRT || o->lat != MPLB_D2Q9) return -1;
+            if (fi != 1 || (o->fd[fi].model != MPLB_LITEMPMRT && o->fd[fi].model != MPLB_MYMRT)) return -1;
             bc_fixedt(o, o->pdf[fi], p, o->bcv[fi][3 * p]);
+            break;
+        case MPLB_BC_FIXEDRANDOMT:
+            if (fi != 1 || o->fd[fi].model != MPLB_MYMRT) return -1;
+            bc_fixedrandomt(o, o->pdf[fi], p, o->bcv[fi] + 3 * p, &o->frdt_step[fi][p]);
+            break;
+        case MPLB_BC_OUTFLOW:
+            if (bc_outflow(o, o->pdf[fi], p)) return -1;
             break;
         case MPLB_BC_FIXEDU:
             if (o->fd[fi].model == MPLB_LIMRT) bc_fixedu(o, o->pdf[fi], p, o->bcv[fi] + 3 * p);
@@ -505,12 +684,13 @@ static void op_velocity(orc* o, uint32_t s, uint32_t e) {
     }
 }
 
-/* macroTemperature.c:7-68, liTempMRTTemperature.c:5-26 */
+/* macroTemperature.c:7-68, liTempMRTTemperature.c:5-26, myMRTTemperature.c:5-37 */
 static void op_temperature(orc* o, uint32_t s, uint32_t e) {
     if (!o->fd[1].update) return;
     for (uint32_t id = s; id < e; id++) {
         double T = 0;
         for (int k = 0; k < o->Q; k++) T += o->pdf[1][(size_t)id * o->Q + k];
+        if (o->fd[1].model == MPLB_MYMRT) T = T + 0.5 * o->S[id];  /* myMRTTemperature.c:22-31 */
         o->T[id] = T;
     }
 }
@@ -553,15 +733,20 @@ static double fd_diff(const orc* o, const double* fld, int stride, int comp, uin
 #undef VAL
 }
 
-/* general/heatSource.c:93-168 (liTempMRT branch) */
+/* general/heatSource.c:28-168 (myMRT and liTempMRT branches) */
 static int op_heatsource(orc* o) {
     if (!o->fd[1].update) return 0;
-    if (o->fd[1].model != MPLB_LITEMPMRT) return -1;
+    const int my = o->fd[1].model == MPLB_MYMRT;
+    if (o->fd[1].model != MPLB_LITEMPMRT && !my) return -1;
     const double* L = o->fd[1].Lambda;
+    const double a1 = o->fd[1].alpha_1, a2 = o->fd[1].alpha_2;
     double Cv = o->eos.Cv;
     int D = o->D;
     for (uint32_t id = 0; id < o->n; id++) {
-        double lambda = o->rho[id] * Cv * (1 / L[3] - 0.5);
+        double lambda;
+        if (!my) lambda = o->rho[id] * Cv * (1 / L[3] - 0.5);
+        else if (o->lat == MPLB_D2Q9) lambda = o->rho[id] * Cv * (1 / L[3] - 0.5) * (4.0 + 3.0 * a1 + 2.0 * a2) / 6.0;
+        else lambda = o->rho[id] * Cv * (1 / L[3] - 0.5) * (6.0 + 11.0 * a1 + a2) / 9.0;
         double gT[3] = {0, 0, 0}, gR[3] = {0, 0, 0}, div = 0, dot = 0;
         int pr;
         for (int d = 0; d < D; d++) {
@@ -574,9 +759,13 @@ static int op_heatsource(orc* o) {
         double T = o->T[id], rho = o->rho[id];
         double dpdT = p_eos(&o->eos, rho, 1.1 * T) - p_eos(&o->eos, rho, 0.9 * T);
         dpdT = dpdT / (0.2 * T);
-        double old = o->current == 0 ? 0 : o->S[id];
         double s = -lambda * dot / Cv + div * T * (1.0 - dpdT / (rho * Cv));
-        o->S[id] = s + 0.5 * (s - old);
+        if (my) {
+            o->S[id] = s;
+        } else {
+            double old = o->current == 0 ? 0 : o->S[id];
+            o->S[id] = s + 0.5 * (s - old);
+        }
     }
     return 0;
 }
@@ -643,6 +832,7 @@ static int op_equilibrium(orc* o, int fi) {
         case MPLB_LIMRT:
         case MPLB_XUMRT: eq_flow(o, o->rho[id], o->U + 3 * (size_t)id, v); break;
         case MPLB_LITEMPMRT: if (o->lat != MPLB_D2Q9) return -1; eq_heat(o, o->T[id], o->U + 3 * (size_t)id, v); break;
+        case MPLB_MYMRT: if (fi != 1) return -1; eq_my(o, o->T[id], o->U + 3 * (size_t)id, v); break;
         default: return -1;
         }
     }
@@ -735,6 +925,7 @@ int orc_download(orc* o, double* rho, double* U, double* T, double* Fi, double* 
 }
 
 void orc_set_time(orc* o, uint32_t t) { o->current = t; }
+void orc_set_rank(orc* o, int32_t pid) { o->rank = pid; }
 uint32_t orc_get_time(orc* o) { return o->current; }
 void orc_set_rho0(orc* o, double r) { o->eos.rho_0 = r; }
 

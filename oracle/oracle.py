@@ -60,6 +60,7 @@ def _lib(kind):
     fn("step").argtypes = [C.c_void_p, C.c_uint32]
     fn("op").argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_uint32, C.c_uint32]
     fn("set_time").argtypes = [C.c_void_p, C.c_uint32]
+    fn("set_rank").argtypes = [C.c_void_p, C.c_int32]
     fn("get_time").argtypes = [C.c_void_p]
     fn("get_time").restype = C.c_uint32
     fn("set_rho0").argtypes = [C.c_void_p, C.c_double]
@@ -76,7 +77,7 @@ def _lib(kind):
 class Checker:
     """One lattice held by a CPU checker."""
 
-    def __init__(self, kind, case, start_time=0):
+    def __init__(self, kind, case, start_time=0, rank=None):
         self.kind, self.case = kind, case
         self.lib = _lib(kind)
         self.p = PREFIX[kind]
@@ -85,6 +86,9 @@ class Checker:
                                    C.byref(self.desc.f), C.byref(self.desc.g), start_time)
         if not self.h:
             raise RuntimeError(f"{kind} checker rejected case {case.name}")
+        if rank is None:
+            rank = (getattr(case, "meta", None) or {}).get("rank", 0)
+        self._f("set_rank")(self.h, rank)
 
     def _f(self, name):
         return getattr(self.lib, self.p + name)

@@ -83,6 +83,11 @@ static void setup_field(ref_case* c, lbeField* fl, const mplb_field_desc* d) {
     case MPLB_LITEMPMRT:
         fl->lbparam.liTempMRT.Lambda = lam;
         break;
+    case MPLB_MYMRT:
+        fl->lbparam.myMRT.Lambda = lam;
+        fl->lbparam.myMRT.alpha_1 = d->alpha_1;
+        fl->lbparam.myMRT.alpha_2 = d->alpha_2;
+        break;
     default:
         fl->lbparam.liMRT.Lambda = lam;
         break;
@@ -95,6 +100,13 @@ static void setup_field(ref_case* c, lbeField* fl, const mplb_field_desc* d) {
             if (d->bc_type[p] == MPLB_BC_FIXEDT) fl->boundary[p].param.ft.T = d->bc_value[3 * p];
             if (d->bc_type[p] == MPLB_BC_FIXEDU)
                 for (int j = 0; j < 3; j++) fl->boundary[p].param.fu.U[j] = d->bc_value[3 * p + j];
+            if (d->bc_type[p] == MPLB_BC_FIXEDRANDOMT) {
+                /* readFixedRandomTParam.c:14-75: value, pert, duration */
+                fl->boundary[p].param.frdt.T = d->bc_value[3 * p];
+                fl->boundary[p].param.frdt.p = d->bc_value[3 * p + 1];
+                fl->boundary[p].param.frdt.psteps = (int)d->bc_value[3 * p + 2];
+                fl->boundary[p].param.frdt.localTStep = 0;
+            }
         }
     }
     fl->nreq = 0;
@@ -245,6 +257,7 @@ int ref_download(ref_case* c, double* rho, double* U, double* T, double* Fi, dou
 }
 
 void ref_set_time(ref_case* c, uint32_t t) { c->mesh.time.current = t; }
+void ref_set_rank(ref_case* c, int32_t pid) { c->mesh.parallel.pid = pid; }
 uint32_t ref_get_time(ref_case* c) { return c->mesh.time.current; }
 void ref_set_rho0(ref_case* c, double r) { c->mesh.EOS.rho_0 = r; }
 double ref_average_rho0(ref_case* c) {

@@ -24,7 +24,8 @@ from multiphaselb_b200 import cases  # noqa: E402
 from tests.helpers import FIELDS, run_checker, small_cases  # noqa: E402
 
 STEPS = {"bubble_d2q9": 12, "column_d2q9": 12, "lid_d2q9": 9, "bubble_d3q15": 5, "walls_d3q15": 5,
-         "st_d2q9": 10, "st_d3q15": 5}
+         "st_d2q9": 10, "st_d3q15": 5, "my_column_d2q9": 9, "my_walls_d3q15": 5, "outflow_d2q9": 8,
+         "outflow_corner_d2q9": 6, "outflow_d3q15": 5}
 
 
 def save_case(path, case, steps, out):
@@ -34,7 +35,7 @@ def save_case(path, case, steps, out):
                                                for k, v in case.f.items()},
                 g=None if case.g is None else {k: (np.asarray(v).tolist() if k in ("bc_value", "Lambda", "bc_type") else v)
                                                for k, v in case.g.items()},
-                steps=steps)
+                steps=steps, rank=int(case.meta.get("rank", 0)))
     arrs = {"in_" + k: getattr(case, k) for k in ("rho", "U", "T")}
     arrs.update({"out_" + k: out[k] for k in FIELDS if not (k == "g" and case.g is None)})
     np.savez_compressed(path, spec=np.frombuffer(json.dumps(spec).encode(), dtype=np.uint8), **arrs)
@@ -46,7 +47,8 @@ def load_case(path):
     nb, points, patches, names = cases.box_mesh(spec["lattice"], tuple(spec["dims"]), tuple(spec["periodic"]))
     eos = {k: (tuple(v) if isinstance(v, list) else v) for k, v in spec["eos"].items()}
     c = cases.Case(spec["name"], spec["lattice"], tuple(spec["dims"]), tuple(spec["periodic"]), nb, points,
-                   patches, names, eos, spec["f"], spec["g"], z["in_rho"], z["in_U"], z["in_T"])
+                   patches, names, eos, spec["f"], spec["g"], z["in_rho"], z["in_U"], z["in_T"],
+                   meta=dict(rank=spec.get("rank", 0)))
     want = {k[4:]: z[k] for k in z.files if k.startswith("out_")}
     return c, spec["steps"], want
 

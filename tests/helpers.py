@@ -18,7 +18,101 @@ def small_cases():
         "walls_d3q15": walled_d3q15(),
         "st_d2q9": surface_tension_d2q9(),
         "st_d3q15": surface_tension_d3q15(),
+        "my_column_d2q9": mymrt_column_d2q9(),
+        "my_walls_d3q15": mymrt_walls_d3q15(),
+        "outflow_d2q9": outflow_d2q9(),
+        "outflow_corner_d2q9": outflow_corner_d2q9(),
+        "outflow_d3q15": outflow_d3q15(),
     }
+
+
+LAMBDA_MY2 = [0.0, 1.1, 1.1, 0.9, 1.0, 0.9, 1.0, 1.0, 1.0]
+LAMBDA_MY3 = [0.0, 1.0, 1.0, 1.1, 1.0, 1.1, 1.0, 1.1, 1.0, 1.0, 1.0, 1.0, 1.0, 1.0, 1.0]
+
+
+def mymrt(lattice, bc_type, bc_value):
+    """A myMRT thermal field (myMRTCollision.c) with its own alpha constants."""
+    d3 = lattice == abi.D3Q15
+    return dict(model=abi.MYMRT, update=1, Lambda=LAMBDA_MY3 if d3 else LAMBDA_MY2,
+                alpha_1=0.25 if d3 else 1.0, alpha_2=0.25 if d3 else -1.0,
+                bc_type=bc_type, bc_value=np.asarray(bc_value, dtype=np.float64).reshape(-1, 3))
+
+
+def mymrt_column_d2q9():
+    """The thermal column with the myMRT thermal model instead of liTempMRT."""
+    c = cases.column_case(12, 24, amp=1e-3, width=3.0, name="my_column_d2q9_12x24")
+    c.g = mymrt(abi.D2Q9, [abi.BC_FIXEDT, abi.BC_FIXEDT], c.g["bc_value"])
+    return cases.perturbed(c, du=1e-3)
+
+
+def thermal_box(lattice, dims, periodic, T_noise=1e-3, seed=7):
+    c = cases.bubble_case(lattice, 8, 2.5, 2.0, 0.75, dims=dims)
+    nb, points, patches, names = cases.box_mesh(lattice, c.dims, periodic)
+    c.nb, c.points, c.patches, c.patch_names = nb, points, patches, names
+    c.periodic = tuple(periodic[:len(dims)])
+    rng = np.random.Generator(np.random.PCG64(seed))
+    c.T = c.T * (1.0 + T_noise * rng.uniform(-1.0, 1.0, size=c.n))
+    return c
+
+
+def mymrt_walls_d3q15():
+    """D3Q15 bubble between bounce-back x walls and fixedT z walls (hot
+    bottom, cold top), myMRT heat, gravity along -z."""
+    c = thermal_box(abi.D3Q15, (8, 6, 7), (False, True, False))
+    T0 = c.meta["T"]
+    bct = {"X0": abi.BC_BOUNCEBACK, "X1": abi.BC_BOUNCEBACK, "Z0": abi.BC_FIXEDT, "Z1": abi.BC_FIXEDT}
+    val = {"Z0": (1.02 * T0, 0, 0), "Z1": (0.98 * T0, 0, 0)}
+    names = c.patch_names
+    c.f = dict(c.f, bc_type=[abi.BC_BOUNCEBACK] * len(names), bc_value=np.zeros((len(names), 3)))
+    c.g = mymrt(abi.D3Q15, [bct[n] for n in names], [val.get(n, (0, 0, 0)) for n in names])
+    c.eos = dict(c.eos, g=(0.0, 0.0, -1e-5), rho_0=0.0)
+    c.name = "my_walls_d3q15_8x6x7"
+    return cases.perturbed(c, du=1e-3)
+
+
+def outflow_d2q9():
+    """Periodic-x D2Q9 channel: bounce-back bottom and outflow top for the
+    flow; fixedRandomT bottom (perturbed for 3 updates) and outflow top for
+    the myMRT heat; rank 3 seeds the perturbation."""
+    c = thermal_box(abi.D2Q9, (12, 14), (True, False))
+    T0 = c.meta["T"]
+    c.f = dict(c.f, bc_type=[abi.BC_BOUNCEBACK, abi.BC_OUTFLOW], bc_value=np.zeros((2, 3)))
+    c.g = mymrt(abi.D2Q9, [abi.BC_FIXEDRANDOMT, abi.BC_OUTFLOW], [(1.03 * T0, 5.0, 3.0), (0, 0, 0)])
+    c.eos = dict(c.eos, g=(0.0, -1e-5, 0.0), rho_0=0.0)
+    c.meta = dict(c.meta, rank=3)
+    c.name = "outflow_d2q9_12x14"
+    return cases.perturbed(c, du=2e-3)
+
+
+def outflow_corner_d2q9():
+    """Walls on all four sides: outflow on the +x and +y walls (their shared
+    corner has a diagonal normal, which truncates to the rest direction), a
+    fixedRandomT wall at the bottom (perturbed for 2 updates, rank 0) and a
+    fixedT wall at -x."""
+    c = thermal_box(abi.D2Q9, (10, 12), (False, False))
+    T0 = c.meta["T"]
+    bct_f = {"X0": abi.BC_BOUNCEBACK, "X1": abi.BC_OUTFLOW, "Y0": abi.BC_BOUNCEBACK, "Y1": abi.BC_OUTFLOW}
+    bct_g = {"X0": abi.BC_FIXEDT, "X1": abi.BC_OUTFLOW, "Y0": abi.BC_FIXEDRANDOMT, "Y1": abi.BC_OUTFLOW}
+    val_g = {"X0": (0.99 * T0, 0, 0), "Y0": (1.02 * T0, 10.0, 2.0)}
+    names = c.patch_names
+    c.f = dict(c.f, bc_type=[bct_f[n] for n in names], bc_value=np.zeros((len(names), 3)))
+    c.g = mymrt(abi.D2Q9, [bct_g[n] for n in names], [val_g.get(n, (0, 0, 0)) for n in names])
+    c.eos = dict(c.eos, g=(0.0, -1e-5, 0.0), rho_0=0.0)
+    c.name = "outflow_corner_d2q9_10x12"
+    return cases.perturbed(c, du=2e-3)
+
+
+def outflow_d3q15():
+    """D3Q15, periodic x and y: bounce-back bottom and outflow top for the
+    flow, fixedRandomT bottom and outflow top for the myMRT heat, rank 1."""
+    c = thermal_box(abi.D3Q15, (6, 5, 8), (True, True, False))
+    T0 = c.meta["T"]
+    c.f = dict(c.f, bc_type=[abi.BC_BOUNCEBACK, abi.BC_OUTFLOW], bc_value=np.zeros((2, 3)))
+    c.g = mymrt(abi.D3Q15, [abi.BC_FIXEDRANDOMT, abi.BC_OUTFLOW], [(1.02 * T0, 4.0, 2.0), (0, 0, 0)])
+    c.eos = dict(c.eos, g=(0.0, 0.0, -1e-5), rho_0=0.0)
+    c.meta = dict(c.meta, rank=1)
+    c.name = "outflow_d3q15_6x5x8"
+    return cases.perturbed(c, du=2e-3)
 
 
 def surface_tension_d2q9():

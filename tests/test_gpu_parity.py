@@ -38,7 +38,17 @@ def test_each_operator_matches_oracle(gpu_lib, name):
     k.initialize()
     k.step(2)
     state = k.download()
-    with Lattice(case, path=abi.PATH_OPERATORS) as lat:
+    # the checker has made 2 boundary updates: a fresh handle's fixedRandomT
+    # patches have 2 fewer perturbed updates left (psteps - localTStep)
+    gcase = case
+    if case.g is not None and abi.BC_FIXEDRANDOMT in list(case.g["bc_type"]):
+        gcase = type(case)(**{**case.__dict__})
+        bcv = np.array(case.g["bc_value"], dtype=float).copy()
+        for p, t in enumerate(case.g["bc_type"]):
+            if t == abi.BC_FIXEDRANDOMT:
+                bcv[p, 2] -= 2
+        gcase.g = dict(case.g, bc_value=bcv)
+    with Lattice(gcase, path=abi.PATH_OPERATORS) as lat:
         lat.upload(rho=state["rho"], U=state["U"], T=state["T"], f=state["f"],
                    g=state["g"] if case.g is not None else None, S=state["S"], Fi=state["Fi"], Ft=state["Ft"])
         lat.set_time(k.get_time())
@@ -249,3 +259,58 @@ def test_surface_tension_rejected_in_fp32(gpu_lib):
     with pytest.raises(MplbError) as e:
         Lattice(small_cases()["st_d2q9"], path=abi.PATH_FUSED, precision=abi.FP32_DEV)
     assert e.value.code == abi.E_UNSUPPORTED
+
+
+THERMAL_MY = ["my_column_d2q9", "my_walls_d3q15", "outflow_d2q9", "outflow_corner_d2q9", "outflow_d3q15"]
+
+
+@pytest.mark.parametrize("name", THERMAL_MY)
+def test_operator_only_options_select_the_operator_path(gpu_lib, name):
+    """myMRT heat, outflow and fixedRandomT run on the operator path: AUTO
+    picks it on a box, FUSED and the FP32 form say they cannot."""
+    from multiphaselb_b200 import Lattice, MplbError
+    case = small_cases()[name]
+    _, info = run_gpu(case, 1)
+    assert info["path"] == abi.PATH_OPERATORS
+    for kw in (dict(path=abi.PATH_FUSED), dict(path=abi.PATH_AUTO, precision=abi.FP32_DEV)):
+        with pytest.raises(MplbError) as e:
+            Lattice(case, **kw)
+        assert e.value.code == abi.E_UNSUPPORTED
+
+
+def test_outflow_corner_runs_in_serial_order(gpu_lib):
+    """A corner node's outflow normal truncates to the rest direction, so it
+    reads its own populations, which other patches write: the reference's
+    serial boundary order is kept, and the result is the oracle's."""
+    case = small_cases()["outflow_corner_d2q9"]
+    got, info = run_gpu(case, 5, path=abi.PATH_OPERATORS)
+    assert info["bc_sequential"] & 1 and info["bc_sequential"] & 2
+    assert_same(got, run_checker("port", case, 5), ctx="outflow corner")
+
+
+def test_fixedrandomt_follows_the_rank_seed(gpu_lib):
+    """srand(pid) at every call: another rank draws other wall temperatures,
+    and after the perturbed updates both ranks apply the plain wall value."""
+    case = small_cases()["outflow_d2q9"]
+    outs = {}
+    for rank in (0, 3, 4):
+        c2 = type(case)(**{**case.__dict__})
+        c2.meta = dict(case.meta, rank=rank)
+        got, _ = run_gpu(c2, 2, path=abi.PATH_OPERATORS)
+        assert_same(got, run_checker("port", c2, 2), ctx=f"rank {rank}")
+        outs[rank] = got["g"]
+    assert not np.array_equal(outs[3], outs[4]) and not np.array_equal(outs[0], outs[3])
+
+
+def test_outflow_without_normal_is_refused(gpu_lib):
+    """Outflow on nodes with every neighbour present has no normal (the
+    reference stops: outflow.c:67-71); create refuses it."""
+    from multiphaselb_b200 import Lattice, MplbError
+    case = small_cases()["outflow_d2q9"]
+    c2 = type(case)(**{**case.__dict__})
+    mid = np.nonzero(case.points[:, 1] == case.dims[1] // 2)[0].astype(np.uint32)
+    c2.patches = [case.patches[0], mid]
+    c2.f = dict(case.f, bc_type=[abi.BC_BOUNCEBACK, abi.BC_OUTFLOW])
+    with pytest.raises(MplbError) as e:
+        Lattice(c2, path=abi.PATH_OPERATORS)
+    assert e.value.code == abi.E_ARG
