@@ -166,6 +166,31 @@ __device__ __forceinline__ void apply_flow_program(const FusedArgs& A, uint32_t 
     for (int o = 0; o < pr.nf; o++) bounce_back<L>(miss, f);
 }
 
+// Prefetch into L2 what pull_node and the heat source will load for node
+// (x, y): the pulled populations, and T, U, S of the node.  Issued at kernel
+// start so these misses overlap the ring work instead of following it.
+__device__ __forceinline__ void prefetch_l2(const void* p) {
+    asm volatile("prefetch.global.L2 [%0];" ::"l"(p));
+}
+template <class L, bool F_ON, bool G_ON>
+__device__ __forceinline__ void prefetch_node(const Params& P, const FusedArgs& A, int x, int y, uint32_t id) {
+    const uint32_t n = P.n;
+    const NodeOffsets no = node_offsets(A, x, y, 0, L::D);
+    static_for<L::Q>([&](auto kk) {
+        constexpr int k = decltype(kk)::value;
+        bool m;
+        const uint32_t src = source_of(no, id, cxk<L>(k), cyk<L>(k), czk<L>(k), m);
+        if constexpr (F_ON) prefetch_l2(A.fin + (size_t)k * n + src);
+        if constexpr (G_ON) prefetch_l2(A.gin + (size_t)k * n + src);
+    });
+    if constexpr (G_ON) {
+        prefetch_l2(A.Told + id);
+        prefetch_l2(A.Uold + id);
+        prefetch_l2(A.Uold + n + id);
+        prefetch_l2(A.S + id);
+    }
+}
+
 // ------------------------------------------------------------ phase A
 // Pull-stream one node, apply its boundary program, sum moments.
 // f, g receive f''_n, g''_n; miss bit k = population k has no source.
@@ -338,8 +363,11 @@ __device__ __forceinline__ void finish_node(const Params& P, const FusedArgs& A,
 // (psi, 1/rho, T_{n-1}, U_{n-1}) computed by the first threads.
 constexpr int min_blocks(int threads) { return threads <= 128 ? 4 : (threads <= 256 ? 2 : 1); }
 
-template <int F2_TX, int F2_TY, bool F_ON, bool G_ON, bool HAS_BC, bool EMIT>
-__global__ void __launch_bounds__(F2_TX * F2_TY, min_blocks(F2_TX * F2_TY)) k_fused_d2q9(Params P, FusedArgs A) {
+// MINB: resident blocks per SM asked of the register allocator (0 = the
+// default of min_blocks); a higher value trades registers for warps.
+template <int F2_TX, int F2_TY, int MINB, bool F_ON, bool G_ON, bool HAS_BC, bool EMIT>
+__global__ void __launch_bounds__(F2_TX * F2_TY, MINB ? MINB : min_blocks(F2_TX * F2_TY))
+    k_fused_d2q9(Params P, FusedArgs A) {
     using L = D2Q9T;
     constexpr int EX = F2_TX + 2, EY = F2_TY + 2, NRING = 2 * EX + 2 * F2_TY;
     constexpr int GY = G_ON ? EY : 1, GX = G_ON ? EX : 1;
@@ -379,6 +407,12 @@ __global__ void __launch_bounds__(F2_TX * F2_TY, min_blocks(F2_TX * F2_TY)) k_fu
         return true;
     };
 
+    {
+        // the own node's loads start now; the ring work below overlaps them
+        const int px = x0 + tx, py = y0 + ty;
+        if (px < A.nx && py < A.ny)
+            prefetch_node<L, F_ON, G_ON>(P, A, px, py, (uint32_t)px + (uint32_t)A.nx * (uint32_t)py);
+    }
     // the ring first, so the own node's populations are live only across the barrier
     for (int r = threadIdx.x; r < NRING; r += blockDim.x) {
         int ex, ey;
@@ -667,10 +701,13 @@ __global__ void __launch_bounds__(F3_TX * F3_TY, min_blocks(F3_TX * F3_TY)) k_fu
 struct TileCfg {
     int tx, ty;
     bool pipe;  // 3D only: cp.async-staged pulls
+    int minb;   // 2D only: resident blocks per SM asked of the register allocator (0 = default)
 };
-constexpr int N_CFG2 = 5, N_CFG3 = 6;
-constexpr TileCfg CFG2[N_CFG2] = {{32, 8, false}, {32, 4, false}, {64, 4, false}, {16, 8, false}, {32, 16, false}};
-constexpr TileCfg CFG3[N_CFG3] = {{32, 8, false}, {32, 8, true}, {32, 4, false}, {64, 4, false}, {32, 16, false}, {64, 8, false}};
+constexpr int N_CFG2 = 8, N_CFG3 = 6;
+constexpr TileCfg CFG2[N_CFG2] = {{32, 8, false, 0}, {32, 4, false, 0}, {64, 4, false, 0}, {16, 8, false, 0},
+                                  {32, 16, false, 0}, {16, 8, false, 6}, {32, 8, false, 3}, {32, 4, false, 8}};
+constexpr TileCfg CFG3[N_CFG3] = {{32, 8, false, 0}, {32, 8, true, 0}, {32, 4, false, 0}, {64, 4, false, 0},
+                                  {32, 16, false, 0}, {64, 8, false, 0}};
 
 struct Geom {
     int tiles_x, tiles_y, zchunk, nblocks;

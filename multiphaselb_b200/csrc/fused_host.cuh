@@ -49,17 +49,17 @@ inline cudaError_t fused_attributes() {
     return e;
 }
 
-template <int TX, int TY, bool F_ON, bool G_ON, bool EMIT>
+template <int TX, int TY, int MINB, bool F_ON, bool G_ON, bool EMIT>
 void launch2(bool bc, int nb, const Params& P, const FusedArgs& A, cudaStream_t s) {
-    if (bc) k_fused_d2q9<TX, TY, F_ON, G_ON, true, EMIT><<<nb, TX * TY, 0, s>>>(P, A);
-    else k_fused_d2q9<TX, TY, F_ON, G_ON, false, EMIT><<<nb, TX * TY, 0, s>>>(P, A);
+    if (bc) k_fused_d2q9<TX, TY, MINB, F_ON, G_ON, true, EMIT><<<nb, TX * TY, 0, s>>>(P, A);
+    else k_fused_d2q9<TX, TY, MINB, F_ON, G_ON, false, EMIT><<<nb, TX * TY, 0, s>>>(P, A);
 }
 
-template <int TX, int TY, bool EMIT>
+template <int TX, int TY, bool EMIT, int MINB = 0>
 void launch2_fg(bool fon, bool gon, bool bc, int nb, const Params& P, const FusedArgs& A, cudaStream_t s) {
-    if (fon && gon) launch2<TX, TY, true, true, EMIT>(bc, nb, P, A, s);
-    else if (fon) launch2<TX, TY, true, false, EMIT>(bc, nb, P, A, s);
-    else if (gon) launch2<TX, TY, false, true, EMIT>(bc, nb, P, A, s);
+    if (fon && gon) launch2<TX, TY, MINB, true, true, EMIT>(bc, nb, P, A, s);
+    else if (fon) launch2<TX, TY, MINB, true, false, EMIT>(bc, nb, P, A, s);
+    else if (gon) launch2<TX, TY, MINB, false, true, EMIT>(bc, nb, P, A, s);
 }
 
 template <int TX, int TY, bool PIPE, bool EMIT>
@@ -90,7 +90,10 @@ inline cudaError_t fused_launch_cfg(const FusedConfig& fc, int cfg, const Params
             case 1: launch2_fg<32, 4, false>(f_on, g_on, bc, nb, P, A, s); break;
             case 2: launch2_fg<64, 4, false>(f_on, g_on, bc, nb, P, A, s); break;
             case 3: launch2_fg<16, 8, false>(f_on, g_on, bc, nb, P, A, s); break;
-            default: launch2_fg<32, 16, false>(f_on, g_on, bc, nb, P, A, s); break;
+            case 4: launch2_fg<32, 16, false>(f_on, g_on, bc, nb, P, A, s); break;
+            case 5: launch2_fg<16, 8, false, 6>(f_on, g_on, bc, nb, P, A, s); break;
+            case 6: launch2_fg<32, 8, false, 3>(f_on, g_on, bc, nb, P, A, s); break;
+            default: launch2_fg<32, 4, false, 8>(f_on, g_on, bc, nb, P, A, s); break;
             }
         }
     } else {

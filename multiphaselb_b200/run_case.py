@@ -2,8 +2,10 @@
 
     python -m multiphaselb_b200.run_case WORKLOAD STEPS [--path auto|fused|operators]
 
-WORKLOAD: column (thermal VdW column, D2Q9 128x512), bubble2d (D2Q9 256x256),
-bubble3d (D3Q15 192^3), bubble3d_small (D3Q15 96^3, for full ncu captures).
+WORKLOAD: column (thermal VdW column, D2Q9 128x512), column_big (the same
+column at 512x2048, larger than L2, for ncu captures), bubble2d (D2Q9
+256x256), bubble2d_big (D2Q9 1024x1024), bubble3d (D3Q15 192^3),
+bubble3d_small (D3Q15 96^3, for full ncu captures).
 """
 import argparse
 import sys
@@ -12,7 +14,9 @@ from . import PATH_AUTO, PATH_FUSED, PATH_OPERATORS, Lattice, abi, cases
 
 WORKLOADS = {
     "column": lambda: cases.column_case(128, 512),
+    "column_big": lambda: cases.column_case(512, 2048),
     "bubble2d": lambda: cases.bubble_case(abi.D2Q9, 256, 40.0, 5.0, 0.8),
+    "bubble2d_big": lambda: cases.bubble_case(abi.D2Q9, 1024, 160.0, 5.0, 0.8),
     "bubble3d": lambda: cases.bubble_case(abi.D3Q15, 192, 48.0, 5.0, 0.75),
     "bubble3d_small": lambda: cases.bubble_case(abi.D3Q15, 96, 24.0, 5.0, 0.75),
 }

@@ -216,7 +216,7 @@ def test_every_tile_candidate_is_exact(gpu_lib, name):
     from multiphaselb_b200 import Lattice
     case = small_cases()[name]
     want = run_checker("port", case, 4)
-    ncand = 5 if case.lattice == abi.D2Q9 else 6
+    ncand = 8 if case.lattice == abi.D2Q9 else 6
     for c in range(1, ncand + 1):
         with Lattice(case, path=abi.PATH_FUSED, tile_config=c) as lat:
             lat.upload_case()
