@@ -59,6 +59,7 @@ struct FusedArgs {
     double* Fi_out;
     double* Ft_out;
     const uint8_t* bcmap;  // per node: 0 = no boundary op, else index into prog
+    int bc_margin;         // largest distance of a node with a boundary op from its nearest face, -1 = none
     double Twall[MPLB_MAX_PATCHES];
     BCProg prog[FUSED_MAX_PROGS];
 };
@@ -363,33 +364,78 @@ __device__ __forceinline__ void finish_node(const Params& P, const FusedArgs& A,
 // (psi, 1/rho, T_{n-1}, U_{n-1}) computed by the first threads.
 constexpr int min_blocks(int threads) { return threads <= 128 ? 4 : (threads <= 256 ? 2 : 1); }
 
-// MINB: resident blocks per SM asked of the register allocator (0 = the
-// default of min_blocks); a higher value trades registers for warps.
-template <int F2_TX, int F2_TY, int MINB, bool F_ON, bool G_ON, bool HAS_BC, bool EMIT>
-__global__ void __launch_bounds__(F2_TX * F2_TY, MINB ? MINB : min_blocks(F2_TX * F2_TY))
-    k_fused_d2q9(Params P, FusedArgs A) {
+// Pull-stream one node of an inner tile (no wrap, no missing source, no
+// boundary program): the arithmetic of pull_node without its bookkeeping.
+template <class L, bool F_ON, bool G_ON>
+__device__ __forceinline__ void pull_node_inner(const Params& P, const FusedArgs& A, uint32_t id, double* f,
+                                                double* g, double& rho, double& T) {
+    const uint32_t n = P.n;
+    const int nx = A.nx;
+    static_for<L::Q>([&](auto kk) {
+        constexpr int k = decltype(kk)::value;
+        const uint32_t src = (uint32_t)((int)id - cxk<L>(k) - cyk<L>(k) * nx);
+        if constexpr (F_ON) f[k] = __ldg(A.fin + (size_t)k * n + src);
+        if constexpr (G_ON) g[k] = __ldg(A.gin + (size_t)k * n + src);
+    });
+    if constexpr (F_ON) {
+        double s = 0;
+#pragma unroll
+        for (int k = 0; k < L::Q; k++) s += f[k];
+        rho = s;
+    } else {
+        rho = A.rho_c[id];
+    }
+    if constexpr (G_ON) {
+        double s = 0;
+#pragma unroll
+        for (int k = 0; k < L::Q; k++) s += g[k];
+        T = s;
+    } else {
+        T = A.Told[id];
+    }
+}
+
+// Is the tile at (x0, y0), with its ring and the ring's pull sources, inside
+// the box (nothing wraps, nothing is missing) and free of boundary programs?
+// Such a tile takes the INNER body.  Every node with a program lies within
+// bc_margin of a face, so a ring farther in than that holds none; the test
+// is arithmetic only (uniform over the block, no load before the work).
+template <int TX, int TY>
+__device__ __forceinline__ bool inner_tile(const FusedArgs& A, int x0, int y0) {
+    const int m = A.bc_margin > 0 ? A.bc_margin : 0;
+    return x0 - 1 > m && x0 + TX < A.nx - 1 - m && y0 - 1 > m && y0 + TY < A.ny - 1 - m;
+}
+
+// The tile: TX x TY nodes, one thread each, plus the one-node ring around it
+// (psi, 1/rho, T_{n-1}, U_{n-1}) computed by the first threads.  INNER
+// tiles skip the wrap / missing-source / boundary bookkeeping; the
+// arithmetic is the same code either way.
+template <int F2_TX, int F2_TY, bool F_ON, bool G_ON, bool HAS_BC, bool EMIT, bool INNER, int EX, int EY, int GX,
+          int GY>
+__device__ __forceinline__ void fused2_tile(const Params& P, const FusedArgs& A, int x0, int y0,
+                                            double (*s_psi)[EX], double (*s_inv)[GX], double (*s_To)[GX],
+                                            double (*s_U0)[GX], double (*s_U1)[GX]) {
     using L = D2Q9T;
-    constexpr int EX = F2_TX + 2, EY = F2_TY + 2, NRING = 2 * EX + 2 * F2_TY;
-    constexpr int GY = G_ON ? EY : 1, GX = G_ON ? EX : 1;
-    __shared__ double s_psi[EY][EX];
-    __shared__ double s_inv[GY][GX];
-    __shared__ double s_To[GY][GX];
-    __shared__ double s_U0[GY][GX];
-    __shared__ double s_U1[GY][GX];
+    constexpr int NRING = 2 * EX + 2 * F2_TY;
     const uint32_t n = P.n;
     const int tx = threadIdx.x % F2_TX, ty = threadIdx.x / F2_TX;
-    const int bx = blockIdx.x % A.tiles_x, by = blockIdx.x / A.tiles_x;
-    const int x0 = bx * F2_TX, y0 = by * F2_TY;
 
     // one ext-grid slot: pull, moments, psi; shared-memory record.  The own
     // slot keeps RN(1/rho) and the density's EOS parts for phase B.
     auto slot = [&](int ex, int ey, double* f, double* g, double& rho, double& T, uint32_t& id, bool mine,
                     double& rr, EosRho& er) -> bool {
-        const int x = slot_coord(x0, ex, A.nx, A.px);
-        const int y = slot_coord(y0, ey, A.ny, A.py);
-        if (x < 0 || y < 0) return false;
+        int x, y;
+        if constexpr (INNER) {
+            x = x0 - 1 + ex;
+            y = y0 - 1 + ey;
+        } else {
+            x = slot_coord(x0, ex, A.nx, A.px);
+            y = slot_coord(y0, ey, A.ny, A.py);
+            if (x < 0 || y < 0) return false;
+        }
         id = (uint32_t)x + (uint32_t)A.nx * (uint32_t)y;
-        pull_node<L, F_ON, G_ON, HAS_BC>(P, A, x, y, 0, id, f, g, rho, T);
+        if constexpr (INNER) pull_node_inner<L, F_ON, G_ON>(P, A, id, f, g, rho, T);
+        else pull_node<L, F_ON, G_ON, HAS_BC>(P, A, x, y, 0, id, f, g, rho, T);
         if (mine) {
             rr = rcp_rn(rho);
             er = eos_rho(P, rho);
@@ -426,7 +472,7 @@ __global__ void __launch_bounds__(F2_TX * F2_TY, MINB ? MINB : min_blocks(F2_TX 
     EosRho er{};
     uint32_t id = 0;
     const int gx = x0 + tx, gy = y0 + ty;
-    const bool own = gx < A.nx && gy < A.ny;
+    const bool own = INNER || (gx < A.nx && gy < A.ny);
     // interior slot (threads outside the box still fill the slot of the
     // wrapped node, so partial tiles see their periodic neighbours)
     const bool have = slot(tx + 1, ty + 1, f, g, rho, T, id, own, rr, er);
@@ -434,7 +480,7 @@ __global__ void __launch_bounds__(F2_TX * F2_TY, MINB ? MINB : min_blocks(F2_TX 
     if (!own || !have) return;
 
     const int ex = tx + 1, ey = ty + 1;
-    const bool onb = on_wall(A, gx, gy, 0);
+    const bool onb = INNER ? false : on_wall(A, gx, gy, 0);
     double heat = 0;
     if constexpr (G_ON && !EMIT) {
         // heatSource.c:119-165 with the one-sided differences of finiteDifference/*.c
@@ -442,7 +488,7 @@ __global__ void __launch_bounds__(F2_TX * F2_TY, MINB ? MINB : min_blocks(F2_TX 
         const double To = s_To[ey][ex], iv = s_inv[ey][ex];
         // x: a = x+1, b = x-1
         {
-            bool a = wrap1(gx + 1, A.nx, A.px) >= 0, b = wrap1(gx - 1, A.nx, A.px) >= 0;
+            bool a = INNER || wrap1(gx + 1, A.nx, A.px) >= 0, b = INNER || wrap1(gx - 1, A.nx, A.px) >= 0;
             FD t = fd_pair(a ? 0 : -1, b ? 0 : -1, s_To[ey][ex + 1], s_To[ey][ex - 1], To);
             FD r = fd_pair(a ? 0 : -1, b ? 0 : -1, s_inv[ey][ex + 1], s_inv[ey][ex - 1], iv);
             FD u = fd_pair(a ? 0 : -1, b ? 0 : -1, s_U0[ey][ex + 1], s_U0[ey][ex - 1], s_U0[ey][ex]);
@@ -451,7 +497,7 @@ __global__ void __launch_bounds__(F2_TX * F2_TY, MINB ? MINB : min_blocks(F2_TX 
             if (u.present) div += u.v;
         }
         {
-            bool a = wrap1(gy + 1, A.ny, A.py) >= 0, b = wrap1(gy - 1, A.ny, A.py) >= 0;
+            bool a = INNER || wrap1(gy + 1, A.ny, A.py) >= 0, b = INNER || wrap1(gy - 1, A.ny, A.py) >= 0;
             FD t = fd_pair(a ? 0 : -1, b ? 0 : -1, s_To[ey + 1][ex], s_To[ey - 1][ex], To);
             FD r = fd_pair(a ? 0 : -1, b ? 0 : -1, s_inv[ey + 1][ex], s_inv[ey - 1][ex], iv);
             FD u = fd_pair(a ? 0 : -1, b ? 0 : -1, s_U1[ey + 1][ex], s_U1[ey - 1][ex], s_U1[ey][ex]);
@@ -468,6 +514,34 @@ __global__ void __launch_bounds__(F2_TX * F2_TY, MINB ? MINB : min_blocks(F2_TX 
     if constexpr (F_ON) psi = s_psi[ey][ex];
     auto nbpsi = [&](int k) { return s_psi[ey + cyk<L>(k)][ex + cxk<L>(k)]; };
     finish_node<L, F_ON, G_ON, EMIT>(P, A, id, onb, f, g, rho, rr, T, psi, nbpsi, heat);
+}
+
+// MINB: resident blocks per SM asked of the register allocator (0 = the
+// default of min_blocks); a higher value trades registers for warps.
+// TRY_INNER: the kernel also carries the INNER body for tiles away from the
+// faces; without it the kernel holds the general body alone (a smaller
+// instruction footprint, which a lattice of one wave notices).
+template <int F2_TX, int F2_TY, int MINB, bool F_ON, bool G_ON, bool HAS_BC, bool EMIT, bool TRY_INNER = false>
+__global__ void __launch_bounds__(F2_TX * F2_TY, MINB ? MINB : min_blocks(F2_TX * F2_TY))
+    k_fused_d2q9(Params P, FusedArgs A) {
+    constexpr int EX = F2_TX + 2, EY = F2_TY + 2;
+    constexpr int GY = G_ON ? EY : 1, GX = G_ON ? EX : 1;
+    __shared__ double s_psi[EY][EX];
+    __shared__ double s_inv[GY][GX];
+    __shared__ double s_To[GY][GX];
+    __shared__ double s_U0[GY][GX];
+    __shared__ double s_U1[GY][GX];
+    const int bx = blockIdx.x % A.tiles_x, by = blockIdx.x / A.tiles_x;
+    const int x0 = bx * F2_TX, y0 = by * F2_TY;
+    if constexpr (TRY_INNER) {
+        if (inner_tile<F2_TX, F2_TY>(A, x0, y0)) {
+            fused2_tile<F2_TX, F2_TY, F_ON, G_ON, HAS_BC, EMIT, true, EX, EY, GX, GY>(P, A, x0, y0, s_psi, s_inv,
+                                                                                      s_To, s_U0, s_U1);
+            return;
+        }
+    }
+    fused2_tile<F2_TX, F2_TY, F_ON, G_ON, HAS_BC, EMIT, false, EX, EY, GX, GY>(P, A, x0, y0, s_psi, s_inv, s_To,
+                                                                               s_U0, s_U1);
 }
 
 // ------------------------------------------------------------ 3D kernels
@@ -700,14 +774,17 @@ __global__ void __launch_bounds__(F3_TX * F3_TY, min_blocks(F3_TX * F3_TY)) k_fu
 // first fused step and keeps the fastest; results are identical for all.
 struct TileCfg {
     int tx, ty;
-    bool pipe;  // 3D only: cp.async-staged pulls
-    int minb;   // 2D only: resident blocks per SM asked of the register allocator (0 = default)
+    bool pipe;   // 3D only: cp.async-staged pulls
+    int minb;    // 2D only: resident blocks per SM asked of the register allocator (0 = default)
+    bool inner;  // 2D only: the kernel variant whose inner tiles take the lean body (pays off
+                 // on large lattices; a lattice of one wave prefers the smaller general kernel)
 };
 constexpr int N_CFG2 = 8, N_CFG3 = 6;
-constexpr TileCfg CFG2[N_CFG2] = {{32, 8, false, 0}, {32, 4, false, 0}, {64, 4, false, 0}, {16, 8, false, 0},
-                                  {32, 16, false, 0}, {16, 8, false, 6}, {32, 8, false, 3}, {32, 4, false, 8}};
-constexpr TileCfg CFG3[N_CFG3] = {{32, 8, false, 0}, {32, 8, true, 0}, {32, 4, false, 0}, {64, 4, false, 0},
-                                  {32, 16, false, 0}, {64, 8, false, 0}};
+constexpr TileCfg CFG2[N_CFG2] = {{32, 8, false, 0, false}, {32, 4, false, 0, false}, {64, 4, false, 0, false},
+                                  {16, 8, false, 0, true},  {64, 4, false, 0, true},  {16, 8, false, 6, true},
+                                  {32, 8, false, 3, true},  {32, 4, false, 8, true}};
+constexpr TileCfg CFG3[N_CFG3] = {{32, 8, false, 0, false}, {32, 8, true, 0, false}, {32, 4, false, 0, false},
+                                  {64, 4, false, 0, false}, {32, 16, false, 0, false}, {64, 8, false, 0, false}};
 
 struct Geom {
     int tiles_x, tiles_y, zchunk, nblocks;

@@ -49,17 +49,17 @@ inline cudaError_t fused_attributes() {
     return e;
 }
 
-template <int TX, int TY, int MINB, bool F_ON, bool G_ON, bool EMIT>
+template <int TX, int TY, int MINB, bool F_ON, bool G_ON, bool EMIT, bool INNER>
 void launch2(bool bc, int nb, const Params& P, const FusedArgs& A, cudaStream_t s) {
-    if (bc) k_fused_d2q9<TX, TY, MINB, F_ON, G_ON, true, EMIT><<<nb, TX * TY, 0, s>>>(P, A);
-    else k_fused_d2q9<TX, TY, MINB, F_ON, G_ON, false, EMIT><<<nb, TX * TY, 0, s>>>(P, A);
+    if (bc) k_fused_d2q9<TX, TY, MINB, F_ON, G_ON, true, EMIT, INNER><<<nb, TX * TY, 0, s>>>(P, A);
+    else k_fused_d2q9<TX, TY, MINB, F_ON, G_ON, false, EMIT, INNER><<<nb, TX * TY, 0, s>>>(P, A);
 }
 
-template <int TX, int TY, bool EMIT, int MINB = 0>
+template <int TX, int TY, bool EMIT, int MINB = 0, bool INNER = false>
 void launch2_fg(bool fon, bool gon, bool bc, int nb, const Params& P, const FusedArgs& A, cudaStream_t s) {
-    if (fon && gon) launch2<TX, TY, MINB, true, true, EMIT>(bc, nb, P, A, s);
-    else if (fon) launch2<TX, TY, MINB, true, false, EMIT>(bc, nb, P, A, s);
-    else if (gon) launch2<TX, TY, MINB, false, true, EMIT>(bc, nb, P, A, s);
+    if (fon && gon) launch2<TX, TY, MINB, true, true, EMIT, INNER>(bc, nb, P, A, s);
+    else if (fon) launch2<TX, TY, MINB, true, false, EMIT, INNER>(bc, nb, P, A, s);
+    else if (gon) launch2<TX, TY, MINB, false, true, EMIT, INNER>(bc, nb, P, A, s);
 }
 
 template <int TX, int TY, bool PIPE, bool EMIT>
@@ -89,11 +89,11 @@ inline cudaError_t fused_launch_cfg(const FusedConfig& fc, int cfg, const Params
             case 0: launch2_fg<32, 8, false>(f_on, g_on, bc, nb, P, A, s); break;
             case 1: launch2_fg<32, 4, false>(f_on, g_on, bc, nb, P, A, s); break;
             case 2: launch2_fg<64, 4, false>(f_on, g_on, bc, nb, P, A, s); break;
-            case 3: launch2_fg<16, 8, false>(f_on, g_on, bc, nb, P, A, s); break;
-            case 4: launch2_fg<32, 16, false>(f_on, g_on, bc, nb, P, A, s); break;
-            case 5: launch2_fg<16, 8, false, 6>(f_on, g_on, bc, nb, P, A, s); break;
-            case 6: launch2_fg<32, 8, false, 3>(f_on, g_on, bc, nb, P, A, s); break;
-            default: launch2_fg<32, 4, false, 8>(f_on, g_on, bc, nb, P, A, s); break;
+            case 3: launch2_fg<16, 8, false, 0, true>(f_on, g_on, bc, nb, P, A, s); break;
+            case 4: launch2_fg<64, 4, false, 0, true>(f_on, g_on, bc, nb, P, A, s); break;
+            case 5: launch2_fg<16, 8, false, 6, true>(f_on, g_on, bc, nb, P, A, s); break;
+            case 6: launch2_fg<32, 8, false, 3, true>(f_on, g_on, bc, nb, P, A, s); break;
+            default: launch2_fg<32, 4, false, 8, true>(f_on, g_on, bc, nb, P, A, s); break;
             }
         }
     } else {
@@ -251,6 +251,17 @@ inline int fused_setup(FusedConfig& fc, int lat, const int* model, const Params&
             }
             map[id] = (uint8_t)found;
         }
+    }
+    // farthest distance of a node with a boundary program from its nearest
+    // box face (-1: none); tiles whose ring lies farther in hold none
+    A.bc_margin = -1;
+    for (uint32_t id = 0; id < n; id++) {
+        if (!map[id]) continue;
+        const int x = (int)(id % (uint32_t)A.nx), y = (int)((id / (uint32_t)A.nx) % (uint32_t)A.ny);
+        const int z = (int)(id / ((uint32_t)A.nx * (uint32_t)A.ny));
+        int d = std::min(std::min(x, A.nx - 1 - x), std::min(y, A.ny - 1 - y));
+        if (lat == MPLB_D3Q15) d = std::min(d, std::min(z, A.nz - 1 - z));
+        A.bc_margin = std::max(A.bc_margin, d);
     }
     for (size_t q = 0; q < progs.size(); q++) A.prog[q] = progs[q];
     for (size_t p = 0; p < fp[1].size() && p < MPLB_MAX_PATCHES; p++) A.Twall[p] = fp[1][p].val[0];
