@@ -7,6 +7,8 @@
 // results equal the reference's binary64 results bit for bit.
 #pragma once
 
+#include <cmath>
+
 #include <stdint.h>
 #include <utility>
 #include <type_traits>
@@ -224,6 +226,20 @@ MPLB_HD void static_for(F&& f) { static_for_impl(f, std::make_integer_sequence<i
 // matVecMult.c:4-20 evaluates res_i = sum_j M_ij v_j left to right from 0.
 // M has integer entries, so each product is exact; terms with a zero
 // coefficient are skipped (they add +-0 and leave a finite sum unchanged).
+// s + c v for an integer c with |c| a power of two >= 2: c v is exact, so one
+// fused multiply-add rounds exactly as the separate multiply and add.
+MPLB_HD constexpr bool pow2_ge2(int c) {
+    const int a = c < 0 ? -c : c;
+    return a >= 2 && (a & (a - 1)) == 0;
+}
+MPLB_HD double add_exact_product(double s, double c, double v) {
+#ifdef __CUDA_ARCH__
+    return __fma_rn(c, v, s);
+#else
+    return std::fma(c, v, s);
+#endif
+}
+
 template <class L>
 MPLB_HD void mul_M(const double* v, double* r) {
     static_for<L::Q>([&](auto i) {
@@ -232,6 +248,7 @@ MPLB_HD void mul_M(const double* v, double* r) {
             constexpr int c = Mint<L>(decltype(i)::value, decltype(j)::value);
             if constexpr (c == 1) s = s + v[j];
             else if constexpr (c == -1) s = s - v[j];
+            else if constexpr (pow2_ge2(c)) s = add_exact_product(s, (double)c, v[j]);
             else if constexpr (c != 0) s = s + (double)c * v[j];
         });
         r[i] = s;
@@ -265,6 +282,7 @@ MPLB_HD void mul_Mi(const Params& P, const double* v, double* r) {
             constexpr int c = Mint<L>(decltype(j)::value, decltype(i)::value);
             if constexpr (c == 1) s = s + p[j];
             else if constexpr (c == -1) s = s - p[j];
+            else if constexpr (pow2_ge2(c)) s = add_exact_product(s, (double)c, p[j]);
             else if constexpr (c != 0) s = s + (double)c * p[j];
         });
         r[i] = s;
