@@ -39,6 +39,7 @@ struct FusedArgs32 {
     float Lf[MPLB_MAX_Q], relax_f[MPLB_MAX_Q], Lg[9];
     float s1_den, s2_den, sig12, sig6, corr3, corr5;
     const uint8_t* bcmap;
+    int bc_margin;  // FusedArgs::bc_margin
     double Twall[MPLB_MAX_PATCHES];
     BCProg prog[FUSED_MAX_PROGS];
 };
@@ -361,6 +362,64 @@ __device__ __forceinline__ void pull_node32(const Params& P, const FusedArgs32& 
     } else {
         T = A.Told[id];
         dT = (float)(T - A.T_ref);
+    }
+}
+
+// pull_node32 for a node of an inner tile (no wrap, no missing source, no
+// boundary program).
+template <class L, bool F_ON, bool G_ON>
+__device__ __forceinline__ void pull_node32_inner(const Params& P, const FusedArgs32& A, uint32_t id, float* f,
+                                                  float* g, double& rho, double& T, float& dr, float& dT) {
+    (void)P;
+    const uint32_t n = A.n;
+    const int nx = A.nx, nxy = A.nx * A.ny;
+    static_for<L::Q>([&](auto kk) {
+        constexpr int k = decltype(kk)::value;
+        const uint32_t src = (uint32_t)((int)id - cxk<L>(k) - cyk<L>(k) * nx - czk<L>(k) * nxy);
+        if constexpr (F_ON) f[k] = __ldg(A.fin + (size_t)k * n + src);
+        if constexpr (G_ON) g[k] = __ldg(A.gin + (size_t)k * n + src);
+    });
+    if constexpr (F_ON) {
+        float s = 0.f;
+#pragma unroll
+        for (int k = 0; k < L::Q; k++) s += f[k];
+        dr = s;
+        rho = A.rho_ref + (double)s;
+    } else {
+        rho = A.rho_c[id];
+        dr = (float)(rho - A.rho_ref);
+    }
+    if constexpr (G_ON) {
+        float s = 0.f;
+#pragma unroll
+        for (int k = 0; k < L::Q; k++) s += g[k];
+        dT = s;
+        T = A.T_ref + (double)s;
+    } else {
+        T = A.Told[id];
+        dT = (float)(T - A.T_ref);
+    }
+}
+
+// L2 prefetch of what pull_node32 and the heat source load for node (x, y).
+template <class L, bool F_ON, bool G_ON>
+__device__ __forceinline__ void prefetch_node32(const FusedArgs32& A, int x, int y, uint32_t id) {
+    const uint32_t n = A.n;
+    FusedArgs G{};
+    G.nx = A.nx; G.ny = A.ny; G.nz = 1; G.px = A.px; G.py = A.py; G.pz = 1;
+    const NodeOffsets no = node_offsets(G, x, y, 0, L::D);
+    static_for<L::Q>([&](auto kk) {
+        constexpr int k = decltype(kk)::value;
+        bool m;
+        const uint32_t src = source_of(no, id, cxk<L>(k), cyk<L>(k), czk<L>(k), m);
+        if constexpr (F_ON) prefetch_l2(A.fin + (size_t)k * n + src);
+        if constexpr (G_ON) prefetch_l2(A.gin + (size_t)k * n + src);
+    });
+    if constexpr (G_ON) {
+        prefetch_l2(A.Told + id);
+        prefetch_l2(A.Uold + id);
+        prefetch_l2(A.Uold + n + id);
+        prefetch_l2(A.S + id);
     }
 }
 

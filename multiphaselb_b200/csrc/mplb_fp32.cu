@@ -21,7 +21,10 @@ struct Smem32 {
 };
 
 // One TX x TY tile (tile coordinates bx, by) of the lattice described by A.
-template <int TX, int TY, bool F_ON, bool G_ON, bool HAS_BC, bool EMIT>
+// INNER: the tile, its ring and the ring's pull sources lie inside the box
+// and away from every boundary program (see the FP64 kernel), so the wrap /
+// missing-source / boundary bookkeeping is skipped.
+template <int TX, int TY, bool F_ON, bool G_ON, bool HAS_BC, bool EMIT, bool INNER = false>
 __device__ __forceinline__ void fused32_tile_d2q9(const Params& P, const FusedArgs32& A, Smem32<TX, TY, G_ON>& sm,
                                                   int bx, int by, double* emit_f, double* emit_g, double* rho_out,
                                                   double* Fi_out, double* Ft_out) {
@@ -33,11 +36,18 @@ __device__ __forceinline__ void fused32_tile_d2q9(const Params& P, const FusedAr
 
     auto slot = [&](int ex, int ey, float* f, float* g, double& rho, double& T, float& dr, float& dT, uint32_t& id,
                     bool mine, double& rr, EosRho& er) -> bool {
-        const int x = slot_coord(x0, ex, A.nx, A.px);
-        const int y = slot_coord(y0, ey, A.ny, A.py);
-        if (x < 0 || y < 0) return false;
+        int x, y;
+        if constexpr (INNER) {
+            x = x0 - 1 + ex;
+            y = y0 - 1 + ey;
+        } else {
+            x = slot_coord(x0, ex, A.nx, A.px);
+            y = slot_coord(y0, ey, A.ny, A.py);
+            if (x < 0 || y < 0) return false;
+        }
         id = (uint32_t)x + (uint32_t)A.nx * (uint32_t)y;
-        pull_node32<L, F_ON, G_ON, HAS_BC>(P, A, x, y, 0, id, f, g, rho, T, dr, dT);
+        if constexpr (INNER) pull_node32_inner<L, F_ON, G_ON>(P, A, id, f, g, rho, T, dr, dT);
+        else pull_node32<L, F_ON, G_ON, HAS_BC>(P, A, x, y, 0, id, f, g, rho, T, dr, dT);
         if (mine) {
             rr = rcp_rn(rho);
             er = eos_rho(P, rho);
@@ -54,6 +64,11 @@ __device__ __forceinline__ void fused32_tile_d2q9(const Params& P, const FusedAr
         }
         return true;
     };
+    if constexpr (INNER) {
+        // the own node's loads start now; the ring work below overlaps them
+        const int px = x0 + tx, py = y0 + ty;
+        prefetch_node32<L, F_ON, G_ON>(A, px, py, (uint32_t)px + (uint32_t)A.nx * (uint32_t)py);
+    }
     for (int r = threadIdx.x; r < NRING; r += blockDim.x) {
         int ex, ey;
         ring_slot(r, TX, TY, ex, ey);
@@ -68,20 +83,20 @@ __device__ __forceinline__ void fused32_tile_d2q9(const Params& P, const FusedAr
     EosRho er{};
     uint32_t id = 0;
     const int gx = x0 + tx, gy = y0 + ty;
-    const bool own = gx < A.nx && gy < A.ny;
+    const bool own = INNER || (gx < A.nx && gy < A.ny);
     const bool have = slot(tx + 1, ty + 1, f, g, rho, T, dr, dT, id, own, rr, er);
     __syncthreads();
     if (own && have) {
         const int ex = tx + 1, ey = ty + 1;
         FusedArgs Gm{};
         Gm.nx = A.nx; Gm.ny = A.ny; Gm.nz = 1; Gm.px = A.px; Gm.py = A.py; Gm.pz = 1;
-        const bool onb = on_wall(Gm, gx, gy, 0);
+        const bool onb = INNER ? false : on_wall(Gm, gx, gy, 0);
         double heat = 0;
         if constexpr (G_ON && !EMIT) {
             double gT[3] = {0, 0, 0}, gR[3] = {0, 0, 0}, div = 0;
             const double To = sm.To[ey][ex], iv = sm.inv[ey][ex];
             {
-                const bool a = wrap1(gx + 1, A.nx, A.px) >= 0, b = wrap1(gx - 1, A.nx, A.px) >= 0;
+                const bool a = INNER || wrap1(gx + 1, A.nx, A.px) >= 0, b = INNER || wrap1(gx - 1, A.nx, A.px) >= 0;
                 FD t = fd_pair(a ? 0 : -1, b ? 0 : -1, sm.To[ey][ex + 1], sm.To[ey][ex - 1], To);
                 FD r = fd_pair(a ? 0 : -1, b ? 0 : -1, sm.inv[ey][ex + 1], sm.inv[ey][ex - 1], iv);
                 FD u = fd_pair(a ? 0 : -1, b ? 0 : -1, sm.U0[ey][ex + 1], sm.U0[ey][ex - 1], sm.U0[ey][ex]);
@@ -90,7 +105,7 @@ __device__ __forceinline__ void fused32_tile_d2q9(const Params& P, const FusedAr
                 if (u.present) div += u.v;
             }
             {
-                const bool a = wrap1(gy + 1, A.ny, A.py) >= 0, b = wrap1(gy - 1, A.ny, A.py) >= 0;
+                const bool a = INNER || wrap1(gy + 1, A.ny, A.py) >= 0, b = INNER || wrap1(gy - 1, A.ny, A.py) >= 0;
                 FD t = fd_pair(a ? 0 : -1, b ? 0 : -1, sm.To[ey + 1][ex], sm.To[ey - 1][ex], To);
                 FD r = fd_pair(a ? 0 : -1, b ? 0 : -1, sm.inv[ey + 1][ex], sm.inv[ey - 1][ex], iv);
                 FD u = fd_pair(a ? 0 : -1, b ? 0 : -1, sm.U1[ey + 1][ex], sm.U1[ey - 1][ex], sm.U1[ey][ex]);
@@ -109,14 +124,32 @@ __device__ __forceinline__ void fused32_tile_d2q9(const Params& P, const FusedAr
 }
 
 // ------------------------------------------------------------- 2D kernel
-template <int TX, int TY, bool F_ON, bool G_ON, bool HAS_BC, bool EMIT>
-__global__ void __launch_bounds__(TX * TY, min_blocks(TX * TY))
+// MINB: resident blocks per SM asked of the register allocator (0 = default).
+// TRY_INNER: inner tiles take the lean body (large lattices); otherwise the
+// kernel holds the general body alone (a lattice of one wave prefers it).
+template <int TX, int TY, bool F_ON, bool G_ON, bool HAS_BC, bool EMIT, int MINB = 0, bool TRY_INNER = false>
+__global__ void __launch_bounds__(TX * TY, MINB ? MINB : min_blocks(TX * TY))
     k_fused32_d2q9(Params P, FusedArgs32 A, double* emit_f, double* emit_g, double* rho_out, double* Fi_out,
                    double* Ft_out) {
     __shared__ Smem32<TX, TY, G_ON> sm;
-    fused32_tile_d2q9<TX, TY, F_ON, G_ON, HAS_BC, EMIT>(P, A, sm, blockIdx.x % A.tiles_x, blockIdx.x / A.tiles_x,
-                                                         emit_f, emit_g, rho_out, Fi_out, Ft_out);
+    const int bx = blockIdx.x % A.tiles_x, by = blockIdx.x / A.tiles_x;
+    if constexpr (TRY_INNER) {
+        const int m = A.bc_margin > 0 ? A.bc_margin : 0;
+        const int x0 = bx * TX, y0 = by * TY;
+        if (x0 - 1 > m && x0 + TX < A.nx - 1 - m && y0 - 1 > m && y0 + TY < A.ny - 1 - m) {
+            fused32_tile_d2q9<TX, TY, F_ON, G_ON, HAS_BC, EMIT, true>(P, A, sm, bx, by, emit_f, emit_g, rho_out,
+                                                                      Fi_out, Ft_out);
+            return;
+        }
+    }
+    fused32_tile_d2q9<TX, TY, F_ON, G_ON, HAS_BC, EMIT, false>(P, A, sm, bx, by, emit_f, emit_g, rho_out, Fi_out,
+                                                               Ft_out);
 }
+
+// Lattices of more tiles than this (32 x 8) take the register-capped
+// inner-tile kernel: several waves, where it measured faster; fewer (one
+// wave or so) keep the general kernel.
+constexpr int F32_INNER_MIN_TILES = 4 * 148;
 
 // ------------------------------------------------------------- 3D kernel
 template <int TX, int TY>
@@ -220,6 +253,7 @@ FusedArgs32 mplb_make_args32(const FusedArgs& A, const Params& P, double rho_ref
     B.tiles_x = A.tiles_x; B.tiles_y = A.tiles_y; B.zchunk = A.zchunk;
     B.n = P.n;
     B.bcmap = A.bcmap;
+    B.bc_margin = A.bc_margin;
     for (int p = 0; p < MPLB_MAX_PATCHES; p++) B.Twall[p] = A.Twall[p];
     for (int q = 0; q < FUSED_MAX_PROGS; q++) B.prog[q] = A.prog[q];
     B.rho_ref = rho_ref;
@@ -264,7 +298,12 @@ cudaError_t mplb_fused32_launch(int lat, bool has_bc, bool f_on, bool g_on, bool
         B.tiles_x = g.tiles_x;
         B.tiles_y = g.tiles_y;
         B.zchunk = 1;
-#define MPLB_L32(F, G, BC, E) k_fused32_d2q9<32, 8, F, G, BC, E><<<g.nblocks, 256, 0, s>>>(P, B, emit_f, emit_g, rho_out, Fi_out, Ft_out)
+        const bool big = !emit && g.nblocks > F32_INNER_MIN_TILES;
+#define MPLB_L32(F, G, BC, E)                                                                                    \
+    (big ? (k_fused32_d2q9<32, 8, F, G, BC, E, 3, true><<<g.nblocks, 256, 0, s>>>(P, B, emit_f, emit_g, rho_out, \
+                                                                                   Fi_out, Ft_out), 0)          \
+         : (k_fused32_d2q9<32, 8, F, G, BC, E><<<g.nblocks, 256, 0, s>>>(P, B, emit_f, emit_g, rho_out, Fi_out,  \
+                                                                        Ft_out), 0))
 #define MPLB_L32_E(F, G, BC) (emit ? (MPLB_L32(F, G, BC, true), 0) : (MPLB_L32(F, G, BC, false), 0))
 #define MPLB_L32_B(F, G) (has_bc ? MPLB_L32_E(F, G, true) : MPLB_L32_E(F, G, false))
         if (f_on && g_on) MPLB_L32_B(true, true);

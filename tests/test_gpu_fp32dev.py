@@ -65,3 +65,23 @@ def test_fp32dev_materialise_and_continue(gpu_lib):
     k = run_checker("port", case, 7)
     assert rel_err(outs[-1]["rho"], k["rho"]) <= TOL_BIG
     assert rel_err(outs[-1]["T"], k["T"]) <= TOL_BIG
+
+
+@pytest.mark.parametrize("shape", ["column", "bubble"])
+def test_fp32dev_large_lattice_kernel(gpu_lib, shape):
+    """Lattices of more than 592 tiles of 32 x 8 run the register-capped
+    FP32 kernel whose inner tiles skip the wrap and boundary bookkeeping:
+    same error bound against FP64 (the FP64 fused path equals the oracle bit
+    for bit elsewhere)."""
+    from multiphaselb_b200 import cases
+    from tests.helpers import run_gpu
+    case = (cases.column_case(256, 640, amp=1e-3) if shape == "column"
+            else cases.perturbed(cases.bubble_case(abi.D2Q9, 512, 80.0, 5.0, 0.8), du=1e-3))
+    assert (case.dims[0] // 32) * (case.dims[1] // 8) > 592
+    want, _ = run_gpu(case, 10, path=abi.PATH_FUSED)
+    got = run32(case, 10)[-1]
+    errs = {k: rel_err(got[k], want[k]) for k in BIG + SMALL if not (k == "g" and case.g is None)
+            and not (k in ("S", "T") and case.g is None)}
+    print(shape, errs)
+    for k, e in errs.items():
+        assert e <= (TOL_BIG if k in BIG else TOL_SMALL), (shape, k, e)
