@@ -373,8 +373,16 @@ __global__ void __launch_bounds__(TX * TY, batch_min_blocks(TX * TY))
         const int2 w = tiles[t];
         const FusedArgs32& A = As[2 * w.x + parity];
         if (A.tiles_x <= 0 || w.y < 0 || w.y >= A.tiles_x * A.tiles_y) continue;  // block-uniform
-        fused32_tile_d2q9<TX, TY, true, false, false, false>(Ps[w.x], A, sm, w.y % A.tiles_x, w.y / A.tiles_x,
-                                                              nullptr, nullptr, nullptr, nullptr, nullptr);
+        const int bx = w.y % A.tiles_x, by = w.y / A.tiles_x;
+        const int x0 = bx * TX, y0 = by * TY;
+        // fully periodic lattices without boundary programs: a tile whose
+        // ring and its pull sources stay inside the box needs no wrap logic
+        if (x0 >= 2 && x0 + TX + 1 <= A.nx - 1 && y0 >= 2 && y0 + TY + 1 <= A.ny - 1)
+            fused32_tile_d2q9<TX, TY, true, false, false, false, true>(Ps[w.x], A, sm, bx, by, nullptr, nullptr,
+                                                                        nullptr, nullptr, nullptr);
+        else
+            fused32_tile_d2q9<TX, TY, true, false, false, false>(Ps[w.x], A, sm, bx, by, nullptr, nullptr, nullptr,
+                                                                  nullptr, nullptr);
         __syncthreads();
     }
 }
