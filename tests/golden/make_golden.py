@@ -25,7 +25,7 @@ from tests.helpers import FIELDS, run_checker, small_cases  # noqa: E402
 
 STEPS = {"bubble_d2q9": 12, "column_d2q9": 12, "lid_d2q9": 9, "bubble_d3q15": 5, "walls_d3q15": 5,
          "st_d2q9": 10, "st_d3q15": 5, "my_column_d2q9": 9, "my_walls_d3q15": 5, "outflow_d2q9": 8,
-         "outflow_corner_d2q9": 6, "outflow_d3q15": 5}
+         "outflow_corner_d2q9": 6, "outflow_d3q15": 5, "cylinder_d2q9": 8}
 
 
 def save_case(path, case, steps, out):
@@ -37,6 +37,12 @@ def save_case(path, case, steps, out):
                                                for k, v in case.g.items()},
                 steps=steps, rank=int(case.meta.get("rank", 0)))
     arrs = {"in_" + k: getattr(case, k) for k in ("rho", "U", "T")}
+    if not case.meta.get("box", True):
+        # not a box: keep the mesh itself
+        arrs.update(mesh_nb=case.nb, mesh_points=case.points,
+                    mesh_patch_count=np.array([len(p) for p in case.patches], dtype=np.int64),
+                    mesh_patch_nodes=np.concatenate([np.asarray(p, dtype=np.int64) for p in case.patches]))
+        spec["patch_names"] = list(case.patch_names)
     arrs.update({"out_" + k: out[k] for k in FIELDS if not (k == "g" and case.g is None)})
     np.savez_compressed(path, spec=np.frombuffer(json.dumps(spec).encode(), dtype=np.uint8), **arrs)
 
@@ -44,11 +50,17 @@ def save_case(path, case, steps, out):
 def load_case(path):
     z = np.load(path)
     spec = json.loads(bytes(z["spec"]).decode())
-    nb, points, patches, names = cases.box_mesh(spec["lattice"], tuple(spec["dims"]), tuple(spec["periodic"]))
+    if "mesh_nb" in z.files:
+        nb, points = z["mesh_nb"], z["mesh_points"]
+        cuts = np.cumsum(z["mesh_patch_count"])[:-1]
+        patches = [p.astype(np.uint32) for p in np.split(z["mesh_patch_nodes"], cuts)]
+        names = spec["patch_names"]
+    else:
+        nb, points, patches, names = cases.box_mesh(spec["lattice"], tuple(spec["dims"]), tuple(spec["periodic"]))
     eos = {k: (tuple(v) if isinstance(v, list) else v) for k, v in spec["eos"].items()}
     c = cases.Case(spec["name"], spec["lattice"], tuple(spec["dims"]), tuple(spec["periodic"]), nb, points,
                    patches, names, eos, spec["f"], spec["g"], z["in_rho"], z["in_U"], z["in_T"],
-                   meta=dict(rank=spec.get("rank", 0)))
+                   meta=dict(rank=spec.get("rank", 0), box="mesh_nb" not in z.files))
     want = {k[4:]: z[k] for k in z.files if k.startswith("out_")}
     return c, spec["steps"], want
 

@@ -23,7 +23,26 @@ def small_cases():
         "outflow_d2q9": outflow_d2q9(),
         "outflow_corner_d2q9": outflow_corner_d2q9(),
         "outflow_d3q15": outflow_d3q15(),
+        "cylinder_d2q9": cylinder_d2q9(),
     }
+
+
+def cylinder_d2q9():
+    """A non-box mesh: periodic-x channel of 24 x 16 with a disc of radius 3.5
+    removed (multiphaselb_b200.mesh.channel_with_cylinder), the thermal VdW
+    column's fields on it; bounce-back walls and cylinder for the flow,
+    fixedT walls and a hot fixedT cylinder for the heat."""
+    from multiphaselb_b200 import mesh as meshmod
+    m = meshmod.channel_with_cylinder(24, 16, 11.5, 6.5, 3.5)
+    col = cases.column_case(24, 16, amp=1e-3, width=3.0)
+    keep = np.array([x + 24 * y for x, y, _ in m.points.tolist()])
+    tc = col.meta["Tc"]
+    f = dict(col.f, bc_type=[abi.BC_BOUNCEBACK] * 3, bc_value=np.zeros((3, 3)))
+    g = dict(col.g, bc_type=[abi.BC_FIXEDT] * 3,
+             bc_value=np.array([[0.86 * tc, 0, 0], [0.84 * tc, 0, 0], [0.9 * tc, 0, 0]]))
+    c = meshmod.mesh_case(m, "cylinder_d2q9_24x16", col.eos, f, g, col.rho[keep], col.U[keep], col.T[keep],
+                          meta=dict(Tc=tc, box=False))
+    return cases.perturbed(c, du=1e-3)
 
 
 LAMBDA_MY2 = [0.0, 1.1, 1.1, 0.9, 1.0, 0.9, 1.0, 1.0, 1.0]
