@@ -60,6 +60,8 @@ struct FusedArgs {
     double* Ft_out;
     const uint8_t* bcmap;  // per node: 0 = no boundary op, else index into prog
     int bc_margin;         // largest distance of a node with a boundary op from its nearest face, -1 = none
+    double* rho_a;         // myMRT thermal field: rho_n and sum g''_n of every node (k_pullsum_d2q9)
+    double* gsum_a;
     double Twall[MPLB_MAX_PATCHES];
     BCProg prog[FUSED_MAX_PROGS];
 };
@@ -232,8 +234,15 @@ __device__ __forceinline__ void pull_node(const Params& P, const FusedArgs& A, i
                             if (mx < 0 || my < 0) continue;
                             uint32_t m = (uint32_t)mx + (uint32_t)A.nx * (uint32_t)my;
                             double u0 = A.Uold[m], u1 = A.Uold[n + m];
-                            double eq_nb = eq_heat_k(P, k, A.Told[m], u0, u1);
-                            double eq_bnd = eq_heat_k(P, k, Tw, u0, u1);
+                            double eq_nb, eq_bnd;
+                            if (P.g_model == MPLB_MYMRT) {
+                                const double u[3] = {u0, u1, A.Uold[2 * (size_t)n + m]};
+                                eq_nb = eq_my_k<L>(P, k, A.Told[m], u);
+                                eq_bnd = eq_my_k<L>(P, k, Tw, u);
+                            } else {
+                                eq_nb = eq_heat_k(P, k, A.Told[m], u0, u1);
+                                eq_bnd = eq_heat_k(P, k, Tw, u0, u1);
+                            }
                             g[k] = eq_bnd + (A.gin[(size_t)k * n + id] - eq_nb);
                         }
                     }
@@ -262,7 +271,7 @@ __device__ __forceinline__ void pull_node(const Params& P, const FusedArgs& A, i
 // ------------------------------------------------------------ phase B
 // Everything after the macros for one node that owns an output.
 // nbpsi(k) returns psi_n at x + c_k.
-template <class L, bool F_ON, bool G_ON, bool EMIT, class PsiAt>
+template <class L, bool F_ON, bool G_ON, bool EMIT, class PsiAt, bool MY = false>
 __device__ __forceinline__ void finish_node(const Params& P, const FusedArgs& A, uint32_t id, bool onb,
                                             double* f, double* g, double rho, double rr, double T, double psi,
                                             PsiAt nbpsi, double src_heat) {
@@ -351,7 +360,8 @@ __device__ __forceinline__ void finish_node(const Params& P, const FusedArgs& A,
         }
     }
     if constexpr (G_ON) {
-        collide_litemp(P, g, T, U[0], U[1], src_heat);
+        if constexpr (MY) collide_mymrt<L>(P, g, T, U, src_heat);
+        else collide_litemp(P, g, T, U[0], U[1], src_heat);
 #pragma unroll
         for (int k = 0; k < 9; k++) A.gout[(size_t)k * n + id] = g[k];
         A.Tnew[id] = T;
@@ -406,12 +416,62 @@ __device__ __forceinline__ bool inner_tile(const FusedArgs& A, int x0, int y0) {
     return x0 - 1 > m && x0 + TX < A.nx - 1 - m && y0 - 1 > m && y0 + TY < A.ny - 1 - m;
 }
 
+// myMRT heat source of node (x, y) from the arrays of k_pullsum_d2q9
+// (heatSource.c:28-90): gradients of T_{n-1} and 1/rho_n, divergence of
+// U_{n-1}, one-sided at a missing axis neighbour, as the operator kernel.
+template <bool INNER>
+__device__ __forceinline__ double heat_my(const Params& P, const FusedArgs& A, int x, int y, uint32_t id) {
+    const uint32_t n = P.n;
+    double gT[3] = {0, 0, 0}, gR[3] = {0, 0, 0}, div = 0;
+    const double Ti = A.Told[id], ri = A.rho_a[id];
+#pragma unroll
+    for (int d = 0; d < 2; d++) {
+        int xa = x, ya = y, xb = x, yb = y;
+        if (d == 0) {
+            xa = INNER ? x + 1 : wrap1(x + 1, A.nx, A.px);
+            xb = INNER ? x - 1 : wrap1(x - 1, A.nx, A.px);
+        } else {
+            ya = INNER ? y + 1 : wrap1(y + 1, A.ny, A.py);
+            yb = INNER ? y - 1 : wrap1(y - 1, A.ny, A.py);
+        }
+        const bool pa = xa >= 0 && ya >= 0, pb = xb >= 0 && yb >= 0;
+        const uint32_t ia = pa ? (uint32_t)xa + (uint32_t)A.nx * (uint32_t)ya : id;
+        const uint32_t ib = pb ? (uint32_t)xb + (uint32_t)A.nx * (uint32_t)yb : id;
+        const FD t = fd_pair(pa ? 0 : -1, pb ? 0 : -1, A.Told[ia], A.Told[ib], Ti);
+        const FD r = fd_pair(pa ? 0 : -1, pb ? 0 : -1, 1.0 / A.rho_a[ia], 1.0 / A.rho_a[ib], 1.0 / ri);
+        const FD u = fd_pair(pa ? 0 : -1, pb ? 0 : -1, A.Uold[(size_t)d * n + ia], A.Uold[(size_t)d * n + ib],
+                             A.Uold[(size_t)d * n + id]);
+        gT[d] = t.v;
+        gR[d] = r.v;
+        if (u.present) div += u.v;
+    }
+    double dot = 0;
+#pragma unroll
+    for (int k = 0; k < 3; k++) dot += gT[k] * gR[k];
+    return heat_source_value_my(P, ri, Ti, dot, div);
+}
+
+// myMRT steps: rho_n and sum g''_n of every node (pull, boundary program,
+// sums), so the fused kernel can take the heat source, T_n = sum g'' + S/2
+// and psi of its ring from them (the heat source of a ring node needs rho_n
+// one node further out).
+template <bool F_ON, bool HAS_BC>
+__global__ void __launch_bounds__(256) k_pullsum_d2q9(Params P, FusedArgs A) {
+    const uint32_t id = blockIdx.x * blockDim.x + threadIdx.x;
+    if (id >= P.n) return;
+    const int x = (int)(id % (uint32_t)A.nx), y = (int)(id / (uint32_t)A.nx);
+    double f[9], g[9], rho, T;
+    pull_node<D2Q9T, F_ON, true, HAS_BC>(P, A, x, y, 0, id, f, g, rho, T);
+    A.rho_a[id] = rho;
+    A.gsum_a[id] = T;
+}
+
 // The tile: TX x TY nodes, one thread each, plus the one-node ring around it
 // (psi, 1/rho, T_{n-1}, U_{n-1}) computed by the first threads.  INNER
 // tiles skip the wrap / missing-source / boundary bookkeeping; the
 // arithmetic is the same code either way.
 template <int F2_TX, int F2_TY, bool F_ON, bool G_ON, bool HAS_BC, bool EMIT, bool INNER, int EX, int EY, int GX,
-          int GY>
+          int GY, bool MY = false>
 __device__ __forceinline__ void fused2_tile(const Params& P, const FusedArgs& A, int x0, int y0,
                                             double (*s_psi)[EX], double (*s_inv)[GX], double (*s_To)[GX],
                                             double (*s_U0)[GX], double (*s_U1)[GX]) {
@@ -422,6 +482,7 @@ __device__ __forceinline__ void fused2_tile(const Params& P, const FusedArgs& A,
 
     // one ext-grid slot: pull, moments, psi; shared-memory record.  The own
     // slot keeps RN(1/rho) and the density's EOS parts for phase B.
+    double s_own = 0;  // myMRT: heat source of the own node
     auto slot = [&](int ex, int ey, double* f, double* g, double& rho, double& T, uint32_t& id, bool mine,
                     double& rr, EosRho& er) -> bool {
         int x, y;
@@ -434,8 +495,26 @@ __device__ __forceinline__ void fused2_tile(const Params& P, const FusedArgs& A,
             if (x < 0 || y < 0) return false;
         }
         id = (uint32_t)x + (uint32_t)A.nx * (uint32_t)y;
+        if constexpr (MY && !EMIT) {
+            // myMRT step: a ring node's rho_n, sum g'' come from k_pullsum_d2q9
+            if (!mine) {
+                rho = A.rho_a[id];
+                T = A.gsum_a[id] + 0.5 * heat_my<INNER>(P, A, x, y, id);
+                if constexpr (F_ON) s_psi[ey][ex] = potential(P, rho, T);
+                return true;
+            }
+        }
         if constexpr (INNER) pull_node_inner<L, F_ON, G_ON>(P, A, id, f, g, rho, T);
         else pull_node<L, F_ON, G_ON, HAS_BC>(P, A, x, y, 0, id, f, g, rho, T);
+        if constexpr (MY) {
+            // myMRTTemperature.c:22-31: T_n = sum g'' + S_n / 2
+            if constexpr (EMIT) {
+                T = T + 0.5 * A.S[id];
+            } else {
+                s_own = heat_my<INNER>(P, A, x, y, id);
+                T = T + 0.5 * s_own;
+            }
+        }
         if (mine) {
             rr = rcp_rn(rho);
             er = eos_rho(P, rho);
@@ -482,7 +561,8 @@ __device__ __forceinline__ void fused2_tile(const Params& P, const FusedArgs& A,
     const int ex = tx + 1, ey = ty + 1;
     const bool onb = INNER ? false : on_wall(A, gx, gy, 0);
     double heat = 0;
-    if constexpr (G_ON && !EMIT) {
+    if constexpr (MY && !EMIT) heat = s_own;
+    if constexpr (G_ON && !EMIT && !MY) {
         // heatSource.c:119-165 with the one-sided differences of finiteDifference/*.c
         double gT[3] = {0, 0, 0}, gR[3] = {0, 0, 0}, div = 0;
         const double To = s_To[ey][ex], iv = s_inv[ey][ex];
@@ -513,7 +593,7 @@ __device__ __forceinline__ void fused2_tile(const Params& P, const FusedArgs& A,
     double psi = 0;
     if constexpr (F_ON) psi = s_psi[ey][ex];
     auto nbpsi = [&](int k) { return s_psi[ey + cyk<L>(k)][ex + cxk<L>(k)]; };
-    finish_node<L, F_ON, G_ON, EMIT>(P, A, id, onb, f, g, rho, rr, T, psi, nbpsi, heat);
+    finish_node<L, F_ON, G_ON, EMIT, decltype(nbpsi), MY>(P, A, id, onb, f, g, rho, rr, T, psi, nbpsi, heat);
 }
 
 // MINB: resident blocks per SM asked of the register allocator (0 = the
@@ -521,7 +601,10 @@ __device__ __forceinline__ void fused2_tile(const Params& P, const FusedArgs& A,
 // TRY_INNER: the kernel also carries the INNER body for tiles away from the
 // faces; without it the kernel holds the general body alone (a smaller
 // instruction footprint, which a lattice of one wave notices).
-template <int F2_TX, int F2_TY, int MINB, bool F_ON, bool G_ON, bool HAS_BC, bool EMIT, bool TRY_INNER = false>
+// MY: the thermal field is myMRT (T = sum g'' + S/2; non-EMIT steps follow
+// k_pullsum_d2q9).
+template <int F2_TX, int F2_TY, int MINB, bool F_ON, bool G_ON, bool HAS_BC, bool EMIT, bool TRY_INNER = false,
+          bool MY = false>
 __global__ void __launch_bounds__(F2_TX * F2_TY, MINB ? MINB : min_blocks(F2_TX * F2_TY))
     k_fused_d2q9(Params P, FusedArgs A) {
     constexpr int EX = F2_TX + 2, EY = F2_TY + 2;
@@ -535,13 +618,13 @@ __global__ void __launch_bounds__(F2_TX * F2_TY, MINB ? MINB : min_blocks(F2_TX 
     const int x0 = bx * F2_TX, y0 = by * F2_TY;
     if constexpr (TRY_INNER) {
         if (inner_tile<F2_TX, F2_TY>(A, x0, y0)) {
-            fused2_tile<F2_TX, F2_TY, F_ON, G_ON, HAS_BC, EMIT, true, EX, EY, GX, GY>(P, A, x0, y0, s_psi, s_inv,
-                                                                                      s_To, s_U0, s_U1);
+            fused2_tile<F2_TX, F2_TY, F_ON, G_ON, HAS_BC, EMIT, true, EX, EY, GX, GY, MY>(P, A, x0, y0, s_psi, s_inv,
+                                                                                          s_To, s_U0, s_U1);
             return;
         }
     }
-    fused2_tile<F2_TX, F2_TY, F_ON, G_ON, HAS_BC, EMIT, false, EX, EY, GX, GY>(P, A, x0, y0, s_psi, s_inv, s_To,
-                                                                               s_U0, s_U1);
+    fused2_tile<F2_TX, F2_TY, F_ON, G_ON, HAS_BC, EMIT, false, EX, EY, GX, GY, MY>(P, A, x0, y0, s_psi, s_inv, s_To,
+                                                                                   s_U0, s_U1);
 }
 
 // ------------------------------------------------------------ 3D kernels

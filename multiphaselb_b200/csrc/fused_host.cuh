@@ -20,6 +20,7 @@ struct FusedConfig {
     float tune_ms[N_CFG3 > N_CFG2 ? N_CFG3 : N_CFG2] = {};
     int ncfg = 0;
     int nblocks = 0;
+    double* my_scratch = nullptr;  // myMRT: rho_a and gsum_a, 2 n doubles
 };
 
 template <int TX, int TY, bool PIPE, bool HAS_BC, bool EMIT>
@@ -49,14 +50,32 @@ inline cudaError_t fused_attributes() {
     return e;
 }
 
-template <int TX, int TY, int MINB, bool F_ON, bool G_ON, bool EMIT, bool INNER>
+template <int TX, int TY, int MINB, bool F_ON, bool G_ON, bool EMIT, bool INNER, bool MY = false>
 void launch2(bool bc, int nb, const Params& P, const FusedArgs& A, cudaStream_t s) {
-    if (bc) k_fused_d2q9<TX, TY, MINB, F_ON, G_ON, true, EMIT, INNER><<<nb, TX * TY, 0, s>>>(P, A);
-    else k_fused_d2q9<TX, TY, MINB, F_ON, G_ON, false, EMIT, INNER><<<nb, TX * TY, 0, s>>>(P, A);
+    if (bc) k_fused_d2q9<TX, TY, MINB, F_ON, G_ON, true, EMIT, INNER, MY><<<nb, TX * TY, 0, s>>>(P, A);
+    else k_fused_d2q9<TX, TY, MINB, F_ON, G_ON, false, EMIT, INNER, MY><<<nb, TX * TY, 0, s>>>(P, A);
+}
+
+// myMRT steps first fill rho_a, gsum_a (k_pullsum_d2q9).
+template <bool F_ON>
+void launch_pullsum(bool bc, const Params& P, const FusedArgs& A, cudaStream_t s) {
+    const unsigned nb = (P.n + 255) / 256;
+    if (bc) k_pullsum_d2q9<F_ON, true><<<nb, 256, 0, s>>>(P, A);
+    else k_pullsum_d2q9<F_ON, false><<<nb, 256, 0, s>>>(P, A);
 }
 
 template <int TX, int TY, bool EMIT, int MINB = 0, bool INNER = false>
 void launch2_fg(bool fon, bool gon, bool bc, int nb, const Params& P, const FusedArgs& A, cudaStream_t s) {
+    const bool my = gon && P.g_model == MPLB_MYMRT;
+    if (my) {
+        if constexpr (!EMIT) {
+            if (fon) launch_pullsum<true>(bc, P, A, s);
+            else launch_pullsum<false>(bc, P, A, s);
+        }
+        if (fon) launch2<TX, TY, MINB, true, true, EMIT, INNER, true>(bc, nb, P, A, s);
+        else launch2<TX, TY, MINB, false, true, EMIT, INNER, true>(bc, nb, P, A, s);
+        return;
+    }
     if (fon && gon) launch2<TX, TY, MINB, true, true, EMIT, INNER>(bc, nb, P, A, s);
     else if (fon) launch2<TX, TY, MINB, true, false, EMIT, INNER>(bc, nb, P, A, s);
     else if (gon) launch2<TX, TY, MINB, false, true, EMIT, INNER>(bc, nb, P, A, s);
@@ -179,7 +198,6 @@ inline bool fused_supported(int lat, const int* model, const Params& P, const st
     if (!active[0] && !active[1]) { why = "no field is updated"; return false; }
     if (!active[0] && model[0] == MPLB_NO_MODEL) { why = "no flow field"; return false; }
     if (lat == MPLB_D3Q15 && active[1]) { why = "thermal field on D3Q15"; return false; }
-    if (active[1] && model[1] != MPLB_LITEMPMRT) { why = "myMRT thermal field"; return false; }
     for (int fi = 0; fi < 2; fi++) {
         if (!active[fi]) continue;
         for (const PatchDev& pt : fp[fi]) {
@@ -276,6 +294,16 @@ inline int fused_setup(FusedConfig& fc, int lat, const int* model, const Params&
         *bytes += n;
     }
     A.bcmap = fc.bcmap;
+    A.rho_a = A.gsum_a = nullptr;
+    if (lat == MPLB_D2Q9 && model[1] == MPLB_MYMRT && P.g_update) {
+        if (cudaMalloc((void**)&fc.my_scratch, 2 * (size_t)n * sizeof(double)) != cudaSuccess) {
+            fc.err = "cudaMalloc myMRT scratch";
+            return MPLB_E_CUDA;
+        }
+        *bytes += 2 * (size_t)n * sizeof(double);
+        A.rho_a = fc.my_scratch;
+        A.gsum_a = fc.my_scratch + n;
+    }
     fc.lat = lat;
     fc.ncfg = lat == MPLB_D2Q9 ? N_CFG2 : N_CFG3;
     for (int c = 0; c < fc.ncfg; c++) {
@@ -295,6 +323,8 @@ inline int fused_setup(FusedConfig& fc, int lat, const int* model, const Params&
 inline void fused_free(FusedConfig& fc) {
     if (fc.bcmap) cudaFree(fc.bcmap);
     fc.bcmap = nullptr;
+    if (fc.my_scratch) cudaFree(fc.my_scratch);
+    fc.my_scratch = nullptr;
 }
 
 

@@ -1060,6 +1060,8 @@ int mplb_gpu_create(const mplb_mesh_desc* mesh, const mplb_eos_desc* eos, const 
                                                  "fused path unavailable: " + (h->box ? fwhy : std::string("mesh is not a box"))));
     if (h->precision == MPLB_FP32_DEV && h->P.st_on)
         return bail(fail(MPLB_E_UNSUPPORTED, "FP32-deviation storage has no surface-tension term"));
+    if (h->precision == MPLB_FP32_DEV && h->model[1] == MPLB_MYMRT && h->P.g_update)
+        return bail(fail(MPLB_E_UNSUPPORTED, "FP32-deviation storage has no myMRT thermal collision"));
     if (h->precision == MPLB_FP32_DEV && want_path == MPLB_PATH_OPERATORS)
         return bail(fail(MPLB_E_UNSUPPORTED, "FP32-deviation storage runs on the fused path only"));
     h->path = (want_path == MPLB_PATH_OPERATORS || !fusable) ? MPLB_PATH_OPERATORS : MPLB_PATH_FUSED;

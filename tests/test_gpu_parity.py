@@ -156,7 +156,7 @@ def test_serial_boundary_order(gpu_lib):
     assert_same(got, run_checker("port", c2, 6), ctx="serial bc")
 
 
-FUSABLE = ["bubble_d2q9", "column_d2q9", "bubble_d3q15", "walls_d3q15", "st_d2q9", "st_d3q15"]
+FUSABLE = ["bubble_d2q9", "column_d2q9", "bubble_d3q15", "walls_d3q15", "st_d2q9", "st_d3q15", "my_column_d2q9"]
 
 
 @pytest.mark.parametrize("name", FUSABLE)
@@ -209,7 +209,8 @@ def test_fused_frozen_fields(gpu_lib, fu, gu):
     assert_same(got, run_checker("port", c2, 6), ctx=f"fused update f={fu} g={gu}")
 
 
-@pytest.mark.parametrize("name", ["column_d2q9", "bubble_d2q9", "bubble_d3q15", "walls_d3q15", "st_d2q9", "st_d3q15"])
+@pytest.mark.parametrize("name", ["column_d2q9", "bubble_d2q9", "bubble_d3q15", "walls_d3q15", "st_d2q9", "st_d3q15",
+                                  "my_column_d2q9"])
 def test_every_tile_candidate_is_exact(gpu_lib, name):
     """Each fused tile shape (forced) gives the oracle's bits; the autotuner
     then times them all and picks one."""
@@ -261,13 +262,13 @@ def test_surface_tension_rejected_in_fp32(gpu_lib):
     assert e.value.code == abi.E_UNSUPPORTED
 
 
-THERMAL_MY = ["my_column_d2q9", "my_walls_d3q15", "outflow_d2q9", "outflow_corner_d2q9", "outflow_d3q15"]
+OPERATOR_ONLY = ["my_walls_d3q15", "outflow_d2q9", "outflow_corner_d2q9", "outflow_d3q15"]
 
 
-@pytest.mark.parametrize("name", THERMAL_MY)
+@pytest.mark.parametrize("name", OPERATOR_ONLY)
 def test_operator_only_options_select_the_operator_path(gpu_lib, name):
-    """myMRT heat, outflow and fixedRandomT run on the operator path: AUTO
-    picks it on a box, FUSED and the FP32 form say they cannot."""
+    """Outflow, fixedRandomT and a D3Q15 thermal field run on the operator
+    path: AUTO picks it on a box, FUSED and the FP32 form say they cannot."""
     from multiphaselb_b200 import Lattice, MplbError
     case = small_cases()[name]
     _, info = run_gpu(case, 1)
@@ -314,3 +315,15 @@ def test_outflow_without_normal_is_refused(gpu_lib):
     with pytest.raises(MplbError) as e:
         Lattice(c2, path=abi.PATH_OPERATORS)
     assert e.value.code == abi.E_ARG
+
+
+def test_mymrt_column_takes_the_fused_path(gpu_lib):
+    """A D2Q9 myMRT thermal field runs fused (a pull-and-sum pre-kernel, then
+    the fused step); the FP32 form has no myMRT collision and refuses."""
+    from multiphaselb_b200 import Lattice, MplbError
+    case = small_cases()["my_column_d2q9"]
+    _, info = run_gpu(case, 1)
+    assert info["path"] == abi.PATH_FUSED
+    with pytest.raises(MplbError) as e:
+        Lattice(case, path=abi.PATH_AUTO, precision=abi.FP32_DEV)
+    assert e.value.code == abi.E_UNSUPPORTED
