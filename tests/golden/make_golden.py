@@ -25,7 +25,8 @@ from tests.helpers import FIELDS, run_checker, small_cases  # noqa: E402
 
 STEPS = {"bubble_d2q9": 12, "column_d2q9": 12, "lid_d2q9": 9, "bubble_d3q15": 5, "walls_d3q15": 5,
          "st_d2q9": 10, "st_d3q15": 5, "my_column_d2q9": 9, "my_walls_d3q15": 5, "outflow_d2q9": 8,
-         "outflow_corner_d2q9": 6, "outflow_d3q15": 5, "cylinder_d2q9": 8}
+         "outflow_corner_d2q9": 6, "outflow_d3q15": 5, "cylinder_d2q9": 8,
+         "my_slab_d3q15": 6}
 
 
 def save_case(path, case, steps, out):

@@ -24,7 +24,21 @@ def small_cases():
         "outflow_corner_d2q9": outflow_corner_d2q9(),
         "outflow_d3q15": outflow_d3q15(),
         "cylinder_d2q9": cylinder_d2q9(),
+        "my_slab_d3q15": mymrt_slab_d3q15(),
     }
+
+
+def mymrt_slab_d3q15():
+    """D3Q15 bubble in a slab: periodic x and y, bounce-back z walls for the
+    flow, fixedT z walls (hot bottom, cold top) for the myMRT heat, gravity
+    along -z; no node lies on two patches, so the fused path takes it."""
+    c = thermal_box(abi.D3Q15, (6, 5, 7), (True, True, False))
+    T0 = c.meta["T"]
+    c.f = dict(c.f, bc_type=[abi.BC_BOUNCEBACK] * 2, bc_value=np.zeros((2, 3)))
+    c.g = mymrt(abi.D3Q15, [abi.BC_FIXEDT, abi.BC_FIXEDT], [(1.02 * T0, 0, 0), (0.98 * T0, 0, 0)])
+    c.eos = dict(c.eos, g=(0.0, 0.0, -1e-5), rho_0=0.0)
+    c.name = "my_slab_d3q15_6x5x7"
+    return cases.perturbed(c, du=1e-3)
 
 
 def cylinder_d2q9():

@@ -262,7 +262,7 @@ def test_surface_tension_rejected_in_fp32(gpu_lib):
     assert e.value.code == abi.E_UNSUPPORTED
 
 
-OPERATOR_ONLY = ["my_walls_d3q15", "outflow_d2q9", "outflow_corner_d2q9", "outflow_d3q15"]
+OPERATOR_ONLY = ["outflow_d2q9", "outflow_corner_d2q9", "outflow_d3q15", "my_slab_d3q15"]
 
 
 @pytest.mark.parametrize("name", OPERATOR_ONLY)
@@ -317,11 +317,12 @@ def test_outflow_without_normal_is_refused(gpu_lib):
     assert e.value.code == abi.E_ARG
 
 
-def test_mymrt_column_takes_the_fused_path(gpu_lib):
+@pytest.mark.parametrize("name", ["my_column_d2q9"])
+def test_mymrt_takes_the_fused_path(gpu_lib, name):
     """A D2Q9 myMRT thermal field runs fused (a pull-and-sum pre-kernel, then
     the fused step); the FP32 form has no myMRT collision and refuses."""
     from multiphaselb_b200 import Lattice, MplbError
-    case = small_cases()["my_column_d2q9"]
+    case = small_cases()[name]
     _, info = run_gpu(case, 1)
     assert info["path"] == abi.PATH_FUSED
     with pytest.raises(MplbError) as e:
