@@ -66,6 +66,36 @@ struct FusedArgs {
     BCProg prog[FUSED_MAX_PROGS];
 };
 
+// ------------------------------------------------------- dependent launch
+// Fused steps are launched with programmatic stream serialization: a step's
+// grid may be scheduled while the previous step drains.  Every kernel waits
+// for the previous grid to complete (and its writes to be visible) before it
+// reads anything, then lets the next step's grid be scheduled.  Launched
+// without the attribute, the wait returns at once.
+__device__ __forceinline__ void step_dependency_wait() {
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+
+// A fused-step launch with programmatic stream serialization (the kernels
+// start with step_dependency_wait).  Launch errors surface through
+// cudaGetLastError, which every caller checks.
+template <class... KArgs, class... Args>
+void launch_step(void (*kernel)(KArgs...), unsigned grid, unsigned block, size_t smem, cudaStream_t s,
+                 Args... args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(grid);
+    cfg.blockDim = dim3(block);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = s;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    cudaLaunchKernelEx(&cfg, kernel, args...);
+}
+
 // ------------------------------------------------------------- geometry
 // Wrap a coordinate one step outside [0, ext): periodic -> wrapped,
 // walled -> -1 (absent).  Inputs are within [-1, ext].
@@ -457,6 +487,7 @@ __device__ __forceinline__ double heat_my(const Params& P, const FusedArgs& A, i
 // one node further out).
 template <bool F_ON, bool HAS_BC>
 __global__ void __launch_bounds__(256) k_pullsum_d2q9(Params P, FusedArgs A) {
+    step_dependency_wait();
     const uint32_t id = blockIdx.x * blockDim.x + threadIdx.x;
     if (id >= P.n) return;
     const int x = (int)(id % (uint32_t)A.nx), y = (int)(id / (uint32_t)A.nx);
@@ -607,6 +638,7 @@ template <int F2_TX, int F2_TY, int MINB, bool F_ON, bool G_ON, bool HAS_BC, boo
           bool MY = false>
 __global__ void __launch_bounds__(F2_TX * F2_TY, MINB ? MINB : min_blocks(F2_TX * F2_TY))
     k_fused_d2q9(Params P, FusedArgs A) {
+    step_dependency_wait();
     constexpr int EX = F2_TX + 2, EY = F2_TY + 2;
     constexpr int GY = G_ON ? EY : 1, GX = G_ON ? EX : 1;
     __shared__ double s_psi[EY][EX];
@@ -641,6 +673,7 @@ constexpr size_t f3_smem() {
 
 template <int F3_TX, int F3_TY, bool HAS_BC, bool EMIT>
 __global__ void __launch_bounds__(F3_TX * F3_TY, min_blocks(F3_TX * F3_TY)) k_fused_d3q15(Params P, FusedArgs A) {
+    step_dependency_wait();
     using L = D3Q15T;
     constexpr int EX = F3_TX + 2, EY = F3_TY + 2, NT = F3_TX * F3_TY, NRING = 2 * EX + 2 * F3_TY;
     extern __shared__ double dsm[];
@@ -732,6 +765,7 @@ __device__ __forceinline__ void cp_async_wait1() { asm volatile("cp.async.wait_g
 
 template <int F3_TX, int F3_TY, bool HAS_BC, bool EMIT>
 __global__ void __launch_bounds__(F3_TX * F3_TY, min_blocks(F3_TX * F3_TY)) k_fused_d3q15_pipe(Params P, FusedArgs A) {
+    step_dependency_wait();
     using L = D3Q15T;
     constexpr int EX = F3_TX + 2, EY = F3_TY + 2, NT = F3_TX * F3_TY, NRING = 2 * EX + 2 * F3_TY;
     extern __shared__ double dsm[];

@@ -52,16 +52,16 @@ inline cudaError_t fused_attributes() {
 
 template <int TX, int TY, int MINB, bool F_ON, bool G_ON, bool EMIT, bool INNER, bool MY = false>
 void launch2(bool bc, int nb, const Params& P, const FusedArgs& A, cudaStream_t s) {
-    if (bc) k_fused_d2q9<TX, TY, MINB, F_ON, G_ON, true, EMIT, INNER, MY><<<nb, TX * TY, 0, s>>>(P, A);
-    else k_fused_d2q9<TX, TY, MINB, F_ON, G_ON, false, EMIT, INNER, MY><<<nb, TX * TY, 0, s>>>(P, A);
+    if (bc) launch_step(k_fused_d2q9<TX, TY, MINB, F_ON, G_ON, true, EMIT, INNER, MY>, nb, TX * TY, 0, s, P, A);
+    else launch_step(k_fused_d2q9<TX, TY, MINB, F_ON, G_ON, false, EMIT, INNER, MY>, nb, TX * TY, 0, s, P, A);
 }
 
 // myMRT steps first fill rho_a, gsum_a (k_pullsum_d2q9).
 template <bool F_ON>
 void launch_pullsum(bool bc, const Params& P, const FusedArgs& A, cudaStream_t s) {
     const unsigned nb = (P.n + 255) / 256;
-    if (bc) k_pullsum_d2q9<F_ON, true><<<nb, 256, 0, s>>>(P, A);
-    else k_pullsum_d2q9<F_ON, false><<<nb, 256, 0, s>>>(P, A);
+    if (bc) launch_step(k_pullsum_d2q9<F_ON, true>, nb, 256, 0, s, P, A);
+    else launch_step(k_pullsum_d2q9<F_ON, false>, nb, 256, 0, s, P, A);
 }
 
 template <int TX, int TY, bool EMIT, int MINB = 0, bool INNER = false>
@@ -85,11 +85,11 @@ template <int TX, int TY, bool PIPE, bool EMIT>
 void launch3(bool bc, int nb, const Params& P, const FusedArgs& A, cudaStream_t s) {
     constexpr size_t sm = f3_smem<TX, TY, PIPE>();
     if constexpr (PIPE) {
-        if (bc) k_fused_d3q15_pipe<TX, TY, true, EMIT><<<nb, TX * TY, sm, s>>>(P, A);
-        else k_fused_d3q15_pipe<TX, TY, false, EMIT><<<nb, TX * TY, sm, s>>>(P, A);
+        if (bc) launch_step(k_fused_d3q15_pipe<TX, TY, true, EMIT>, nb, TX * TY, sm, s, P, A);
+        else launch_step(k_fused_d3q15_pipe<TX, TY, false, EMIT>, nb, TX * TY, sm, s, P, A);
     } else {
-        if (bc) k_fused_d3q15<TX, TY, true, EMIT><<<nb, TX * TY, sm, s>>>(P, A);
-        else k_fused_d3q15<TX, TY, false, EMIT><<<nb, TX * TY, sm, s>>>(P, A);
+        if (bc) launch_step(k_fused_d3q15<TX, TY, true, EMIT>, nb, TX * TY, sm, s, P, A);
+        else launch_step(k_fused_d3q15<TX, TY, false, EMIT>, nb, TX * TY, sm, s, P, A);
     }
 }
 

@@ -131,6 +131,7 @@ template <int TX, int TY, bool F_ON, bool G_ON, bool HAS_BC, bool EMIT, int MINB
 __global__ void __launch_bounds__(TX * TY, MINB ? MINB : min_blocks(TX * TY))
     k_fused32_d2q9(Params P, FusedArgs32 A, double* emit_f, double* emit_g, double* rho_out, double* Fi_out,
                    double* Ft_out) {
+    step_dependency_wait();
     __shared__ Smem32<TX, TY, G_ON> sm;
     const int bx = blockIdx.x % A.tiles_x, by = blockIdx.x / A.tiles_x;
     if constexpr (TRY_INNER) {
@@ -160,6 +161,7 @@ constexpr size_t f3_smem32() {
 template <int TX, int TY, bool HAS_BC, bool EMIT>
 __global__ void __launch_bounds__(TX * TY, min_blocks(TX * TY))
     k_fused32_d3q15(Params P, FusedArgs32 A, double* emit_f, double* rho_out, double* Fi_out, double* Ft_out) {
+    step_dependency_wait();
     using L = D3Q15T;
     constexpr int EX = TX + 2, EY = TY + 2, NT = TX * TY, NRING = 2 * EX + 2 * TY;
     extern __shared__ double dsm[];
@@ -299,11 +301,11 @@ cudaError_t mplb_fused32_launch(int lat, bool has_bc, bool f_on, bool g_on, bool
         B.tiles_y = g.tiles_y;
         B.zchunk = 1;
         const bool big = !emit && g.nblocks > F32_INNER_MIN_TILES;
-#define MPLB_L32(F, G, BC, E)                                                                                    \
-    (big ? (k_fused32_d2q9<32, 8, F, G, BC, E, 3, true><<<g.nblocks, 256, 0, s>>>(P, B, emit_f, emit_g, rho_out, \
-                                                                                   Fi_out, Ft_out), 0)          \
-         : (k_fused32_d2q9<32, 8, F, G, BC, E><<<g.nblocks, 256, 0, s>>>(P, B, emit_f, emit_g, rho_out, Fi_out,  \
-                                                                        Ft_out), 0))
+#define MPLB_L32(F, G, BC, E)                                                                              \
+    (big ? (launch_step(k_fused32_d2q9<32, 8, F, G, BC, E, 3, true>, g.nblocks, 256, 0, s, P, B, emit_f, emit_g, \
+                        rho_out, Fi_out, Ft_out), 0)                                                              \
+         : (launch_step(k_fused32_d2q9<32, 8, F, G, BC, E>, g.nblocks, 256, 0, s, P, B, emit_f, emit_g, rho_out,  \
+                        Fi_out, Ft_out), 0))
 #define MPLB_L32_E(F, G, BC) (emit ? (MPLB_L32(F, G, BC, true), 0) : (MPLB_L32(F, G, BC, false), 0))
 #define MPLB_L32_B(F, G) (has_bc ? MPLB_L32_E(F, G, true) : MPLB_L32_E(F, G, false))
         if (f_on && g_on) MPLB_L32_B(true, true);
@@ -318,13 +320,13 @@ cudaError_t mplb_fused32_launch(int lat, bool has_bc, bool f_on, bool g_on, bool
         if (emit) {
             const Geom g = fused_geometry(MPLB_D3Q15, tmp, 32, 8);
             B.tiles_x = g.tiles_x; B.tiles_y = g.tiles_y; B.zchunk = g.zchunk;
-            if (has_bc) k_fused32_d3q15<32, 8, true, true><<<g.nblocks, 256, f3_smem32<32, 8>(), s>>>(P, B, emit_f, rho_out, Fi_out, Ft_out);
-            else k_fused32_d3q15<32, 8, false, true><<<g.nblocks, 256, f3_smem32<32, 8>(), s>>>(P, B, emit_f, rho_out, Fi_out, Ft_out);
+            if (has_bc) launch_step(k_fused32_d3q15<32, 8, true, true>, g.nblocks, 256, f3_smem32<32, 8>(), s, P, B, emit_f, rho_out, Fi_out, Ft_out);
+            else launch_step(k_fused32_d3q15<32, 8, false, true>, g.nblocks, 256, f3_smem32<32, 8>(), s, P, B, emit_f, rho_out, Fi_out, Ft_out);
         } else {
             const Geom g = fused_geometry(MPLB_D3Q15, tmp, 32, 4);
             B.tiles_x = g.tiles_x; B.tiles_y = g.tiles_y; B.zchunk = g.zchunk;
-            if (has_bc) k_fused32_d3q15<32, 4, true, false><<<g.nblocks, 128, f3_smem32<32, 4>(), s>>>(P, B, emit_f, rho_out, Fi_out, Ft_out);
-            else k_fused32_d3q15<32, 4, false, false><<<g.nblocks, 128, f3_smem32<32, 4>(), s>>>(P, B, emit_f, rho_out, Fi_out, Ft_out);
+            if (has_bc) launch_step(k_fused32_d3q15<32, 4, true, false>, g.nblocks, 128, f3_smem32<32, 4>(), s, P, B, emit_f, rho_out, Fi_out, Ft_out);
+            else launch_step(k_fused32_d3q15<32, 4, false, false>, g.nblocks, 128, f3_smem32<32, 4>(), s, P, B, emit_f, rho_out, Fi_out, Ft_out);
         }
     }
     return cudaGetLastError();
