@@ -575,4 +575,35 @@ MPLB_HD double heat_source_value_er(const Params& P, const EosRho& er, double rh
     return s + 0.5 * (s - oldss);
 }
 
+// ------------------------------------------------------- dependent launch
+// Step kernels (fused steps and the operator kernels of a step) are launched
+// with programmatic stream serialization: a kernel's grid may be scheduled
+// while the previous kernel drains.  Every kernel waits
+// for the previous grid to complete (and its writes to be visible) before it
+// reads anything, then lets the next step's grid be scheduled.  Launched
+// without the attribute, the wait returns at once.
+__device__ __forceinline__ void step_dependency_wait() {
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+
+// A fused-step launch with programmatic stream serialization (the kernels
+// start with step_dependency_wait).  Launch errors surface through
+// cudaGetLastError, which every caller checks.
+template <class... KArgs, class... Args>
+void launch_step(void (*kernel)(KArgs...), unsigned grid, unsigned block, size_t smem, cudaStream_t s,
+                 Args... args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(grid);
+    cfg.blockDim = dim3(block);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = s;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    cudaLaunchKernelEx(&cfg, kernel, args...);
+}
+
 }  // namespace mplb

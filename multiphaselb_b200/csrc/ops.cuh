@@ -23,6 +23,7 @@ struct PatchDev {
 template <class L>
 __global__ void k_equilibrium_flow(Params P, double* __restrict__ f, const double* __restrict__ rho,
                                    const double* __restrict__ U) {
+    step_dependency_wait();
     uint32_t n = P.n, id = blockIdx.x * blockDim.x + threadIdx.x;
     if (id >= n) return;
     double v[3] = {U[id], U[n + id], U[2 * n + id]};
@@ -34,6 +35,7 @@ __global__ void k_equilibrium_flow(Params P, double* __restrict__ f, const doubl
 template <class L>
 __global__ void k_equilibrium_heat(Params P, double* __restrict__ g, const double* __restrict__ T,
                                    const double* __restrict__ U) {
+    step_dependency_wait();
     uint32_t n = P.n, id = blockIdx.x * blockDim.x + threadIdx.x;
     if (id >= n) return;
     double v[L::Q];
@@ -54,6 +56,7 @@ __global__ void k_collide_flow(Params P, double* __restrict__ f, const double* _
                                const double* __restrict__ U, const double* __restrict__ T,
                                const double* __restrict__ Fi, const double* __restrict__ Ft,
                                const int32_t* __restrict__ nb) {
+    step_dependency_wait();
     uint32_t n = P.n, id = blockIdx.x * blockDim.x + threadIdx.x;
     if (id >= n) return;
     double v[L::Q];
@@ -96,6 +99,7 @@ __global__ void k_collide_flow(Params P, double* __restrict__ f, const double* _
 template <class L>
 __global__ void k_collide_heat(Params P, double* __restrict__ g, const double* __restrict__ T,
                                const double* __restrict__ U, const double* __restrict__ S) {
+    step_dependency_wait();
     uint32_t n = P.n, id = blockIdx.x * blockDim.x + threadIdx.x;
     if (id >= n) return;
     double v[L::Q];
@@ -116,6 +120,7 @@ __global__ void k_collide_heat(Params P, double* __restrict__ g, const double* _
 template <int Q>
 __global__ void k_stream(uint32_t n, double* __restrict__ out, const double* __restrict__ in,
                          const int32_t* __restrict__ nb) {
+    step_dependency_wait();
     uint32_t id = blockIdx.x * blockDim.x + threadIdx.x;
     if (id >= n) return;
 #pragma unroll
@@ -131,6 +136,7 @@ __global__ void k_stream(uint32_t n, double* __restrict__ out, const double* __r
 template <int Q>
 __global__ void k_moment0(uint32_t n, double* __restrict__ out, const double* __restrict__ pdf,
                           uint32_t start, uint32_t end) {
+    step_dependency_wait();
     uint32_t id = start + blockIdx.x * blockDim.x + threadIdx.x;
     if (id >= end) return;
     double s = 0;
@@ -143,6 +149,7 @@ __global__ void k_moment0(uint32_t n, double* __restrict__ out, const double* __
 template <int Q>
 __global__ void k_temperature_my(uint32_t n, double* __restrict__ T, const double* __restrict__ g,
                                  const double* __restrict__ S, uint32_t start, uint32_t end) {
+    step_dependency_wait();
     uint32_t id = start + blockIdx.x * blockDim.x + threadIdx.x;
     if (id >= end) return;
     double s = 0;
@@ -156,6 +163,7 @@ template <class L>
 __global__ void k_velocity(Params P, double* __restrict__ U, const double* __restrict__ f,
                            const double* __restrict__ rho, const double* __restrict__ Fi,
                            const double* __restrict__ Ft, uint32_t start, uint32_t end) {
+    step_dependency_wait();
     uint32_t n = P.n, id = start + blockIdx.x * blockDim.x + threadIdx.x;
     if (id >= end) return;
     double v[L::Q];
@@ -181,6 +189,7 @@ template <class L>
 __global__ void k_interforce(Params P, double* __restrict__ Fi, double* __restrict__ Ft,
                              const double* __restrict__ rho, const double* __restrict__ T,
                              const int32_t* __restrict__ nb, const uint8_t* __restrict__ onb) {
+    step_dependency_wait();
     uint32_t n = P.n, id = blockIdx.x * blockDim.x + threadIdx.x;
     if (id >= n) return;
     double Ff[3] = {0, 0, 0};
@@ -230,6 +239,7 @@ template <class L>
 __global__ void k_heatsource(Params P, double* __restrict__ S, const double* __restrict__ rho,
                              const double* __restrict__ T, const double* __restrict__ U,
                              const int32_t* __restrict__ nb, int first) {
+    step_dependency_wait();
     uint32_t n = P.n, id = blockIdx.x * blockDim.x + threadIdx.x;
     if (id >= n) return;
     double gT[3] = {0, 0, 0}, gR[3] = {0, 0, 0}, div = 0;
@@ -441,6 +451,7 @@ __global__ void k_bc_patch(Params P, PatchDev pt, int model, const uint32_t* __r
                            const double* __restrict__ rho, const double* __restrict__ T,
                            const double* __restrict__ U, const double* __restrict__ Fi,
                            const double* __restrict__ tab, int rnd) {
+    step_dependency_wait();
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= pt.count) return;
     bc_node<L>(P, pt, model, nodes[pt.off + i], pdf, nb, rho, T, U, Fi, tab, pt.off + i, rnd != 0);
@@ -456,6 +467,7 @@ __global__ void k_bc_serial(Params P, const PatchDev* __restrict__ pts, int npat
                             const double* __restrict__ T, const double* __restrict__ U,
                             const double* __restrict__ Fi, const double* __restrict__ tab,
                             unsigned long long rnd_mask) {
+    step_dependency_wait();
     if (blockIdx.x != 0 || threadIdx.x != 0) return;
     for (int p = 0; p < npatch; p++) {
         PatchDev pt = pts[p];
