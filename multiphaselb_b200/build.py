@@ -77,17 +77,7 @@ def build(force=False, verbose=False, extra=()):
     if not force and not needs_build():
         return LIB
     os.makedirs(LIB_DIR, exist_ok=True)
-    objs = []
-    import concurrent.futures as cf
-    jobs = []
-    for src, fmad in SOURCES:
-        obj = os.path.join(LIB_DIR, os.path.basename(src) + ".o")
-        cmd = [nvcc()] + NVCC_FLAGS + ["-fmad=" + ("true" if fmad else "false")] + list(extra) + \
-              ["-I", os.path.join(ROOT, "include"), "-c", "-o", obj, src]
-        jobs.append(cmd)
-        objs.append(obj)
-    with cf.ThreadPoolExecutor(max_workers=len(jobs)) as ex:
-        list(ex.map(lambda c: _run(c, verbose), jobs))
+    objs = compile_objects(LIB_DIR, verbose=verbose, extra=extra)
     _run([nvcc(), "-gencode", "arch=compute_100a,code=sm_100a", "-shared", "-Xcompiler", "-fPIC", "-o", LIB] + objs,
          verbose)
     for o in objs:
