@@ -192,7 +192,7 @@ def cpu_baseline(workload, steps, procs):
     wall = time.perf_counter() - t0
     lups = sum(r[0] for r in res)
     slowest = max(r[1] for r in res)
-    return dict(value=lups / slowest / 1e9, unit="GLUPS", cores=procs,
+    return dict(value=lups / slowest / 1e9, unit="GLUPS", cores=procs, step_ms=slowest / max(steps, 1) * 1e3,
                 kind="reference" if kind == "ref" else "port",
                 sample=f"{steps} steps of the full {WORKLOADS[workload]['desc']} lattice per core, "
                        f"{procs} independent single-threaded copies (the reference has no threads; its "
@@ -340,18 +340,21 @@ def run_reference(a):
         return
     procs = a.cpu_procs or max(1, (os.cpu_count() or 1))
     procs = min(procs, 64)
+    # one step = one time step of the full lattice on every core; K is capped
+    # so that the run stays within minutes (a reference step of the column
+    # takes about 25 ms on one core)
+    steps = max(1, min(a.steps, a.ref_max_steps))
     samples = []
-    for _ in range(a.warmup and 1 or 0):
-        cpu_baseline(a.workload, max(1, a.cpu_steps // 10), procs)
+    cpu_baseline(a.workload, max(1, min(a.warmup, 20)), procs)  # warm-up: process start, page-in
     t0 = time.perf_counter()
     for _ in range(max(1, a.ref_repeats)):
-        samples.append(cpu_baseline(a.workload, a.cpu_steps, procs))
+        samples.append(cpu_baseline(a.workload, steps, procs))
     wall = time.perf_counter() - t0
     best = samples[-1]
     v = statistics.median(s["value"] for s in samples)
     line = {
-        "metric": METRIC, "value": round(v, 6), "unit": "GLUPS", "n_gpus": world, "steps": a.cpu_steps,
-        "warmup": a.warmup, "ms_per_step": None, "higher_is_better": True, "scaling": "weak",
+        "metric": METRIC, "value": round(v, 6), "unit": "GLUPS", "n_gpus": world, "steps": steps,
+        "warmup": a.warmup, "ms_per_step": round(best["step_ms"], 4), "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded lattice of the named shape)",
         "impl": "reference",
         "config": {"workload": a.workload, "desc": WORKLOADS[a.workload]["desc"],
@@ -361,6 +364,8 @@ def run_reference(a):
         "e2e": {"value": round(v, 6), "unit": "GLUPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         "wall_s": round(wall, 2),
     }
+    if steps != a.steps:
+        line["steps_requested"] = a.steps
     print(json.dumps(line), flush=True)
 
 
@@ -375,6 +380,8 @@ def main():
     ap.add_argument("--cpu-steps", type=int, default=150)
     ap.add_argument("--cpu-procs", type=int, default=0)
     ap.add_argument("--ref-repeats", type=int, default=1)
+    ap.add_argument("--ref-max-steps", type=int, default=3000,
+                    help="reference arm: at most this many steps per core (keeps the run within minutes)")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-fp32", action="store_true")
     a = ap.parse_args()
