@@ -39,7 +39,7 @@
 extern "C" {
 #endif
 
-#define MPLB_ABI_VERSION 1
+#define MPLB_ABI_VERSION 2  /* 2: mplb_field_desc.alpha_1/alpha_2, mplb_opts.rank */
 #define MPLB_MAX_Q 15
 #define MPLB_MAX_PATCHES 64
 

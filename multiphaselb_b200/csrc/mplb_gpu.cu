@@ -51,6 +51,9 @@ cudaError_t mplb_batch32_fix(int cfg, const FusedArgs32* dA, const int2* tiles, 
 cudaError_t mplb_mom_sum32(int lat, uint32_t n, const float* f, long long* J, cudaStream_t s);
 cudaError_t mplb_mom_fix32(int lat, uint32_t n, float* f, const long long* J, const long long* J0, cudaStream_t s);
 
+#define MPLB_STR2(x) #x
+#define MPLB_STR(x) MPLB_STR2(x)
+
 namespace {
 
 thread_local std::string g_err = "";
@@ -825,7 +828,7 @@ int mplb_internal_fail(int code, const std::string& msg) { return fail(code, msg
 // ================================================================= C-ABI
 extern "C" {
 
-const char* mplb_gpu_version(void) { return "multiphaselb-b200 1 (sm_100a, FP64)"; }
+const char* mplb_gpu_version(void) { return "multiphaselb-b200 ABI " MPLB_STR(MPLB_ABI_VERSION) " (sm_100a, FP64)"; }
 const char* mplb_gpu_last_error(void) { return g_err.c_str(); }
 
 int mplb_gpu_create(const mplb_mesh_desc* mesh, const mplb_eos_desc* eos, const mplb_field_desc* f,
