@@ -1348,7 +1348,7 @@ int mplb_gpu_snapshot_write(mplb_gpu_t* h, const char* root, int32_t pid, int32_
         return fail(MPLB_E_ARG, "unknown data format");
     writer_wait(h);
     std::string dir = root ? root : "";
-    h->writer = std::thread([h, dir, pid, format]() {
+    auto job = [h, dir, pid, format]() {
         int rc = 0;
         std::string err;
         cudaSetDevice(h->dev);
@@ -1375,7 +1375,12 @@ int mplb_gpu_snapshot_write(mplb_gpu_t* h, const char* root, int32_t pid, int32_
             h->writer_rc = rc;
             h->writer_err = err;
         }
-    });
+    };
+    try {
+        h->writer = std::thread(job);
+    } catch (const std::exception& e) {
+        return fail(MPLB_E_STATE, std::string("cannot start the writer thread: ") + e.what());
+    }
     return 0;
 }
 

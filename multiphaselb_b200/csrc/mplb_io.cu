@@ -122,9 +122,17 @@ bool write_chunked(std::FILE* fp, const double* v, uint64_t n, uint32_t vs, bool
         if (threads == 1) {
             work(c0, c1, 0);
         } else {
+            // a worker that cannot be started leaves its chunks to this thread
             std::vector<std::thread> pool;
-            for (int w = 1; w < threads; w++) pool.emplace_back(work, c0, c1, w);
-            work(c0, c1, 0);
+            std::vector<int> mine(1, 0);
+            for (int w = 1; w < threads; w++) {
+                try {
+                    pool.emplace_back(work, c0, c1, w);
+                } catch (...) {
+                    mine.push_back(w);
+                }
+            }
+            for (int w : mine) work(c0, c1, w);
             for (auto& th : pool) th.join();
         }
         for (uint64_t c = c0; c < c1; c++) {
