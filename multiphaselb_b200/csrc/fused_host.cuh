@@ -138,7 +138,8 @@ inline cudaError_t fused_launch(const FusedConfig& fc, const Params& P, const Fu
     return fused_launch_cfg(fc, fc.cfg, P, A, f_on, g_on, emit, s);
 }
 
-// Time every candidate on the current state (2 warm-up + 3 timed launches)
+// Time every candidate on the current state (2 warm-up launches, then the
+// median of 10)
 // and keep the fastest.  The step's outputs are rewritten by the real launch
 // that follows; the heat-source history S, updated in place, is saved to
 // `save` before and restored after every trial.
@@ -154,26 +155,35 @@ inline int fused_autotune(FusedConfig& fc, const Params& P, const FusedArgs& A, 
         fc.err = "autotune: saving S failed";
         return MPLB_E_CUDA;
     }
+    // 2 warm-up launches, then the median of 10 timed ones (a one-wave
+    // lattice's step is ~10 us: a few launches give a noisy pick)
+    constexpr int WARM = 2, TIMED = 10;
     float best = 1e30f;
     int best_cfg = 0;
     for (int c = 0; c < fc.ncfg; c++) {
-        float tot = 0;
+        float ms_r[TIMED];
+        int nt = 0;
         bool ok = true;
-        for (int r = 0; r < 5 && ok; r++) {
-            if (r >= 2) cudaEventRecord(e0, s);
+        for (int r = 0; r < WARM + TIMED && ok; r++) {
+            if (r >= WARM) cudaEventRecord(e0, s);
             ok = fused_launch_cfg(fc, c, P, A, f_on, g_on, false, s) == cudaSuccess;
-            if (r >= 2) {
+            if (r >= WARM) {
                 cudaEventRecord(e1, s);
                 cudaEventSynchronize(e1);
                 float ms = 0;
                 cudaEventElapsedTime(&ms, e0, e1);
-                tot += ms;
+                ms_r[nt++] = ms;
             }
             if (keep_s) cudaMemcpyAsync(S, save, n * sizeof(double), cudaMemcpyDeviceToDevice, s);
         }
-        fc.tune_ms[c] = ok ? tot / 3 : -1.0f;
-        if (ok && tot < best) {
-            best = tot;
+        float med = -1.0f;
+        if (ok && nt == TIMED) {
+            std::sort(ms_r, ms_r + nt);
+            med = 0.5f * (ms_r[nt / 2 - 1] + ms_r[nt / 2]);
+        }
+        fc.tune_ms[c] = ok ? med : -1.0f;
+        if (ok && med >= 0 && med < best) {
+            best = med;
             best_cfg = c;
         }
     }

@@ -576,9 +576,11 @@ MPLB_HD double heat_source_value_er(const Params& P, const EosRho& er, double rh
 }
 
 // ------------------------------------------------------- dependent launch
-// Step kernels (fused steps and the operator kernels of a step) are launched
-// with programmatic stream serialization: a kernel's grid may be scheduled
-// while the previous kernel drains.  Every kernel waits
+// Fused step kernels are launched with programmatic stream serialization: a
+// step's grid may be scheduled while the previous step drains.  Only kernels
+// whose inputs come through plain (non-restrict) pointers and __ldg take part:
+// a load through a const __restrict__ parameter may be compiled as an
+// invariant load, which the compiler is free to move above the wait.  Every kernel waits
 // for the previous grid to complete (and its writes to be visible) before it
 // reads anything, then lets the next step's grid be scheduled.  Launched
 // without the attribute, the wait returns at once.

@@ -487,15 +487,6 @@ int launch_check(mplb_gpu* h) {
     return 0;
 }
 
-// Step-operator kernels (each starts with step_dependency_wait) are
-// launched with programmatic stream serialization.
-#define LAUNCH_STEP(kernel, grid, ...)                                       \
-    do {                                                                     \
-        launch_step(kernel, (grid), TPB, 0, h->stream, __VA_ARGS__);         \
-        h->launches++;                                                       \
-        if (int rc_ = launch_check(h)) return rc_;                           \
-    } while (0)
-
 #define LAUNCH(kernel, grid, ...)                                    \
     do {                                                             \
         kernel<<<(grid), TPB, 0, h->stream>>>(__VA_ARGS__);          \
@@ -507,16 +498,16 @@ int launch_check(mplb_gpu* h) {
 template <class L>
 int op_equilibrium(mplb_gpu* h, int fi) {
     if (h->model[fi] == MPLB_NO_MODEL || !(fi == 0 ? h->P.f_update : h->P.g_update)) return 0;
-    if (fi == 0) LAUNCH_STEP(k_equilibrium_flow<L>, blocks(h->n), h->P, h->F(), h->rho, h->U);
-    else LAUNCH_STEP(k_equilibrium_heat<L>, blocks(h->n), h->P, h->G(), h->T, h->U);
+    if (fi == 0) LAUNCH(k_equilibrium_flow<L>, blocks(h->n), h->P, h->F(), h->rho, h->U);
+    else LAUNCH(k_equilibrium_heat<L>, blocks(h->n), h->P, h->G(), h->T, h->U);
     return 0;
 }
 
 template <class L>
 int op_collision(mplb_gpu* h, int fi) {
     if (h->model[fi] == MPLB_NO_MODEL || !(fi == 0 ? h->P.f_update : h->P.g_update)) return 0;
-    if (fi == 0) LAUNCH_STEP(k_collide_flow<L>, blocks(h->n), h->P, h->F(), h->rho, h->U, h->T, h->Fi, h->Ft, h->nb);
-    else LAUNCH_STEP(k_collide_heat<L>, blocks(h->n), h->P, h->G(), h->T, h->U, h->S);
+    if (fi == 0) LAUNCH(k_collide_flow<L>, blocks(h->n), h->P, h->F(), h->rho, h->U, h->T, h->Fi, h->Ft, h->nb);
+    else LAUNCH(k_collide_heat<L>, blocks(h->n), h->P, h->G(), h->T, h->U, h->S);
     return 0;
 }
 
@@ -525,7 +516,7 @@ int op_stream(mplb_gpu* h, int fi) {
     if (h->model[fi] == MPLB_NO_MODEL || !(fi == 0 ? h->P.f_update : h->P.g_update)) return 0;
     double* in = h->pdf[fi][h->cur[fi]];
     double* out = h->pdf[fi][h->cur[fi] ^ 1];
-    LAUNCH_STEP(k_stream<L::Q>, blocks(h->n), h->n, out, in, h->nb);
+    LAUNCH(k_stream<L::Q>, blocks(h->n), h->n, out, in, h->nb);
     h->cur[fi] ^= 1;
     return 0;
 }
@@ -548,7 +539,7 @@ int op_boundaries(mplb_gpu* h, int fi) {
         if (pts[p].type == MPLB_BC_FIXEDRANDOMT && (int64_t)h->bc_calls[fi] < h->rnd_left[fi][p]) rnd |= 1ull << p;
     h->bc_calls[fi]++;
     if (h->serial[fi]) {
-        LAUNCH_STEP(k_bc_serial<L>, 1, h->P, h->dpatches + fi * pts.size(), (int)pts.size(), h->model[fi],
+        LAUNCH(k_bc_serial<L>, 1, h->P, h->dpatches + fi * pts.size(), (int)pts.size(), h->model[fi],
                h->pnodes, pdf, h->nb, h->rho, h->T, h->U, h->Fi, h->bctab[fi], rnd);
         return 0;
     }
@@ -556,7 +547,7 @@ int op_boundaries(mplb_gpu* h, int fi) {
         const PatchDev& pt = pts[p];
         if (pt.type == MPLB_BC_PERIODIC || pt.count == 0) continue;
         if (pt.type == MPLB_BC_FIXEDU && h->model[fi] != MPLB_LIMRT) continue;
-        LAUNCH_STEP(k_bc_patch<L>, blocks(pt.count), h->P, pt, h->model[fi], h->pnodes, pdf, h->nb, h->rho,
+        LAUNCH(k_bc_patch<L>, blocks(pt.count), h->P, pt, h->model[fi], h->pnodes, pdf, h->nb, h->rho,
                h->T, h->U, h->Fi, h->bctab[fi], (int)((rnd >> p) & 1ull));
     }
     return 0;
@@ -565,35 +556,35 @@ int op_boundaries(mplb_gpu* h, int fi) {
 template <class L>
 int op_density(mplb_gpu* h, uint32_t s, uint32_t e) {
     if (h->model[0] == MPLB_NO_MODEL || !h->P.f_update || e <= s) return 0;
-    LAUNCH_STEP(k_moment0<L::Q>, blocks(e - s), h->n, h->rho, h->F(), s, e);
+    LAUNCH(k_moment0<L::Q>, blocks(e - s), h->n, h->rho, h->F(), s, e);
     return 0;
 }
 
 template <class L>
 int op_temperature(mplb_gpu* h, uint32_t s, uint32_t e) {
     if (h->model[1] == MPLB_NO_MODEL || !h->P.g_update || e <= s) return 0;
-    if (h->model[1] == MPLB_MYMRT) LAUNCH_STEP(k_temperature_my<L::Q>, blocks(e - s), h->n, h->T, h->G(), h->S, s, e);
-    else LAUNCH_STEP(k_moment0<L::Q>, blocks(e - s), h->n, h->T, h->G(), s, e);
+    if (h->model[1] == MPLB_MYMRT) LAUNCH(k_temperature_my<L::Q>, blocks(e - s), h->n, h->T, h->G(), h->S, s, e);
+    else LAUNCH(k_moment0<L::Q>, blocks(e - s), h->n, h->T, h->G(), s, e);
     return 0;
 }
 
 template <class L>
 int op_velocity(mplb_gpu* h, uint32_t s, uint32_t e) {
     if (h->model[0] == MPLB_NO_MODEL || !h->P.f_update || e <= s) return 0;
-    LAUNCH_STEP(k_velocity<L>, blocks(e - s), h->P, h->U, h->F(), h->rho, h->Fi, h->Ft, s, e);
+    LAUNCH(k_velocity<L>, blocks(e - s), h->P, h->U, h->F(), h->rho, h->Fi, h->Ft, s, e);
     return 0;
 }
 
 template <class L>
 int op_interforce(mplb_gpu* h) {
-    LAUNCH_STEP(k_interforce<L>, blocks(h->n), h->P, h->Fi, h->Ft, h->rho, h->T, h->nb, h->onb);
+    LAUNCH(k_interforce<L>, blocks(h->n), h->P, h->Fi, h->Ft, h->rho, h->T, h->nb, h->onb);
     return 0;
 }
 
 template <class L>
 int op_heatsource(mplb_gpu* h) {
     if (h->model[1] == MPLB_NO_MODEL || !h->P.g_update) return 0;
-    LAUNCH_STEP(k_heatsource<L>, blocks(h->n), h->P, h->S, h->rho, h->T, h->U, h->nb, h->current == 0 ? 1 : 0);
+    LAUNCH(k_heatsource<L>, blocks(h->n), h->P, h->S, h->rho, h->T, h->U, h->nb, h->current == 0 ? 1 : 0);
     return 0;
 }
 

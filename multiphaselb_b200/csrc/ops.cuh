@@ -23,7 +23,6 @@ struct PatchDev {
 template <class L>
 __global__ void k_equilibrium_flow(Params P, double* __restrict__ f, const double* __restrict__ rho,
                                    const double* __restrict__ U) {
-    step_dependency_wait();
     uint32_t n = P.n, id = blockIdx.x * blockDim.x + threadIdx.x;
     if (id >= n) return;
     double v[3] = {U[id], U[n + id], U[2 * n + id]};
@@ -35,7 +34,6 @@ __global__ void k_equilibrium_flow(Params P, double* __restrict__ f, const doubl
 template <class L>
 __global__ void k_equilibrium_heat(Params P, double* __restrict__ g, const double* __restrict__ T,
                                    const double* __restrict__ U) {
-    step_dependency_wait();
     uint32_t n = P.n, id = blockIdx.x * blockDim.x + threadIdx.x;
     if (id >= n) return;
     double v[L::Q];
@@ -56,7 +54,6 @@ __global__ void k_collide_flow(Params P, double* __restrict__ f, const double* _
                                const double* __restrict__ U, const double* __restrict__ T,
                                const double* __restrict__ Fi, const double* __restrict__ Ft,
                                const int32_t* __restrict__ nb) {
-    step_dependency_wait();
     uint32_t n = P.n, id = blockIdx.x * blockDim.x + threadIdx.x;
     if (id >= n) return;
     double v[L::Q];
@@ -99,7 +96,6 @@ __global__ void k_collide_flow(Params P, double* __restrict__ f, const double* _
 template <class L>
 __global__ void k_collide_heat(Params P, double* __restrict__ g, const double* __restrict__ T,
                                const double* __restrict__ U, const double* __restrict__ S) {
-    step_dependency_wait();
     uint32_t n = P.n, id = blockIdx.x * blockDim.x + threadIdx.x;
     if (id >= n) return;
     double v[L::Q];
@@ -120,7 +116,6 @@ __global__ void k_collide_heat(Params P, double* __restrict__ g, const double* _
 template <int Q>
 __global__ void k_stream(uint32_t n, double* __restrict__ out, const double* __restrict__ in,
                          const int32_t* __restrict__ nb) {
-    step_dependency_wait();
     uint32_t id = blockIdx.x * blockDim.x + threadIdx.x;
     if (id >= n) return;
 #pragma unroll
@@ -136,7 +131,6 @@ __global__ void k_stream(uint32_t n, double* __restrict__ out, const double* __r
 template <int Q>
 __global__ void k_moment0(uint32_t n, double* __restrict__ out, const double* __restrict__ pdf,
                           uint32_t start, uint32_t end) {
-    step_dependency_wait();
     uint32_t id = start + blockIdx.x * blockDim.x + threadIdx.x;
     if (id >= end) return;
     double s = 0;
@@ -149,7 +143,6 @@ __global__ void k_moment0(uint32_t n, double* __restrict__ out, const double* __
 template <int Q>
 __global__ void k_temperature_my(uint32_t n, double* __restrict__ T, const double* __restrict__ g,
                                  const double* __restrict__ S, uint32_t start, uint32_t end) {
-    step_dependency_wait();
     uint32_t id = start + blockIdx.x * blockDim.x + threadIdx.x;
     if (id >= end) return;
     double s = 0;
@@ -163,7 +156,6 @@ template <class L>
 __global__ void k_velocity(Params P, double* __restrict__ U, const double* __restrict__ f,
                            const double* __restrict__ rho, const double* __restrict__ Fi,
                            const double* __restrict__ Ft, uint32_t start, uint32_t end) {
-    step_dependency_wait();
     uint32_t n = P.n, id = start + blockIdx.x * blockDim.x + threadIdx.x;
     if (id >= end) return;
     double v[L::Q];
@@ -189,7 +181,6 @@ template <class L>
 __global__ void k_interforce(Params P, double* __restrict__ Fi, double* __restrict__ Ft,
                              const double* __restrict__ rho, const double* __restrict__ T,
                              const int32_t* __restrict__ nb, const uint8_t* __restrict__ onb) {
-    step_dependency_wait();
     uint32_t n = P.n, id = blockIdx.x * blockDim.x + threadIdx.x;
     if (id >= n) return;
     double Ff[3] = {0, 0, 0};
@@ -239,7 +230,6 @@ template <class L>
 __global__ void k_heatsource(Params P, double* __restrict__ S, const double* __restrict__ rho,
                              const double* __restrict__ T, const double* __restrict__ U,
                              const int32_t* __restrict__ nb, int first) {
-    step_dependency_wait();
     uint32_t n = P.n, id = blockIdx.x * blockDim.x + threadIdx.x;
     if (id >= n) return;
     double gT[3] = {0, 0, 0}, gR[3] = {0, 0, 0}, div = 0;
@@ -451,7 +441,6 @@ __global__ void k_bc_patch(Params P, PatchDev pt, int model, const uint32_t* __r
                            const double* __restrict__ rho, const double* __restrict__ T,
                            const double* __restrict__ U, const double* __restrict__ Fi,
                            const double* __restrict__ tab, int rnd) {
-    step_dependency_wait();
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= pt.count) return;
     bc_node<L>(P, pt, model, nodes[pt.off + i], pdf, nb, rho, T, U, Fi, tab, pt.off + i, rnd != 0);
@@ -467,7 +456,6 @@ __global__ void k_bc_serial(Params P, const PatchDev* __restrict__ pts, int npat
                             const double* __restrict__ T, const double* __restrict__ U,
                             const double* __restrict__ Fi, const double* __restrict__ tab,
                             unsigned long long rnd_mask) {
-    step_dependency_wait();
     if (blockIdx.x != 0 || threadIdx.x != 0) return;
     for (int p = 0; p < npatch; p++) {
         PatchDev pt = pts[p];
