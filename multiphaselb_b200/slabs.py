@@ -1,0 +1,243 @@
+"""Slab decomposition of a box lattice over several handles (one per rank or
+device), with the reference's ghost-node exchange.
+
+The reference runs each MPI rank on its part of the mesh plus ghost nodes
+and exchanges them inside the time step (multiPhasePP.c:163-240):
+sendPdfField / recvPdfField after each field's boundaries, syncScalarField
+of the heat source and syncVectorField of the interaction force.  Here a box
+(cases.box_mesh layout, x fastest) is cut into slabs along its slowest axis
+(y in 2D, z in 3D); each slab's lattice holds its own planes plus one ghost
+plane on each cut (wrapping on a periodic axis), and a step runs the
+reference's operators on every slab with the ghost planes refreshed from
+their owners at the same points:
+
+    collision f, lbstream f, updateBoundaries f   -> ghost f
+    collision g, lbstream g, updateBoundaries g   -> ghost g
+    macroDensity
+    heatSource                                     -> ghost S
+    macroTemperature
+    interForce                                     -> ghost Fi, Ft
+    macroVelocity
+
+Ghost nodes have no neighbours and lie on no boundary patch, as in the
+reference's partitioned meshes (latticeMeshPartition.c:564-590, 679-725);
+whatever a ghost node computes is overwritten by the exchange before an
+owned node reads it, except its post-collision PDFs, which the owned nodes
+next to a cut pull in lbstream.  Those equal the single domain's unless the
+collision needs neighbours: the surface-tension term is zero on a node with
+a missing neighbour, so with surface tension on, the reference's multi-rank
+run (and this one) differs from its single-domain run next to every cut.
+Without surface tension the gathered owned nodes are bit-identical to the
+single-domain run (tests/test_slabs.py).  fixedRandomT seeds rand() with the
+rank; slab r runs as rank rank0 + r.
+
+The exchange is staged through host copies of the fields (download, copy the
+ghost planes, upload), which makes the scheme runnable on any handle with
+the operator interface: device handles on one or several GPUs, or a CPU
+checker.  A device-to-device exchange over NVLink would move only the ghost
+planes.
+"""
+from dataclasses import dataclass
+from typing import Callable, List, Optional
+
+import numpy as np
+
+from . import abi
+from .cases import Case
+
+FIELDS = ("rho", "U", "T", "Fi", "Ft", "S", "f", "g")
+
+
+@dataclass
+class Slab:
+    rank: int
+    planes: List[int]        # global plane index of every local plane, in local order
+    own_lo: int              # local index of the first owned plane
+    own_hi: int              # one past the last owned plane (local index)
+    case: Case
+    gidx: np.ndarray         # global node of every local node
+
+
+def _box_geometry(case):
+    d3 = case.lattice == abi.D3Q15
+    dims = tuple(case.dims)
+    nplanes = dims[2] if d3 else dims[1]
+    plane = int(np.prod(dims[:-1]))
+    periodic = bool(case.periodic[-1])
+    return nplanes, plane, periodic
+
+
+def split(case: Case, ranks: int, rank0: int = 0) -> List[Slab]:
+    """Cut a box case into `ranks` slabs along its slowest axis; slab r runs
+    as rank rank0 + r (the pid that seeds fixedRandomT)."""
+    nplanes, P, periodic = _box_geometry(case)
+    if ranks < 2:
+        raise ValueError("a split needs at least two slabs")
+    if nplanes < 2 * ranks:
+        raise ValueError(f"{nplanes} planes cannot give {ranks} slabs of at least two planes")
+    cuts = [round(r * nplanes / ranks) for r in range(ranks + 1)]
+    slabs = []
+    for r in range(ranks):
+        a, b = cuts[r], cuts[r + 1]
+        lo = a - 1 if a > 0 else (nplanes - 1 if periodic else None)
+        hi = b if b < nplanes else (0 if periodic else None)
+        planes = ([lo] if lo is not None else []) + list(range(a, b)) + ([hi] if hi is not None else [])
+        own_lo = 1 if lo is not None else 0
+        own_hi = own_lo + (b - a)
+        where = {p: j for j, p in enumerate(planes)}
+        gidx = np.concatenate([p * P + np.arange(P) for p in planes]).astype(np.int64)
+        # neighbour table: the global source mapped into the slab, -1 outside it
+        gnb = np.asarray(case.nb, dtype=np.int64)[gidx]
+        src_plane = np.where(gnb >= 0, gnb // P, -1)
+        lut = np.full(nplanes, -1, dtype=np.int64)
+        for p, j in where.items():
+            lut[p] = j
+        lj = np.where(gnb >= 0, lut[np.maximum(src_plane, 0)], -1)
+        nb = np.where(lj >= 0, lj * P + gnb % P, -1).astype(np.int32)
+        # ghost nodes get no neighbours, as in the reference's partition
+        # (latticeMeshPartition.c:564-590 fills nb for local nodes only)
+        nb[:own_lo * P] = -1
+        nb[own_hi * P:] = -1
+        # owned part of every patch, in patch order
+        owned = np.zeros(case.n, dtype=bool)
+        owned[a * P:b * P] = True
+        local_of = np.full(case.n, -1, dtype=np.int64)
+        local_of[gidx[own_lo * P:own_hi * P]] = np.arange(own_lo * P, own_hi * P)
+        patches = [local_of[np.asarray(p, dtype=np.int64)[owned[np.asarray(p, dtype=np.int64)]]].astype(np.uint32)
+                   for p in case.patches]
+        pts = np.asarray(case.points)[gidx]
+        local = Case(f"{case.name}_slab{r}", case.lattice, tuple(case.dims[:-1]) + (len(planes),),
+                     tuple(case.periodic[:-1]) + (False,), nb, pts.astype(np.int32), patches,
+                     list(case.patch_names), case.eos, case.f, case.g, np.asarray(case.rho)[gidx],
+                     np.asarray(case.U)[gidx], np.asarray(case.T)[gidx], meta=dict(case.meta, box=False, rank=rank0 + r))
+        slabs.append(Slab(r, planes, own_lo, own_hi, local, gidx))
+    return slabs
+
+
+class SlabRun:
+    """Step a split box case on `ranks` handles.
+
+    make_handle(case) -> an object with upload(**fields), download() -> dict
+    of the fields in the reference layouts, set_time(t), get_time() and
+    op(name, field=None) for the reference operators named as the Lattice
+    methods (equilibrium, collision, lbstream, update_boundaries,
+    macro_density, heat_source, macro_temperature, inter_force,
+    macro_velocity).  See lattice_handle for device handles.
+    """
+
+    def __init__(self, case: Case, ranks: int, make_handle: Callable, rank0: int = 0):
+        self.case = case
+        self.slabs = split(case, ranks, rank0)
+        self.handles = [make_handle(s.case) for s in self.slabs]
+        _, self.P, _ = _box_geometry(case)
+        self.has_g = case.g is not None
+        self.f_on = case.f is not None and bool(case.f.get("update", 1))
+        self.g_on = self.has_g and bool(case.g.get("update", 1))
+
+    # -------------------------------------------------------------- exchange
+    def _owner(self, plane):
+        for s in self.slabs:
+            if s.planes[s.own_lo] <= plane < s.planes[s.own_lo] + (s.own_hi - s.own_lo):
+                return s
+        raise AssertionError(plane)
+
+    def exchange(self, names):
+        """Ghost planes of the fields `names` from their owners."""
+        states = [h.download() for h in self.handles]
+        P = self.P
+        for s, st in zip(self.slabs, states):
+            ghosts = [j for j in range(len(s.planes)) if not s.own_lo <= j < s.own_hi]
+            for j in ghosts:
+                o = self._owner(s.planes[j])
+                oj = o.planes.index(s.planes[j], o.own_lo, o.own_hi)
+                src = states[o.rank]
+                for nm in names:
+                    st[nm][j * P:(j + 1) * P] = src[nm][oj * P:(oj + 1) * P]
+        for h, st in zip(self.handles, states):
+            up = {nm: st[nm] for nm in FIELDS if not (nm == "g" and not self.has_g)}
+            h.upload(**up)
+
+    def _all(self, name, field=None):
+        for h in self.handles:
+            h.op(name, field)
+
+    # ------------------------------------------------------------- the loop
+    def initialize(self):
+        """multiPhasePP.c:122-147 on every slab, ghosts exchanged."""
+        for h, s in zip(self.handles, self.slabs):
+            h.upload(rho=s.case.rho, U=s.case.U, T=s.case.T)
+        self._all("equilibrium", abi.FIELD_F)
+        if self.has_g:
+            self._all("equilibrium", abi.FIELD_G)
+        self._all("inter_force")
+        self.exchange(("Fi", "Ft"))
+        if self.g_on:
+            self._all("heat_source")
+            self.exchange(("S",))
+
+    def step(self, n=1):
+        """multiPhasePP.c:157-240 with the ghost exchanges of the reference."""
+        for _ in range(n):
+            for h in self.handles:
+                h.set_time(h.get_time() + 1)
+            for fi, on, name in ((abi.FIELD_F, self.f_on, "f"), (abi.FIELD_G, self.g_on, "g")):
+                if not on:
+                    continue
+                self._all("collision", fi)
+                self._all("lbstream", fi)
+                self._all("update_boundaries", fi)
+                self.exchange((name,))
+            self._all("macro_density")
+            if self.g_on:
+                self._all("heat_source")
+                self.exchange(("S",))
+            self._all("macro_temperature")
+            if self.f_on:
+                self._all("inter_force")
+                self.exchange(("Fi", "Ft"))
+            self._all("macro_velocity")
+
+    def gather(self):
+        """The owned planes of every slab, as the single-domain fields."""
+        n = self.case.n
+        out = None
+        for s, h in zip(self.slabs, self.handles):
+            st = h.download()
+            if out is None:
+                out = {k: np.zeros((n,) + st[k].shape[1:]) for k in st}
+            lo, hi = s.own_lo * self.P, s.own_hi * self.P
+            for k in st:
+                out[k][s.gidx[lo:hi]] = st[k][lo:hi]
+        return out
+
+
+class lattice_handle:
+    """Operator-interface adapter of a device Lattice (operator path)."""
+
+    def __init__(self, case, device=-1):
+        from . import PATH_OPERATORS, Lattice
+        self.lat = Lattice(case, path=PATH_OPERATORS, device=device)
+
+    def upload(self, **fields):
+        self.lat.upload(**fields)
+
+    def download(self):
+        return self.lat.download()
+
+    def set_time(self, t):
+        self.lat.set_time(t)
+
+    def get_time(self):
+        return self.lat.info()["current_time"]
+
+    def op(self, name, field=None):
+        m = getattr(self.lat, name)
+        return m(field) if field is not None else m()
+
+    def close(self):
+        self.lat.close()
+
+
+def owned_fields(run: SlabRun) -> Optional[dict]:
+    """Alias of SlabRun.gather, for callers that think in ranks."""
+    return run.gather()

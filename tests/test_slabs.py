@@ -1,0 +1,161 @@
+"""Slab decomposition (multiphaselb_b200.slabs) against the single domain:
+a box cut into 2 or 3 slabs along its slowest axis, each slab on its own
+oracle lattice with one ghost plane per cut, the ghost planes exchanged at
+the reference's points in the step (multiPhasePP.c:163-240).  The owned
+nodes of the slabs, gathered, are bit-identical to the single-domain run.
+Host code and the CPU oracle only."""
+import numpy as np
+import pytest
+
+from multiphaselb_b200 import abi, slabs
+from oracle import oracle as orc
+from tests.helpers import FIELDS, assert_same, run_checker, small_cases
+
+OPS = {"equilibrium": orc.OP_EQUILIBRIUM, "collision": orc.OP_COLLISION, "lbstream": orc.OP_LBSTREAM,
+       "update_boundaries": orc.OP_BOUNDARIES, "macro_density": orc.OP_DENSITY,
+       "macro_velocity": orc.OP_VELOCITY, "macro_temperature": orc.OP_TEMPERATURE,
+       "inter_force": orc.OP_INTERFORCE, "heat_source": orc.OP_HEATSOURCE}
+
+
+class checker_handle:
+    """The slab runner's operator interface over a CPU checker."""
+
+    def __init__(self, case):
+        self.k = orc.Checker("port", case)
+
+    def upload(self, **fields):
+        self.k.upload(**fields)
+
+    def download(self):
+        return self.k.download()
+
+    def set_time(self, t):
+        self.k.set_time(t)
+
+    def get_time(self):
+        return self.k.get_time()
+
+    def op(self, name, field=None):
+        self.k.op(OPS[name], abi.FIELD_F if field is None else field)
+
+
+def fields_of(case):
+    return [f for f in FIELDS if not (f == "g" and case.g is None)]
+
+
+@pytest.mark.parametrize("name,ranks", [
+    ("column_d2q9", 2), ("column_d2q9", 3),      # fixedT / bounce-back walls at the ends
+    ("bubble_d2q9", 2), ("bubble_d2q9", 3),      # periodic: the ghost planes wrap
+    ("lid_d2q9", 2),                             # fixedU lid
+    ("my_column_d2q9", 3),                       # myMRT heat
+    ("outflow_d2q9", 2),                         # outflow top, fixedRandomT bottom
+    ("bubble_d3q15", 3),                         # D3Q15, cut along z
+    ("walls_d3q15", 2),
+    ("my_slab_d3q15", 2),
+])
+def test_slabs_equal_single_domain(name, ranks):
+    case = small_cases()[name]
+    steps = 6
+    want = run_checker("port", case, steps)
+    # the bottom slab takes the single domain's pid, which seeds fixedRandomT
+    run = slabs.SlabRun(case, ranks, checker_handle, rank0=case.meta.get("rank", 0))
+    run.initialize()
+    run.step(steps)
+    assert_same(run.gather(), want, fields=fields_of(case), ctx=f"{name} in {ranks} slabs")
+
+
+def test_cut_deviations_of_the_reference():
+    """Where the reference's multi-rank run differs from its single-domain
+    run, the split differs the same way and nowhere else.  A ghost node has no
+    neighbours, so (1) its collision has no surface-tension term
+    (liMRTSurfaceTension.c zeroes it on a node with a missing neighbour) and
+    the owned nodes next to a cut pull those PDFs in lbstream; (2) it does
+    not stream, and a fixedT / fixedU wall node next to a cut extrapolates
+    from the ghost's post-collision PDF (the exchange follows the
+    boundaries).  After one step the differing PDFs are exactly those."""
+    # (1) surface tension, 20 x 18 with walls in y: one cut at y = 9
+    case = small_cases()["st_d2q9"]
+    nx = case.dims[0]
+    want = run_checker("port", case, 1)
+    run = slabs.SlabRun(case, 2, checker_handle)
+    run.initialize()
+    run.step(1)
+    got = run.gather()
+    node, k = np.nonzero(got["f"] != want["f"])
+    assert len(node) > 0
+    src = case.nb[node, k]
+    assert ((node // nx >= 9) != (src // nx >= 9)).all()      # every one pulled across the cut
+    assert set((np.nonzero(got["rho"] != want["rho"])[0] // nx).tolist()) <= {8, 9}
+
+    # (2) fixedT side wall, 10 x 12 walled box in 3 slabs: cuts at y = 4 and 8
+    case = small_cases()["outflow_corner_d2q9"]
+    nx, Q = case.dims[0], case.Q
+    want = run_checker("port", case, 1)
+    run = slabs.SlabRun(case, 3, checker_handle, rank0=case.meta.get("rank", 0))
+    run.initialize()
+    run.step(1)
+    got = run.gather()
+    assert np.array_equal(got["f"], want["f"])
+    node, k = np.nonzero(got["g"] != want["g"])
+    assert len(node) > 0
+    rev = np.asarray(orc_rev(case))
+    assert (case.nb[node, k] == -1).all()                      # unknown populations of wall nodes
+    slab_of = np.searchsorted([4, 8], node // nx, side="right")
+    xsrc = case.nb[node, rev[k]]
+    assert (slab_of != np.searchsorted([4, 8], xsrc // nx, side="right")).all()   # extrapolated from a ghost
+
+
+def orc_rev(case):
+    """Index of the opposite velocity of each lattice velocity."""
+    from multiphaselb_b200 import cases as cs
+    c = np.asarray(cs.VEL[case.lattice])
+    return [int(np.nonzero((c == -c[k]).all(1))[0][0]) for k in range(len(c))]
+
+
+def test_surface_tension_off_is_bit_identical():
+    case = small_cases()["st_d2q9"]
+    case.f = dict(case.f, surface_tension=0)
+    want = run_checker("port", case, 6)
+    run = slabs.SlabRun(case, 2, checker_handle)
+    run.initialize()
+    run.step(6)
+    assert_same(run.gather(), want, fields=fields_of(case), ctx="st_d2q9 with the term off, 2 slabs")
+
+
+def test_split_layout():
+    """Planes, owned ranges and the neighbour table of a periodic 2D split."""
+    case = small_cases()["bubble_d2q9"]          # 24 x 20, periodic in x and y
+    ss = slabs.split(case, 3)
+    nx = case.dims[0]
+    assert [s.planes[s.own_lo] for s in ss] == [0, 7, 13]
+    assert [s.own_hi - s.own_lo for s in ss] == [7, 6, 7]
+    assert ss[0].planes[0] == 19 and ss[2].planes[-1] == 0           # wrapped ghosts
+    for s in ss:
+        lc = s.case
+        assert lc.n == len(s.planes) * nx and lc.meta["rank"] == s.rank
+        own = slice(s.own_lo * nx, s.own_hi * nx)
+        # an owned node pulls from the node the single domain pulls from
+        g = case.nb[s.gidx[own]]
+        got = lc.nb[own]
+        assert (got >= 0).all()
+        assert np.array_equal(s.gidx[got], g)
+        assert (np.delete(lc.nb, np.arange(own.start, own.stop), axis=0) == -1).all()   # ghosts
+
+
+def test_split_walls_patches_and_refusals():
+    case = small_cases()["column_d2q9"]          # 12 x 24, walls at y = 0 and 23
+    ss = slabs.split(case, 2)
+    nx = case.dims[0]
+    assert ss[0].own_lo == 0 and ss[0].planes == list(range(0, 13))   # no ghost below the wall
+    assert ss[1].own_hi == len(ss[1].planes)
+    # every wall node lands in exactly one slab, as an owned node
+    for p, pts in enumerate(case.patches):
+        got = np.concatenate([s.gidx[s.case.patches[p].astype(np.int64)] for s in ss])
+        assert np.array_equal(np.sort(got), np.sort(pts.astype(np.int64)))
+        for s in ss:
+            loc = s.case.patches[p].astype(np.int64)
+            assert ((loc >= s.own_lo * nx) & (loc < s.own_hi * nx)).all()
+    with pytest.raises(ValueError):
+        slabs.split(case, 1)
+    with pytest.raises(ValueError):
+        slabs.split(case, 13)
