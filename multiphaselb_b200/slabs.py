@@ -38,7 +38,7 @@ checker.  A device-to-device exchange over NVLink would move only the ghost
 planes.
 """
 from dataclasses import dataclass
-from typing import Callable, List, Optional
+from typing import Callable, List
 
 import numpy as np
 
@@ -122,7 +122,7 @@ class SlabRun:
     op(name, field=None) for the reference operators named as the Lattice
     methods (equilibrium, collision, lbstream, update_boundaries,
     macro_density, heat_source, macro_temperature, inter_force,
-    macro_velocity).  See lattice_handle for device handles.
+    macro_velocity).  See LatticeHandle for device handles.
     """
 
     def __init__(self, case: Case, ranks: int, make_handle: Callable, rank0: int = 0):
@@ -211,7 +211,7 @@ class SlabRun:
         return out
 
 
-class lattice_handle:
+class LatticeHandle:
     """Operator-interface adapter of a device Lattice (operator path)."""
 
     def __init__(self, case, device=-1):
@@ -236,8 +236,3 @@ class lattice_handle:
 
     def close(self):
         self.lat.close()
-
-
-def owned_fields(run: SlabRun) -> Optional[dict]:
-    """Alias of SlabRun.gather, for callers that think in ranks."""
-    return run.gather()

@@ -1,12 +1,12 @@
 """Slab decomposition on the device: every slab a device lattice on the
-operator path (multiphaselb_b200.slabs.lattice_handle), the ghost planes
+operator path (multiphaselb_b200.slabs.LatticeHandle), the ghost planes
 exchanged at the reference's points, against the same split run on CPU
 checkers.  Bitwise."""
 import pytest
 
 from multiphaselb_b200 import slabs
 from tests.helpers import assert_same, small_cases
-from tests.test_slabs import checker_handle, fields_of
+from tests.test_slabs import CheckerHandle, fields_of
 
 pytestmark = pytest.mark.gpu
 
@@ -17,7 +17,7 @@ def test_device_slabs_match_checker_slabs(gpu_lib, name, ranks):
     case = small_cases()[name]
     rank0 = case.meta.get("rank", 0)
     runs = []
-    for make in (checker_handle, slabs.lattice_handle):
+    for make in (CheckerHandle, slabs.LatticeHandle):
         run = slabs.SlabRun(case, ranks, make, rank0=rank0)
         run.initialize()
         run.step(5)

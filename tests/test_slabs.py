@@ -17,7 +17,7 @@ OPS = {"equilibrium": orc.OP_EQUILIBRIUM, "collision": orc.OP_COLLISION, "lbstre
        "inter_force": orc.OP_INTERFORCE, "heat_source": orc.OP_HEATSOURCE}
 
 
-class checker_handle:
+class CheckerHandle:
     """The slab runner's operator interface over a CPU checker."""
 
     def __init__(self, case):
@@ -58,7 +58,7 @@ def test_slabs_equal_single_domain(name, ranks):
     steps = 6
     want = run_checker("port", case, steps)
     # the bottom slab takes the single domain's pid, which seeds fixedRandomT
-    run = slabs.SlabRun(case, ranks, checker_handle, rank0=case.meta.get("rank", 0))
+    run = slabs.SlabRun(case, ranks, CheckerHandle, rank0=case.meta.get("rank", 0))
     run.initialize()
     run.step(steps)
     assert_same(run.gather(), want, fields=fields_of(case), ctx=f"{name} in {ranks} slabs")
@@ -77,7 +77,7 @@ def test_cut_deviations_of_the_reference():
     case = small_cases()["st_d2q9"]
     nx = case.dims[0]
     want = run_checker("port", case, 1)
-    run = slabs.SlabRun(case, 2, checker_handle)
+    run = slabs.SlabRun(case, 2, CheckerHandle)
     run.initialize()
     run.step(1)
     got = run.gather()
@@ -91,7 +91,7 @@ def test_cut_deviations_of_the_reference():
     case = small_cases()["outflow_corner_d2q9"]
     nx, Q = case.dims[0], case.Q
     want = run_checker("port", case, 1)
-    run = slabs.SlabRun(case, 3, checker_handle, rank0=case.meta.get("rank", 0))
+    run = slabs.SlabRun(case, 3, CheckerHandle, rank0=case.meta.get("rank", 0))
     run.initialize()
     run.step(1)
     got = run.gather()
@@ -116,7 +116,7 @@ def test_surface_tension_off_is_bit_identical():
     case = small_cases()["st_d2q9"]
     case.f = dict(case.f, surface_tension=0)
     want = run_checker("port", case, 6)
-    run = slabs.SlabRun(case, 2, checker_handle)
+    run = slabs.SlabRun(case, 2, CheckerHandle)
     run.initialize()
     run.step(6)
     assert_same(run.gather(), want, fields=fields_of(case), ctx="st_d2q9 with the term off, 2 slabs")
