@@ -39,7 +39,7 @@
 extern "C" {
 #endif
 
-#define MPLB_ABI_VERSION 2  /* 2: mplb_field_desc.alpha_1/alpha_2, mplb_opts.rank */
+#define MPLB_ABI_VERSION 3  /* 2: mplb_field_desc.alpha_1/alpha_2, mplb_opts.rank; 3: mplb_gpu_copy_nodes */
 #define MPLB_MAX_Q 15
 #define MPLB_MAX_PATCHES 64
 
@@ -273,6 +273,32 @@ int mplb_gpu_run_to_equilibrium(mplb_gpu_t* h, uint32_t max_steps, uint32_t chec
 
 /* Wait for the handle's stream. */
 int mplb_gpu_sync(mplb_gpu_t* h);
+
+/* Ghost-node exchange between lattices, on the devices.  Replaces the
+ * reference's host-side exchanges of a multi-rank run (sendPdfField /
+ * recvPdfField, src/basic/sendPdfField.c:6-102 and recvPdfField.c:6-54, for
+ * f and g; syncScalarField.c and syncVectorField.c for S, Fi and Ft) when
+ * the ranks' lattices are handles of this library, on one GPU or on several.
+ * Copies nodes [src_start, src_start + count) of src into nodes
+ * [dst_start, dst_start + count) of dst, for every field named in `fields`
+ * (MPLB_NODES_* bits), in the reference state of both handles.  The copy is
+ * queued on src's stream after all work already queued on dst's stream, and
+ * dst's stream waits for it; the call does not block the host.  Between
+ * devices the copy goes peer to peer (peer access is enabled on first use
+ * where the devices allow it).  Both handles hold the same lattice in FP64;
+ * on one handle the two ranges must not overlap. */
+enum {
+    MPLB_NODES_RHO = 1,
+    MPLB_NODES_U = 2,
+    MPLB_NODES_T = 4,
+    MPLB_NODES_FI = 8,
+    MPLB_NODES_FT = 16,
+    MPLB_NODES_S = 32,
+    MPLB_NODES_F = 64,
+    MPLB_NODES_G = 128
+};
+int mplb_gpu_copy_nodes(mplb_gpu_t* dst, uint32_t dst_start, mplb_gpu_t* src, uint32_t src_start,
+                        uint32_t count, int32_t fields);
 
 /* Total mass sum(rho[i]) and energy sum(T[i]) of plain device arrays, without
  * allocating device memory.  No counterpart in the reference: it is for

@@ -69,6 +69,7 @@ def load_library(path=LIB_PATH):
         "mplb_gpu_average_rho0": ([H, D], C.c_int),
         "mplb_gpu_mass_energy": ([H, D, D], C.c_int),
         "mplb_gpu_sync": ([H], C.c_int),
+        "mplb_gpu_copy_nodes": ([H, C.c_uint32, H, C.c_uint32, C.c_uint32, C.c_int32], C.c_int),
         "mplb_gpu_snapshot": ([H, C.c_int32], C.c_int),
         "mplb_gpu_snapshot_wait": ([H, D, D, D, D], C.c_int),
         "mplb_gpu_snapshot_write": ([H, C.c_char_p, C.c_int32, C.c_int32], C.c_int),
@@ -240,6 +241,16 @@ class Lattice:
 
     def set_time(self, t):
         self._check(self.lib.mplb_gpu_set_time(self.h, t))
+
+    def copy_nodes(self, src, dst_start, src_start, count, fields=("f",)):
+        """Copy nodes [src_start, src_start + count) of the Lattice `src` into
+        nodes [dst_start, ...) of this one, device to device (peer to peer
+        between GPUs), for the fields named as in download(); queued after
+        both handles' earlier work, without blocking the host."""
+        mask = 0
+        for name in fields:
+            mask |= abi.NODES[name]
+        self._check(self.lib.mplb_gpu_copy_nodes(self.h, dst_start, src.h, src_start, count, mask))
 
     def set_rho0(self, r):
         self._check(self.lib.mplb_gpu_set_rho0(self.h, r))

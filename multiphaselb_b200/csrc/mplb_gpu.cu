@@ -1637,6 +1637,88 @@ int mplb_gpu_sync(mplb_gpu_t* h) {
     return 0;
 }
 
+int mplb_gpu_copy_nodes(mplb_gpu_t* dst, uint32_t dst_start, mplb_gpu_t* src, uint32_t src_start,
+                        uint32_t count, int32_t fields) {
+    if (!dst || !src) return fail(MPLB_E_ARG, "NULL handle");
+    const int32_t all = MPLB_NODES_RHO | MPLB_NODES_U | MPLB_NODES_T | MPLB_NODES_FI | MPLB_NODES_FT |
+                        MPLB_NODES_S | MPLB_NODES_F | MPLB_NODES_G;
+    if (fields & ~all) return fail(MPLB_E_ARG, "unknown field bits");
+    if (dst->Q != src->Q) return fail(MPLB_E_ARG, "the lattices differ");
+    if (dst->precision != MPLB_FP64 || src->precision != MPLB_FP64)
+        return fail(MPLB_E_UNSUPPORTED, "node copies need FP64 storage");
+    if ((uint64_t)dst_start + count > dst->n || (uint64_t)src_start + count > src->n)
+        return fail(MPLB_E_ARG, "node range out of bounds");
+    for (int fi = 0; fi < 2; fi++)
+        if ((fields & (fi ? MPLB_NODES_G : MPLB_NODES_F)) &&
+            (dst->model[fi] == MPLB_NO_MODEL || src->model[fi] == MPLB_NO_MODEL))
+            return fail(MPLB_E_ARG, fi ? "no g field" : "no f field");
+    if (dst == src && (uint64_t)dst_start < (uint64_t)src_start + count &&
+        (uint64_t)src_start < (uint64_t)dst_start + count)
+        return fail(MPLB_E_ARG, "overlapping ranges on one handle");
+    if (count == 0 || fields == 0) return 0;
+    {
+        DeviceGuard guard(src->dev);
+        RET(materialize(src));
+    }
+    {
+        DeviceGuard guard(dst->dev);
+        RET(materialize(dst));
+    }
+    // every field is [component][node] on the device: one strided copy each
+    struct Part { double* d; const double* s; int rows; };
+    Part parts[8];
+    int np = 0;
+    auto add = [&](int32_t bit, double* d, const double* s, int rows) {
+        if (fields & bit) parts[np++] = Part{d, s, rows};
+    };
+    add(MPLB_NODES_RHO, dst->rho, src->rho, 1);
+    add(MPLB_NODES_U, dst->U, src->U, 3);
+    add(MPLB_NODES_T, dst->T, src->T, 1);
+    add(MPLB_NODES_FI, dst->Fi, src->Fi, 3);
+    add(MPLB_NODES_FT, dst->Ft, src->Ft, 3);
+    add(MPLB_NODES_S, dst->S, src->S, 1);
+    if (fields & MPLB_NODES_F) add(MPLB_NODES_F, dst->F(), src->F(), dst->Q);
+    if (fields & MPLB_NODES_G) add(MPLB_NODES_G, dst->G(), src->G(), dst->Q);
+    const bool same_queue = dst->dev == src->dev && dst->stream == src->stream;
+    struct Events {
+        cudaEvent_t dst_ready = nullptr, copied = nullptr;
+        ~Events() {
+            if (dst_ready) cudaEventDestroy(dst_ready);
+            if (copied) cudaEventDestroy(copied);
+        }
+    } ev;
+    if (!same_queue) {
+        DeviceGuard guard(dst->dev);
+        CK(cudaEventCreateWithFlags(&ev.dst_ready, cudaEventDisableTiming));
+        CK(cudaEventRecord(ev.dst_ready, dst->stream));
+    }
+    DeviceGuard guard(src->dev);
+    if (dst->dev != src->dev) {
+        int can = 0;
+        CK(cudaDeviceCanAccessPeer(&can, src->dev, dst->dev));
+        if (can) {
+            cudaError_t e = cudaDeviceEnablePeerAccess(dst->dev, 0);
+            if (e == cudaErrorPeerAccessAlreadyEnabled) cudaGetLastError();
+            else CK(e);
+        }
+    }
+    if (!same_queue) CK(cudaStreamWaitEvent(src->stream, ev.dst_ready, 0));
+    const size_t dpitch = (size_t)dst->n * sizeof(double), spitch = (size_t)src->n * sizeof(double);
+    const size_t width = (size_t)count * sizeof(double);
+    for (int i = 0; i < np; i++) {
+        const Part& p = parts[i];
+        CK(cudaMemcpy2DAsync(p.d + dst_start, dpitch, p.s + src_start, spitch, width, p.rows, cudaMemcpyDefault,
+                             src->stream));
+    }
+    if (!same_queue) {
+        CK(cudaEventCreateWithFlags(&ev.copied, cudaEventDisableTiming));
+        CK(cudaEventRecord(ev.copied, src->stream));
+        DeviceGuard dguard(dst->dev);
+        CK(cudaStreamWaitEvent(dst->stream, ev.copied, 0));
+    }
+    return 0;
+}
+
 }  // extern "C"
 
 // ================================================================= batch

@@ -31,11 +31,12 @@ Without surface tension the gathered owned nodes are bit-identical to the
 single-domain run (tests/test_slabs.py).  fixedRandomT seeds rand() with the
 rank; slab r runs as rank rank0 + r.
 
-The exchange is staged through host copies of the fields (download, copy the
-ghost planes, upload), which makes the scheme runnable on any handle with
-the operator interface: device handles on one or several GPUs, or a CPU
-checker.  A device-to-device exchange over NVLink would move only the ghost
-planes.
+Between device handles (LatticeHandle) the exchange moves only the ghost
+planes, device to device (mplb_gpu_copy_nodes: one strided copy per field
+and plane, peer to peer when the slabs sit on different GPUs, ordered on the
+handles' streams without a host synchronisation).  Any other handle with the
+operator interface (a CPU checker in the tests) is exchanged through host
+copies of its fields: download, copy the ghost planes, upload.
 """
 from dataclasses import dataclass
 from typing import Callable, List
@@ -125,10 +126,12 @@ class SlabRun:
     macro_velocity).  See LatticeHandle for device handles.
     """
 
-    def __init__(self, case: Case, ranks: int, make_handle: Callable, rank0: int = 0):
+    def __init__(self, case: Case, ranks: int, make_handle: Callable, rank0: int = 0, staged: bool = False):
         self.case = case
         self.slabs = split(case, ranks, rank0)
         self.handles = [make_handle(s.case) for s in self.slabs]
+        # device-to-device ghost copies when every handle offers them
+        self.direct = not staged and all(hasattr(h, "copy_from") for h in self.handles)
         _, self.P, _ = _box_geometry(case)
         self.has_g = case.g is not None
         self.f_on = case.f is not None and bool(case.f.get("update", 1))
@@ -141,18 +144,29 @@ class SlabRun:
                 return s
         raise AssertionError(plane)
 
+    def ghost_sources(self):
+        """(slab, ghost plane, owner slab, owner's plane) of every ghost plane,
+        all in local plane indices."""
+        out = []
+        for s in self.slabs:
+            for j in range(len(s.planes)):
+                if not s.own_lo <= j < s.own_hi:
+                    o = self._owner(s.planes[j])
+                    out.append((s, j, o, o.planes.index(s.planes[j], o.own_lo, o.own_hi)))
+        return out
+
     def exchange(self, names):
         """Ghost planes of the fields `names` from their owners."""
-        states = [h.download() for h in self.handles]
         P = self.P
-        for s, st in zip(self.slabs, states):
-            ghosts = [j for j in range(len(s.planes)) if not s.own_lo <= j < s.own_hi]
-            for j in ghosts:
-                o = self._owner(s.planes[j])
-                oj = o.planes.index(s.planes[j], o.own_lo, o.own_hi)
-                src = states[o.rank]
-                for nm in names:
-                    st[nm][j * P:(j + 1) * P] = src[nm][oj * P:(oj + 1) * P]
+        if self.direct:
+            for s, j, o, oj in self.ghost_sources():
+                self.handles[s.rank].copy_from(self.handles[o.rank], j * P, oj * P, P, names)
+            return
+        states = [h.download() for h in self.handles]
+        for s, j, o, oj in self.ghost_sources():
+            st, src = states[s.rank], states[o.rank]
+            for nm in names:
+                st[nm][j * P:(j + 1) * P] = src[nm][oj * P:(oj + 1) * P]
         for h, st in zip(self.handles, states):
             up = {nm: st[nm] for nm in FIELDS if not (nm == "g" and not self.has_g)}
             h.upload(**up)
@@ -233,6 +247,9 @@ class LatticeHandle:
     def op(self, name, field=None):
         m = getattr(self.lat, name)
         return m(field) if field is not None else m()
+
+    def copy_from(self, src, dst_start, src_start, count, names):
+        self.lat.copy_nodes(src.lat, dst_start, src_start, count, names)
 
     def close(self):
         self.lat.close()

@@ -134,6 +134,7 @@ def test_null_handles_are_refused():
         lambda: lib.mplb_gpu_snapshot_join(None),
         lambda: lib.mplb_gpu_collision(None, 0),
         lambda: lib.mplb_gpu_macro_pressure(None),
+        lambda: lib.mplb_gpu_copy_nodes(None, 0, None, 0, 1, 64),
     ]
     for call in calls:
         assert call() == abi.E_ARG

@@ -1,28 +1,67 @@
 """Slab decomposition on the device: every slab a device lattice on the
 operator path (multiphaselb_b200.slabs.LatticeHandle), the ghost planes
 exchanged at the reference's points, against the same split run on CPU
-checkers.  Bitwise."""
+checkers; the ghost exchange device to device (mplb_gpu_copy_nodes) and
+through the host.  Bitwise.  Also mplb_gpu_copy_nodes itself: what it
+copies and what it refuses."""
+import numpy as np
 import pytest
 
-from multiphaselb_b200 import slabs
+from multiphaselb_b200 import Lattice, MplbError, abi, slabs
 from tests.helpers import assert_same, small_cases
 from tests.test_slabs import CheckerHandle, fields_of
 
 pytestmark = pytest.mark.gpu
 
 
+def run_split(case, ranks, make, staged=False):
+    run = slabs.SlabRun(case, ranks, make, rank0=case.meta.get("rank", 0), staged=staged)
+    assert run.direct == (make is slabs.LatticeHandle and not staged)
+    run.initialize()
+    run.step(5)
+    out = run.gather()
+    for h in run.handles:
+        if hasattr(h, "close"):
+            h.close()
+    return out
+
+
 @pytest.mark.parametrize("name,ranks", [("column_d2q9", 3), ("bubble_d2q9", 2), ("outflow_corner_d2q9", 3),
-                                        ("st_d2q9", 2), ("my_slab_d3q15", 2)])
+                                        ("st_d2q9", 2), ("my_slab_d3q15", 2), ("bubble_d3q15", 3)])
 def test_device_slabs_match_checker_slabs(gpu_lib, name, ranks):
     case = small_cases()[name]
-    rank0 = case.meta.get("rank", 0)
-    runs = []
-    for make in (CheckerHandle, slabs.LatticeHandle):
-        run = slabs.SlabRun(case, ranks, make, rank0=rank0)
-        run.initialize()
-        run.step(5)
-        runs.append(run.gather())
-        for h in run.handles:
-            if hasattr(h, "close"):
-                h.close()
-    assert_same(runs[1], runs[0], fields=fields_of(case), ctx=f"{name} in {ranks} slabs, device vs checker")
+    want = run_split(case, ranks, CheckerHandle)
+    fields = fields_of(case)
+    assert_same(run_split(case, ranks, slabs.LatticeHandle), want, fields=fields,
+                ctx=f"{name} in {ranks} slabs, device-to-device exchange vs checker")
+    assert_same(run_split(case, ranks, slabs.LatticeHandle, staged=True), want, fields=fields,
+                ctx=f"{name} in {ranks} slabs, host-staged exchange vs checker")
+
+
+def test_copy_nodes_copies_ranges_of_every_field(gpu_lib):
+    case = small_cases()["column_d2q9"]
+    rng = np.random.default_rng(7)
+    n, Q = case.n, case.Q
+    a_fields = dict(rho=rng.random(n), U=rng.random((n, 3)), T=rng.random(n), f=rng.random((n, Q)),
+                    g=rng.random((n, Q)), S=rng.random(n), Fi=rng.random((n, 3)), Ft=rng.random((n, 3)))
+    b_fields = {k: np.zeros_like(v) for k, v in a_fields.items()}
+    with Lattice(case, path=abi.PATH_OPERATORS) as a, Lattice(case, path=abi.PATH_OPERATORS) as b:
+        a.upload(**a_fields)
+        b.upload(**b_fields)
+        b.copy_nodes(a, 30, 100, 17, fields=("f", "S", "U"))
+        b.copy_nodes(b, 200, 30, 5, fields=("f",))          # on one handle, after the first copy
+        got = b.download()
+        for k in a_fields:
+            want = b_fields[k].copy()
+            if k in ("f", "S", "U"):
+                want[30:47] = a_fields[k][100:117]
+            if k == "f":
+                want[200:205] = a_fields[k][100:105]
+            assert np.array_equal(got[k], want), k
+        with pytest.raises(MplbError) as e:
+            b.copy_nodes(a, n - 3, 0, 4)
+        assert e.value.code == abi.E_ARG
+        with pytest.raises(MplbError) as e:
+            b.copy_nodes(b, 10, 12, 4)
+        assert e.value.code == abi.E_ARG
+        assert b.lib.mplb_gpu_copy_nodes(b.h, 0, a.h, 0, 1, 256) == abi.E_ARG
