@@ -115,70 +115,45 @@ def split(case: Case, ranks: int, rank0: int = 0) -> List[Slab]:
     return slabs
 
 
-class SlabRun:
-    """Step a split box case on `ranks` handles.
+def ghost_sources(slabs: List[Slab]):
+    """(slab, ghost plane, owner slab, owner's plane) of every ghost plane,
+    all in local plane indices, in a fixed order (every rank lists them the
+    same way)."""
+    def owner(plane):
+        for s in slabs:
+            if s.planes[s.own_lo] <= plane < s.planes[s.own_lo] + (s.own_hi - s.own_lo):
+                return s
+        raise AssertionError(plane)
+    out = []
+    for s in slabs:
+        for j in range(len(s.planes)):
+            if not s.own_lo <= j < s.own_hi:
+                o = owner(s.planes[j])
+                out.append((s, j, o, o.planes.index(s.planes[j], o.own_lo, o.own_hi)))
+    return out
 
-    make_handle(case) -> an object with upload(**fields), download() -> dict
-    of the fields in the reference layouts, set_time(t), get_time() and
-    op(name, field=None) for the reference operators named as the Lattice
-    methods (equilibrium, collision, lbstream, update_boundaries,
-    macro_density, heat_source, macro_temperature, inter_force,
-    macro_velocity).  See LatticeHandle for device handles.
-    """
 
-    def __init__(self, case: Case, ranks: int, make_handle: Callable, rank0: int = 0, staged: bool = False):
+class _SlabSteps:
+    """The reference's step on the slabs this process drives (self.local:
+    (slab, handle) pairs), with exchange(names) refreshing ghost planes."""
+
+    def _setup(self, case):
         self.case = case
-        self.slabs = split(case, ranks, rank0)
-        self.handles = [make_handle(s.case) for s in self.slabs]
-        # device-to-device ghost copies when every handle offers them
-        self.direct = not staged and all(hasattr(h, "copy_from") for h in self.handles)
         _, self.P, _ = _box_geometry(case)
         self.has_g = case.g is not None
         self.f_on = case.f is not None and bool(case.f.get("update", 1))
         self.g_on = self.has_g and bool(case.g.get("update", 1))
 
-    # -------------------------------------------------------------- exchange
-    def _owner(self, plane):
-        for s in self.slabs:
-            if s.planes[s.own_lo] <= plane < s.planes[s.own_lo] + (s.own_hi - s.own_lo):
-                return s
-        raise AssertionError(plane)
-
-    def ghost_sources(self):
-        """(slab, ghost plane, owner slab, owner's plane) of every ghost plane,
-        all in local plane indices."""
-        out = []
-        for s in self.slabs:
-            for j in range(len(s.planes)):
-                if not s.own_lo <= j < s.own_hi:
-                    o = self._owner(s.planes[j])
-                    out.append((s, j, o, o.planes.index(s.planes[j], o.own_lo, o.own_hi)))
-        return out
-
-    def exchange(self, names):
-        """Ghost planes of the fields `names` from their owners."""
-        P = self.P
-        if self.direct:
-            for s, j, o, oj in self.ghost_sources():
-                self.handles[s.rank].copy_from(self.handles[o.rank], j * P, oj * P, P, names)
-            return
-        states = [h.download() for h in self.handles]
-        for s, j, o, oj in self.ghost_sources():
-            st, src = states[s.rank], states[o.rank]
-            for nm in names:
-                st[nm][j * P:(j + 1) * P] = src[nm][oj * P:(oj + 1) * P]
-        for h, st in zip(self.handles, states):
-            up = {nm: st[nm] for nm in FIELDS if not (nm == "g" and not self.has_g)}
-            h.upload(**up)
-
     def _all(self, name, field=None):
-        for h in self.handles:
+        for _, h in self.local:
             h.op(name, field)
 
-    # ------------------------------------------------------------- the loop
+    def _upload_fields(self, h, st):
+        h.upload(**{nm: st[nm] for nm in FIELDS if not (nm == "g" and not self.has_g)})
+
     def initialize(self):
         """multiPhasePP.c:122-147 on every slab, ghosts exchanged."""
-        for h, s in zip(self.handles, self.slabs):
+        for s, h in self.local:
             h.upload(rho=s.case.rho, U=s.case.U, T=s.case.T)
         self._all("equilibrium", abi.FIELD_F)
         if self.has_g:
@@ -192,7 +167,7 @@ class SlabRun:
     def step(self, n=1):
         """multiPhasePP.c:157-240 with the ghost exchanges of the reference."""
         for _ in range(n):
-            for h in self.handles:
+            for _, h in self.local:
                 h.set_time(h.get_time() + 1)
             for fi, on, name in ((abi.FIELD_F, self.f_on, "f"), (abi.FIELD_G, self.g_on, "g")):
                 if not on:
@@ -211,18 +186,120 @@ class SlabRun:
                 self.exchange(("Fi", "Ft"))
             self._all("macro_velocity")
 
+    def owned(self):
+        """(global node indices, fields) of the owned planes of this
+        process's slabs."""
+        out = []
+        for s, h in self.local:
+            st = h.download()
+            lo, hi = s.own_lo * self.P, s.own_hi * self.P
+            out.append((s.gidx[lo:hi], {k: v[lo:hi] for k, v in st.items()}))
+        return out
+
+    def _assemble(self, parts):
+        n = self.case.n
+        out = {}
+        for gi, st in parts:
+            for k, v in st.items():
+                if k not in out:
+                    out[k] = np.zeros((n,) + v.shape[1:])
+                out[k][gi] = v
+        return out
+
+
+class SlabRun(_SlabSteps):
+    """Step a split box case on `ranks` handles, all driven by this process.
+
+    make_handle(case) -> an object with upload(**fields), download() -> dict
+    of the fields in the reference layouts, set_time(t), get_time() and
+    op(name, field=None) for the reference operators named as the Lattice
+    methods (equilibrium, collision, lbstream, update_boundaries,
+    macro_density, heat_source, macro_temperature, inter_force,
+    macro_velocity).  See LatticeHandle for device handles.
+    """
+
+    def __init__(self, case: Case, ranks: int, make_handle: Callable, rank0: int = 0, staged: bool = False):
+        self._setup(case)
+        self.slabs = split(case, ranks, rank0)
+        self.handles = [make_handle(s.case) for s in self.slabs]
+        self.local = list(zip(self.slabs, self.handles))
+        # device-to-device ghost copies when every handle offers them
+        self.direct = not staged and all(hasattr(h, "copy_from") for h in self.handles)
+
+    def exchange(self, names):
+        """Ghost planes of the fields `names` from their owners."""
+        P = self.P
+        if self.direct:
+            for s, j, o, oj in ghost_sources(self.slabs):
+                self.handles[s.rank].copy_from(self.handles[o.rank], j * P, oj * P, P, names)
+            return
+        states = [h.download() for h in self.handles]
+        for s, j, o, oj in ghost_sources(self.slabs):
+            st, src = states[s.rank], states[o.rank]
+            for nm in names:
+                st[nm][j * P:(j + 1) * P] = src[nm][oj * P:(oj + 1) * P]
+        for h, st in zip(self.handles, states):
+            self._upload_fields(h, st)
+
     def gather(self):
         """The owned planes of every slab, as the single-domain fields."""
-        n = self.case.n
-        out = None
-        for s, h in zip(self.slabs, self.handles):
-            st = h.download()
-            if out is None:
-                out = {k: np.zeros((n,) + st[k].shape[1:]) for k in st}
-            lo, hi = s.own_lo * self.P, s.own_hi * self.P
-            for k in st:
-                out[k][s.gidx[lo:hi]] = st[k][lo:hi]
-        return out
+        return self._assemble(self.owned())
+
+
+class DistSlabRun(_SlabSteps):
+    """One slab per process of a torch.distributed group, as one reference
+    MPI rank per process: the ghost planes travel by point-to-point messages
+    (isend / irecv of the planes' values, in the order ghost_sources lists
+    them; tensors on `device`, e.g. CUDA for NCCL, CPU for gloo).  The group's
+    rank r holds slab r and runs as reference rank rank0 + r."""
+
+    def __init__(self, case: Case, make_handle: Callable, group=None, rank0: int = 0, device="cpu"):
+        import torch
+        import torch.distributed as dist
+        self._torch, self._dist, self.group = torch, dist, group
+        self._setup(case)
+        self.rank = dist.get_rank(group)
+        self.slabs = split(case, dist.get_world_size(group), rank0)
+        self.slab = self.slabs[self.rank]
+        self.handle = make_handle(self.slab.case)
+        self.local = [(self.slab, self.handle)]
+        self.device = torch.device(device)
+
+    def _peer(self, r):
+        return r if self.group is None else self._dist.get_global_rank(self.group, r)
+
+    def exchange(self, names):
+        torch, dist, P = self._torch, self._dist, self.P
+        st = self.handle.download()
+        ops, recvs = [], []
+        for tag, (s, j, o, oj) in enumerate(ghost_sources(self.slabs)):
+            if o.rank == self.rank and s.rank != self.rank:
+                buf = np.concatenate([st[nm][oj * P:(oj + 1) * P].reshape(-1) for nm in names])
+                t = torch.from_numpy(buf).to(self.device)
+                ops.append(dist.P2POp(dist.isend, t, self._peer(s.rank), self.group, tag))
+            elif s.rank == self.rank and o.rank != self.rank:
+                size = sum(st[nm][j * P:(j + 1) * P].size for nm in names)
+                t = torch.empty(size, dtype=torch.float64, device=self.device)
+                ops.append(dist.P2POp(dist.irecv, t, self._peer(o.rank), self.group, tag))
+                recvs.append((j, t))
+        # one group of sends and receives: two ranks that send to each other
+        # do not wait on each other's receive
+        if ops:
+            for r in dist.batch_isend_irecv(ops):
+                r.wait()
+        for j, t in recvs:
+            buf, off = t.cpu().numpy(), 0
+            for nm in names:
+                dst = st[nm][j * P:(j + 1) * P]
+                dst[...] = buf[off:off + dst.size].reshape(dst.shape)
+                off += dst.size
+        self._upload_fields(self.handle, st)
+
+    def gather(self):
+        """Every rank's owned planes, as the single-domain fields (on every rank)."""
+        parts = [None] * self._dist.get_world_size(self.group)
+        self._dist.all_gather_object(parts, self.owned(), group=self.group)
+        return self._assemble([p for ps in parts for p in ps])
 
 
 class LatticeHandle:
