@@ -11,7 +11,8 @@ plane on each cut (wrapping on a periodic axis), and a step runs the
 reference's operators on every slab with the ghost planes refreshed from
 their owners at the same points:
 
-    collision f, lbstream f, updateBoundaries f   -> ghost f
+    collision f                                    -> ghost f (surface tension on only)
+    lbstream f, updateBoundaries f                 -> ghost f
     collision g, lbstream g, updateBoundaries g   -> ghost g
     macroDensity
     heatSource                                     -> ghost S
@@ -20,16 +21,18 @@ their owners at the same points:
     macroVelocity
 
 Ghost nodes have no neighbours and lie on no boundary patch, as in the
-reference's partitioned meshes (latticeMeshPartition.c:564-590, 679-725);
-whatever a ghost node computes is overwritten by the exchange before an
-owned node reads it, except its post-collision PDFs, which the owned nodes
-next to a cut pull in lbstream.  Those equal the single domain's unless the
-collision needs neighbours: the surface-tension term is zero on a node with
-a missing neighbour, so with surface tension on, the reference's multi-rank
-run (and this one) differs from its single-domain run next to every cut.
-Without surface tension the gathered owned nodes are bit-identical to the
-single-domain run (tests/test_slabs.py).  fixedRandomT seeds rand() with the
-rank; slab r runs as rank rank0 + r.
+reference's partitioned meshes (latticeMeshPartition.c:564-590, 679-725):
+they do not stream, and whatever a ghost node computes is overwritten by an
+exchange before an owned node reads it.  The surface-tension collision needs
+neighbours, so with it on the reference collides the local nodes only and
+syncs the post-collision PDFs to the ghosts (liMRTCollision.c:33-37,126-131;
+xuMRTCollision.c:32-36,108-113); so does this runner.  The gathered owned
+nodes are then bit-identical to the single-domain run, with one exception
+that the reference has too: a fixedT / fixedU / fixedRandomT wall that
+crosses a cut extrapolates from the ghost's PDF, which has not streamed when
+the boundaries run (the exchange follows them), where the single domain
+reads the streamed value (tests/test_slabs.py).  fixedRandomT seeds rand()
+with the rank; slab r runs as rank rank0 + r.
 
 Between device handles (LatticeHandle) the exchange moves only the ghost
 planes, device to device (mplb_gpu_copy_nodes: one strided copy per field
@@ -142,6 +145,7 @@ class _SlabSteps:
         _, self.P, _ = _box_geometry(case)
         self.has_g = case.g is not None
         self.f_on = case.f is not None and bool(case.f.get("update", 1))
+        self.f_st = self.f_on and bool(case.f.get("surface_tension", 0))
         self.g_on = self.has_g and bool(case.g.get("update", 1))
 
     def _all(self, name, field=None):
@@ -173,6 +177,8 @@ class _SlabSteps:
                 if not on:
                     continue
                 self._all("collision", fi)
+                if fi == abi.FIELD_F and self.f_st:
+                    self.exchange(("f",))
                 self._all("lbstream", fi)
                 self._all("update_boundaries", fi)
                 self.exchange((name,))

@@ -49,6 +49,8 @@ def fields_of(case):
     ("lid_d2q9", 2),                             # fixedU lid
     ("my_column_d2q9", 3),                       # myMRT heat
     ("outflow_d2q9", 2),                         # outflow top, fixedRandomT bottom
+    ("st_d2q9", 2), ("st_d2q9", 3),              # surface tension: post-collision sync
+    ("st_d3q15", 2),
     ("bubble_d3q15", 3),                         # D3Q15, cut along z
     ("walls_d3q15", 2),
     ("my_slab_d3q15", 2),
@@ -64,32 +66,16 @@ def test_slabs_equal_single_domain(name, ranks):
     assert_same(run.gather(), want, fields=fields_of(case), ctx=f"{name} in {ranks} slabs")
 
 
-def test_cut_deviations_of_the_reference():
+def test_cut_deviation_of_the_reference():
     """Where the reference's multi-rank run differs from its single-domain
-    run, the split differs the same way and nowhere else.  A ghost node has no
-    neighbours, so (1) its collision has no surface-tension term
-    (liMRTSurfaceTension.c zeroes it on a node with a missing neighbour) and
-    the owned nodes next to a cut pull those PDFs in lbstream; (2) it does
-    not stream, and a fixedT / fixedU wall node next to a cut extrapolates
-    from the ghost's post-collision PDF (the exchange follows the
-    boundaries).  After one step the differing PDFs are exactly those."""
-    # (1) surface tension, 20 x 18 with walls in y: one cut at y = 9
-    case = small_cases()["st_d2q9"]
-    nx = case.dims[0]
-    want = run_checker("port", case, 1)
-    run = slabs.SlabRun(case, 2, CheckerHandle)
-    run.initialize()
-    run.step(1)
-    got = run.gather()
-    node, k = np.nonzero(got["f"] != want["f"])
-    assert len(node) > 0
-    src = case.nb[node, k]
-    assert ((node // nx >= 9) != (src // nx >= 9)).all()      # every one pulled across the cut
-    assert set((np.nonzero(got["rho"] != want["rho"])[0] // nx).tolist()) <= {8, 9}
-
-    # (2) fixedT side wall, 10 x 12 walled box in 3 slabs: cuts at y = 4 and 8
+    run, the split differs the same way and nowhere else: a ghost node does
+    not stream (lbstream.c loops over the local nodes), and a fixedT wall node
+    next to a cut extrapolates from the ghost's post-collision PDF (the
+    exchange follows the boundaries) where the single domain reads the
+    streamed one.  After one step the differing PDFs are exactly those."""
+    # fixedT side wall, 10 x 12 walled box in 3 slabs: cuts at y = 4 and 8
     case = small_cases()["outflow_corner_d2q9"]
-    nx, Q = case.dims[0], case.Q
+    nx = case.dims[0]
     want = run_checker("port", case, 1)
     run = slabs.SlabRun(case, 3, CheckerHandle, rank0=case.meta.get("rank", 0))
     run.initialize()
@@ -110,16 +96,6 @@ def orc_rev(case):
     from multiphaselb_b200 import cases as cs
     c = np.asarray(cs.VEL[case.lattice])
     return [int(np.nonzero((c == -c[k]).all(1))[0][0]) for k in range(len(c))]
-
-
-def test_surface_tension_off_is_bit_identical():
-    case = small_cases()["st_d2q9"]
-    case.f = dict(case.f, surface_tension=0)
-    want = run_checker("port", case, 6)
-    run = slabs.SlabRun(case, 2, CheckerHandle)
-    run.initialize()
-    run.step(6)
-    assert_same(run.gather(), want, fields=fields_of(case), ctx="st_d2q9 with the term off, 2 slabs")
 
 
 def test_split_layout():
@@ -185,7 +161,7 @@ dist.destroy_process_group()
 
 
 @pytest.mark.parametrize("name,world", [("column_d2q9", 2), ("bubble_d2q9", 3), ("outflow_d2q9", 2),
-                                        ("bubble_d3q15", 2)])
+                                        ("st_d2q9", 3), ("bubble_d3q15", 2)])
 def test_one_process_per_slab_gloo(tmp_path, name, world):
     """DistSlabRun: one slab per gloo rank, ghost planes by point-to-point
     messages; the gathered fields equal the single-domain run bitwise."""
