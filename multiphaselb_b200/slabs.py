@@ -1,15 +1,14 @@
-"""Slab decomposition of a box lattice over several handles (one per rank or
-device), with the reference's ghost-node exchange.
+"""Multi-rank runs of a lattice: the mesh split over ranks (one handle per
+rank, on one device or several), with the reference's ghost-node exchange.
 
 The reference runs each MPI rank on its part of the mesh plus ghost nodes
 and exchanges them inside the time step (multiPhasePP.c:163-240):
 sendPdfField / recvPdfField after each field's boundaries, syncScalarField
-of the heat source and syncVectorField of the interaction force.  Here a box
-(cases.box_mesh layout, x fastest) is cut into slabs along its slowest axis
-(y in 2D, z in 3D); each slab's lattice holds its own planes plus one ghost
-plane on each cut (wrapping on a periodic axis), and a step runs the
-reference's operators on every slab with the ghost planes refreshed from
-their owners at the same points:
+of the heat source and syncVectorField of the interaction force.  Every rank
+here holds its owned nodes and its ghost nodes, with per-peer lists of the
+ghost nodes it receives and of the owned nodes it sends (the
+recvGhosts / sendGhosts of the reference's partitioned meshes), and a step
+runs the reference's operators with the ghosts refreshed at the same points:
 
     collision f                                    -> ghost f (surface tension on only)
     lbstream f, updateBoundaries f                 -> ghost f
@@ -32,17 +31,26 @@ that the reference has too: a fixedT / fixedU / fixedRandomT wall that
 crosses a cut extrapolates from the ghost's PDF, which has not streamed when
 the boundaries run (the exchange follows them), where the single domain
 reads the streamed value (tests/test_slabs.py).  fixedRandomT seeds rand()
-with the rank; slab r runs as rank rank0 + r.
+with the rank.
 
-Between device handles (LatticeHandle) the exchange moves only the ghost
-planes, device to device (mplb_gpu_copy_nodes: one strided copy per field
-and plane, peer to peer when the slabs sit on different GPUs, ordered on the
-handles' streams without a host synchronisation).  Any other handle with the
-operator interface (a CPU checker in the tests) is exchanged through host
-copies of its fields: download, copy the ghost planes, upload.
+Three ways to get the ranks' parts:
+  split(case, R)          a box cut into R slabs along its slowest axis
+                          (y in 2D, z in 3D), one ghost plane per cut
+  partition(case, owner)  any mesh and an owner rank per node, indexed as the
+                          reference's partitioner does (localIndexing.c)
+  from_meshes(meshes,...) the reference's per-rank mesh files, read with
+                          mesh.read_lattice_mesh
+
+RankRun drives every part from one process.  Between device handles
+(LatticeHandle) the exchange moves only the ghost nodes, device to device
+(mplb_gpu_copy_nodes: one strided copy per field and contiguous run of
+nodes, peer to peer between GPUs, ordered on the handles' streams without a
+host synchronisation); other handles (a CPU checker in the tests) exchange
+through host copies of their fields.  DistRankRun is one part per process of
+a torch.distributed group, the ghosts sent as point-to-point messages.
 """
-from dataclasses import dataclass
-from typing import Callable, List
+from dataclasses import dataclass, field
+from typing import Callable, List, Optional
 
 import numpy as np
 
@@ -53,13 +61,21 @@ FIELDS = ("rho", "U", "T", "Fi", "Ft", "S", "f", "g")
 
 
 @dataclass
-class Slab:
-    rank: int
-    planes: List[int]        # global plane index of every local plane, in local order
-    own_lo: int              # local index of the first owned plane
-    own_hi: int              # one past the last owned plane (local index)
-    case: Case
-    gidx: np.ndarray         # global node of every local node
+class Part:
+    """One rank's lattice: owned nodes and ghost nodes."""
+    rank: int                    # index in the group
+    case: Case                   # the rank's nodes, neighbour table, patches and fields
+    own: np.ndarray              # local indices of the owned nodes
+    recv: List[np.ndarray]       # per peer: local ghost nodes filled from that peer, in message order
+    send: List[np.ndarray]       # per peer: local owned nodes sent to that peer, in message order
+    gidx: Optional[np.ndarray] = None   # global node of every local node, where known
+
+
+@dataclass
+class Slab(Part):
+    planes: List[int] = field(default_factory=list)  # global plane of every local plane
+    own_lo: int = 0              # local index of the first owned plane
+    own_hi: int = 0              # one past the last owned plane
 
 
 def _box_geometry(case):
@@ -69,6 +85,30 @@ def _box_geometry(case):
     plane = int(np.prod(dims[:-1]))
     periodic = bool(case.periodic[-1])
     return nplanes, plane, periodic
+
+
+def _local_case(case, name, gidx, own_mask_local, local_of, owned_global, rank, dims=None, periodic=None):
+    """The Case of one rank: nodes gidx (owned ones first or not), neighbour
+    rows of the owned nodes mapped through local_of, ghost rows empty, and
+    the owned part of every patch."""
+    Q = case.Q
+    gnb = np.asarray(case.nb, dtype=np.int64)[gidx]
+    nb = np.where(gnb >= 0, local_of[np.maximum(gnb, 0)], -1)
+    nb[~own_mask_local] = -1
+    patches = []
+    for p in case.patches:
+        p = np.asarray(p, dtype=np.int64)
+        patches.append(local_of[p[owned_global[p]]].astype(np.uint32))
+    pts = np.asarray(case.points)[gidx].astype(np.int32)
+    d = 3 if case.lattice == abi.D3Q15 else 2
+    if dims is None:
+        dims = tuple(int(pts[:, j].max() - pts[:, j].min() + 1) for j in range(d))
+    if periodic is None:
+        periodic = (False,) * d
+    assert nb.shape == (len(gidx), Q)
+    return Case(name, case.lattice, tuple(dims), tuple(periodic), nb.astype(np.int32), pts, patches,
+                list(case.patch_names), case.eos, case.f, case.g, np.asarray(case.rho)[gidx],
+                np.asarray(case.U)[gidx], np.asarray(case.T)[gidx], meta=dict(case.meta, box=False, rank=rank))
 
 
 def split(case: Case, ranks: int, rank0: int = 0) -> List[Slab]:
@@ -88,33 +128,23 @@ def split(case: Case, ranks: int, rank0: int = 0) -> List[Slab]:
         planes = ([lo] if lo is not None else []) + list(range(a, b)) + ([hi] if hi is not None else [])
         own_lo = 1 if lo is not None else 0
         own_hi = own_lo + (b - a)
-        where = {p: j for j, p in enumerate(planes)}
         gidx = np.concatenate([p * P + np.arange(P) for p in planes]).astype(np.int64)
-        # neighbour table: the global source mapped into the slab, -1 outside it
-        gnb = np.asarray(case.nb, dtype=np.int64)[gidx]
-        src_plane = np.where(gnb >= 0, gnb // P, -1)
-        lut = np.full(nplanes, -1, dtype=np.int64)
-        for p, j in where.items():
-            lut[p] = j
-        lj = np.where(gnb >= 0, lut[np.maximum(src_plane, 0)], -1)
-        nb = np.where(lj >= 0, lj * P + gnb % P, -1).astype(np.int32)
-        # ghost nodes get no neighbours, as in the reference's partition
-        # (latticeMeshPartition.c:564-590 fills nb for local nodes only)
-        nb[:own_lo * P] = -1
-        nb[own_hi * P:] = -1
-        # owned part of every patch, in patch order
-        owned = np.zeros(case.n, dtype=bool)
-        owned[a * P:b * P] = True
         local_of = np.full(case.n, -1, dtype=np.int64)
-        local_of[gidx[own_lo * P:own_hi * P]] = np.arange(own_lo * P, own_hi * P)
-        patches = [local_of[np.asarray(p, dtype=np.int64)[owned[np.asarray(p, dtype=np.int64)]]].astype(np.uint32)
-                   for p in case.patches]
-        pts = np.asarray(case.points)[gidx]
-        local = Case(f"{case.name}_slab{r}", case.lattice, tuple(case.dims[:-1]) + (len(planes),),
-                     tuple(case.periodic[:-1]) + (False,), nb, pts.astype(np.int32), patches,
-                     list(case.patch_names), case.eos, case.f, case.g, np.asarray(case.rho)[gidx],
-                     np.asarray(case.U)[gidx], np.asarray(case.T)[gidx], meta=dict(case.meta, box=False, rank=rank0 + r))
-        slabs.append(Slab(r, planes, own_lo, own_hi, local, gidx))
+        local_of[gidx] = np.arange(len(gidx))
+        own_mask = np.zeros(len(gidx), dtype=bool)
+        own_mask[own_lo * P:own_hi * P] = True
+        owned_global = np.zeros(case.n, dtype=bool)
+        owned_global[a * P:b * P] = True
+        local = _local_case(case, f"{case.name}_slab{r}", gidx, own_mask, local_of, owned_global, rank0 + r,
+                            dims=tuple(case.dims[:-1]) + (len(planes),),
+                            periodic=tuple(case.periodic[:-1]) + (False,))
+        empty = [np.zeros(0, dtype=np.int64) for _ in range(ranks)]
+        slabs.append(Slab(r, local, np.arange(own_lo * P, own_hi * P), list(empty), list(empty), gidx,
+                          planes, own_lo, own_hi))
+    # message lists, in ghost_sources order on both sides
+    for s, j, o, oj in ghost_sources(slabs):
+        s.recv[o.rank] = np.concatenate([s.recv[o.rank], np.arange(j * P, (j + 1) * P)])
+        o.send[s.rank] = np.concatenate([o.send[s.rank], np.arange(oj * P, (oj + 1) * P)])
     return slabs
 
 
@@ -136,17 +166,101 @@ def ghost_sources(slabs: List[Slab]):
     return out
 
 
-class _SlabSteps:
-    """The reference's step on the slabs this process drives (self.local:
-    (slab, handle) pairs), with exchange(names) refreshing ghost planes."""
+def partition(case: Case, owner, rank0: int = 0) -> List[Part]:
+    """Split any mesh by an owner rank per node, as the reference's
+    partitioner does: a rank's local nodes are its owned nodes in global
+    order, then its ghosts (every pull source of an owned node owned
+    elsewhere) in the order a scan of the owned nodes and their velocities
+    first meets them (localIndexing.c:7-95); the ghost lists pair the
+    receiving rank's ghost with the owner's node, in global node order
+    (latticeMeshPartition.c:745-770).  Rank r runs as rank0 + r."""
+    owner = np.asarray(owner, dtype=np.int64)
+    n = case.n
+    if owner.shape != (n,) or owner.min() < 0:
+        raise ValueError("owner needs one rank >= 0 per node")
+    ranks = int(owner.max()) + 1
+    nb = np.asarray(case.nb, dtype=np.int64)
+    locals_, gidxs, nlocal = [], [], []
+    for r in range(ranks):
+        own = np.nonzero(owner == r)[0]
+        if len(own) == 0:
+            raise ValueError(f"rank {r} owns no node")
+        local_of = np.full(n, -1, dtype=np.int64)
+        local_of[own] = np.arange(len(own))
+        cand = nb[own].reshape(-1)
+        cand = cand[cand >= 0]
+        cand = cand[local_of[cand] < 0]
+        _, first = np.unique(cand, return_index=True)
+        ghosts = cand[np.sort(first)]
+        local_of[ghosts] = len(own) + np.arange(len(ghosts))
+        locals_.append(local_of)
+        gidxs.append(np.concatenate([own, ghosts]))
+        nlocal.append(len(own))
+    parts = []
+    for r in range(ranks):
+        gidx = gidxs[r]
+        own_mask = np.zeros(len(gidx), dtype=bool)
+        own_mask[:nlocal[r]] = True
+        local = _local_case(case, f"{case.name}_rank{r}", gidx, own_mask, locals_[r], owner == r, rank0 + r)
+        parts.append(Part(r, local, np.arange(nlocal[r]), [None] * ranks, [None] * ranks, gidx))
+    for r in range(ranks):
+        ghosts = np.sort(gidxs[r][nlocal[r]:])       # global node order
+        for s in range(ranks):
+            sel = ghosts[owner[ghosts] == s] if s != r else ghosts[:0]
+            parts[r].recv[s] = locals_[r][sel]
+            parts[s].send[r] = locals_[s][sel]
+    return parts
 
-    def _setup(self, case):
-        self.case = case
-        _, self.P, _ = _box_geometry(case)
-        self.has_g = case.g is not None
-        self.f_on = case.f is not None and bool(case.f.get("update", 1))
-        self.f_st = self.f_on and bool(case.f.get("surface_tension", 0))
-        self.g_on = self.has_g and bool(case.g.get("update", 1))
+
+def from_meshes(meshes, name, eos, f, g, fields, rank0: int = 0) -> List[Part]:
+    """Parts from the reference's per-rank mesh files (mesh.LatticeMesh of
+    every rank, as read_lattice_mesh returns them) and each rank's initial
+    (rho, U, T) over its nlocal + nghosts nodes.  Rank r runs as rank0 + r."""
+    parts = []
+    ranks = len(meshes)
+    for r, (m, (rho, U, T)) in enumerate(zip(meshes, fields)):
+        npts = m.nlocal + m.nghosts
+        nb = np.full((npts, m.Q), -1, dtype=np.int32)
+        nb[:m.nlocal] = np.asarray(m.nb, dtype=np.int32)
+        pts = np.asarray(m.points, dtype=np.int32)
+        d = 3 if m.lattice == abi.D3Q15 else 2
+        dims = tuple(int(pts[:, j].max() - pts[:, j].min() + 1) for j in range(d))
+        case = Case(f"{name}_rank{r}", m.lattice, dims, (False,) * d, nb, pts, list(m.patches),
+                    list(m.patch_names), eos, f, g, np.asarray(rho, dtype=np.float64),
+                    np.asarray(U, dtype=np.float64), np.asarray(T, dtype=np.float64),
+                    meta=dict(box=False, rank=rank0 + r))
+        lists = lambda ls: [np.asarray(ls[s], dtype=np.int64) if s < len(ls) else np.zeros(0, dtype=np.int64)
+                            for s in range(ranks)]
+        parts.append(Part(r, case, np.arange(m.nlocal), lists(m.recv_ghosts), lists(m.send_ghosts)))
+    for r, p in enumerate(parts):
+        for s, q in enumerate(parts):
+            if len(p.recv[s]) != len(q.send[r]):
+                raise ValueError(f"rank {r} receives {len(p.recv[s])} ghosts from rank {s}, which sends "
+                                 f"{len(q.send[r])}")
+    return parts
+
+
+def node_runs(dst, src):
+    """Pairs of local node lists -> (dst_start, src_start, count) runs where
+    both lists step by one."""
+    dst, src = np.asarray(dst, dtype=np.int64), np.asarray(src, dtype=np.int64)
+    if len(dst) == 0:
+        return []
+    brk = np.nonzero((np.diff(dst) != 1) | (np.diff(src) != 1))[0] + 1
+    starts = np.concatenate([[0], brk])
+    ends = np.concatenate([brk, [len(dst)]])
+    return [(int(dst[a]), int(src[a]), int(b - a)) for a, b in zip(starts, ends)]
+
+
+class _Steps:
+    """The reference's step on the parts this process drives (self.local:
+    (part, handle) pairs), with exchange(names) refreshing ghost nodes."""
+
+    def _setup(self, case_like):
+        self.has_g = case_like.g is not None
+        self.f_on = case_like.f is not None and bool(case_like.f.get("update", 1))
+        self.f_st = self.f_on and bool(case_like.f.get("surface_tension", 0))
+        self.g_on = self.has_g and bool(case_like.g.get("update", 1))
 
     def _all(self, name, field=None):
         for _, h in self.local:
@@ -156,9 +270,10 @@ class _SlabSteps:
         h.upload(**{nm: st[nm] for nm in FIELDS if not (nm == "g" and not self.has_g)})
 
     def initialize(self):
-        """multiPhasePP.c:122-147 on every slab, ghosts exchanged."""
-        for s, h in self.local:
-            h.upload(rho=s.case.rho, U=s.case.U, T=s.case.T)
+        """multiPhasePP.c:122-147 on every rank, ghosts exchanged."""
+        for p, h in self.local:
+            h.upload(rho=p.case.rho, U=p.case.U, T=p.case.T)
+        self.exchange(("rho", "U", "T"))
         self._all("equilibrium", abi.FIELD_F)
         if self.has_g:
             self._all("equilibrium", abi.FIELD_G)
@@ -193,119 +308,159 @@ class _SlabSteps:
             self._all("macro_velocity")
 
     def owned(self):
-        """(global node indices, fields) of the owned planes of this
-        process's slabs."""
+        """(part, fields of its owned nodes) of every part of this process."""
         out = []
-        for s, h in self.local:
+        for p, h in self.local:
             st = h.download()
-            lo, hi = s.own_lo * self.P, s.own_hi * self.P
-            out.append((s.gidx[lo:hi], {k: v[lo:hi] for k, v in st.items()}))
+            out.append((p, {k: v[p.own] for k, v in st.items()}))
         return out
 
-    def _assemble(self, parts):
-        n = self.case.n
+    @staticmethod
+    def _assemble(parts, n):
         out = {}
-        for gi, st in parts:
+        for p, st in parts:
+            if p.gidx is None:
+                raise ValueError("parts read from mesh files have no global numbering")
             for k, v in st.items():
                 if k not in out:
                     out[k] = np.zeros((n,) + v.shape[1:])
-                out[k][gi] = v
+                out[k][p.gidx[p.own]] = v
         return out
 
 
-class SlabRun(_SlabSteps):
-    """Step a split box case on `ranks` handles, all driven by this process.
+class RankRun(_Steps):
+    """Step every part from this process.
 
     make_handle(case) -> an object with upload(**fields), download() -> dict
     of the fields in the reference layouts, set_time(t), get_time() and
     op(name, field=None) for the reference operators named as the Lattice
     methods (equilibrium, collision, lbstream, update_boundaries,
     macro_density, heat_source, macro_temperature, inter_force,
-    macro_velocity).  See LatticeHandle for device handles.
+    macro_velocity); with copy_from(src, dst_start, src_start, count, names)
+    the ghosts move handle to handle (LatticeHandle does this on the
+    devices), else through host copies.
     """
 
-    def __init__(self, case: Case, ranks: int, make_handle: Callable, rank0: int = 0, staged: bool = False):
-        self._setup(case)
-        self.slabs = split(case, ranks, rank0)
-        self.handles = [make_handle(s.case) for s in self.slabs]
-        self.local = list(zip(self.slabs, self.handles))
-        # device-to-device ghost copies when every handle offers them
+    def __init__(self, parts: List[Part], make_handle: Callable, staged: bool = False, n_global=None):
+        self.parts = parts
+        self._setup(parts[0].case)
+        self.n_global = n_global
+        self.handles = [make_handle(p.case) for p in parts]
+        self.local = list(zip(parts, self.handles))
+        # (dst rank, dst start, src rank, src start, count) of every run of ghosts
+        self.transfers = []
+        for p in parts:
+            for s, q in enumerate(parts):
+                for d0, s0, c in node_runs(p.recv[s], q.send[p.rank]):
+                    self.transfers.append((p.rank, d0, s, s0, c))
         self.direct = not staged and all(hasattr(h, "copy_from") for h in self.handles)
 
     def exchange(self, names):
-        """Ghost planes of the fields `names` from their owners."""
-        P = self.P
+        """Ghost nodes of the fields `names` from their owners."""
         if self.direct:
-            for s, j, o, oj in ghost_sources(self.slabs):
-                self.handles[s.rank].copy_from(self.handles[o.rank], j * P, oj * P, P, names)
+            for d, d0, s, s0, c in self.transfers:
+                self.handles[d].copy_from(self.handles[s], d0, s0, c, names)
             return
         states = [h.download() for h in self.handles]
-        for s, j, o, oj in ghost_sources(self.slabs):
-            st, src = states[s.rank], states[o.rank]
+        for d, d0, s, s0, c in self.transfers:
             for nm in names:
-                st[nm][j * P:(j + 1) * P] = src[nm][oj * P:(oj + 1) * P]
+                states[d][nm][d0:d0 + c] = states[s][nm][s0:s0 + c]
         for h, st in zip(self.handles, states):
             self._upload_fields(h, st)
 
     def gather(self):
-        """The owned planes of every slab, as the single-domain fields."""
-        return self._assemble(self.owned())
+        """The owned nodes of every part, as the single-domain fields."""
+        n = self.n_global
+        if n is None:
+            n = sum(len(p.own) for p in self.parts)
+        return self._assemble(self.owned(), n)
+
+    def close(self):
+        for h in self.handles:
+            if hasattr(h, "close"):
+                h.close()
 
 
-class DistSlabRun(_SlabSteps):
-    """One slab per process of a torch.distributed group, as one reference
-    MPI rank per process: the ghost planes travel by point-to-point messages
-    (isend / irecv of the planes' values, in the order ghost_sources lists
-    them; tensors on `device`, e.g. CUDA for NCCL, CPU for gloo).  The group's
-    rank r holds slab r and runs as reference rank rank0 + r."""
+class SlabRun(RankRun):
+    """A box case cut into `ranks` slabs (split) and stepped from this
+    process; slab r runs as rank rank0 + r."""
 
-    def __init__(self, case: Case, make_handle: Callable, group=None, rank0: int = 0, device="cpu"):
+    def __init__(self, case: Case, ranks: int, make_handle: Callable, rank0: int = 0, staged: bool = False):
+        self.case = case
+        self.slabs = split(case, ranks, rank0)
+        super().__init__(self.slabs, make_handle, staged=staged, n_global=case.n)
+
+
+class DistRankRun(_Steps):
+    """One part per process of a torch.distributed group, as one reference
+    MPI rank per process: the ghosts travel as one message per peer and
+    exchange (isend / irecv of the listed nodes' values, grouped so that two
+    ranks sending to each other do not wait on each other's receive; tensors
+    on `device`, e.g. CUDA for NCCL, CPU for gloo).  `part` is this rank's
+    (its recv / send lists are all the exchange needs)."""
+
+    def __init__(self, part: Part, make_handle: Callable, group=None, device="cpu", n_global=None):
         import torch
         import torch.distributed as dist
         self._torch, self._dist, self.group = torch, dist, group
-        self._setup(case)
-        self.rank = dist.get_rank(group)
-        self.slabs = split(case, dist.get_world_size(group), rank0)
-        self.slab = self.slabs[self.rank]
-        self.handle = make_handle(self.slab.case)
-        self.local = [(self.slab, self.handle)]
+        if part.rank != dist.get_rank(group):
+            raise ValueError(f"part of rank {part.rank} given to rank {dist.get_rank(group)}")
+        self.part = part
+        self._setup(part.case)
+        self.handle = make_handle(part.case)
+        self.local = [(part, self.handle)]
         self.device = torch.device(device)
+        self.n_global = n_global
 
     def _peer(self, r):
         return r if self.group is None else self._dist.get_global_rank(self.group, r)
 
     def exchange(self, names):
-        torch, dist, P = self._torch, self._dist, self.P
+        torch, dist, p = self._torch, self._dist, self.part
         st = self.handle.download()
         ops, recvs = [], []
-        for tag, (s, j, o, oj) in enumerate(ghost_sources(self.slabs)):
-            if o.rank == self.rank and s.rank != self.rank:
-                buf = np.concatenate([st[nm][oj * P:(oj + 1) * P].reshape(-1) for nm in names])
-                t = torch.from_numpy(buf).to(self.device)
-                ops.append(dist.P2POp(dist.isend, t, self._peer(s.rank), self.group, tag))
-            elif s.rank == self.rank and o.rank != self.rank:
-                size = sum(st[nm][j * P:(j + 1) * P].size for nm in names)
+        for peer in range(len(p.send)):
+            idx = p.send[peer]
+            if peer != p.rank and len(idx):
+                buf = np.concatenate([st[nm][idx].reshape(-1) for nm in names])
+                ops.append(dist.P2POp(dist.isend, torch.from_numpy(buf).to(self.device), self._peer(peer),
+                                      self.group))
+        for peer in range(len(p.recv)):
+            idx = p.recv[peer]
+            if peer != p.rank and len(idx):
+                size = sum(st[nm][idx].size for nm in names)
                 t = torch.empty(size, dtype=torch.float64, device=self.device)
-                ops.append(dist.P2POp(dist.irecv, t, self._peer(o.rank), self.group, tag))
-                recvs.append((j, t))
-        # one group of sends and receives: two ranks that send to each other
-        # do not wait on each other's receive
+                ops.append(dist.P2POp(dist.irecv, t, self._peer(peer), self.group))
+                recvs.append((idx, t))
         if ops:
             for r in dist.batch_isend_irecv(ops):
                 r.wait()
-        for j, t in recvs:
+        for idx, t in recvs:
             buf, off = t.cpu().numpy(), 0
             for nm in names:
-                dst = st[nm][j * P:(j + 1) * P]
-                dst[...] = buf[off:off + dst.size].reshape(dst.shape)
-                off += dst.size
+                shape = st[nm][idx].shape
+                size = int(np.prod(shape))
+                st[nm][idx] = buf[off:off + size].reshape(shape)
+                off += size
         self._upload_fields(self.handle, st)
 
     def gather(self):
-        """Every rank's owned planes, as the single-domain fields (on every rank)."""
+        """Every rank's owned nodes, as the single-domain fields (on every rank)."""
         parts = [None] * self._dist.get_world_size(self.group)
         self._dist.all_gather_object(parts, self.owned(), group=self.group)
-        return self._assemble([p for ps in parts for p in ps])
+        flat = [x for ps in parts for x in ps]
+        n = self.n_global if self.n_global is not None else sum(len(p.own) for p, _ in flat)
+        return self._assemble(flat, n)
+
+
+class DistSlabRun(DistRankRun):
+    """One slab of a box case per process: rank r of the group holds slab r
+    and runs as reference rank rank0 + r."""
+
+    def __init__(self, case: Case, make_handle: Callable, group=None, rank0: int = 0, device="cpu"):
+        import torch.distributed as dist
+        slabs = split(case, dist.get_world_size(group), rank0)
+        super().__init__(slabs[dist.get_rank(group)], make_handle, group=group, device=device, n_global=case.n)
 
 
 class LatticeHandle:

@@ -65,3 +65,21 @@ def test_copy_nodes_copies_ranges_of_every_field(gpu_lib):
             b.copy_nodes(b, 10, 12, 4)
         assert e.value.code == abi.E_ARG
         assert b.lib.mplb_gpu_copy_nodes(b.h, 0, a.h, 0, 1, 256) == abi.E_ARG
+
+
+@pytest.mark.parametrize("name", ["bubble_d2q9", "cylinder", "bubble_d3q15"])
+def test_device_partition_matches_checker_partition(gpu_lib, name):
+    """Irregular partitions: the ghosts of a rank form many short runs of
+    nodes, each one device copy per field."""
+    from tests.test_partition import OWNERS, get_case
+    case = get_case(name)
+    parts = slabs.partition(case, OWNERS[name](case))
+    outs = []
+    for make in (CheckerHandle, slabs.LatticeHandle):
+        run = slabs.RankRun(parts, make, n_global=case.n)
+        assert run.direct == (make is slabs.LatticeHandle)
+        run.initialize()
+        run.step(5)
+        outs.append(run.gather())
+        run.close()
+    assert_same(outs[1], outs[0], fields=fields_of(case), ctx=f"{name} partitioned, device vs checker")
