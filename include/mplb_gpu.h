@@ -300,6 +300,28 @@ enum {
 int mplb_gpu_copy_nodes(mplb_gpu_t* dst, uint32_t dst_start, mplb_gpu_t* src, uint32_t src_start,
                         uint32_t count, int32_t fields);
 
+/* Several ranks' lattices driven from one process (one handle per rank, on
+ * one GPU or several), each holding its owned nodes and its ghost nodes (no
+ * neighbours, on no patch: the layout of the reference's partitioned meshes).
+ * runs[] lists the ghost exchange once: nodes [src_start, src_start + count)
+ * of handle h[src] fill nodes [dst_start, ...) of handle h[dst].
+ * mplb_ranks_initialize is multiPhasePP.c:122-147 on every rank (after the
+ * caller's uploads of rho, U, T) with the ghosts of rho, U, T, then Fi, Ft,
+ * then S exchanged; mplb_ranks_step is nsteps of multiPhasePP.c:157-240 on
+ * every rank, exchanging the ghosts with mplb_gpu_copy_nodes where the
+ * reference exchanges them: f after its boundaries (and after its collision
+ * when surface tension is on, liMRTCollision.c:126-131), g after its
+ * boundaries, S after heatSource, Fi and Ft after interForce.  All handles
+ * hold the same lattice and field options. */
+typedef struct mplb_ghost_run {
+    uint32_t dst, dst_start;
+    uint32_t src, src_start;
+    uint32_t count;
+} mplb_ghost_run;
+int mplb_ranks_initialize(mplb_gpu_t* const* h, uint32_t count, const mplb_ghost_run* runs, uint32_t nruns);
+int mplb_ranks_step(mplb_gpu_t* const* h, uint32_t count, const mplb_ghost_run* runs, uint32_t nruns,
+                    uint32_t nsteps);
+
 /* Total mass sum(rho[i]) and energy sum(T[i]) of plain device arrays, without
  * allocating device memory.  No counterpart in the reference: it is for
  * callers that may not call cudaMalloc where they want this check (a

@@ -70,6 +70,8 @@ def load_library(path=LIB_PATH):
         "mplb_gpu_mass_energy": ([H, D, D], C.c_int),
         "mplb_gpu_sync": ([H], C.c_int),
         "mplb_gpu_copy_nodes": ([H, C.c_uint32, H, C.c_uint32, C.c_uint32, C.c_int32], C.c_int),
+        "mplb_ranks_initialize": ([C.POINTER(H), C.c_uint32, C.POINTER(abi.GhostRun), C.c_uint32], C.c_int),
+        "mplb_ranks_step": ([C.POINTER(H), C.c_uint32, C.POINTER(abi.GhostRun), C.c_uint32, C.c_uint32], C.c_int),
         "mplb_gpu_snapshot": ([H, C.c_int32], C.c_int),
         "mplb_gpu_snapshot_wait": ([H, D, D, D, D], C.c_int),
         "mplb_gpu_snapshot_write": ([H, C.c_char_p, C.c_int32, C.c_int32], C.c_int),

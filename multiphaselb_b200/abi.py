@@ -99,6 +99,18 @@ class BatchOpts(C.Structure):
     ]
 
 
+class GhostRun(C.Structure):
+    """mplb_ghost_run: nodes [src_start, +count) of handle src fill nodes
+    [dst_start, +count) of handle dst."""
+    _fields_ = [
+        ("dst", C.c_uint32),
+        ("dst_start", C.c_uint32),
+        ("src", C.c_uint32),
+        ("src_start", C.c_uint32),
+        ("count", C.c_uint32),
+    ]
+
+
 class BatchInfo(C.Structure):
     _fields_ = [
         ("n_lattices", C.c_uint32),

@@ -1721,6 +1721,88 @@ int mplb_gpu_copy_nodes(mplb_gpu_t* dst, uint32_t dst_start, mplb_gpu_t* src, ui
 
 }  // extern "C"
 
+namespace {
+
+// The ranks of one process: every handle must hold the same lattice and
+// field options, and every run must name handles of the list.
+int ranks_check(mplb_gpu_t* const* h, uint32_t count, const mplb_ghost_run* runs, uint32_t nruns) {
+    if (!h || count == 0) return fail(MPLB_E_ARG, "no handles");
+    if (nruns && !runs) return fail(MPLB_E_ARG, "runs missing");
+    for (uint32_t r = 0; r < count; r++) {
+        if (!h[r]) return fail(MPLB_E_ARG, "NULL handle");
+        const mplb_gpu* a = h[0];
+        const mplb_gpu* b = h[r];
+        if (b->Q != a->Q || b->model[0] != a->model[0] || b->model[1] != a->model[1] ||
+            b->P.f_update != a->P.f_update || b->P.g_update != a->P.g_update || b->P.st_on != a->P.st_on)
+            return fail(MPLB_E_ARG, "the ranks' lattices or field options differ");
+    }
+    for (uint32_t i = 0; i < nruns; i++)
+        if (runs[i].dst >= count || runs[i].src >= count) return fail(MPLB_E_ARG, "run names a handle outside the list");
+    return 0;
+}
+
+int ranks_exchange(mplb_gpu_t* const* h, const mplb_ghost_run* runs, uint32_t nruns, int32_t fields) {
+    for (uint32_t i = 0; i < nruns; i++) {
+        const mplb_ghost_run& g = runs[i];
+        RET(mplb_gpu_copy_nodes(h[g.dst], g.dst_start, h[g.src], g.src_start, g.count, fields));
+    }
+    return 0;
+}
+
+}  // namespace
+
+extern "C" {
+
+int mplb_ranks_initialize(mplb_gpu_t* const* h, uint32_t count, const mplb_ghost_run* runs, uint32_t nruns) {
+    RET(ranks_check(h, count, runs, nruns));
+    RET(ranks_exchange(h, runs, nruns, MPLB_NODES_RHO | MPLB_NODES_U | MPLB_NODES_T));
+    for (uint32_t r = 0; r < count; r++) RET(mplb_gpu_equilibrium(h[r], MPLB_FIELD_F));
+    if (h[0]->model[1] != MPLB_NO_MODEL)
+        for (uint32_t r = 0; r < count; r++) RET(mplb_gpu_equilibrium(h[r], MPLB_FIELD_G));
+    for (uint32_t r = 0; r < count; r++) RET(mplb_gpu_inter_force(h[r]));
+    RET(ranks_exchange(h, runs, nruns, MPLB_NODES_FI | MPLB_NODES_FT));
+    if (h[0]->model[1] != MPLB_NO_MODEL && h[0]->P.g_update) {
+        for (uint32_t r = 0; r < count; r++) RET(mplb_gpu_heat_source(h[r]));
+        RET(ranks_exchange(h, runs, nruns, MPLB_NODES_S));
+    }
+    for (uint32_t r = 0; r < count; r++) h[r]->initialized = true;
+    return 0;
+}
+
+int mplb_ranks_step(mplb_gpu_t* const* h, uint32_t count, const mplb_ghost_run* runs, uint32_t nruns,
+                    uint32_t nsteps) {
+    RET(ranks_check(h, count, runs, nruns));
+    const bool f_on = h[0]->model[0] != MPLB_NO_MODEL && h[0]->P.f_update;
+    const bool g_on = h[0]->model[1] != MPLB_NO_MODEL && h[0]->P.g_update;
+    const bool f_st = f_on && h[0]->P.st_on;
+    for (uint32_t s = 0; s < nsteps; s++) {
+        for (uint32_t r = 0; r < count; r++) h[r]->current++;
+        for (int fi = 0; fi < 2; fi++) {
+            if (!(fi ? g_on : f_on)) continue;
+            const int32_t bit = fi ? MPLB_NODES_G : MPLB_NODES_F;
+            for (uint32_t r = 0; r < count; r++) RET(mplb_gpu_collision(h[r], fi));
+            if (fi == 0 && f_st) RET(ranks_exchange(h, runs, nruns, bit));
+            for (uint32_t r = 0; r < count; r++) RET(mplb_gpu_lbstream(h[r], fi));
+            for (uint32_t r = 0; r < count; r++) RET(mplb_gpu_update_boundaries(h[r], fi));
+            RET(ranks_exchange(h, runs, nruns, bit));
+        }
+        for (uint32_t r = 0; r < count; r++) RET(mplb_gpu_macro_density(h[r], 0, h[r]->n));
+        if (g_on) {
+            for (uint32_t r = 0; r < count; r++) RET(mplb_gpu_heat_source(h[r]));
+            RET(ranks_exchange(h, runs, nruns, MPLB_NODES_S));
+        }
+        for (uint32_t r = 0; r < count; r++) RET(mplb_gpu_macro_temperature(h[r], 0, h[r]->n));
+        if (f_on) {
+            for (uint32_t r = 0; r < count; r++) RET(mplb_gpu_inter_force(h[r]));
+            RET(ranks_exchange(h, runs, nruns, MPLB_NODES_FI | MPLB_NODES_FT));
+        }
+        for (uint32_t r = 0; r < count; r++) RET(mplb_gpu_macro_velocity(h[r], 0, h[r]->n));
+    }
+    return 0;
+}
+
+}  // extern "C"
+
 // ================================================================= batch
 struct mplb_batch {
     int dev = 0;

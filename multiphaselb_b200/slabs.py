@@ -45,10 +45,12 @@ RankRun drives every part from one process.  Between device handles
 (LatticeHandle) the exchange moves only the ghost nodes, device to device
 (mplb_gpu_copy_nodes: one strided copy per field and contiguous run of
 nodes, peer to peer between GPUs, ordered on the handles' streams without a
-host synchronisation); other handles (a CPU checker in the tests) exchange
+host synchronisation), and the whole step runs in the library
+(mplb_ranks_step); other handles (a CPU checker in the tests) exchange
 through host copies of their fields.  DistRankRun is one part per process of
 a torch.distributed group, the ghosts sent as point-to-point messages.
 """
+import ctypes as C
 from dataclasses import dataclass, field
 from typing import Callable, List, Optional
 
@@ -341,7 +343,8 @@ class RankRun(_Steps):
     devices), else through host copies.
     """
 
-    def __init__(self, parts: List[Part], make_handle: Callable, staged: bool = False, n_global=None):
+    def __init__(self, parts: List[Part], make_handle: Callable, staged: bool = False, n_global=None,
+                 native: bool = True):
         self.parts = parts
         self._setup(parts[0].case)
         self.n_global = n_global
@@ -354,6 +357,27 @@ class RankRun(_Steps):
                 for d0, s0, c in node_runs(p.recv[s], q.send[p.rank]):
                     self.transfers.append((p.rank, d0, s, s0, c))
         self.direct = not staged and all(hasattr(h, "copy_from") for h in self.handles)
+        # device lattices: the whole step in the library (mplb_ranks_step)
+        self.native = native and self.direct and all(isinstance(h, LatticeHandle) for h in self.handles)
+        if self.native:
+            self._lib = self.handles[0].lat.lib
+            self._harr = (C.c_void_p * len(self.handles))(*[h.lat.h.value for h in self.handles])
+            self._runs = (abi.GhostRun * max(1, len(self.transfers)))(
+                *[abi.GhostRun(d, d0, s, s0, c) for d, d0, s, s0, c in self.transfers])
+
+    def initialize(self):
+        if not self.native:
+            return super().initialize()
+        for p, h in self.local:
+            h.upload(rho=p.case.rho, U=p.case.U, T=p.case.T)
+        self.handles[0].lat._check(self._lib.mplb_ranks_initialize(self._harr, len(self.handles), self._runs,
+                                                                   len(self.transfers)))
+
+    def step(self, n=1):
+        if not self.native:
+            return super().step(n)
+        self.handles[0].lat._check(self._lib.mplb_ranks_step(self._harr, len(self.handles), self._runs,
+                                                             len(self.transfers), n))
 
     def exchange(self, names):
         """Ghost nodes of the fields `names` from their owners."""
@@ -385,10 +409,11 @@ class SlabRun(RankRun):
     """A box case cut into `ranks` slabs (split) and stepped from this
     process; slab r runs as rank rank0 + r."""
 
-    def __init__(self, case: Case, ranks: int, make_handle: Callable, rank0: int = 0, staged: bool = False):
+    def __init__(self, case: Case, ranks: int, make_handle: Callable, rank0: int = 0, staged: bool = False,
+                 native: bool = True):
         self.case = case
         self.slabs = split(case, ranks, rank0)
-        super().__init__(self.slabs, make_handle, staged=staged, n_global=case.n)
+        super().__init__(self.slabs, make_handle, staged=staged, n_global=case.n, native=native)
 
 
 class DistRankRun(_Steps):

@@ -46,6 +46,7 @@ STRUCTS = {
     "mplb_info": abi.Info,
     "mplb_batch_opts": abi.BatchOpts,
     "mplb_batch_info": abi.BatchInfo,
+    "mplb_ghost_run": abi.GhostRun,
 }
 
 

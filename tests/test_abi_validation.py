@@ -135,6 +135,8 @@ def test_null_handles_are_refused():
         lambda: lib.mplb_gpu_collision(None, 0),
         lambda: lib.mplb_gpu_macro_pressure(None),
         lambda: lib.mplb_gpu_copy_nodes(None, 0, None, 0, 1, 64),
+        lambda: lib.mplb_ranks_initialize(None, 0, None, 0),
+        lambda: lib.mplb_ranks_step(None, 2, None, 0, 1),
     ]
     for call in calls:
         assert call() == abi.E_ARG

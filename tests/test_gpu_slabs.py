@@ -1,7 +1,8 @@
 """Slab decomposition on the device: every slab a device lattice on the
 operator path (multiphaselb_b200.slabs.LatticeHandle), the ghost planes
 exchanged at the reference's points, against the same split run on CPU
-checkers; the ghost exchange device to device (mplb_gpu_copy_nodes) and
+checkers; the whole step in the library (mplb_ranks_step), the ghost
+exchange device to device driven from Python (mplb_gpu_copy_nodes), and
 through the host.  Bitwise.  Also mplb_gpu_copy_nodes itself: what it
 copies and what it refuses."""
 import numpy as np
@@ -14,9 +15,10 @@ from tests.test_slabs import CheckerHandle, fields_of
 pytestmark = pytest.mark.gpu
 
 
-def run_split(case, ranks, make, staged=False):
-    run = slabs.SlabRun(case, ranks, make, rank0=case.meta.get("rank", 0), staged=staged)
+def run_split(case, ranks, make, staged=False, native=True):
+    run = slabs.SlabRun(case, ranks, make, rank0=case.meta.get("rank", 0), staged=staged, native=native)
     assert run.direct == (make is slabs.LatticeHandle and not staged)
+    assert run.native == (run.direct and native)
     run.initialize()
     run.step(5)
     out = run.gather()
@@ -33,7 +35,9 @@ def test_device_slabs_match_checker_slabs(gpu_lib, name, ranks):
     want = run_split(case, ranks, CheckerHandle)
     fields = fields_of(case)
     assert_same(run_split(case, ranks, slabs.LatticeHandle), want, fields=fields,
-                ctx=f"{name} in {ranks} slabs, device-to-device exchange vs checker")
+                ctx=f"{name} in {ranks} slabs, whole step in the library vs checker")
+    assert_same(run_split(case, ranks, slabs.LatticeHandle, native=False), want, fields=fields,
+                ctx=f"{name} in {ranks} slabs, device-to-device exchange driven from Python vs checker")
     assert_same(run_split(case, ranks, slabs.LatticeHandle, staged=True), want, fields=fields,
                 ctx=f"{name} in {ranks} slabs, host-staged exchange vs checker")
 
@@ -77,7 +81,7 @@ def test_device_partition_matches_checker_partition(gpu_lib, name):
     outs = []
     for make in (CheckerHandle, slabs.LatticeHandle):
         run = slabs.RankRun(parts, make, n_global=case.n)
-        assert run.direct == (make is slabs.LatticeHandle)
+        assert run.native == (make is slabs.LatticeHandle)
         run.initialize()
         run.step(5)
         outs.append(run.gather())
