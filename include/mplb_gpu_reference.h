@@ -10,10 +10,16 @@
  *   #include <lbeField.h>
  *   #include "mplb_gpu_reference.h"
  *
- * Requires the DP build (scalar == double, src/dataTypes/dataTypes.h:19-21)
- * and one rank (nPoints == nlocal).  What it reads, with the reference
+ * Requires the DP build (scalar == double, src/dataTypes/dataTypes.h:19-21).
+ * A mesh is one rank's: the whole lattice at one rank (nPoints == nlocal),
+ * or a rank of a partitioned mesh (nlocal owned nodes, then the ghosts, which
+ * get no neighbours); mplb_ref_ghost_runs turns the ranks' ghost lists into
+ * the exchange of mplb_ranks_step.  What it reads, with the reference
  * definitions it follows:
  *   mesh->mesh.nb, points, bd            basicMesh   (src/dataTypes/basicMesh.h:19-70)
+ *   mesh->parallel.pid, worldSize,
+ *   nlocal, nrg, recvGhosts, nsg,
+ *   sendGhosts                           mpiInfo     (src/dataTypes/mpiInfo.h)
  *   mesh->EOS                            EOSInfo     (src/EOS/EOSInfo.h:80-102)
  *   field->model, lbparam, update,
  *   boundary[p].type / param             lbeField    (src/dataTypes/lbeField.h:32-108)
@@ -110,14 +116,18 @@ static inline void mplb_ref_pack_field(const latticeMesh* mesh, const lbeField* 
 /* Pack the reference's structures into descriptors (no device work). */
 static inline int mplb_ref_pack(const latticeMesh* mesh, const lbeField* f, const lbeField* g, mplb_ref_descs* d) {
     memset(d, 0, sizeof(*d));
-    if (mesh->parallel.worldSize != 1 || mesh->mesh.nPoints != mesh->parallel.nlocal) return MPLB_E_UNSUPPORTED;
-    uint32_t n = mesh->mesh.nPoints;
+    /* A rank of a partitioned mesh holds nlocal owned nodes, then its ghosts;
+     * readLatticeMesh.c:135-160 reads neighbours for the owned nodes only. */
+    if (mesh->parallel.worldSize < 1 || mesh->parallel.nlocal > mesh->mesh.nPoints ||
+        (mesh->parallel.worldSize == 1 && mesh->parallel.nlocal != mesh->mesh.nPoints))
+        return MPLB_E_UNSUPPORTED;
+    uint32_t n = mesh->mesh.nPoints, nlocal = mesh->parallel.nlocal;
     int Q = mesh->lattice.Q;
     d->nb = (int32_t*)malloc((size_t)n * Q * sizeof(int32_t));
     d->points = (int32_t*)malloc((size_t)n * 3 * sizeof(int32_t));
     if (!d->nb || !d->points) { mplb_ref_free(d); return MPLB_E_ARG; }
     for (uint32_t i = 0; i < n; i++) {
-        for (int k = 0; k < Q; k++) d->nb[(size_t)i * Q + k] = mesh->mesh.nb[i][k];
+        for (int k = 0; k < Q; k++) d->nb[(size_t)i * Q + k] = i < nlocal ? mesh->mesh.nb[i][k] : -1;
         for (int j = 0; j < 3; j++) d->points[(size_t)i * 3 + j] = mesh->mesh.points[i][j];
     }
     uint32_t np = mesh->mesh.bd.nbd, tot = 0;
@@ -220,6 +230,60 @@ static inline int mplb_ref_download(mplb_gpu_t* h, const latticeMesh* mesh, macr
     }
     free(U); free(Fi); free(Ft); free(fv); free(gv);
     return rc;
+}
+
+/* The ghost exchange of nranks ranks driven from one process
+ * (mplb_ranks_initialize / mplb_ranks_step), from their partitioned meshes:
+ * meshes[r] is rank r's mesh (readLatticeMesh(r)).  The i-th node of rank r's
+ * recvGhosts[s] is filled from the i-th node of rank s's sendGhosts[r], the
+ * pairing of the reference's exchange (sendPdfField.c:23-35 packs
+ * sendGhosts[pid] in order, recvPdfField.c:29-41 unpacks into
+ * recvGhosts[pid] in order).  Nodes that step by one on both sides merge
+ * into one run.  *runs is malloc'd (release it with free()).  Returns
+ * MPLB_E_ARG when a rank's pid or world size disagrees with its place in
+ * meshes[], or when rank r receives a different number of ghosts from s
+ * than s sends to r. */
+static inline int mplb_ref_ghost_runs(const latticeMesh* const* meshes, uint32_t nranks, mplb_ghost_run** runs,
+                                      uint32_t* nruns) {
+    *runs = NULL;
+    *nruns = 0;
+    uint32_t cap = 0;
+    for (uint32_t r = 0; r < nranks; r++)
+        if (meshes[r]->parallel.pid != r || meshes[r]->parallel.worldSize != nranks) return MPLB_E_ARG;
+    for (uint32_t r = 0; r < nranks; r++) {
+        const mpiInfo* pr = &meshes[r]->parallel;
+        for (uint32_t s = 0; s < nranks; s++) {
+            const mpiInfo* ps = &meshes[s]->parallel;
+            if (pr->nrg[s] != ps->nsg[r]) {
+                free(*runs);
+                *runs = NULL;
+                *nruns = 0;
+                return MPLB_E_ARG;
+            }
+            for (uint32_t i = 0; i < pr->nrg[s]; i++) {
+                uint32_t d0 = pr->recvGhosts[s][i], s0 = ps->sendGhosts[r][i];
+                mplb_ghost_run* last = (i > 0) ? &(*runs)[*nruns - 1] : NULL;
+                if (last && last->dst_start + last->count == d0 && last->src_start + last->count == s0) {
+                    last->count++;
+                    continue;
+                }
+                if (*nruns == cap) {
+                    cap = 2 * cap + 16;
+                    mplb_ghost_run* grown = (mplb_ghost_run*)realloc(*runs, cap * sizeof(mplb_ghost_run));
+                    if (!grown) {
+                        free(*runs);
+                        *runs = NULL;
+                        *nruns = 0;
+                        return MPLB_E_ARG;
+                    }
+                    *runs = grown;
+                }
+                mplb_ghost_run run = {r, d0, s, s0, 1};
+                (*runs)[(*nruns)++] = run;
+            }
+        }
+    }
+    return 0;
 }
 
 #endif /* MPLB_GPU_REFERENCE_H */

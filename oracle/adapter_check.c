@@ -98,3 +98,94 @@ int adapter_gpu_run(ref_case* c, uint32_t nsteps, int path, uint32_t start_time)
     mplb_gpu_destroy(h);
     return rc;
 }
+
+/* One rank of a partitioned mesh packed by mplb_ref_pack: the reference case's
+ * lattice, EOS and fields with the rank's own nodes (npts = nlocal owned +
+ * ghosts; nb_owned holds the owned nodes' neighbours, as readLatticeMesh reads
+ * them) and no patches.  0 when the descriptor holds the owned neighbours,
+ * no neighbours for the ghosts and every point; 1000 + code when the pack
+ * refuses. */
+int adapter_pack_part_check(ref_case* c, uint32_t npts, uint32_t nlocal, const int32_t* nb_owned,
+                            const int32_t* points, uint32_t pid, uint32_t world) {
+    latticeMesh* m;
+    macroFields* mf;
+    lbeField *f, *g;
+    ref_structs(c, &m, &mf, &f, &g);
+    const int Q = m->lattice.Q;
+    latticeMesh lm = *m;
+    int** nbrows = (int**)malloc((nlocal ? nlocal : 1) * sizeof(int*));
+    int** ptrows = (int**)malloc((npts ? npts : 1) * sizeof(int*));
+    for (uint32_t i = 0; i < nlocal; i++) nbrows[i] = (int*)(nb_owned + (size_t)i * Q);
+    for (uint32_t i = 0; i < npts; i++) ptrows[i] = (int*)(points + (size_t)i * 3);
+    lm.mesh.nPoints = npts;
+    lm.mesh.nb = nbrows;
+    lm.mesh.points = ptrows;
+    lm.mesh.bd.nbd = 0;
+    lm.parallel.pid = pid;
+    lm.parallel.worldSize = world;
+    lm.parallel.nlocal = nlocal;
+    lm.parallel.nghosts = npts - nlocal;
+    mplb_ref_descs d;
+    int rc = mplb_ref_pack(&lm, f, g, &d);
+    int bad = 0;
+    if (rc) bad = 1000 + (-rc);
+    else {
+        if (d.mesh.n_points != npts || d.mesh.n_patches != 0) bad |= 1;
+        for (uint32_t i = 0; i < npts; i++) {
+            for (int k = 0; k < Q; k++)
+                if (d.nb[(size_t)i * Q + k] != (i < nlocal ? nb_owned[(size_t)i * Q + k] : -1)) bad |= 2;
+            for (int j = 0; j < 3; j++)
+                if (d.points[(size_t)i * 3 + j] != points[(size_t)i * 3 + j]) bad |= 4;
+        }
+        mplb_ref_free(&d);
+    }
+    free(nbrows);
+    free(ptrows);
+    return bad;
+}
+
+/* mplb_ref_ghost_runs over nranks meshes that carry only their mpiInfo:
+ * nrg[r * nranks + s] ghosts of rank r come from rank s, listed in recv (rank
+ * major, peer minor); nsg and send likewise.  pid_of[r] is rank r's pid.
+ * The runs (dst, dst_start, src, src_start, count) go to out, at most cap. */
+int adapter_ghost_runs(uint32_t nranks, const uint32_t* pid_of, const uint32_t* nrg, const uint32_t* recv,
+                       const uint32_t* nsg, const uint32_t* send, uint32_t* out, uint32_t cap, uint32_t* nout) {
+    latticeMesh* ms = (latticeMesh*)calloc(nranks, sizeof(latticeMesh));
+    const latticeMesh** mp = (const latticeMesh**)malloc(nranks * sizeof(latticeMesh*));
+    uint** rg = (uint**)malloc((size_t)nranks * nranks * sizeof(uint*));
+    uint** sg = (uint**)malloc((size_t)nranks * nranks * sizeof(uint*));
+    size_t ro = 0, so = 0;
+    for (uint32_t r = 0; r < nranks; r++) {
+        mpiInfo* p = &ms[r].parallel;
+        p->pid = pid_of[r];
+        p->worldSize = nranks;
+        p->nrg = (uint*)(nrg + (size_t)r * nranks);
+        p->nsg = (uint*)(nsg + (size_t)r * nranks);
+        p->recvGhosts = rg + (size_t)r * nranks;
+        p->sendGhosts = sg + (size_t)r * nranks;
+        for (uint32_t s = 0; s < nranks; s++) {
+            p->recvGhosts[s] = (uint*)(recv + ro);
+            p->sendGhosts[s] = (uint*)(send + so);
+            ro += nrg[(size_t)r * nranks + s];
+            so += nsg[(size_t)r * nranks + s];
+        }
+        mp[r] = &ms[r];
+    }
+    mplb_ghost_run* runs = NULL;
+    uint32_t nruns = 0;
+    int rc = mplb_ref_ghost_runs(mp, nranks, &runs, &nruns);
+    *nout = nruns;
+    for (uint32_t i = 0; i < nruns && i < cap; i++) {
+        out[5 * i] = runs[i].dst;
+        out[5 * i + 1] = runs[i].dst_start;
+        out[5 * i + 2] = runs[i].src;
+        out[5 * i + 3] = runs[i].src_start;
+        out[5 * i + 4] = runs[i].count;
+    }
+    free(runs);
+    free(rg);
+    free(sg);
+    free(mp);
+    free(ms);
+    return rc;
+}
