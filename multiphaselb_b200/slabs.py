@@ -37,7 +37,9 @@ Three ways to get the ranks' parts:
   split(case, R)          a box cut into R slabs along its slowest axis
                           (y in 2D, z in 3D), one ghost plane per cut
   partition(case, owner)  any mesh and an owner rank per node, indexed as the
-                          reference's partitioner does (localIndexing.c)
+                          reference's partitioner does (localIndexing.c);
+                          standard_owner(n, R) is the owner array of the
+                          partitioner's default method
   from_meshes(meshes,...) the reference's per-rank mesh files, read with
                           mesh.read_lattice_mesh
 
@@ -166,6 +168,19 @@ def ghost_sources(slabs: List[Slab]):
                 o = owner(s.planes[j])
                 out.append((s, j, o, o.planes.index(s.planes[j], o.own_lo, o.own_hi)))
     return out
+
+
+def standard_owner(n: int, ranks: int) -> np.ndarray:
+    """Owner rank per node of the reference partitioner's default method
+    ("standard", standardDecomp.c:5-48): consecutive blocks of n // ranks
+    nodes in global node order, the last rank also taking the remainder.
+    The reference's unsigned arithmetic breaks when ranks > n (its first
+    block would end at node -1); that is refused here."""
+    n, ranks = int(n), int(ranks)
+    if ranks < 1 or ranks > n:
+        raise ValueError(f"standard decomposition of {n} nodes needs 1 <= ranks <= {n}, got {ranks}")
+    owner = np.minimum(np.arange(n, dtype=np.int64) // (n // ranks), ranks - 1)
+    return owner
 
 
 def partition(case: Case, owner, rank0: int = 0) -> List[Part]:

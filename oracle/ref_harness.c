@@ -259,6 +259,17 @@ int ref_download(ref_case* c, double* rho, double* U, double* T, double* Fi, dou
 void ref_set_time(ref_case* c, uint32_t t) { c->mesh.time.current = t; }
 void ref_set_rank(ref_case* c, int32_t pid) { c->mesh.parallel.pid = pid; }
 uint32_t ref_get_time(ref_case* c) { return c->mesh.time.current; }
+
+/* Owner rank per node from the reference partitioner's default method
+ * (applications/mesh/latticeMeshPartition/standardDecomp.c), which reads only
+ * the node count.  The caller keeps 1 <= np <= n. */
+void standardDecomp(uint* owner, basicMesh* mesh, uint np);
+void ref_standard_decomp(uint32_t n, uint32_t np, uint32_t* owner) {
+    basicMesh m;
+    memset(&m, 0, sizeof(m));
+    m.nPoints = n;
+    standardDecomp((uint*)owner, &m, np);
+}
 void ref_set_rho0(ref_case* c, double r) { c->mesh.EOS.rho_0 = r; }
 double ref_average_rho0(ref_case* c) {
     c->mesh.EOS.rho_0 = averageScalarField(&c->mesh, c->mf.rho);

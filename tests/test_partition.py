@@ -106,12 +106,50 @@ def test_mesh_files_round_trip_run(tmp_path):
         assert_same(b, a, fields=fields_of(case), ctx=f"rank {p.rank} from files")
 
 
+def _ref_standard(n, ranks):
+    import ctypes as C
+    import os
+    from oracle import oracle as orc
+    if not orc.available("ref") and not os.path.isdir("/root/reference/src"):
+        pytest.skip("reference build absent")
+    lib = orc._lib("ref")
+    fn = lib.ref_standard_decomp
+    fn.argtypes = [C.c_uint32, C.c_uint32, C.c_void_p]
+    out = np.full(n, 0xFFFFFFFF, dtype=np.uint32)
+    fn(n, ranks, out.ctypes.data)
+    return out.astype(np.int64)
+
+
+@pytest.mark.parametrize("n,ranks", [(480, 3), (481, 7), (10, 10), (7, 1), (65536, 148), (7_077_888, 8)])
+def test_standard_owner_is_the_reference_decomposition(n, ranks):
+    """slabs.standard_owner equals the reference partitioner's default method
+    (standardDecomp.c, compiled from the reference's source)."""
+    assert np.array_equal(slabs.standard_owner(n, ranks), _ref_standard(n, ranks))
+
+
+@pytest.mark.parametrize("name,ranks", [("bubble_d2q9", 3), ("bubble_d3q15", 4), ("st_d2q9", 2)])
+def test_standard_partition_run_equals_single_domain(name, ranks):
+    """The reference's default partition of a periodic mesh, stepped rank by
+    rank with its ghost exchange, is the single-domain run bit for bit."""
+    case = get_case(name)
+    parts = slabs.partition(case, slabs.standard_owner(case.n, ranks), rank0=case.meta.get("rank", 0))
+    assert len(parts) == ranks
+    run = slabs.RankRun(parts, CheckerHandle, n_global=case.n)
+    run.initialize()
+    run.step(6)
+    assert_same(run.gather(), run_checker("port", case, 6), fields=fields_of(case),
+                ctx=f"{name} standard decomposition on {ranks} ranks")
+
+
 def test_refusals():
     case = small_cases()["bubble_d2q9"]
     with pytest.raises(ValueError):
         slabs.partition(case, np.zeros(case.n - 1, dtype=int))
     with pytest.raises(ValueError):
         slabs.partition(case, np.where(np.arange(case.n) < 10, 0, 2))    # rank 1 owns nothing
+    for ranks in (0, case.n + 1):                                         # the reference's block of 0 nodes
+        with pytest.raises(ValueError):
+            slabs.standard_owner(case.n, ranks)
     parts = slabs.partition(case, OWNERS["bubble_d2q9"](case))
     m = [mesh.LatticeMesh(case.lattice, p.case.points, p.case.nb[:len(p.own)], [], [], len(p.own),
                           len(p.gidx) - len(p.own), None, p.recv, p.send) for p in parts]
