@@ -1,12 +1,18 @@
 /*
- * Single-rank stand-in for <mpi.h>, used ONLY to compile the reference's
- * hot-path C sources into the parity checker under oracle/_ref/.
+ * Stand-in for <mpi.h>, used ONLY to compile the reference's hot-path C
+ * sources into the parity checker under oracle/_ref/.
  *
- * This is test infrastructure, not product code.  Every call behaves as if
- * the job had exactly one rank: rank 0, world size 1.  At world size 1 the
+ * This is test infrastructure, not product code.  MPI_Comm_rank / _size
+ * answer rank 0 of 1 (the reference reads its pid and world size from
+ * latticeMesh.parallel on the path, not from MPI).  At world size 1 the
  * reference never posts a message (sendPdfField.c:10 returns early, the
- * sync* helpers loop over zero peers), so the point-to-point calls below are
- * never reached with real traffic; they exist so the sources link.
+ * sync* helpers loop over zero peers).  For multi-rank checks the harness
+ * runs every rank of a partitioned mesh in one process, one thread per rank
+ * (oracle/ref_harness.c, ref_ranks_*): MPI_Isend, MPI_Irecv and MPI_Waitall
+ * then pass messages between the threads through an in-process mailbox
+ * (oracle/mpi_stub/mpi_stub.c), matched by source rank and tag as MPI
+ * matches them.  Every wait is bounded; a receive that is never matched
+ * returns an error and is counted (mplb_stub_failures).
  */
 #ifndef MPLB_ORACLE_MPI_STUB_H
 #define MPLB_ORACLE_MPI_STUB_H
@@ -51,15 +57,21 @@ static inline int MPI_Finalize(void) { return 0; }
 static inline int MPI_Comm_rank(MPI_Comm c, int* r) { (void)c; *r = 0; return 0; }
 static inline int MPI_Comm_size(MPI_Comm c, int* s) { (void)c; *s = 1; return 0; }
 static inline int MPI_Barrier(MPI_Comm c) { (void)c; return 0; }
-static inline int MPI_Isend(const void* b, int n, MPI_Datatype t, int d, int tag, MPI_Comm c, MPI_Request* r)
-{ (void)b; (void)n; (void)t; (void)d; (void)tag; (void)c; *r = 0; return 0; }
-static inline int MPI_Irecv(void* b, int n, MPI_Datatype t, int s, int tag, MPI_Comm c, MPI_Request* r)
-{ (void)b; (void)n; (void)t; (void)s; (void)tag; (void)c; *r = 0; return 0; }
+/* Point-to-point calls between the rank threads of one process
+ * (mpi_stub.c).  A send is buffered: it completes at once. */
+int MPI_Isend(const void* b, int n, MPI_Datatype t, int d, int tag, MPI_Comm c, MPI_Request* r);
+int MPI_Irecv(void* b, int n, MPI_Datatype t, int s, int tag, MPI_Comm c, MPI_Request* r);
+int MPI_Waitall(int n, MPI_Request* r, MPI_Status* s);
+/* The calling thread acts as rank `rank` (the sender of its messages). */
+void mplb_stub_set_rank(int rank);
+/* Receives that gave up waiting since the last reset; reset clears the
+ * mailbox too. */
+int mplb_stub_failures(void);
+void mplb_stub_reset(void);
 static inline int MPI_Send(const void* b, int n, MPI_Datatype t, int d, int tag, MPI_Comm c)
 { (void)b; (void)n; (void)t; (void)d; (void)tag; (void)c; return 0; }
 static inline int MPI_Recv(void* b, int n, MPI_Datatype t, int s, int tag, MPI_Comm c, MPI_Status* st)
 { (void)b; (void)n; (void)t; (void)s; (void)tag; (void)c; (void)st; return 0; }
-static inline int MPI_Waitall(int n, MPI_Request* r, MPI_Status* s) { (void)n; (void)r; (void)s; return 0; }
 /* One rank: the reduction of a single contribution is the contribution. */
 static inline int MPI_Allreduce(const void* in, void* out, int n, MPI_Datatype t, MPI_Op op, MPI_Comm c)
 { (void)op; (void)c; memcpy(out, in, (size_t)n * mplb_stub_size(t)); return 0; }

@@ -23,6 +23,7 @@
 #include <stdlib.h>
 #include <string.h>
 #include <stdint.h>
+#include <pthread.h>
 
 #include <latticeMesh.h>
 #include <macroFields.h>
@@ -386,4 +387,151 @@ int ref_write_field(int format, int scalar, const char* name, const double* fiel
     }
     rows_free(r, n);
     return 0;
+}
+
+/* ------------------------------------------------------------------------
+ * Several ranks of a partitioned mesh, each a ref_case, run by the
+ * reference's own exchange code (sendPdfField / recvPdfField,
+ * syncScalarField, syncVectorField, and syncPdfField inside the
+ * surface-tension collisions) with one thread per rank and the stub's
+ * in-process messages.  The caller creates every rank's case from its own
+ * nodes (owned first, then ghosts), then sets its place here. */
+
+/* mpiInfo of rank `pid` of `world` as readLatticeMesh fills it
+ * (readLatticeMesh.c:299-425): nrg[s] ghosts received from s, listed in recv
+ * (peer by peer), nsg[s] owned nodes sent to s, listed in send, and the
+ * buffers of the exchange; the fields' PDF buffers as createLbeField sizes
+ * them. */
+int ref_set_parallel(ref_case* c, uint32_t pid, uint32_t world, uint32_t nlocal, const uint32_t* nrg,
+                     const uint32_t* recv, const uint32_t* nsg, const uint32_t* send) {
+    if (world < 1 || pid >= world || nlocal > c->n) return -1;
+    mpiInfo* P = &c->mesh.parallel;
+    P->pid = pid;
+    P->worldSize = world;
+    P->nlocal = nlocal;
+    P->nghosts = c->n - nlocal;
+    free(P->nrg);
+    free(P->nsg);
+    P->nrg = (uint*)calloc(world, sizeof(uint));
+    P->nsg = (uint*)calloc(world, sizeof(uint));
+    P->recvGhosts = (uint**)calloc(world, sizeof(uint*));
+    P->sendGhosts = (uint**)calloc(world, sizeof(uint*));
+    P->sbuf = (scalar**)calloc(world, sizeof(scalar*));
+    P->rbuf = (scalar**)calloc(world, sizeof(scalar*));
+    P->vsbuf = (scalar**)calloc(world, sizeof(scalar*));
+    P->vrbuf = (scalar**)calloc(world, sizeof(scalar*));
+    lbeField* fl[2] = {&c->f, &c->g};
+    for (int w = 0; w < 2; w++) {
+        fl[w]->sbuf = (scalar**)calloc(world, sizeof(scalar*));
+        fl[w]->rbuf = (scalar**)calloc(world, sizeof(scalar*));
+        fl[w]->nreq = 0;
+    }
+    size_t ro = 0, so = 0;
+    for (uint32_t s = 0; s < world; s++) {
+        P->nrg[s] = nrg[s];
+        P->nsg[s] = nsg[s];
+        P->recvGhosts[s] = (uint*)malloc((nrg[s] ? nrg[s] : 1) * sizeof(uint));
+        P->sendGhosts[s] = (uint*)malloc((nsg[s] ? nsg[s] : 1) * sizeof(uint));
+        for (uint32_t i = 0; i < nrg[s]; i++) {
+            if (recv[ro + i] < nlocal || recv[ro + i] >= c->n) return -2;  /* a ghost is not owned */
+            P->recvGhosts[s][i] = recv[ro + i];
+        }
+        for (uint32_t i = 0; i < nsg[s]; i++) {
+            if (send[so + i] >= nlocal) return -3;  /* only owned nodes are sent */
+            P->sendGhosts[s][i] = send[so + i];
+        }
+        ro += nrg[s];
+        so += nsg[s];
+        size_t rq = (size_t)(nrg[s] ? nrg[s] : 1) * c->Q, sq = (size_t)(nsg[s] ? nsg[s] : 1) * c->Q;
+        P->rbuf[s] = (scalar*)calloc(rq, sizeof(scalar));
+        P->sbuf[s] = (scalar*)calloc(sq, sizeof(scalar));
+        P->vrbuf[s] = (scalar*)calloc((size_t)(nrg[s] ? nrg[s] : 1) * 3, sizeof(scalar));
+        P->vsbuf[s] = (scalar*)calloc((size_t)(nsg[s] ? nsg[s] : 1) * 3, sizeof(scalar));
+        for (int w = 0; w < 2; w++) {
+            fl[w]->rbuf[s] = (scalar*)calloc(rq, sizeof(scalar));
+            fl[w]->sbuf[s] = (scalar*)calloc(sq, sizeof(scalar));
+        }
+    }
+    return 0;
+}
+
+/* multiPhasePP.c:122-147 with the exchanges of a multi-rank run. */
+static void rank_initialize(ref_case* c) {
+    latticeMesh* m = &c->mesh;
+    equilibrium(m, &c->mf, &c->f);
+    equilibrium(m, &c->mf, &c->g);
+    interForce(m, &c->mf);
+    syncVectorField(m, c->mf.Fi);
+    syncVectorField(m, c->mf.Ft);
+    heatSource(m, &c->mf, &c->g);
+    syncScalarField(m, c->g.scalarSource);
+}
+
+/* multiPhasePP.c:157-240 with its exchanges; the solver's --frozen / --nht
+ * switches are the fields' update flags (multiPhasePP.c:106,116). */
+static void rank_steps(ref_case* c, uint32_t nsteps) {
+    latticeMesh* m = &c->mesh;
+    for (uint32_t s = 0; s < nsteps; s++) {
+        ++m->time.current;
+        collision(m, &c->mf, &c->f);
+        lbstream(m, &c->f);
+        updateBoundaries(m, &c->mf, &c->f);
+        if (c->f.update != 0) sendPdfField(m, &c->f);
+        collision(m, &c->mf, &c->g);
+        lbstream(m, &c->g);
+        updateBoundaries(m, &c->mf, &c->g);
+        if (c->g.update != 0) sendPdfField(m, &c->g);
+        macroDensity(m, &c->mf, &c->f, 0, m->parallel.nlocal);
+        if (c->f.update != 0) recvPdfField(m, &c->f);
+        macroDensity(m, &c->mf, &c->f, m->parallel.nlocal, m->mesh.nPoints);
+        if (c->g.update != 0) recvPdfField(m, &c->g);
+        if (c->g.update != 0) {
+            heatSource(m, &c->mf, &c->g);
+            syncScalarField(m, c->g.scalarSource);
+        }
+        macroTemperature(m, &c->mf, &c->g, 0, m->mesh.nPoints);
+        if (c->f.update != 0) {
+            interForce(m, &c->mf);
+            syncVectorField(m, c->mf.Fi);
+            syncVectorField(m, c->mf.Ft);
+        }
+        macroVelocity(m, &c->mf, &c->f, 0, m->mesh.nPoints);
+    }
+}
+
+typedef struct {
+    ref_case* c;
+    uint32_t nsteps;
+    int init;
+} rank_job;
+
+static void* rank_thread(void* a) {
+    rank_job* j = (rank_job*)a;
+    mplb_stub_set_rank((int)j->c->mesh.parallel.pid);
+    if (j->init) rank_initialize(j->c);
+    else rank_steps(j->c, j->nsteps);
+    return NULL;
+}
+
+/* Every rank's start-up (init != 0) or nsteps time steps, one thread per
+ * rank; cases[r] is rank r.  0, or -1 when a message went missing. */
+int ref_ranks_run(ref_case** cases, uint32_t nranks, int init, uint32_t nsteps) {
+    for (uint32_t r = 0; r < nranks; r++)
+        if (cases[r]->mesh.parallel.pid != r || cases[r]->mesh.parallel.worldSize != nranks) return -2;
+    mplb_stub_reset();
+    pthread_t* th = (pthread_t*)calloc(nranks, sizeof(pthread_t));
+    rank_job* jobs = (rank_job*)calloc(nranks, sizeof(rank_job));
+    uint32_t started = 0;
+    for (uint32_t r = 0; r < nranks; r++) {
+        jobs[r].c = cases[r];
+        jobs[r].nsteps = nsteps;
+        jobs[r].init = init;
+        if (pthread_create(&th[r], NULL, rank_thread, &jobs[r]) != 0) break;
+        started++;
+    }
+    for (uint32_t r = 0; r < started; r++) pthread_join(th[r], NULL);
+    free(th);
+    free(jobs);
+    if (started != nranks) return -3;
+    return mplb_stub_failures() ? -1 : 0;
 }
