@@ -189,3 +189,45 @@ int adapter_ghost_runs(uint32_t nranks, const uint32_t* pid_of, const uint32_t* 
     free(ms);
     return rc;
 }
+
+/* mplb_ref_ghost_runs and mplb_ref_pack on the harness's ranks (reference
+ * structures whose mpiInfo ref_set_parallel filled): the runs go to out as
+ * in adapter_ghost_runs; every rank must pack, with its ghost rows carrying
+ * no neighbours.  0, the ghost-runs error, or 2000 + the first rank that
+ * does not pack as expected. */
+int adapter_ghost_runs_of_ranks(ref_case** cs, uint32_t nranks, uint32_t* out, uint32_t cap, uint32_t* nout) {
+    const latticeMesh** mp = (const latticeMesh**)malloc(nranks * sizeof(latticeMesh*));
+    int bad = 0;
+    for (uint32_t r = 0; r < nranks; r++) {
+        latticeMesh* m;
+        macroFields* mf;
+        lbeField *f, *g;
+        ref_structs(cs[r], &m, &mf, &f, &g);
+        mp[r] = m;
+        mplb_ref_descs d;
+        if (!bad && mplb_ref_pack(m, f, g, &d) == 0) {
+            const int Q = m->lattice.Q;
+            for (uint32_t i = m->parallel.nlocal; i < m->mesh.nPoints; i++)
+                for (int k = 0; k < Q; k++)
+                    if (d.nb[(size_t)i * Q + k] != -1) bad = 2000 + (int)r;
+            if (d.mesh.n_points != m->mesh.nPoints) bad = 2000 + (int)r;
+            mplb_ref_free(&d);
+        } else if (!bad) {
+            bad = 2000 + (int)r;
+        }
+    }
+    mplb_ghost_run* runs = NULL;
+    uint32_t nruns = 0;
+    int rc = mplb_ref_ghost_runs(mp, nranks, &runs, &nruns);
+    *nout = nruns;
+    for (uint32_t i = 0; i < nruns && i < cap; i++) {
+        out[5 * i] = runs[i].dst;
+        out[5 * i + 1] = runs[i].dst_start;
+        out[5 * i + 2] = runs[i].src;
+        out[5 * i + 3] = runs[i].src_start;
+        out[5 * i + 4] = runs[i].count;
+    }
+    free(runs);
+    free(mp);
+    return rc ? rc : bad;
+}

@@ -97,3 +97,25 @@ def test_runner_equals_reference_ranks(name):
     run.step(6)
     for (p, want), (_, got) in zip(ref.owned(), run.owned()):
         assert_same(got, want, fields=fields_of(case), ctx=f"{name} rank {p.rank} of {len(parts)}")
+
+
+@pytest.mark.parametrize("name", ["bubble_d2q9", "column_d2q9", "walls_d3q15"])
+def test_adapter_on_reference_ranks(name):
+    """include/mplb_gpu_reference.h on the reference's own multi-rank
+    structures: every rank packs (ghost rows without neighbours) and the
+    ghost runs built from their mpiInfo are the runner's transfers, i.e. the
+    exchange mplb_ranks_step is given."""
+    from tests.test_adapter import adapter_lib
+    lib = adapter_lib()
+    lib.adapter_ghost_runs_of_ranks.argtypes = [C.POINTER(C.c_void_p), C.c_uint32, C.c_void_p, C.c_uint32,
+                                                C.POINTER(C.c_uint32)]
+    lib.adapter_ghost_runs_of_ranks.restype = C.c_int
+    case = small_cases()[name]
+    parts = slabs.partition(case, CASES[name](case))
+    ref = RefRanks(parts)
+    cap = sum(len(p.recv[s]) for p in parts for s in range(len(parts))) + 1
+    out = np.zeros((cap, 5), dtype=np.uint32)
+    n = C.c_uint32(0)
+    assert lib.adapter_ghost_runs_of_ranks(ref.harr, len(parts), out.ctypes.data, cap, C.byref(n)) == 0
+    run = slabs.RankRun(parts, lambda c: None, staged=True)
+    assert [tuple(int(v) for v in row) for row in out[:n.value]] == [tuple(t) for t in run.transfers]
