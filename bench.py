@@ -333,6 +333,33 @@ def run_ours(a):
         print(json.dumps(line), flush=True)
 
 
+def cpu_ranks(workload, steps, procs):
+    """The reference's own multi-rank step (oracle/_ref: its collisions,
+    streaming, boundaries and its sendPdfField / recvPdfField / sync*
+    exchanges, multiPhasePP.c:122-240) on `procs` host threads, one rank per
+    thread, over the reference partitioner's standard decomposition of the
+    full lattice.  Messages pass through an in-process mailbox instead of an
+    MPI library."""
+    from multiphaselb_b200 import cases, slabs
+    from oracle import oracle as orc
+    if not orc.available("ref"):
+        orc.build("ref")
+    case = WORKLOADS[workload]["build"](cases)
+    parts = slabs.partition(case, slabs.standard_owner(case.n, procs))
+    ranks = orc.RefRanks(parts)
+    ranks.initialize()
+    t0 = time.perf_counter()
+    ranks.step(steps)
+    dt = time.perf_counter() - t0
+    ghosts = sum(len(p.gidx) - len(p.own) for p in parts)
+    return dict(value=case.n * steps / dt / 1e9, unit="GLUPS", cores=procs, step_ms=dt / max(steps, 1) * 1e3,
+                kind="reference",
+                sample=f"{steps} steps of the full {WORKLOADS[workload]['desc']} lattice as {procs} ranks "
+                       f"(standard decomposition, {ghosts} ghost nodes), one thread per rank, exchanging "
+                       f"through the reference's own send/recv/sync code over an in-process mailbox; "
+                       f"wall {dt:.1f}s")
+
+
 def run_reference(a):
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -345,10 +372,11 @@ def run_reference(a):
     # takes about 25 ms on one core)
     steps = max(1, min(a.steps, a.ref_max_steps))
     samples = []
-    cpu_baseline(a.workload, max(1, min(a.warmup, 20)), procs)  # warm-up: process start, page-in
+    leg = cpu_ranks if a.ref_mode == "ranks" else cpu_baseline
+    leg(a.workload, max(1, min(a.warmup, 20)), procs)  # warm-up: process start, page-in
     t0 = time.perf_counter()
     for _ in range(max(1, a.ref_repeats)):
-        samples.append(cpu_baseline(a.workload, steps, procs))
+        samples.append(leg(a.workload, steps, procs))
     wall = time.perf_counter() - t0
     best = samples[-1]
     v = statistics.median(s["value"] for s in samples)
@@ -358,7 +386,9 @@ def run_reference(a):
         "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded lattice of the named shape)",
         "impl": "reference",
         "config": {"workload": a.workload, "desc": WORKLOADS[a.workload]["desc"],
-                   "parallelism": f"{procs} independent single-threaded reference processes"},
+                   "parallelism": (f"{procs} reference ranks, one thread each, standard decomposition"
+                                   if a.ref_mode == "ranks" else
+                                   f"{procs} independent single-threaded reference processes")},
         "cpu_baseline": {"value": round(v, 6), "unit": "GLUPS", "cores": procs, "kind": best["kind"],
                          "sample": best["sample"]},
         "e2e": {"value": round(v, 6), "unit": "GLUPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -382,6 +412,10 @@ def main():
     ap.add_argument("--ref-repeats", type=int, default=1)
     ap.add_argument("--ref-max-steps", type=int, default=3000,
                     help="reference arm: at most this many steps per core (keeps the run within minutes)")
+    ap.add_argument("--ref-mode", default="copies", choices=["copies", "ranks"],
+                    help="reference arm: independent single-rank copies of the lattice, one per core (an upper "
+                         "bound on the reference's MPI scaling), or the lattice split into ranks that run the "
+                         "reference's own exchange code, one thread each")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-fp32", action="store_true")
     a = ap.parse_args()

@@ -157,6 +157,50 @@ class Checker:
 
 
 # ------------------------------------------------------------- field files
+class RefRanks:
+    """The ranks of a partitioned mesh (multiphaselb_b200.slabs Part objects,
+    rank r = pid r) as reference cases with their mpiInfo, stepped together
+    by the reference's own exchange code, one thread per rank
+    (ref_harness.c::ref_ranks_run)."""
+
+    def __init__(self, parts):
+        import numpy as np
+        self.lib = lib = _lib("ref")
+        lib.ref_set_parallel.argtypes = [C.c_void_p, C.c_uint32, C.c_uint32, C.c_uint32] + [C.c_void_p] * 4
+        lib.ref_set_parallel.restype = C.c_int
+        lib.ref_ranks_run.argtypes = [C.POINTER(C.c_void_p), C.c_uint32, C.c_int, C.c_uint32]
+        lib.ref_ranks_run.restype = C.c_int
+        self.parts = parts
+        R = len(parts)
+        self.k = [Checker("ref", p.case, rank=p.rank) for p in parts]
+        cat = lambda a: np.ascontiguousarray(np.concatenate([np.asarray(x, dtype=np.uint32) for x in a]  # noqa: E731
+                                                            + [np.zeros(1, np.uint32)]))
+        for k, p in zip(self.k, parts):
+            nrg = np.array([len(p.recv[s]) for s in range(R)], dtype=np.uint32)
+            nsg = np.array([len(p.send[s]) for s in range(R)], dtype=np.uint32)
+            recv, send = cat(p.recv), cat(p.send)
+            rc = lib.ref_set_parallel(k.h, p.rank, R, len(p.own), nrg.ctypes.data, recv.ctypes.data,
+                                      nsg.ctypes.data, send.ctypes.data)
+            if rc != 0:
+                raise ValueError(f"rank {p.rank}: ref_set_parallel refused the lists ({rc})")
+            k.upload(rho=p.case.rho, U=p.case.U, T=p.case.T)
+        self.harr = (C.c_void_p * R)(*[k.h for k in self.k])
+
+    def run(self, init, nsteps=0):
+        rc = self.lib.ref_ranks_run(self.harr, len(self.k), int(init), nsteps)
+        if rc != 0:
+            raise RuntimeError(f"reference ranks failed ({rc}: a message went missing)")
+
+    def initialize(self):
+        self.run(True)
+
+    def step(self, n):
+        self.run(False, n)
+
+    def owned(self):
+        return [(p, {n: v[:len(p.own)] for n, v in k.download().items()}) for p, k in zip(self.parts, self.k)]
+
+
 def field_file_bytes(fmt, name, field, scalar):
     """The bytes the reference's writers put in one file, restated in Python.
 

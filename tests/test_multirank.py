@@ -72,3 +72,18 @@ def test_reference_arm_prints_on_rank0_only():
     outs = run_ranks(code)
     printed = [o for o in outs if o.strip()]
     assert len(printed) == 1 and '"impl": "reference"' in printed[0]
+
+
+def test_reference_arm_ranks_mode():
+    """--ref-mode ranks: the reference's own multi-rank step on host threads
+    prints one line on the arm's metric, unit and config."""
+    import json
+    import subprocess
+    import sys
+    p = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference", "--ref-mode", "ranks",
+                        "--cpu-procs", "3", "--steps", "2", "--warmup", "3"],
+                       capture_output=True, text=True, timeout=300, cwd=ROOT)
+    assert p.returncode == 0, p.stderr
+    line = json.loads(p.stdout.strip().splitlines()[-1])
+    assert line["impl"] == "reference" and line["unit"] == "GLUPS" and line["value"] > 0
+    assert line["cpu_baseline"]["cores"] == 3 and "3 reference ranks" in line["config"]["parallelism"]

@@ -24,45 +24,10 @@ from tests.test_partition import blocks as blocks_owner
 from tests.test_slabs import CheckerHandle, fields_of
 
 
-def ref_lib():
+def RefRanks(parts):
     if not orc.available("ref") and not os.path.isdir("/root/reference/src"):
         pytest.skip("reference build absent")
-    lib = orc._lib("ref")
-    if not hasattr(lib, "ref_ranks_run"):
-        pytest.skip("reference build predates the multi-rank harness")
-    lib.ref_set_parallel.argtypes = [C.c_void_p, C.c_uint32, C.c_uint32, C.c_uint32] + [C.c_void_p] * 4
-    lib.ref_set_parallel.restype = C.c_int
-    lib.ref_ranks_run.argtypes = [C.POINTER(C.c_void_p), C.c_uint32, C.c_int, C.c_uint32]
-    lib.ref_ranks_run.restype = C.c_int
-    return lib
-
-
-class RefRanks:
-    """Every part as a reference case with its mpiInfo, stepped together."""
-
-    def __init__(self, parts):
-        self.lib = ref_lib()
-        self.parts = parts
-        R = len(parts)
-        self.k = [orc.Checker("ref", p.case, rank=p.rank) for p in parts]
-        u32 = lambda a: np.ascontiguousarray(np.concatenate([np.asarray(x, dtype=np.uint32) for x in a]
-                                                            + [np.zeros(1, np.uint32)]))
-        for k, p in zip(self.k, parts):
-            nrg = np.array([len(p.recv[s]) for s in range(R)], dtype=np.uint32)
-            nsg = np.array([len(p.send[s]) for s in range(R)], dtype=np.uint32)
-            recv, send = u32(p.recv), u32(p.send)
-            rc = self.lib.ref_set_parallel(k.h, p.rank, R, len(p.own), nrg.ctypes.data, recv.ctypes.data,
-                                           nsg.ctypes.data, send.ctypes.data)
-            assert rc == 0, rc
-            k.upload(rho=p.case.rho, U=p.case.U, T=p.case.T)
-        self.harr = (C.c_void_p * R)(*[k.h for k in self.k])
-
-    def run(self, init, nsteps=0):
-        rc = self.lib.ref_ranks_run(self.harr, len(self.k), int(init), nsteps)
-        assert rc == 0, f"reference ranks: {rc}"
-
-    def owned(self):
-        return [(p, {n: v[:len(p.own)] for n, v in k.download().items()}) for p, k in zip(self.parts, self.k)]
+    return orc.RefRanks(parts)
 
 
 def x_halves(c):
