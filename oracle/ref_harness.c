@@ -467,6 +467,20 @@ static void rank_initialize(ref_case* c) {
     syncScalarField(m, c->g.scalarSource);
 }
 
+/* fixedRandomT seeds the C library's single rand() state with its rank's
+ * pid at every application (fixedRandomT.c) and then draws from it.  Separate
+ * processes each own that state; rank threads share it, so each thread's
+ * boundary update runs alone, which gives every rank the draws it would get
+ * in its own process.  updateBoundaries sends no message, so holding the
+ * lock across it cannot stall another rank's exchange. */
+static pthread_mutex_t boundary_mu = PTHREAD_MUTEX_INITIALIZER;
+
+static void rank_boundaries(latticeMesh* m, macroFields* mf, lbeField* fl) {
+    pthread_mutex_lock(&boundary_mu);
+    updateBoundaries(m, mf, fl);
+    pthread_mutex_unlock(&boundary_mu);
+}
+
 /* multiPhasePP.c:157-240 with its exchanges; the solver's --frozen / --nht
  * switches are the fields' update flags (multiPhasePP.c:106,116). */
 static void rank_steps(ref_case* c, uint32_t nsteps) {
@@ -475,11 +489,11 @@ static void rank_steps(ref_case* c, uint32_t nsteps) {
         ++m->time.current;
         collision(m, &c->mf, &c->f);
         lbstream(m, &c->f);
-        updateBoundaries(m, &c->mf, &c->f);
+        rank_boundaries(m, &c->mf, &c->f);
         if (c->f.update != 0) sendPdfField(m, &c->f);
         collision(m, &c->mf, &c->g);
         lbstream(m, &c->g);
-        updateBoundaries(m, &c->mf, &c->g);
+        rank_boundaries(m, &c->mf, &c->g);
         if (c->g.update != 0) sendPdfField(m, &c->g);
         macroDensity(m, &c->mf, &c->f, 0, m->parallel.nlocal);
         if (c->f.update != 0) recvPdfField(m, &c->f);

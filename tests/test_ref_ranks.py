@@ -9,8 +9,10 @@ the same exchange points and lists as mplb_ranks_step) must give every
 rank's owned nodes bit for bit, including where the reference's multi-rank
 run is not its single-domain run (a fixedT wall across a cut).
 
-fixedRandomT cases are left out: the reference draws its wall values from
-the C library's one rand() state, which rank threads would share."""
+fixedRandomT draws from the C library's one rand() state, seeded with the
+rank's pid at every application; the harness runs each rank thread's
+boundary update alone so that every rank draws what it would draw in its
+own process."""
 import ctypes as C
 import os
 
@@ -47,6 +49,9 @@ CASES = {
     "walls_d3q15": lambda c: slabs.standard_owner(c.n, 4),
     "my_column_d2q9": x_halves,
     "cylinder_d2q9": lambda c: blocks_owner(c, lambda x, y, z: int(y >= 7)),
+    # outflow with fixedRandomT walls (myMRT): every rank seeds with its pid
+    "outflow_d2q9": x_halves,
+    "outflow_d3q15": lambda c: slabs.standard_owner(c.n, 3),
 }
 
 
