@@ -89,3 +89,50 @@ def test_adapter_on_reference_ranks(name):
     assert lib.adapter_ghost_runs_of_ranks(ref.harr, len(parts), out.ctypes.data, cap, C.byref(n)) == 0
     run = slabs.RankRun(parts, lambda c: None, staged=True)
     assert [tuple(int(v) for v in row) for row in out[:n.value]] == [tuple(t) for t in run.transfers]
+
+
+DIST_WORKER = r"""
+import os, sys, pickle
+sys.path.insert(0, {root!r})
+import torch.distributed as dist
+dist.init_process_group("gloo", init_method="tcp://127.0.0.1:{port}", rank=int(os.environ["RANK"]),
+                        world_size=int(os.environ["WORLD_SIZE"]))
+from multiphaselb_b200 import slabs
+from tests.helpers import small_cases
+from tests.test_ref_ranks import CASES
+from tests.test_slabs import CheckerHandle
+case = small_cases()[{name!r}]
+parts = slabs.partition(case, CASES[{name!r}](case))
+run = slabs.DistRankRun(parts[dist.get_rank()], CheckerHandle, n_global=case.n)
+run.initialize()
+run.step({steps})
+out = run.gather()
+if dist.get_rank() == 0:
+    with open({path!r}, "wb") as fh:
+        pickle.dump(out, fh)
+dist.barrier()
+dist.destroy_process_group()
+"""
+
+
+def test_gloo_ranks_equal_reference_ranks(tmp_path):
+    """One process per rank (DistRankRun over gloo) against the reference's
+    multi-rank run, on the thermal column cut across its fixedT walls, where
+    the reference's multi-rank result is not its single-domain result."""
+    import pickle
+    from tests.test_multirank import ROOT, free_port, run_ranks
+    name, steps = "column_d2q9", 6
+    case = small_cases()[name]
+    parts = slabs.partition(case, CASES[name](case))
+    ref = RefRanks(parts)
+    ref.run(init=True)
+    ref.run(init=False, nsteps=steps)
+    want = {}
+    for p, fields in ref.owned():
+        for n, v in fields.items():
+            want.setdefault(n, np.zeros((case.n,) + v.shape[1:], dtype=v.dtype))[p.gidx[:len(p.own)]] = v
+    path = str(tmp_path / "out.pkl")
+    run_ranks(DIST_WORKER.format(root=ROOT, port=free_port(), name=name, steps=steps, path=path), world=len(parts))
+    with open(path, "rb") as fh:
+        got = pickle.load(fh)
+    assert_same(got, want, fields=fields_of(case), ctx=f"{name} on {len(parts)} gloo ranks vs reference ranks")
