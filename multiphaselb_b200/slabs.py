@@ -274,6 +274,7 @@ class _Steps:
     (part, handle) pairs), with exchange(names) refreshing ghost nodes."""
 
     def _setup(self, case_like):
+        self.rho_0 = float(case_like.eos.get("rho_0", 0.0))
         self.has_g = case_like.g is not None
         self.f_on = case_like.f is not None and bool(case_like.f.get("update", 1))
         self.f_st = self.f_on and bool(case_like.f.get("surface_tension", 0))
@@ -323,6 +324,45 @@ class _Steps:
                 self._all("inter_force")
                 self.exchange(("Fi", "Ft"))
             self._all("macro_velocity")
+
+    def _local_rho_sums(self):
+        """(rank, serial sum of rho over its owned nodes in node order, owned
+        count) of every part of this process: the local half of
+        averageScalarField (averageScalarField.c, localSum += fld[i])."""
+        out = []
+        for p, h in self.local:
+            rho = np.asarray(h.download()["rho"], dtype=np.float64)[p.own]
+            out.append((p.rank, float(np.cumsum(rho)[-1]) if len(rho) else 0.0, len(rho)))
+        return out
+
+    @staticmethod
+    def _fold_rho_sums(sums):
+        """The global half of averageScalarField: MPI_Allreduce of the local
+        sums and counts, folded in rank order (((s0 + s1) + s2) + ...; an MPI
+        library may fold in another order, and with two ranks every order
+        gives the same bits), then the division."""
+        sums = sorted(sums)
+        total, count = sums[0][1], sums[0][2]
+        for _, s, c in sums[1:]:
+            total += s
+            count += c
+        return total / count
+
+    def _average(self, sums):
+        return 0.0 if self.rho_0 <= 0 else self._fold_rho_sums(sums)
+
+    def average_rho0(self):
+        """The write step's buoyancy reference (multiPhasePP.c:271,
+        averageScalarField.c): 0 when the configured rho_0 is <= 0, else
+        the mean density over every rank's owned nodes.  Set it with
+        set_rho0, as the solver does."""
+        return self._average(self._local_rho_sums())
+
+    def set_rho0(self, rho_0):
+        """rho_0 on every rank's lattice (the Ft buoyancy term, interForce.c:33)."""
+        self.rho_0 = float(rho_0)
+        for _, h in self.local:
+            h.set_rho0(self.rho_0)
 
     def owned(self):
         """(part, fields of its owned nodes) of every part of this process."""
@@ -484,6 +524,13 @@ class DistRankRun(_Steps):
                 off += size
         self._upload_fields(self.handle, st)
 
+    def average_rho0(self):
+        """averageScalarField over the group: every rank's local sum and
+        count gathered, folded in rank order on every rank."""
+        sums = [None] * self._dist.get_world_size(self.group)
+        self._dist.all_gather_object(sums, self._local_rho_sums(), group=self.group)
+        return self._average([x for ss in sums for x in ss])
+
     def gather(self):
         """Every rank's owned nodes, as the single-domain fields (on every rank)."""
         parts = [None] * self._dist.get_world_size(self.group)
@@ -521,6 +568,9 @@ class LatticeHandle:
 
     def get_time(self):
         return self.lat.info()["current_time"]
+
+    def set_rho0(self, rho_0):
+        self.lat.set_rho0(rho_0)
 
     def op(self, name, field=None):
         m = getattr(self.lat, name)

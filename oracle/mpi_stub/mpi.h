@@ -72,8 +72,9 @@ static inline int MPI_Send(const void* b, int n, MPI_Datatype t, int d, int tag,
 { (void)b; (void)n; (void)t; (void)d; (void)tag; (void)c; return 0; }
 static inline int MPI_Recv(void* b, int n, MPI_Datatype t, int s, int tag, MPI_Comm c, MPI_Status* st)
 { (void)b; (void)n; (void)t; (void)s; (void)tag; (void)c; (void)st; return 0; }
-/* One rank: the reduction of a single contribution is the contribution. */
-static inline int MPI_Allreduce(const void* in, void* out, int n, MPI_Datatype t, MPI_Op op, MPI_Comm c)
-{ (void)op; (void)c; memcpy(out, in, (size_t)n * mplb_stub_size(t)); return 0; }
+/* Sum over the rank threads (mpi_stub.c); with one rank, the contribution. */
+int MPI_Allreduce(const void* in, void* out, int n, MPI_Datatype t, MPI_Op op, MPI_Comm c);
+/* Number of rank threads taking part in MPI_Allreduce (1 outside ref_ranks_*). */
+void mplb_stub_set_world(int world);
 
 #endif

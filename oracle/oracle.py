@@ -200,6 +200,17 @@ class RefRanks:
     def owned(self):
         return [(p, {n: v[:len(p.own)] for n, v in k.download().items()}) for p, k in zip(self.parts, self.k)]
 
+    def average_rho0(self):
+        """averageScalarField on every rank thread (its MPI_Allreduce across
+        them); each rank's rho_0 is set to its result, which is returned."""
+        self.lib.ref_ranks_average_rho0.argtypes = [C.POINTER(C.c_void_p), C.c_uint32, C.POINTER(C.c_double)]
+        self.lib.ref_ranks_average_rho0.restype = C.c_int
+        out = (C.c_double * len(self.k))()
+        rc = self.lib.ref_ranks_average_rho0(self.harr, len(self.k), out)
+        if rc != 0:
+            raise RuntimeError(f"reference ranks failed ({rc})")
+        return list(out)
+
 
 def field_file_bytes(fmt, name, field, scalar):
     """The bytes the reference's writers put in one file, restated in Python.

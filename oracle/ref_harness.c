@@ -513,39 +513,63 @@ static void rank_steps(ref_case* c, uint32_t nsteps) {
     }
 }
 
+enum { JOB_STEPS = 0, JOB_INIT = 1, JOB_AVERAGE_RHO0 = 2 };
+
 typedef struct {
     ref_case* c;
     uint32_t nsteps;
-    int init;
+    int kind;
+    double result;
 } rank_job;
 
 static void* rank_thread(void* a) {
     rank_job* j = (rank_job*)a;
     mplb_stub_set_rank((int)j->c->mesh.parallel.pid);
-    if (j->init) rank_initialize(j->c);
-    else rank_steps(j->c, j->nsteps);
+    if (j->kind == JOB_INIT) rank_initialize(j->c);
+    else if (j->kind == JOB_AVERAGE_RHO0) {
+        /* the write step's buoyancy reference (multiPhasePP.c:271) */
+        j->result = averageScalarField(&j->c->mesh, j->c->mf.rho);
+        j->c->mesh.EOS.rho_0 = j->result;
+    } else rank_steps(j->c, j->nsteps);
     return NULL;
 }
+
+static int ranks_run(ref_case** cases, uint32_t nranks, int kind, uint32_t nsteps, double* results);
 
 /* Every rank's start-up (init != 0) or nsteps time steps, one thread per
  * rank; cases[r] is rank r.  0, or -1 when a message went missing. */
 int ref_ranks_run(ref_case** cases, uint32_t nranks, int init, uint32_t nsteps) {
+    return ranks_run(cases, nranks, init ? JOB_INIT : JOB_STEPS, nsteps, NULL);
+}
+
+/* averageScalarField of every rank's density, as the write step calls it
+ * (local serial sums, MPI_Allreduce of the sums and of the node counts),
+ * stored as each rank's rho_0; out[r] = rank r's result. */
+int ref_ranks_average_rho0(ref_case** cases, uint32_t nranks, double* out) {
+    return ranks_run(cases, nranks, JOB_AVERAGE_RHO0, 0, out);
+}
+
+static int ranks_run(ref_case** cases, uint32_t nranks, int kind, uint32_t nsteps, double* results) {
     for (uint32_t r = 0; r < nranks; r++)
         if (cases[r]->mesh.parallel.pid != r || cases[r]->mesh.parallel.worldSize != nranks) return -2;
     mplb_stub_reset();
+    mplb_stub_set_world((int)nranks);
     pthread_t* th = (pthread_t*)calloc(nranks, sizeof(pthread_t));
     rank_job* jobs = (rank_job*)calloc(nranks, sizeof(rank_job));
     uint32_t started = 0;
     for (uint32_t r = 0; r < nranks; r++) {
         jobs[r].c = cases[r];
         jobs[r].nsteps = nsteps;
-        jobs[r].init = init;
+        jobs[r].kind = kind;
         if (pthread_create(&th[r], NULL, rank_thread, &jobs[r]) != 0) break;
         started++;
     }
     for (uint32_t r = 0; r < started; r++) pthread_join(th[r], NULL);
+    if (results)
+        for (uint32_t r = 0; r < started; r++) results[r] = jobs[r].result;
     free(th);
     free(jobs);
+    mplb_stub_set_world(1);
     if (started != nranks) return -3;
     return mplb_stub_failures() ? -1 : 0;
 }

@@ -99,17 +99,20 @@ dist.init_process_group("gloo", init_method="tcp://127.0.0.1:{port}", rank=int(o
                         world_size=int(os.environ["WORLD_SIZE"]))
 from multiphaselb_b200 import slabs
 from tests.helpers import small_cases
-from tests.test_ref_ranks import CASES
+from tests.test_ref_ranks import CASES, with_rho0
 from tests.test_slabs import CheckerHandle
-case = small_cases()[{name!r}]
+case = with_rho0(small_cases()[{name!r}], 1.0)
 parts = slabs.partition(case, CASES[{name!r}](case))
 run = slabs.DistRankRun(parts[dist.get_rank()], CheckerHandle, n_global=case.n)
 run.initialize()
 run.step({steps})
+avg = run.average_rho0()
+run.set_rho0(avg)
+run.step(2)
 out = run.gather()
 if dist.get_rank() == 0:
     with open({path!r}, "wb") as fh:
-        pickle.dump(out, fh)
+        pickle.dump((out, avg), fh)
 dist.barrier()
 dist.destroy_process_group()
 """
@@ -118,15 +121,18 @@ dist.destroy_process_group()
 def test_gloo_ranks_equal_reference_ranks(tmp_path):
     """One process per rank (DistRankRun over gloo) against the reference's
     multi-rank run, on the thermal column cut across its fixedT walls, where
-    the reference's multi-rank result is not its single-domain result."""
+    the reference's multi-rank result is not its single-domain result, with
+    a write step's rho_0 update between the steps."""
     import pickle
     from tests.test_multirank import ROOT, free_port, run_ranks
     name, steps = "column_d2q9", 6
-    case = small_cases()[name]
+    case = with_rho0(small_cases()[name], 1.0)
     parts = slabs.partition(case, CASES[name](case))
     ref = RefRanks(parts)
     ref.run(init=True)
     ref.run(init=False, nsteps=steps)
+    avg = ref.average_rho0()
+    ref.run(init=False, nsteps=2)
     want = {}
     for p, fields in ref.owned():
         for n, v in fields.items():
@@ -134,5 +140,48 @@ def test_gloo_ranks_equal_reference_ranks(tmp_path):
     path = str(tmp_path / "out.pkl")
     run_ranks(DIST_WORKER.format(root=ROOT, port=free_port(), name=name, steps=steps, path=path), world=len(parts))
     with open(path, "rb") as fh:
-        got = pickle.load(fh)
+        got, got_avg = pickle.load(fh)
+    assert all(a == got_avg for a in avg), (got_avg, avg)
     assert_same(got, want, fields=fields_of(case), ctx=f"{name} on {len(parts)} gloo ranks vs reference ranks")
+
+
+def with_rho0(case, rho_0):
+    import dataclasses
+    return dataclasses.replace(case, eos=dict(case.eos, rho_0=rho_0))
+
+
+@pytest.mark.parametrize("name,ranks", [("column_d2q9", None), ("bubble_d2q9", 3), ("walls_d3q15", 4)])
+def test_write_step_rho0_equals_reference_ranks(name, ranks):
+    """The write step's rho_0 (averageScalarField: local serial sums, then
+    MPI_Allreduce of sums and counts) on every rank, and the steps after it
+    with the new buoyancy reference, bit for bit against the reference's
+    own function on its rank threads."""
+    case = with_rho0(small_cases()[name], 1.0)
+    owner = CASES[name](case) if ranks is None else slabs.standard_owner(case.n, ranks)
+    parts = slabs.partition(case, owner)
+    ref = RefRanks(parts)
+    ref.run(init=True)
+    ref.run(init=False, nsteps=4)
+    want = ref.average_rho0()
+    ref.run(init=False, nsteps=4)
+    run = slabs.RankRun(parts, CheckerHandle, n_global=case.n)
+    run.initialize()
+    run.step(4)
+    got = run.average_rho0()
+    assert all(w == got for w in want), (got, want)
+    assert got != 1.0
+    run.set_rho0(got)
+    run.step(4)
+    for (p, w), (_, g) in zip(ref.owned(), run.owned()):
+        assert_same(g, w, fields=fields_of(case), ctx=f"{name} rank {p.rank} after the rho_0 update")
+
+
+def test_rho0_off_when_not_configured():
+    """rho_0 <= 0 keeps the average at 0, as averageScalarField does."""
+    case = small_cases()["column_d2q9"]
+    parts = slabs.partition(case, CASES["column_d2q9"](case))
+    ref = RefRanks(parts)
+    ref.run(init=True)
+    run = slabs.RankRun(parts, CheckerHandle, n_global=case.n)
+    run.initialize()
+    assert ref.average_rho0() == [0.0] * len(parts) and run.average_rho0() == 0.0

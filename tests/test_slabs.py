@@ -35,6 +35,9 @@ class CheckerHandle:
     def get_time(self):
         return self.k.get_time()
 
+    def set_rho0(self, r):
+        self.k.set_rho0(r)
+
     def op(self, name, field=None):
         self.k.op(OPS[name], abi.FIELD_F if field is None else field)
 
