@@ -286,4 +286,25 @@ static inline int mplb_ref_ghost_runs(const latticeMesh* const* meshes, uint32_t
     return 0;
 }
 
+/* The write step's buoyancy reference across nranks ranks driven from one
+ * process (multiPhasePP.c:271), as averageScalarField computes it
+ * (src/basic/averageScalarField.c): 0 when the configured rho_0 is <= 0,
+ * else each rank's serial sum of rho over its nlocal owned nodes, the sums
+ * and counts combined as its MPI_Allreduce combines them (here in rank
+ * order; with two ranks every order gives the same bits), and the division.
+ * meshes[r] and mf[r] are rank r's, with rho downloaded (mplb_ref_download). */
+static inline double mplb_ref_average_rho0(const latticeMesh* const* meshes, const macroFields* const* mf,
+                                           uint32_t nranks) {
+    if (nranks == 0 || meshes[0]->EOS.rho_0 <= 0) return 0.0;
+    double total = 0.0;
+    uint32_t count = 0;
+    for (uint32_t r = 0; r < nranks; r++) {
+        double local = 0.0;
+        for (uint32_t i = 0; i < meshes[r]->parallel.nlocal; i++) local += mf[r]->rho[i];
+        total = r ? total + local : local;
+        count += meshes[r]->parallel.nlocal;
+    }
+    return total / count;
+}
+
 #endif /* MPLB_GPU_REFERENCE_H */

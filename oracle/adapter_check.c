@@ -231,3 +231,21 @@ int adapter_ghost_runs_of_ranks(ref_case** cs, uint32_t nranks, uint32_t* out, u
     free(mp);
     return rc ? rc : bad;
 }
+
+/* mplb_ref_average_rho0 on the harness's ranks (reference structures). */
+double adapter_average_rho0_of_ranks(ref_case** cs, uint32_t nranks) {
+    const latticeMesh** mp = (const latticeMesh**)malloc(nranks * sizeof(latticeMesh*));
+    const macroFields** mfp = (const macroFields**)malloc(nranks * sizeof(macroFields*));
+    for (uint32_t r = 0; r < nranks; r++) {
+        latticeMesh* m;
+        macroFields* mf;
+        lbeField *f, *g;
+        ref_structs(cs[r], &m, &mf, &f, &g);
+        mp[r] = m;
+        mfp[r] = mf;
+    }
+    double v = mplb_ref_average_rho0(mp, mfp, nranks);
+    free(mp);
+    free(mfp);
+    return v;
+}

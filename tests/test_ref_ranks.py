@@ -163,6 +163,12 @@ def test_write_step_rho0_equals_reference_ranks(name, ranks):
     ref.run(init=True)
     ref.run(init=False, nsteps=4)
     want = ref.average_rho0()
+    # the adapter's helper for C drivers, on the same reference structures
+    from tests.test_adapter import adapter_lib
+    lib = adapter_lib()
+    lib.adapter_average_rho0_of_ranks.argtypes = [C.POINTER(C.c_void_p), C.c_uint32]
+    lib.adapter_average_rho0_of_ranks.restype = C.c_double
+    assert lib.adapter_average_rho0_of_ranks(ref.harr, len(parts)) == want[0]
     ref.run(init=False, nsteps=4)
     run = slabs.RankRun(parts, CheckerHandle, n_global=case.n)
     run.initialize()
