@@ -6,7 +6,9 @@ Default workload: the thermal van der Waals column, D2Q9, 128 x 512 nodes,
 liMRT flow + liTempMRT heat, bounce-back / fixedT walls, FP64, on the fused
 box path.  One step = one time step of the whole lattice.  The lattice state
 (~21 MB) fits in L2, so a 256 MiB buffer is written between timed steps and
-each step is timed alone with CUDA events on the library's stream.
+each step is timed alone with CUDA events on the library's stream.  The
+other named workloads (D3Q15 bubble 192^3, D2Q9 bubble 256^2) follow under
+"extra", device-timed the same way, FP64 and FP32-deviation.
 
 For N > 1 (torchrun, one process per GPU) every rank advances its own
 replica of the workload (weak scaling; the path has no exchange step on one
@@ -38,12 +40,20 @@ METRIC = "GLUPS on 1 B200 (FP64 vs FP32-dev); time-to-equilibrium w/ warm start"
 WORKLOADS = {
     "column_d2q9_128x512": dict(bytes_per_lup=304, bytes_per_lup32=160,
                                 desc="thermal VdW column, D2Q9, f+g, bounceBack+fixedT walls, periodic x",
+                                eos="van der Waals a=9/392, b=2/21, R=1, T0=0.85 Tc, fixedT walls 0.86/0.84 Tc, "
+                                    "g=-1e-5: the stated a=9/49 makes psi NaN at 0.85 Tc (p - rho/3 > 0 in the "
+                                    "vapour; the reference's own solver gives NaN); a=9/392 keeps T/Tc, rho_c and "
+                                    "the coexistence densities",
                                 build=lambda c: c.column_case(128, 512)),
     "bubble_d2q9_256": dict(bytes_per_lup=144, bytes_per_lup32=72, desc="static bubble, D2Q9 liMRT, fully periodic",
+                            eos="Carnahan-Starling a=1, b=4, R=1, T=0.8 Tc, G=-1, vapour disc R=40, tanh width 5",
                             build=lambda c: c.bubble_case(0, 256, 40.0, 5.0, 0.8)),
     "bubble_d3q15_192": dict(bytes_per_lup=240, bytes_per_lup32=120, desc="static bubble, D3Q15 xuMRT, fully periodic",
+                             eos="Carnahan-Starling a=1, b=4, R=1, T=0.75 Tc, G=-1, vapour sphere R=48, tanh width 5",
                              build=lambda c: c.bubble_case(1, 192, 48.0, 5.0, 0.75)),
 }
+# timed after the named workload in a default run (device time, FP64 and FP32-deviation)
+EXTRA_WORKLOADS = ("bubble_d3q15_192", "bubble_d2q9_256")
 PROFILE_TRAFFIC = {  # per-launch DRAM bytes summaries committed under profiles/
     "column_d2q9_128x512": "k_fused_d2q9_column_128x512.txt",
     "bubble_d2q9_256": "k_fused_d2q9_bubble_256.txt",
@@ -200,64 +210,101 @@ def cpu_baseline(workload, steps, procs):
 
 
 # -------------------------------------------------------------------- our arm
+def measure(case, path, precision, steps, warmup, local, stream, flush, world, dev):
+    """Warm-up, then `steps` steps each timed alone after an L2 flush (CUDA
+    events on the library's stream, clocks sampled meanwhile); then the same
+    steps back to back (informational)."""
+    import torch
+    from multiphaselb_b200 import Lattice
+    with torch.cuda.stream(stream):
+        lat = Lattice(case, path=path, device=local, stream=stream.cuda_stream, precision=precision)
+        lat.upload_case()
+        lat.initialize()
+        info0 = lat.info()
+        for _ in range(warmup):
+            lat.step(1)
+        torch.cuda.synchronize()
+        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+        barrier(world, dev)
+        torch.cuda.synchronize()
+        with ClockSampler(local) as clk:
+            time.sleep(0.3)
+            mark = clk.mark()
+            launches0 = lat.info()["kernel_launches"]
+            for i in range(steps):
+                flush.zero_()
+                ev[i][0].record(stream)
+                lat.step(1)
+                ev[i][1].record(stream)
+            torch.cuda.synchronize()
+            launches = lat.info()["kernel_launches"] - launches0
+            time.sleep(0.25)
+            clocks = clk.summary(mark)
+        s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s0.record(stream)
+        lat.step(steps)
+        s1.record(stream)
+        torch.cuda.synchronize()
+        steady_ms = s0.elapsed_time(s1) / steps
+        barrier(world, dev)
+        step_ms = [st.elapsed_time(en) for st, en in ev]
+        info = lat.info()
+        lat.close()
+    return dict(step_ms=step_ms, steady_ms=steady_ms, launches=launches, clocks=clocks, info=info, info0=info0)
+
+
+def kernel_name(case, precision):
+    from multiphaselb_b200 import abi
+    base = "k_fused_d2q9" if case.lattice == abi.D2Q9 else "k_fused_d3q15"
+    return base.replace("k_fused", "k_fused32") if precision == abi.FP32_DEV else base
+
+
 def run_ours(a):
     import torch
-    from multiphaselb_b200 import PATH_AUTO, PATH_FUSED, PATH_OPERATORS, Lattice, cases
+    from multiphaselb_b200 import PATH_AUTO, PATH_FUSED, PATH_OPERATORS, Lattice, abi, cases
     world, rank, local = dist_setup()
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
-    wl = WORKLOADS[a.workload]
-    case = wl["build"](cases)
     path = {"auto": PATH_AUTO, "fused": PATH_FUSED, "operators": PATH_OPERATORS}[a.path]
     stream = torch.cuda.Stream(device=dev)
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)  # 256 MiB > 126 MB L2
     peak, peak_kind = peaks()
+    peak_source = f"{peak_kind} MEASURED_PEAKS hbm_gbs" if peak_kind == "measured" else "fallback 6.65 TB/s"
 
-    def timed(precision, steps):
-        """Warm-up, then `steps` steps each timed alone after an L2 flush;
-        then the same steps back to back (informational)."""
-        with torch.cuda.stream(stream):
-            lat = Lattice(case, path=path, device=local, stream=stream.cuda_stream, precision=precision)
-            lat.upload_case()
-            lat.initialize()
-            info0 = lat.info()
-            for _ in range(a.warmup):
-                lat.step(1)
-            torch.cuda.synchronize()
-            ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
-            barrier(world, dev)
-            torch.cuda.synchronize()
-            with ClockSampler(local) as clk:
-                time.sleep(0.3)
-                mark = clk.mark()
-                launches0 = lat.info()["kernel_launches"]
-                for i in range(steps):
-                    flush.zero_()
-                    ev[i][0].record(stream)
-                    lat.step(1)
-                    ev[i][1].record(stream)
-                torch.cuda.synchronize()
-                launches = lat.info()["kernel_launches"] - launches0
-                time.sleep(0.25)
-                clocks = clk.summary(mark)
-            s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            s0.record(stream)
-            lat.step(steps)
-            s1.record(stream)
-            torch.cuda.synchronize()
-            steady_ms = s0.elapsed_time(s1) / steps
-            barrier(world, dev)
-            step_ms = [st.elapsed_time(en) for st, en in ev]
-            info = lat.info()
-            lat.close()
-        return dict(step_ms=step_ms, steady_ms=steady_ms, launches=launches, clocks=clocks, info=info, info0=info0)
+    def device_line(name, steps):
+        """FP64 and FP32-deviation device timings of one workload."""
+        wl = WORKLOADS[name]
+        case = wl["build"](cases)
+        r64 = measure(case, path, abi.FP64, steps, a.warmup, local, stream, flush, world, dev)
+        total_ms = max_over_ranks(sum(r64["step_ms"]), world, dev)
+        kernel_ms = sum(r64["step_ms"]) / len(r64["step_ms"])  # one fused launch per step
+        achieved = wl["bytes_per_lup"] * case.n / (kernel_ms * 1e-3) / 1e9
+        out = {
+            "case": case, "r64": r64, "total_ms": total_ms,
+            "value": round(case.n * steps * world / (total_ms * 1e-3) / 1e9, 4),
+            "ms_per_step": round(total_ms / steps, 6),
+            "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                         "frac": round(achieved / peak, 4), "peak_source": peak_source,
+                         "traffic": profiled_traffic(name), "kernel": kernel_name(case, abi.FP64),
+                         "kernel_ms": round(kernel_ms, 6)},
+        }
+        if not a.no_fp32:
+            r32 = measure(case, path, abi.FP32_DEV, steps, a.warmup, local, stream, flush, world, dev)
+            ms32 = max_over_ranks(sum(r32["step_ms"]), world, dev) / steps
+            ach32 = wl["bytes_per_lup32"] * case.n / (sum(r32["step_ms"]) / steps * 1e-3) / 1e9
+            out["fp32_dev"] = {"value": round(case.n * world / (ms32 * 1e-3) / 1e9, 4), "unit": "GLUPS",
+                               "ms_per_step": round(ms32, 6), "bytes_per_lup": wl["bytes_per_lup32"],
+                               "roofline_frac": round(ach32 / peak, 4), "kernel": kernel_name(case, abi.FP32_DEV),
+                               "steady_state_glups": round(case.n / (r32["steady_ms"] * 1e-3) / 1e9, 4),
+                               "launches": int(r32["launches"]),
+                               "note": "same workload, FP32-deviation storage (not bit-identical to FP64; "
+                                       "its error against FP64 is measured by multiphaselb_b200.accuracy)"}
+        return out
 
-    from multiphaselb_b200 import abi
-    r64 = timed(abi.FP64, a.steps)
-    total_ms = max_over_ranks(sum(r64["step_ms"]), world, dev)
-    kernel_ms = sum(r64["step_ms"]) / len(r64["step_ms"])  # one fused launch per step
-    steady_ms, launches, clocks, info, info0 = r64["steady_ms"], r64["launches"], r64["clocks"], r64["info"], r64["info0"]
-    r32 = timed(abi.FP32_DEV, a.steps) if not a.no_fp32 else None
+    head = device_line(a.workload, a.steps)
+    case, wl, r64 = head["case"], WORKLOADS[a.workload], head["r64"]
+    info, info0 = r64["info"], r64["info0"]
+    launches = {"fp64_timed_steps": int(r64["launches"]), "fp32_dev_timed_steps": int(head.get("fp32_dev", {}).get("launches", 0))}
 
     # end to end through the C-ABI: pinned host fields -> device, steps, all fields back
     n, Q = case.n, case.Q
@@ -277,6 +324,7 @@ def run_ours(a):
         torch.cuda.synchronize()
         t0 = torch.cuda.Event(enable_timing=True)
         t1 = torch.cuda.Event(enable_timing=True)
+        k0 = lat.info()["kernel_launches"]
         t0.record(stream)
         lat.upload(rho=h_rho, U=h_U, T=h_T)
         lat.initialize()
@@ -284,45 +332,47 @@ def run_ours(a):
         lat.download(out)
         t1.record(stream)
         torch.cuda.synchronize()
+        launches["e2e"] = int(lat.info()["kernel_launches"] - k0)
         e2e_ms = max_over_ranks(t0.elapsed_time(t1), world, dev)
         lat.close()
     h2d = n * (1 + 3 + 1) * 8
     d2h = n * (1 + 3 + 1 + 3 + 3 + 1 + Q + (Q if case.g is not None else Q)) * 8
 
-    glups = n * a.steps * world / (total_ms * 1e-3) / 1e9
-    achieved = wl["bytes_per_lup"] * n / (kernel_ms * 1e-3) / 1e9
-    traffic = profiled_traffic(a.workload)
     line = {
-        "metric": METRIC, "value": round(glups, 4), "unit": "GLUPS", "n_gpus": world,
-        "steps": a.steps, "warmup": a.warmup, "ms_per_step": round(total_ms / a.steps, 6),
+        "metric": METRIC, "value": head["value"], "unit": "GLUPS", "n_gpus": world,
+        "steps": a.steps, "warmup": a.warmup, "ms_per_step": head["ms_per_step"],
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic (seeded lattice of the named shape; no dataset)",
-        "config": {"workload": a.workload, "desc": wl["desc"], "nodes_per_gpu": n,
+        "config": {"workload": a.workload, "desc": wl["desc"], "eos": wl["eos"], "nodes_per_gpu": n,
                    "path": {0: "auto", 1: "operators", 2: "fused"}[path] + f" -> {['', 'operators', 'fused'][info0['path']]}",
                    "l2": "256 MiB buffer written between timed steps; each step timed alone",
                    "parallelism": f"replicas x{world}", "bytes_per_lup": wl["bytes_per_lup"]},
-        "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
-                     "frac": round(achieved / peak, 4), "peak_source": f"{peak_kind} MEASURED_PEAKS hbm_gbs" if peak_kind == "measured" else "fallback 6.65 TB/s",
-                     "traffic": traffic,
-                     "kernel": "k_fused_d2q9" if case.lattice == 0 else "k_fused_d3q15",
-                     "kernel_ms": round(kernel_ms, 6)},
+        "roofline": head["roofline"],
         "e2e": {"value": round(n * e2e_steps * world / (e2e_ms * 1e-3) / 1e9, 4), "unit": "GLUPS",
                 "h2d_bytes_per_step": round(h2d / e2e_steps, 1), "d2h_bytes_per_step": round(d2h / e2e_steps, 1),
                 "timed": f"upload rho/U/T from pinned host memory, initialize, {e2e_steps} steps, download every field"},
-        "steady_state": {"ms_per_step": round(steady_ms, 6), "value": round(n / (steady_ms * 1e-3) / 1e9, 4),
+        "steady_state": {"ms_per_step": round(r64["steady_ms"], 6), "value": round(n / (r64["steady_ms"] * 1e-3) / 1e9, 4),
                          "unit": "GLUPS", "note": "no L2 flush between steps (informational, not the headline)"},
         "tile_config": info["tile_config"],
-        "gpu_launches": int(launches),
-        "clocks": clocks,
+        "clocks": r64["clocks"],
     }
-    if r32 is not None:
-        ms32 = max_over_ranks(sum(r32["step_ms"]), world, dev) / a.steps
-        ach32 = wl["bytes_per_lup32"] * n / (sum(r32["step_ms"]) / a.steps * 1e-3) / 1e9
-        line["fp32_dev"] = {"value": round(n * world / (ms32 * 1e-3) / 1e9, 4), "unit": "GLUPS",
-                            "ms_per_step": round(ms32, 6), "bytes_per_lup": wl["bytes_per_lup32"],
-                            "roofline_frac": round(ach32 / peak, 4),
-                            "steady_state_glups": round(n / (r32["steady_ms"] * 1e-3) / 1e9, 4),
-                            "note": "same workload, FP32-deviation storage (not bit-identical; error in DESIGN)"}
+    if "fp32_dev" in head:
+        line["fp32_dev"] = {k: v for k, v in head["fp32_dev"].items() if k != "launches"}
+    # the other named workloads, device-timed the same way (FP64 and FP32-deviation)
+    extra = {}
+    for name in ([] if a.no_extra else [w for w in EXTRA_WORKLOADS if w != a.workload]):
+        x = device_line(name, a.extra_steps or a.steps)
+        launches[name] = int(x["r64"]["launches"] + x.get("fp32_dev", {}).get("launches", 0))
+        extra[name] = {"desc": WORKLOADS[name]["desc"], "eos": WORKLOADS[name]["eos"], "nodes": x["case"].n,
+                       "steps": a.extra_steps or a.steps, "value": x["value"], "unit": "GLUPS",
+                       "ms_per_step": x["ms_per_step"], "roofline": x["roofline"],
+                       "tile_config": x["r64"]["info"]["tile_config"], "clocks": x["r64"]["clocks"]}
+        if "fp32_dev" in x:
+            extra[name]["fp32_dev"] = {k: v for k, v in x["fp32_dev"].items() if k != "launches"}
+    if extra:
+        line["extra"] = extra
+    line["gpu_launches"] = launches["fp64_timed_steps"]  # the headline's timed region
+    line["gpu_launches_by_region"] = launches
     if rank == 0 and world == 1 and not a.no_cpu:
         line["cpu_baseline"] = cpu_baseline(a.workload, a.cpu_steps, 1)
     if world > 1:
@@ -418,6 +468,8 @@ def main():
                          "reference's own exchange code, one thread each")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-fp32", action="store_true")
+    ap.add_argument("--no-extra", action="store_true", help="time the named workload only")
+    ap.add_argument("--extra-steps", type=int, default=0, help="timed steps of each extra workload (default --steps)")
     a = ap.parse_args()
     if a.warmup < 3:
         ap.error("--warmup must be >= 3")

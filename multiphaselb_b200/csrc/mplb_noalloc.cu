@@ -19,7 +19,6 @@
 // has to be cleared between calls (the array keeps the last call's partials).
 #include <cuda_runtime.h>
 
-#include <mutex>
 #include <string>
 
 #include "../../include/mplb_gpu.h"
@@ -33,15 +32,12 @@ constexpr int NA_TPB = 256;
 constexpr int NA_ITEMS = 16;  // elements per thread
 constexpr int NA_MAX_BLOCKS = 4096;
 constexpr uint64_t NA_MAX_N = (uint64_t)NA_MAX_BLOCKS * NA_TPB * NA_ITEMS;  // 16,777,216
-constexpr int NA_MAX_DEVICES = 256;
 
+// In host code this name is only a host-side stand-in, never a device
+// address: every call asks the runtime for the array's address on the
+// current device (cudaGetSymbolAddress), so a module loaded again after a
+// device reset is found where it now lies.
 static __device__ __align__(256) double g_noalloc_scratch[2 * NA_MAX_BLOCKS];
-
-// Device address of g_noalloc_scratch per device, looked up on the first
-// call made with that device current.  In host code the symbol's name is
-// only a host-side stand-in, never a device address.
-double* g_scratch_ptr[NA_MAX_DEVICES] = {};
-std::mutex g_scratch_mu;
 
 __device__ __forceinline__ void block_sum2(double& a, double& b, double* sa, double* sb) {
 #pragma unroll
@@ -110,22 +106,24 @@ extern "C" int mplb_mass_energy_noalloc(const double* rho, const double* T, uint
                                                   " nodes; use mplb_gpu_mass_energy for larger lattices");
     int dev = -1;
     cudaError_t e = cudaGetDevice(&dev);
-    if (e != cudaSuccess || dev < 0 || dev >= NA_MAX_DEVICES)
+    if (e != cudaSuccess)
         return mplb_internal_fail(MPLB_E_CUDA, std::string("mplb_mass_energy_noalloc: no current device: ") +
                                                    cudaGetErrorString(e));
-    double* scratch = nullptr;
-    {
-        std::lock_guard<std::mutex> lock(g_scratch_mu);
-        if (!g_scratch_ptr[dev]) {
-            void* p = nullptr;
-            e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-            if (e != cudaSuccess || !p)
-                return mplb_internal_fail(MPLB_E_CUDA, std::string("mplb_mass_energy_noalloc: scratch lookup failed: ") +
-                                                           cudaGetErrorString(e));
-            g_scratch_ptr[dev] = static_cast<double*>(p);
-        }
-        scratch = g_scratch_ptr[dev];
-    }
+    // An error left pending by earlier work would otherwise be read back after
+    // the launches below and reported as theirs.
+    e = cudaGetLastError();
+    if (e != cudaSuccess)
+        return mplb_internal_fail(MPLB_E_CUDA, std::string("mplb_mass_energy_noalloc: an error from earlier CUDA "
+                                                           "work was pending (now cleared), nothing was queued: ") +
+                                                   cudaGetErrorString(e));
+    // The first call on a device loads the library's module there; later
+    // calls only look the address up.
+    void* p = nullptr;
+    e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess || !p)
+        return mplb_internal_fail(MPLB_E_CUDA, std::string("mplb_mass_energy_noalloc: scratch lookup failed on device ") +
+                                                   std::to_string(dev) + ": " + cudaGetErrorString(e));
+    double* scratch = static_cast<double*>(p);
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     const int nblocks = (int)(((uint64_t)n + (uint64_t)NA_TPB * NA_ITEMS - 1) / ((uint64_t)NA_TPB * NA_ITEMS));
     if (nblocks > 0) na_partial<<<nblocks, NA_TPB, 0, s>>>(rho, T, n, scratch);

@@ -31,10 +31,24 @@ OP_EQUILIBRIUM, OP_COLLISION, OP_LBSTREAM, OP_BOUNDARIES, OP_DENSITY, OP_VELOCIT
 _loaded = {}
 
 
+# The reference tree that oracle/Makefile compiles the reference checker from
+# (read in place, never copied): MPLB_REFERENCE, else the default location.
+REF_ROOT = os.environ.get("MPLB_REFERENCE", "/root/reference")
+
+
+def ref_tree_present():
+    """Whether the reference sources are here to build the reference checkers."""
+    return os.path.isdir(os.path.join(REF_ROOT, "src"))
+
+
+def make(*targets):
+    """Run oracle/Makefile for `targets` against REF_ROOT."""
+    subprocess.run(["make", "-s", "-C", HERE, f"REF={REF_ROOT}", *targets], check=True)
+
+
 def build(kind="port"):
     """Compile a checker with oracle/Makefile if it is missing."""
-    target = "oracle" if kind == "port" else "ref"
-    subprocess.run(["make", "-s", "-C", HERE, target], check=True)
+    make("oracle" if kind == "port" else "ref")
 
 
 def available(kind):

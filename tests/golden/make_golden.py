@@ -27,6 +27,11 @@ STEPS = {"bubble_d2q9": 12, "column_d2q9": 12, "lid_d2q9": 9, "bubble_d3q15": 5,
          "st_d2q9": 10, "st_d3q15": 5, "my_column_d2q9": 9, "my_walls_d3q15": 5, "outflow_d2q9": 8,
          "outflow_corner_d2q9": 6, "outflow_d3q15": 5, "cylinder_d2q9": 8,
          "my_slab_d3q15": 6}
+# Long runs (fixtures named long_<case>_<steps>steps.npz): a thermal column
+# with bounce-back and fixedT walls, a walled D3Q15 box with gravity and an
+# external force, and the surface-tension channel, each far past the first
+# steps, where a divergence that starts late would show.
+LONG_STEPS = {"column_d2q9": 1000, "walls_d3q15": 1000, "st_d2q9": 1000}
 
 
 def save_case(path, case, steps, out):
@@ -71,11 +76,12 @@ def main(names=None):
     for name, case in small_cases().items():
         if names and name not in names:
             continue
-        steps = STEPS[name]
-        out = run_checker("ref", case, steps)
-        path = os.path.join(HERE, f"{name}_{steps}steps.npz")
-        save_case(path, case, steps, out)
-        print(path, os.path.getsize(path))
+        runs = [("", STEPS[name])] + ([("long_", LONG_STEPS[name])] if name in LONG_STEPS else [])
+        for prefix, steps in runs:
+            out = run_checker("ref", case, steps)
+            path = os.path.join(HERE, f"{prefix}{name}_{steps}steps.npz")
+            save_case(path, case, steps, out)
+            print(path, os.path.getsize(path))
 
 
 if __name__ == "__main__":

@@ -6,7 +6,6 @@ handle -> steps -> results written back into the reference structs) leaves
 exactly the state the reference's own CPU loop produces."""
 import ctypes as C
 import os
-import subprocess
 
 import numpy as np
 import pytest
@@ -21,11 +20,11 @@ ADAPTER = os.path.join(HERE, "..", "oracle", "_ref", "libmplb_adapter_check.so")
 
 def adapter_lib():
     if not os.path.exists(ADAPTER):
-        if not os.path.isdir("/root/reference/src"):
+        if not orc.ref_tree_present():
             pytest.skip("adapter checker not built and the reference tree is absent")
         from multiphaselb_b200 import build
         build.build()
-        subprocess.run(["make", "-s", "-C", os.path.join(HERE, "..", "oracle"), "adapter"], check=True)
+        orc.make("adapter")
     orc._lib("ref")  # load the harness first (same file the adapter links)
     lib = C.CDLL(ADAPTER)
     lib.adapter_pack_check.argtypes = [C.c_void_p]

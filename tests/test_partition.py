@@ -110,7 +110,7 @@ def _ref_standard(n, ranks):
     import ctypes as C
     import os
     from oracle import oracle as orc
-    if not orc.available("ref") and not os.path.isdir("/root/reference/src"):
+    if not orc.available("ref") and not orc.ref_tree_present():
         pytest.skip("reference build absent")
     lib = orc._lib("ref")
     fn = lib.ref_standard_decomp

@@ -13,6 +13,7 @@ import numpy as np
 import pytest
 
 from multiphaselb_b200 import abi, mesh, slabs
+from oracle import oracle as orc
 from tests.helpers import small_cases
 
 HERE = os.path.dirname(os.path.abspath(__file__))
@@ -21,9 +22,9 @@ PARTITIONER = os.path.join(HERE, "..", "oracle", "_ref", "latticeMeshPartition")
 
 def partitioner():
     if not os.path.exists(PARTITIONER):
-        if not os.path.isdir("/root/reference/src"):
+        if not orc.ref_tree_present():
             pytest.skip("reference partitioner not built and the reference tree is absent")
-        subprocess.run(["make", "-s", "-C", os.path.join(HERE, "..", "oracle"), "ref", "partition"], check=True)
+        orc.make("ref", "partition")
     return PARTITIONER
 
 

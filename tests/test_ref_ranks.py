@@ -27,7 +27,7 @@ from tests.test_slabs import CheckerHandle, fields_of
 
 
 def RefRanks(parts):
-    if not orc.available("ref") and not os.path.isdir("/root/reference/src"):
+    if not orc.available("ref") and not orc.ref_tree_present():
         pytest.skip("reference build absent")
     return orc.RefRanks(parts)
 

@@ -50,6 +50,34 @@ def test_noalloc_matches_handle_sums_twice(gpu_lib):
             assert abs(e - want_e) <= RTOL * abs(want_e), (call, e, want_e)
 
 
+def test_noalloc_many_blocks_then_fewer_then_no_energy(gpu_lib):
+    """Plain device arrays of a few million nodes (over a thousand partial
+    blocks, summed again by the final pass) against torch.sum; then a call on
+    fewer nodes, which must not pick up partials the larger call left in the
+    shared scratch; then a call without T, whose energy is 0."""
+    import torch
+    fn = _bind(gpu_lib)
+    g = torch.Generator(device="cuda").manual_seed(20261203)
+    n_big, n_small = 5_000_000, 70_001
+    rho = torch.rand(n_big, dtype=torch.float64, device="cuda", generator=g) + 0.5
+    T = torch.rand(n_big, dtype=torch.float64, device="cuda", generator=g) * 0.1 + 0.05
+    out = torch.full((2,), float("nan"), dtype=torch.float64, device="cuda")
+    for n in (n_big, n_small):
+        rc = fn(rho.data_ptr(), T.data_ptr(), n, out.data_ptr(), None)
+        assert rc == 0, gpu_lib.mplb_gpu_last_error().decode()
+        torch.cuda.synchronize()
+        m, e = out.tolist()
+        want_m, want_e = rho[:n].sum().item(), T[:n].sum().item()
+        assert abs(m - want_m) <= RTOL * abs(want_m), (n, m, want_m)
+        assert abs(e - want_e) <= RTOL * abs(want_e), (n, e, want_e)
+    rc = fn(rho.data_ptr(), None, n_small, out.data_ptr(), None)
+    assert rc == 0, gpu_lib.mplb_gpu_last_error().decode()
+    torch.cuda.synchronize()
+    m, e = out.tolist()
+    assert abs(m - rho[:n_small].sum().item()) <= RTOL * abs(m)
+    assert e == 0.0
+
+
 def test_noalloc_rejects_oversized_input(gpu_lib):
     import torch
     fn = _bind(gpu_lib)
