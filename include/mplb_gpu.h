@@ -39,7 +39,8 @@
 extern "C" {
 #endif
 
-#define MPLB_ABI_VERSION 3  /* 2: mplb_field_desc.alpha_1/alpha_2, mplb_opts.rank; 3: mplb_gpu_copy_nodes */
+#define MPLB_ABI_VERSION 4  /* 2: mplb_field_desc.alpha_1/alpha_2, mplb_opts.rank; 3: mplb_gpu_copy_nodes;
+                               4: mplb_info.tile_ms[16], MPLB_E_TIMEOUT */
 #define MPLB_MAX_Q 15
 #define MPLB_MAX_PATCHES 64
 
@@ -84,7 +85,10 @@ enum {
     MPLB_E_CUDA = -3,        /* CUDA runtime error */
     MPLB_E_STATE = -4,       /* call not valid in the handle's current state */
     MPLB_E_NONFINITE = -5,   /* NaN/Inf found by a check */
-    MPLB_E_IO = -6           /* a field file or its folder could not be made or written */
+    MPLB_E_IO = -6,          /* a field file or its folder could not be made or written */
+    MPLB_E_TIMEOUT = -7      /* a bounded wait inside a kernel ran out: the steps since the last
+                                synchronising call are not valid (reported by mplb_gpu_sync and
+                                mplb_gpu_download) */
 };
 
 /*
@@ -154,7 +158,8 @@ typedef struct mplb_info {
     uint64_t device_bytes;   /* device memory held by the handle */
     uint64_t kernel_launches;/* kernels this handle has launched so far */
     int32_t tile_config;     /* fused path: candidate in use (0-based), -1 before the first step */
-    float tile_ms[8];        /* fused path: autotuner time per candidate (ms per step), 0 = not timed */
+    float tile_ms[16];       /* fused path: autotuner time per candidate (ms per step), 0 = not timed,
+                                -1 = the candidate does not take this lattice */
 } mplb_info;
 
 typedef struct mplb_gpu mplb_gpu_t;

@@ -17,7 +17,7 @@ FIELD_F, FIELD_G = 0, 1
 FP64, FP32_DEV = 0, 1
 PATH_AUTO, PATH_OPERATORS, PATH_FUSED = 0, 1, 2
 
-OK, E_ARG, E_UNSUPPORTED, E_CUDA, E_STATE, E_NONFINITE, E_IO = 0, -1, -2, -3, -4, -5, -6
+OK, E_ARG, E_UNSUPPORTED, E_CUDA, E_STATE, E_NONFINITE, E_IO, E_TIMEOUT = 0, -1, -2, -3, -4, -5, -6, -7
 FMT_ASCII_RAW, FMT_BINARY_RAW, FMT_PVTU, FMT_ENSIGHT = 0, 1, 2, 3
 FORMATS = {"asciiRaw": FMT_ASCII_RAW, "binaryRaw": FMT_BINARY_RAW, "pvtu": FMT_PVTU, "ensight": FMT_ENSIGHT}
 SNAP_PRESSURE, SNAP_PDFS = 1, 2
@@ -87,7 +87,7 @@ class Info(C.Structure):
         ("device_bytes", C.c_uint64),
         ("kernel_launches", C.c_uint64),
         ("tile_config", C.c_int32),
-        ("tile_ms", C.c_float * 8),
+        ("tile_ms", C.c_float * 16),
     ]
 
 

@@ -4,9 +4,22 @@
 // object (compiled without multiply-add contraction).
 #pragma once
 
+#include <cudaTypedefs.h>
+
 #include "fused.cuh"
+#include "fused_tma.cuh"
 
 namespace mplb {
+
+// Tensor maps of one TMA candidate over one input population buffer and the
+// temperature field (a map holds its box shape, so each candidate has its own).
+struct TmaMaps {
+    int cfg = -1;
+    const void* f = nullptr;
+    const void* T = nullptr;
+    alignas(64) CUtensorMap mf;
+    alignas(64) CUtensorMap mT;
+};
 
 struct FusedConfig {
     std::string err;
@@ -16,12 +29,67 @@ struct FusedConfig {
     int lat = 0;
     int cfg = 0;           // chosen candidate
     bool tuned = false;    // autotuner has run (or a candidate was forced)
-    Geom geom[N_CFG3 > N_CFG2 ? N_CFG3 : N_CFG2];
-    float tune_ms[N_CFG3 > N_CFG2 ? N_CFG3 : N_CFG2] = {};
+    Geom geom[N_CFG_MAX];
+    float tune_ms[N_CFG_MAX] = {};
     int ncfg = 0;
     int nblocks = 0;
     double* my_scratch = nullptr;  // myMRT: rho_a and gsum_a, 2 n doubles
+    int* kerr = nullptr;           // kernel error flag (bounded waits), one int
+    int* kerr_host = nullptr;      // its pinned host copy
+    TmaMaps tmaps[4];              // two TMA candidates x two population buffers
+    int tmaps_next = 0;
 };
+
+// cuTensorMapEncodeTiled from the driver, found through the runtime (the
+// library does not link the driver API).
+inline PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = [] {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q{};
+        if (cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &p, 12000, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess)
+            p = nullptr;
+        return reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+    }();
+    return fn;
+}
+
+// The maps of TMA candidate `cfg` for the step's input buffers: the
+// populations as a 4D tensor (x, y, z, k) and T as a 3D one (x, y, z), FP64,
+// boxes of (TX+4) x (TY+2) x 1 (x 1), no swizzle, zero fill (never read: the
+// kernel takes tensor copies only for boxes inside the lattice).
+inline const TmaMaps* tma_maps(FusedConfig& fc, int cfg, const FusedArgs& A, uint32_t n) {
+    for (const TmaMaps& m : fc.tmaps)
+        if (m.cfg == cfg && m.f == A.fin && m.T == A.Told) return &m;
+    auto enc = tensor_map_encoder();
+    if (!enc) {
+        fc.err = "cuTensorMapEncodeTiled is not available from the driver";
+        return nullptr;
+    }
+    TmaMaps& m = fc.tmaps[fc.tmaps_next];
+    const TileCfg t = CFG3[cfg];
+    const cuuint64_t dims[4] = {(cuuint64_t)A.nx, (cuuint64_t)A.ny, (cuuint64_t)A.nz, 15};
+    const cuuint64_t strides[3] = {(cuuint64_t)A.nx * 8, (cuuint64_t)A.nx * A.ny * 8, (cuuint64_t)n * 8};
+    const cuuint32_t box[4] = {(cuuint32_t)(t.tx + 4), (cuuint32_t)(t.ty + 2), 1, 1};
+    const cuuint32_t es[4] = {1, 1, 1, 1};
+    CUresult r = enc(&m.mf, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 4, const_cast<double*>(A.fin), dims, strides, box, es,
+                     CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                     CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r == CUDA_SUCCESS)
+        r = enc(&m.mT, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, const_cast<double*>(A.Told), dims, strides, box, es,
+                CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) {
+        fc.err = "cuTensorMapEncodeTiled failed (" + std::to_string((int)r) + ")";
+        m.cfg = -1;
+        return nullptr;
+    }
+    m.cfg = cfg;
+    m.f = A.fin;
+    m.T = A.Told;
+    fc.tmaps_next = (fc.tmaps_next + 1) % 4;
+    return &m;
+}
 
 template <int TX, int TY, bool PIPE, bool HAS_BC, bool EMIT>
 cudaError_t set_smem3() {
@@ -47,7 +115,25 @@ inline cudaError_t fused_attributes() {
     MPLB_SET3(32, 16, false)
     MPLB_SET3(64, 8, false)
 #undef MPLB_SET3
+    chk(cudaFuncSetAttribute(k_fused_d3q15_tma<32, 4, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)TmaTile<32, 4>::SMEM));
+    chk(cudaFuncSetAttribute(k_fused_d3q15_tma<32, 8, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)TmaTile<32, 8>::SMEM));
     return e;
+}
+
+template <int TX, int TY, int MINB>
+cudaError_t launch3_tma(FusedConfig& fc, int cfg, int nb, const Params& P, const FusedArgs& A, cudaStream_t s) {
+    const TmaMaps* m = tma_maps(fc, cfg, A, P.n);
+    if (!m) return cudaErrorInvalidValue;
+    launch_step(k_fused_d3q15_tma<TX, TY, MINB>, nb, TX * TY, TmaTile<TX, TY>::SMEM, s, P, A, m->mf, m->mT);
+    return cudaSuccess;
+}
+
+template <int TX, int TY, int MINB, bool TRY_INNER>
+void launch2_split(bool bc, int nb, const Params& P, const FusedArgs& A, cudaStream_t s) {
+    if (bc) launch_step(k_fused_d2q9_fg<TX, TY, MINB, true, TRY_INNER>, nb, 2 * TX * TY, 0, s, P, A);
+    else launch_step(k_fused_d2q9_fg<TX, TY, MINB, false, TRY_INNER>, nb, 2 * TX * TY, 0, s, P, A);
 }
 
 template <int TX, int TY, int MINB, bool F_ON, bool G_ON, bool EMIT, bool INNER, bool MY = false>
@@ -94,11 +180,12 @@ void launch3(bool bc, int nb, const Params& P, const FusedArgs& A, cudaStream_t 
 }
 
 // Launch one fused step with candidate `cfg` (EMIT always uses candidate 0).
-inline cudaError_t fused_launch_cfg(const FusedConfig& fc, int cfg, const Params& P, FusedArgs A, bool f_on, bool g_on,
+inline cudaError_t fused_launch_cfg(FusedConfig& fc, int cfg, const Params& P, FusedArgs A, bool f_on, bool g_on,
                                     bool emit, cudaStream_t s) {
     if (emit) cfg = 0;
     apply_geom(A, fc.geom[cfg]);
     const int nb = fc.geom[cfg].nblocks;
+    if (nb == 0) return cudaErrorInvalidConfiguration;  // the candidate does not take this lattice
     const bool bc = fc.has_bc;
     if (fc.lat == MPLB_D2Q9) {
         if (emit) {
@@ -112,7 +199,11 @@ inline cudaError_t fused_launch_cfg(const FusedConfig& fc, int cfg, const Params
             case 4: launch2_fg<64, 4, false, 0, true>(f_on, g_on, bc, nb, P, A, s); break;
             case 5: launch2_fg<16, 8, false, 6, true>(f_on, g_on, bc, nb, P, A, s); break;
             case 6: launch2_fg<32, 8, false, 3, true>(f_on, g_on, bc, nb, P, A, s); break;
-            default: launch2_fg<32, 4, false, 8, true>(f_on, g_on, bc, nb, P, A, s); break;
+            case 7: launch2_fg<32, 4, false, 8, true>(f_on, g_on, bc, nb, P, A, s); break;
+            case 8: launch2_split<32, 4, 2, false>(bc, nb, P, A, s); break;
+            case 9: launch2_split<32, 4, 2, true>(bc, nb, P, A, s); break;
+            case 10: launch2_split<16, 4, 4, false>(bc, nb, P, A, s); break;
+            default: launch2_split<32, 2, 4, false>(bc, nb, P, A, s); break;
             }
         }
     } else {
@@ -125,14 +216,16 @@ inline cudaError_t fused_launch_cfg(const FusedConfig& fc, int cfg, const Params
             case 2: launch3<32, 4, false, false>(bc, nb, P, A, s); break;
             case 3: launch3<64, 4, false, false>(bc, nb, P, A, s); break;
             case 4: launch3<32, 16, false, false>(bc, nb, P, A, s); break;
-            default: launch3<64, 8, false, false>(bc, nb, P, A, s); break;
+            case 5: launch3<64, 8, false, false>(bc, nb, P, A, s); break;
+            case 6: if (cudaError_t e = launch3_tma<32, 4, 3>(fc, cfg, nb, P, A, s)) return e; break;
+            default: if (cudaError_t e = launch3_tma<32, 8, 2>(fc, cfg, nb, P, A, s)) return e; break;
             }
         }
     }
     return cudaGetLastError();
 }
 
-inline cudaError_t fused_launch(const FusedConfig& fc, const Params& P, const FusedArgs& A, int lat, bool f_on,
+inline cudaError_t fused_launch(FusedConfig& fc, const Params& P, const FusedArgs& A, int lat, bool f_on,
                                 bool g_on, bool emit, cudaStream_t s) {
     (void)lat;
     return fused_launch_cfg(fc, fc.cfg, P, A, f_on, g_on, emit, s);
@@ -163,7 +256,7 @@ inline int fused_autotune(FusedConfig& fc, const Params& P, const FusedArgs& A, 
     for (int c = 0; c < fc.ncfg; c++) {
         float ms_r[TIMED];
         int nt = 0;
-        bool ok = true;
+        bool ok = fc.geom[c].nblocks > 0;
         for (int r = 0; r < WARM + TIMED && ok; r++) {
             if (r >= WARM) cudaEventRecord(e0, s);
             ok = fused_launch_cfg(fc, c, P, A, f_on, g_on, false, s) == cudaSuccess;
@@ -318,8 +411,22 @@ inline int fused_setup(FusedConfig& fc, int lat, const int* model, const Params&
     fc.ncfg = lat == MPLB_D2Q9 ? N_CFG2 : N_CFG3;
     for (int c = 0; c < fc.ncfg; c++) {
         const TileCfg t = lat == MPLB_D2Q9 ? CFG2[c] : CFG3[c];
-        fc.geom[c] = fused_geometry(lat, A, t.tx, t.ty);
+        if (t.tma) {
+            fc.geom[c] = tma3_fits(A, any, t.tx, t.ty) ? resident_geometry(A, t.tx, t.ty, t.minb) : Geom{0, 0, 0, 0};
+        } else if (t.fg) {
+            // flow and liTempMRT heat, both updated
+            const bool fits = P.f_update && P.g_update && model[0] != MPLB_NO_MODEL && model[1] == MPLB_LITEMPMRT;
+            fc.geom[c] = fits ? fused_geometry(lat, A, t.tx, t.ty) : Geom{0, 0, 0, 0};
+        } else {
+            fc.geom[c] = fused_geometry(lat, A, t.tx, t.ty);
+        }
     }
+    if (cudaMalloc((void**)&fc.kerr, sizeof(int)) != cudaSuccess) { fc.err = "cudaMalloc kernel flag"; return MPLB_E_CUDA; }
+    if (cudaMallocHost((void**)&fc.kerr_host, sizeof(int)) != cudaSuccess) { fc.err = "cudaMallocHost kernel flag"; return MPLB_E_CUDA; }
+    *fc.kerr_host = 0;
+    if (cudaMemsetAsync(fc.kerr, 0, sizeof(int), stream) != cudaSuccess) { fc.err = "clear kernel flag"; return MPLB_E_CUDA; }
+    *bytes += sizeof(int);
+    A.kerr = fc.kerr;
     fc.cfg = 0;
     apply_geom(A, fc.geom[0]);
     fc.nblocks = fc.geom[0].nblocks;
@@ -330,7 +437,21 @@ inline int fused_setup(FusedConfig& fc, int lat, const int* model, const Params&
     return 0;
 }
 
+// The kernel error flag (0, or MPLB_KERR_WAIT after a bounded wait ran
+// out): queue its copy to the pinned host int and its reset on the stream;
+// after the caller's next synchronisation fused_kerr_value() holds it.
+inline bool fused_queue_kerr(FusedConfig& fc, cudaStream_t s) {
+    if (!fc.kerr) return true;
+    return cudaMemcpyAsync(fc.kerr_host, fc.kerr, sizeof(int), cudaMemcpyDeviceToHost, s) == cudaSuccess &&
+           cudaMemsetAsync(fc.kerr, 0, sizeof(int), s) == cudaSuccess;
+}
+inline int fused_kerr_value(const FusedConfig& fc) { return fc.kerr_host ? *fc.kerr_host : 0; }
+
 inline void fused_free(FusedConfig& fc) {
+    if (fc.kerr) cudaFree(fc.kerr);
+    fc.kerr = nullptr;
+    if (fc.kerr_host) cudaFreeHost(fc.kerr_host);
+    fc.kerr_host = nullptr;
     if (fc.bcmap) cudaFree(fc.bcmap);
     fc.bcmap = nullptr;
     if (fc.my_scratch) cudaFree(fc.my_scratch);

@@ -648,20 +648,25 @@ int put_aos(mplb_gpu* h, const double* host, double* dev, int m) {
     return 0;
 }
 
-int get_aos(mplb_gpu* h, double* host, const double* dev, int m) {
+// Device-to-host copies of one field, queued on the handle's stream (the
+// caller synchronises once after the last one).  get_aos transposes through
+// the staging buffer, which the caller has sized for the largest field so
+// that no reallocation happens between queued copies; stream order keeps the
+// next transpose behind the previous copy out of it.
+int get_aos(mplb_gpu* h, double* host, const double* dev, int m, bool sync = true) {
     if (!host) return 0;
     size_t e = (size_t)h->n * m;
     RET(staging(h, e));
     LAUNCH(k_soa_to_aos, blocks(e), h->n, m, dev, h->stage);
     CK(cudaMemcpyAsync(host, h->stage, e * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
-    CK(cudaStreamSynchronize(h->stream));
+    if (sync) CK(cudaStreamSynchronize(h->stream));
     return 0;
 }
 
-int get_scalar(mplb_gpu* h, double* host, const double* dev) {
+int get_scalar(mplb_gpu* h, double* host, const double* dev, bool sync = true) {
     if (!host) return 0;
     CK(cudaMemcpyAsync(host, dev, (size_t)h->n * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
-    CK(cudaStreamSynchronize(h->stream));
+    if (sync) CK(cudaStreamSynchronize(h->stream));
     return 0;
 }
 
@@ -689,6 +694,22 @@ struct DeviceGuard {
         if (prev >= 0 && now != prev) cudaSetDevice(prev);
     }
 };
+
+// A bounded wait inside a fused kernel that ran out leaves MPLB_KERR_WAIT in
+// the handle's kernel flag; the steps before the check are not valid.
+// queue_kernel_flag() queues the flag's read on the stream; after the
+// caller has synchronised the stream, kernel_flag_status() reports it.
+int queue_kernel_flag(mplb_gpu* h) {
+    if (h->path != MPLB_PATH_FUSED) return 0;
+    if (!fused_queue_kerr(h->fc, h->stream)) return fail(MPLB_E_CUDA, "queueing the kernel flag read failed");
+    return 0;
+}
+int kernel_flag_status(mplb_gpu* h) {
+    if (h->path != MPLB_PATH_FUSED || !fused_kerr_value(h->fc)) return 0;
+    *h->fc.kerr_host = 0;
+    return fail(MPLB_E_TIMEOUT, "a bounded wait inside a fused step kernel ran out (TMA plane copy not "
+                                "complete); the steps before this call are not valid");
+}
 
 // One fused time step, or (emit) the rebuild of the reference state after
 // the last step from that step's retained input buffers.
@@ -722,6 +743,8 @@ int fused_step(mplb_gpu* h, bool emit) {
         } else {
             int c = h->tile_request > 0 ? h->tile_request - 1 : 0;
             if (c >= h->fc.ncfg) return fail(MPLB_E_ARG, "tile_config out of range");
+            if (h->fc.geom[c].nblocks == 0)
+                return fail(MPLB_E_ARG, "tile_config " + std::to_string(h->tile_request) + " does not take this lattice");
             h->fc.cfg = c;
             h->fc.tuned = true;
         }
@@ -1116,7 +1139,7 @@ int mplb_gpu_info(mplb_gpu_t* h, mplb_info* info) {
     info->device_bytes = h->bytes;
     info->kernel_launches = h->launches;
     info->tile_config = (h->path == MPLB_PATH_FUSED && h->fc.tuned) ? h->fc.cfg : -1;
-    for (int c = 0; c < 8; c++) info->tile_ms[c] = c < h->fc.ncfg ? h->fc.tune_ms[c] : 0.0f;
+    for (int c = 0; c < 16; c++) info->tile_ms[c] = c < h->fc.ncfg ? h->fc.tune_ms[c] : 0.0f;
     return 0;
 }
 
@@ -1141,22 +1164,27 @@ int mplb_gpu_download(mplb_gpu_t* h, double* rho, double* U, double* T, double* 
                       double* f, double* g) {
     if (!h) return fail(MPLB_E_ARG, "NULL handle");
     DeviceGuard guard(h->dev);
+    RET(queue_kernel_flag(h));
     RET(materialize(h));
-    RET(get_scalar(h, rho, h->rho));
-    RET(get_scalar(h, T, h->T));
-    RET(get_scalar(h, S, h->S));
-    RET(get_aos(h, U, h->U, 3));
-    RET(get_aos(h, Fi, h->Fi, 3));
-    RET(get_aos(h, Ft, h->Ft, 3));
+    // every copy queued behind the last, one wait at the end
+    const bool pdfs = (f && h->model[0] != MPLB_NO_MODEL) || (g && h->model[1] != MPLB_NO_MODEL);
+    RET(staging(h, (size_t)h->n * (pdfs ? std::max(3, h->Q) : 3)));
+    RET(get_scalar(h, rho, h->rho, false));
+    RET(get_scalar(h, T, h->T, false));
+    RET(get_scalar(h, S, h->S, false));
+    RET(get_aos(h, U, h->U, 3, false));
+    RET(get_aos(h, Fi, h->Fi, 3, false));
+    RET(get_aos(h, Ft, h->Ft, 3, false));
     if (f) {
         if (h->model[0] == MPLB_NO_MODEL) std::memset(f, 0, (size_t)h->n * h->Q * sizeof(double));
-        else RET(get_aos(h, f, h->F(), h->Q));
+        else RET(get_aos(h, f, h->F(), h->Q, false));
     }
     if (g) {
         if (h->model[1] == MPLB_NO_MODEL) std::memset(g, 0, (size_t)h->n * h->Q * sizeof(double));
-        else RET(get_aos(h, g, h->G(), h->Q));
+        else RET(get_aos(h, g, h->G(), h->Q, false));
     }
-    return 0;
+    CK(cudaStreamSynchronize(h->stream));
+    return kernel_flag_status(h);
 }
 
 int mplb_gpu_initialize(mplb_gpu_t* h) {
@@ -1633,8 +1661,9 @@ int mplb_mlp_init_bubble_mass(mplb_mlp_t* m, mplb_gpu_t* h, double t_ratio, cons
 int mplb_gpu_sync(mplb_gpu_t* h) {
     if (!h) return fail(MPLB_E_ARG, "NULL handle");
     DeviceGuard guard(h->dev);
+    RET(queue_kernel_flag(h));
     CK(cudaStreamSynchronize(h->stream));
-    return 0;
+    return kernel_flag_status(h);
 }
 
 int mplb_gpu_copy_nodes(mplb_gpu_t* dst, uint32_t dst_start, mplb_gpu_t* src, uint32_t src_start,

@@ -85,3 +85,21 @@ def test_fp32dev_large_lattice_kernel(gpu_lib, shape):
     print(shape, errs)
     for k, e in errs.items():
         assert e <= (TOL_BIG if k in BIG else TOL_SMALL), (shape, k, e)
+
+
+def test_fp32dev_thermal_column_short_run(gpu_lib):
+    """The full thermal column (128 x 512, liMRT + liTempMRT, fixedT walls,
+    gravity) in both precisions from the same state: after 1000 and 2000
+    steps the FP32-deviation run's bulk densities, temperatures and energy
+    stay within 2e-5 relative of the FP64 run and its interface height within
+    1e-3 lattice units (measured at 50,000 steps: 2.4e-6, 1.2e-6, 1.2e-7 and
+    4e-6, by multiphaselb_b200.accuracy)."""
+    from multiphaselb_b200 import accuracy, cases
+    r = accuracy.compare_column(cases.column_case(128, 512), 2000, [1000])
+    assert [c["steps"] for c in r["checkpoints"]] == [1000, 2000]
+    for c in r["checkpoints"]:
+        e = c["rel_err"]
+        print(c["steps"], e)
+        assert e["rho_liquid"] <= 2e-5 and e["rho_vapour"] <= 2e-5, e
+        assert e["T_rows"] <= 2e-5 and e["T_nodes"] <= 2e-5 and e["energy"] <= 2e-5, e
+        assert e["interface_y_abs"] <= 1e-3, e
