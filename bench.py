@@ -54,10 +54,11 @@ WORKLOADS = {
 }
 # timed after the named workload in a default run (device time, FP64 and FP32-deviation)
 EXTRA_WORKLOADS = ("bubble_d3q15_192", "bubble_d2q9_256")
-PROFILE_TRAFFIC = {  # per-launch DRAM bytes summaries committed under profiles/
-    "column_d2q9_128x512": "k_fused_d2q9_column_128x512.txt",
-    "bubble_d2q9_256": "k_fused_d2q9_bubble_256.txt",
-    "bubble_d3q15_192": "k_fused_d3q15_bubble.txt",
+PROFILE_TRAFFIC = {  # (workload, kernel) -> ncu summary under profiles/ holding the per-launch DRAM bytes
+    ("column_d2q9_128x512", "k_fused_d2q9"): "k_fused_d2q9_column_128x512.txt",
+    ("bubble_d2q9_256", "k_fused_d2q9"): "k_fused_d2q9_bubble_256.txt",
+    ("bubble_d3q15_192", "k_fused_d3q15"): "k_fused_d3q15_bubble.txt",
+    ("bubble_d3q15_192", "k_fused_d3q15_tma"): "k_fused_d3q15_tma_bubble_192.txt",
 }
 FALLBACK_HBM_GBS = 6650.0
 
@@ -72,9 +73,9 @@ def peaks():
         return FALLBACK_HBM_GBS, "fallback"
 
 
-def profiled_traffic(workload):
-    """DRAM bytes per launch of the fused kernel from the committed ncu summary."""
-    name = PROFILE_TRAFFIC.get(workload)
+def profiled_traffic(workload, kernel):
+    """DRAM bytes per launch of the step kernel from the committed ncu summary."""
+    name = PROFILE_TRAFFIC.get((workload, kernel))
     if not name:
         return None
     path = os.path.join(ROOT, "profiles", name)
@@ -253,10 +254,14 @@ def measure(case, path, precision, steps, warmup, local, stream, flush, world, d
     return dict(step_ms=step_ms, steady_ms=steady_ms, launches=launches, clocks=clocks, info=info, info0=info0)
 
 
-def kernel_name(case, precision):
+def kernel_name(case, precision, tile_config=-1):
+    """The step kernel the autotuner picked (3D candidates 6 and 7 are the TMA-staged kernel)."""
     from multiphaselb_b200 import abi
-    base = "k_fused_d2q9" if case.lattice == abi.D2Q9 else "k_fused_d3q15"
-    return base.replace("k_fused", "k_fused32") if precision == abi.FP32_DEV else base
+    if precision == abi.FP32_DEV:
+        return "k_fused32_d2q9" if case.lattice == abi.D2Q9 else "k_fused32_d3q15"
+    if case.lattice == abi.D2Q9:
+        return "k_fused_d2q9"
+    return "k_fused_d3q15_tma" if tile_config in (6, 7) else "k_fused_d3q15"
 
 
 def run_ours(a):
@@ -279,13 +284,14 @@ def run_ours(a):
         total_ms = max_over_ranks(sum(r64["step_ms"]), world, dev)
         kernel_ms = sum(r64["step_ms"]) / len(r64["step_ms"])  # one fused launch per step
         achieved = wl["bytes_per_lup"] * case.n / (kernel_ms * 1e-3) / 1e9
+        kname = kernel_name(case, abi.FP64, r64["info"]["tile_config"])
         out = {
             "case": case, "r64": r64, "total_ms": total_ms,
             "value": round(case.n * steps * world / (total_ms * 1e-3) / 1e9, 4),
             "ms_per_step": round(total_ms / steps, 6),
             "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                          "frac": round(achieved / peak, 4), "peak_source": peak_source,
-                         "traffic": profiled_traffic(name), "kernel": kernel_name(case, abi.FP64),
+                         "traffic": profiled_traffic(name, kname), "kernel": kname,
                          "kernel_ms": round(kernel_ms, 6)},
         }
         if not a.no_fp32:

@@ -198,10 +198,7 @@ __device__ __forceinline__ void prefetch_node(const Params& P, const FusedArgs& 
 // ------------------------------------------------------------ phase A
 // Pull-stream one node, apply its boundary program, sum moments.
 // f, g receive f''_n, g''_n; miss bit k = population k has no source.
-// OTHER: a field that is not pulled still gives its macro value (rho of a
-// frozen flow field, T of a frozen thermal field); without it that value
-// is left unset (a caller that pulls the two fields in different threads).
-template <class L, bool F_ON, bool G_ON, bool HAS_BC, bool OTHER = true>
+template <class L, bool F_ON, bool G_ON, bool HAS_BC>
 __device__ __forceinline__ void pull_node(const Params& P, const FusedArgs& A, int x, int y, int z,
                                           uint32_t id, double* f, double* g, double& rho, double& T) {
     const uint32_t n = P.n;
@@ -259,7 +256,7 @@ __device__ __forceinline__ void pull_node(const Params& P, const FusedArgs& A, i
 #pragma unroll
         for (int k = 0; k < L::Q; k++) s += f[k];
         rho = s;
-    } else if constexpr (OTHER) {
+    } else {
         rho = A.rho_c[id];
     }
     if constexpr (G_ON) {
@@ -267,7 +264,7 @@ __device__ __forceinline__ void pull_node(const Params& P, const FusedArgs& A, i
 #pragma unroll
         for (int k = 0; k < L::Q; k++) s += g[k];
         T = s;
-    } else if constexpr (OTHER) {
+    } else {
         T = A.Told[id];
     }
 }
@@ -390,7 +387,7 @@ constexpr int min_blocks(int threads) { return threads <= 128 ? 4 : (threads <= 
 
 // Pull-stream one node of an inner tile (no wrap, no missing source, no
 // boundary program): the arithmetic of pull_node without its bookkeeping.
-template <class L, bool F_ON, bool G_ON, bool OTHER = true>
+template <class L, bool F_ON, bool G_ON>
 __device__ __forceinline__ void pull_node_inner(const Params& P, const FusedArgs& A, uint32_t id, double* f,
                                                 double* g, double& rho, double& T) {
     const uint32_t n = P.n;
@@ -406,7 +403,7 @@ __device__ __forceinline__ void pull_node_inner(const Params& P, const FusedArgs
 #pragma unroll
         for (int k = 0; k < L::Q; k++) s += f[k];
         rho = s;
-    } else if constexpr (OTHER) {
+    } else {
         rho = A.rho_c[id];
     }
     if constexpr (G_ON) {
@@ -414,7 +411,7 @@ __device__ __forceinline__ void pull_node_inner(const Params& P, const FusedArgs
 #pragma unroll
         for (int k = 0; k < L::Q; k++) s += g[k];
         T = s;
-    } else if constexpr (OTHER) {
+    } else {
         T = A.Told[id];
     }
 }
@@ -641,216 +638,6 @@ __global__ void __launch_bounds__(F2_TX * F2_TY, MINB ? MINB : min_blocks(F2_TX 
     }
     fused2_tile<F2_TX, F2_TY, F_ON, G_ON, HAS_BC, EMIT, false, EX, EY, GX, GY, MY>(P, A, x0, y0, s_psi, s_inv, s_To,
                                                                                    s_U0, s_U1);
-}
-
-// ---------------------------------------------- 2D kernel, two threads per node
-// The thermal step with liTempMRT heat (flow and heat both updated), with
-// the two populations of a node in two threads: even warps take the flow
-// role, odd warps the heat role, and warp pair q holds the tile's nodes
-// 32q .. 32q+31.  Same operations, same order per value as fused2_tile:
-//
-//   flow role: pull f, flow boundary program, rho (lbstream.c, bounceBack.c,
-//              liMRTDensity.c); psi (potential.c); force and velocity
-//              (interactionForce.c, interForce.c, liMRTVelocity.c); liMRT
-//              collision (liMRTCollision.c); stores f and U.
-//   heat role: pull g, thermal boundary program, T (fixedT.c,
-//              liTempMRTTemperature.c); 1/rho; heat source (heatSource.c);
-//              liTempMRT collision (liTempMRTCollision.c); stores g, T, S.
-//
-// The ring slots split the same way.  Shared memory carries rho and T
-// between the roles (barrier), then psi and 1/rho (barrier), then U_n from
-// the flow role to the heat role through a named barrier, so the flow
-// collision does not wait for the heat source.  Twice the threads of the
-// one-node-per-thread kernel, each with half the dependent work: lattices of
-// one wave (the 128 x 512 column) gain latency hiding.
-template <int TX, int TY, bool HAS_BC, bool INNER>
-__device__ __forceinline__ void fg_tile(const Params& P, const FusedArgs& A, int x0, int y0, double* sm) {
-    using L = D2Q9T;
-    constexpr int EX = TX + 2, EY = TY + 2, NN = TX * TY, NRING = 2 * EX + 2 * TY;
-    double(*s_rho)[EX] = reinterpret_cast<double(*)[EX]>(sm);
-    double(*s_T)[EX] = s_rho + EY;
-    double(*s_psi)[EX] = s_T + EY;
-    double(*s_inv)[EX] = s_psi + EY;
-    double(*s_To)[EX] = s_inv + EY;
-    double(*s_U0)[EX] = s_To + EY;
-    double(*s_U1)[EX] = s_U0 + EY;
-    double* s_Un = sm + 7 * EY * EX;  // [2][NN]
-    const uint32_t n = P.n;
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const bool flow = (warp & 1) == 0;
-    const int t = (warp >> 1) * 32 + lane;  // node of the tile
-    const int tx = t % TX, ty = t / TX;
-
-    // node of ext slot (ex, ey), or false when absent
-    auto locate = [&](int ex, int ey, int& x, int& y, uint32_t& id) -> bool {
-        if constexpr (INNER) {
-            x = x0 - 1 + ex;
-            y = y0 - 1 + ey;
-        } else {
-            x = slot_coord(x0, ex, A.nx, A.px);
-            y = slot_coord(y0, ey, A.ny, A.py);
-            if (x < 0 || y < 0) return false;
-        }
-        id = (uint32_t)x + (uint32_t)A.nx * (uint32_t)y;
-        return true;
-    };
-    // one field of one slot: pulled, boundary program, moment into shared memory
-    double v[9];
-    double mom = 0;
-    auto pull_one = [&](int ex, int ey, bool keep) -> bool {
-        int x, y;
-        uint32_t id;
-        if (!locate(ex, ey, x, y, id)) return false;
-        double rv[9], dummy[1], r = 0, T = 0;
-        double* dst = keep ? v : rv;
-        if (flow) {
-            if constexpr (INNER) pull_node_inner<L, true, false, false>(P, A, id, dst, dummy, r, T);
-            else pull_node<L, true, false, HAS_BC, false>(P, A, x, y, 0, id, dst, dummy, r, T);
-            s_rho[ey][ex] = r;
-            if (keep) mom = r;
-        } else {
-            if constexpr (INNER) pull_node_inner<L, false, true, false>(P, A, id, dummy, dst, r, T);
-            else pull_node<L, false, true, HAS_BC, false>(P, A, x, y, 0, id, dummy, dst, r, T);
-            s_T[ey][ex] = T;
-            s_To[ey][ex] = A.Told[id];
-            s_U0[ey][ex] = A.Uold[id];
-            s_U1[ey][ex] = A.Uold[n + id];
-            if (keep) mom = T;
-        }
-        return true;
-    };
-
-    // phase 1: ring slots, then the own slot (its populations stay in v)
-    for (int r = t; r < NRING; r += NN) {
-        int ex, ey;
-        ring_slot(r, TX, TY, ex, ey);
-        pull_one(ex, ey, false);
-    }
-    const int gx = x0 + tx, gy = y0 + ty;
-    const bool own = INNER || (gx < A.nx && gy < A.ny);
-    const int ex = tx + 1, ey = ty + 1;
-    // threads outside the box still fill the slot of the wrapped node, so
-    // partial tiles see their periodic neighbours
-    const bool have = pull_one(ex, ey, true);
-    __syncthreads();
-
-    // phase 2: psi (flow role) and 1/rho (heat role) of every slot
-    double rho = 0, T = 0, rr = 0;
-    EosRho er{};
-    if (have) {
-        rho = s_rho[ey][ex];
-        T = s_T[ey][ex];
-        if (own) {
-            rr = rcp_rn(rho);
-            er = eos_rho(P, rho);
-            if (flow) s_psi[ey][ex] = potential_p(P, rho, p_eos_at(P, er, rho, T));
-            else s_inv[ey][ex] = rr;
-        } else {
-            if (flow) s_psi[ey][ex] = potential(P, rho, T);
-            else s_inv[ey][ex] = 1.0 / rho;
-        }
-    }
-    for (int r = t; r < NRING; r += NN) {
-        int rex, rey, x, y;
-        uint32_t id;
-        ring_slot(r, TX, TY, rex, rey);
-        if (!locate(rex, rey, x, y, id)) continue;
-        if (flow) s_psi[rey][rex] = potential(P, s_rho[rey][rex], s_T[rey][rex]);
-        else s_inv[rey][rex] = 1.0 / s_rho[rey][rex];
-    }
-    __syncthreads();
-
-    const bool act = own && have;
-    const uint32_t id = (uint32_t)gx + (uint32_t)A.nx * (uint32_t)gy;
-    const bool onb = INNER ? false : on_wall(A, gx, gy, 0);
-    if (flow) {
-        double Fi[3], Ft[3], U[3];
-        const double psi = act ? s_psi[ey][ex] : 0.0;
-        auto nbpsi = [&](int k) { return s_psi[ey + cyk<L>(k)][ex + cxk<L>(k)]; };
-        if (act) {
-            force_velocity<L>(P, onb, v, rho, rr, psi, nbpsi, Fi, Ft, U);
-            s_Un[t] = U[0];
-            s_Un[NN + t] = U[1];
-        }
-        // U_n is in shared memory: let the heat role go on
-        asm volatile("bar.arrive 1, %0;" ::"n"(2 * NN) : "memory");
-        if (act) {
-            double C[L::Q];
-            const double* Cp = nullptr;
-            if (P.st_on) {
-                if (!onb) {
-                    surface_tension<L>(P, psi, nbpsi, C);
-                } else {
-#pragma unroll
-                    for (int k = 0; k < L::Q; k++) C[k] = 0;
-                }
-                Cp = C;
-            }
-            collide_limrt_psi(P, v, rho, U, Ft, Fi, psi, Cp);
-#pragma unroll
-            for (int k = 0; k < 9; k++) A.fout[(size_t)k * n + id] = v[k];
-            A.Unew[id] = U[0];
-            A.Unew[n + id] = U[1];
-        }
-    } else {
-        double heat = 0;
-        if (act) {
-            // heatSource.c:119-165 with the one-sided differences of finiteDifference/*.c
-            double gT[3] = {0, 0, 0}, gR[3] = {0, 0, 0}, div = 0;
-            const double To = s_To[ey][ex], iv = s_inv[ey][ex];
-            {
-                bool a = INNER || wrap1(gx + 1, A.nx, A.px) >= 0, b = INNER || wrap1(gx - 1, A.nx, A.px) >= 0;
-                FD ft = fd_pair(a ? 0 : -1, b ? 0 : -1, s_To[ey][ex + 1], s_To[ey][ex - 1], To);
-                FD fr = fd_pair(a ? 0 : -1, b ? 0 : -1, s_inv[ey][ex + 1], s_inv[ey][ex - 1], iv);
-                FD fu = fd_pair(a ? 0 : -1, b ? 0 : -1, s_U0[ey][ex + 1], s_U0[ey][ex - 1], s_U0[ey][ex]);
-                gT[0] = ft.v;
-                gR[0] = fr.v;
-                if (fu.present) div += fu.v;
-            }
-            {
-                bool a = INNER || wrap1(gy + 1, A.ny, A.py) >= 0, b = INNER || wrap1(gy - 1, A.ny, A.py) >= 0;
-                FD ft = fd_pair(a ? 0 : -1, b ? 0 : -1, s_To[ey + 1][ex], s_To[ey - 1][ex], To);
-                FD fr = fd_pair(a ? 0 : -1, b ? 0 : -1, s_inv[ey + 1][ex], s_inv[ey - 1][ex], iv);
-                FD fu = fd_pair(a ? 0 : -1, b ? 0 : -1, s_U1[ey + 1][ex], s_U1[ey - 1][ex], s_U1[ey][ex]);
-                gT[1] = ft.v;
-                gR[1] = fr.v;
-                if (fu.present) div += fu.v;
-            }
-            double dot = 0;
-#pragma unroll
-            for (int k = 0; k < 3; k++) dot += gT[k] * gR[k];
-            heat = heat_source_value_er(P, er, rho, rr, To, dot, div, A.S[id]);
-        }
-        asm volatile("bar.sync 1, %0;" ::"n"(2 * NN) : "memory");
-        if (act) {
-            collide_litemp(P, v, T, s_Un[t], s_Un[NN + t], heat);
-#pragma unroll
-            for (int k = 0; k < 9; k++) A.gout[(size_t)k * n + id] = v[k];
-            A.Tnew[id] = T;
-            A.S[id] = heat;
-        }
-    }
-}
-
-template <int TX, int TY>
-constexpr size_t fg_smem() {
-    return (size_t)(7 * (TY + 2) * (TX + 2) + 2 * TX * TY) * sizeof(double);
-}
-
-template <int TX, int TY, int MINB, bool HAS_BC, bool TRY_INNER>
-__global__ void __launch_bounds__(2 * TX * TY, MINB) k_fused_d2q9_fg(Params P, FusedArgs A) {
-    static_assert(TX * TY % 32 == 0, "a warp pair holds 32 nodes");
-    step_dependency_wait();
-    __shared__ double sm[fg_smem<TX, TY>() / sizeof(double)];
-    const int bx = blockIdx.x % A.tiles_x, by = blockIdx.x / A.tiles_x;
-    const int x0 = bx * TX, y0 = by * TY;
-    if constexpr (TRY_INNER) {
-        if (inner_tile<TX, TY>(A, x0, y0)) {
-            fg_tile<TX, TY, HAS_BC, true>(P, A, x0, y0, sm);
-            return;
-        }
-    }
-    fg_tile<TX, TY, HAS_BC, false>(P, A, x0, y0, sm);
 }
 
 // ------------------------------------------------------------ 3D kernels
@@ -1090,14 +877,11 @@ struct TileCfg {
     bool inner;  // 2D only: the kernel variant whose inner tiles take the lean body (pays off
                  // on large lattices; a lattice of one wave prefers the smaller general kernel)
     bool tma;    // 3D only: planes staged by TMA (k_fused_d3q15_tma; fully periodic boxes)
-    bool fg;     // 2D only: two threads per node (k_fused_d2q9_fg; flow + liTempMRT heat)
 };
-constexpr int N_CFG2 = 12, N_CFG3 = 8, N_CFG_MAX = 12;
+constexpr int N_CFG2 = 8, N_CFG3 = 8, N_CFG_MAX = 8;
 constexpr TileCfg CFG2[N_CFG2] = {{32, 8, false, 0, false}, {32, 4, false, 0, false}, {64, 4, false, 0, false},
                                   {16, 8, false, 0, true},  {64, 4, false, 0, true},  {16, 8, false, 6, true},
-                                  {32, 8, false, 3, true},  {32, 4, false, 8, true},
-                                  {32, 4, false, 2, false, false, true}, {32, 4, false, 2, true, false, true},
-                                  {16, 4, false, 4, false, false, true}, {32, 2, false, 4, false, false, true}};
+                                  {32, 8, false, 3, true},  {32, 4, false, 8, true}};
 constexpr TileCfg CFG3[N_CFG3] = {{32, 8, false, 0, false}, {32, 8, true, 0, false}, {32, 4, false, 0, false},
                                   {64, 4, false, 0, false}, {32, 16, false, 0, false}, {64, 8, false, 0, false},
                                   {32, 4, false, 3, false, true}, {32, 8, false, 2, false, true}};
@@ -1109,6 +893,8 @@ struct Geom {
 // Launch geometry of a kernel whose blocks stay resident, minb per SM of a
 // 148-SM part: the z chunk count that wastes the fewest block slots over
 // the launch's waves (fewer chunks on a tie: each chunk re-reads two planes).
+// Blocks are ordered column fastest, so the blocks running together hold
+// neighbouring columns at the same planes and share their ring rows in L2.
 inline Geom resident_geometry(const FusedArgs& A, int TX, int TY, int minb) {
     Geom g;
     g.tiles_x = A.nx / TX;

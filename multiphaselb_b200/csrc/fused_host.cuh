@@ -73,11 +73,11 @@ inline const TmaMaps* tma_maps(FusedConfig& fc, int cfg, const FusedArgs& A, uin
     const cuuint32_t box[4] = {(cuuint32_t)(t.tx + 4), (cuuint32_t)(t.ty + 2), 1, 1};
     const cuuint32_t es[4] = {1, 1, 1, 1};
     CUresult r = enc(&m.mf, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 4, const_cast<double*>(A.fin), dims, strides, box, es,
-                     CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                     CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_NONE,
                      CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     if (r == CUDA_SUCCESS)
         r = enc(&m.mT, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, const_cast<double*>(A.Told), dims, strides, box, es,
-                CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_NONE,
                 CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     if (r != CUDA_SUCCESS) {
         fc.err = "cuTensorMapEncodeTiled failed (" + std::to_string((int)r) + ")";
@@ -128,12 +128,6 @@ cudaError_t launch3_tma(FusedConfig& fc, int cfg, int nb, const Params& P, const
     if (!m) return cudaErrorInvalidValue;
     launch_step(k_fused_d3q15_tma<TX, TY, MINB>, nb, TX * TY, TmaTile<TX, TY>::SMEM, s, P, A, m->mf, m->mT);
     return cudaSuccess;
-}
-
-template <int TX, int TY, int MINB, bool TRY_INNER>
-void launch2_split(bool bc, int nb, const Params& P, const FusedArgs& A, cudaStream_t s) {
-    if (bc) launch_step(k_fused_d2q9_fg<TX, TY, MINB, true, TRY_INNER>, nb, 2 * TX * TY, 0, s, P, A);
-    else launch_step(k_fused_d2q9_fg<TX, TY, MINB, false, TRY_INNER>, nb, 2 * TX * TY, 0, s, P, A);
 }
 
 template <int TX, int TY, int MINB, bool F_ON, bool G_ON, bool EMIT, bool INNER, bool MY = false>
@@ -199,11 +193,7 @@ inline cudaError_t fused_launch_cfg(FusedConfig& fc, int cfg, const Params& P, F
             case 4: launch2_fg<64, 4, false, 0, true>(f_on, g_on, bc, nb, P, A, s); break;
             case 5: launch2_fg<16, 8, false, 6, true>(f_on, g_on, bc, nb, P, A, s); break;
             case 6: launch2_fg<32, 8, false, 3, true>(f_on, g_on, bc, nb, P, A, s); break;
-            case 7: launch2_fg<32, 4, false, 8, true>(f_on, g_on, bc, nb, P, A, s); break;
-            case 8: launch2_split<32, 4, 2, false>(bc, nb, P, A, s); break;
-            case 9: launch2_split<32, 4, 2, true>(bc, nb, P, A, s); break;
-            case 10: launch2_split<16, 4, 4, false>(bc, nb, P, A, s); break;
-            default: launch2_split<32, 2, 4, false>(bc, nb, P, A, s); break;
+            default: launch2_fg<32, 4, false, 8, true>(f_on, g_on, bc, nb, P, A, s); break;
             }
         }
     } else {
@@ -413,10 +403,6 @@ inline int fused_setup(FusedConfig& fc, int lat, const int* model, const Params&
         const TileCfg t = lat == MPLB_D2Q9 ? CFG2[c] : CFG3[c];
         if (t.tma) {
             fc.geom[c] = tma3_fits(A, any, t.tx, t.ty) ? resident_geometry(A, t.tx, t.ty, t.minb) : Geom{0, 0, 0, 0};
-        } else if (t.fg) {
-            // flow and liTempMRT heat, both updated
-            const bool fits = P.f_update && P.g_update && model[0] != MPLB_NO_MODEL && model[1] == MPLB_LITEMPMRT;
-            fc.geom[c] = fits ? fused_geometry(lat, A, t.tx, t.ty) : Geom{0, 0, 0, 0};
         } else {
             fc.geom[c] = fused_geometry(lat, A, t.tx, t.ty);
         }

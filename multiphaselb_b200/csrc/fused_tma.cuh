@@ -205,19 +205,18 @@ __global__ void __launch_bounds__(TX * TY, MINB)
     bool failed = false;
     for (int p = pfirst; p <= plast; p++) {
         const int j = p - pfirst, s = j % G::NSTAGE;
-        if (!mbar_wait_bounded(&bar[s], (parity >> s) & 1u, TMA_WAIT_LIMIT)) {
-            failed = true;
-            break;
+        const bool landed = mbar_wait_bounded(&bar[s], (parity >> s) & 1u, TMA_WAIT_LIMIT);
+        if (landed) {
+            parity ^= 1u << s;
+            pending &= ~(1u << s);
         }
-        parity ^= 1u << s;
-        pending &= ~(1u << s);
         // psi of plane p: ring slots, then the own slot (whose populations
         // stay in registers).  Population k of ext slot (ex, ey) sits at
         // box k, row ey, column ex + 1 - c_kx; T at box 15, column ex + 1.
         const double* sb = box_ptr(s, 0);
         constexpr int BP = G::BOX_PITCH / 8;
         double(*psi_p)[EX] = s_psi[(p + G::NPSI) % G::NPSI];
-        for (int r = tid; r < NRING; r += NT) {
+        for (int r = tid; landed && r < NRING; r += NT) {
             int ex, ey;
             ring_slot(r, TX, TY, ex, ey);
             const double* sl = sb + ey * G::BX + ex + 1;
@@ -228,7 +227,7 @@ __global__ void __launch_bounds__(TX * TY, MINB)
             });
             psi_p[ey][ex] = potential(P, rho, sl[15 * BP]);
         }
-        {
+        if (landed) {
             const int ex = tx + 1, ey = ty + 1;
             const double* sl = sb + ey * G::BX + ex + 1;
             double rho = 0;
@@ -242,7 +241,11 @@ __global__ void __launch_bounds__(TX * TY, MINB)
             rrc = rcp_rn(rho);
             psi_p[ey][ex] = potential(P, rho, Tcur);
         }
-        __syncthreads();
+        // one decision for the whole block: a wait that ran out in any thread ends the kernel
+        if (__syncthreads_or(!landed)) {
+            failed = true;
+            break;
+        }
         // stage s has been read: request plane p + NSTAGE into it
         if (p + G::NSTAGE <= plast) {
             fill(p + G::NSTAGE, s);

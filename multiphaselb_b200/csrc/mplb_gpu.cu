@@ -1051,11 +1051,18 @@ int mplb_gpu_create(const mplb_mesh_desc* mesh, const mplb_eos_desc* eos, const 
         if (h->model[fi] == MPLB_NO_MODEL) continue;
         if ((rc = dalloc(h, &h->pdf[fi][0], nq)) || (rc = dalloc(h, &h->pdf[fi][1], nq))) return bail(rc);
     }
+    // Create-time tables go to the device on the handle's own stream, which
+    // does not wait for the legacy default stream: a synchronous cudaMemcpy
+    // from pageable memory may return before its DMA lands, and a kernel on a
+    // non-blocking stream could then read the old contents.  Stream order plus
+    // one synchronisation before create returns.
+    auto to_dev = [&](void* dst, const void* src, size_t bytes) {
+        return cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, h->stream) == cudaSuccess;
+    };
     for (int fi = 0; fi < 2; fi++) {
         if (tabs[fi].empty()) continue;
         if ((rc = dalloc(h, &h->bctab[fi], tabs[fi].size()))) return bail(rc);
-        if (cudaMemcpy(h->bctab[fi], tabs[fi].data(), tabs[fi].size() * sizeof(double), cudaMemcpyHostToDevice) !=
-            cudaSuccess)
+        if (!to_dev(h->bctab[fi], tabs[fi].data(), tabs[fi].size() * sizeof(double)))
             return bail(fail(MPLB_E_CUDA, "copying the boundary tables failed"));
     }
     {
@@ -1068,15 +1075,16 @@ int mplb_gpu_create(const mplb_mesh_desc* mesh, const mplb_eos_desc* eos, const 
                 nbs[(size_t)k * h->n + i] = s;
                 if (s == -1) onb[i] = 1;  // readLatticeMesh.c:171-203
             }
-        if (cudaMemcpy(h->nb, nbs.data(), nq * sizeof(int32_t), cudaMemcpyHostToDevice) != cudaSuccess ||
-            cudaMemcpy(h->onb, onb.data(), h->n, cudaMemcpyHostToDevice) != cudaSuccess ||
-            (tot && cudaMemcpy(h->pnodes, mesh->patch_nodes, tot * sizeof(uint32_t), cudaMemcpyHostToDevice) != cudaSuccess))
+        if (!to_dev(h->nb, nbs.data(), nq * sizeof(int32_t)) || !to_dev(h->onb, onb.data(), h->n) ||
+            (tot && !to_dev(h->pnodes, mesh->patch_nodes, tot * sizeof(uint32_t))))
             return bail(fail(MPLB_E_CUDA, "copying the mesh failed"));
         std::vector<PatchDev> both(h->fpatch[0]);
         both.insert(both.end(), h->fpatch[1].begin(), h->fpatch[1].end());
-        if (!both.empty() &&
-            cudaMemcpy(h->dpatches, both.data(), both.size() * sizeof(PatchDev), cudaMemcpyHostToDevice) != cudaSuccess)
+        if (!both.empty() && !to_dev(h->dpatches, both.data(), both.size() * sizeof(PatchDev)))
             return bail(fail(MPLB_E_CUDA, "copying the patches failed"));
+        // the host vectors above go out of scope here
+        if (cudaStreamSynchronize(h->stream) != cudaSuccess)
+            return bail(fail(MPLB_E_CUDA, "copying the mesh failed"));
     }
     // Execution path.
     std::string fwhy;

@@ -5,7 +5,8 @@
 WORKLOAD: column (thermal VdW column, D2Q9 128x512), column_big (the same
 column at 512x2048, larger than L2, for ncu captures), bubble2d (D2Q9
 256x256), bubble2d_big (D2Q9 1024x1024), bubble3d (D3Q15 192^3),
-bubble3d_small (D3Q15 96^3, for full ncu captures).
+bubble3d_small (D3Q15 96^3, for full ncu captures), bubble3d_mid (D3Q15
+128^3, 0.7 GB on the device: ncu captures where half the tiles are inner).
 """
 import argparse
 import sys
@@ -19,6 +20,7 @@ WORKLOADS = {
     "bubble2d_big": lambda: cases.bubble_case(abi.D2Q9, 1024, 160.0, 5.0, 0.8),
     "bubble3d": lambda: cases.bubble_case(abi.D3Q15, 192, 48.0, 5.0, 0.75),
     "bubble3d_small": lambda: cases.bubble_case(abi.D3Q15, 96, 24.0, 5.0, 0.75),
+    "bubble3d_mid": lambda: cases.bubble_case(abi.D3Q15, 128, 32.0, 5.0, 0.75),
 }
 
 
