@@ -305,6 +305,20 @@ enum {
 int mplb_gpu_copy_nodes(mplb_gpu_t* dst, uint32_t dst_start, mplb_gpu_t* src, uint32_t src_start,
                         uint32_t count, int32_t fields);
 
+/* Copy the fused-path state of nodes [src_start, src_start + count) of src
+ * to [dst_start, dst_start + count) of dst: the post-collision populations
+ * of every updated field (the input of the next fused step), and T and U of
+ * the last step.  No counterpart in the reference; it is the halo exchange
+ * of slabs run on the fused path (the reference's sendPdfField /
+ * recvPdfField, src/lbEquation/general/sendPdfField.c:7-102 and
+ * recvPdfField.c:7-54, move the post-stream PDFs of ghost nodes instead,
+ * inside its operator sequence).  Both handles must be on the fused FP64
+ * path with the same lattice and field options; a handle still in the
+ * reference's state (after initialize) first takes the loop's first
+ * collision, as mplb_gpu_step does.  Device to device, ordered on the
+ * handles' streams as mplb_gpu_copy_nodes. */
+int mplb_gpu_copy_state(mplb_gpu_t* dst, uint32_t dst_start, mplb_gpu_t* src, uint32_t src_start, uint32_t count);
+
 /* Several ranks' lattices driven from one process (one handle per rank, on
  * one GPU or several), each holding its owned nodes and its ghost nodes (no
  * neighbours, on no patch: the layout of the reference's partitioned meshes).

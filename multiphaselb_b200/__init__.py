@@ -70,6 +70,7 @@ def load_library(path=LIB_PATH):
         "mplb_gpu_mass_energy": ([H, D, D], C.c_int),
         "mplb_gpu_sync": ([H], C.c_int),
         "mplb_gpu_copy_nodes": ([H, C.c_uint32, H, C.c_uint32, C.c_uint32, C.c_int32], C.c_int),
+        "mplb_gpu_copy_state": ([H, C.c_uint32, H, C.c_uint32, C.c_uint32], C.c_int),
         "mplb_ranks_initialize": ([C.POINTER(H), C.c_uint32, C.POINTER(abi.GhostRun), C.c_uint32], C.c_int),
         "mplb_ranks_step": ([C.POINTER(H), C.c_uint32, C.POINTER(abi.GhostRun), C.c_uint32, C.c_uint32], C.c_int),
         "mplb_gpu_snapshot": ([H, C.c_int32], C.c_int),
@@ -253,6 +254,13 @@ class Lattice:
         for name in fields:
             mask |= abi.NODES[name]
         self._check(self.lib.mplb_gpu_copy_nodes(self.h, dst_start, src.h, src_start, count, mask))
+
+    def copy_state(self, src, dst_start, src_start, count):
+        """Copy the fused-path state (post-collision populations, T and U of the
+        last step) of nodes [src_start, src_start + count) of `src` into nodes
+        [dst_start, ...) of this Lattice, device to device: the halo exchange
+        of slabs run on the fused path."""
+        self._check(self.lib.mplb_gpu_copy_state(self.h, dst_start, src.h, src_start, count))
 
     def set_rho0(self, r):
         self._check(self.lib.mplb_gpu_set_rho0(self.h, r))

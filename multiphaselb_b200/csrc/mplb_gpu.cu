@@ -826,6 +826,25 @@ int prologue32(mplb_gpu* h) {
 }
 
 // Bring the buffers back to the reference's state (after the last step).
+// Enter the fused path's state (post-collision populations) from the
+// reference's: the first collision of the loop (multiPhasePP.c:163,194).
+int enter_fused(mplb_gpu* h) {
+    if (h->path != MPLB_PATH_FUSED || h->precision != MPLB_FP64 || h->fstate == 1) return 0;
+    RET(DISPATCH(h, op_collision, h, 0));
+    RET(DISPATCH(h, op_collision, h, 1));
+    h->fstate = 1;
+    return 0;
+}
+
+// One strided node copy: `rows` component rows of a [component][node] array.
+struct NodeCopy {
+    double* d;
+    const double* s;
+    int rows;
+};
+int copy_node_rows(mplb_gpu* dst, uint32_t dst_start, mplb_gpu* src, uint32_t src_start, uint32_t count,
+                   const NodeCopy* parts, int np);
+
 int materialize(mplb_gpu* h) {
     if (h->fstate == 0) return 0;
     if (h->precision == MPLB_FP32_DEV) RET(fused32_step(h, true));
@@ -1213,12 +1232,7 @@ int mplb_gpu_step(mplb_gpu_t* h, uint32_t nsteps) {
         return 0;
     }
     if (h->path == MPLB_PATH_FUSED) {
-        if (h->fstate == 0) {
-            // prologue: the first collision of the loop, on the reference state
-            RET(DISPATCH(h, op_collision, h, 0));
-            RET(DISPATCH(h, op_collision, h, 1));
-            h->fstate = 1;
-        }
+        RET(enter_fused(h));  // prologue: the first collision of the loop, on the reference state
         for (uint32_t s = 0; s < nsteps; s++) RET(fused_step(h, false));
         h->current += nsteps;
         return 0;
@@ -1702,11 +1716,10 @@ int mplb_gpu_copy_nodes(mplb_gpu_t* dst, uint32_t dst_start, mplb_gpu_t* src, ui
         RET(materialize(dst));
     }
     // every field is [component][node] on the device: one strided copy each
-    struct Part { double* d; const double* s; int rows; };
-    Part parts[8];
+    NodeCopy parts[8];
     int np = 0;
     auto add = [&](int32_t bit, double* d, const double* s, int rows) {
-        if (fields & bit) parts[np++] = Part{d, s, rows};
+        if (fields & bit) parts[np++] = NodeCopy{d, s, rows};
     };
     add(MPLB_NODES_RHO, dst->rho, src->rho, 1);
     add(MPLB_NODES_U, dst->U, src->U, 3);
@@ -1716,6 +1729,50 @@ int mplb_gpu_copy_nodes(mplb_gpu_t* dst, uint32_t dst_start, mplb_gpu_t* src, ui
     add(MPLB_NODES_S, dst->S, src->S, 1);
     if (fields & MPLB_NODES_F) add(MPLB_NODES_F, dst->F(), src->F(), dst->Q);
     if (fields & MPLB_NODES_G) add(MPLB_NODES_G, dst->G(), src->G(), dst->Q);
+    return copy_node_rows(dst, dst_start, src, src_start, count, parts, np);
+}
+
+int mplb_gpu_copy_state(mplb_gpu_t* dst, uint32_t dst_start, mplb_gpu_t* src, uint32_t src_start, uint32_t count) {
+    if (!dst || !src) return fail(MPLB_E_ARG, "NULL handle");
+    if (dst->path != MPLB_PATH_FUSED || src->path != MPLB_PATH_FUSED || dst->precision != MPLB_FP64 ||
+        src->precision != MPLB_FP64)
+        return fail(MPLB_E_UNSUPPORTED, "state copies need two handles on the fused FP64 path");
+    if (dst->lat != src->lat || dst->model[0] != src->model[0] || dst->model[1] != src->model[1] ||
+        dst->P.f_update != src->P.f_update || dst->P.g_update != src->P.g_update)
+        return fail(MPLB_E_ARG, "the lattices or field options differ");
+    if ((uint64_t)dst_start + count > dst->n || (uint64_t)src_start + count > src->n)
+        return fail(MPLB_E_ARG, "node range out of bounds");
+    if (dst == src && (uint64_t)dst_start < (uint64_t)src_start + count &&
+        (uint64_t)src_start < (uint64_t)dst_start + count)
+        return fail(MPLB_E_ARG, "overlapping ranges on one handle");
+    if (count == 0) return 0;
+    for (mplb_gpu* h : {src, dst}) {
+        DeviceGuard guard(h->dev);
+        RET(enter_fused(h));
+    }
+    // the input buffers of the next fused step: post-collision populations of
+    // every updated field, T and U of the last step
+    NodeCopy parts[4];
+    int np = 0;
+    for (int fi = 0; fi < 2; fi++)
+        if (dst->model[fi] != MPLB_NO_MODEL && (fi == 0 ? dst->P.f_update : dst->P.g_update))
+            parts[np++] = NodeCopy{dst->pdf[fi][dst->cur[fi]], src->pdf[fi][src->cur[fi]], dst->Q};
+    parts[np++] = NodeCopy{dst->T, src->T, 1};
+    parts[np++] = NodeCopy{dst->U, src->U, 3};
+    return copy_node_rows(dst, dst_start, src, src_start, count, parts, np);
+}
+
+}  // extern "C"
+
+namespace {
+
+// Rows of [component][node] device arrays, `count` nodes from src_start of
+// src to dst_start of dst: one strided copy per part, queued on the source
+// handle's stream after the destination's queued work, and the destination's
+// stream made to wait for it (nothing blocks the host; between GPUs the copy
+// goes peer to peer, peer access enabled on first use).
+int copy_node_rows(mplb_gpu* dst, uint32_t dst_start, mplb_gpu* src, uint32_t src_start, uint32_t count,
+                   const NodeCopy* parts, int np) {
     const bool same_queue = dst->dev == src->dev && dst->stream == src->stream;
     struct Events {
         cudaEvent_t dst_ready = nullptr, copied = nullptr;
@@ -1743,7 +1800,7 @@ int mplb_gpu_copy_nodes(mplb_gpu_t* dst, uint32_t dst_start, mplb_gpu_t* src, ui
     const size_t dpitch = (size_t)dst->n * sizeof(double), spitch = (size_t)src->n * sizeof(double);
     const size_t width = (size_t)count * sizeof(double);
     for (int i = 0; i < np; i++) {
-        const Part& p = parts[i];
+        const NodeCopy& p = parts[i];
         CK(cudaMemcpy2DAsync(p.d + dst_start, dpitch, p.s + src_start, spitch, width, p.rows, cudaMemcpyDefault,
                              src->stream));
     }
@@ -1755,10 +1812,6 @@ int mplb_gpu_copy_nodes(mplb_gpu_t* dst, uint32_t dst_start, mplb_gpu_t* src, ui
     }
     return 0;
 }
-
-}  // extern "C"
-
-namespace {
 
 // The ranks of one process: every handle must hold the same lattice and
 // field options, and every run must name handles of the list.

@@ -581,3 +581,149 @@ class LatticeHandle:
 
     def close(self):
         self.lat.close()
+
+
+class FusedSlabRun:
+    """A box lattice cut into slabs along its slowest axis (y in 2D, z in 3D),
+    every slab a handle on the fused FP64 path: one kernel per slab and step,
+    and before each step a halo exchange device to device.
+
+    Slab r owns planes [a_r, b_r) and holds HALO more planes on each side
+    that faces another slab (wrapping on a periodic axis; none on a walled
+    face of the box).  A fused step needs, for a node, its pull sources one
+    plane away and, for the psi / 1/rho / T / U ring of its tile, the pull
+    sources of the ring one plane further: so the halo holds two planes of
+    the fused state (post-collision populations, T and U of the last step),
+    copied from the neighbouring slabs' owned planes before every step
+    (mplb_gpu_copy_state, two copies per cut and direction).  The kernel also
+    updates the halo planes; what it writes there is never read before the
+    next exchange overwrites it.  The owned planes are then bit-identical to
+    the single domain (tests/test_gpu_slabs.py).  This is the multi-rank form
+    of the fused path: the reference's exchange inside its operator sequence
+    (sendPdfField.c, recvPdfField.c, multiPhasePP.c:163-240) becomes one
+    exchange of the fused state per step, which for walls that do not cross a
+    cut gives the single domain's result (for a fixedT wall across a cut the
+    reference's multi-rank run deviates from its single domain; the operator
+    runner RankRun reproduces that deviation, this one does not take such
+    cases: the cut is always across the slab axis, walls of that axis lie in
+    the first and last slab).
+    """
+
+    HALO = 2
+
+    def __init__(self, case: Case, nslabs: int, device: int = -1, stream=None, tile_config: int = 0):
+        from . import Lattice, PATH_FUSED
+        self.case, self.nslabs = case, nslabs
+        self.nplanes, self.plane, self.periodic = _box_geometry(case)
+        self.slabs = fused_slab_parts(case, nslabs, self.HALO)
+        for s in self.slabs:
+            s["lat"] = Lattice(s["case"], path=PATH_FUSED, device=device, stream=stream, tile_config=tile_config)
+
+    def exchanges(self):
+        """(destination slab, destination node, source slab, source node, nodes)
+        of every halo copy of a step."""
+        return halo_copies(self.slabs, self.nslabs, self.plane, self.HALO)
+
+    def initialize(self):
+        for s in self.slabs:
+            s["lat"].upload_case()
+            s["lat"].initialize()
+
+    def exchange(self):
+        """Halo planes of every slab from its neighbours' owned planes."""
+        for d, dn, src, sn, cnt in self.exchanges():
+            self.slabs[d]["lat"].copy_state(self.slabs[src]["lat"], dn, sn, cnt)
+
+    def step(self, n=1):
+        for _ in range(n):
+            self.exchange()
+            for s in self.slabs:
+                s["lat"].step(1)
+
+    def sync(self):
+        for s in self.slabs:
+            s["lat"].sync()
+
+    def gather(self):
+        """The reference state of the whole box: every slab's owned planes."""
+        out = {}
+        for s in self.slabs:
+            d = s["lat"].download()
+            for k, v in d.items():
+                out.setdefault(k, []).append(v[s["own0"]:s["own0"] + s["nown"]])
+        return {k: np.concatenate(v, axis=0) for k, v in out.items()}
+
+    def close(self):
+        for s in self.slabs:
+            s["lat"].close()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+
+def fused_slab_parts(case: Case, nslabs: int, halo: int):
+    """The slabs of FusedSlabRun: per slab its owned planes [a, b), its local
+    planes [lo, hi) (global planes mod the extent), the global node of every
+    local node (gidx), the first owned local node and the owned node count,
+    and its local box case (halo faces carry no boundary condition)."""
+    from .cases import box_mesh
+    if nslabs < 2:
+        raise ValueError("at least two slabs")
+    nplanes, plane, periodic = _box_geometry(case)
+    if nplanes < nslabs * (halo + 1):
+        raise ValueError(f"{nplanes} planes cannot give {nslabs} slabs of at least {halo + 1} planes")
+    bounds = [round(r * nplanes / nslabs) for r in range(nslabs + 1)]
+    axis_name = "Z" if case.lattice == abi.D3Q15 else "Y"
+    names_g = list(case.patch_names)
+    parts = []
+    for r in range(nslabs):
+        a, b = bounds[r], bounds[r + 1]
+        lo = a - halo if (periodic or r > 0) else a
+        hi = b + halo if (periodic or r < nslabs - 1) else b
+        gplanes = np.arange(lo, hi) % nplanes
+        gidx = (gplanes[:, None] * plane + np.arange(plane)[None, :]).ravel()
+        dims = tuple(case.dims[:-1]) + (hi - lo,)
+        per = tuple(case.periodic[:-1]) + (False,)
+        nb, points, patches, names = box_mesh(case.lattice, dims, per)
+        # patch types by face name: the box's own faces keep the case's
+        # conditions; a slab face on the cut axis is a wall only where the box
+        # has one, else it carries a halo and no condition (periodic)
+        fields = {}
+        for key, fd in (("f", case.f), ("g", case.g)):
+            if fd is None:
+                fields[key] = None
+                continue
+            bt, bv = [], []
+            for nm in names:
+                cut_face = nm[0] == axis_name and ((nm[1] == "0" and lo != 0) or
+                                                   (nm[1] == "1" and hi != nplanes) or periodic)
+                if cut_face or nm not in names_g:
+                    bt.append(abi.BC_PERIODIC)
+                    bv.append((0.0, 0.0, 0.0))
+                else:
+                    j = names_g.index(nm)
+                    bt.append(int(fd["bc_type"][j]))
+                    bv.append(tuple(np.asarray(fd["bc_value"], dtype=np.float64).reshape(-1, 3)[j]))
+            fields[key] = dict(fd, bc_type=bt, bc_value=np.array(bv, dtype=np.float64).reshape(-1, 3))
+        lc = Case(f"{case.name}_slab{r}", case.lattice, dims, per, nb, points, patches, names, case.eos,
+                  fields["f"], fields["g"], np.asarray(case.rho)[gidx], np.asarray(case.U)[gidx],
+                  np.asarray(case.T)[gidx], meta=dict(case.meta, box=True))
+        parts.append(dict(case=lc, a=a, b=b, lo=lo, hi=hi, gidx=gidx, own0=(a - lo) * plane, nown=(b - a) * plane))
+    return parts
+
+
+def halo_copies(parts, nslabs: int, plane: int, halo: int):
+    """Every halo copy of a FusedSlabRun step: (destination slab, first
+    destination node, source slab, first source node, node count)."""
+    out = []
+    for r, s in enumerate(parts):
+        if s["a"] != s["lo"]:   # halo below <- the top owned planes of the slab below
+            nbr = parts[(r - 1) % nslabs]
+            out.append((r, 0, (r - 1) % nslabs, nbr["own0"] + nbr["nown"] - halo * plane, halo * plane))
+        if s["b"] != s["hi"]:   # halo above <- the bottom owned planes of the slab above
+            nbr = parts[(r + 1) % nslabs]
+            out.append((r, s["own0"] + s["nown"], (r + 1) % nslabs, nbr["own0"], halo * plane))
+    return out

@@ -87,3 +87,53 @@ def test_device_partition_matches_checker_partition(gpu_lib, name):
         outs.append(run.gather())
         run.close()
     assert_same(outs[1], outs[0], fields=fields_of(case), ctx=f"{name} partitioned, device vs checker")
+
+
+# ---------------------------------------------------------------- fused slabs
+def bubble_d3q15_z12():
+    from multiphaselb_b200 import cases
+    return cases.perturbed(cases.bubble_case(abi.D3Q15, 10, 3.0, 2.0, 0.75, dims=(10, 8, 12)), du=1e-3)
+
+
+FUSED_SLAB_CASES = [("column_d2q9", 2), ("column_d2q9", 4), ("bubble_d2q9", 3), ("st_d2q9", 3),
+                    ("walls_d3q15", 2), ("bubble_d3q15_z12", 4)]
+
+
+def fused_case(name):
+    return bubble_d3q15_z12() if name == "bubble_d3q15_z12" else small_cases()[name]
+
+
+@pytest.mark.parametrize("name,ranks", FUSED_SLAB_CASES)
+def test_fused_slabs_match_oracle(gpu_lib, name, ranks):
+    """Slabs on the fused path, the halo exchanged as fused state
+    (mplb_gpu_copy_state), against the single-domain oracle run: the owned
+    planes bit for bit after 12 steps, and after 12 more with the reference
+    state rebuilt in between."""
+    from tests.helpers import run_checker
+    case = fused_case(name)
+    fields = [f for f in fields_of(case) if f != "S" or case.g is not None]
+    with slabs.FusedSlabRun(case, ranks) as run:
+        assert all(s["lat"].info()["path"] == abi.PATH_FUSED for s in run.slabs)
+        run.initialize()
+        run.step(12)
+        assert_same(run.gather(), run_checker("port", case, 12), fields=fields, ctx=f"{name} in {ranks} fused slabs @12")
+        run.step(12)
+        assert_same(run.gather(), run_checker("port", case, 24), fields=fields, ctx=f"{name} in {ranks} fused slabs @24")
+
+
+def test_copy_state_refuses(gpu_lib):
+    """State copies need two fused FP64 handles of the same lattice and options."""
+    a_case = small_cases()["column_d2q9"]
+    with Lattice(a_case, path=abi.PATH_FUSED) as a, Lattice(a_case, path=abi.PATH_OPERATORS) as b, \
+            Lattice(small_cases()["bubble_d2q9"], path=abi.PATH_FUSED) as c:
+        for lat in (a, b, c):
+            lat.upload_case()
+            lat.initialize()
+        with pytest.raises(MplbError, match="fused FP64 path"):
+            a.copy_state(b, 0, 0, 10)
+        with pytest.raises(MplbError, match="differ"):
+            a.copy_state(c, 0, 0, 10)
+        with pytest.raises(MplbError, match="out of bounds"):
+            a.copy_state(a, 0, a_case.n - 5, 10)
+        with pytest.raises(MplbError, match="overlapping"):
+            a.copy_state(a, 0, 5, 10)

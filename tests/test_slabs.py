@@ -177,3 +177,37 @@ def test_one_process_per_slab_gloo(tmp_path, name, world):
         got = pickle.load(fh)
     case = small_cases()[name]
     assert_same(got, run_checker("port", case, 6), fields=fields_of(case), ctx=f"{name} on {world} gloo ranks")
+
+
+@pytest.mark.parametrize("R", [2, 3, 4])
+@pytest.mark.parametrize("name", ["column_d2q9", "bubble_d2q9", "walls_d3q15"])
+def test_fused_slab_plan(name, R):
+    """FusedSlabRun's plan: the owned planes cover the box once in order,
+    every halo copy fills halo nodes from owned nodes of the same global
+    nodes, each local case is a box whose halo faces carry no condition, and
+    its fields are the box's fields of its nodes."""
+    case = small_cases()[name]
+    nplanes, plane, periodic = slabs._box_geometry(case)
+    if nplanes < 3 * R:
+        with pytest.raises(ValueError, match="cannot give"):
+            slabs.fused_slab_parts(case, R, 2)
+        return
+    parts = slabs.fused_slab_parts(case, R, 2)
+    own = np.concatenate([p["gidx"][p["own0"]:p["own0"] + p["nown"]] for p in parts])
+    assert np.array_equal(own, np.arange(case.n))
+    copies = slabs.halo_copies(parts, R, plane, 2)
+    filled = [set() for _ in parts]
+    for d, dn, s, sn, c in copies:
+        assert np.array_equal(parts[d]["gidx"][dn:dn + c], parts[s]["gidx"][sn:sn + c])
+        assert parts[s]["own0"] <= sn and sn + c <= parts[s]["own0"] + parts[s]["nown"]
+        filled[d].update(range(dn, dn + c))
+    for p, f in zip(parts, filled):
+        halo = set(range(p["case"].n)) - set(range(p["own0"], p["own0"] + p["nown"]))
+        assert f == halo
+        lc = p["case"]
+        assert np.array_equal(lc.rho, np.asarray(case.rho)[p["gidx"]])
+        for nm, t in zip(lc.patch_names, lc.f["bc_type"]):
+            wall = nm in case.patch_names and not (
+                nm[0] in "YZ" and ((nm[1] == "0" and p["lo"] != 0) or (nm[1] == "1" and p["hi"] != nplanes) or periodic))
+            if not wall:
+                assert t == abi.BC_PERIODIC
