@@ -39,8 +39,9 @@
 extern "C" {
 #endif
 
-#define MPLB_ABI_VERSION 4  /* 2: mplb_field_desc.alpha_1/alpha_2, mplb_opts.rank; 3: mplb_gpu_copy_nodes;
-                               4: mplb_info.tile_ms[16], MPLB_E_TIMEOUT */
+#define MPLB_ABI_VERSION 5  /* 2: mplb_field_desc.alpha_1/alpha_2, mplb_opts.rank; 3: mplb_gpu_copy_nodes;
+                               4: mplb_info.tile_ms[16], MPLB_E_TIMEOUT;
+                               5: mplb_batch_filter, mplb_batch_average */
 #define MPLB_MAX_Q 15
 #define MPLB_MAX_PATCHES 64
 
@@ -411,6 +412,33 @@ int mplb_batch_step(mplb_batch_t* b, uint32_t nsteps);
  * (may be NULL); *n_converged: lattices that met tol. */
 int mplb_batch_run(mplb_batch_t* b, uint32_t max_steps, uint32_t* steps_out, double* rate_out,
                    uint32_t* n_converged);
+
+/* Time-averaging filter (off until set).  A static lattice settles to a
+ * fixed point of the time step; near it the state is that fixed point plus
+ * decaying oscillations, the slowest being the acoustic modes of the box,
+ * whose damping (viscosity x (2 pi / L)^2) makes large lattices slow to
+ * settle.  A filter window replaces lattice i's populations by their mean
+ * over its last window[i] steps: the fixed point is unchanged (the mean is
+ * linear in the state and every state of an equilibrium is the same), an
+ * oscillation of period P shrinks by about |sin(pi window / P)| / (pi window
+ * / P) -- nearly to zero for window = P, where plain stepping would take
+ * many periods.  window[i] = 0 leaves lattice i unfiltered; window = NULL
+ * turns the filter off.  mplb_batch_run then runs a window once `first`
+ * steps are done and again `every` steps after the end of each window
+ * (every = 0: only on request, mplb_batch_average), at the end of a check
+ * interval, followed by a check of its own (steps_out counts window steps).
+ * A window is M steps, M the smallest even number above the longest window
+ * among the lattices still running: lattice i averages the states after
+ * its steps M-1-window[i] .. M-2, and the window's last step runs from
+ * that mean (so the populations the reference state is emitted from and
+ * those the next step reads are both filtered).  Sums are FP64 (exact for
+ * FP32 states), the mean is rounded once.  Device memory: 9 n doubles per
+ * filtered lattice. */
+#define MPLB_BATCH_MAX_WINDOW 1048576u
+int mplb_batch_filter(mplb_batch_t* b, const uint32_t* window, uint32_t first, uint32_t every);
+/* One filter window on every lattice now; *steps_out = its length in steps
+ * (0 when no lattice is filtered). */
+int mplb_batch_average(mplb_batch_t* b, uint32_t* steps_out);
 
 /* ------------------------------------------------------------------------
  * Learned warm start.  No counterpart in the reference, whose initial fields

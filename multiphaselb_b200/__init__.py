@@ -89,6 +89,8 @@ def load_library(path=LIB_PATH):
         "mplb_batch_info_get": ([H, C.POINTER(abi.BatchInfo)], C.c_int),
         "mplb_batch_step": ([H, C.c_uint32], C.c_int),
         "mplb_batch_run": ([H, C.c_uint32, C.POINTER(C.c_uint32), D, C.POINTER(C.c_uint32)], C.c_int),
+        "mplb_batch_filter": ([H, C.POINTER(C.c_uint32), C.c_uint32, C.c_uint32], C.c_int),
+        "mplb_batch_average": ([H, C.POINTER(C.c_uint32)], C.c_int),
     }
     for name, (args, res) in sig.items():
         fn = getattr(lib, name)
@@ -374,3 +376,22 @@ class Batch:
         conv = C.c_uint32()
         self._check(self.lib.mplb_batch_run(self.h, max_steps, abi.uptr(steps), abi.dptr(rate), C.byref(conv)))
         return steps, rate, conv.value
+
+    def filter(self, window, first=0, every=0):
+        """Time-averaging filter: lattice i's state replaced by its mean over
+        its last window[i] steps (0: not filtered), in run() once `first`
+        steps are done and `every` steps after each window (every = 0: only
+        through average()).  window=None turns the filter off."""
+        if window is None:
+            self._check(self.lib.mplb_batch_filter(self.h, None, 0, 0))
+            return
+        w = np.ascontiguousarray(window, dtype=np.uint32)
+        if w.shape != (len(self.lattices),):
+            raise ValueError("one window per lattice")
+        self._check(self.lib.mplb_batch_filter(self.h, abi.uptr(w), first, every))
+
+    def average(self):
+        """One filter window on every lattice now; returns its length in steps."""
+        s = C.c_uint32()
+        self._check(self.lib.mplb_batch_average(self.h, C.byref(s)))
+        return s.value

@@ -21,6 +21,7 @@ OK, E_ARG, E_UNSUPPORTED, E_CUDA, E_STATE, E_NONFINITE, E_IO, E_TIMEOUT = 0, -1,
 FMT_ASCII_RAW, FMT_BINARY_RAW, FMT_PVTU, FMT_ENSIGHT = 0, 1, 2, 3
 FORMATS = {"asciiRaw": FMT_ASCII_RAW, "binaryRaw": FMT_BINARY_RAW, "pvtu": FMT_PVTU, "ensight": FMT_ENSIGHT}
 SNAP_PRESSURE, SNAP_PDFS = 1, 2
+BATCH_MAX_WINDOW = 1048576  # MPLB_BATCH_MAX_WINDOW
 # mplb_gpu_copy_nodes field bits, by the field names of download()
 NODES = {"rho": 1, "U": 2, "T": 4, "Fi": 8, "Ft": 16, "S": 32, "f": 64, "g": 128}
 

@@ -453,6 +453,44 @@ __global__ void __launch_bounds__(TX * TY)
     }
 }
 
+// Time-averaging filter.  A window is M steps; the launch after step s
+// (0 <= s < last = M - 1) adds the state that step produced, and one more
+// launch (finish = 1) before step `last` replaces the state that step reads
+// by the mean; step `last` then runs from the mean, so both buffers hold
+// filtered states (the one the reference state is emitted from, and the
+// one the next step reads).  Lattice i, with a window of N = win[i] states
+// (0: not filtered), sums the states after steps last-N .. last-1 into its
+// FP64 accumulator (the first of them assigns).  An FP64 sum of at most
+// 2^29 FP32 values is exact, so the mean is rounded once.  `parity` selects
+// the buffer the next step reads, as in k_batch32_check.
+template <int TX, int TY>
+__global__ void __launch_bounds__(TX * TY)
+    k_batch32_average(const FusedArgs32* __restrict__ As, const int2* __restrict__ tiles,
+                      const int* __restrict__ ntiles, int parity, double* const* __restrict__ acc,
+                      const uint32_t* __restrict__ win, uint32_t s, uint32_t last, int finish) {
+    const int nt = *ntiles;
+    for (int t = blockIdx.x; t < nt; t += gridDim.x) {
+        const int2 w = tiles[t];
+        const uint32_t N = win[w.x];
+        if (N == 0 || N > last || (!finish && s + N < last)) continue;  // block-uniform
+        const FusedArgs32& A = As[2 * w.x + parity];
+        if (A.tiles_x <= 0 || w.y < 0 || w.y >= A.tiles_x * A.tiles_y) continue;
+        const int bx = w.y % A.tiles_x, by = w.y / A.tiles_x;
+        const int x = bx * TX + (int)threadIdx.x % TX, y = by * TY + (int)threadIdx.x / TX;
+        if (x >= A.nx || y >= A.ny) continue;
+        const uint32_t id = (uint32_t)x + (uint32_t)A.nx * (uint32_t)y;
+        double* a = acc[w.x];
+        float* f = const_cast<float*>(A.fin);
+#pragma unroll
+        for (int k = 0; k < 9; k++) {
+            const size_t i = (size_t)k * A.n + id;
+            if (finish) f[i] = (float)(a[i] / (double)N);
+            else if (s + N == last) a[i] = (double)f[i];
+            else a[i] += (double)f[i];
+        }
+    }
+}
+
 // Lone lattice: total momentum of the current FP32 buffer, and its reset.
 template <class L>
 __global__ void k_mom_sum32(uint32_t n, const float* __restrict__ f, long long* __restrict__ J) {
@@ -535,6 +573,18 @@ cudaError_t mplb_batch32_check(int cfg, const Params* dP, const FusedArgs32* dA,
     case 1: k_batch32_check<32, 4><<<grid, 128, 0, s>>>(dP, dA, tiles, ntiles, parity, snaps, dmax, jsum); break;
     case 2: k_batch32_check<16, 8><<<grid, 128, 0, s>>>(dP, dA, tiles, ntiles, parity, snaps, dmax, jsum); break;
     default: k_batch32_check<64, 4><<<grid, 256, 0, s>>>(dP, dA, tiles, ntiles, parity, snaps, dmax, jsum); break;
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t mplb_batch32_average(int cfg, const FusedArgs32* dA, const int2* tiles, const int* ntiles, int parity,
+                                 int grid, double* const* acc, const uint32_t* win, uint32_t s, uint32_t last,
+                                 int finish, cudaStream_t st) {
+    switch (cfg) {
+    case 0: k_batch32_average<32, 8><<<grid, 256, 0, st>>>(dA, tiles, ntiles, parity, acc, win, s, last, finish); break;
+    case 1: k_batch32_average<32, 4><<<grid, 128, 0, st>>>(dA, tiles, ntiles, parity, acc, win, s, last, finish); break;
+    case 2: k_batch32_average<16, 8><<<grid, 128, 0, st>>>(dA, tiles, ntiles, parity, acc, win, s, last, finish); break;
+    default: k_batch32_average<64, 4><<<grid, 256, 0, st>>>(dA, tiles, ntiles, parity, acc, win, s, last, finish); break;
     }
     return cudaGetLastError();
 }

@@ -48,6 +48,9 @@ cudaError_t mplb_batch32_check(int cfg, const Params* dP, const FusedArgs32* dA,
 cudaError_t mplb_batch32_fix(int cfg, const FusedArgs32* dA, const int2* tiles, const int* ntiles, int parity,
                              int grid, const long long* jsum, const long long* j0, const int* proj,
                              cudaStream_t s);
+cudaError_t mplb_batch32_average(int cfg, const FusedArgs32* dA, const int2* tiles, const int* ntiles, int parity,
+                                 int grid, double* const* acc, const uint32_t* win, uint32_t s, uint32_t last,
+                                 int finish, cudaStream_t st);
 cudaError_t mplb_mom_sum32(int lat, uint32_t n, const float* f, long long* J, cudaStream_t s);
 cudaError_t mplb_mom_fix32(int lat, uint32_t n, float* f, const long long* J, const long long* J0, cudaStream_t s);
 
@@ -1921,13 +1924,21 @@ struct mplb_batch {
     int graph_cfg = -1;
     uint32_t graph_K = 0;
     uint64_t launches = 0, graph_launches = 0;
+    // time-averaging filter (mplb_batch_filter)
+    std::vector<uint32_t> win;  // per lattice: window in steps, 0 = not filtered
+    uint32_t* dwin = nullptr;
+    double* acc = nullptr;      // 9 n doubles per filtered lattice
+    double** dacc = nullptr;    // per-lattice pointers into acc (null when not filtered)
+    uint32_t filter_first = 0, filter_every = 0;
+    uint64_t windows = 0;       // filter windows run
 };
 
 namespace {
 
 void batch_free(mplb_batch* b) {
     if (b->graph) cudaGraphExecDestroy(b->graph);
-    void* ps[] = {b->dP, b->dA, b->dtiles, b->dnt, b->dsnap, b->snap, b->dmax, b->jsum, b->j0, b->proj};
+    void* ps[] = {b->dP,   b->dA, b->dtiles, b->dnt,  b->dsnap, b->snap, b->dmax,
+                  b->jsum, b->j0, b->proj,   b->dwin, b->acc,   b->dacc};
     for (void* p : ps)
         if (p) cudaFree(p);
     if (b->hmax) cudaFreeHost(b->hmax);
@@ -2124,6 +2135,36 @@ int batch_graph(mplb_batch* b) {
     return 0;
 }
 
+// One filter window over the lattices in the work table: M steps, M the
+// smallest even count above the longest window among `active` (even, so
+// every lattice ends on the buffer it started from).  Lattice i sums the
+// states after steps last-win[i] .. last-1 (last = M - 1); their mean
+// replaces the state step `last` reads, and step `last` runs from it.
+// *M_out = 0 when no active lattice is filtered (nothing launched).
+int batch_window(mplb_batch* b, const std::vector<char>& active, uint32_t* M_out) {
+    uint32_t W = 0;
+    for (size_t i = 0; i < b->lat.size(); i++)
+        if (active[i] && !b->win.empty()) W = std::max(W, b->win[i]);
+    const uint32_t M = W ? (W + 2u) & ~1u : 0u, last = M - 1u;
+    *M_out = M;
+    if (!M) return 0;
+    auto avg = [&](int parity, uint32_t s, int finish) -> int {
+        cudaError_t e = mplb_batch32_average(b->cfg, b->dA, b->dtiles, b->dnt, parity, b->grid, b->dacc, b->dwin, s,
+                                             last, finish, b->stream);
+        b->launches++;
+        if (e != cudaSuccess) return fail(MPLB_E_CUDA, std::string("batch filter launch: ") + cudaGetErrorString(e));
+        return 0;
+    };
+    for (uint32_t s = 0; s < last; s++) {
+        RET(batch_launch(b, b->cfg, b->grid, (int)(s & 1)));
+        RET(avg((int)((s + 1) & 1), s, 0));
+    }
+    RET(avg((int)(last & 1), last, 1));
+    RET(batch_launch(b, b->cfg, b->grid, (int)(last & 1)));
+    b->windows++;
+    return 0;
+}
+
 }  // namespace
 
 extern "C" {
@@ -2267,20 +2308,18 @@ int mplb_batch_run(mplb_batch_t* b, uint32_t max_steps, uint32_t* steps_out, dou
     CK(cudaMemcpyAsync(b->j0, b->jsum, 3 * N * sizeof(long long), cudaMemcpyDeviceToDevice, b->stream));
     size_t left = N;
     uint32_t done = 0, conv = 0;
-    while (left && done < max_steps) {
-        CK(cudaGraphLaunch(b->graph, b->stream));
-        b->graph_launches++;
-        b->launches += b->K + 2;
+    // the check of an interval of `len` steps has been queued: read it, retire lattices
+    auto account = [&](uint32_t len) -> int {
         CK(cudaMemcpyAsync(b->hmax, b->dmax, N * sizeof(unsigned long long), cudaMemcpyDeviceToHost, b->stream));
         CK(cudaStreamSynchronize(b->stream));
-        done += b->K;
+        done += len;
         bool retired = false;
         for (size_t i = 0; i < N; i++) {
             if (!active[i]) continue;
-            steps[i] += b->K;
+            steps[i] += len;
             double d;
             std::memcpy(&d, &b->hmax[i], sizeof(double));
-            rate[i] = d / b->K;
+            rate[i] = d / len;
             if (rate[i] < b->tol || !std::isfinite(rate[i])) {  // converged, or failed (non-finite)
                 active[i] = 0;
                 left--;
@@ -2289,6 +2328,28 @@ int mplb_batch_run(mplb_batch_t* b, uint32_t max_steps, uint32_t* steps_out, dou
             }
         }
         if (retired && left) RET(batch_table(b, b->cfg, active, &nt));
+        return 0;
+    };
+    // filter windows: the first once `filter_first` steps are done, then one
+    // `filter_every` steps after the end of the previous, each at the end of
+    // a check interval and followed by a check of its own
+    uint64_t next_window = b->filter_every && !b->win.empty() ? b->filter_first : UINT64_MAX;
+    while (left && done < max_steps) {
+        if (done >= next_window) {
+            uint32_t M = 0;
+            RET(batch_window(b, active, &M));
+            if (M) {
+                RET(batch_check(b, 0, true));
+                RET(account(M));
+                next_window = (uint64_t)done + b->filter_every;
+                continue;
+            }
+            next_window = UINT64_MAX;  // no active lattice is filtered
+        }
+        CK(cudaGraphLaunch(b->graph, b->stream));
+        b->graph_launches++;
+        b->launches += b->K + 2;
+        RET(account(b->K));
     }
     for (size_t i = 0; i < N; i++) {
         b->lat[i]->current += steps[i];
@@ -2296,6 +2357,72 @@ int mplb_batch_run(mplb_batch_t* b, uint32_t max_steps, uint32_t* steps_out, dou
         if (rate_out) rate_out[i] = rate[i];
     }
     if (n_converged) *n_converged = conv;
+    return batch_leave(b);
+}
+
+int mplb_batch_filter(mplb_batch_t* b, const uint32_t* window, uint32_t first, uint32_t every) {
+    if (!b) return fail(MPLB_E_ARG, "NULL batch");
+    DeviceGuard guard(b->dev);
+    const size_t N = b->lat.size();
+    // finish queued work before the accumulators change
+    CK(cudaStreamSynchronize(b->stream));
+    for (void* p : {(void*)b->dwin, (void*)b->acc, (void*)b->dacc})
+        if (p) cudaFree(p);
+    b->dwin = nullptr;
+    b->acc = nullptr;
+    b->dacc = nullptr;
+    b->win.clear();
+    b->filter_first = b->filter_every = 0;
+    if (!window) return 0;  // filter off
+    size_t tot = 0;
+    for (size_t i = 0; i < N; i++) {
+        if (window[i] > MPLB_BATCH_MAX_WINDOW)
+            return fail(MPLB_E_ARG, "lattice " + std::to_string(i) + ": window longer than MPLB_BATCH_MAX_WINDOW");
+        if (window[i]) tot += (size_t)b->lat[i]->Q * b->lat[i]->n;
+    }
+    std::vector<double*> ptr(N, nullptr);
+    auto setup = [&]() -> int {
+        if (tot) CK(cudaMalloc((void**)&b->acc, tot * sizeof(double)));
+        CK(cudaMalloc((void**)&b->dacc, N * sizeof(double*)));
+        CK(cudaMalloc((void**)&b->dwin, N * sizeof(uint32_t)));
+        size_t off = 0;
+        for (size_t i = 0; i < N; i++) {
+            if (!window[i]) continue;
+            ptr[i] = b->acc + off;
+            off += (size_t)b->lat[i]->Q * b->lat[i]->n;
+        }
+        CK(cudaMemcpyAsync(b->dacc, ptr.data(), N * sizeof(double*), cudaMemcpyHostToDevice, b->stream));
+        CK(cudaMemcpyAsync(b->dwin, window, N * sizeof(uint32_t), cudaMemcpyHostToDevice, b->stream));
+        CK(cudaStreamSynchronize(b->stream));
+        return 0;
+    };
+    if (int rc = setup()) {
+        for (void* p : {(void*)b->dwin, (void*)b->acc, (void*)b->dacc})
+            if (p) cudaFree(p);
+        b->dwin = nullptr;
+        b->acc = nullptr;
+        b->dacc = nullptr;
+        return rc;
+    }
+    b->win.assign(window, window + N);
+    b->filter_first = first;
+    b->filter_every = every;
+    return 0;
+}
+
+int mplb_batch_average(mplb_batch_t* b, uint32_t* steps_out) {
+    if (!b) return fail(MPLB_E_ARG, "NULL batch");
+    if (steps_out) *steps_out = 0;
+    if (b->win.empty()) return fail(MPLB_E_STATE, "no filter windows set (mplb_batch_filter)");
+    DeviceGuard guard(b->dev);
+    RET(batch_enter(b));
+    const std::vector<char> all(b->lat.size(), 1);
+    int nt = 0;
+    RET(batch_ready(b, all, &nt));
+    uint32_t M = 0;
+    RET(batch_window(b, all, &M));
+    for (mplb_gpu* h : b->lat) h->current += M;
+    if (steps_out) *steps_out = M;
     return batch_leave(b);
 }
 

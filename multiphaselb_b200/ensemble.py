@@ -75,10 +75,25 @@ def run_plain(specs, K, tol, max_steps, log=None):
     return out
 
 
-def run_batched(specs, K, tol, max_steps, init=None, tile_config=0):
+def crossing_steps(case):
+    """Steps for sound in the liquid to cross the box: L / c_l with
+    c_l^2 = dp/drho of the EOS at the Maxwell liquid density."""
+    eos, T, rl = case.eos, case.meta["T"], case.meta["rho_l"]
+    h = 1e-6 * rl
+    c2 = (cases.p_eos(eos, rl + h, T) - cases.p_eos(eos, rl - h, T)) / (2 * h)
+    return max(case.dims) / float(np.sqrt(c2))
+
+
+def filter_windows(cs, scale):
+    """Filter window of each case: scale x the sound crossing time, even."""
+    return [int(2 * round(0.5 * scale * crossing_steps(c))) for c in cs]
+
+
+def run_batched(specs, K, tol, max_steps, init=None, tile_config=0, filt=None):
     """All specs as one batch.  `init(lat, case)` (the learned warm start) may
     replace a lattice's tanh/Maxwell state on the device; it returns False to
-    keep the fallback."""
+    keep the fallback.  `filt` = (scale, first, every): time-averaging filter
+    windows of `scale` sound crossing times (Batch.filter)."""
     t0 = time.perf_counter()
     cs = [make_case(s) for s in specs]
     t1 = time.perf_counter()
@@ -95,6 +110,8 @@ def run_batched(specs, K, tol, max_steps, init=None, tile_config=0):
     t2 = time.perf_counter()
     host_s, setup = t1 - t0, t2 - t1
     with Batch(lats, check_interval=K, tol=tol, tile_config=tile_config) as b:
+        if filt and filt[0] > 0:
+            b.filter(filter_windows(cs, filt[0]), filt[1], filt[2])
         t0 = time.perf_counter()
         steps, rate, conv = b.run(max_steps)
         lats[0].sync()
@@ -111,7 +128,7 @@ def run_batched(specs, K, tol, max_steps, init=None, tile_config=0):
     # lattice that diverged runs again from it (its time counts).
     bad = [i for i, r in enumerate(res) if r["diverged"]] if init is not None else []
     if bad:
-        again = run_batched([specs[i] for i in bad], K, tol, max_steps, None, tile_config)
+        again = run_batched([specs[i] for i in bad], K, tol, max_steps, None, tile_config, filt)
         for i, r in zip(bad, again["cases"]):
             res[i] = dict(r, fallback=True)
         out["wall_s"] += again["wall_s"]
@@ -149,14 +166,20 @@ def main(argv=None):
     ap.add_argument("--init", choices=("tanh", "mlp", "both"), default="tanh")
     ap.add_argument("--weights", default=None, help="warm-start weights (.npz); default: the packaged D2Q9 network")
     ap.add_argument("--sizes", default=None, help="comma list: one case per size at T/Tc=0.8, R=0.2L")
+    ap.add_argument("--filter", type=float, default=0.0,
+                    help="time-averaging filter windows of this many sound crossing times (0: off)")
+    ap.add_argument("--filter-first", type=int, default=2000)
+    ap.add_argument("--filter-every", type=int, default=10000)
     ap.add_argument("--out", default=None)
     a = ap.parse_args(argv)
+    filt = (a.filter, a.filter_first, a.filter_every) if a.filter > 0 else None
     if a.sizes:
         specs = [dict(L=int(x), t_ratio=0.8, radius=0.2 * int(x)) for x in a.sizes.split(",")]
     else:
         specs = draw(a.cases, a.seed)
     log = lambda m: print(m, file=sys.stderr, flush=True)  # noqa: E731
-    rep = dict(specs=specs, tol=a.tol, check_interval=a.check, max_steps=a.max_steps)
+    rep = dict(specs=specs, tol=a.tol, check_interval=a.check, max_steps=a.max_steps,
+               filter=dict(scale=a.filter, first=a.filter_first, every=a.filter_every) if filt else None)
     m = min(a.plain, len(specs))
     if m:
         rep["plain"] = run_plain(specs[:m], a.check, a.tol, a.max_steps, log)
@@ -166,13 +189,13 @@ def main(argv=None):
             init = warmstart.initializer(abi.D2Q9, a.weights)
             if init is None:
                 raise SystemExit("no trained warm-start weights")
-        b = run_batched(specs, a.check, a.tol, a.max_steps, init)
+        b = run_batched(specs, a.check, a.tol, a.max_steps, init, filt=filt)
         rep["batched_" + mode] = b
         log(f"batched ({mode}): {b['converged']}/{len(specs)} converged, {b['wall_s']:.2f} s")
         if m:
             # batched wall time is for all cases; compare per case on the
             # first m, and on the wall only when m covers every case
-            sub = b if m == len(specs) else run_batched(specs[:m], a.check, a.tol, a.max_steps, init)
+            sub = b if m == len(specs) else run_batched(specs[:m], a.check, a.tol, a.max_steps, init, filt=filt)
             rep["compare_" + mode] = compare(sub, rep["plain"])
             log(json.dumps(rep["compare_" + mode]))
     txt = json.dumps(rep, indent=1)

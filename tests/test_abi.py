@@ -38,6 +38,11 @@ def test_version_reports_the_header_abi():
     assert f"ABI {m.group(1)} " in v, v
 
 
+def test_constants_mirror_the_header():
+    h = open(HEADER).read()
+    assert int(re.search(r"#define MPLB_BATCH_MAX_WINDOW (\d+)u", h).group(1)) == abi.BATCH_MAX_WINDOW
+
+
 STRUCTS = {
     "mplb_mesh_desc": abi.MeshDesc,
     "mplb_eos_desc": abi.EosDesc,
