@@ -23,7 +23,7 @@ SOURCES = [(os.path.join(HERE, "csrc", "mplb_gpu.cu"), False),
            (os.path.join(HERE, "csrc", "mplb_fp32.cu"), True),
            (os.path.join(HERE, "csrc", "mplb_mlp.cu"), False),
            (os.path.join(HERE, "csrc", "mplb_io.cu"), False)]
-HEADERS = [os.path.join(HERE, "csrc", f) for f in ("lattice.cuh", "ops.cuh", "fused.cuh", "fused_host.cuh", "fused_tma.cuh", "tma_util.cuh", "fused32.cuh", "mplb_io.h")] + \
+HEADERS = [os.path.join(HERE, "csrc", f) for f in ("lattice.cuh", "ops.cuh", "fused.cuh", "fused_host.cuh", "fused_tma.cuh", "tma_util.cuh", "umma.cuh", "fused32.cuh", "mplb_io.h")] + \
           [os.path.join(ROOT, "include", "mplb_gpu.h")]
 
 NVCC_FLAGS = [

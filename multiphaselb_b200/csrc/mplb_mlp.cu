@@ -7,11 +7,13 @@
 // order, biases, gradients and the Adam state are FP32.  The master weights
 // are FP32; the BF16 copy is refreshed after every update.
 //
-// Kernels (CUDA cores): at 64 units a layer is a 64 x 64 matrix, far below a
-// tensor-core tile's useful size; one block of 64 threads (thread j = unit j)
-// carries SB samples through all layers with the weights in shared memory.
-// Training writes per-block gradient partials that a second kernel sums in a
-// fixed order (deterministic) and feeds to Adam.
+// Kernels.  Inference (mplb_mlp_predict, mplb_mlp_init_bubble) runs the two
+// 64 x 64 layers on the tensor cores, 128 samples per CTA (tcgen05.mma from
+// shared memory into tensor memory, see k_mlp_predict).  Training runs on
+// the CUDA cores: one block of 64 threads (thread j = unit j) carries SB
+// samples through all layers with the weights in shared memory, forward and
+// backward, and writes per-block gradient partials that a second kernel sums
+// in a fixed order (deterministic) and feeds to Adam.
 //
 // This translation unit is compiled without FMA contraction: the feature
 // normalisation below runs on host and device and must agree bit for bit.
@@ -25,6 +27,7 @@
 #include <vector>
 
 #include "../../include/mplb_gpu.h"
+#include "umma.cuh"
 
 int mplb_internal_fail(int code, const std::string& msg);
 
@@ -302,44 +305,176 @@ __global__ void k_mlp_reduce(const float* __restrict__ partial, int nblk, const 
     Wb[p] = bf16_bits(w);
 }
 
-// Forward pass over arbitrary samples (features already normalised).
-__global__ void __launch_bounds__(NH) k_mlp_predict(const float* __restrict__ P, const uint16_t* __restrict__ Wb,
-                                                    const float* __restrict__ X, uint32_t n,
-                                                    float* __restrict__ Y) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    Block& s = *reinterpret_cast<Block*>(smem_raw);
-    const int j = threadIdx.x;
-    load_weights(s, P, Wb);
-    const uint32_t e = blockIdx.x * SB + j;
-    if (j < SB) {
-#pragma unroll
-        for (int i = 0; i < NIN; i++) s.x[j][i] = e < n ? X[(size_t)e * NIN + i] : 0.f;
+// ------------------------------------------------- inference on tcgen05
+// 128 samples per CTA, one per thread and tensor-memory lane.  Layer 1
+// (5 -> 64) runs on the CUDA cores; layers 2 and 3 (64 x 64) are each one
+// 128 x 64 x 64 BF16 product on the tensor core (activations and weights in
+// shared memory in the core-matrix layout of umma.cuh, FP32 accumulators in
+// tensor memory, four K = 16 instructions issued by one thread); bias, tanh
+// and the BF16 rounding of each activation happen in the epilogue after
+// tcgen05.ld; layer 4 (64 -> 1) is a per-thread dot product.  The FP32 sums
+// of layers 2 and 3 are the tensor core's (their order and rounding differ
+// from the CUDA-core fmaf chain of training), so an activation on a BF16
+// rounding boundary can land one BF16 step away.
+constexpr int TC_M = 128;
+constexpr uint32_t TC_COLS = 128;  // two 64-column accumulators
+struct TcBlock {
+    uint16_t A[TC_M * NH];  // activations (16 KB; first, at the aligned base)
+    uint16_t W2[NH * NH];   // weights [out][in] (8 KB each)
+    uint16_t W3[NH * NH];
+    float W1[NH * NIN], b1[NH], b2[NH], b3[NH], W4[NH], b4;
+    uint64_t bar;
+    uint32_t tmem;
+};
+// 1 KB alignment slack; at least 48 KB so that at most four CTAs share an
+// SM and their tensor-memory allocations (4 x 128 of 512 columns) all fit
+constexpr size_t TC_SMEM = sizeof(TcBlock) + 1024 > 48 * 1024 ? sizeof(TcBlock) + 1024 : 48 * 1024;
+
+__device__ inline TcBlock& tc_block() {
+    extern __shared__ unsigned char tc_raw[];
+    return *reinterpret_cast<TcBlock*>(((uintptr_t)tc_raw + 1023) & ~(uintptr_t)1023);
+}
+
+// Weights into shared memory, mbarrier, tensor memory.
+__device__ void tc_setup(TcBlock& s, const float* __restrict__ P, const uint16_t* __restrict__ Wb) {
+    const int t = threadIdx.x;
+    for (int i = t; i < NH * NH; i += blockDim.x) {
+        const int o = i / NH, k = i % NH;
+        s.W2[mplb::umma_core_index(o, k, NH)] = Wb[OFF_W2 + i];
+        s.W3[mplb::umma_core_index(o, k, NH)] = Wb[OFF_W3 + i];
     }
+    for (int i = t; i < NH * NIN; i += blockDim.x) s.W1[i] = bf16_float(Wb[OFF_W1 + i]);
+    for (int i = t; i < NH; i += blockDim.x) {
+        s.b1[i] = P[OFF_B1 + i];
+        s.b2[i] = P[OFF_B2 + i];
+        s.b3[i] = P[OFF_B3 + i];
+        s.W4[i] = bf16_float(Wb[OFF_W4 + i]);
+    }
+    if (t == 0) {
+        s.b4 = P[OFF_B4];
+        mplb::mbar_init(&s.bar, 1);
+        mplb::mbar_init_fence();
+    }
+    if (t < 32) mplb::tmem_alloc(&s.tmem, TC_COLS);
+    mplb::tc_fence_before();
     __syncthreads();
-    forward(s);
-    if (j < SB && e < n) Y[e] = s.out[j];
+    mplb::tc_fence_after();
+}
+
+// This thread's row of activations h[0..63] into the A operand.
+__device__ inline void tc_store_row(TcBlock& s, const float* h) {
+    const int r = threadIdx.x;
+#pragma unroll
+    for (int c = 0; c < NH / 8; c++) {
+        uint32_t w[4];
+#pragma unroll
+        for (int q = 0; q < 4; q++)
+            w[q] = (uint32_t)bf16_bits(h[8 * c + 2 * q]) | ((uint32_t)bf16_bits(h[8 * c + 2 * q + 1]) << 16);
+        *reinterpret_cast<uint4*>(&s.A[mplb::umma_core_index(r, 8 * c, NH)]) = make_uint4(w[0], w[1], w[2], w[3]);
+    }
+    mplb::fence_async_smem();
+}
+
+// One thread issues A x W^T into tensor-memory columns col .. col+63.
+__device__ inline void tc_layer(TcBlock& s, const uint16_t* W, uint32_t col) {
+    if (threadIdx.x != 0) return;
+    constexpr uint32_t IDESC = mplb::umma_idesc_bf16(TC_M, NH), LBO = 128, SBO = NH / 8 * 128;
+    const uint32_t a0 = mplb::smem_u32(s.A), b0 = mplb::smem_u32(W);
+#pragma unroll
+    for (int kk = 0; kk < NH / 16; kk++)
+        mplb::umma_bf16(s.tmem + col, mplb::umma_smem_desc(a0 + 256 * kk, LBO, SBO),
+                        mplb::umma_smem_desc(b0 + 256 * kk, LBO, SBO), IDESC, kk > 0);
+    mplb::umma_commit(&s.bar);
+}
+
+// Epilogue: bias, tanh and BF16 rounding of this thread's row of columns col .. col+63.
+__device__ inline void tc_epilogue(TcBlock& s, uint32_t col, const float* bias, float* h) {
+    const uint32_t lane0 = (uint32_t)(threadIdx.x & ~31) << 16;
+#pragma unroll
+    for (int half = 0; half < 2; half++) {
+        float v[32];
+        mplb::tmem_ld32(s.tmem + lane0 + col + 32 * half, v);
+#pragma unroll
+        for (int c = 0; c < 32; c++) h[32 * half + c] = bf16_round(tanhf(v[c] + bias[32 * half + c]));
+    }
+}
+
+// The network on this thread's features x (all 128 threads of the CTA
+// call it together); false when a bounded wait for the tensor core ran out
+// (the CTA then records the error and its outputs are not valid).
+__device__ bool tc_forward(TcBlock& s, const float* x, float& out, int* kerr) {
+    float h[NH];
+#pragma unroll
+    for (int j = 0; j < NH; j++) {
+        float z = s.b1[j];
+#pragma unroll
+        for (int i = 0; i < NIN; i++) z = fmaf(s.W1[j * NIN + i], x[i], z);
+        h[j] = bf16_round(tanhf(z));
+    }
+    bool good = true;
+    uint32_t phase = 0;
+#pragma unroll
+    for (int layer = 0; layer < 2; layer++) {
+        tc_store_row(s, h);
+        mplb::tc_fence_before();
+        __syncthreads();
+        mplb::tc_fence_after();
+        tc_layer(s, layer == 0 ? s.W2 : s.W3, 64u * layer);
+        const bool landed = mplb::mbar_wait_bounded(&s.bar, phase, mplb::TMA_WAIT_LIMIT);
+        mplb::tc_fence_after();
+        if (__syncthreads_or(!landed)) {
+            good = false;
+            // let the products in flight finish before the tensor memory is released
+            mplb::mbar_wait_bounded(&s.bar, phase, mplb::TMA_WAIT_LIMIT);
+            break;
+        }
+        phase ^= 1u;
+        tc_epilogue(s, 64u * layer, layer == 0 ? s.b2 : s.b3, h);
+    }
+    if (good) {
+        float z = s.b4;
+#pragma unroll
+        for (int i = 0; i < NH; i++) z = fmaf(s.W4[i], h[i], z);
+        out = z;
+    } else if (threadIdx.x == 0) {
+        atomicExch(kerr, mplb::MPLB_KERR_WAIT);
+    }
+    mplb::tc_fence_before();
+    __syncthreads();
+    if (threadIdx.x < 32) mplb::tmem_dealloc(s.tmem, TC_COLS);
+    return good;
+}
+
+// Forward pass over arbitrary samples (features already normalised).
+__global__ void __launch_bounds__(TC_M) k_mlp_predict(const float* __restrict__ P, const uint16_t* __restrict__ Wb,
+                                                      const float* __restrict__ X, uint32_t n, float* __restrict__ Y,
+                                                      int* __restrict__ kerr) {
+    TcBlock& s = tc_block();
+    tc_setup(s, P, Wb);
+    const uint32_t e = blockIdx.x * TC_M + threadIdx.x;
+    float x[NIN];
+#pragma unroll
+    for (int i = 0; i < NIN; i++) x[i] = e < n ? X[(size_t)e * NIN + i] : 0.f;
+    float out = 0.f;
+    if (tc_forward(s, x, out, kerr) && e < n) Y[e] = out;
 }
 
 // Initial density of a box lattice: node i at (i % nx, i / nx % ny, i / (nx ny)),
 // r = distance to the bubble centre, rho = network(T/Tc, a, b, r/R) / b.
-__global__ void __launch_bounds__(NH) k_mlp_bubble(const float* __restrict__ P, const uint16_t* __restrict__ Wb,
-                                                   uint32_t n, int nx, int ny, double cx, double cy, double cz,
-                                                   double R, double t_ratio, double a, double b,
-                                                   double* __restrict__ rho) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    Block& s = *reinterpret_cast<Block*>(smem_raw);
-    const int j = threadIdx.x;
-    load_weights(s, P, Wb);
-    const uint32_t e = blockIdx.x * SB + j;
-    if (j < SB) {
-        const uint32_t i = e < n ? e : 0;
-        const double x = (double)(i % (uint32_t)nx) - cx, y = (double)((i / (uint32_t)nx) % (uint32_t)ny) - cy,
-                     z = (double)(i / ((uint32_t)nx * (uint32_t)ny)) - cz;
-        features(t_ratio, a, b, sqrt(x * x + y * y + z * z), R, s.x[j]);
-    }
-    __syncthreads();
-    forward(s);
-    if (j < SB && e < n) rho[e] = (double)s.out[j] / b;
+__global__ void __launch_bounds__(TC_M) k_mlp_bubble(const float* __restrict__ P, const uint16_t* __restrict__ Wb,
+                                                     uint32_t n, int nx, int ny, double cx, double cy, double cz,
+                                                     double R, double t_ratio, double a, double b,
+                                                     double* __restrict__ rho, int* __restrict__ kerr) {
+    TcBlock& s = tc_block();
+    tc_setup(s, P, Wb);
+    const uint32_t e = blockIdx.x * TC_M + threadIdx.x;
+    const uint32_t i = e < n ? e : 0;
+    const double x = (double)(i % (uint32_t)nx) - cx, y = (double)((i / (uint32_t)nx) % (uint32_t)ny) - cy,
+                 z = (double)(i / ((uint32_t)nx * (uint32_t)ny)) - cz;
+    float f[NIN];
+    features(t_ratio, a, b, sqrt(x * x + y * y + z * z), R, f);
+    float out = 0.f;
+    if (tc_forward(s, f, out, kerr) && e < n) rho[e] = (double)out / b;
 }
 
 constexpr size_t SMEM = sizeof(Block);
@@ -350,9 +485,9 @@ int set_attrs() {
     std::call_once(once, [] {
         err = cudaFuncSetAttribute(k_mlp_grad, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM);
         if (err == cudaSuccess)
-            err = cudaFuncSetAttribute(k_mlp_predict, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM);
+            err = cudaFuncSetAttribute(k_mlp_predict, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TC_SMEM);
         if (err == cudaSuccess)
-            err = cudaFuncSetAttribute(k_mlp_bubble, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM);
+            err = cudaFuncSetAttribute(k_mlp_bubble, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TC_SMEM);
     });
     return err == cudaSuccess ? 0 : mplb_internal_fail(MPLB_E_CUDA, std::string("MLP kernel attributes: ") +
                                                                        cudaGetErrorString(err));
@@ -390,6 +525,7 @@ struct mplb_mlp {
     int nblk_cap = 0;
     double* loss = nullptr;
     float* grad = nullptr;
+    int* kerr = nullptr;  // inference kernels: a bounded wait for the tensor core ran out
     uint32_t seed = 0;
     uint64_t step = 0;
 };
@@ -397,7 +533,7 @@ struct mplb_mlp {
 namespace {
 
 void mlp_free(mplb_mlp* m) {
-    void* ps[] = {m->P, m->M, m->V, m->Wb, m->X, m->Y, m->partial, m->loss_partial, m->loss, m->grad};
+    void* ps[] = {m->P, m->M, m->V, m->Wb, m->X, m->Y, m->partial, m->loss_partial, m->loss, m->grad, m->kerr};
     for (void* p : ps)
         if (p) cudaFree(p);
     if (m->stream) cudaStreamDestroy(m->stream);
@@ -426,6 +562,18 @@ int upload_params(mplb_mlp* m, const float* host) {
     CKM(cudaStreamSynchronize(m->stream));
     m->step = 0;
     return 0;
+}
+
+// After an inference launch on stream s: wait for it and report a tensor-core
+// wait that ran out (the flag is cleared for the next call).
+int inference_status(mplb_mlp* m, cudaStream_t s) {
+    int v = 0;
+    CKM(cudaMemcpyAsync(&v, m->kerr, sizeof(int), cudaMemcpyDeviceToHost, s));
+    CKM(cudaStreamSynchronize(s));
+    if (!v) return 0;
+    CKM(cudaMemsetAsync(m->kerr, 0, sizeof(int), s));
+    CKM(cudaStreamSynchronize(s));
+    return mplb_internal_fail(MPLB_E_TIMEOUT, "MLP inference: a bounded wait for the tensor core ran out");
 }
 
 // One pass: gradient over `nbatch` samples (drawn, or the first nbatch in
@@ -467,9 +615,10 @@ int mplb_mlp_bubble_launch(mplb_mlp* m, double* rho, uint32_t n, int nx, int ny,
     if (e == cudaSuccess) e = cudaStreamWaitEvent(s, ev, 0);
     cudaEventDestroy(ev);
     CKM(e);
-    k_mlp_bubble<<<(n + SB - 1) / SB, NH, SMEM, s>>>(m->P, m->Wb, n, nx, ny, c[0], c[1], c[2], R, t_ratio, a, b, rho);
+    k_mlp_bubble<<<(n + TC_M - 1) / TC_M, TC_M, TC_SMEM, s>>>(m->P, m->Wb, n, nx, ny, c[0], c[1], c[2], R, t_ratio,
+                                                               a, b, rho, m->kerr);
     CKM(cudaGetLastError());
-    return 0;
+    return inference_status(m, s);
 }
 
 int mplb_mlp_device(const mplb_mlp* m) { return m->dev; }
@@ -498,6 +647,8 @@ int mplb_mlp_create(int32_t device, uint64_t seed, mplb_mlp_t** out) {
         CKM(cudaMalloc((void**)&m->Wb, NPARAM * sizeof(uint16_t)));
         CKM(cudaMalloc((void**)&m->grad, NPARAM * sizeof(float)));
         CKM(cudaMalloc((void**)&m->loss, sizeof(double)));
+        CKM(cudaMalloc((void**)&m->kerr, sizeof(int)));
+        CKM(cudaMemsetAsync(m->kerr, 0, sizeof(int), m->stream));
         // Glorot-uniform weights from a seeded xorshift generator, zero biases.
         std::vector<float> p(NPARAM, 0.f);
         uint64_t st = seed * 0x9E3779B97F4A7C15ull + 1;
@@ -612,8 +763,9 @@ int mplb_mlp_predict(mplb_mlp_t* m, const double* t_ratio, const double* a, cons
         CKM(cudaMalloc((void**)&dx, x.size() * sizeof(float)));
         CKM(cudaMalloc((void**)&dy, y.size() * sizeof(float)));
         CKM(cudaMemcpyAsync(dx, x.data(), x.size() * sizeof(float), cudaMemcpyHostToDevice, m->stream));
-        k_mlp_predict<<<(n + SB - 1) / SB, NH, SMEM, m->stream>>>(m->P, m->Wb, dx, n, dy);
+        k_mlp_predict<<<(n + TC_M - 1) / TC_M, TC_M, TC_SMEM, m->stream>>>(m->P, m->Wb, dx, n, dy, m->kerr);
         CKM(cudaGetLastError());
+        if (int rc = inference_status(m, m->stream)) return rc;
         CKM(cudaMemcpyAsync(y.data(), dy, y.size() * sizeof(float), cudaMemcpyDeviceToHost, m->stream));
         CKM(cudaStreamSynchronize(m->stream));
         return 0;
