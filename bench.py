@@ -8,7 +8,9 @@ box path.  One step = one time step of the whole lattice.  The lattice state
 (~21 MB) fits in L2, so a 256 MiB buffer is written between timed steps and
 each step is timed alone with CUDA events on the library's stream.  The
 other named workloads (D3Q15 bubble 192^3, D2Q9 bubble 256^2) follow under
-"extra", device-timed the same way, FP64 and FP32-deviation.
+"extra", device-timed the same way, FP64 and FP32-deviation.  On one GPU,
+"time_to_equilibrium" compares the plain FP64 path with the batched
+FP32-deviation + warm-start + filter form on a seeded bubble ensemble.
 
 For N > 1 (torchrun, one process per GPU) every rank advances its own
 replica of the workload (weak scaling; the path has no exchange step on one
@@ -264,6 +266,31 @@ def kernel_name(case, precision, tile_config=-1):
     return "k_fused_d3q15_tma" if tile_config in (6, 7) else "k_fused_d3q15"
 
 
+def time_to_equilibrium(ncases):
+    """Seeded static-bubble ensemble (D2Q9 CS, L in 64..512, T/Tc in [0.6, 0.95],
+    R in [8, 0.3 L]) to max |drho/dt| < 1e-9 over 1000 steps: the plain FP64
+    path (lone handles one after another) against the accelerated form
+    (FP32-deviation lattices in one batch, learned warm start, time-averaging
+    filter windows of two sound crossing times).  Wall seconds of the stepping
+    on the host clock around device-synchronised runs, set-up excluded."""
+    from multiphaselb_b200 import abi, ensemble, warmstart
+    specs = ensemble.draw(ncases)
+    plain = ensemble.run_plain(specs, 1000, 1e-9, 400000)
+    init = warmstart.initializer(abi.D2Q9)
+    filt = (2.0, 2000, 4000)
+    acc = ensemble.run_batched(specs, 1000, 1e-9, 400000, init, filt=filt)
+    c = ensemble.compare(acc, plain)
+    return {"cases": ncases, "tol": 1e-9, "check_interval": 1000,
+            "plain_fp64_s": round(c["plain_wall_s"], 3), "accelerated_s": round(c["batched_wall_s"], 3),
+            "ratio": round(c["speedup"], 3), "target_ratio": 5.0,
+            "plain_steps": c["plain_steps"], "accelerated_steps": c["batched_steps"],
+            "converged": f"{acc['converged']}/{ncases}", "warm_started": acc["warm_started"],
+            "max_rel_coexistence": c["max_rel_coexistence"], "within_1e-3": f"{c['within_1e3']}/{c['compared']}",
+            "accelerated_form": "batched FP32-deviation + learned warm start (tcgen05 inference) + "
+                                f"time-averaging filter (scale {filt[0]}, first {filt[1]}, every {filt[2]})",
+            "data": f"ensemble.draw({ncases}), seeded; plain = FP64 fused path, tanh/Maxwell start"}
+
+
 def run_ours(a):
     import torch
     from multiphaselb_b200 import PATH_AUTO, PATH_FUSED, PATH_OPERATORS, Lattice, abi, cases
@@ -399,6 +426,8 @@ def run_ours(a):
     line["gpu_launches_by_region"] = launches
     if rank == 0 and world == 1 and not a.no_cpu:
         line["cpu_baseline"] = cpu_baseline(a.workload, a.cpu_steps, 1)
+    if world == 1 and a.tte_cases > 0:
+        line["time_to_equilibrium"] = time_to_equilibrium(a.tte_cases)
     if world > 1:
         import torch.distributed as dist
         dist.barrier()
@@ -494,6 +523,8 @@ def main():
     ap.add_argument("--no-fp32", action="store_true")
     ap.add_argument("--no-extra", action="store_true", help="time the named workload only")
     ap.add_argument("--extra-steps", type=int, default=0, help="timed steps of each extra workload (default --steps)")
+    ap.add_argument("--tte-cases", type=int, default=24,
+                    help="bubbles of the time-to-equilibrium comparison (1 GPU only; 0 = skip)")
     a = ap.parse_args()
     if a.warmup < 3:
         ap.error("--warmup must be >= 3")
