@@ -41,7 +41,7 @@ extern "C" {
 
 #define MPLB_ABI_VERSION 5  /* 2: mplb_field_desc.alpha_1/alpha_2, mplb_opts.rank; 3: mplb_gpu_copy_nodes;
                                4: mplb_info.tile_ms[16], MPLB_E_TIMEOUT;
-                               5: mplb_batch_filter, mplb_batch_average */
+                               5: mplb_batch_filter, mplb_batch_average, mplb_mlp_init_column(_mass) */
 #define MPLB_MAX_Q 15
 #define MPLB_MAX_PATCHES 64
 
@@ -493,6 +493,22 @@ int mplb_mlp_init_bubble(mplb_mlp_t* m, mplb_gpu_t* h, double t_ratio, const dou
  * effective radius.  Allocates one scratch array of n doubles. */
 int mplb_mlp_init_bubble_mass(mplb_mlp_t* m, mplb_gpu_t* h, double t_ratio, const double* center, double radius,
                               double T, double target_mass, double* radius_used);
+/* Axial profile: a liquid band (a column or layer) of thickness `height`
+ * along `axis` (0 = x, 1 = y, 2 = z), centred at coordinate `center`
+ * (periodic distance over the box), in vapour: rho of every node from the
+ * network with a flat interface (features with R = +inf, r = height/2 minus
+ * the node's distance to the band centre), U = 0, T = T.  Use a network
+ * trained on flat interfaces (the packaged column weights).  Call
+ * mplb_gpu_initialize next.  No counterpart in the reference, whose column
+ * starts from its tanh profile (tgProfileScalarField.c). */
+int mplb_mlp_init_column(mplb_mlp_t* m, mplb_gpu_t* h, double t_ratio, int32_t axis, double center, double height,
+                         double T);
+/* As mplb_mlp_init_column, with the lattice's total density made equal to
+ * target_mass in the same way as mplb_mlp_init_bubble_mass (the band height
+ * bracketed and two fields blended); *height_used (may be NULL) receives the
+ * effective height.  Allocates one scratch array of n doubles. */
+int mplb_mlp_init_column_mass(mplb_mlp_t* m, mplb_gpu_t* h, double t_ratio, int32_t axis, double center,
+                              double height, double T, double target_mass, double* height_used);
 
 /*
  * Field files in the reference's per-rank formats, the data format chosen as

@@ -271,6 +271,36 @@ def bubble_case(lattice=abi.D2Q9, L=256, radius=40.0, width=5.0, t_ratio=0.8,
                 meta=dict(Tc=tc, T=T0, rho_v=rv, rho_l=rl, radius=radius))
 
 
+def band_case(lattice=abi.D2Q9, dims=(8, 256), axis=1, height=96.0, width=5.0, t_ratio=0.8,
+              a=1.0, b=4.0, sigma=0.125, Lambda=None, name=None):
+    """Liquid band (a column or layer with flat interfaces) in vapour, fully
+    periodic, Carnahan-Starling EOS, isothermal: along `axis` the band spans
+    [c - height/2, c + height/2] around the box centre c, joined to the vapour
+    by tanh profiles of width `width` at the Maxwell densities, as the
+    reference's tgProfileScalarField builds an axial profile
+    (src/applications/fields/setInitialFields/tgProfileScalarField.c:66-76,
+    there with the band between z1 and z2)."""
+    eos = dict(type=abi.EOS_CS, a=a, b=b, R=1.0, G=-1.0, M=1.0, Cv=1.0,
+               g=(0.0, 0.0, 0.0), fext=(0.0, 0.0, 0.0), rho_0=0.0)
+    d3 = lattice == abi.D3Q15
+    nb, points, patches, names = box_mesh(lattice, tuple(dims), (True,) * len(dims))
+    tc = critical_temperature(eos)
+    T0 = t_ratio * tc
+    rv, rl = maxwell_densities(eos, T0)
+    c = (dims[axis] - 1) / 2.0
+    z = points[:, axis].astype(np.float64)
+    z1, z2 = c - 0.5 * height, c + 0.5 * height
+    rho = rv + 0.5 * (rl - rv) * (np.tanh(2.0 * (z - z1) / width) - np.tanh(2.0 * (z - z2) / width))
+    n = rho.size
+    f = dict(model=abi.XUMRT if d3 else abi.LIMRT, update=1,
+             Lambda=Lambda or (LAMBDA_XU if d3 else LAMBDA_C1), sigma=sigma,
+             bc_type=[], bc_value=np.zeros((0, 3)))
+    return Case(name or f"band_{'d3q15' if d3 else 'd2q9'}_{'x'.join(map(str, dims))}_h{height:g}",
+                lattice, tuple(dims), (True,) * len(dims), nb, points, patches, names, eos, f, None,
+                rho.astype(np.float64), np.zeros((n, 3)), np.full(n, T0),
+                meta=dict(Tc=tc, T=T0, rho_v=rv, rho_l=rl, axis=axis, center=c, height=height))
+
+
 def column_case(nx=128, ny=512, liquid_frac=0.4, width=4.0, t0=0.85, t_bot=0.86, t_top=0.84,
                 gy=-1e-5, amp=1e-4, seed=SEED, name=None, f_bc=abi.BC_BOUNCEBACK, wall_u=None,
                 a=9.0 / 392.0, b=2.0 / 21.0):

@@ -11,6 +11,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <functional>
 #include <string>
 #include <thread>
 #include <unordered_set>
@@ -34,6 +35,8 @@ cudaError_t mplb_to_dev32(uint32_t n, int Q, const double* src, float* dst, cons
 // Learned warm start (mplb_mlp.cu).
 int mplb_mlp_bubble_launch(mplb_mlp* m, double* rho, uint32_t n, int nx, int ny, const double* c, double R,
                            double t_ratio, double a, double b, cudaStream_t s);
+int mplb_mlp_column_launch(mplb_mlp* m, double* rho, uint32_t n, int nx, int ny, int axis, int ext, double c,
+                           double height, double t_ratio, double a, double b, cudaStream_t s);
 int mplb_mlp_device(const mplb_mlp* m);
 
 // Batched ensemble kernels (mplb_fp32.cu).
@@ -1593,11 +1596,16 @@ int mplb_mlp_init_bubble(mplb_mlp_t* m, mplb_gpu_t* h, double t_ratio, const dou
     return 0;
 }
 
-int mplb_mlp_init_bubble_mass(mplb_mlp_t* m, mplb_gpu_t* h, double t_ratio, const double* center, double radius,
-                              double T, double target_mass, double* radius_used) {
-    if (!m || !h || !center) return fail(MPLB_E_ARG, "NULL argument");
-    if (!(radius > 0.0) || !(target_mass > 0.0)) return fail(MPLB_E_ARG, "radius and mass must be positive");
-    DeviceGuard guard(h->dev);
+// Common part of the *_mass warm starts: place_at(p) writes the network's
+// density for the shape parameter p (bubble radius, band height); the
+// lattice mass is monotonic in p, falling as p grows for dir = -1 (a bubble)
+// and rising for dir = +1 (a liquid band).  The network's inputs are BF16,
+// so the mass is a step function of p: secant steps to get close, a bracket
+// [pa, pb] with g(pa) >= 0 >= g(pb) (g = the mass excess, signed so that it
+// falls with p), bisection down to one step, then the two fields blended so
+// that the lattice holds the target mass exactly.  *used = the effective p.
+int place_with_mass(mplb_gpu* h, const std::function<int(double)>& place_at, double p0, int dir, double target_mass,
+                    double* used) {
     const int parts = std::min<int>(h->red_parts, (int)blocks(h->n));
     auto total = [&](double* M) -> int {
         k_sum2_partial<<<parts, TPB, 0, h->stream>>>(h->n, h->rho, nullptr, h->red);
@@ -1608,46 +1616,40 @@ int mplb_mlp_init_bubble_mass(mplb_mlp_t* m, mplb_gpu_t* h, double t_ratio, cons
         CK(cudaStreamSynchronize(h->stream));
         return 0;
     };
-    // mass of the network's bubble of radius R, minus the target
-    auto mass_at = [&](double R, double* f) -> int {
-        RET(mplb_mlp_init_bubble(m, h, t_ratio, center, R, T));
+    // mass excess of the network's field at p, signed to fall as p grows
+    auto g_at = [&](double p, double* f) -> int {
+        RET(place_at(p));
         RET(total(f));
-        *f -= target_mass;
+        *f = (*f - target_mass) * (double)(-dir);
         return 0;
     };
-    // The mass falls as the bubble grows, but the network's inputs are BF16,
-    // so it is a step function of R.  Secant steps to get close, bracket
-    // [ra, rb] with f(ra) >= 0 >= f(rb), bisect down to one step, then blend
-    // the two fields so that the lattice holds the target mass exactly: the
-    // bulk densities stay the network's, the interface moves by a fraction of
-    // a step.
-    double r0 = radius, r1 = radius * 1.02, f0 = 0, f1 = 0;
-    RET(mass_at(r0, &f0));
-    RET(mass_at(r1, &f1));
+    double r0 = p0, r1 = p0 * 1.02, f0 = 0, f1 = 0;
+    RET(g_at(r0, &f0));
+    RET(g_at(r1, &f1));
     for (int it = 0; it < 8 && f1 != f0 && f1 != 0.0; it++) {
-        const double r2 = std::min(2.0 * radius, std::max(0.5 * radius, r1 - f1 * (r1 - r0) / (f1 - f0)));
+        const double r2 = std::min(2.0 * p0, std::max(0.5 * p0, r1 - f1 * (r1 - r0) / (f1 - f0)));
         r0 = r1;
         f0 = f1;
         r1 = r2;
-        RET(mass_at(r1, &f1));
+        RET(g_at(r1, &f1));
     }
     double ra = r1, fa = f1, rb = r1, fb = f1, step = 0.01 * r1;
     for (int it = 0; it < 40 && !(fa >= 0.0 && fb <= 0.0); it++, step *= 2.0) {
         if (fa < 0.0) {
             ra = std::max(1e-3, ra - step);
-            RET(mass_at(ra, &fa));
+            RET(g_at(ra, &fa));
         }
         if (fb > 0.0) {
             rb += step;
-            RET(mass_at(rb, &fb));
+            RET(g_at(rb, &fb));
         }
     }
     double w = 0.0;  // weight of the rb field
     if (fa >= 0.0 && fb <= 0.0) {
-        for (int it = 0; it < 40 && rb - ra > 1e-9 * radius && fa != 0.0 && fb != 0.0; it++) {
+        for (int it = 0; it < 40 && rb - ra > 1e-9 * p0 && fa != 0.0 && fb != 0.0; it++) {
             const double rm = 0.5 * (ra + rb);
             double fm = 0;
-            RET(mass_at(rm, &fm));
+            RET(g_at(rm, &fm));
             if (fm >= 0.0) {
                 ra = rm;
                 fa = fm;
@@ -1661,9 +1663,9 @@ int mplb_mlp_init_bubble_mass(mplb_mlp_t* m, mplb_gpu_t* h, double t_ratio, cons
     double* tmp = nullptr;
     CK(cudaMalloc((void**)&tmp, (size_t)h->n * sizeof(double)));
     auto blend = [&]() -> int {
-        RET(mass_at(ra, &fa));
+        RET(g_at(ra, &fa));
         CK(cudaMemcpyAsync(tmp, h->rho, (size_t)h->n * sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
-        RET(mass_at(rb, &fb));
+        RET(g_at(rb, &fb));
         k_blend<<<blocks(h->n), TPB, 0, h->stream>>>(h->n, w, tmp, h->rho);
         h->launches++;
         RET(launch_check(h));
@@ -1679,8 +1681,50 @@ int mplb_mlp_init_bubble_mass(mplb_mlp_t* m, mplb_gpu_t* h, double t_ratio, cons
     const int rc = blend();
     cudaFree(tmp);
     if (rc) return rc;
-    if (radius_used) *radius_used = ra + w * (rb - ra);
+    if (used) *used = ra + w * (rb - ra);
     return 0;
+}
+
+int mplb_mlp_init_bubble_mass(mplb_mlp_t* m, mplb_gpu_t* h, double t_ratio, const double* center, double radius,
+                              double T, double target_mass, double* radius_used) {
+    if (!m || !h || !center) return fail(MPLB_E_ARG, "NULL argument");
+    if (!(radius > 0.0) || !(target_mass > 0.0)) return fail(MPLB_E_ARG, "radius and mass must be positive");
+    DeviceGuard guard(h->dev);
+    return place_with_mass(
+        h, [&](double R) { return mplb_mlp_init_bubble(m, h, t_ratio, center, R, T); }, radius, -1, target_mass,
+        radius_used);
+}
+
+int mplb_mlp_init_column(mplb_mlp_t* m, mplb_gpu_t* h, double t_ratio, int32_t axis, double center, double height,
+                         double T) {
+    if (!m || !h) return fail(MPLB_E_ARG, "NULL argument");
+    if (!(height > 0.0)) return fail(MPLB_E_ARG, "height must be positive");
+    if (!h->box) return fail(MPLB_E_UNSUPPORTED, "warm start needs a box lattice");
+    const int D = h->lat == MPLB_D2Q9 ? 2 : 3;
+    if (axis < 0 || axis >= D) return fail(MPLB_E_ARG, "axis must be 0 .. dimensions - 1");
+    if (h->P.eos != MPLB_EOS_CS) return fail(MPLB_E_UNSUPPORTED, "warm start is trained on the Carnahan-Starling EOS");
+    if (mplb_mlp_device(m) != h->dev) return fail(MPLB_E_ARG, "network and lattice on different devices");
+    DeviceGuard guard(h->dev);
+    RET(materialize(h));
+    RET(mplb_mlp_column_launch(m, h->rho, h->n, h->dims[0], h->dims[1], axis, h->dims[axis], center, height, t_ratio,
+                               h->P.a, h->P.b, h->stream));
+    h->launches++;
+    CK(cudaMemsetAsync(h->U, 0, 3 * (size_t)h->n * sizeof(double), h->stream));
+    k_fill<<<blocks(h->n), TPB, 0, h->stream>>>(h->n, T, h->T);
+    h->launches++;
+    RET(launch_check(h));
+    h->initialized = false;
+    return 0;
+}
+
+int mplb_mlp_init_column_mass(mplb_mlp_t* m, mplb_gpu_t* h, double t_ratio, int32_t axis, double center,
+                              double height, double T, double target_mass, double* height_used) {
+    if (!m || !h) return fail(MPLB_E_ARG, "NULL argument");
+    if (!(height > 0.0) || !(target_mass > 0.0)) return fail(MPLB_E_ARG, "height and mass must be positive");
+    DeviceGuard guard(h->dev);
+    return place_with_mass(
+        h, [&](double H) { return mplb_mlp_init_column(m, h, t_ratio, axis, center, H, T); }, height, +1,
+        target_mass, height_used);
 }
 
 int mplb_gpu_sync(mplb_gpu_t* h) {

@@ -74,11 +74,14 @@ __device__ inline float bf16_float(uint16_t b) { return __uint_as_float((uint32_
 // as the pair d = (r - R)/W and k = W/R (W = 5 lattice units, the initial
 // interface width; r/R = 1 + d k), so the interface sits at d = 0 with a
 // width independent of R and the curvature k carries the Laplace shift of
-// the bulk densities.  d is clamped to [-6, 6] (bulk beyond).  Rounded to
-// BF16 (GEMM operands).  Output: b * rho.
+// the bulk densities.  A flat interface (a liquid column or band) is the
+// limit R -> infinity: R = +inf, and r is then the signed distance to the
+// interface, positive on the liquid side (k = 0).  d is clamped to [-6, 6]
+// (bulk beyond).  Rounded to BF16 (GEMM operands).  Output: b * rho.
 constexpr double W_IFACE = 5.0;
 __host__ __device__ inline void features(double t_ratio, double a, double b, double r, double R, float* x) {
-    double d = (r - R) / W_IFACE;
+    const bool flat = R > 1.0e300;
+    double d = (flat ? r : r - R) / W_IFACE;
     d = d < -6.0 ? -6.0 : (d > 6.0 ? 6.0 : d);
     x[0] = bf16_round((float)((t_ratio - 0.775) / 0.175));
     x[1] = bf16_round((float)(a - 1.0));
@@ -459,6 +462,28 @@ __global__ void __launch_bounds__(TC_M) k_mlp_predict(const float* __restrict__ 
     if (tc_forward(s, x, out, kerr) && e < n) Y[e] = out;
 }
 
+// Initial density of a liquid band of a box lattice: along `axis`, nodes
+// within height/2 of `c` (periodic distance over the axis length `ext`) are
+// liquid; the feature distance is height/2 - |s - c|, a flat interface.
+__global__ void __launch_bounds__(TC_M) k_mlp_column(const float* __restrict__ P, const uint16_t* __restrict__ Wb,
+                                                     uint32_t n, int nx, int ny, int axis, int ext, double c,
+                                                     double height, double t_ratio, double a, double b,
+                                                     double* __restrict__ rho, int* __restrict__ kerr) {
+    TcBlock& s = tc_block();
+    tc_setup(s, P, Wb);
+    const uint32_t e = blockIdx.x * TC_M + threadIdx.x;
+    const uint32_t i = e < n ? e : 0;
+    const uint32_t coord = axis == 0 ? i % (uint32_t)nx
+                                     : (axis == 1 ? (i / (uint32_t)nx) % (uint32_t)ny : i / ((uint32_t)nx * (uint32_t)ny));
+    double ds = (double)coord - c;
+    if (ds > 0.5 * ext) ds -= ext;
+    if (ds < -0.5 * ext) ds += ext;
+    float f[NIN];
+    features(t_ratio, a, b, 0.5 * height - fabs(ds), INFINITY, f);
+    float out = 0.f;
+    if (tc_forward(s, f, out, kerr) && e < n) rho[e] = (double)out / b;
+}
+
 // Initial density of a box lattice: node i at (i % nx, i / nx % ny, i / (nx ny)),
 // r = distance to the bubble centre, rho = network(T/Tc, a, b, r/R) / b.
 __global__ void __launch_bounds__(TC_M) k_mlp_bubble(const float* __restrict__ P, const uint16_t* __restrict__ Wb,
@@ -488,6 +513,8 @@ int set_attrs() {
             err = cudaFuncSetAttribute(k_mlp_predict, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TC_SMEM);
         if (err == cudaSuccess)
             err = cudaFuncSetAttribute(k_mlp_bubble, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TC_SMEM);
+        if (err == cudaSuccess)
+            err = cudaFuncSetAttribute(k_mlp_column, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TC_SMEM);
     });
     return err == cudaSuccess ? 0 : mplb_internal_fail(MPLB_E_CUDA, std::string("MLP kernel attributes: ") +
                                                                        cudaGetErrorString(err));
@@ -616,6 +643,23 @@ int mplb_mlp_bubble_launch(mplb_mlp* m, double* rho, uint32_t n, int nx, int ny,
     cudaEventDestroy(ev);
     CKM(e);
     k_mlp_bubble<<<(n + TC_M - 1) / TC_M, TC_M, TC_SMEM, s>>>(m->P, m->Wb, n, nx, ny, c[0], c[1], c[2], R, t_ratio,
+                                                               a, b, rho, m->kerr);
+    CKM(cudaGetLastError());
+    return inference_status(m, s);
+}
+
+// Used by mplb_gpu.cu for mplb_mlp_init_column.
+int mplb_mlp_column_launch(mplb_mlp* m, double* rho, uint32_t n, int nx, int ny, int axis, int ext, double c,
+                           double height, double t_ratio, double a, double b, cudaStream_t s) {
+    DevGuard g(m->dev);
+    if (int rc = set_attrs()) return rc;
+    cudaEvent_t ev;
+    CKM(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+    cudaError_t e = cudaEventRecord(ev, m->stream);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(s, ev, 0);
+    cudaEventDestroy(ev);
+    CKM(e);
+    k_mlp_column<<<(n + TC_M - 1) / TC_M, TC_M, TC_SMEM, s>>>(m->P, m->Wb, n, nx, ny, axis, ext, c, height, t_ratio,
                                                                a, b, rho, m->kerr);
     CKM(cudaGetLastError());
     return inference_status(m, s);

@@ -1,7 +1,10 @@
-"""Learned warm start for static bubbles (mplb_mlp_* in include/mplb_gpu.h).
+"""Learned warm start for static bubbles and liquid columns (mplb_mlp_* in
+include/mplb_gpu.h).
 
     python -m multiphaselb_b200.warmstart train --lattice d2q9 --out weights.npz
     python -m multiphaselb_b200.warmstart evaluate --lattice d3q15 --weights weights.npz --cases 64
+    python -m multiphaselb_b200.warmstart train --geometry column
+    python -m multiphaselb_b200.warmstart evaluate --geometry column --cases 32
 
 Pipeline:
   1. converge a grid of bubbles (T/Tc, R) with the plain FP64 solver
@@ -16,7 +19,9 @@ None for inputs outside the trained ranges.  The converged plain solver is the
 judge: ``evaluate`` runs every case from both initial states to equilibrium
 and reports the steps, the wall time and the network's initial error against
 the converged profile.  One network per lattice family (2D and 3D bubbles
-have different Laplace pressures).
+have different Laplace pressures), and one for axial profiles: liquid bands
+(a column or layer) with flat interfaces, whose features carry R = +inf and
+the signed distance to the interface (mplb_mlp_init_column).
 """
 import argparse
 import ctypes as C
@@ -33,6 +38,8 @@ NPARAM = 8769
 HERE = os.path.dirname(os.path.abspath(__file__))
 DEFAULT_WEIGHTS = {abi.D2Q9: os.path.join(HERE, "data", "warmstart_d2q9.npz"),
                    abi.D3Q15: os.path.join(HERE, "data", "warmstart_d3q15.npz")}
+# axial profiles (liquid bands with flat interfaces), D2Q9
+COLUMN_WEIGHTS = os.path.join(HERE, "data", "warmstart_d2q9_column.npz")
 T_RANGE = (0.6, 0.95)
 CS_A, CS_B = 1.0, 4.0
 
@@ -55,6 +62,9 @@ def _lib():
             "mplb_mlp_predict": ([H, D, D, D, D, D, C.c_uint32, D], C.c_int),
             "mplb_mlp_init_bubble": ([H, H, C.c_double, D, C.c_double, C.c_double], C.c_int),
             "mplb_mlp_init_bubble_mass": ([H, H, C.c_double, D, C.c_double, C.c_double, C.c_double, D], C.c_int),
+            "mplb_mlp_init_column": ([H, H, C.c_double, C.c_int32, C.c_double, C.c_double, C.c_double], C.c_int),
+            "mplb_mlp_init_column_mass": ([H, H, C.c_double, C.c_int32, C.c_double, C.c_double, C.c_double,
+                                           C.c_double, D], C.c_int),
         }
         for name, (args, res) in sig.items():
             fn = getattr(lib, name)
@@ -150,6 +160,9 @@ class Network:
         c, cp = _f64(np.asarray(center, dtype=np.float64).ravel().tolist() + [0.0] * (3 - len(center)))
         self._check(self.lib.mplb_mlp_init_bubble(self.h, lat.h, t_ratio, cp, radius, T))
 
+    def init_column(self, lat, t_ratio, axis, center, height, T):
+        self._check(self.lib.mplb_mlp_init_column(self.h, lat.h, t_ratio, axis, center, height, T))
+
     def save(self, path):
         os.makedirs(os.path.dirname(os.path.abspath(path)), exist_ok=True)
         np.savez(path, params=self.params())
@@ -187,6 +200,62 @@ def profile_samples(case, rho, radius, rng, per_bin=48, bins=64):
             idx.append(rng.choice(sel, size=min(per_bin * (4 if k in (-1, bins) else 1), sel.size), replace=False))
     idx = np.concatenate(idx)
     return r[idx], rho[idx]
+
+
+def band_distance(case):
+    """Signed distance of every node to the nearest flat interface of a band
+    case, positive inside the liquid band (height/2 - |z - c|)."""
+    m = case.meta
+    return 0.5 * m["height"] - np.abs(case.points[:, m["axis"]] - m["center"])
+
+
+def band_samples(case, rho, rng, per_bin=48, bins=64):
+    """As profile_samples, in the signed distance to the interface; returns
+    (distance, rho)."""
+    dist = band_distance(case)
+    idx = []
+    edges = np.linspace(-30.0, 30.0, bins + 1)
+    which = np.digitize(dist, edges) - 1
+    for k in range(-1, bins + 1):
+        sel = np.flatnonzero(which == k)
+        if sel.size:
+            idx.append(rng.choice(sel, size=min(per_bin * (4 if k in (-1, bins) else 1), sel.size), replace=False))
+    idx = np.concatenate(idx)
+    return dist[idx], rho[idx]
+
+
+def band(L, height, t_ratio, nx=8):
+    """A D2Q9 liquid band across a periodic nx x L box (flat interfaces along x)."""
+    return cases.band_case(abi.D2Q9, dims=(nx, L), axis=1, height=height, width=5.0, t_ratio=t_ratio)
+
+
+def column_training_grid():
+    """(L, height, T/Tc) of the training bands."""
+    ts = np.linspace(T_RANGE[0], T_RANGE[1], 8)
+    return [(L, H, float(t)) for L, H in [(128, 48.0), (256, 112.0)] for t in ts]
+
+
+def build_column_training_set(grid=None, seed=1, log=None, **conv):
+    """Converged bands -> samples (T/Tc, distance, rho); R = +inf marks the
+    flat interface in the network's features."""
+    rng = np.random.default_rng(seed)
+    T, Dd, Y, meta = [], [], [], []
+    for L, H, t in grid or column_training_grid():
+        c = band(L, H, t)
+        rho, steps, rate, wall = converge(c, **conv)
+        if not np.isfinite(rate) or not np.all(np.isfinite(rho)):
+            if log:
+                log(f"column-set L={L} H={H} t={t:.3f}: diverged, skipped")
+            continue
+        d, y = band_samples(c, rho, rng)
+        T.append(np.full(d.size, t))
+        Dd.append(d)
+        Y.append(y)
+        meta.append(dict(L=L, height=H, t_ratio=t, steps=steps, rate=rate, wall_s=wall))
+        if log:
+            log(f"column-set L={L} H={H} t={t:.3f}: {steps} steps, {d.size} samples")
+    d = np.concatenate(Dd)
+    return np.concatenate(T), d, np.full(d.size, np.inf), np.concatenate(Y), meta
 
 
 def bubble(lattice, L, R, t_ratio):
@@ -274,6 +343,36 @@ def place(net, lat, t_ratio, centre_, R, T, mass):
     return used.value
 
 
+def place_column(net, lat, t_ratio, axis, center, height, T, mass):
+    """The network's band on the lattice holding `mass` (mplb_mlp_init_column_mass);
+    returns the effective height."""
+    used = C.c_double()
+    net._check(net.lib.mplb_mlp_init_column_mass(net.h, lat.h, t_ratio, axis, center, height, T, mass,
+                                                 C.byref(used)))
+    return used.value
+
+
+def column_initializer(weights=None, device=-1):
+    """As `initializer`, for band cases (cases.band_case) and the column network."""
+    path = weights or COLUMN_WEIGHTS
+    if not os.path.exists(path):
+        return None
+    net = Network.load(path, device)
+
+    def init(lat, case):
+        m = case.meta
+        t_ratio = m["T"] / m["Tc"]
+        if not (T_RANGE[0] - 1e-9 <= t_ratio <= T_RANGE[1] + 1e-9) or case.eos["type"] != abi.EOS_CS:
+            return False
+        mass = lat.mass_energy()[0]
+        init.radius = place_column(net, lat, t_ratio, m["axis"], m["center"], m["height"], m["T"], mass)
+        return True
+
+    init.net = net
+    init.radius = None
+    return init
+
+
 def initializer(lattice, weights=None, device=-1):
     """Function (lat, case) -> bool that overwrites a freshly uploaded bubble
     lattice with the network's profile (same mass as the uploaded state, see
@@ -301,10 +400,12 @@ def initializer(lattice, weights=None, device=-1):
 
 # ---------------------------------------------------------------- evaluation
 def evaluate(lattice, init, specs, K=1000, tol=1e-9, max_steps=400000, precision=abi.FP64, log=None):
-    """Both initial states to equilibrium for every spec (L, R, T/Tc)."""
+    """Both initial states to equilibrium for every spec (L, R, T/Tc; or L,
+    height, T/Tc for bands)."""
     rows = []
     for s in specs:
-        c = bubble(lattice, s["L"], s["radius"], s["t_ratio"])
+        c = band(s["L"], s["height"], s["t_ratio"]) if "height" in s else \
+            bubble(lattice, s["L"], s["radius"], s["t_ratio"])
         rec = dict(s)
         for mode in ("plain", "warm"):
             with Lattice(c, path=abi.PATH_FUSED, precision=precision) as lat:
@@ -331,7 +432,7 @@ def evaluate(lattice, init, specs, K=1000, tol=1e-9, max_steps=400000, precision
                 # the converged plain solver judges the network's initial profile
                 rec["init_err_max"] = float(np.abs(rho0 - rho_eq).max() / rho_eq.max())
                 rec["final_rel_diff"] = float(np.abs(rho - rho_eq).max() / rho_eq.max())
-                ctr = int(np.argmin(radial(c)))
+                ctr = int(np.argmin(radial(c))) if "height" not in s else int(np.argmin(np.abs(band_distance(c))))
                 rec["coexistence_rel_diff"] = float(max(abs(rho[ctr] - rho_eq[ctr]) / rho_eq[ctr],
                                                         abs(rho[0] - rho_eq[0]) / rho_eq[0]))
         rows.append(rec)
@@ -347,9 +448,19 @@ def draw_3d(n, seed=7):
     return [dict(L=128, radius=float(r), t_ratio=float(x)) for x, r in zip(t, R)]
 
 
+def draw_columns(n, seed=11):
+    rng = np.random.Generator(np.random.PCG64(seed))
+    L = rng.choice(np.array([128, 192, 256, 384]), size=n)
+    t = rng.uniform(0.6, 0.95, n)
+    h = rng.uniform(0.2, 0.6, n) * L
+    return [dict(L=int(a), height=float(b), t_ratio=float(x)) for a, b, x in zip(L, h, t)]
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("cmd", choices=("train", "evaluate"))
+    ap.add_argument("--geometry", choices=("bubble", "column"), default="bubble",
+                    help="column: liquid bands with flat interfaces (D2Q9, the column network)")
     ap.add_argument("--lattice", choices=("d2q9", "d3q15"), default="d3q15")
     ap.add_argument("--weights", default=None)
     ap.add_argument("--out", default=None)
@@ -362,9 +473,15 @@ def main(argv=None):
     lat = abi.D2Q9 if a.lattice == "d2q9" else abi.D3Q15
     prec = abi.FP64 if a.precision == "fp64" else abi.FP32_DEV
     log = lambda m: print(m, file=sys.stderr, flush=True)  # noqa: E731
+    column = a.geometry == "column"
+    if column:
+        lat = abi.D2Q9
     if a.cmd == "train":
         t0 = time.perf_counter()
-        t, r, R, rho, meta = build_training_set(lat, log=log, K=a.check, tol=a.tol)
+        if column:
+            t, r, R, rho, meta = build_column_training_set(log=log, K=a.check, tol=a.tol)
+        else:
+            t, r, R, rho, meta = build_training_set(lat, log=log, K=a.check, tol=a.tol)
         t1 = time.perf_counter()
         net = Network(seed=1)
         hist = train(net, t, r, R, rho, steps=a.steps)
@@ -373,13 +490,13 @@ def main(argv=None):
         rep = dict(samples=int(r.size), cases=meta, loss=hist, data_s=t1 - t0, train_s=t2 - t1,
                    fit_max_abs=float(np.abs(pred - rho).max()), fit_rms=float(np.sqrt(np.mean((pred - rho) ** 2))),
                    fit_max_rel=float(np.abs(pred / rho - 1.0).max()))
-        net.save(a.weights or DEFAULT_WEIGHTS[lat])
+        net.save(a.weights or (COLUMN_WEIGHTS if column else DEFAULT_WEIGHTS[lat]))
         txt = json.dumps(rep, indent=1)
     else:
-        init = initializer(lat, a.weights)
+        init = column_initializer(a.weights) if column else initializer(lat, a.weights)
         if init is None:
             raise SystemExit("no trained weights")
-        specs = draw_3d(a.cases) if lat == abi.D3Q15 else None
+        specs = draw_3d(a.cases) if lat == abi.D3Q15 else (draw_columns(a.cases) if column else None)
         if specs is None:
             from .ensemble import draw
             specs = draw(a.cases)

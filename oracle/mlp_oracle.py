@@ -35,8 +35,12 @@ def bf16(x):
 
 
 def features(t_ratio, a, b, r, R):
+    """Network inputs (multiphaselb_b200/csrc/mplb_mlp.cu features()); R = +inf
+    marks a flat interface, r then being the signed distance to it."""
     R = np.asarray(R, dtype=np.float64)
-    d = np.clip((np.asarray(r, dtype=np.float64) - R) / 5.0, -6.0, 6.0)
+    r = np.asarray(r, dtype=np.float64)
+    flat = np.isinf(R)
+    d = np.clip(np.where(flat, r, r - np.where(flat, 0.0, R)) / 5.0, -6.0, 6.0)
     cols = [(np.asarray(t_ratio, dtype=np.float64) - 0.775) / 0.175,
             np.asarray(a, dtype=np.float64) - 1.0,
             np.asarray(b, dtype=np.float64) * 0.25 - 1.0,

@@ -121,3 +121,52 @@ def test_warm_start_gains_over_tanh(gpu_lib):
     ctr = (c.dims[0] // 2) + c.dims[0] * (c.dims[1] // 2)
     for i in (ctr, 0):
         assert abs(rho_warm[i] - rho_eq[i]) < 1e-3 * rho_eq[i], (i, rho_warm[i], rho_eq[i])
+
+
+def test_init_column_equals_predict(gpu_lib):
+    """The axial warm start (a liquid band with flat interfaces) writes what
+    the network predicts for the signed distance to the interface with
+    R = +inf, bit for bit."""
+    c = cases.band_case(abi.D2Q9, dims=(8, 64), axis=1, height=24.0, width=4.0, t_ratio=0.8)
+    with warmstart.Network(seed=9) as net, Lattice(c, path=abi.PATH_FUSED) as lat:
+        lat.upload_case()
+        net.init_column(lat, 0.8, 1, c.meta["center"], 24.0, c.meta["T"])
+        lat.initialize()
+        out = lat.download()
+        want = net.predict(0.8, 1.0, 4.0, warmstart.band_distance(c), np.inf)
+    assert np.array_equal(out["rho"], want)
+    assert np.all(out["U"] == 0.0) and np.all(out["T"] == c.meta["T"])
+
+
+def test_column_warm_start_gains_over_tanh(gpu_lib):
+    """Train on converged liquid bands (flat interfaces), then start a held-out
+    band from the network with the mass of its tanh/Maxwell state.  The
+    converged plain solver judges: the network's initial profile is much
+    closer to the equilibrium than the tanh/Maxwell one, and both runs end at
+    the same coexistence densities."""
+    grid = [(64, H, t) for H in (18.0, 30.0) for t in (0.65, 0.75, 0.85, 0.95)]
+    K, tol = 500, 1e-9
+    t, d, R, rho, meta = warmstart.build_column_training_set(grid, K=K, tol=tol, max_steps=80000)
+    assert np.all(np.isinf(R))
+    with warmstart.Network(seed=2) as net:
+        warmstart.train(net, t, d, R, rho, steps=8000, batch=2048, lr=3e-3, lr_end=1e-4, chunks=8)
+        c = warmstart.band(64, 24.0, 0.8)
+        rho_eq, plain_steps, _, _ = warmstart.converge(c, K=K, tol=tol, max_steps=80000)
+        with Lattice(c, path=abi.PATH_FUSED) as lat:
+            lat.upload_case()
+            mass = lat.mass_energy()[0]
+            H_used = warmstart.place_column(net, lat, 0.8, 1, c.meta["center"], 24.0, c.meta["T"], mass)
+            assert abs(lat.mass_energy()[0] - mass) < 1e-9 * mass
+            lat.initialize()
+            rho_warm0 = lat.download()["rho"]
+            warm_steps, rate = lat.run_to_equilibrium(80000, K, tol)
+            rho_warm = lat.download()["rho"]
+    err_tanh = np.abs(c.rho - rho_eq).max()
+    err_warm = np.abs(rho_warm0 - rho_eq).max()
+    print("steps plain", plain_steps, "warm", warm_steps, "H", H_used, "init err tanh", err_tanh, "warm", err_warm)
+    assert rate < tol
+    assert err_warm < 0.5 * err_tanh
+    liquid = int(np.argmax(warmstart.band_distance(c)))
+    vapour = int(np.argmin(warmstart.band_distance(c)))
+    for i in (liquid, vapour):
+        assert abs(rho_warm[i] - rho_eq[i]) < 1e-3 * rho_eq[i], (i, rho_warm[i], rho_eq[i])

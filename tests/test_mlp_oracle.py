@@ -38,3 +38,17 @@ def test_features_match_library_host_code():
         want = np.ravel(mo.features(t, a, b, r, R)).astype(np.float32)
         got = warmstart.features(t, a, b, r, R)
         assert np.array_equal(got, want), (t, a, b, r, R, got, want)
+
+
+def test_flat_interface_features_match_library_host_code():
+    """R = +inf: r is the signed distance to a flat interface (liquid bands,
+    mplb_mlp_init_column); the curvature input is -1 (k = 0)."""
+    from multiphaselb_b200 import warmstart
+    rng = np.random.default_rng(6)
+    for _ in range(300):
+        t, d = rng.uniform(0.5, 1.0), rng.uniform(-40.0, 40.0)
+        want = np.ravel(mo.features(t, 1.0, 4.0, d, np.inf)).astype(np.float32)
+        got = warmstart.features(t, 1.0, 4.0, d, np.inf)
+        assert np.array_equal(got, want), (t, d, got, want)
+        assert got[4] == -1.0
+        assert got[3] == mo.bf16(np.float32(np.clip(d / 5.0, -6.0, 6.0) / 6.0))
