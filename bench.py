@@ -75,19 +75,23 @@ def peaks():
         return FALLBACK_HBM_GBS, "fallback"
 
 
-def profiled_traffic(workload, kernel):
-    """DRAM bytes per launch of the step kernel from the committed ncu summary."""
+def profiled_traffic(workload, kernel, tile_config=-1):
+    """DRAM bytes per launch of the step kernel from the committed ncu summary:
+    the line for this tile candidate (dram_bytes_per_full_launch_cfgN) where
+    the summary has one, else its only figure."""
     name = PROFILE_TRAFFIC.get((workload, kernel))
     if not name:
         return None
     path = os.path.join(ROOT, "profiles", name)
+    found = {}
     try:
         for line in open(path):
-            if line.startswith("dram_bytes_per_full_launch:"):
-                return float(line.split(":", 1)[1].split()[0])
+            if line.startswith("dram_bytes_per_full_launch"):
+                key, val = line.split(":", 1)
+                found[key.strip()] = float(val.split()[0])
     except OSError:
         return None
-    return None
+    return found.get(f"dram_bytes_per_full_launch_cfg{tile_config}", found.get("dram_bytes_per_full_launch"))
 
 
 class ClockSampler:
@@ -257,13 +261,13 @@ def measure(case, path, precision, steps, warmup, local, stream, flush, world, d
 
 
 def kernel_name(case, precision, tile_config=-1):
-    """The step kernel the autotuner picked (3D candidates 6 and 7 are the TMA-staged kernel)."""
+    """The step kernel the autotuner picked (3D candidates 6 to 9 are the TMA-staged kernel)."""
     from multiphaselb_b200 import abi
     if precision == abi.FP32_DEV:
         return "k_fused32_d2q9" if case.lattice == abi.D2Q9 else "k_fused32_d3q15"
     if case.lattice == abi.D2Q9:
         return "k_fused_d2q9"
-    return "k_fused_d3q15_tma" if tile_config in (6, 7) else "k_fused_d3q15"
+    return "k_fused_d3q15_tma" if tile_config in (6, 7, 8, 9) else "k_fused_d3q15"
 
 
 def time_to_equilibrium(ncases):
@@ -318,7 +322,7 @@ def run_ours(a):
             "ms_per_step": round(total_ms / steps, 6),
             "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                          "frac": round(achieved / peak, 4), "peak_source": peak_source,
-                         "traffic": profiled_traffic(name, kname), "kernel": kname,
+                         "traffic": profiled_traffic(name, kname, r64["info"]["tile_config"]), "kernel": kname,
                          "kernel_ms": round(kernel_ms, 6)},
         }
         if not a.no_fp32:

@@ -878,13 +878,14 @@ struct TileCfg {
                  // on large lattices; a lattice of one wave prefers the smaller general kernel)
     bool tma;    // 3D only: planes staged by TMA (k_fused_d3q15_tma; fully periodic boxes)
 };
-constexpr int N_CFG2 = 8, N_CFG3 = 8, N_CFG_MAX = 8;
+constexpr int N_CFG2 = 8, N_CFG3 = 10, N_CFG_MAX = 10;
 constexpr TileCfg CFG2[N_CFG2] = {{32, 8, false, 0, false}, {32, 4, false, 0, false}, {64, 4, false, 0, false},
                                   {16, 8, false, 0, true},  {64, 4, false, 0, true},  {16, 8, false, 6, true},
                                   {32, 8, false, 3, true},  {32, 4, false, 8, true}};
 constexpr TileCfg CFG3[N_CFG3] = {{32, 8, false, 0, false}, {32, 8, true, 0, false}, {32, 4, false, 0, false},
                                   {64, 4, false, 0, false}, {32, 16, false, 0, false}, {64, 8, false, 0, false},
-                                  {32, 4, false, 3, false, true}, {32, 8, false, 2, false, true}};
+                                  {32, 4, false, 3, false, true}, {32, 8, false, 2, false, true},
+                                  {32, 16, false, 1, false, true}, {64, 8, false, 1, false, true}};
 
 struct Geom {
     int tiles_x, tiles_y, zchunk, nblocks;  // nblocks 0: the candidate does not take this lattice

@@ -119,6 +119,10 @@ inline cudaError_t fused_attributes() {
                              (int)TmaTile<32, 4>::SMEM));
     chk(cudaFuncSetAttribute(k_fused_d3q15_tma<32, 8, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)TmaTile<32, 8>::SMEM));
+    chk(cudaFuncSetAttribute(k_fused_d3q15_tma<32, 16, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)TmaTile<32, 16>::SMEM));
+    chk(cudaFuncSetAttribute(k_fused_d3q15_tma<64, 8, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)TmaTile<64, 8>::SMEM));
     return e;
 }
 
@@ -208,7 +212,9 @@ inline cudaError_t fused_launch_cfg(FusedConfig& fc, int cfg, const Params& P, F
             case 4: launch3<32, 16, false, false>(bc, nb, P, A, s); break;
             case 5: launch3<64, 8, false, false>(bc, nb, P, A, s); break;
             case 6: if (cudaError_t e = launch3_tma<32, 4, 3>(fc, cfg, nb, P, A, s)) return e; break;
-            default: if (cudaError_t e = launch3_tma<32, 8, 2>(fc, cfg, nb, P, A, s)) return e; break;
+            case 7: if (cudaError_t e = launch3_tma<32, 8, 2>(fc, cfg, nb, P, A, s)) return e; break;
+            case 8: if (cudaError_t e = launch3_tma<32, 16, 1>(fc, cfg, nb, P, A, s)) return e; break;
+            default: if (cudaError_t e = launch3_tma<64, 8, 1>(fc, cfg, nb, P, A, s)) return e; break;
             }
         }
     }

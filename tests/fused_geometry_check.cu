@@ -203,10 +203,13 @@ int main() {
     int dims3[][3] = {{2, 2, 2}, {10, 8, 6}, {8, 6, 7}, {33, 9, 17}, {40, 40, 40}, {70, 20, 30}, {40, 24, 100}};
     for (auto& d : dims3)
         for (int p = 0; p < 8; p++) { check<D3Q15T>(d[0], d[1], d[2], p & 1, (p >> 1) & 1, (p >> 2) & 1); cases++; }
-    int dims_tma[][3] = {{32, 8, 2}, {64, 16, 9}, {96, 40, 33}, {192, 192, 12}, {128, 128, 128}, {64, 8, 64}};
+    int dims_tma[][3] = {{32, 8, 2},      {64, 16, 9},     {96, 40, 33},   {192, 192, 12},
+                         {128, 128, 128}, {64, 8, 64},     {192, 48, 6},   {192, 192, 192}, {128, 64, 5}};
     for (auto& d : dims_tma) {
         check_tma<32, 4, 3>(d[0], d[1], d[2]);
         check_tma<32, 8, 2>(d[0], d[1], d[2]);
+        check_tma<32, 16, 1>(d[0], d[1], d[2]);
+        check_tma<64, 8, 1>(d[0], d[1], d[2]);
         cases++;
     }
     if (fails) { printf("FAILED %d checks\n", fails); return 1; }
