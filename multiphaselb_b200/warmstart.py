@@ -16,7 +16,7 @@ Pipeline:
 
 The tanh/Maxwell initial state stays the fallback: ``initializer`` returns
 None for inputs outside the trained ranges.  The converged plain solver is the
-judge: ``evaluate`` runs every case from both initial states to equilibrium
+yardstick: ``evaluate`` runs every case from both initial states to equilibrium
 and reports the steps, the wall time and the network's initial error against
 the converged profile.  One network per lattice family (2D and 3D bubbles
 have different Laplace pressures), and one for axial profiles: liquid bands
@@ -429,7 +429,7 @@ def evaluate(lattice, init, specs, K=1000, tol=1e-9, max_steps=400000, precision
                 rho_eq = rho
                 rec["tanh_err_max"] = float(np.abs(c.rho - rho_eq).max() / rho_eq.max())
             elif not rec["plain"]["diverged"] and not rec["warm"]["diverged"]:
-                # the converged plain solver judges the network's initial profile
+                # the converged plain solver is the yardstick of the network's initial profile
                 rec["init_err_max"] = float(np.abs(rho0 - rho_eq).max() / rho_eq.max())
                 rec["final_rel_diff"] = float(np.abs(rho - rho_eq).max() / rho_eq.max())
                 ctr = int(np.argmin(radial(c))) if "height" not in s else int(np.argmin(np.abs(band_distance(c))))

@@ -1,7 +1,7 @@
 """Warm-start network on the device (mplb_mlp_*): forward pass and gradients
 against the CPU oracle (oracle/mlp_oracle.py), training, lattice
 initialisation, and what the trained network gains over the tanh/Maxwell
-initial state on small bubbles judged by the converged plain solver."""
+initial state on small bubbles, measured against the converged plain solver."""
 import numpy as np
 import pytest
 
@@ -141,7 +141,7 @@ def test_init_column_equals_predict(gpu_lib):
 def test_column_warm_start_gains_over_tanh(gpu_lib):
     """Train on converged liquid bands (flat interfaces), then start a held-out
     band from the network with the mass of its tanh/Maxwell state.  The
-    converged plain solver judges: the network's initial profile is much
+    converged plain solver is the yardstick: the network's initial profile is much
     closer to the equilibrium than the tanh/Maxwell one, and both runs end at
     the same coexistence densities."""
     grid = [(64, H, t) for H in (18.0, 30.0) for t in (0.65, 0.75, 0.85, 0.95)]
