@@ -483,7 +483,7 @@ __global__ void __launch_bounds__(256) k_pullsum_d2q9(Params P, FusedArgs A) {
 // tiles skip the wrap / missing-source / boundary bookkeeping; the
 // arithmetic is the same code either way.
 template <int F2_TX, int F2_TY, bool F_ON, bool G_ON, bool HAS_BC, bool EMIT, bool INNER, int EX, int EY, int GX,
-          int GY, bool MY = false>
+          int GY, bool MY = false, int RINGW = 0>
 __device__ __forceinline__ void fused2_tile(const Params& P, const FusedArgs& A, int x0, int y0,
                                             double (*s_psi)[EX], double (*s_inv)[GX], double (*s_To)[GX],
                                             double (*s_U0)[GX], double (*s_U1)[GX]) {
@@ -544,29 +544,46 @@ __device__ __forceinline__ void fused2_tile(const Params& P, const FusedArgs& A,
         return true;
     };
 
-    {
+    // RINGW > 0: the block has RINGW more warps after its TX x TY node
+    // threads, one thread per ring slot, so every thread fills one slot
+    // before the barrier (a node thread: its own node) through one copy of
+    // the slot code; RINGW == 0: the node threads fill the ring first.
+    constexpr int NT = F2_TX * F2_TY;
+    static_assert(RINGW == 0 || NRING <= 32 * RINGW, "one ring slot per ring thread");
+    const bool ringer = RINGW > 0 && (int)threadIdx.x >= NT;
+    if (!ringer) {
         // the own node's loads start now; the ring work below overlaps them
         const int px = x0 + tx, py = y0 + ty;
         if (px < A.nx && py < A.ny)
             prefetch_node<L, F_ON, G_ON>(P, A, px, py, (uint32_t)px + (uint32_t)A.nx * (uint32_t)py);
     }
-    // the ring first, so the own node's populations are live only across the barrier
-    for (int r = threadIdx.x; r < NRING; r += blockDim.x) {
-        int ex, ey;
-        ring_slot(r, F2_TX, F2_TY, ex, ey);
-        double rf[9], rg[9], rrho, rt, rrr;
-        EosRho rer;
-        uint32_t rid;
-        slot(ex, ey, rf, rg, rrho, rt, rid, false, rrr, rer);
+    if constexpr (RINGW == 0) {
+        // the ring first, so the own node's populations are live only across the barrier
+        for (int r = threadIdx.x; r < NRING; r += blockDim.x) {
+            int ex, ey;
+            ring_slot(r, F2_TX, F2_TY, ex, ey);
+            double rf[9], rg[9], rrho, rt, rrr;
+            EosRho rer;
+            uint32_t rid;
+            slot(ex, ey, rf, rg, rrho, rt, rid, false, rrr, rer);
+        }
     }
     double f[9], g[9], rho = 0, T = 0, rr = 0;
     EosRho er{};
     uint32_t id = 0;
     const int gx = x0 + tx, gy = y0 + ty;
-    const bool own = INNER || (gx < A.nx && gy < A.ny);
+    const bool own = !ringer && (INNER || (gx < A.nx && gy < A.ny));
     // interior slot (threads outside the box still fill the slot of the
-    // wrapped node, so partial tiles see their periodic neighbours)
-    const bool have = slot(tx + 1, ty + 1, f, g, rho, T, id, own, rr, er);
+    // wrapped node, so partial tiles see their periodic neighbours); a ring
+    // thread's slot is its ring slot
+    int sx = tx + 1, sy = ty + 1;
+    bool act = true;
+    if (ringer) {
+        const int r = (int)threadIdx.x - NT;
+        act = r < NRING;
+        if (act) ring_slot(r, F2_TX, F2_TY, sx, sy);
+    }
+    const bool have = act && slot(sx, sy, f, g, rho, T, id, own, rr, er);
     __syncthreads();
     if (!own || !have) return;
 
@@ -615,9 +632,11 @@ __device__ __forceinline__ void fused2_tile(const Params& P, const FusedArgs& A,
 // instruction footprint, which a lattice of one wave notices).
 // MY: the thermal field is myMRT (T = sum g'' + S/2; non-EMIT steps follow
 // k_pullsum_d2q9).
+// RINGW: warps added to the block that compute the tile's ring (launch with
+// TX * TY + 32 * RINGW threads); 0: the node threads compute it first.
 template <int F2_TX, int F2_TY, int MINB, bool F_ON, bool G_ON, bool HAS_BC, bool EMIT, bool TRY_INNER = false,
-          bool MY = false>
-__global__ void __launch_bounds__(F2_TX * F2_TY, MINB ? MINB : min_blocks(F2_TX * F2_TY))
+          bool MY = false, int RINGW = 0>
+__global__ void __launch_bounds__(F2_TX * F2_TY + 32 * RINGW, MINB ? MINB : min_blocks(F2_TX * F2_TY))
     k_fused_d2q9(Params P, FusedArgs A) {
     step_dependency_wait();
     constexpr int EX = F2_TX + 2, EY = F2_TY + 2;
@@ -631,13 +650,13 @@ __global__ void __launch_bounds__(F2_TX * F2_TY, MINB ? MINB : min_blocks(F2_TX 
     const int x0 = bx * F2_TX, y0 = by * F2_TY;
     if constexpr (TRY_INNER) {
         if (inner_tile<F2_TX, F2_TY>(A, x0, y0)) {
-            fused2_tile<F2_TX, F2_TY, F_ON, G_ON, HAS_BC, EMIT, true, EX, EY, GX, GY, MY>(P, A, x0, y0, s_psi, s_inv,
-                                                                                          s_To, s_U0, s_U1);
+            fused2_tile<F2_TX, F2_TY, F_ON, G_ON, HAS_BC, EMIT, true, EX, EY, GX, GY, MY, RINGW>(
+                P, A, x0, y0, s_psi, s_inv, s_To, s_U0, s_U1);
             return;
         }
     }
-    fused2_tile<F2_TX, F2_TY, F_ON, G_ON, HAS_BC, EMIT, false, EX, EY, GX, GY, MY>(P, A, x0, y0, s_psi, s_inv, s_To,
-                                                                                   s_U0, s_U1);
+    fused2_tile<F2_TX, F2_TY, F_ON, G_ON, HAS_BC, EMIT, false, EX, EY, GX, GY, MY, RINGW>(P, A, x0, y0, s_psi, s_inv,
+                                                                                          s_To, s_U0, s_U1);
 }
 
 // ------------------------------------------------------------ 3D kernels
@@ -877,11 +896,13 @@ struct TileCfg {
     bool inner;  // 2D only: the kernel variant whose inner tiles take the lean body (pays off
                  // on large lattices; a lattice of one wave prefers the smaller general kernel)
     bool tma;    // 3D only: planes staged by TMA (k_fused_d3q15_tma; fully periodic boxes)
+    int ringw;   // 2D only: added warps that compute the ring (k_fused_d2q9 RINGW)
 };
-constexpr int N_CFG2 = 8, N_CFG3 = 10, N_CFG_MAX = 10;
+constexpr int N_CFG2 = 10, N_CFG3 = 10, N_CFG_MAX = 10;
 constexpr TileCfg CFG2[N_CFG2] = {{32, 8, false, 0, false}, {32, 4, false, 0, false}, {64, 4, false, 0, false},
                                   {16, 8, false, 0, true},  {64, 4, false, 0, true},  {16, 8, false, 6, true},
-                                  {32, 8, false, 3, true},  {32, 4, false, 8, true}};
+                                  {32, 8, false, 3, true},  {32, 4, false, 8, true},
+                                  {32, 8, false, 2, false, false, 3}, {16, 8, false, 4, false, false, 2}};
 constexpr TileCfg CFG3[N_CFG3] = {{32, 8, false, 0, false}, {32, 8, true, 0, false}, {32, 4, false, 0, false},
                                   {64, 4, false, 0, false}, {32, 16, false, 0, false}, {64, 8, false, 0, false},
                                   {32, 4, false, 3, false, true}, {32, 8, false, 2, false, true},

@@ -134,10 +134,11 @@ cudaError_t launch3_tma(FusedConfig& fc, int cfg, int nb, const Params& P, const
     return cudaSuccess;
 }
 
-template <int TX, int TY, int MINB, bool F_ON, bool G_ON, bool EMIT, bool INNER, bool MY = false>
+template <int TX, int TY, int MINB, bool F_ON, bool G_ON, bool EMIT, bool INNER, bool MY = false, int RINGW = 0>
 void launch2(bool bc, int nb, const Params& P, const FusedArgs& A, cudaStream_t s) {
-    if (bc) launch_step(k_fused_d2q9<TX, TY, MINB, F_ON, G_ON, true, EMIT, INNER, MY>, nb, TX * TY, 0, s, P, A);
-    else launch_step(k_fused_d2q9<TX, TY, MINB, F_ON, G_ON, false, EMIT, INNER, MY>, nb, TX * TY, 0, s, P, A);
+    constexpr int nt = TX * TY + 32 * RINGW;
+    if (bc) launch_step(k_fused_d2q9<TX, TY, MINB, F_ON, G_ON, true, EMIT, INNER, MY, RINGW>, nb, nt, 0, s, P, A);
+    else launch_step(k_fused_d2q9<TX, TY, MINB, F_ON, G_ON, false, EMIT, INNER, MY, RINGW>, nb, nt, 0, s, P, A);
 }
 
 // myMRT steps first fill rho_a, gsum_a (k_pullsum_d2q9).
@@ -148,7 +149,7 @@ void launch_pullsum(bool bc, const Params& P, const FusedArgs& A, cudaStream_t s
     else launch_step(k_pullsum_d2q9<F_ON, false>, nb, 256, 0, s, P, A);
 }
 
-template <int TX, int TY, bool EMIT, int MINB = 0, bool INNER = false>
+template <int TX, int TY, bool EMIT, int MINB = 0, bool INNER = false, int RINGW = 0>
 void launch2_fg(bool fon, bool gon, bool bc, int nb, const Params& P, const FusedArgs& A, cudaStream_t s) {
     const bool my = gon && P.g_model == MPLB_MYMRT;
     if (my) {
@@ -156,13 +157,13 @@ void launch2_fg(bool fon, bool gon, bool bc, int nb, const Params& P, const Fuse
             if (fon) launch_pullsum<true>(bc, P, A, s);
             else launch_pullsum<false>(bc, P, A, s);
         }
-        if (fon) launch2<TX, TY, MINB, true, true, EMIT, INNER, true>(bc, nb, P, A, s);
-        else launch2<TX, TY, MINB, false, true, EMIT, INNER, true>(bc, nb, P, A, s);
+        if (fon) launch2<TX, TY, MINB, true, true, EMIT, INNER, true, RINGW>(bc, nb, P, A, s);
+        else launch2<TX, TY, MINB, false, true, EMIT, INNER, true, RINGW>(bc, nb, P, A, s);
         return;
     }
-    if (fon && gon) launch2<TX, TY, MINB, true, true, EMIT, INNER>(bc, nb, P, A, s);
-    else if (fon) launch2<TX, TY, MINB, true, false, EMIT, INNER>(bc, nb, P, A, s);
-    else if (gon) launch2<TX, TY, MINB, false, true, EMIT, INNER>(bc, nb, P, A, s);
+    if (fon && gon) launch2<TX, TY, MINB, true, true, EMIT, INNER, false, RINGW>(bc, nb, P, A, s);
+    else if (fon) launch2<TX, TY, MINB, true, false, EMIT, INNER, false, RINGW>(bc, nb, P, A, s);
+    else if (gon) launch2<TX, TY, MINB, false, true, EMIT, INNER, false, RINGW>(bc, nb, P, A, s);
 }
 
 template <int TX, int TY, bool PIPE, bool EMIT>
@@ -197,7 +198,9 @@ inline cudaError_t fused_launch_cfg(FusedConfig& fc, int cfg, const Params& P, F
             case 4: launch2_fg<64, 4, false, 0, true>(f_on, g_on, bc, nb, P, A, s); break;
             case 5: launch2_fg<16, 8, false, 6, true>(f_on, g_on, bc, nb, P, A, s); break;
             case 6: launch2_fg<32, 8, false, 3, true>(f_on, g_on, bc, nb, P, A, s); break;
-            default: launch2_fg<32, 4, false, 8, true>(f_on, g_on, bc, nb, P, A, s); break;
+            case 7: launch2_fg<32, 4, false, 8, true>(f_on, g_on, bc, nb, P, A, s); break;
+            case 8: launch2_fg<32, 8, false, 2, false, 3>(f_on, g_on, bc, nb, P, A, s); break;
+            default: launch2_fg<16, 8, false, 4, false, 2>(f_on, g_on, bc, nb, P, A, s); break;
             }
         }
     } else {
@@ -227,49 +230,54 @@ inline cudaError_t fused_launch(FusedConfig& fc, const Params& P, const FusedArg
     return fused_launch_cfg(fc, fc.cfg, P, A, f_on, g_on, emit, s);
 }
 
-// Time every candidate on the current state (2 warm-up launches, then the
-// median of 10)
-// and keep the fastest.  The step's outputs are rewritten by the real launch
-// that follows; the heat-source history S, updated in place, is saved to
-// `save` before and restored after every trial.
+// Time every candidate on the current state and keep the fastest: 2 warm-up
+// launches, then 10 timed ones, all queued back to back with an event between
+// consecutive launches and one host wait at the end, so a launch's interval
+// holds its device time only (a host wait between launches would add the
+// host's launch latency, several microseconds, to every interval: on a
+// lattice of one wave that is as large as the differences between
+// candidates).  The median interval is kept.  The step's outputs are
+// rewritten by the real launch that follows; the heat-source history S,
+// updated in place, is saved to `save` before and restored after every
+// candidate's launches.
 inline int fused_autotune(FusedConfig& fc, const Params& P, const FusedArgs& A, bool f_on, bool g_on, double* S,
                           double* save, size_t n, cudaStream_t s) {
-    cudaEvent_t e0, e1;
-    if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess) {
+    constexpr int WARM = 2, TIMED = 10;
+    cudaEvent_t ev[TIMED + 1];
+    int made = 0;
+    for (; made < TIMED + 1; made++)
+        if (cudaEventCreate(&ev[made]) != cudaSuccess) break;
+    if (made < TIMED + 1) {
+        for (int i = 0; i < made; i++) cudaEventDestroy(ev[i]);
         fc.err = "autotune: event creation failed";
         return MPLB_E_CUDA;
     }
     const bool keep_s = g_on && S && save;
     if (keep_s && cudaMemcpyAsync(save, S, n * sizeof(double), cudaMemcpyDeviceToDevice, s) != cudaSuccess) {
+        for (int i = 0; i < TIMED + 1; i++) cudaEventDestroy(ev[i]);
         fc.err = "autotune: saving S failed";
         return MPLB_E_CUDA;
     }
-    // 2 warm-up launches, then the median of 10 timed ones (a one-wave
-    // lattice's step is ~10 us: a few launches give a noisy pick)
-    constexpr int WARM = 2, TIMED = 10;
     float best = 1e30f;
     int best_cfg = 0;
     for (int c = 0; c < fc.ncfg; c++) {
-        float ms_r[TIMED];
-        int nt = 0;
         bool ok = fc.geom[c].nblocks > 0;
         for (int r = 0; r < WARM + TIMED && ok; r++) {
-            if (r >= WARM) cudaEventRecord(e0, s);
+            if (r >= WARM) cudaEventRecord(ev[r - WARM], s);
             ok = fused_launch_cfg(fc, c, P, A, f_on, g_on, false, s) == cudaSuccess;
-            if (r >= WARM) {
-                cudaEventRecord(e1, s);
-                cudaEventSynchronize(e1);
-                float ms = 0;
-                cudaEventElapsedTime(&ms, e0, e1);
-                ms_r[nt++] = ms;
-            }
-            if (keep_s) cudaMemcpyAsync(S, save, n * sizeof(double), cudaMemcpyDeviceToDevice, s);
         }
+        if (ok) cudaEventRecord(ev[TIMED], s);
         float med = -1.0f;
-        if (ok && nt == TIMED) {
-            std::sort(ms_r, ms_r + nt);
-            med = 0.5f * (ms_r[nt / 2 - 1] + ms_r[nt / 2]);
+        if (ok && cudaEventSynchronize(ev[TIMED]) == cudaSuccess) {
+            float ms_r[TIMED];
+            for (int r = 0; r < TIMED; r++) {
+                ms_r[r] = 0;
+                cudaEventElapsedTime(&ms_r[r], ev[r], ev[r + 1]);
+            }
+            std::sort(ms_r, ms_r + TIMED);
+            med = 0.5f * (ms_r[TIMED / 2 - 1] + ms_r[TIMED / 2]);
         }
+        if (keep_s) cudaMemcpyAsync(S, save, n * sizeof(double), cudaMemcpyDeviceToDevice, s);
         fc.tune_ms[c] = ok ? med : -1.0f;
         if (ok && med >= 0 && med < best) {
             best = med;
@@ -277,8 +285,7 @@ inline int fused_autotune(FusedConfig& fc, const Params& P, const FusedArgs& A, 
         }
     }
     cudaGetLastError();
-    cudaEventDestroy(e0);
-    cudaEventDestroy(e1);
+    for (int i = 0; i < TIMED + 1; i++) cudaEventDestroy(ev[i]);
     fc.cfg = best_cfg;
     fc.nblocks = fc.geom[best_cfg].nblocks;
     fc.tuned = true;

@@ -217,9 +217,10 @@ def test_every_tile_candidate_is_exact(gpu_lib, name):
     from multiphaselb_b200 import Lattice, MplbError
     case = small_cases()[name]
     want = run_checker("port", case, 4)
-    # 2D: 8 shapes; 3D: 6 shapes, then 2 TMA-staged ones (fully periodic
-    # boxes whose extents the tile divides only)
-    ncand = 8
+    # 2D: 10 shapes (the last two with added ring warps); 3D: 6 shapes, then
+    # 4 TMA-staged ones (fully periodic boxes whose extents the tile divides
+    # only)
+    ncand = 10
     ran = []
     for c in range(1, ncand + 1):
         with Lattice(case, path=abi.PATH_FUSED, tile_config=c) as lat:
@@ -233,7 +234,7 @@ def test_every_tile_candidate_is_exact(gpu_lib, name):
             assert lat.info()["tile_config"] == c - 1
             assert_same(lat.download(), want, ctx=f"{name} tile candidate {c - 1}")
             ran.append(c)
-    assert set(range(1, 7 if case.lattice == abi.D3Q15 else 9)) <= set(ran), ran
+    assert set(range(1, 7 if case.lattice == abi.D3Q15 else 11)) <= set(ran), ran
     with Lattice(case, path=abi.PATH_FUSED) as lat:
         lat.upload_case()
         lat.initialize()
