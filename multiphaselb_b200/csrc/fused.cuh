@@ -551,8 +551,9 @@ __device__ __forceinline__ void fused2_tile(const Params& P, const FusedArgs& A,
     constexpr int NT = F2_TX * F2_TY;
     static_assert(RINGW == 0 || NRING <= 32 * RINGW, "one ring slot per ring thread");
     const bool ringer = RINGW > 0 && (int)threadIdx.x >= NT;
-    if (!ringer) {
+    if (RINGW == 0) {
         // the own node's loads start now; the ring work below overlaps them
+        // (with ring warps the node threads load their pulls at once)
         const int px = x0 + tx, py = y0 + ty;
         if (px < A.nx && py < A.ny)
             prefetch_node<L, F_ON, G_ON>(P, A, px, py, (uint32_t)px + (uint32_t)A.nx * (uint32_t)py);
