@@ -409,6 +409,7 @@ def run_ours(a):
         "steady_state": {"ms_per_step": round(r64["steady_ms"], 6), "value": round(n / (r64["steady_ms"] * 1e-3) / 1e9, 4),
                          "unit": "GLUPS", "note": "no L2 flush between steps (informational, not the headline)"},
         "tile_config": info["tile_config"],
+        "tile_ms": [round(t, 5) for t in info["tile_ms"] if t != 0.0],
         "clocks": r64["clocks"],
     }
     if "fp32_dev" in head:

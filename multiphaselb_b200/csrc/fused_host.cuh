@@ -230,19 +230,21 @@ inline cudaError_t fused_launch(FusedConfig& fc, const Params& P, const FusedArg
     return fused_launch_cfg(fc, fc.cfg, P, A, f_on, g_on, emit, s);
 }
 
-// Time every candidate on the current state and keep the fastest: 2 warm-up
-// launches, then 10 timed ones, all queued back to back with an event between
-// consecutive launches and one host wait at the end, so a launch's interval
-// holds its device time only (a host wait between launches would add the
-// host's launch latency, several microseconds, to every interval: on a
-// lattice of one wave that is as large as the differences between
-// candidates).  The median interval is kept.  The step's outputs are
-// rewritten by the real launch that follows; the heat-source history S,
-// updated in place, is saved to `save` before and restored after every
-// candidate's launches.
+// Time every candidate on the current state and keep the fastest.  Three
+// sweeps over the candidates (so a transient -- clocks settling, another
+// process -- does not favour the candidates timed during it); in each, a
+// candidate's warm-up launch and 8 timed launches are queued back to back
+// with an event between consecutive launches and one host wait at the end,
+// so a launch's interval holds its device time only (a host wait between
+// launches would add the host's launch latency, several microseconds, to
+// every interval: on a lattice of one wave that is as large as the
+// differences between candidates).  A candidate's time is the median of its
+// 24 intervals.  The step's outputs are rewritten by the real launch that
+// follows; the heat-source history S, updated in place, is saved to `save`
+// before and restored after every candidate's launches.
 inline int fused_autotune(FusedConfig& fc, const Params& P, const FusedArgs& A, bool f_on, bool g_on, double* S,
                           double* save, size_t n, cudaStream_t s) {
-    constexpr int WARM = 2, TIMED = 10;
+    constexpr int SWEEPS = 3, WARM = 1, TIMED = 8;
     cudaEvent_t ev[TIMED + 1];
     int made = 0;
     for (; made < TIMED + 1; made++)
@@ -258,28 +260,41 @@ inline int fused_autotune(FusedConfig& fc, const Params& P, const FusedArgs& A, 
         fc.err = "autotune: saving S failed";
         return MPLB_E_CUDA;
     }
+    float ms_all[N_CFG_MAX][SWEEPS * TIMED];
+    bool ok_c[N_CFG_MAX];
+    for (int c = 0; c < fc.ncfg; c++) ok_c[c] = fc.geom[c].nblocks > 0;
+    for (int sw = 0; sw < SWEEPS; sw++) {
+        for (int c = 0; c < fc.ncfg; c++) {
+            bool ok = ok_c[c];
+            for (int r = 0; r < WARM + TIMED && ok; r++) {
+                if (r >= WARM) cudaEventRecord(ev[r - WARM], s);
+                ok = fused_launch_cfg(fc, c, P, A, f_on, g_on, false, s) == cudaSuccess;
+            }
+            if (ok) cudaEventRecord(ev[TIMED], s);
+            if (ok && cudaEventSynchronize(ev[TIMED]) == cudaSuccess) {
+                for (int r = 0; r < TIMED; r++) {
+                    float ms = 0;
+                    cudaEventElapsedTime(&ms, ev[r], ev[r + 1]);
+                    ms_all[c][sw * TIMED + r] = ms;
+                }
+            } else {
+                ok = false;
+            }
+            if (keep_s) cudaMemcpyAsync(S, save, n * sizeof(double), cudaMemcpyDeviceToDevice, s);
+            ok_c[c] = ok;
+        }
+    }
     float best = 1e30f;
     int best_cfg = 0;
     for (int c = 0; c < fc.ncfg; c++) {
-        bool ok = fc.geom[c].nblocks > 0;
-        for (int r = 0; r < WARM + TIMED && ok; r++) {
-            if (r >= WARM) cudaEventRecord(ev[r - WARM], s);
-            ok = fused_launch_cfg(fc, c, P, A, f_on, g_on, false, s) == cudaSuccess;
-        }
-        if (ok) cudaEventRecord(ev[TIMED], s);
         float med = -1.0f;
-        if (ok && cudaEventSynchronize(ev[TIMED]) == cudaSuccess) {
-            float ms_r[TIMED];
-            for (int r = 0; r < TIMED; r++) {
-                ms_r[r] = 0;
-                cudaEventElapsedTime(&ms_r[r], ev[r], ev[r + 1]);
-            }
-            std::sort(ms_r, ms_r + TIMED);
-            med = 0.5f * (ms_r[TIMED / 2 - 1] + ms_r[TIMED / 2]);
+        if (ok_c[c]) {
+            float* m = ms_all[c];
+            std::sort(m, m + SWEEPS * TIMED);
+            med = 0.5f * (m[SWEEPS * TIMED / 2 - 1] + m[SWEEPS * TIMED / 2]);
         }
-        if (keep_s) cudaMemcpyAsync(S, save, n * sizeof(double), cudaMemcpyDeviceToDevice, s);
-        fc.tune_ms[c] = ok ? med : -1.0f;
-        if (ok && med >= 0 && med < best) {
+        fc.tune_ms[c] = ok_c[c] ? med : -1.0f;
+        if (ok_c[c] && med >= 0 && med < best) {
             best = med;
             best_cfg = c;
         }
