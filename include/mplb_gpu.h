@@ -39,9 +39,10 @@
 extern "C" {
 #endif
 
-#define MPLB_ABI_VERSION 5  /* 2: mplb_field_desc.alpha_1/alpha_2, mplb_opts.rank; 3: mplb_gpu_copy_nodes;
+#define MPLB_ABI_VERSION 6  /* 2: mplb_field_desc.alpha_1/alpha_2, mplb_opts.rank; 3: mplb_gpu_copy_nodes;
                                4: mplb_info.tile_ms[16], MPLB_E_TIMEOUT;
-                               5: mplb_batch_filter, mplb_batch_average, mplb_mlp_init_column(_mass) */
+                               5: mplb_batch_filter, mplb_batch_average, mplb_mlp_init_column(_mass);
+                               6: mplb_gpu_set_owned, mplb_gpu_add_mirror, mplb_gpu_clear_mirrors */
 #define MPLB_MAX_Q 15
 #define MPLB_MAX_PATCHES 64
 
@@ -319,6 +320,37 @@ int mplb_gpu_copy_nodes(mplb_gpu_t* dst, uint32_t dst_start, mplb_gpu_t* src, ui
  * collision, as mplb_gpu_step does.  Device to device, ordered on the
  * handles' streams as mplb_gpu_copy_nodes. */
 int mplb_gpu_copy_state(mplb_gpu_t* dst, uint32_t dst_start, mplb_gpu_t* src, uint32_t src_start, uint32_t count);
+
+/* Slabs on the fused path with the halo written by the step kernels
+ * themselves.  No counterpart in the reference; they replace its
+ * sendPdfField / recvPdfField exchange (src/lbEquation/general/
+ * sendPdfField.c:7-102, recvPdfField.c:7-54) for slabs on the fused path.
+ *
+ * mplb_gpu_set_owned: a fused step stores the outputs of nodes
+ * [start, start + count) only (count 0: every node, the default); the other
+ * nodes are this handle's halo, written by its neighbours.
+ *
+ * mplb_gpu_add_mirror: every fused step of h also stores the outputs of its
+ * owned nodes [src_start, src_start + count) (the post-collision populations
+ * of every updated field, and T and U where the step writes them) into nodes
+ * [dst_start, dst_start + count) of dst's next-step input buffers -- the
+ * state mplb_gpu_copy_state copies, written by the kernel instead of by
+ * copies between the steps.  At most two ranges per handle; the target
+ * range must lie outside dst's owned range (set that first); dst on another
+ * GPU takes plain peer stores (peer access is enabled here).  dst must
+ * outlive h's mirrors (mplb_gpu_clear_mirrors drops them).
+ *
+ * Rules for the stepping: a handle with mirrors takes one step per
+ * mplb_gpu_step call; linked handles take their steps in turn (a neighbour
+ * must be at the same time or one step ahead, else MPLB_E_STATE); each step
+ * is queued after the neighbours' queued work and before their next step
+ * (events between the handles' streams; nothing on one stream).  The halo
+ * must hold the neighbours' fused state before the first mirrored step, and
+ * again after any call that brings a handle back to the reference's state
+ * (a download, an operator): exchange it once with mplb_gpu_copy_state. */
+int mplb_gpu_set_owned(mplb_gpu_t* h, uint32_t start, uint32_t count);
+int mplb_gpu_add_mirror(mplb_gpu_t* h, uint32_t src_start, uint32_t count, mplb_gpu_t* dst, uint32_t dst_start);
+int mplb_gpu_clear_mirrors(mplb_gpu_t* h);
 
 /* Several ranks' lattices driven from one process (one handle per rank, on
  * one GPU or several), each holding its owned nodes and its ghost nodes (no

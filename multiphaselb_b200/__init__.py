@@ -71,6 +71,9 @@ def load_library(path=LIB_PATH):
         "mplb_gpu_sync": ([H], C.c_int),
         "mplb_gpu_copy_nodes": ([H, C.c_uint32, H, C.c_uint32, C.c_uint32, C.c_int32], C.c_int),
         "mplb_gpu_copy_state": ([H, C.c_uint32, H, C.c_uint32, C.c_uint32], C.c_int),
+        "mplb_gpu_set_owned": ([H, C.c_uint32, C.c_uint32], C.c_int),
+        "mplb_gpu_add_mirror": ([H, C.c_uint32, C.c_uint32, H, C.c_uint32], C.c_int),
+        "mplb_gpu_clear_mirrors": ([H], C.c_int),
         "mplb_ranks_initialize": ([C.POINTER(H), C.c_uint32, C.POINTER(abi.GhostRun), C.c_uint32], C.c_int),
         "mplb_ranks_step": ([C.POINTER(H), C.c_uint32, C.POINTER(abi.GhostRun), C.c_uint32, C.c_uint32], C.c_int),
         "mplb_gpu_snapshot": ([H, C.c_int32], C.c_int),
@@ -263,6 +266,19 @@ class Lattice:
         [dst_start, ...) of this Lattice, device to device: the halo exchange
         of slabs run on the fused path."""
         self._check(self.lib.mplb_gpu_copy_state(self.h, dst_start, src.h, src_start, count))
+
+    def set_owned(self, start, count):
+        """Fused steps store the outputs of nodes [start, start + count) only
+        (the rest is the halo its neighbours write)."""
+        self._check(self.lib.mplb_gpu_set_owned(self.h, start, count))
+
+    def add_mirror(self, src_start, count, dst, dst_start):
+        """Fused steps also store the outputs of owned nodes [src_start, ...)
+        into nodes [dst_start, ...) of `dst`'s next-step input (its halo)."""
+        self._check(self.lib.mplb_gpu_add_mirror(self.h, src_start, count, dst.h, dst_start))
+
+    def clear_mirrors(self):
+        self._check(self.lib.mplb_gpu_clear_mirrors(self.h))
 
     def set_rho0(self, r):
         self._check(self.lib.mplb_gpu_set_rho0(self.h, r))

@@ -41,6 +41,19 @@ struct BCProg {
     uint8_t gp[FUSED_MAX_OPS];                      // patch index of a fixedT op
 };
 
+// Slabs on the fused path (mplb_gpu_add_mirror): the step outputs of owned
+// nodes [lo, lo + cnt) are also stored into nodes [dst, dst + cnt) of a
+// neighbouring slab's next-step input buffers (its halo); f / g / T / U are
+// that slab's arrays (stride n_dst per component), NULL when not mirrored.
+struct MirrorRange {
+    uint32_t lo, cnt, dst, n_dst;
+    double* f;
+    double* g;
+    double* T;
+    double* U;
+};
+constexpr int MPLB_MAX_MIRRORS = 2;
+
 struct FusedArgs {
     int nx, ny, nz;
     int px, py, pz;     // 1 = periodic axis
@@ -63,6 +76,9 @@ struct FusedArgs {
     int* kerr;             // kernel-side error flag (a bounded wait that ran out), read by the host
     double* rho_a;         // myMRT thermal field: rho_n and sum g''_n of every node (k_pullsum_d2q9)
     double* gsum_a;
+    uint32_t own_lo, own_cnt;  // a step stores the outputs of nodes [own_lo, own_lo + own_cnt) only
+    int nmirror;               // slabs: mirrored ranges in mirror[0 .. nmirror)
+    MirrorRange mirror[MPLB_MAX_MIRRORS];
     double Twall[MPLB_MAX_PATCHES];
     BCProg prog[FUSED_MAX_PROGS];
 };
@@ -322,6 +338,9 @@ __device__ __forceinline__ void finish_node(const Params& P, const FusedArgs& A,
                                             double* f, double* g, double rho, double rr, double T, double psi,
                                             PsiAt nbpsi, double src_heat) {
     const uint32_t n = P.n;
+    // slabs: a halo node's step outputs are stored by the neighbour that owns it
+    if constexpr (!EMIT)
+        if (id - A.own_lo >= A.own_cnt) return;
     double Fi[3] = {0, 0, 0}, Ft[3], U[3];
     if constexpr (F_ON) {
         force_velocity<L>(P, onb, f, rho, rr, psi, nbpsi, Fi, Ft, U);
@@ -377,6 +396,25 @@ __device__ __forceinline__ void finish_node(const Params& P, const FusedArgs& A,
         for (int k = 0; k < 9; k++) A.gout[(size_t)k * n + id] = g[k];
         A.Tnew[id] = T;
         A.S[id] = src_heat;
+    }
+    // slabs: the same outputs into a neighbour's halo (the input of its next step)
+    for (int m = 0; m < A.nmirror; m++) {
+        const MirrorRange& M = A.mirror[m];
+        if (id - M.lo >= M.cnt) continue;
+        const size_t d = (size_t)M.dst + (id - M.lo), nd = M.n_dst;
+        if constexpr (F_ON) {
+#pragma unroll
+            for (int k = 0; k < L::Q; k++) M.f[(size_t)k * nd + d] = f[k];
+            if constexpr (G_ON) {
+                M.U[d] = U[0];
+                M.U[nd + d] = U[1];
+            }
+        }
+        if constexpr (G_ON) {
+#pragma unroll
+            for (int k = 0; k < 9; k++) M.g[(size_t)k * nd + d] = g[k];
+            M.T[d] = T;
+        }
     }
 }
 

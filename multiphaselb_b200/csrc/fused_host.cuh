@@ -346,6 +346,9 @@ inline int fused_setup(FusedConfig& fc, int lat, const int* model, const Params&
     A.px = per[0];
     A.py = per[1];
     A.pz = lat == MPLB_D3Q15 ? per[2] : 1;
+    A.own_lo = 0;
+    A.own_cnt = P.n;  // every node's outputs stored; slabs narrow it (mplb_gpu_set_owned)
+    A.nmirror = 0;
     // Node programs: for every node, the ops of every patch holding it, in
     // patch order, per field.  Identical programs share one table entry.
     const uint32_t n = P.n;

@@ -148,6 +148,16 @@ struct mplb_gpu {
     std::string writer_err;
     int tile_request = 0;  // mplb_opts.tile_config
     uint32_t current = 0;
+    // slabs on the fused path: the owned nodes (count 0 = every node), the
+    // owned ranges whose step outputs also go into a neighbour's halo, and an
+    // event that orders this handle's stream before a neighbour's next step
+    uint32_t own_start = 0, own_count = 0;
+    struct Mirror {
+        uint32_t src_start, count, dst_start;
+        mplb_gpu* dst;
+    } mirrors[MPLB_MAX_MIRRORS] = {};
+    int nmirror = 0;
+    cudaEvent_t order_ev = nullptr;
     uint64_t launches = 0;
     uint64_t bytes = 0;
     bool initialized = false;
@@ -717,6 +727,59 @@ int kernel_flag_status(mplb_gpu* h) {
                                 "complete); the steps before this call are not valid");
 }
 
+// Order `waiter`'s stream after the work queued so far on `h`'s stream (no
+// host wait; nothing to do on one stream).
+int order_streams(mplb_gpu* h, mplb_gpu* waiter) {
+    if (h->dev == waiter->dev && h->stream == waiter->stream) return 0;
+    {
+        DeviceGuard guard(h->dev);
+        if (!h->order_ev) CK(cudaEventCreateWithFlags(&h->order_ev, cudaEventDisableTiming));
+        CK(cudaEventRecord(h->order_ev, h->stream));
+    }
+    DeviceGuard guard(waiter->dev);
+    CK(cudaStreamWaitEvent(waiter->stream, h->order_ev, 0));
+    return 0;
+}
+
+// Slabs: the mirrored ranges of this step.  A neighbour that has not yet
+// taken this step (same time) receives into the buffers its step writes and
+// the step after reads; one that has (one step ahead) into its current
+// buffers.  This handle's step is queued after the neighbours' queued work:
+// their last step reads and writes the buffers this step writes into, and
+// wrote this handle's halo.
+int mirror_args(mplb_gpu* h, FusedArgs& A, bool fon, bool gon) {
+    const bool udb = fon && gon;
+    A.nmirror = h->nmirror;
+    for (int m = 0; m < h->nmirror; m++) {
+        const mplb_gpu::Mirror& M = h->mirrors[m];
+        mplb_gpu* d = M.dst;
+        if (d->path != MPLB_PATH_FUSED || d->fstate == 0)
+            return fail(MPLB_E_STATE, "a mirror's neighbour is not in the fused state (exchange its state once, "
+                                      "mplb_gpu_copy_state, before the first mirrored step)");
+        if (d->current != h->current && d->current != h->current + 1)
+            return fail(MPLB_E_STATE, "a mirror's neighbour is not at this step's time or one step ahead (linked "
+                                      "slabs take one step each, in turn)");
+        const int nx = d->current == h->current ? 1 : 0;  // 1: the buffers its coming step writes
+        MirrorRange& R = A.mirror[m];
+        R.lo = M.src_start;
+        R.cnt = M.count;
+        R.dst = M.dst_start;
+        R.n_dst = d->n;
+        R.f = fon ? d->pdf[0][d->cur[0] ^ nx] : nullptr;
+        R.g = gon ? d->pdf[1][d->cur[1] ^ nx] : nullptr;
+        R.T = gon ? (nx ? d->T2 : d->T) : nullptr;
+        R.U = udb ? (nx ? d->U2 : d->U) : nullptr;
+        RET(order_streams(d, h));
+    }
+    return 0;
+}
+
+// ... and the neighbours' next steps after this one (it wrote their halos).
+int mirror_order_after(mplb_gpu* h) {
+    for (int m = 0; m < h->nmirror; m++) RET(order_streams(h, h->mirrors[m].dst));
+    return 0;
+}
+
 // One fused time step, or (emit) the rebuild of the reference state after
 // the last step from that step's retained input buffers.
 int fused_step(mplb_gpu* h, bool emit) {
@@ -741,6 +804,11 @@ int fused_step(mplb_gpu* h, bool emit) {
     A.rho_out = h->rho;
     A.Fi_out = h->Fi;
     A.Ft_out = h->Ft;
+    if (!emit && h->own_count) {
+        A.own_lo = h->own_start;
+        A.own_cnt = h->own_count;
+    }
+    if (!emit && h->nmirror) RET(mirror_args(h, A, fon, gon));
     if (!emit && !h->fc.tuned) {
         if (h->tile_request == 0) {
             RET(staging(h, h->n));
@@ -758,6 +826,7 @@ int fused_step(mplb_gpu* h, bool emit) {
     cudaError_t e = fused_launch(h->fc, h->P, A, h->lat, fon, gon, emit, h->stream);
     h->launches++;
     if (e != cudaSuccess) return fail(MPLB_E_CUDA, std::string("fused kernel launch: ") + cudaGetErrorString(e));
+    if (!emit && h->nmirror) RET(mirror_order_after(h));
     if (!emit) {
         if (fon) h->cur[0] ^= 1;
         if (gon) {
@@ -1152,6 +1221,7 @@ int mplb_gpu_destroy(mplb_gpu_t* h) {
         cudaStreamSynchronize(h->snap_stream);
         cudaStreamDestroy(h->snap_stream);
     }
+    if (h->order_ev) cudaEventDestroy(h->order_ev);
     if (h->snap_ready) cudaEventDestroy(h->snap_ready);
     if (h->snap_done) cudaEventDestroy(h->snap_done);
     if (h->snap_dev) cudaFree(h->snap_dev);
@@ -1238,6 +1308,9 @@ int mplb_gpu_step(mplb_gpu_t* h, uint32_t nsteps) {
         return 0;
     }
     if (h->path == MPLB_PATH_FUSED) {
+        if (h->nmirror && nsteps > 1)
+            return fail(MPLB_E_STATE, "a handle with mirrored ranges takes one step per call (its neighbours "
+                                      "step in between)");
         RET(enter_fused(h));  // prologue: the first collision of the loop, on the reference state
         for (uint32_t s = 0; s < nsteps; s++) RET(fused_step(h, false));
         h->current += nsteps;
@@ -1807,6 +1880,58 @@ int mplb_gpu_copy_state(mplb_gpu_t* dst, uint32_t dst_start, mplb_gpu_t* src, ui
     parts[np++] = NodeCopy{dst->T, src->T, 1};
     parts[np++] = NodeCopy{dst->U, src->U, 3};
     return copy_node_rows(dst, dst_start, src, src_start, count, parts, np);
+}
+
+int mplb_gpu_set_owned(mplb_gpu_t* h, uint32_t start, uint32_t count) {
+    if (!h) return fail(MPLB_E_ARG, "NULL handle");
+    if (h->path != MPLB_PATH_FUSED || h->precision != MPLB_FP64)
+        return fail(MPLB_E_UNSUPPORTED, "an owned range needs a handle on the fused FP64 path");
+    if ((uint64_t)start + count > h->n) return fail(MPLB_E_ARG, "node range out of bounds");
+    for (int m = 0; m < h->nmirror; m++)
+        if (h->mirrors[m].src_start < start || (uint64_t)h->mirrors[m].src_start + h->mirrors[m].count >
+                                                   (uint64_t)start + (count ? count : h->n))
+            return fail(MPLB_E_ARG, "a mirrored range lies outside the owned range");
+    h->own_start = count ? start : 0;
+    h->own_count = count;
+    return 0;
+}
+
+int mplb_gpu_add_mirror(mplb_gpu_t* h, uint32_t src_start, uint32_t count, mplb_gpu_t* dst, uint32_t dst_start) {
+    if (!h || !dst) return fail(MPLB_E_ARG, "NULL handle");
+    if (h == dst) return fail(MPLB_E_ARG, "a handle cannot mirror into itself");
+    if (h->path != MPLB_PATH_FUSED || dst->path != MPLB_PATH_FUSED || h->precision != MPLB_FP64 ||
+        dst->precision != MPLB_FP64)
+        return fail(MPLB_E_UNSUPPORTED, "mirrors need two handles on the fused FP64 path");
+    if (dst->lat != h->lat || dst->model[0] != h->model[0] || dst->model[1] != h->model[1] ||
+        dst->P.f_update != h->P.f_update || dst->P.g_update != h->P.g_update)
+        return fail(MPLB_E_ARG, "the lattices or field options differ");
+    if (h->nmirror >= MPLB_MAX_MIRRORS) return fail(MPLB_E_ARG, "at most two mirrored ranges per handle");
+    if (count == 0) return fail(MPLB_E_ARG, "empty range");
+    if ((uint64_t)src_start + count > h->n || (uint64_t)dst_start + count > dst->n)
+        return fail(MPLB_E_ARG, "node range out of bounds");
+    const uint64_t olo = h->own_start, ohi = olo + (h->own_count ? h->own_count : h->n);
+    if (src_start < olo || (uint64_t)src_start + count > ohi)
+        return fail(MPLB_E_ARG, "the mirrored range lies outside this handle's owned range");
+    const uint64_t dlo = dst->own_start, dhi = dlo + (dst->own_count ? dst->own_count : dst->n);
+    if ((uint64_t)dst_start < dhi && dlo < (uint64_t)dst_start + count)
+        return fail(MPLB_E_ARG, "the target range overlaps the neighbour's owned range (set it first)");
+    if (dst->dev != h->dev) {
+        DeviceGuard guard(h->dev);
+        int can = 0;
+        CK(cudaDeviceCanAccessPeer(&can, h->dev, dst->dev));
+        if (!can) return fail(MPLB_E_UNSUPPORTED, "the neighbour's GPU is not reachable from this one");
+        cudaError_t e = cudaDeviceEnablePeerAccess(dst->dev, 0);
+        if (e == cudaErrorPeerAccessAlreadyEnabled) cudaGetLastError();
+        else CK(e);
+    }
+    h->mirrors[h->nmirror++] = mplb_gpu::Mirror{src_start, count, dst_start, dst};
+    return 0;
+}
+
+int mplb_gpu_clear_mirrors(mplb_gpu_t* h) {
+    if (!h) return fail(MPLB_E_ARG, "NULL handle");
+    h->nmirror = 0;
+    return 0;
 }
 
 }  // extern "C"

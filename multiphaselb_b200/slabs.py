@@ -611,13 +611,28 @@ class FusedSlabRun:
 
     HALO = 2
 
-    def __init__(self, case: Case, nslabs: int, device: int = -1, stream=None, tile_config: int = 0):
+    def __init__(self, case: Case, nslabs: int, device: int = -1, stream=None, tile_config: int = 0,
+                 mirror: bool = False):
+        """mirror=True: the step kernels write the halo themselves
+        (mplb_gpu_set_owned, mplb_gpu_add_mirror): every slab stores its owned
+        nodes only and also stores its two planes next to each cut into the
+        neighbour's next-step input, so a step is one kernel per slab and no
+        copies; the halo is exchanged with copies only before the first step
+        and after a gather (which brings the handles back to the reference's
+        state)."""
         from . import Lattice, PATH_FUSED
         self.case, self.nslabs = case, nslabs
         self.nplanes, self.plane, self.periodic = _box_geometry(case)
         self.slabs = fused_slab_parts(case, nslabs, self.HALO)
+        self.mirror = mirror
+        self._primed = False
         for s in self.slabs:
             s["lat"] = Lattice(s["case"], path=PATH_FUSED, device=device, stream=stream, tile_config=tile_config)
+        if mirror:
+            for s in self.slabs:
+                s["lat"].set_owned(s["own0"], s["nown"])
+            for d, dn, src, sn, cnt in self.exchanges():
+                self.slabs[src]["lat"].add_mirror(sn, cnt, self.slabs[d]["lat"], dn)
 
     def exchanges(self):
         """(destination slab, destination node, source slab, source node, nodes)
@@ -628,6 +643,7 @@ class FusedSlabRun:
         for s in self.slabs:
             s["lat"].upload_case()
             s["lat"].initialize()
+        self._primed = False
 
     def exchange(self):
         """Halo planes of every slab from its neighbours' owned planes."""
@@ -636,7 +652,9 @@ class FusedSlabRun:
 
     def step(self, n=1):
         for _ in range(n):
-            self.exchange()
+            if not self.mirror or not self._primed:
+                self.exchange()
+                self._primed = True
             for s in self.slabs:
                 s["lat"].step(1)
 
@@ -646,6 +664,7 @@ class FusedSlabRun:
 
     def gather(self):
         """The reference state of the whole box: every slab's owned planes."""
+        self._primed = False  # the downloads bring the handles back to the reference's state
         out = {}
         for s in self.slabs:
             d = s["lat"].download()

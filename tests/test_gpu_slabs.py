@@ -121,6 +121,54 @@ def test_fused_slabs_match_oracle(gpu_lib, name, ranks):
         assert_same(run.gather(), run_checker("port", case, 24), fields=fields, ctx=f"{name} in {ranks} fused slabs @24")
 
 
+@pytest.mark.parametrize("name,ranks", FUSED_SLAB_CASES)
+def test_fused_slabs_mirror_match_oracle(gpu_lib, name, ranks):
+    """Slabs whose step kernels write the neighbours' halos themselves
+    (mplb_gpu_set_owned, mplb_gpu_add_mirror: no copies between the steps,
+    one exchange before the first step and after each gather) against the
+    single-domain oracle run: the owned planes bit for bit after 12 steps, and
+    after 12 more with the reference state rebuilt in between."""
+    from tests.helpers import run_checker
+    case = fused_case(name)
+    fields = [f for f in fields_of(case) if f != "S" or case.g is not None]
+    with slabs.FusedSlabRun(case, ranks, mirror=True) as run:
+        run.initialize()
+        run.step(12)
+        assert_same(run.gather(), run_checker("port", case, 12), fields=fields,
+                    ctx=f"{name} in {ranks} mirrored slabs @12")
+        run.step(12)
+        assert_same(run.gather(), run_checker("port", case, 24), fields=fields,
+                    ctx=f"{name} in {ranks} mirrored slabs @24")
+
+
+def test_mirrors_refuse(gpu_lib):
+    """Mirrored ranges: owned sources, targets outside the neighbour's owned
+    nodes, at most two, one step per call, neighbours in turn."""
+    case = small_cases()["column_d2q9"]
+    with slabs.FusedSlabRun(case, 2, mirror=True) as run:
+        a, b = run.slabs[0]["lat"], run.slabs[1]["lat"]
+        sa, sb = run.slabs[0], run.slabs[1]
+        with pytest.raises(MplbError, match="into itself"):
+            a.add_mirror(sa["own0"], 1, a, 0)
+        with pytest.raises(MplbError, match="outside this handle's owned range"):
+            a.add_mirror(sa["own0"] + sa["nown"], 1, b, 0)
+        with pytest.raises(MplbError, match="overlaps the neighbour's owned range"):
+            a.add_mirror(sa["own0"], 1, b, sb["own0"])
+        run.initialize()
+        run.step(2)
+        with pytest.raises(MplbError, match="one step per call"):
+            a.step(2)
+        a.step(1)
+        with pytest.raises(MplbError, match="one step ahead"):
+            a.step(1)
+        a.add_mirror(sa["own0"], 1, b, 0)  # the second range of slab 0 (slab 0 of a walled column has one)
+        with pytest.raises(MplbError, match="at most two"):
+            a.add_mirror(sa["own0"], 1, b, 0)
+    with Lattice(case, path=abi.PATH_OPERATORS) as op:
+        with pytest.raises(MplbError, match="fused FP64 path"):
+            op.set_owned(0, 1)
+
+
 def test_copy_state_refuses(gpu_lib):
     """State copies need two fused FP64 handles of the same lattice and options."""
     a_case = small_cases()["column_d2q9"]
