@@ -759,6 +759,9 @@ int mirror_args(mplb_gpu* h, FusedArgs& A, bool fon, bool gon) {
         if (d->current != h->current && d->current != h->current + 1)
             return fail(MPLB_E_STATE, "a mirror's neighbour is not at this step's time or one step ahead (linked "
                                       "slabs take one step each, in turn)");
+        const uint64_t dlo = d->own_start, dhi = dlo + (d->own_count ? d->own_count : d->n);
+        if ((uint64_t)M.dst_start < dhi && dlo < (uint64_t)M.dst_start + M.count)
+            return fail(MPLB_E_STATE, "a mirror's target overlaps the neighbour's owned range");
         const int nx = d->current == h->current ? 1 : 0;  // 1: the buffers its coming step writes
         MirrorRange& R = A.mirror[m];
         R.lo = M.src_start;

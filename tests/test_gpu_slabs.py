@@ -164,6 +164,10 @@ def test_mirrors_refuse(gpu_lib):
         a.add_mirror(sa["own0"], 1, b, 0)  # the second range of slab 0 (slab 0 of a walled column has one)
         with pytest.raises(MplbError, match="at most two"):
             a.add_mirror(sa["own0"], 1, b, 0)
+        b.set_owned(0, sb["own0"] + sb["nown"])  # now the targets lie in b's owned nodes
+        with pytest.raises(MplbError, match="overlaps the neighbour's owned range"):
+            b.step(1)
+            a.step(1)
     with Lattice(case, path=abi.PATH_OPERATORS) as op:
         with pytest.raises(MplbError, match="fused FP64 path"):
             op.set_owned(0, 1)
