@@ -181,6 +181,33 @@ def test_one_process_per_slab_gloo(tmp_path, name, world):
 
 @pytest.mark.parametrize("R", [2, 3, 4])
 @pytest.mark.parametrize("name", ["column_d2q9", "bubble_d2q9", "walls_d3q15"])
+def test_fused_slab_mirror_plan(name, R):
+    """FusedSlabRun(mirror=True) turns every halo copy into a mirrored range
+    of its source slab (mplb_gpu_add_mirror): at most two per slab (the
+    library's limit), each inside its slab's owned nodes, each target outside
+    the destination's owned nodes, and every halo node of every slab written
+    by exactly one range, so no two kernels store the same node in a step."""
+    case = small_cases()[name]
+    nplanes, plane, periodic = slabs._box_geometry(case)
+    if nplanes < 3 * R:
+        return
+    parts = slabs.fused_slab_parts(case, R, 2)
+    per_src = [0] * R
+    writes = [np.zeros(p["case"].n, dtype=int) for p in parts]
+    for d, dn, s, sn, c in slabs.halo_copies(parts, R, plane, 2):
+        per_src[s] += 1
+        assert parts[s]["own0"] <= sn and sn + c <= parts[s]["own0"] + parts[s]["nown"]
+        assert dn + c <= parts[d]["own0"] or dn >= parts[d]["own0"] + parts[d]["nown"]
+        writes[d][dn:dn + c] += 1
+    assert max(per_src) <= 2
+    for p, w in zip(parts, writes):
+        own = np.zeros(p["case"].n, dtype=bool)
+        own[p["own0"]:p["own0"] + p["nown"]] = True
+        assert np.all(w[own] == 0) and np.all(w[~own] == 1)
+
+
+@pytest.mark.parametrize("R", [2, 3, 4])
+@pytest.mark.parametrize("name", ["column_d2q9", "bubble_d2q9", "walls_d3q15"])
 def test_fused_slab_plan(name, R):
     """FusedSlabRun's plan: the owned planes cover the box once in order,
     every halo copy fills halo nodes from owned nodes of the same global
