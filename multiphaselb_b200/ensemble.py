@@ -12,7 +12,9 @@ interval of K steps.
 Two ways to get there are timed:
 
 * plain: each case alone, FP64, fused path, tanh/Maxwell initial profile,
-  one case after the other (mplb_gpu_run_to_equilibrium);
+  one case after the other (mplb_gpu_run_to_equilibrium), on the tile the
+  autotuner keeps for its lattice (found on a throwaway handle outside the
+  timed region, so the plain wall times hold no tuning);
 * batched: all cases as FP32-deviation lattices advanced together
   (mplb_batch_run), initial profile from the tanh/Maxwell formula or from the
   learned warm start (multiphaselb_b200.warmstart).
@@ -56,11 +58,22 @@ def coexistence(case, rho):
     return float(rho[cx + nx * cy]), float(rho[0])
 
 
+def tuned_tile(case):
+    """The tile candidate the autotuner keeps for this lattice, as a
+    Lattice tile_config (1-based), found on a throwaway handle."""
+    with Lattice(case, path=abi.PATH_FUSED, precision=abi.FP64) as lat:
+        lat.upload_case()
+        lat.initialize()
+        lat.step(1)
+        return lat.info()["tile_config"] + 1
+
+
 def run_plain(specs, K, tol, max_steps, log=None):
     out = []
     for i, s in enumerate(specs):
         c = make_case(s)
-        with Lattice(c, path=abi.PATH_FUSED, precision=abi.FP64) as lat:
+        tile = tuned_tile(c)
+        with Lattice(c, path=abi.PATH_FUSED, precision=abi.FP64, tile_config=tile) as lat:
             lat.upload_case()
             lat.initialize()
             lat.sync()
